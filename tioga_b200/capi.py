@@ -1,0 +1,178 @@
+"""ctypes mirror of TIOGA's C API (src/tiogaInterface.C:36-328).
+
+``TiogaLibrary`` binds any shared library that exports the TIOGA symbols:
+this package's GPU library, the C restatement in ``oracle/`` or the compiled
+reference.  The call sequence a solver makes is the reference's own:
+
+    init -> registergrid_data_mb (per block) -> preprocess_grids ->
+    performconnectivity -> registersolution (per block) -> dataupdate_mb
+
+Scalars are passed by pointer and connectivity is 1-based, exactly as TIOGA
+expects; ``registergrid_data_mb`` forwards its cell types as the trailing
+varargs triples ``(int *nv, int *nc, int *vconn)``.  The library keeps the
+caller's pointers (src/MeshBlock.C:37-72), so this class owns the arrays for
+as long as the library may read them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_P = C.c_void_p
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _iref(v: int):
+    return C.byref(C.c_int(int(v)))
+
+
+class TiogaLibrary:
+    """One loaded TIOGA-ABI library with its registered system."""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.lib = C.CDLL(path, mode=C.RTLD_LOCAL)
+        self._keep = []          # arrays the library points into
+        self.blocks = {}         # tag -> dict of host arrays
+        self._order = []         # tags in registration order
+
+    # -- lifecycle ---------------------------------------------------------
+    def init(self):
+        self.lib.tioga_init_.argtypes = [C.c_int]
+        self.lib.tioga_init_.restype = None
+        self.lib.tioga_init_(C.c_int(91))
+
+    def delete(self):
+        self.lib.tioga_delete_()
+        self._keep.clear()
+        self.blocks.clear()
+        self._order.clear()
+
+    # -- registration ------------------------------------------------------
+    def registergrid_data_mb(self, bid: int, block):
+        """Register one cases.Block under block id ``bid`` (1-based)."""
+        x = np.ascontiguousarray(block.x, dtype=np.float64).reshape(-1)
+        ibl = np.ones(block.nnodes, dtype=np.int32)
+        wbc = np.ascontiguousarray(block.wbc, dtype=np.int32) + 1
+        obc = np.ascontiguousarray(block.obc, dtype=np.int32) + 1
+        conns = []
+        args = []
+        for nv, conn in block.cells:
+            c1 = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1) + 1
+            conns.append(c1)
+            nvc = C.c_int(int(nv))
+            ncc = C.c_int(int(conn.shape[0]))
+            self._keep += [nvc, ncc]
+            args += [C.byref(nvc), C.byref(ncc), _ptr(c1)]
+        self._keep += [x, ibl, wbc, obc] + conns
+        cbid, ctag, cnn = C.c_int(bid), C.c_int(block.tag), C.c_int(block.nnodes)
+        cnw, cno, cnt = C.c_int(len(wbc)), C.c_int(len(obc)), C.c_int(len(block.cells))
+        self._keep += [cbid, ctag, cnn, cnw, cno, cnt]
+        self.lib.tioga_registergrid_data_mb_(
+            C.byref(cbid), C.byref(ctag), C.byref(cnn), _ptr(x), _ptr(ibl),
+            C.byref(cnw), C.byref(cno), _ptr(wbc), _ptr(obc), C.byref(cnt), *args)
+        self.blocks[block.tag] = {"x": x, "iblank": ibl, "nnodes": block.nnodes,
+                                  "ncells": block.ncells, "bid": bid}
+        if block.tag not in self._order:
+            self._order.append(block.tag)
+
+    def register_system(self, system):
+        for bid, b in enumerate(system.blocks, start=1):
+            self.registergrid_data_mb(bid, b)
+
+    # -- settings ----------------------------------------------------------
+    def setsymmetry(self, isym: int):
+        self.lib.tioga_setsymmetry_(_iref(isym))
+
+    def setnfringe(self, nfringe: int):
+        self.lib.tioga_setnfringe_(_iref(nfringe))
+
+    def setmexclude(self, mexclude: int):
+        self.lib.tioga_setmexclude_(_iref(mexclude))
+
+    def setresolutions_multi(self, tag: int, nres: np.ndarray, cres: np.ndarray):
+        nres = np.ascontiguousarray(nres, dtype=np.float64)
+        cres = np.ascontiguousarray(cres, dtype=np.float64)
+        self._keep += [nres, cres]
+        self.lib.tioga_setresolutions_multi_(_iref(tag), _ptr(nres), _ptr(cres))
+
+    # -- the hot path ------------------------------------------------------
+    def preprocess_grids(self):
+        self.lib.tioga_preprocess_grids_()
+
+    def performconnectivity(self):
+        self.lib.tioga_performconnectivity_()
+
+    def registersolution(self, tag: int, q: np.ndarray):
+        assert q.dtype == np.float64 and q.flags.c_contiguous
+        self._keep.append(q)
+        self.lib.tioga_registersolution_(_iref(tag), _ptr(q))
+
+    def dataupdate_mb(self, nvar: int, itype: str = "row"):
+        s = C.create_string_buffer(itype.encode())
+        self.lib.tioga_dataupdate_mb_(_iref(nvar), s)
+
+    # -- queries -----------------------------------------------------------
+    def getdonorcount(self, tag: int):
+        d, f = C.c_int(0), C.c_int(0)
+        self.lib.tioga_getdonorcount_(_iref(tag), C.byref(d), C.byref(f))
+        return d.value, f.value
+
+    def getdonorinfo(self, tag: int):
+        """Returns (receptors (dcount,4), indices (fcount,), frac (fcount,))."""
+        d, f = self.getdonorcount(tag)
+        rec = np.zeros(4 * max(d, 1), dtype=np.int32)
+        ind = np.zeros(max(f, 1), dtype=np.int32)
+        frac = np.zeros(max(f, 1), dtype=np.float64)
+        dc = C.c_int(d)
+        if d > 0:
+            self.lib.tioga_getdonorinfo_(_iref(tag), _ptr(rec), _ptr(ind), _ptr(frac), C.byref(dc))
+        return rec[:4 * d].reshape(d, 4), ind[:f], frac[:f]
+
+    def iblank(self, tag: int) -> np.ndarray:
+        return self.blocks[tag]["iblank"]
+
+    @property
+    def tags(self):
+        return list(self._order)
+
+
+def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str = "row",
+               isym=None, nfringe=None, mexclude=None, resolutions=None):
+    """Drive one library through the full north-star sequence and collect
+    every observable: iblank per block, donor info per block and the updated
+    fields.  ``q_blocks`` are copied (the library updates them in place)."""
+    t = TiogaLibrary(lib_path)
+    t.init()
+    t.register_system(system)
+    if isym is not None:
+        t.setsymmetry(isym)
+    if nfringe is not None:
+        t.setnfringe(nfringe)
+    if mexclude is not None:
+        t.setmexclude(mexclude)
+    if resolutions is not None:
+        for tag, (nres, cres) in resolutions.items():
+            t.setresolutions_multi(tag, nres, cres)
+    t.preprocess_grids()
+    t.performconnectivity()
+    out = {"iblank": {}, "donors": {}, "q": {}}
+    for b in system.blocks:
+        out["iblank"][b.tag] = t.iblank(b.tag).copy()
+        out["donors"][b.tag] = t.getdonorinfo(b.tag)
+    if q_blocks is not None:
+        qs = [np.array(q, dtype=np.float64, copy=True) for q in q_blocks]
+        for b, q in zip(system.blocks, qs):
+            t.registersolution(b.tag, q)
+        t.dataupdate_mb(nvar, itype)
+        for b, q in zip(system.blocks, qs):
+            out["q"][b.tag] = q
+    t.delete()
+    return out
