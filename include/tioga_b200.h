@@ -1,0 +1,122 @@
+/*
+ * tioga_b200 -- the TIOGA overset-connectivity C API on a B200 GPU.
+ *
+ * libtioga_b200.so exports the symbols of TIOGA's C/Fortran interface
+ * (src/tiogaInterface.C in the TIOGA sources), so a solver that links
+ * against TIOGA links against this library unchanged.  Every scalar is passed
+ * by pointer (Fortran binding), connectivity and boundary-node lists are
+ * 1-based, and every array stays the caller's: the library keeps the
+ * pointers and reads coordinates again at each preprocess/connectivity call.
+ * All mesh blocks live on one GPU; TIOGA's MPI exchanges are device-buffer
+ * hand-offs inside the library.
+ *
+ * Errors: the TIOGA functions return void, as in TIOGA.  A failure prints a
+ * "#tioga_b200:" line on stderr and is kept for tioga_b200_last_error().
+ * The library never aborts the process and never traps on the device.
+ */
+#ifndef TIOGA_B200_H
+#define TIOGA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- TIOGA's interface (src/tiogaInterface.C) -------------------------- */
+
+/* tiogaInterface.C:38 -- Fortran communicator handle; one rank, ignored. */
+void tioga_init_f90_(int *scomm);
+/* tiogaInterface.C:61 -- MPI_Comm is an int (MPICH) or a pointer (Open MPI):
+ * taken as an opaque word and ignored (one rank). */
+void tioga_init_(intptr_t comm);
+
+/* tiogaInterface.C:84-105 -- register a block; the varargs are *ntypes
+ * triples (int *nv, int *nc, int *vconn) with nv in {4,5,6,8}. */
+void tioga_registergrid_data_(int *btag, int *nnodes, double *xyz, int *ibl, int *nwbc, int *nobc,
+                              int *wbcnode, int *obcnode, int *ntypes, ...);
+/* tiogaInterface.C:108-130 -- the same with an explicit 1-based block id. */
+void tioga_registergrid_data_mb_(int *bid, int *btag, int *nnodes, double *xyz, int *ibl, int *nwbc,
+                                 int *nobc, int *wbcnode, int *obcnode, int *ntypes, ...);
+
+/* tiogaInterface.C:150-153 -- cell volumes, node resolutions, mandatory
+ * receptors, oriented boxes; sets every iblank to 1. */
+void tioga_preprocess_grids_(void);
+/* tiogaInterface.C:155-158 -- hole maps, box pairs, donor search, donor
+ * selection and cancellation; writes ibl[] in {1, 0, -1}. */
+void tioga_performconnectivity_(void);
+
+/* tiogaInterface.C:170-173 -- bind block btag's solution (host array,
+ * updated in place by the next data update). */
+void tioga_registersolution_(int *btag, double *q);
+/* tiogaInterface.C:175-216 -- interpolate nvar fields into every receptor;
+ * itype contains "row" (q[node*nvar+k]) or "column" (q[k*nnodes+node]). */
+void tioga_dataupdate_mb_(int *nvar, char *itype);
+/* tiogaInterface.C:218-224 -- TIOGA looks up mesh tag 0 here, which never
+ * exists; this library binds q to the first registered block. */
+void tioga_dataupdate_(double *q, int *nvar, char *itype);
+
+/* tiogaInterface.C:244-251 -- donor stencils held by block btag: dcount
+ * receptors and fcount = sum(nweights + 1) indices/weights. */
+void tioga_getdonorcount_(int *btag, int *dcount, int *fcount);
+/* receptors[4*i..] = {rank, receptor node, receptor block, nweights};
+ * indices: donor nodes then the donor cell id; frac: weights then 0. */
+void tioga_getdonorinfo_(int *btag, int *receptors, int *indices, double *frac, int *dcount);
+
+/* tiogaInterface.C:253-316 -- settings */
+void tioga_setsymmetry_(int *isym);
+void tioga_setresolutions_(double *nres, double *cres);
+void tioga_setresolutions_multi_(int *btag, double *nres, double *cres);
+void tioga_setcelliblank_(int *iblank_cell);
+void tioga_setnfringe_(int *nfringe);
+void tioga_setmexclude_(int *mexclude);
+/* tiogaInterface.C:317-326 */
+void tioga_delete_(void);
+
+/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
+ * p4est, high-order callbacks, fringe reduction, Tecplot output).  They are
+ * exported so that existing solvers link; each reports "not supported" and
+ * sets the last error. */
+void tioga_performconnectivity_highorder_(void);
+void tioga_performconnectivity_amr_(void);
+void tioga_set_highorder_callback_(void (*f1)(int *, int *), void (*f2)(int *, int *, double *),
+                                   void (*f3)(int *, double *, int *, double *),
+                                   void (*f4)(int *, double *, int *, int *, double *, double *, int *),
+                                   void (*f5)(int *, int *, double *, int *, int *, double *));
+void tioga_reduce_fringes_(void);
+void tioga_writeoutputfiles_(int *nvar, char *itype);
+
+/* ---- additions of this library (no counterpart in TIOGA) -------------- */
+
+/* 0 when the last call succeeded, else a negative code. */
+int tioga_b200_last_error(void);
+/* 1 when a CUDA device is present and the library initialised it. */
+int tioga_b200_device_ok(void);
+/* Search arithmetic: 0 = FP64 throughout; 1 (default) = FP32 screen of the
+ * Newton inversion with FP64 refinement of every undecided candidate.
+ * Results are identical (every accept/reject near the TOL band is FP64). */
+void tioga_b200_set_precision_(int *mode);
+/* 1: the coordinates have not moved since the last call, so connectivity
+ * skips their upload.  Default 0 (TIOGA re-reads x at every call). */
+void tioga_b200_set_coords_resident_(int *flag);
+/* Bind block btag's solution as a DEVICE array (same layout as the host
+ * one); tioga_dataupdate_mb_ then updates it without host copies. */
+void tioga_b200_registersolution_device_(int *btag, double *dq);
+/* Cell iblank of block btag (ncells ints), for any block. */
+void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
+/* Counters of the last connectivity call: [0] query points, [1] queries with
+ * a donor, [2] order-dependent ties, [3] Newton candidates, [4] FP64
+ * refinements, [5] receptors, [6] holes, [7] donor records, [8] device
+ * error bits, [9] pairs of blocks. */
+void tioga_b200_stats_(long long out[16]);
+/* Device time (ms) of the last connectivity call per phase: [0] coordinate
+ * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
+ * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,
+ * [8] total. */
+void tioga_b200_timing_(float out[16]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TIOGA_B200_H */

@@ -145,7 +145,7 @@ class TiogaLibrary:
 
 
 def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str = "row",
-               isym=None, nfringe=None, mexclude=None, resolutions=None):
+               isym=None, nfringe=None, mexclude=None, resolutions=None, setup=None, after=None):
     """Drive one library through the full north-star sequence and collect
     every observable: iblank per block, donor info per block and the updated
     fields.  ``q_blocks`` are copied (the library updates them in place)."""
@@ -161,9 +161,13 @@ def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str =
     if resolutions is not None:
         for tag, (nres, cres) in resolutions.items():
             t.setresolutions_multi(tag, nres, cres)
+    if setup is not None:
+        setup(t)
     t.preprocess_grids()
     t.performconnectivity()
     out = {"iblank": {}, "donors": {}, "q": {}}
+    if after is not None:
+        out["after"] = after(t)
     for b in system.blocks:
         out["iblank"][b.tag] = t.iblank(b.tag).copy()
         out["donors"][b.tag] = t.getdonorinfo(b.tag)

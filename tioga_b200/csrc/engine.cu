@@ -1,0 +1,968 @@
+// Host orchestration of the B200 connectivity path: preprocess, connectivity,
+// data update and the donor queries, all on one CUDA stream.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "kernels.cuh"
+
+namespace tb {
+
+static int g_last_cuda_error = 0;
+int fail(cudaError_t e) {
+  g_last_cuda_error = (int)e;
+  return -(int)e - 1000;
+}
+
+static const int kT = 256;
+
+// After every launch: a launch error is reported at once; with
+// TIOGA_B200_CHECK=1 in the environment the stream is also synchronised so a
+// fault is attributed to the kernel that caused it.
+static int sync_check() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("TIOGA_B200_CHECK");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v;
+}
+#define TB_LAUNCHED(name)                                                              \
+  do {                                                                                 \
+    cudaError_t le_ = cudaGetLastError();                                              \
+    if (le_ == cudaSuccess && sync_check()) le_ = cudaStreamSynchronize(stream_);      \
+    if (le_ != cudaSuccess) {                                                          \
+      fprintf(stderr, "#tioga_b200: kernel %s failed: %s\n", name, cudaGetErrorString(le_)); \
+      return tb::fail(le_);                                                            \
+    }                                                                                  \
+  } while (0)
+
+#define TB_TRY(call)      \
+  do {                    \
+    int rc_ = (call);     \
+    if (rc_) return rc_;  \
+  } while (0)
+
+Engine::Engine() {
+  cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+  for (auto& e : ev_) cudaEventCreate(&e);
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& e : ev_) cudaEventDestroy(e);
+  x_.release(); node_res_.release(); cell_res_.release(); iblank_.release(); iblank_cell_.release();
+  conn8_.release(); node_blk_.release(); cell_blk_.release(); cell_nv_.release(); wallf_.release();
+  obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
+  wall_list_.release(); obc_list_.release(); csr_off_.release(); csr_cell_.release(); deg_.release();
+  d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
+  for (auto& h : hm_state_) h.release();
+  wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
+  cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
+  qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
+  rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
+  reset_t_.release(); interp2rec_.release(); it_node_.release(); it_w_.release(); it_rec_.release();
+  it_don_.release(); it_nv_.release(); it_cancel_.release(); rres_.release(); q_.release();
+  qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
+  mkey_.release(); mkey_alt_.release(); mval_alt_.release();
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Engine::find_tag(int tag) const {
+  auto it = tag2idx_.find(tag);
+  return it == tag2idx_.end() ? -1 : it->second;
+}
+
+// src/tioga.C:64-86 + MeshBlock.C:37-72: one block per mesh tag; a second
+// registration of a tag replaces that block's data.  Pointers stay the
+// caller's.
+int Engine::register_block(int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
+                           int* obc, int ntypes, const int* nv, const int* nc, int** conn) {
+  if (ntypes < 1 || ntypes > 4) {
+    fprintf(stderr, "#tioga_b200: %d cell types given, 1..4 supported\n", ntypes);
+    return -1;
+  }
+  for (int t = 0; t < ntypes; t++)
+    if (nv[t] != 4 && nv[t] != 5 && nv[t] != 6 && nv[t] != 8) {
+      fprintf(stderr, "#tioga_b200: cells with %d vertices are not supported\n", nv[t]);
+      return -1;
+    }
+  if (tag < 1 || tag > 128) {
+    fprintf(stderr, "#tioga_b200: mesh tags must lie in 1..128 (got %d)\n", tag);
+    return -1;
+  }
+  int ib = find_tag(tag);
+  if (ib < 0) {
+    if ((int)hb_.size() >= 16) {
+      fprintf(stderr, "#tioga_b200: at most 16 blocks per instance\n");
+      return -1;
+    }
+    hb_.emplace_back();
+    ib = (int)hb_.size() - 1;
+    tag2idx_[tag] = ib;
+  }
+  HostBlock& b = hb_[ib];
+  b.tag = tag;
+  b.nnodes = nnodes;
+  b.hx = x;
+  b.hibl = ibl;
+  b.nwbc = nwbc;
+  b.nobc = nobc;
+  b.hwbc = wbc;
+  b.hobc = obc;
+  b.ntypes = ntypes;
+  b.ncells = 0;
+  for (int t = 0; t < 4; t++) {
+    b.nv[t] = t < ntypes ? nv[t] : 0;
+    b.nc[t] = t < ntypes ? nc[t] : 0;
+    b.hconn[t] = t < ntypes ? conn[t] : nullptr;
+    b.ncells += b.nc[t];
+  }
+  topo_dirty_ = true;
+  preprocessed_ = false;
+  connected_ = false;
+  return 0;
+}
+
+int Engine::set_resolutions(int tag, double* nres, double* cres) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].user_nres = nres;
+  hb_[ib].user_cres = cres;
+  return 0;
+}
+
+int Engine::set_cell_iblank(int tag, int* ibc) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].h_iblank_cell = ibc;
+  return 0;
+}
+
+int Engine::register_solution(int tag, double* q, bool device) {
+  int ib = find_tag(tag);
+  if (ib < 0 || !connected_) {
+    fprintf(stderr, "#tioga_b200: registersolution needs a known tag after performconnectivity\n");
+    return -1;
+  }
+  if (device) {
+    hb_[ib].dq = q;
+    hb_[ib].hq = nullptr;
+  } else {
+    hb_[ib].hq = q;
+    hb_[ib].dq = nullptr;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// topology upload (once per registration)
+// ---------------------------------------------------------------------------
+int Engine::upload_topology() {
+  const int nb = (int)hb_.size();
+  bi_.assign(nb, BlockInfo{});
+  ntot_ = 0;
+  ctot_ = 0;
+  long long nwall = 0, nobcn = 0;
+  maxtag_ = 0;
+  for (int b = 0; b < nb; b++) {
+    BlockInfo& B = bi_[b];
+    const HostBlock& H = hb_[b];
+    B.tag = H.tag;
+    B.nnodes = H.nnodes;
+    B.ncells = H.ncells;
+    B.node_off = (int)ntot_;
+    B.cell_off = (int)ctot_;
+    B.ntypes = H.ntypes;
+    B.type_off[0] = 0;
+    for (int t = 0; t < 4; t++) {
+      B.nv[t] = H.nv[t];
+      B.type_off[t + 1] = B.type_off[t] + H.nc[t];
+    }
+    B.nwbc = H.nwbc;
+    B.wall_off = (int)nwall;
+    B.nobc = H.nobc;
+    B.obc_off = (int)nobcn;
+    ntot_ += H.nnodes;
+    ctot_ += H.ncells;
+    nwall += H.nwbc;
+    nobcn += H.nobc;
+    maxtag_ = std::max(maxtag_, H.tag);
+  }
+  if (ntot_ >= (1ll << 31) || ctot_ >= (1ll << 31)) {
+    fprintf(stderr, "#tioga_b200: more than 2^31 nodes or cells\n");
+    return -1;
+  }
+  K_ = nb;
+  TB_CUDA(x_.ensure(3 * ntot_));
+  TB_CUDA(node_res_.ensure(ntot_));
+  TB_CUDA(iblank_.ensure(ntot_));
+  TB_CUDA(node_blk_.ensure(ntot_));
+  TB_CUDA(wallf_.ensure(ntot_));
+  TB_CUDA(obcf_.ensure(ntot_));
+  TB_CUDA(ex0_.ensure(ntot_));
+  TB_CUDA(ex1_.ensure(ntot_));
+  TB_CUDA(m0_.ensure(ntot_));
+  TB_CUDA(m1_.ensure(ntot_));
+  TB_CUDA(cmark_.ensure(ntot_));
+  TB_CUDA(reset_t_.ensure(ntot_));
+  TB_CUDA(cell_res_.ensure(ctot_));
+  TB_CUDA(iblank_cell_.ensure(ctot_));
+  TB_CUDA(conn8_.ensure(8 * ctot_));
+  TB_CUDA(cell_blk_.ensure(ctot_));
+  TB_CUDA(cell_nv_.ensure(ctot_));
+  TB_CUDA(wall_list_.ensure(nwall));
+  TB_CUDA(obc_list_.ensure(nobcn));
+  TB_CUDA(slot_.ensure(ntot_ * K_));
+  TB_CUDA(d_bi_.ensure(nb));
+  TB_CUDA(err_.ensure(4));
+  TB_CUDA(counters_.ensure(16));
+  TB_CUDA(cudaMemsetAsync(wallf_.p, 0, ntot_, stream_));
+  TB_CUDA(cudaMemsetAsync(obcf_.p, 0, ntot_, stream_));
+  TB_CUDA(cudaMemsetAsync(err_.p, 0, 4 * sizeof(unsigned), stream_));
+  // staging buffer for the 1-based caller arrays
+  size_t stage = 0;
+  for (auto& H : hb_) {
+    for (int t = 0; t < H.ntypes; t++) stage = std::max(stage, (size_t)H.nc[t] * H.nv[t]);
+    stage = std::max(stage, (size_t)H.nwbc);
+    stage = std::max(stage, (size_t)H.nobc);
+  }
+  DBuf<int> stg;
+  TB_CUDA(stg.ensure(stage));
+  for (int b = 0; b < nb; b++) {
+    const HostBlock& H = hb_[b];
+    const BlockInfo& B = bi_[b];
+    k_node_blk<<<grid_for(H.nnodes, kT), kT, 0, stream_>>>(B.node_off, H.nnodes, b, node_blk_.p);
+    TB_LAUNCHED("k_node_blk");
+    for (int t = 0; t < H.ntypes; t++) {
+      size_t n = (size_t)H.nc[t] * H.nv[t];
+      if (n == 0) continue;
+      TB_CUDA(cudaMemcpyAsync(stg.p, H.hconn[t], n * sizeof(int), cudaMemcpyHostToDevice, stream_));
+      k_conn_convert<<<grid_for(H.nc[t], kT), kT, 0, stream_>>>(stg.p, H.nc[t], H.nv[t], B.node_off,
+                                                                B.cell_off + B.type_off[t], b, conn8_.p,
+                                                                cell_nv_.p, cell_blk_.p);
+      TB_LAUNCHED("k_conn_convert");
+      TB_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused
+    }
+    if (H.nwbc > 0) {
+      TB_CUDA(cudaMemcpyAsync(stg.p, H.hwbc, H.nwbc * sizeof(int), cudaMemcpyHostToDevice, stream_));
+      k_mark_list<<<grid_for(H.nwbc, kT), kT, 0, stream_>>>(stg.p, H.nwbc, B.node_off, wall_list_.p,
+                                                            B.wall_off, wallf_.p);
+      TB_LAUNCHED("k_mark_list");
+      TB_CUDA(cudaStreamSynchronize(stream_));
+    }
+    if (H.nobc > 0) {
+      TB_CUDA(cudaMemcpyAsync(stg.p, H.hobc, H.nobc * sizeof(int), cudaMemcpyHostToDevice, stream_));
+      k_mark_list<<<grid_for(H.nobc, kT), kT, 0, stream_>>>(stg.p, H.nobc, B.node_off, obc_list_.p,
+                                                            B.obc_off, obcf_.p);
+      TB_LAUNCHED("k_mark_list");
+      TB_CUDA(cudaStreamSynchronize(stream_));
+    }
+  }
+  stg.release();
+  TB_TRY(build_csr());
+  // hole map state buffers for every wall-bearing tag
+  hm_state_.resize(maxtag_);
+  std::vector<HoleMapDev> hmd;
+  for (int b = 0; b < nb; b++) {
+    if (hb_[b].nwbc <= 0) continue;
+    int t = hb_[b].tag - 1;
+    const size_t cap = 197ull * 197ull * 197ull;
+    TB_CUDA(hm_state_[t].ensure(cap));
+  }
+  TB_CUDA(d_hm_.ensure(maxtag_));
+  TB_CUDA(wall_bb_.ensure(6 * maxtag_));
+  TB_CUDA(d_hmdev_.ensure(maxtag_));
+  topo_dirty_ = false;
+  interps_fetched_ = false;
+  return 0;
+}
+
+int Engine::build_csr() {
+  TB_CUDA(deg_.ensure(ntot_ + 1));
+  TB_CUDA(csr_off_.ensure(ntot_ + 1));
+  TB_CUDA(cudaMemsetAsync(deg_.p, 0, (ntot_ + 1) * sizeof(int), stream_));
+  k_csr_count<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, deg_.p);
+  TB_LAUNCHED("k_csr_count");
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, deg_.p, csr_off_.p, (int)(ntot_ + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, deg_.p, csr_off_.p, (int)(ntot_ + 1), stream_);
+  int total = 0;
+  TB_CUDA(cudaMemcpyAsync(&total, csr_off_.p + ntot_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  inc_tot_ = total;
+  TB_CUDA(csr_cell_.ensure(total));
+  TB_CUDA(cudaMemsetAsync(deg_.p, 0, (ntot_ + 1) * sizeof(int), stream_));
+  k_csr_fill<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, csr_off_.p, deg_.p,
+                                                      csr_cell_.p);
+  TB_LAUNCHED("k_csr_fill");
+  k_csr_sort<<<grid_for(ntot_, kT), kT, 0, stream_>>>(csr_off_.p, ntot_, csr_cell_.p);
+  TB_LAUNCHED("k_csr_sort");
+  return 0;
+}
+
+int Engine::upload_coords() {
+  for (size_t b = 0; b < hb_.size(); b++)
+    TB_CUDA(cudaMemcpyAsync(x_.p + 3 * (long long)bi_[b].node_off, hb_[b].hx,
+                            3 * (size_t)hb_[b].nnodes * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  return 0;
+}
+
+int Engine::compute_obbs() {
+  const int nparts = 148;
+  TB_CUDA(red_.ensure(12 * nparts));
+  for (size_t b = 0; b < hb_.size(); b++) {
+    const BlockInfo& B = bi_[b];
+    Obb* dobb = &d_bi_.p[b].obb;
+    int n = B.nnodes;
+    if (n == 0) continue;
+    for (int pass = 0; pass < 3; pass++) {
+      if (pass == 1 && n < 4) break;
+      k_obb_partial<<<nparts, 256, 0, stream_>>>(x_.p, B.node_off, n, pass, dobb, red_.p);
+      TB_LAUNCHED("k_obb_partial");
+      k_obb_finish<<<1, 1, 0, stream_>>>(red_.p, nparts, n, pass, x_.p, B.node_off, dobb, &d_bi_.p[b]);
+      TB_LAUNCHED("k_obb_finish");
+    }
+    if (n < 4) {  // the raw box is still needed for the Morton keys
+      k_obb_partial<<<nparts, 256, 0, stream_>>>(x_.p, B.node_off, n, 2, dobb, red_.p);
+      TB_LAUNCHED("k_obb_partial");
+    }
+  }
+  return 0;
+}
+
+int Engine::build_tree_topology() {
+  // Morton order of the cell centroids per block (block id in the key's
+  // high word), leaves of kLeafCells consecutive cells, one implicit tree per
+  // block.  Rebuilt only when the registration changes; every connectivity
+  // call refits the boxes to the current coordinates.
+  TB_CUDA(mkey_.ensure(ctot_));
+  TB_CUDA(mkey_alt_.ensure(ctot_));
+  TB_CUDA(sorted_cell_.ensure(ctot_));
+  TB_CUDA(mval_alt_.ensure(ctot_));
+  k_morton<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p,
+                                                    ctot_, mkey_.p, mval_alt_.p);
+  TB_LAUNCHED("k_morton");
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
+                                  (int)ctot_, 0, 40, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
+                                  (int)ctot_, 0, 40, stream_);
+  long long off = 0;
+  for (auto& B : bi_) {
+    long long nleaf = std::max(1ll, ((long long)B.ncells + kLeafCells - 1) / kLeafCells);
+    long long P = 1;
+    while (P < nleaf) P <<= 1;
+    B.P = (int)P;
+    B.tree_off = (int)off;
+    off += 2 * P - 1;
+  }
+  tree_nodes_ = off;
+  TB_CUDA(cbox_.ensure(2 * ctot_));
+  TB_CUDA(tnode_.ensure(2 * tree_nodes_));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// preprocess (src/tioga.C:95-110, MeshBlock.C:74-339)
+// ---------------------------------------------------------------------------
+int Engine::preprocess() {
+  if (hb_.empty()) return 0;
+  bool fresh = topo_dirty_;
+  if (topo_dirty_) {
+    int rc = upload_topology();
+    if (rc) return rc;
+  }
+  for (auto& B : bi_) B.nfringe = nfringe_;
+  for (size_t b = 0; b < hb_.size(); b++) bi_[b].has_user_res = (hb_[b].user_nres || hb_[b].user_cres);
+  TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
+                          stream_));
+  TB_TRY(upload_coords());
+  for (size_t b = 0; b < hb_.size(); b++) {
+    const HostBlock& H = hb_[b];
+    if (!bi_[b].has_user_res) continue;
+    TB_CUDA(cudaMemcpyAsync(node_res_.p + bi_[b].node_off, H.user_nres, H.nnodes * sizeof(double),
+                            cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaMemcpyAsync(cell_res_.p + bi_[b].cell_off, H.user_cres, H.ncells * sizeof(double),
+                            cudaMemcpyHostToDevice, stream_));
+  }
+  k_cell_volume<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p,
+                                                          ctot_, cell_res_.p);
+  TB_LAUNCHED("k_cell_volume");
+  k_node_res<<<grid_for(ntot_, kT), kT, 0, stream_>>>(csr_off_.p, csr_cell_.p, cell_res_.p, node_blk_.p,
+                                                       d_bi_.p, ntot_, node_res_.p);
+  TB_LAUNCHED("k_node_res");
+  TB_TRY(compute_obbs());
+  TB_CUDA(cudaMemsetAsync(ex0_.p, 0, ntot_, stream_));
+  TB_CUDA(cudaMemsetAsync(ex1_.p, 0, ntot_, stream_));
+  k_mandatory<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, obcf_.p, node_res_.p,
+                                                        ex0_.p, ex1_.p);
+  TB_LAUNCHED("k_mandatory");
+  for (int it = 0; it < mexclude_; it++) {
+    k_mexclude<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, ex0_.p, ex1_.p,
+                                                         cell_res_.p);
+    TB_LAUNCHED("k_mexclude");
+    k_copy_u8<<<grid_for(ntot_, kT), kT, 0, stream_>>>(ex1_.p, ex0_.p, ntot_);
+    TB_LAUNCHED("k_copy_u8");
+  }
+  k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, 1, ntot_);
+  TB_LAUNCHED("k_fill_int");
+  // keep the OBBs and block boxes on the host too
+  TB_CUDA(cudaMemcpyAsync(bi_.data(), d_bi_.p, bi_.size() * sizeof(BlockInfo), cudaMemcpyDeviceToHost,
+                          stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (fresh || tree_nodes_ == 0) {
+    TB_TRY(build_tree_topology());
+    TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
+                            stream_));
+  }
+  for (auto& H : hb_)
+    for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;  // preprocess sets iblank = 1 (MeshBlock.C:80)
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  preprocessed_ = true;
+  connected_ = false;
+  interps_fetched_ = false;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// connectivity (src/tioga.C:112-160)
+// ---------------------------------------------------------------------------
+int Engine::run_holemaps() {
+  // wall bounds per mesh tag -> extents and sizes -> mark -> fill
+  std::vector<unsigned long long> init(6 * maxtag_);
+  for (int t = 0; t < maxtag_; t++)
+    for (int j = 0; j < 6; j++) init[6 * t + j] = 0;
+  for (int t = 0; t < maxtag_; t++) {
+    // identity elements of min (all ones) and max (zero) over ordered keys
+    for (int j = 0; j < 3; j++) init[6 * t + j] = ~0ull;
+  }
+  TB_CUDA(cudaMemcpyAsync(wall_bb_.p, init.data(), init.size() * sizeof(unsigned long long),
+                          cudaMemcpyHostToDevice, stream_));
+  std::vector<HoleMapInfo> hinfo(maxtag_);
+  for (auto& h : hinfo) h.exist = 0;
+  TB_CUDA(cudaMemcpyAsync(d_hm_.p, hinfo.data(), maxtag_ * sizeof(HoleMapInfo), cudaMemcpyHostToDevice,
+                          stream_));
+  std::vector<HoleMapDev> hdev;
+  for (size_t b = 0; b < hb_.size(); b++) {
+    const BlockInfo& B = bi_[b];
+    if (B.nwbc <= 0) continue;
+    int t = B.tag - 1;
+    k_wall_bounds<<<grid_for(B.nwbc, kT, 148), kT, 0, stream_>>>(x_.p, wall_list_.p, B.wall_off, B.nwbc,
+                                                                 wall_bb_.p + 6 * t);
+    TB_LAUNCHED("k_wall_bounds");
+  }
+  for (size_t b = 0; b < hb_.size(); b++) {
+    const BlockInfo& B = bi_[b];
+    if (B.nwbc <= 0) continue;
+    int t = B.tag - 1;
+    k_holemap_setup<<<1, 1, 0, stream_>>>(wall_bb_.p, d_hm_.p, t);
+    TB_LAUNCHED("k_holemap_setup");
+    TB_CUDA(cudaMemsetAsync(hm_state_[t].p, 0, hm_state_[t].n, stream_));
+    k_holemap_mark<<<grid_for(B.ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, B.cell_off,
+                                                               B.ncells, wallf_.p, d_hm_.p + t,
+                                                               hm_state_[t].p);
+    TB_LAUNCHED("k_holemap_mark");
+  }
+  TB_CUDA(cudaMemcpyAsync(hinfo.data(), d_hm_.p, maxtag_ * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost,
+                          stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  for (int t = 0; t < maxtag_; t++) {
+    const HoleMapInfo& h = hinfo[t];
+    if (!h.exist) continue;
+    if (h.nx[0] > 197 || h.nx[1] > 197 || h.nx[2] > 197 || h.nx[0] < 1 || h.nx[1] < 1 || h.nx[2] < 1) {
+      fprintf(stderr, "#tioga_b200: hole map of mesh %d has an unexpected size\n", t + 1);
+      return -1;
+    }
+    int isym = isym_;
+    bool planar = (isym == 1 || isym == 2 || isym == 3);
+    int pa = (isym == 1) ? 0 : (isym == 2) ? 1 : 2;
+    int a0 = (pa == 0) ? 1 : 0, a1 = (pa == 2) ? 1 : 2;
+    size_t smem = (size_t)h.nx[a0] * h.nx[a1];
+    k_holemap_fill_planes<<<std::min(h.nx[pa], 148 * 4), 256, smem, stream_>>>(
+        hm_state_[t].p, d_hm_.p + t, planar ? isym : 3, planar ? 0 : 1, nullptr, err_.p);
+    TB_LAUNCHED("k_holemap_fill_planes");
+    if (!planar) {  // 6-neighbour fill: line sweeps over the three axes
+      unsigned* d_changed = err_.p + 1;
+      for (int round = 0; round < 4 * (h.nx[0] + h.nx[1] + h.nx[2]); round++) {
+        TB_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(unsigned), stream_));
+        for (int axis = 0; axis < 3; axis++) {
+          k_holemap_lines<<<grid_for((long long)h.nx[0] * h.nx[1] * h.nx[2] / 64 + 1, kT), kT, 0,
+                            stream_>>>(hm_state_[t].p, d_hm_.p + t, axis, d_changed);
+          TB_LAUNCHED("k_holemap_lines");
+        }
+        unsigned ch = 0;
+        TB_CUDA(cudaMemcpyAsync(&ch, d_changed, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+        TB_CUDA(cudaStreamSynchronize(stream_));
+        if (!ch) break;
+      }
+    }
+    k_holemap_final<<<grid_for((long long)h.nx[0] * h.nx[1] * h.nx[2], kT), kT, 0, stream_>>>(
+        hm_state_[t].p, d_hm_.p + t);
+    TB_LAUNCHED("k_holemap_final");
+    HoleMapDev d;
+    d.tagidx = t;
+    for (int j = 0; j < 3; j++) d.nx[j] = h.nx[j];
+    for (int j = 0; j < 6; j++) d.ext[j] = h.ext[j];
+    d.hole = hm_state_[t].p;
+    hdev.push_back(d);
+  }
+  nhm_ = (int)hdev.size();
+  if (nhm_ > 0)
+    TB_CUDA(cudaMemcpyAsync(d_hmdev_.p, hdev.data(), nhm_ * sizeof(HoleMapDev), cudaMemcpyHostToDevice,
+                            stream_));
+  return 0;
+}
+
+int Engine::run_pairs_and_refit() {
+  const int nb = (int)hb_.size();
+  TB_CUDA(d_pairs_.ensure(nb * nb + 1));
+  TB_CUDA(d_npairs_.ensure(1));
+  k_pairs<<<1, 1, 0, stream_>>>(d_bi_.p, nb, d_pairs_.p, d_npairs_.p);
+  TB_LAUNCHED("k_pairs");
+  TB_CUDA(cudaMemcpyAsync(&npairs_, d_npairs_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  h_pairs_.resize(nb * nb + 1);
+  TB_CUDA(cudaMemcpyAsync(h_pairs_.data(), d_pairs_.p, (nb * nb + 1) * sizeof(PairInfo),
+                          cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (npairs_ == 0) return 0;
+  // tree refit to the current coordinates
+  const bool fp64 = (precision_ == 0);
+  if (fp64) {
+    TB_CUDA(cbox64_.ensure(6 * ctot_));
+    TB_CUDA(tnode64_.ensure(6 * tree_nodes_));
+  }
+  k_cell_boxes<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, sorted_cell_.p, ctot_,
+                                                        cbox_.p, fp64 ? cbox64_.p : nullptr);
+  TB_LAUNCHED("k_cell_boxes");
+  std::vector<long long> leaf_base(nb + 1, 0);
+  for (int b = 0; b < nb; b++) leaf_base[b + 1] = leaf_base[b] + bi_[b].P;
+  TB_CUDA(visit_.ensure(tree_nodes_ + nb + 1));
+  TB_CUDA(cudaMemsetAsync(visit_.p, 0, tree_nodes_ * sizeof(int), stream_));
+  long long* d_lb = reinterpret_cast<long long*>(visit_.p + tree_nodes_);
+  // leaf_base lives in a small separate buffer
+  TB_CUDA(leafbase_.ensure(nb + 1));
+  TB_CUDA(cudaMemcpyAsync(leafbase_.p, leaf_base.data(), (nb + 1) * sizeof(long long),
+                          cudaMemcpyHostToDevice, stream_));
+  (void)d_lb;
+  k_tree_leaves<<<grid_for(leaf_base[nb], kT), kT, 0, stream_>>>(
+      d_bi_.p, nb, cbox_.p, fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, visit_.p,
+      leaf_base[nb], leafbase_.p);
+  TB_LAUNCHED("k_tree_leaves");
+  // reduced boxes, one pass over each donor's cells
+  std::vector<unsigned long long> acc(6 * npairs_);
+  for (int p = 0; p < npairs_; p++)
+    for (int j = 0; j < 3; j++) {
+      acc[6 * p + j] = 0;
+      acc[6 * p + j + 3] = 0;
+    }
+  // initial values BIG / -BIG as getReducedOBB (MeshBlock.C:790-794)
+  for (int p = 0; p < npairs_; p++)
+    for (int j = 0; j < 3; j++) {
+      double lo = kBig, hi = -kBig;
+      unsigned long long bl, bh;
+      memcpy(&bl, &lo, 8);
+      memcpy(&bh, &hi, 8);
+      acc[6 * p + j] = (bl & 0x8000000000000000ull) ? ~bl : (bl | 0x8000000000000000ull);
+      acc[6 * p + j + 3] = (bh & 0x8000000000000000ull) ? ~bh : (bh | 0x8000000000000000ull);
+    }
+  TB_CUDA(pair_acc_.ensure(6 * npairs_));
+  TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
+                          cudaMemcpyHostToDevice, stream_));
+  std::vector<int> has(nb, 0);
+  for (int p = 0; p < npairs_; p++) has[h_pairs_[p].don] = 1;
+  for (int b = 0; b < nb; b++)
+    if (has[b] && bi_[b].ncells > 0) {
+      k_reduced_obb<<<grid_for(bi_[b].ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, d_bi_.p, b,
+                                                                     d_pairs_.p, npairs_, pair_acc_.p);
+      TB_LAUNCHED("k_reduced_obb");
+    }
+  k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
+  TB_LAUNCHED("k_pair_finish");
+  return 0;
+}
+
+int Engine::run_queries() {
+  // ordered compaction of each pair's receptor nodes inside the donor region
+  int maxn = 0;
+  for (int p = 0; p < npairs_; p++) maxn = std::max(maxn, bi_[h_pairs_[p].rec].nnodes);
+  const int tile = 256 * 8;
+  const int tiles_x = std::max(1, (maxn + tile - 1) / tile);
+  const long long ntiles = (long long)tiles_x * npairs_;
+  TB_CUDA(tile_cnt_.ensure(ntiles + 1));
+  TB_CUDA(tile_off_.ensure(ntiles + 1));
+  TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
+  dim3 grid(std::min(tiles_x, 148 * 8), npairs_);
+  k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_cnt_.p);
+  TB_LAUNCHED("k_query_count");
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
+  int nq = 0;
+  TB_CUDA(cudaMemcpyAsync(&nq, tile_off_.p + ntiles, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  nq_ = nq;
+  TB_CUDA(qnode_.ensure(nq));
+  TB_CUDA(qdon_.ensure(nq));
+  TB_CUDA(qres_.ensure(nq));
+  TB_CUDA(qcell_.ensure(nq));
+  TB_CUDA(qtie_.ensure(nq));
+  TB_CUDA(interp2rec_.ensure(nq));
+  if (nq > 0) {
+    k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_off_.p,
+                                             node_res_.p, qnode_.p, qdon_.p, qres_.p);
+    TB_LAUNCHED("k_query_write");
+  }
+  return 0;
+}
+
+int Engine::run_search() {
+  TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
+  if (nq_ == 0) return 0;
+  TB_CUDA(cudaMemsetAsync(qcell_.p, 0xff, nq_ * sizeof(int), stream_));
+  const int threads = 128;
+  const int blocks = (int)std::min<long long>((nq_ + threads - 1) / threads, 148ll * 64);
+  launch_search(precision_ == 0 ? 0 : 1, blocks, threads, stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p,
+                d_bi_.p, sorted_cell_.p, cbox_.p, precision_ == 0 ? cbox64_.p : nullptr, tnode_.p,
+                precision_ == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p, nq_, early_exit_, qcell_.p, qtie_.p,
+                counters_.p);
+  TB_LAUNCHED("k_search");
+  return 0;
+}
+
+int Engine::run_donors() {
+  // candidate slots: one per (receptor node, donor block)
+  TB_CUDA(cudaMemsetAsync(slot_.p, 0xff, (size_t)ntot_ * K_ * sizeof(int), stream_));
+  if (nq_ > 0) {
+    k_fill_slots<<<grid_for(nq_, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, qcell_.p, nq_, K_, ntot_, ctot_,
+                                                        slot_.p, err_.p);
+    TB_LAUNCHED("k_fill_slots");
+  }
+  k_process_donors<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, slot_.p, K_, qres_.p,
+                                                             d_hmdev_.p, nhm_, ntot_, iblank_.p, node_res_.p,
+                                                             m0_.p, m1_.p);
+  TB_LAUNCHED("k_process_donors");
+  int maxfr = 0;
+  for (auto& B : bi_) maxfr = std::max(maxfr, B.nfringe);
+  for (int it = 0; it < maxfr; it++) {
+    k_dilate<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p, ctot_, it,
+                                                       m0_.p, m1_.p);
+    TB_LAUNCHED("k_dilate");
+    k_copy_u8<<<grid_for(ntot_, kT), kT, 0, stream_>>>(m1_.p, m0_.p, ntot_);
+    TB_LAUNCHED("k_copy_u8");
+  }
+  k_fringe_big<<<grid_for(ntot_, kT), kT, 0, stream_>>>(m1_.p, iblank_.p, ntot_, node_res_.p);
+  TB_LAUNCHED("k_fringe_big");
+  // fringe choice -> records keyed (donor block, receptor node)
+  TB_CUDA(rcount_.ensure(2));
+  TB_CUDA(cudaMemsetAsync(rcount_.p, 0, 2 * sizeof(int), stream_));
+  long long rcap = std::max<long long>(1, std::min<long long>(ntot_, nq_));
+  TB_CUDA(rkey_.ensure(rcap));
+  TB_CUDA(rkey_alt_.ensure(rcap));
+  TB_CUDA(rval_.ensure(rcap));
+  TB_CUDA(rval_alt_.ensure(rcap));
+  k_select<<<grid_for(ntot_, kT), kT, 0, stream_>>>(node_blk_.p, d_bi_.p, slot_.p, K_, qcell_.p, cell_res_.p,
+                                                     ntot_, iblank_.p, node_res_.p, rkey_alt_.p, rval_alt_.p,
+                                                     rcount_.p, (int)rcap, err_.p);
+  TB_LAUNCHED("k_select");
+  int R = 0;
+  TB_CUDA(cudaMemcpyAsync(&R, rcount_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (R > rcap) {  // cannot happen: one record per receptor node at most
+    fprintf(stderr, "#tioga_b200: donor records overflowed their capacity\n");
+    R = (int)rcap;
+    TB_CUDA(cudaMemcpyAsync(rcount_.p, &R, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  }
+  nrec_ = R;
+  if (R > 0) {
+    size_t tmp = 0;
+    int hi_bit = 32;
+    while ((1ll << (hi_bit - 32)) < K_) hi_bit++;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, rkey_alt_.p, rkey_.p, rval_alt_.p, rval_.p, R, 0, hi_bit,
+                                    stream_);
+    TB_CUDA(cub_tmp_.ensure(tmp));
+    cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, rkey_alt_.p, rkey_.p, rval_alt_.p, rval_.p, R, 0,
+                                    hi_bit, stream_);
+  }
+  TB_CUDA(it_node_.ensure(9 * (size_t)std::max(R, 1)));
+  TB_CUDA(it_w_.ensure(9 * (size_t)std::max(R, 1)));
+  TB_CUDA(it_rec_.ensure(std::max(R, 1)));
+  TB_CUDA(it_don_.ensure(std::max(R, 1)));
+  TB_CUDA(it_nv_.ensure(std::max(R, 1)));
+  TB_CUDA(it_cancel_.ensure(std::max(R, 1)));
+  TB_CUDA(rres_.ensure(std::max(R, 1)));
+  TB_CUDA(cudaMemsetAsync(cmark_.p, 0, ntot_, stream_));
+  k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(reset_t_.p, 0x7fffffff, ntot_);
+  TB_LAUNCHED("k_fill_int");
+  if (nq_ > 0) {
+    k_fill_int<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, -1, nq_);
+    TB_LAUNCHED("k_fill_int");
+  }
+  if (R > 0) {
+    k_interp_marks<<<grid_for(R, kT), kT, 0, stream_>>>(rkey_.p, rval_.p, rcount_.p, qcell_.p, conn8_.p,
+                                                         cell_nv_.p, iblank_.p, node_res_.p, cmark_.p,
+                                                         reset_t_.p);
+    TB_LAUNCHED("k_interp_marks");
+    k_interp<<<grid_for(R, 128), 128, 0, stream_>>>(x_.p, rkey_.p, rval_.p, rcount_.p, qcell_.p, conn8_.p,
+                                                     cell_nv_.p, node_blk_.p, d_bi_.p, iblank_.p, node_res_.p,
+                                                     reset_t_.p, it_node_.p, it_w_.p, it_rec_.p, it_don_.p,
+                                                     it_nv_.p, it_cancel_.p, rres_.p, interp2rec_.p, err_.p);
+    TB_LAUNCHED("k_interp");
+    k_cancel<<<grid_for(ntot_, kT), kT, 0, stream_>>>(cmark_.p, ntot_, slot_.p, K_, qcell_.p, cell_res_.p,
+                                                       interp2rec_.p, it_cancel_.p);
+    TB_LAUNCHED("k_cancel");
+  }
+  k_iblank_clear<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, ntot_);
+  TB_LAUNCHED("k_iblank_clear");
+  if (R > 0) {
+    k_iblank_set<<<grid_for(R, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, iblank_.p);
+    TB_LAUNCHED("k_iblank_set");
+  }
+  return 0;
+}
+
+int Engine::run_celliblank() {
+  k_cell_iblank<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, iblank_.p,
+                                                          iblank_cell_.p);
+  TB_LAUNCHED("k_cell_iblank");
+  k_count_iblank<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, ntot_, counters_.p);
+  TB_LAUNCHED("k_count_iblank");
+  return 0;
+}
+
+int Engine::download_iblank() {
+  for (size_t b = 0; b < hb_.size(); b++) {
+    TB_CUDA(cudaMemcpyAsync(hb_[b].hibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
+                            cudaMemcpyDeviceToHost, stream_));
+    if (hb_[b].h_iblank_cell)
+      TB_CUDA(cudaMemcpyAsync(hb_[b].h_iblank_cell, iblank_cell_.p + bi_[b].cell_off,
+                              hb_[b].ncells * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  }
+  return 0;
+}
+
+int Engine::connectivity() {
+  if (!preprocessed_) {
+    fprintf(stderr, "#tioga_b200: performconnectivity called before preprocess_grids\n");
+    return -1;
+  }
+  stats_ = Stats{};
+  interps_fetched_ = false;
+  TB_CUDA(cudaEventRecord(ev_[0], stream_));
+  if (!coords_resident_) TB_TRY(upload_coords());
+  TB_CUDA(cudaEventRecord(ev_[1], stream_));
+  int rc = run_holemaps();
+  if (rc) return rc;
+  TB_CUDA(cudaEventRecord(ev_[2], stream_));
+  rc = run_pairs_and_refit();
+  if (rc) return rc;
+  TB_CUDA(cudaEventRecord(ev_[3], stream_));
+  nq_ = 0;
+  nrec_ = 0;
+  if (npairs_ > 0) {
+    rc = run_queries();
+    if (rc) return rc;
+    TB_CUDA(cudaEventRecord(ev_[4], stream_));
+    rc = run_search();
+    if (rc) return rc;
+    TB_CUDA(cudaEventRecord(ev_[5], stream_));
+    rc = run_donors();
+    if (rc) return rc;
+  } else {
+    TB_CUDA(cudaEventRecord(ev_[4], stream_));
+    TB_CUDA(cudaEventRecord(ev_[5], stream_));
+    TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
+  }
+  TB_CUDA(cudaEventRecord(ev_[6], stream_));
+  rc = run_celliblank();
+  if (rc) return rc;
+  TB_CUDA(cudaEventRecord(ev_[7], stream_));
+  TB_TRY(download_iblank());
+  TB_CUDA(cudaEventRecord(ev_[8], stream_));
+  unsigned long long cnt[16];
+  unsigned err = 0;
+  TB_CUDA(cudaMemcpyAsync(cnt, counters_.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  stats_.nquery = nq_;
+  stats_.ncand = (long long)cnt[0];
+  stats_.nrefine = (long long)cnt[1];
+  stats_.nties = (long long)cnt[2];
+  stats_.ndonor = (long long)cnt[3];
+  stats_.nhole = (long long)cnt[4];
+  stats_.nreceptor = (long long)cnt[5];
+  stats_.nrecords = nrec_;
+  stats_.npairs = npairs_;
+  stats_.error = err;
+  float ms[9];
+  for (int i = 1; i < 9; i++) cudaEventElapsedTime(&ms[i], ev_[i - 1], ev_[i]);
+  timing_.upload = ms[1];
+  timing_.holemap = ms[2];
+  timing_.boxes = ms[3];
+  timing_.query = ms[4];
+  timing_.search = ms[5];
+  timing_.donors = ms[6];
+  timing_.celliblank = ms[7];
+  timing_.download = ms[8];
+  cudaEventElapsedTime(&timing_.total, ev_[0], ev_[8]);
+  if (err & kErrWeightRange)
+    fprintf(stderr, "#tioga_b200: an interpolation weight fell outside [-0.2,1.2] (the reference aborts)\n");
+  if (err & kErrFloodFillBound) fprintf(stderr, "#tioga_b200: hole-map fill hit its round limit\n");
+  connected_ = true;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// queries on the interpolation lists (dataUpdate.C:121-159)
+// ---------------------------------------------------------------------------
+int Engine::fetch_interps() {
+  if (interps_fetched_) return 0;
+  const long long R = nrec_;
+  h_it_node_.resize(9 * R);
+  h_it_w_.resize(9 * R);
+  h_it_rec_.resize(R);
+  h_it_don_.resize(R);
+  h_it_nv_.resize(R);
+  h_it_cancel_.resize(R);
+  if (R > 0) {
+    TB_CUDA(cudaMemcpyAsync(h_it_node_.data(), it_node_.p, 9 * R * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_it_w_.data(), it_w_.p, 9 * R * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_it_rec_.data(), it_rec_.p, R * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_it_don_.data(), it_don_.p, R * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_it_nv_.data(), it_nv_.p, R, cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_it_cancel_.data(), it_cancel_.p, R, cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+  }
+  interps_fetched_ = true;
+  return 0;
+}
+
+int Engine::donor_count(int tag, int* dcount, int* fcount) {
+  *dcount = *fcount = 0;
+  if (!connected_ || npairs_ == 0) return 0;
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  int rc = fetch_interps();
+  if (rc) return rc;
+  for (long long r = 0; r < nrec_; r++)
+    if (h_it_don_[r] == ib && !h_it_cancel_[r]) {
+      (*dcount)++;
+      (*fcount) += h_it_nv_[r] + 1;
+    }
+  return 0;
+}
+
+int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
+  if (!connected_ || npairs_ == 0) return 0;
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  int rc = fetch_interps();
+  if (rc) return rc;
+  long long j = 0, k = 0;
+  for (long long r = 0; r < nrec_; r++) {
+    if (h_it_don_[r] != ib || h_it_cancel_[r]) continue;
+    const int nv = h_it_nv_[r];
+    for (int m = 0; m < nv + 1; m++) {
+      indices[j] = h_it_node_[9 * r + m];
+      frac[j] = h_it_w_[9 * r + m];
+      j++;
+    }
+    const int g = h_it_rec_[r];
+    int rb = 0;
+    while (rb + 1 < (int)bi_.size() && bi_[rb + 1].node_off <= g) rb++;
+    receptors[k++] = 0;  // rank of the receptor: the only one
+    receptors[k++] = g - bi_[rb].node_off;
+    receptors[k++] = rb;
+    receptors[k++] = nv;
+  }
+  return 0;
+}
+
+int Engine::cell_iblank(int tag, int* out) {
+  int ib = find_tag(tag);
+  if (ib < 0 || !connected_) return -1;
+  TB_CUDA(cudaMemcpyAsync(out, iblank_cell_.p + bi_[ib].cell_off, bi_[ib].ncells * sizeof(int),
+                          cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// data update (src/tioga.C:336-524)
+// ---------------------------------------------------------------------------
+int Engine::dataupdate(int nvar, int interptype) {
+  if (!connected_) return -1;
+  bool device = true, host = true;
+  for (auto& H : hb_) {
+    if (!H.hq && !H.dq) {
+      printf("Solution data not set, cannot update \n");
+      return 0;
+    }
+    device = device && H.dq;
+    host = host && H.hq;
+  }
+  if (npairs_ == 0 || nrec_ == 0) return 0;
+  if (!device && !host) {
+    fprintf(stderr, "#tioga_b200: register every block's solution on the same side (host or device)\n");
+    return -1;
+  }
+  TB_CUDA(qvals_.ensure((size_t)nrec_ * nvar));
+  double* qdev;
+  if (host) {
+    TB_CUDA(q_.ensure((size_t)ntot_ * nvar));
+    for (size_t b = 0; b < hb_.size(); b++)
+      TB_CUDA(cudaMemcpyAsync(q_.p + (size_t)bi_[b].node_off * nvar, hb_[b].hq,
+                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    qdev = q_.p;
+  } else {
+    // device solutions: the blocks' arrays must form one flat array in
+    // registration order (the layout tioga_b200_registersolution_device_
+    // documents); a gather keeps it general
+    TB_CUDA(q_.ensure((size_t)ntot_ * nvar));
+    for (size_t b = 0; b < hb_.size(); b++)
+      TB_CUDA(cudaMemcpyAsync(q_.p + (size_t)bi_[b].node_off * nvar, hb_[b].dq,
+                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    qdev = q_.p;
+  }
+  k_interp_gather<<<grid_for(nrec_, 128), 128, 0, stream_>>>(it_node_.p, it_w_.p, it_don_.p, it_nv_.p,
+                                                              it_cancel_.p, rcount_.p, d_bi_.p, qdev, nvar,
+                                                              interptype, qvals_.p);
+  TB_LAUNCHED("k_interp_gather");
+  if (host) {
+    int rc = fetch_interps();
+    if (rc) return rc;
+    std::vector<double> vals((size_t)nrec_ * nvar);
+    TB_CUDA(cudaMemcpyAsync(vals.data(), qvals_.p, vals.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    // scatter into the caller's arrays (updateSolnData, dataUpdate.C:105-119)
+    for (long long r = 0; r < nrec_; r++) {
+      if (h_it_cancel_[r]) continue;
+      const int g = h_it_rec_[r];
+      int rb = 0;
+      while (rb + 1 < (int)bi_.size() && bi_[rb + 1].node_off <= g) rb++;
+      const int local = g - bi_[rb].node_off;
+      double* q = hb_[rb].hq;
+      for (int k = 0; k < nvar; k++) {
+        if (interptype == 0) q[(size_t)local * nvar + k] = vals[(size_t)r * nvar + k];
+        else q[(size_t)k * hb_[rb].nnodes + local] = vals[(size_t)r * nvar + k];
+      }
+    }
+  } else {
+    k_interp_scatter<<<grid_for(nrec_, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, node_blk_.p,
+                                                               d_bi_.p, qvals_.p, nvar, interptype, qdev);
+    TB_LAUNCHED("k_interp_scatter");
+    for (size_t b = 0; b < hb_.size(); b++)
+      TB_CUDA(cudaMemcpyAsync(hb_[b].dq, q_.p + (size_t)bi_[b].node_off * nvar,
+                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+  }
+  return 0;
+}
+
+}  // namespace tb

@@ -1,0 +1,246 @@
+// Host-side engine of the B200 TIOGA connectivity path.
+//
+// Layout in HBM: the nodes and cells of every registered block are
+// concatenated into flat arrays (block b owns nodes [node_off, node_off+nnodes)
+// and cells [cell_off, cell_off+ncells)), so each stage of the path is one
+// launch over all blocks.  Connectivity is stored padded to 8 vertices per
+// cell with global (0-based) node ids.  The reference's MPI packet exchanges
+// (src/exchangeBoxes.C, exchangeSearchData.C, exchangeDonors.C) become device
+// buffers written by one kernel and read by the next.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace tb {
+
+constexpr int kLeafCells = 4;   // cells per BVH leaf
+constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t c = count ? count : 1;
+    cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+    if (e == cudaSuccess) n = c;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// POD block descriptor mirrored to the device
+struct BlockInfo {
+  int tag;
+  int nnodes, ncells;
+  int node_off, cell_off;
+  int ntypes;
+  int type_off[5];  // cell offsets of the types inside the block
+  int nv[4];
+  int nwbc, wall_off;  // wall nodes in the global wall list
+  int nobc, obc_off;
+  int nfringe;         // snapshot taken at preprocess (tioga.C:95-110)
+  int tree_off;        // first tree node in the node pool
+  int P;               // padded leaf count (power of two)
+  int has_user_res;
+  Obb obb;
+  float bb_lo[3], bb_hi[3];  // block box for the Morton keys
+};
+
+struct PairInfo {  // one (receptor block, donor block) pair, src/exchangeBoxes.C:133-160
+  int rec, don;
+  double rd[6];    // reduced box accumulator in the donor's OBB frame (ordered bits)
+  Obb region;      // donor cells overlapping the receptor OBB, donor axes
+};
+
+struct HoleMapInfo {
+  int exist;
+  int nx[3];
+  double ext[6];
+};
+
+struct HostBlock {
+  int tag = 0, nnodes = 0, ncells = 0, ntypes = 0;
+  int nv[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
+  double* hx = nullptr;
+  int* hibl = nullptr;
+  int nwbc = 0, nobc = 0;
+  int* hwbc = nullptr;
+  int* hobc = nullptr;
+  int* hconn[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* user_nres = nullptr;
+  double* user_cres = nullptr;
+  int* h_iblank_cell = nullptr;  // caller array (tioga_setcelliblank_)
+  double* hq = nullptr;          // registered host solution
+  double* dq = nullptr;          // registered device solution
+};
+
+struct Stats {
+  long long nquery = 0;       // Q: query points handed to donor searches
+  long long ndonor = 0;       // queries with a donor cell
+  long long nties = 0;        // queries whose donor depends on the search order
+  long long ncand = 0;        // candidate cells tested with Newton
+  long long nrefine = 0;      // FP64 refinements in the split-precision form
+  long long nreceptor = 0;    // final iblank == -1
+  long long nhole = 0;        // final iblank == 0
+  long long nrecords = 0;     // chosen donors (before cancellation)
+  long long npairs = 0;       // intersecting (receptor, donor) block pairs
+  unsigned error = 0;
+};
+
+struct Timing {
+  float holemap = 0, boxes = 0, refit = 0, query = 0, search = 0, donors = 0, celliblank = 0,
+        total = 0, upload = 0, download = 0;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+
+  // registration / settings (src/tioga.C:64-93, tioga.h:181-205)
+  int register_block(int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
+                     int* obc, int ntypes, const int* nv, const int* nc, int** conn);
+  void set_symmetry(int s) { isym_ = s; }
+  void set_nfringe(int n) { nfringe_ = n; }
+  void set_mexclude(int m) { mexclude_ = m; }
+  int set_resolutions(int tag, double* nres, double* cres);
+  int set_cell_iblank(int tag, int* ibc);
+  int register_solution(int tag, double* q, bool device);
+  void set_precision(int p) { precision_ = p; }
+  void set_coords_resident(int r) { coords_resident_ = r; }
+  void set_early_exit(int e) { early_exit_ = e; }
+
+  // the path
+  int preprocess();
+  int connectivity();
+  int dataupdate(int nvar, int interptype);
+
+  // queries (src/dataUpdate.C:121-159, tioga.C:533-570)
+  int donor_count(int tag, int* dcount, int* fcount);
+  int donor_info(int tag, int* receptors, int* indices, double* frac);
+  int cell_iblank(int tag, int* out);
+  const Stats& stats() const { return stats_; }
+  const Timing& timing() const { return timing_; }
+  cudaStream_t stream() const { return stream_; }
+  int nblocks() const { return (int)hb_.size(); }
+  int first_tag() const { return hb_.empty() ? -1 : hb_[0].tag; }
+  int last_error() const { return last_error_; }
+
+ private:
+  int upload_topology();
+  int build_csr();
+  int compute_obbs();
+  int build_tree_topology();
+  int upload_coords();
+  int run_holemaps();
+  int run_pairs_and_refit();
+  int run_queries();
+  int run_search();
+  int run_donors();
+  int run_celliblank();
+  int download_iblank();
+  int fetch_interps();
+  int find_tag(int tag) const;
+
+  std::vector<HostBlock> hb_;
+  std::vector<BlockInfo> bi_;
+  std::map<int, int> tag2idx_;
+  int isym_ = 3, nfringe_ = 1, mexclude_ = 3;
+  int precision_ = 1;        // 0 = FP64 throughout, 1 = FP32 screen + FP64 refine
+  int early_exit_ = 0;
+  int coords_resident_ = 0;  // 1: the caller promises x has not moved
+  bool topo_dirty_ = true;
+  bool preprocessed_ = false;
+  bool connected_ = false;
+  int npairs_ = 0;
+  int maxtag_ = 0;
+  int nhm_ = 0;
+  long long nq_ = 0;
+  std::vector<PairInfo> h_pairs_;
+  DBuf<int> visit_;
+  DBuf<long long> leafbase_;
+  DBuf<unsigned long long> pair_acc_;
+  long long ntot_ = 0, ctot_ = 0, inc_tot_ = 0;
+  int last_error_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev_[12];
+
+  // flat device arrays
+  DBuf<double> x_, node_res_, cell_res_;
+  DBuf<int> iblank_, iblank_cell_, conn8_;
+  DBuf<unsigned char> node_blk_, cell_blk_, cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_, m1_, cmark_;
+  DBuf<int> wall_list_, obc_list_;
+  DBuf<int> csr_off_, csr_cell_, deg_;
+  DBuf<BlockInfo> d_bi_;
+  DBuf<PairInfo> d_pairs_;
+  DBuf<int> d_npairs_;
+  DBuf<HoleMapInfo> d_hm_;
+  DBuf<HoleMapDev> d_hmdev_;
+  std::vector<DBuf<unsigned char>> hm_state_;
+  DBuf<unsigned long long> wall_bb_;
+  // tree
+  DBuf<int> sorted_cell_;
+  DBuf<float4> cbox_;      // 2 per sorted cell
+  DBuf<float4> tnode_;     // 2 per tree node
+  DBuf<double> tnode64_;   // 6 per tree node (FP64 form)
+  DBuf<double> cbox64_;    // 6 per sorted cell (FP64 form)
+  long long tree_nodes_ = 0;
+  // queries
+  DBuf<int> qnode_, qdon_, qcell_;
+  DBuf<double> qres_;
+  DBuf<unsigned char> qtie_;
+  DBuf<int> qcount_;
+  DBuf<int> tile_cnt_, tile_off_;
+  long long qcap_ = 0;
+  // donors
+  DBuf<int> slot_;          // K per node
+  int K_ = 1;
+  DBuf<unsigned long long> rkey_, rkey_alt_;
+  DBuf<int> rval_, rval_alt_;
+  DBuf<int> rcount_;
+  DBuf<int> reset_t_;
+  DBuf<int> interp2rec_;    // per query
+  DBuf<int> it_node_;       // 9 per record (nv donor nodes + donor cell, block-local)
+  DBuf<double> it_w_;       // 9 per record
+  DBuf<int> it_rec_;        // receptor global node per record
+  DBuf<int> it_don_;        // donor block per record
+  DBuf<unsigned char> it_nv_, it_cancel_;
+  DBuf<double> rres_;       // receptor resolution per record
+  long long nrec_ = 0;
+  // data update
+  DBuf<double> q_, qvals_;
+  // scratch for CUB and reductions
+  DBuf<unsigned char> cub_tmp_;
+  DBuf<double> red_;
+  DBuf<unsigned> err_;
+  DBuf<unsigned long long> counters_;
+  DBuf<unsigned long long> mkey_, mkey_alt_;
+  DBuf<int> mval_alt_;
+
+  // host copies of the interpolation lists (filled lazily for queries)
+  bool interps_fetched_ = false;
+  std::vector<int> h_it_node_, h_it_rec_, h_it_don_;
+  std::vector<double> h_it_w_;
+  std::vector<unsigned char> h_it_nv_, h_it_cancel_;
+
+  Stats stats_;
+  Timing timing_;
+};
+
+}  // namespace tb

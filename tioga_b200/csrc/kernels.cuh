@@ -1,0 +1,145 @@
+// Kernel declarations and small device helpers shared by the kernel files.
+#pragma once
+
+#include <string.h>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace tb {
+
+__device__ __forceinline__ void gather_vertices(const double* __restrict__ x, const int* __restrict__ cv,
+                                                int nv, double xv[8][3]) {
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    if (m < nv) {
+      const double* p = x + 3 * (long long)cv[m];
+      xv[m][0] = p[0];
+      xv[m][1] = p[1];
+      xv[m][2] = p[2];
+    }
+  }
+}
+
+// order-preserving map of a double onto an unsigned 64-bit key, so that
+// atomicMin/atomicMax on the key are exact min/max on the double
+__device__ __forceinline__ unsigned long long dkey(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__host__ __device__ inline double dkey_inv(unsigned long long k) {
+  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  double d;
+  memcpy(&d, &b, sizeof(d));
+  return d;
+}
+
+// ---- preprocess (kernels_pre.cu) ----
+__global__ void k_conn_convert(const int* raw, int nc, int nv, int node_off, int cell_base, int blk,
+                               int* conn8, unsigned char* cell_nv, unsigned char* cell_blk);
+__global__ void k_node_blk(int node_off, int nnodes, int blk, unsigned char* node_blk);
+__global__ void k_mark_list(const int* list, int n, int node_off, int* glist, int goff,
+                            unsigned char* flag);
+__global__ void k_csr_count(const int* conn8, const unsigned char* cell_nv, long long ctot, int* deg);
+__global__ void k_csr_fill(const int* conn8, const unsigned char* cell_nv, long long ctot,
+                           const int* off, int* cursor, int* cells);
+__global__ void k_csr_sort(const int* off, long long ntot, int* cells);
+__global__ void k_cell_volume(const double* x, const int* conn8, const unsigned char* cell_nv,
+                              const unsigned char* cell_blk, const BlockInfo* bi, long long ctot,
+                              double* cell_res);
+__global__ void k_node_res(const int* off, const int* cells, const double* cell_res,
+                           const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+                           double* node_res);
+__global__ void k_mandatory(const int* conn8, const unsigned char* cell_nv, long long ctot,
+                            const unsigned char* obcf, double* node_res, unsigned char* ex0,
+                            unsigned char* ex1);
+__global__ void k_mexclude(const int* conn8, const unsigned char* cell_nv, long long ctot,
+                           const unsigned char* ex0, unsigned char* ex1, double* cell_res);
+__global__ void k_copy_u8(const unsigned char* a, unsigned char* b, long long n);
+__global__ void k_fill_int(int* a, int v, long long n);
+__global__ void k_obb_partial(const double* x, int off, int n, int pass, const Obb* obb, double* part);
+__global__ void k_obb_finish(const double* part, int nparts, int n, int pass, const double* x, int off,
+                             Obb* obb, BlockInfo* bi);
+__global__ void k_morton(const double* x, const int* conn8, const unsigned char* cell_nv,
+                         const unsigned char* cell_blk, const BlockInfo* bi, long long ctot,
+                         unsigned long long* key, int* val);
+
+// ---- connectivity (kernels_conn.cu) ----
+__global__ void k_wall_bounds(const double* x, const int* wall_list, int off, int n,
+                              unsigned long long* bb);
+__global__ void k_holemap_setup(const unsigned long long* bb, HoleMapInfo* hm, int tag0);
+__global__ void k_holemap_mark(const double* x, const int* conn8, const unsigned char* cell_nv,
+                               int cell_off, int ncells, const unsigned char* wallf,
+                               const HoleMapInfo* hm, unsigned char* sam);
+__global__ void k_holemap_fill_planes(unsigned char* sam, const HoleMapInfo* hm, int isym,
+                                      int seed, unsigned* changed, unsigned* err);
+__global__ void k_holemap_lines(unsigned char* sam, const HoleMapInfo* hm, int axis, unsigned* changed);
+__global__ void k_holemap_final(unsigned char* sam, const HoleMapInfo* hm);
+__global__ void k_pairs(BlockInfo* bi, int nb, PairInfo* pairs, int* npairs);
+__global__ void k_reduced_obb(const double* x, const int* conn8, const unsigned char* cell_nv,
+                              const BlockInfo* bi, int don, PairInfo* pairs, int npairs,
+                              unsigned long long* acc);
+__global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
+                              const unsigned long long* acc);
+__global__ void k_cell_boxes(const double* x, const int* conn8, const unsigned char* cell_nv,
+                             const int* sorted_cell, long long ctot, float4* cbox, double* cbox64);
+__global__ void k_tree_leaves(const BlockInfo* bi, int nb, const float4* cbox, const double* cbox64,
+                              float4* tnode, double* tnode64, int* visit, long long total_leaves,
+                              const long long* leaf_base);
+__global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs,
+                              int tiles_x, int tile, int* tile_cnt);
+__global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs,
+                              int tiles_x, int tile, const int* tile_off, const double* node_res,
+                              int* qnode, int* qdon, double* qres);
+// host launcher of the templated search kernel (same translation unit as
+// its instantiations)
+void launch_search(int form, int blocks, int threads, cudaStream_t st, const double* x, const int* conn8,
+                   const unsigned char* cell_nv, const double* cell_res, const BlockInfo* bi,
+                   const int* sorted_cell, const float4* cbox, const double* cbox64, const float4* tnode,
+                   const double* tnode64, const int* qnode, const int* qdon, long long nq, int early_exit,
+                   int* qcell, unsigned char* qtie, unsigned long long* counters);
+
+// ---- donors (kernels_donor.cu) ----
+__global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
+                             long long ntot, long long ctot, int* slot, unsigned* err);
+__global__ void k_process_donors(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
+                                 const int* slot, int K, const double* qres,
+                                 const HoleMapDev* hm, int nhm, long long ntot, int* iblank,
+                                 double* node_res, unsigned char* m0, unsigned char* m1);
+__global__ void k_dilate(const int* conn8, const unsigned char* cell_nv, const unsigned char* cell_blk,
+                         const BlockInfo* bi, long long ctot, int iter, const unsigned char* m0,
+                         unsigned char* m1);
+__global__ void k_fringe_big(const unsigned char* m1, const int* iblank, long long ntot, double* node_res);
+__global__ void k_select(const unsigned char* node_blk, const BlockInfo* bi, const int* slot, int K,
+                         const int* qcell, const double* cell_res, long long ntot, int* iblank,
+                         const double* node_res, unsigned long long* rkey, int* rval, int* rcount,
+                         int rcap, unsigned* err);
+__global__ void k_interp_marks(const unsigned long long* rkey, const int* rval, const int* rcount,
+                               const int* qcell, const int* conn8, const unsigned char* cell_nv,
+                               const int* iblank, const double* node_res, unsigned char* cmark,
+                               int* reset_t);
+__global__ void k_interp(const double* x, const unsigned long long* rkey, const int* rval,
+                         const int* rcount, const int* qcell, const int* conn8,
+                         const unsigned char* cell_nv, const unsigned char* node_blk,
+                         const BlockInfo* bi, const int* iblank, const double* node_res,
+                         const int* reset_t, int* it_node, double* it_w, int* it_rec, int* it_don,
+                         unsigned char* it_nv, unsigned char* it_cancel, double* rres,
+                         int* interp2rec, unsigned* err);
+__global__ void k_cancel(const unsigned char* cmark, long long ntot, const int* slot, int K,
+                         const int* qcell, const double* cell_res, const int* interp2rec,
+                         unsigned char* it_cancel);
+__global__ void k_iblank_clear(int* iblank, long long ntot);
+__global__ void k_iblank_set(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
+                             int* iblank);
+__global__ void k_cell_iblank(const int* conn8, const unsigned char* cell_nv, long long ctot,
+                              const int* iblank, int* iblank_cell);
+__global__ void k_count_iblank(const int* iblank, long long ntot, unsigned long long* counters);
+__global__ void k_interp_gather(const int* it_node, const double* it_w, const int* it_don,
+                                const unsigned char* it_nv, const unsigned char* it_cancel,
+                                const int* rcount, const BlockInfo* bi, const double* q, int nvar,
+                                int interptype, double* vals);
+__global__ void k_interp_scatter(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
+                                 const unsigned char* node_blk, const BlockInfo* bi, const double* vals,
+                                 int nvar, int interptype, double* q);
+
+}  // namespace tb
