@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the TIOGA overset-connectivity path on B200.
+
+One step = one tioga_performconnectivity_ call (hole maps, box pairs, query
+gathering, donor search with Newton containment, donor selection and
+cancellation, final iblanks) on the mixed-element workload: a 257^3 Cartesian
+background whose z<0 hexes are split into prisms, plus three 65x65x129
+spherical shells whose first four radial layers are split into tets, prisms
+and pyramids (seeded synthetic mesh, 18.5 M nodes, 27 M cells).
+
+The metric unit is the query point (a receptor-candidate node handed to a
+donor search), as in the reference's own bookkeeping (the nsearch lists).
+
+  value   device-resident inputs (coordinates already in HBM), split-precision
+          search, aggregate over all GPUs (replicas: each GPU runs its own
+          system, no data-path collective)
+  plain   the same with FP64 arithmetic throughout (the plain GPU form)
+  e2e     through the C ABI with the caller's host buffers: coordinates copied
+          host->device and iblank device->host inside every step
+  latency_ms  p50/p99 of the per-step device time (split form)
+
+  python bench.py [--gpus N --steps K --warmup W]
+  python bench.py --impl reference      # the compiled reference on the CPU
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from tioga_b200 import cases  # noqa: E402
+from tioga_b200.capi import TiogaLibrary  # noqa: E402
+
+METRIC = "connectivity receptors/s & p99 latency vs plain GPU form, 0 iblank/donor mismatch"
+UNIT = "receptors/s"
+WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherical shells "
+            "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
+PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
+# bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
+CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
+CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
+                   "4 split layers): one connectivity call per sample")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="tioga_b200", choices=["tioga_b200", "reference"])
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-reps", type=int, default=3)
+    p.add_argument("--small", action="store_true", help="cfg1 geometry at test size (smoke runs)")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, replicas)
+# ---------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    def __init__(self, ws, device):
+        self.ws = ws
+        self.pg = None
+        if ws > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=device)
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: str):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.index, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def pinned_copy(system):
+    """The caller's arrays in pinned host memory (coordinates and iblank)."""
+    import torch
+    blocks, ibls, keep = [], [], []
+    for b in system.blocks:
+        xt = torch.empty((b.nnodes, 3), dtype=torch.float64, pin_memory=True)
+        xt.numpy()[:] = b.x
+        it = torch.ones(b.nnodes, dtype=torch.int32, pin_memory=True)
+        keep += [xt, it]
+        blocks.append(cases.Block(b.tag, xt.numpy(), b.cells, b.wbc, b.obc, b.name))
+        ibls.append(it.numpy())
+    return cases.System(blocks, system.name, system.meta), ibls, keep
+
+
+def run_gpu(args, ws, rank, local, dist):
+    import torch
+
+    import tioga_b200 as tb
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    system = cases.small_config1(args.seed) if args.small else cases.config1(args.seed)
+    psys, ibls, keep = pinned_copy(system)
+    lib = TiogaLibrary(tb.library_path())
+    tb.extras(lib.lib)
+    lib.init()
+    if lib.lib.tioga_b200_last_error() != 0:
+        raise RuntimeError("libtioga_b200 could not initialise the GPU")
+    lib.register_system(psys, ibls)
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+    lib.preprocess_grids()
+    lib.performconnectivity()
+    if lib.lib.tioga_b200_last_error() != 0:
+        raise RuntimeError("connectivity failed")
+
+    def timed(precision, resident, steps, warmup, clocks=None):
+        tb.set_int(lib.lib, "tioga_b200_set_precision_", precision)
+        tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", resident)
+        for _ in range(warmup):
+            lib.performconnectivity()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        phases, launches = [], 0
+        dist.barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        ev[0].record(stream)
+        for k in range(steps):
+            lib.performconnectivity()
+            ev[k + 1].record(stream)
+            phases.append(tb.timing(lib.lib))
+            launches += tb.stats(lib.lib)["launches"]
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        dist.barrier()
+        if lib.lib.tioga_b200_last_error() != 0:
+            raise RuntimeError("connectivity failed during timing")
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        total = dist.max(ev[0].elapsed_time(ev[steps]))
+        st = tb.stats(lib.lib)
+        avg = {k: float(np.mean([p[k] for p in phases])) for k in phases[0]}
+        return total / steps, per, st, avg, launches, clk
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    idx = vis.split(",")[local] if vis else str(local)
+    clocks = Clocks(idx)
+    ms_split, per_split, st, ph, launches, clk = timed(1, 1, args.steps, args.warmup, clocks)
+    ms_plain, per_plain, st_plain, ph_plain, _, _ = timed(0, 1, args.steps, args.warmup)
+    ms_e2e, per_e2e, st_e2e, ph_e2e, _, _ = timed(1, 0, args.steps, args.warmup)
+    Q = st["nquery"]
+    assert st_plain["nquery"] == Q and st_e2e["nquery"] == Q
+    h2d = sum(24 * b.nnodes for b in system.blocks)
+    d2h = sum(4 * b.nnodes for b in system.blocks)
+    # dominant kernel: the fused search (one launch per step)
+    search_ms = ph["search"]
+    alg_bytes = Q * 37 + st["ncand"] * 41 + st["cand_verts"] * 24
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (search_ms * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": ws * Q / (ms_split * 1e-3), "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator tioga_b200.cases)",
+        "config": {"workload": WORKLOAD if not args.small else "cfg1 geometry at test size",
+                   "nodes": system.nnodes, "cells": system.ncells, "blocks": len(system.blocks),
+                   "query_points": Q, "receptors": st["nreceptor"], "holes": st["nhole"],
+                   "precision": "fp32 Newton screen + fp64 refinement",
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (coordinates %.0f MB, connectivity %.0f MB)" % (
+                       h2d / 1e6, sum(32 * b.ncells for b in system.blocks) / 1e6)},
+        "latency_ms": {"p50": float(np.percentile(per_split, 50)), "p99": float(np.percentile(per_split, 99)),
+                       "max": float(np.max(per_split))},
+        "plain": {"value": ws * Q / (ms_plain * 1e-3), "ms_per_step": ms_plain,
+                  "p99_ms": float(np.percentile(per_plain, 99)), "precision": "fp64 throughout"},
+        "speedup_vs_plain": ms_plain / ms_split,
+        "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+        "roofline": {"kernel": "k_search (fused tree traversal + Newton containment)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "algorithmic_bytes": alg_bytes, "launch_ms": search_ms,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "phases_ms": ph,
+        "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
+                   "donors": st["ndonor"]},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
+    lib.delete()
+    del keep
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU: the compiled reference (or the C restatement) on a bounded sample
+# ---------------------------------------------------------------------------
+def sample_query_count(sample):
+    """Q of the sample, from the C restatement's query lists (identical to the
+    reference's; cheap next to the timed calls)."""
+    t = TiogaLibrary(PORT_LIB)
+    t.init()
+    t.register_system(sample)
+    t.preprocess_grids()
+    t.performconnectivity()
+    ns, nd, tot = C.c_int(), C.c_int(), 0
+    for b in sample.blocks:
+        t.lib.tioga_oracle_searchstats(C.c_int(b.tag), C.byref(ns), C.byref(nd))
+        tot += ns.value
+    t.delete()
+    return tot
+
+
+def cpu_reference(reps: int, warmup: int = 1):
+    lib = REF_LIB if os.path.exists(REF_LIB) else PORT_LIB
+    kind = "reference" if lib == REF_LIB else "port"
+    if not os.path.exists(lib):
+        return None, "no CPU build of the reference or the port (run `make -C oracle`)"
+    sample = cases.config1(1, **CPU_SAMPLE)
+    Q = sample_query_count(sample)
+    t = TiogaLibrary(lib)
+    t.init()
+    t.register_system(sample)
+    t.preprocess_grids()
+    for _ in range(warmup):
+        t.performconnectivity()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        t.performconnectivity()
+        times.append(time.perf_counter() - t0)
+    t.delete()
+    mean = float(np.mean(times))
+    return {"value": Q / mean, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": CPU_SAMPLE_TEXT + f" (Q={Q} query points, {reps} timed calls, mean {mean:.2f} s)",
+            "per_step_s": times}, None
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        res, why = cpu_reference(args.steps, args.warmup)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * float(np.mean(res["per_step_s"])), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded mesh generator tioga_b200.cases)",
+                "config": {"workload": WORKLOAD, "sample": res["sample"]},
+                "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    dist = Dist(ws, None)
+    try:
+        if ws > 1:
+            import torch
+            torch.cuda.set_device(local)
+        out = run_gpu(args, ws, rank, local, dist)
+    finally:
+        dist.close()
+    if rank == 0:
+        if ws == 1 and not args.no_cpu_baseline:
+            res, why = cpu_reference(args.cpu_reps)
+            out["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                                   if res else {"unavailable": why})
+        else:
+            out["cpu_baseline"] = None
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -107,8 +107,12 @@ void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
 /* Counters of the last connectivity call: [0] query points, [1] queries with
  * a donor, [2] order-dependent ties, [3] Newton candidates, [4] FP64
  * refinements, [5] receptors, [6] holes, [7] donor records, [8] device
- * error bits, [9] pairs of blocks. */
+ * error bits, [9] pairs of blocks, [10] kernels launched by the library,
+ * [11] sum of the candidates' vertex counts. */
 void tioga_b200_stats_(long long out[16]);
+/* Run on the caller's CUDA stream (a cudaStream_t; NULL restores the
+ * library's own stream), e.g. to time the calls with the caller's events. */
+void tioga_b200_set_stream_(void *stream);
 /* Device time (ms) of the last connectivity call per phase: [0] coordinate
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,

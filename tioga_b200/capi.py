@@ -56,10 +56,12 @@ class TiogaLibrary:
         self._order.clear()
 
     # -- registration ------------------------------------------------------
-    def registergrid_data_mb(self, bid: int, block):
-        """Register one cases.Block under block id ``bid`` (1-based)."""
+    def registergrid_data_mb(self, bid: int, block, ibl=None):
+        """Register one cases.Block under block id ``bid`` (1-based).  ``ibl``
+        may supply the iblank array (e.g. pinned host memory)."""
         x = np.ascontiguousarray(block.x, dtype=np.float64).reshape(-1)
-        ibl = np.ones(block.nnodes, dtype=np.int32)
+        if ibl is None:
+            ibl = np.ones(block.nnodes, dtype=np.int32)
         wbc = np.ascontiguousarray(block.wbc, dtype=np.int32) + 1
         obc = np.ascontiguousarray(block.obc, dtype=np.int32) + 1
         conns = []
@@ -83,9 +85,9 @@ class TiogaLibrary:
         if block.tag not in self._order:
             self._order.append(block.tag)
 
-    def register_system(self, system):
+    def register_system(self, system, iblanks=None):
         for bid, b in enumerate(system.blocks, start=1):
-            self.registergrid_data_mb(bid, b)
+            self.registergrid_data_mb(bid, b, None if iblanks is None else iblanks[bid - 1])
 
     # -- settings ----------------------------------------------------------
     def setsymmetry(self, isym: int):

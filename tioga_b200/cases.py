@@ -227,14 +227,16 @@ def config0(seed: int = 0, nbg: int = 65, nr: int = 33, nt: int = 33, nphi: int 
 
 
 def shell_centres(rng: np.random.Generator, nshell: int, rwall: np.ndarray, router: np.ndarray,
-                  box: float = 3.0, margin: float = 0.05, tries: int = 10000) -> np.ndarray:
-    """Random centres in [-box, box]^3 such that no wall sphere lies inside
-    another shell (walls stay out of every other mesh's donor region)."""
+                  box: float = 3.0, margin: float = 0.05, tries: int = 10000,
+                  domain: float = 4.9) -> np.ndarray:
+    """Random centres in [-box, box]^3 such that every shell lies inside the
+    background box [-domain, domain]^3 and no wall sphere lies inside another
+    shell (walls stay out of every other mesh's donor region)."""
     c = np.zeros((nshell, 3))
     for a in range(nshell):
         for _ in range(tries):
             cand = rng.uniform(-box, box, 3)
-            ok = True
+            ok = bool(np.all(np.abs(cand) + router[a] <= domain))
             for b in range(a):
                 d = np.linalg.norm(cand - c[b])
                 if d < max(router[a] + rwall[b], router[b] + rwall[a]) + margin:

@@ -211,6 +211,12 @@ void tioga_b200_stats_(long long out[16]) {
   out[7] = s.nrecords;
   out[8] = s.error;
   out[9] = s.npairs;
+  out[10] = s.launches;
+  out[11] = s.cand_verts;
+}
+
+void tioga_b200_set_stream_(void* stream) {
+  if (ready("tioga_b200_set_stream_")) g_tg->set_stream((cudaStream_t)stream);
 }
 
 void tioga_b200_timing_(float out[16]) {

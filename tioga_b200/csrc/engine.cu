@@ -31,6 +31,7 @@ static int sync_check() {
 }
 #define TB_LAUNCHED(name)                                                              \
   do {                                                                                 \
+    nlaunch_++;                                                                        \
     cudaError_t le_ = cudaGetLastError();                                              \
     if (le_ == cudaSuccess && sync_check()) le_ = cudaStreamSynchronize(stream_);      \
     if (le_ != cudaSuccess) {                                                          \
@@ -46,7 +47,8 @@ static int sync_check() {
   } while (0)
 
 Engine::Engine() {
-  cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking);
+  stream_ = own_stream_;
   for (auto& e : ev_) cudaEventCreate(&e);
 }
 
@@ -67,7 +69,13 @@ Engine::~Engine() {
   it_don_.release(); it_nv_.release(); it_cancel_.release(); rres_.release(); q_.release();
   qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
-  if (stream_) cudaStreamDestroy(stream_);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+// Work on the caller's stream (nullptr: back to the library's own stream).
+void Engine::set_stream(cudaStream_t s) {
+  cudaStreamSynchronize(stream_);
+  stream_ = s ? s : own_stream_;
 }
 
 int Engine::find_tag(int tag) const {
@@ -752,6 +760,7 @@ int Engine::connectivity() {
     return -1;
   }
   stats_ = Stats{};
+  nlaunch_ = 0;
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   if (!coords_resident_) TB_TRY(upload_coords());
@@ -798,6 +807,8 @@ int Engine::connectivity() {
   stats_.nreceptor = (long long)cnt[5];
   stats_.nrecords = nrec_;
   stats_.npairs = npairs_;
+  stats_.launches = nlaunch_;
+  stats_.cand_verts = (long long)cnt[6];
   stats_.error = err;
   float ms[9];
   for (int i = 1; i < 9; i++) cudaEventElapsedTime(&ms[i], ev_[i - 1], ev_[i]);

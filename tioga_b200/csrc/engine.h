@@ -100,6 +100,8 @@ struct Stats {
   long long nhole = 0;        // final iblank == 0
   long long nrecords = 0;     // chosen donors (before cancellation)
   long long npairs = 0;       // intersecting (receptor, donor) block pairs
+  long long launches = 0;     // kernels this library launched in the call
+  long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
   unsigned error = 0;
 };
 
@@ -125,6 +127,7 @@ class Engine {
   void set_precision(int p) { precision_ = p; }
   void set_coords_resident(int r) { coords_resident_ = r; }
   void set_early_exit(int e) { early_exit_ = e; }
+  void set_stream(cudaStream_t s);
 
   // the path
   int preprocess();
@@ -179,6 +182,8 @@ class Engine {
   long long ntot_ = 0, ctot_ = 0, inc_tot_ = 0;
   int last_error_ = 0;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t own_stream_ = nullptr;
+  long long nlaunch_ = 0;
   cudaEvent_t ev_[12];
 
   // flat device arrays

@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(128) k_search(
     const double* __restrict__ tnode64, const int* __restrict__ qnode, const int* __restrict__ qdon,
     long long nq, int early_exit, int* __restrict__ qcell, unsigned char* __restrict__ qtie,
     unsigned long long* __restrict__ counters) {
-  unsigned long long my_cand = 0, my_refine = 0, my_tie = 0, my_found = 0;
+  unsigned long long my_cand = 0, my_refine = 0, my_tie = 0, my_found = 0, my_verts = 0;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
     const int g = qnode[q];
@@ -710,6 +710,7 @@ __global__ void __launch_bounds__(128) k_search(
             if (!in_box64(p, lo, hi)) continue;
           }
           my_cand++;
+          my_verts += nv;
           const bool big = cell_res[c] == kBig;
           int cls = -1;
           if (FORM == 1 && nv != 4) cls = screen32(xv, p, nv);
@@ -749,12 +750,14 @@ __global__ void __launch_bounds__(128) k_search(
     my_refine += __shfl_xor_sync(0xffffffffu, my_refine, o);
     my_tie += __shfl_xor_sync(0xffffffffu, my_tie, o);
     my_found += __shfl_xor_sync(0xffffffffu, my_found, o);
+    my_verts += __shfl_xor_sync(0xffffffffu, my_verts, o);
   }
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&counters[0], my_cand);
     atomicAdd(&counters[1], my_refine);
     atomicAdd(&counters[2], my_tie);
     atomicAdd(&counters[3], my_found);
+    atomicAdd(&counters[6], my_verts);
   }
 }
 
