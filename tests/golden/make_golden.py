@@ -1,0 +1,93 @@
+"""Generate the golden fixtures from the compiled TIOGA reference.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The reference (oracle/_ref/libtioga_ref.so, compiled from the reference's own
+sources with a single-rank MPI shim) is driven through its C API on small
+seeded systems; its outputs are stored as compressed .npz files next to this
+script together with a digest of the inputs.  The CPU tests check the C
+restatement in oracle/ against these files, and the GPU tests check the B200
+library against them, so parity is pinned to the reference itself.
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from tioga_b200 import cases  # noqa: E402
+from tioga_b200.capi import run_system  # noqa: E402
+
+
+def user_resolutions(system, seed):
+    """Seeded user node/cell resolutions for the first block."""
+    rng = np.random.default_rng(seed)
+    b = system.blocks[0]
+    nres = rng.uniform(0.5, 1.5, b.nnodes) * 1e-2
+    cres = rng.uniform(0.5, 1.5, b.ncells) * 1e-2
+    return {b.tag: (nres, cres)}
+
+
+# name -> (system factory, settings, nvar, itype, field seed)
+CASES = {
+    "cfg0_small_s0": (lambda: cases.small_config0(0), {}, 5, "row", 11),
+    "cfg1_small_s1": (lambda: cases.small_config1(1), {}, 5, "row", 12),
+    "cfg0_small_s1_opts": (lambda: cases.small_config0(1), dict(isym=0, nfringe=2, mexclude=1), 3, "column", 13),
+    "cfg1_small_s2_userres": (lambda: cases.small_config1(2), "userres", 2, "row", 14),
+}
+
+
+def digest(system):
+    h = hashlib.sha256()
+    for b in system.blocks:
+        h.update(np.ascontiguousarray(b.x).tobytes())
+        for nv, c in b.cells:
+            h.update(np.int32(nv).tobytes())
+            h.update(np.ascontiguousarray(c, dtype=np.int32).tobytes())
+        h.update(np.ascontiguousarray(b.wbc, dtype=np.int32).tobytes())
+        h.update(np.ascontiguousarray(b.obc, dtype=np.int32).tobytes())
+    return h.hexdigest()
+
+
+def settings_for(name, system):
+    s = CASES[name][1]
+    if s == "userres":
+        return {"resolutions": user_resolutions(system, 99)}
+    return dict(s)
+
+
+def run_case(lib, name):
+    fac, _, nvar, itype, fseed = CASES[name]
+    system = fac()
+    q = cases.fields(system, nvar=nvar, seed=fseed)
+    out = run_system(lib, system, q_blocks=q, nvar=nvar, itype=itype, **settings_for(name, system))
+    return system, q, out
+
+
+def save(name, system, q, out):
+    arrs = {"digest": np.array(digest(system))}
+    for b, q0 in zip(system.blocks, q):
+        t = b.tag
+        arrs[f"iblank_{t}"] = out["iblank"][t].astype(np.int8)
+        rec, ind, frac = out["donors"][t]
+        arrs[f"receptors_{t}"] = rec
+        arrs[f"indices_{t}"] = ind
+        arrs[f"frac_{t}"] = frac
+        changed = np.nonzero(out["q"][t] != q0)[0]
+        arrs[f"qidx_{t}"] = changed.astype(np.int32)
+        arrs[f"qval_{t}"] = out["q"][t][changed]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+
+
+if __name__ == "__main__":
+    lib = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
+    if not os.path.exists(lib):
+        sys.exit("build the compiled reference first: make -C oracle ref")
+    for name in CASES:
+        system, q, out = run_case(lib, name)
+        save(name, system, q, out)
+        print(name, "saved")

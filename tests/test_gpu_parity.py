@@ -85,3 +85,29 @@ def test_linear_field_exact():
         err = np.abs(gpu["q"][b.tag].reshape(-1, 5) - exact[:, None]).max()
         assert err < 1e-12
         assert (gpu["iblank"][b.tag] == -1).sum() > 0
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "split"])
+@pytest.mark.parametrize("name", ["cfg0_small_s0", "cfg1_small_s1", "cfg0_small_s1_opts",
+                                  "cfg1_small_s2_userres"])
+def test_gpu_matches_reference_fixtures(name, precision):
+    """The GPU library against the compiled reference's own outputs."""
+    from tests.golden import make_golden as mg
+    from tests.test_oracle_golden import load
+    g = load(name)
+    fac, _, nvar, itype, fseed = mg.CASES[name]
+    system = fac()
+    assert str(g["digest"]) == mg.digest(system)
+    q = cases.fields(system, nvar=nvar, seed=fseed)
+    out = run_system(tb.library_path(), system, q_blocks=q, nvar=nvar, itype=itype,
+                     setup=_gpu_setup(precision), **mg.settings_for(name, system))
+    for b, q0 in zip(system.blocks, q):
+        t = b.tag
+        np.testing.assert_array_equal(out["iblank"][t], g[f"iblank_{t}"].astype(np.int32))
+        rec, ind, frac = out["donors"][t]
+        np.testing.assert_array_equal(rec, g[f"receptors_{t}"])
+        np.testing.assert_array_equal(ind, g[f"indices_{t}"])
+        assert np.array_equal(frac.view(np.int64), g[f"frac_{t}"].view(np.int64))
+        changed = np.nonzero(out["q"][t] != q0)[0]
+        np.testing.assert_array_equal(changed, g[f"qidx_{t}"])
+        assert np.array_equal(out["q"][t][changed].view(np.int64), g[f"qval_{t}"].view(np.int64))
