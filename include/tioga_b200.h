@@ -113,6 +113,23 @@ void tioga_b200_stats_(long long out[16]);
 /* Run on the caller's CUDA stream (a cudaStream_t; NULL restores the
  * library's own stream), e.g. to time the calls with the caller's events. */
 void tioga_b200_set_stream_(void *stream);
+/* Interpolate nvar fields of a device array d_q in place from donor
+ * stencils the caller keeps on the device, allocating no device memory
+ * (no counterpart in TIOGA).  For callers that cannot allocate: a solver
+ * whose time step runs inside a captured CUDA graph (cudaMalloc is not
+ * allowed while a stream is captured), or one whose memory pool must not be
+ * disturbed by cudaMalloc's device-wide synchronisation.  Stencil r has
+ * d_nweights[r] <= 8 entries at d_inode[9r+m] (node index into d_q) with
+ * weights d_weights[9r+m], and writes node d_receptor[r]; interptype 0 is
+ * row layout (q[node*nvar+k]), 1 column (q[k*nnodes+node]).  The
+ * gather-to-scatter staging lives in a fixed device array of 2^20 doubles:
+ * nrec*nvar above that is rejected (-1).  The first call on a device looks up
+ * that array's address (make it before any stream capture); calls that
+ * overlap on the GPU share the array and race.  Asynchronous on `stream`;
+ * returns 0, -1 for bad arguments, -2 for a CUDA error. */
+int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights, const int *d_nweights,
+                                    const int *d_receptor, int nrec, double *d_q, long long nnodes,
+                                    int nvar, int interptype, void *stream);
 /* Device time (ms) of the last connectivity call per phase: [0] coordinate
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,
