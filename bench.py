@@ -62,7 +62,10 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-reps", type=int, default=3)
-    p.add_argument("--small", action="store_true", help="cfg1 geometry at test size (smoke runs)")
+    p.add_argument("--size", default="full", choices=["full", "medium", "small"],
+                   help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
+    p.add_argument("--forms", default="split,plain,e2e",
+                   help="comma list of measured forms (the first one gives `value`)")
     return p.parse_args()
 
 
@@ -183,7 +186,12 @@ def run_gpu(args, ws, rank, local, dist):
     import tioga_b200 as tb
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    system = cases.small_config1(args.seed) if args.small else cases.config1(args.seed)
+    if args.size == "small":
+        system = cases.small_config1(args.seed)
+    elif args.size == "medium":
+        system = cases.config1(args.seed, nbg=161, nshell=3, nr=49, nt=49, nphi=97, split_layers=4)
+    else:
+        system = cases.config1(args.seed)
     psys, ibls, keep = pinned_copy(system)
     lib = TiogaLibrary(tb.library_path())
     tb.extras(lib.lib)
@@ -229,11 +237,19 @@ def run_gpu(args, ws, rank, local, dist):
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     idx = vis.split(",")[local] if vis else str(local)
     clocks = Clocks(idx)
+    forms = args.forms.split(",")
     ms_split, per_split, st, ph, launches, clk = timed(1, 1, args.steps, args.warmup, clocks)
-    ms_plain, per_plain, st_plain, ph_plain, _, _ = timed(0, 1, args.steps, args.warmup)
-    ms_e2e, per_e2e, st_e2e, ph_e2e, _, _ = timed(1, 0, args.steps, args.warmup)
     Q = st["nquery"]
-    assert st_plain["nquery"] == Q and st_e2e["nquery"] == Q
+    if "plain" in forms:
+        ms_plain, per_plain, st_plain, ph_plain, _, _ = timed(0, 1, args.steps, args.warmup)
+        assert st_plain["nquery"] == Q
+    else:
+        ms_plain, per_plain = float("nan"), [float("nan")]
+    if "e2e" in forms:
+        ms_e2e, per_e2e, st_e2e, ph_e2e, _, _ = timed(1, 0, args.steps, args.warmup)
+        assert st_e2e["nquery"] == Q
+    else:
+        ms_e2e = float("nan")
     h2d = sum(24 * b.nnodes for b in system.blocks)
     d2h = sum(4 * b.nnodes for b in system.blocks)
     # dominant kernel: the fused search (one launch per step)
@@ -251,7 +267,7 @@ def run_gpu(args, ws, rank, local, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded mesh generator tioga_b200.cases)",
-        "config": {"workload": WORKLOAD if not args.small else "cfg1 geometry at test size",
+        "config": {"workload": WORKLOAD if args.size == "full" else f"cfg1 geometry, {args.size} size",
                    "nodes": system.nnodes, "cells": system.ncells, "blocks": len(system.blocks),
                    "query_points": Q, "receptors": st["nreceptor"], "holes": st["nhole"],
                    "precision": "fp32 Newton screen + fp64 refinement",
