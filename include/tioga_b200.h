@@ -102,6 +102,10 @@ void tioga_b200_set_coords_resident_(int *flag);
 /* Bind block btag's solution as a DEVICE array (same layout as the host
  * one); tioga_dataupdate_mb_ then updates it without host copies. */
 void tioga_b200_registersolution_device_(int *btag, double *dq);
+/* Write block btag's node iblank into a DEVICE array of nnodes ints instead
+ * of the host array given at registration (solvers that keep iblank on the
+ * GPU); NULL returns to the host array. */
+void tioga_b200_registeriblank_device_(int *btag, int *d_ibl);
 /* Cell iblank of block btag (ncells ints), for any block. */
 void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
 /* Counters of the last connectivity call: [0] query points, [1] queries with

@@ -193,6 +193,9 @@ void tioga_b200_set_coords_resident_(int* flag) {
 void tioga_b200_registersolution_device_(int* btag, double* dq) {
   if (ready("tioga_b200_registersolution_device_")) set_rc(g_tg->register_solution(*btag, dq, true));
 }
+void tioga_b200_registeriblank_device_(int* btag, int* d_ibl) {
+  if (ready("tioga_b200_registeriblank_device_")) set_rc(g_tg->register_iblank_device(*btag, d_ibl));
+}
 void tioga_b200_getcelliblank_(int* btag, int* out) {
   if (ready("tioga_b200_getcelliblank_")) set_rc(g_tg->cell_iblank(*btag, out));
 }

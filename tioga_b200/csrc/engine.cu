@@ -149,6 +149,13 @@ int Engine::set_cell_iblank(int tag, int* ibc) {
   return 0;
 }
 
+int Engine::register_iblank_device(int tag, int* d_ibl) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].dibl = d_ibl;
+  return 0;
+}
+
 int Engine::register_solution(int tag, double* q, bool device) {
   int ib = find_tag(tag);
   if (ib < 0 || !connected_) {
@@ -360,18 +367,55 @@ int Engine::build_tree_topology() {
   TB_CUDA(cub_tmp_.ensure(tmp));
   cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
                                   (int)ctot_, 0, 40, stream_);
+  TB_CUDA(inv_sorted_.ensure(ctot_));
+  k_invert<<<grid_for(ctot_, kT), kT, 0, stream_>>>(sorted_cell_.p, ctot_, inv_sorted_.p);
+  TB_LAUNCHED("k_invert");
   long long off = 0;
-  for (auto& B : bi_) {
+  int maxlev = 0;
+  std::vector<int> lev(bi_.size());
+  for (size_t b = 0; b < bi_.size(); b++) {
+    BlockInfo& B = bi_[b];
     long long nleaf = std::max(1ll, ((long long)B.ncells + kLeafCells - 1) / kLeafCells);
     long long P = 1;
-    while (P < nleaf) P <<= 1;
+    int L = 0;
+    while (P < nleaf) {
+      P <<= 1;
+      L++;
+    }
     B.P = (int)P;
     B.tree_off = (int)off;
     off += 2 * P - 1;
+    lev[b] = L;
+    maxlev = std::max(maxlev, L);
   }
   tree_nodes_ = off;
+  // refit groups: pass p starts at level L-8p of each block and climbs 8 levels
+  std::vector<RefitGroup> groups;
+  refit_pass_off_.assign(1, 0);
+  for (int pass = 0; 8 * pass <= maxlev; pass++) {
+    for (size_t b = 0; b < bi_.size(); b++) {
+      const int L = lev[b] - 8 * pass;
+      if (L < 0 || (pass > 0 && L == 0 && lev[b] - 8 * (pass - 1) <= 8)) continue;
+      if (pass > 0 && lev[b] - 8 * (pass - 1) <= 8) continue;  // reached the root already
+      const long long width = 1ll << L;
+      for (long long f = 0; f < width; f += 256) groups.push_back(RefitGroup{(int)b, L, (int)f});
+    }
+    refit_pass_off_.push_back((int)groups.size());
+  }
+  TB_CUDA(refit_groups_.ensure(groups.size()));
+  TB_CUDA(cudaMemcpyAsync(refit_groups_.p, groups.data(), groups.size() * sizeof(RefitGroup),
+                          cudaMemcpyHostToDevice, stream_));
+  // query-gathering tiles of kNodeTile nodes per block
+  h_tile_base_.assign(bi_.size() + 1, 0);
+  for (size_t b = 0; b < bi_.size(); b++)
+    h_tile_base_[b + 1] = h_tile_base_[b] + (bi_[b].nnodes + kNodeTile - 1) / kNodeTile;
+  TB_CUDA(tile_base_.ensure(bi_.size() + 1));
+  TB_CUDA(cudaMemcpyAsync(tile_base_.p, h_tile_base_.data(), h_tile_base_.size() * sizeof(long long),
+                          cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
   TB_CUDA(cbox_.ensure(2 * ctot_));
   TB_CUDA(tnode_.ensure(2 * tree_nodes_));
+  TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   return 0;
 }
 
@@ -428,8 +472,14 @@ int Engine::preprocess() {
     TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
                             stream_));
   }
-  for (auto& H : hb_)
-    for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;  // preprocess sets iblank = 1 (MeshBlock.C:80)
+  for (size_t b = 0; b < hb_.size(); b++) {  // preprocess sets iblank = 1 (MeshBlock.C:80)
+    HostBlock& H = hb_[b];
+    if (H.dibl)
+      TB_CUDA(cudaMemcpyAsync(H.dibl, iblank_.p + bi_[b].node_off, H.nnodes * sizeof(int),
+                              cudaMemcpyDeviceToDevice, stream_));
+    else
+      for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;
+  }
   TB_CUDA(cudaStreamSynchronize(stream_));
   preprocessed_ = true;
   connected_ = false;
@@ -538,39 +588,17 @@ int Engine::run_pairs_and_refit() {
                           cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   if (npairs_ == 0) return 0;
-  // tree refit to the current coordinates
+  // refit to the current coordinates: one pass over the cells (tree-order
+  // cell boxes + reduced boxes of every pair), then the tree levels, then the
+  // node tiles of the query gathering
   const bool fp64 = (precision_ == 0);
   if (fp64) {
     TB_CUDA(cbox64_.ensure(6 * ctot_));
     TB_CUDA(tnode64_.ensure(6 * tree_nodes_));
   }
-  k_cell_boxes<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, sorted_cell_.p, ctot_,
-                                                        cbox_.p, fp64 ? cbox64_.p : nullptr);
-  TB_LAUNCHED("k_cell_boxes");
-  std::vector<long long> leaf_base(nb + 1, 0);
-  for (int b = 0; b < nb; b++) leaf_base[b + 1] = leaf_base[b] + bi_[b].P;
-  TB_CUDA(visit_.ensure(tree_nodes_ + nb + 1));
-  TB_CUDA(cudaMemsetAsync(visit_.p, 0, tree_nodes_ * sizeof(int), stream_));
-  long long* d_lb = reinterpret_cast<long long*>(visit_.p + tree_nodes_);
-  // leaf_base lives in a small separate buffer
-  TB_CUDA(leafbase_.ensure(nb + 1));
-  TB_CUDA(cudaMemcpyAsync(leafbase_.p, leaf_base.data(), (nb + 1) * sizeof(long long),
-                          cudaMemcpyHostToDevice, stream_));
-  (void)d_lb;
-  k_tree_leaves<<<grid_for(leaf_base[nb], kT), kT, 0, stream_>>>(
-      d_bi_.p, nb, cbox_.p, fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, visit_.p,
-      leaf_base[nb], leafbase_.p);
-  TB_LAUNCHED("k_tree_leaves");
-  // reduced boxes, one pass over each donor's cells
   std::vector<unsigned long long> acc(6 * npairs_);
   for (int p = 0; p < npairs_; p++)
-    for (int j = 0; j < 3; j++) {
-      acc[6 * p + j] = 0;
-      acc[6 * p + j + 3] = 0;
-    }
-  // initial values BIG / -BIG as getReducedOBB (MeshBlock.C:790-794)
-  for (int p = 0; p < npairs_; p++)
-    for (int j = 0; j < 3; j++) {
+    for (int j = 0; j < 3; j++) {  // BIG / -BIG as getReducedOBB starts (MeshBlock.C:790-794)
       double lo = kBig, hi = -kBig;
       unsigned long long bl, bh;
       memcpy(&bl, &lo, 8);
@@ -581,14 +609,21 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  std::vector<int> has(nb, 0);
-  for (int p = 0; p < npairs_; p++) has[h_pairs_[p].don] = 1;
-  for (int b = 0; b < nb; b++)
-    if (has[b] && bi_[b].ncells > 0) {
-      k_reduced_obb<<<grid_for(bi_[b].ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, d_bi_.p, b,
-                                                                     d_pairs_.p, npairs_, pair_acc_.p);
-      TB_LAUNCHED("k_reduced_obb");
-    }
+  k_cell_pass<<<grid_for(ctot_, 256), 256, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, inv_sorted_.p,
+                                                         ctot_, d_bi_.p, d_pairs_.p, npairs_, cbox_.p,
+                                                         fp64 ? cbox64_.p : nullptr, pair_acc_.p);
+  TB_LAUNCHED("k_cell_pass");
+  for (size_t pass = 0; pass + 1 < refit_pass_off_.size(); pass++) {
+    const int g0 = refit_pass_off_[pass], g1 = refit_pass_off_[pass + 1];
+    if (g1 <= g0) continue;
+    k_tree_levels<<<g1 - g0, 256, 0, stream_>>>(d_bi_.p, refit_groups_.p + g0, pass == 0 ? 1 : 0, cbox_.p,
+                                                fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr);
+    TB_LAUNCHED("k_tree_levels");
+  }
+  if (h_tile_base_.back() > 0) {
+    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p);
+    TB_LAUNCHED("k_node_tiles");
+  }
   k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
   TB_LAUNCHED("k_pair_finish");
   return 0;
@@ -598,14 +633,15 @@ int Engine::run_queries() {
   // ordered compaction of each pair's receptor nodes inside the donor region
   int maxn = 0;
   for (int p = 0; p < npairs_; p++) maxn = std::max(maxn, bi_[h_pairs_[p].rec].nnodes);
-  const int tile = 256 * 8;
+  const int tile = kNodeTile;  // 256 threads x 8 nodes, one node tile
   const int tiles_x = std::max(1, (maxn + tile - 1) / tile);
   const long long ntiles = (long long)tiles_x * npairs_;
   TB_CUDA(tile_cnt_.ensure(ntiles + 1));
   TB_CUDA(tile_off_.ensure(ntiles + 1));
   TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
   dim3 grid(std::min(tiles_x, 148 * 8), npairs_);
-  k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_cnt_.p);
+  k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_cnt_.p, tbox_.p,
+                                           tile_base_.p);
   TB_LAUNCHED("k_query_count");
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
@@ -623,23 +659,59 @@ int Engine::run_queries() {
   TB_CUDA(interp2rec_.ensure(nq));
   if (nq > 0) {
     k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_off_.p,
-                                             node_res_.p, qnode_.p, qdon_.p, qres_.p);
+                                             node_res_.p, qnode_.p, qdon_.p, qres_.p, tbox_.p, tile_base_.p);
     TB_LAUNCHED("k_query_write");
   }
   return 0;
 }
 
+// search in four stages: traversal -> candidate list -> one thread per
+// candidate (exact box test, FP32 screen) -> FP64 refinement -> outcome
 int Engine::run_search() {
   TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
+  TB_CUDA(scount_.ensure(2));
+  TB_CUDA(cudaMemsetAsync(scount_.p, 0, 2 * sizeof(unsigned), stream_));
+  ncand_ = 0;
   if (nq_ == 0) return 0;
-  TB_CUDA(cudaMemsetAsync(qcell_.p, 0xff, nq_ * sizeof(int), stream_));
-  const int threads = 128;
-  const int blocks = (int)std::min<long long>((nq_ + threads - 1) / threads, 148ll * 64);
-  launch_search(precision_ == 0 ? 0 : 1, blocks, threads, stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p,
-                d_bi_.p, sorted_cell_.p, cbox_.p, precision_ == 0 ? cbox64_.p : nullptr, tnode_.p,
-                precision_ == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p, nq_, early_exit_, qcell_.p, qtie_.p,
-                counters_.p);
-  TB_LAUNCHED("k_search");
+  const int form = (precision_ == 0) ? 0 : 1;
+  TB_CUDA(qkey_.ensure(nq_));
+  TB_CUDA(qacc_.ensure(nq_));
+  TB_CUDA(cudaMemsetAsync(qkey_.p, 0xff, nq_ * sizeof(unsigned long long), stream_));
+  TB_CUDA(cudaMemsetAsync(qacc_.p, 0, nq_ * sizeof(unsigned), stream_));
+  long long cap = std::max<long long>(cand_cap_, std::max<long long>(4 * nq_, 1 << 16));
+  unsigned count = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    if (cap >= (1ll << 31)) {
+      fprintf(stderr, "#tioga_b200: more than 2^31 search candidates\n");
+      return -1;
+    }
+    TB_CUDA(cand_.ensure(cap));
+    TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
+    launch_traverse(form, grid_for(nq_, 256), stream_, x_.p, d_bi_.p, cbox_.p, form == 0 ? cbox64_.p : nullptr,
+                    tnode_.p, form == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p, nq_, cand_.p, (int)cap,
+                    scount_.p);
+    TB_LAUNCHED("k_traverse");
+    TB_CUDA(cudaMemcpyAsync(&count, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    cand_cap_ = cap;
+    if ((long long)count <= cap) break;
+    cap = (long long)count + count / 4 + 1024;  // grow and traverse again
+  }
+  ncand_ = count;
+  if (count > 0) {
+    TB_CUDA(refine_.ensure(count));
+    launch_candidates(form, grid_for(count, 256), stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p, sorted_cell_.p,
+                      qnode_.p, cand_.p, (int)count, qkey_.p, qacc_.p, refine_.p, scount_.p + 1, counters_.p);
+    TB_LAUNCHED("k_candidates");
+    if (form == 1) {
+      k_refine<<<grid_for(count / 4 + 1, 128), 128, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_res_.p,
+                                                                  sorted_cell_.p, qnode_.p, cand_.p, refine_.p,
+                                                                  scount_.p + 1, qkey_.p, qacc_.p);
+      TB_LAUNCHED("k_refine");
+    }
+  }
+  k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, qcell_.p, qtie_.p, counters_.p);
+  TB_LAUNCHED("k_search_finish");
   return 0;
 }
 
@@ -745,8 +817,12 @@ int Engine::run_celliblank() {
 
 int Engine::download_iblank() {
   for (size_t b = 0; b < hb_.size(); b++) {
-    TB_CUDA(cudaMemcpyAsync(hb_[b].hibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
-                            cudaMemcpyDeviceToHost, stream_));
+    if (hb_[b].dibl)
+      TB_CUDA(cudaMemcpyAsync(hb_[b].dibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
+                              cudaMemcpyDeviceToDevice, stream_));
+    else
+      TB_CUDA(cudaMemcpyAsync(hb_[b].hibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
+                              cudaMemcpyDeviceToHost, stream_));
     if (hb_[b].h_iblank_cell)
       TB_CUDA(cudaMemcpyAsync(hb_[b].h_iblank_cell, iblank_cell_.p + bi_[b].cell_off,
                               hb_[b].ncells * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -797,10 +873,12 @@ int Engine::connectivity() {
   unsigned err = 0;
   TB_CUDA(cudaMemcpyAsync(cnt, counters_.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaMemcpyAsync(&err, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  unsigned sc[2] = {0, 0};
+  if (npairs_ > 0) TB_CUDA(cudaMemcpyAsync(sc, scount_.p, sizeof(sc), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   stats_.nquery = nq_;
   stats_.ncand = (long long)cnt[0];
-  stats_.nrefine = (long long)cnt[1];
+  stats_.nrefine = (long long)sc[1];
   stats_.nties = (long long)cnt[2];
   stats_.ndonor = (long long)cnt[3];
   stats_.nhole = (long long)cnt[4];

@@ -21,6 +21,7 @@
 namespace tb {
 
 constexpr int kLeafCells = 4;   // cells per BVH leaf
+constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
 
 template <class T>
@@ -66,6 +67,12 @@ struct PairInfo {  // one (receptor block, donor block) pair, src/exchangeBoxes.
   int rec, don;
   double rd[6];    // reduced box accumulator in the donor's OBB frame (ordered bits)
   Obb region;      // donor cells overlapping the receptor OBB, donor axes
+  double wbox[6];  // world-axis box holding the region (tile culling)
+};
+
+// one CTA of the level-by-level tree refit: up to 256 nodes of one level
+struct RefitGroup {
+  int block, level, first;
 };
 
 struct HoleMapInfo {
@@ -88,6 +95,7 @@ struct HostBlock {
   int* h_iblank_cell = nullptr;  // caller array (tioga_setcelliblank_)
   double* hq = nullptr;          // registered host solution
   double* dq = nullptr;          // registered device solution
+  int* dibl = nullptr;           // caller's device iblank array (optional)
 };
 
 struct Stats {
@@ -124,9 +132,9 @@ class Engine {
   int set_resolutions(int tag, double* nres, double* cres);
   int set_cell_iblank(int tag, int* ibc);
   int register_solution(int tag, double* q, bool device);
+  int register_iblank_device(int tag, int* d_ibl);
   void set_precision(int p) { precision_ = p; }
   void set_coords_resident(int r) { coords_resident_ = r; }
-  void set_early_exit(int e) { early_exit_ = e; }
   void set_stream(cudaStream_t s);
 
   // the path
@@ -166,7 +174,6 @@ class Engine {
   std::map<int, int> tag2idx_;
   int isym_ = 3, nfringe_ = 1, mexclude_ = 3;
   int precision_ = 1;        // 0 = FP64 throughout, 1 = FP32 screen + FP64 refine
-  int early_exit_ = 0;
   int coords_resident_ = 0;  // 1: the caller promises x has not moved
   bool topo_dirty_ = true;
   bool preprocessed_ = false;
@@ -179,6 +186,19 @@ class Engine {
   DBuf<int> visit_;
   DBuf<long long> leafbase_;
   DBuf<unsigned long long> pair_acc_;
+  // search stages
+  DBuf<unsigned long long> qkey_;
+  DBuf<unsigned> qacc_, scount_;
+  DBuf<int2> cand_;
+  DBuf<int> refine_;
+  long long cand_cap_ = 0, ncand_ = 0;
+  // tree refit and query tiles
+  DBuf<int> inv_sorted_;
+  DBuf<RefitGroup> refit_groups_;
+  std::vector<int> refit_pass_off_;  // first group of each pass, plus the end
+  DBuf<long long> tile_base_;
+  std::vector<long long> h_tile_base_;
+  DBuf<float4> tbox_;
   long long ntot_ = 0, ctot_ = 0, inc_tot_ = 0;
   int last_error_ = 0;
   cudaStream_t stream_ = nullptr;

@@ -76,28 +76,37 @@ __global__ void k_holemap_fill_planes(unsigned char* sam, const HoleMapInfo* hm,
 __global__ void k_holemap_lines(unsigned char* sam, const HoleMapInfo* hm, int axis, unsigned* changed);
 __global__ void k_holemap_final(unsigned char* sam, const HoleMapInfo* hm);
 __global__ void k_pairs(BlockInfo* bi, int nb, PairInfo* pairs, int* npairs);
-__global__ void k_reduced_obb(const double* x, const int* conn8, const unsigned char* cell_nv,
-                              const BlockInfo* bi, int don, PairInfo* pairs, int npairs,
-                              unsigned long long* acc);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-__global__ void k_cell_boxes(const double* x, const int* conn8, const unsigned char* cell_nv,
-                             const int* sorted_cell, long long ctot, float4* cbox, double* cbox64);
-__global__ void k_tree_leaves(const BlockInfo* bi, int nb, const float4* cbox, const double* cbox64,
-                              float4* tnode, double* tnode64, int* visit, long long total_leaves,
-                              const long long* leaf_base);
+__global__ void k_cell_pass(const double* x, const int* conn8, const unsigned char* cell_nv,
+                            const unsigned char* cell_blk, const int* inv_sorted, long long ctot,
+                            const BlockInfo* bi, const PairInfo* pairs, int npairs, float4* cbox, double* cbox64,
+                            unsigned long long* acc);
+__global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, int pass0, const float4* cbox,
+                              const double* cbox64, float4* tnode, double* tnode64);
+__global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
+                             float4* tbox);
+__global__ void k_invert(const int* perm, long long n, int* inv);
 __global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs,
-                              int tiles_x, int tile, int* tile_cnt);
+                              int tiles_x, int tile, int* tile_cnt, const float4* tbox, const long long* tile_base);
 __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs,
                               int tiles_x, int tile, const int* tile_off, const double* node_res,
-                              int* qnode, int* qdon, double* qres);
-// host launcher of the templated search kernel (same translation unit as
-// its instantiations)
-void launch_search(int form, int blocks, int threads, cudaStream_t st, const double* x, const int* conn8,
-                   const unsigned char* cell_nv, const double* cell_res, const BlockInfo* bi,
-                   const int* sorted_cell, const float4* cbox, const double* cbox64, const float4* tnode,
-                   const double* tnode64, const int* qnode, const int* qdon, long long nq, int early_exit,
-                   int* qcell, unsigned char* qtie, unsigned long long* counters);
+                              int* qnode, int* qdon, double* qres, const float4* tbox,
+                              const long long* tile_base);
+// host launchers of the templated search stages (same translation unit as
+// their instantiations)
+void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
+                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const int* qnode, const int* qdon, long long nq, int2* cand, int cap, unsigned* count);
+void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,
+                       const unsigned char* cell_nv, const double* cell_res, const int* sorted_cell,
+                       const int* qnode, const int2* cand, int ncand, unsigned long long* qkey, unsigned* qacc,
+                       int* refine, unsigned* nrefine, unsigned long long* counters);
+__global__ void k_refine(const double* x, const int* conn8, const unsigned char* cell_nv, const double* cell_res,
+                         const int* sorted_cell, const int* qnode, const int2* cand, const int* refine,
+                         const unsigned* nrefine, unsigned long long* qkey, unsigned* qacc);
+__global__ void k_search_finish(const unsigned long long* qkey, const unsigned* qacc, long long nq, int* qcell,
+                                unsigned char* qtie, unsigned long long* counters);
 
 // ---- donors (kernels_donor.cu) ----
 __global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,

@@ -269,75 +269,6 @@ __global__ void k_pairs(BlockInfo* __restrict__ bi, int nb, PairInfo* __restrict
   *npairs = np;
 }
 
-// Region of the donor's cells whose boxes overlap the receptor's OBB, in the
-// donor's OBB frame (getReducedOBB).  One pass over the donor's cells serves
-// every pair that has this donor.  acc holds 6 ordered keys per pair.
-__global__ void k_reduced_obb(const double* __restrict__ x, const int* __restrict__ conn8,
-                              const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi,
-                              int don, PairInfo* __restrict__ pairs, int npairs,
-                              unsigned long long* __restrict__ acc) {
-  const BlockInfo& D = bi[don];
-  const int lane = threadIdx.x & 31;
-  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long base = warp0 * 32; base < D.ncells; base += nwarps * 32) {
-    long long i = base + lane;
-    bool valid = i < D.ncells;
-    double xv[8][3];
-    int nv = 0;
-    if (valid) {
-      long long c = (long long)D.cell_off + i;
-      nv = cell_nv[c];
-      gather_vertices(x, conn8 + 8 * c, nv, xv);
-    }
-    for (int p = 0; p < npairs; p++) {
-      if (pairs[p].don != don) continue;
-      const Obb& R = bi[pairs[p].rec].obb;
-      bool ov = false;
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      if (valid) {
-        double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
-        for (int m = 0; m < nv; m++) {
-          double xd[3];
-          for (int j = 0; j < 3; j++) {
-            xd[j] = 0;
-            for (int k = 0; k < 3; k++) xd[j] += (xv[m][k] - R.xc[k]) * R.vec[j][k];
-          }
-          for (int j = 0; j < 3; j++) {
-            bb[j] = dmin(bb[j], xd[j]);
-            bb[j + 3] = dmax(bb[j + 3], xd[j]);
-          }
-        }
-        ov = true;
-        for (int j = 0; j < 3; j++) ov = ov && !(bb[j] > R.dxc[j]);
-        for (int j = 0; j < 3; j++) ov = ov && !(bb[j + 3] < -R.dxc[j]);
-        if (ov) {
-          for (int m = 0; m < nv; m++) {
-            for (int j = 0; j < 3; j++) {
-              double xd = 0;
-              for (int k = 0; k < 3; k++) xd += (xv[m][k] - D.obb.xc[k]) * D.obb.vec[j][k];
-              lo[j] = dmin(lo[j], xd);
-              hi[j] = dmax(hi[j], xd);
-            }
-          }
-        }
-      }
-      if (__any_sync(0xffffffffu, ov)) {
-        for (int j = 0; j < 3; j++)
-          for (int o = 16; o > 0; o >>= 1) {
-            lo[j] = dmin(lo[j], __shfl_xor_sync(0xffffffffu, lo[j], o));
-            hi[j] = dmax(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
-          }
-        if (lane == 0)
-          for (int j = 0; j < 3; j++) {
-            atomicMin(&acc[6 * p + j], dkey(lo[j]));
-            atomicMax(&acc[6 * p + j + 3], dkey(hi[j]));
-          }
-      }
-    }
-  }
-}
-
 __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __restrict__ pairs, int npairs,
                               const unsigned long long* __restrict__ acc) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,6 +285,15 @@ __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __rest
   }
   for (int k = 0; k < 6; k++) pairs[p].rd[k] = rd[k];
   pairs[p].region = r;
+  // world box of the region, widened so rounding can never exclude a node
+  // the exact test keeps
+  for (int k = 0; k < 3; k++) {
+    double h = 0;
+    for (int j = 0; j < 3; j++) h += fabs(r.dxc[j]) * fabs(r.vec[j][k]);
+    const double slack = 1e-9 * (fabs(r.xc[k]) + h) + 1e-12;
+    pairs[p].wbox[k] = r.xc[k] - h - slack;
+    pairs[p].wbox[k + 3] = r.xc[k] + h + slack;
+  }
 }
 
 // ===========================================================================
@@ -363,81 +303,236 @@ __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __rest
 __device__ __forceinline__ float f_rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float f_ru(double v) { return __double2float_ru(v); }
 
-__global__ void k_cell_boxes(const double* __restrict__ x, const int* __restrict__ conn8,
-                             const unsigned char* __restrict__ cell_nv, const int* __restrict__ sorted_cell,
-                             long long ctot, float4* __restrict__ cbox, double* __restrict__ cbox64) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < ctot;
-       j += (long long)gridDim.x * blockDim.x) {
-    int c = sorted_cell[j];
-    int nv = cell_nv[c];
-    const int* cv = conn8 + 8 * (long long)c;
+// One pass over all cells in their natural order (coalesced connectivity):
+// the FP64 element box, stored (FP32, rounded outward) at the cell's
+// position in the tree order, and the reduced-box accumulation of every pair
+// whose donor is the cell's block (getReducedOBB, MeshBlock.C:774-838).  A
+// cell is projected vertex by vertex only if the projection of its box centre
+// does not already prove every vertex outside the receptor box, so the
+// overlap decision is the reference's exact one.
+__global__ void __launch_bounds__(256) k_cell_pass(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const unsigned char* __restrict__ cell_blk, const int* __restrict__ inv_sorted, long long ctot,
+    const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs, int npairs,
+    float4* __restrict__ cbox, double* __restrict__ cbox64, unsigned long long* __restrict__ acc) {
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long base = warp0 * 32; base < ctot; base += nwarps * 32) {
+    const long long c = base + lane;
+    const bool valid = c < ctot;
+    double xv[8][3];
+    int nv = 0, b = -1;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int m = 0; m < nv; m++) {
-      const double* p = x + 3 * (long long)cv[m];
-      for (int k = 0; k < 3; k++) {
-        lo[k] = dmin(lo[k], p[k]);
-        hi[k] = dmax(hi[k], p[k]);
+    if (valid) {
+      nv = cell_nv[c];
+      b = cell_blk[c];
+      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+      gather_vertices(x, cv, nv, xv);
+      for (int m = 0; m < nv; m++)
+        for (int k = 0; k < 3; k++) {
+          lo[k] = dmin(lo[k], xv[m][k]);
+          hi[k] = dmax(hi[k], xv[m][k]);
+        }
+      const long long j = inv_sorted[c];
+      cbox[2 * j] = make_float4(f_rd(lo[0]), f_rd(lo[1]), f_rd(lo[2]), f_ru(hi[0]));
+      cbox[2 * j + 1] = make_float4(f_ru(hi[1]), f_ru(hi[2]), 0.f, 0.f);
+      if (cbox64) {
+        double* o = cbox64 + 6 * j;
+        o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
+        o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
       }
     }
-    cbox[2 * j] = make_float4(f_rd(lo[0]), f_rd(lo[1]), f_rd(lo[2]), f_ru(hi[0]));
-    cbox[2 * j + 1] = make_float4(f_ru(hi[1]), f_ru(hi[2]), 0.f, 0.f);
-    if (cbox64) {
-      double* o = cbox64 + 6 * j;
-      o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
-      o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+    for (int p = 0; p < npairs; p++) {
+      const int don = pairs[p].don;
+      bool ov = false;
+      double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+      if (valid && b == don) {
+        const Obb& R = bi[pairs[p].rec].obb;
+        // centre/half-size bound of the vertex projections onto R's axes
+        bool maybe = true;
+        for (int jx = 0; jx < 3 && maybe; jx++) {
+          double cp = 0, rad = 0;
+          for (int k = 0; k < 3; k++) {
+            cp += (0.5 * (lo[k] + hi[k]) - R.xc[k]) * R.vec[jx][k];
+            rad += 0.5 * (hi[k] - lo[k]) * fabs(R.vec[jx][k]);
+          }
+          const double slack = 1e-9 * (fabs(cp) + rad + R.dxc[jx]) + 1e-12;
+          if (cp - rad - slack > R.dxc[jx] || cp + rad + slack < -R.dxc[jx]) maybe = false;
+        }
+        if (maybe) {
+          double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
+          for (int m = 0; m < nv; m++) {
+            double xd[3];
+            for (int jx = 0; jx < 3; jx++) {
+              xd[jx] = 0;
+              for (int k = 0; k < 3; k++) xd[jx] += (xv[m][k] - R.xc[k]) * R.vec[jx][k];
+            }
+            for (int jx = 0; jx < 3; jx++) {
+              bb[jx] = dmin(bb[jx], xd[jx]);
+              bb[jx + 3] = dmax(bb[jx + 3], xd[jx]);
+            }
+          }
+          ov = true;
+          for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx] > R.dxc[jx]);
+          for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx + 3] < -R.dxc[jx]);
+          if (ov) {
+            const Obb& D = bi[don].obb;
+            for (int m = 0; m < nv; m++)
+              for (int jx = 0; jx < 3; jx++) {
+                double xd = 0;
+                for (int k = 0; k < 3; k++) xd += (xv[m][k] - D.xc[k]) * D.vec[jx][k];
+                rlo[jx] = dmin(rlo[jx], xd);
+                rhi[jx] = dmax(rhi[jx], xd);
+              }
+          }
+        }
+      }
+      if (__any_sync(0xffffffffu, ov)) {
+        for (int jx = 0; jx < 3; jx++)
+          for (int o = 16; o > 0; o >>= 1) {
+            rlo[jx] = dmin(rlo[jx], __shfl_xor_sync(0xffffffffu, rlo[jx], o));
+            rhi[jx] = dmax(rhi[jx], __shfl_xor_sync(0xffffffffu, rhi[jx], o));
+          }
+        if (lane == 0)
+          for (int jx = 0; jx < 3; jx++) {
+            atomicMin(&acc[6 * p + jx], dkey(rlo[jx]));
+            atomicMax(&acc[6 * p + jx + 3], dkey(rhi[jx]));
+          }
+      }
     }
   }
 }
 
-// Leaves, then parents bottom-up: the second child to finish builds the
-// parent (the usual refit with per-node arrival counters).
-__global__ void k_tree_leaves(const BlockInfo* __restrict__ bi, int nb, const float4* __restrict__ cbox,
-                              const double* __restrict__ cbox64, float4* __restrict__ tnode,
-                              double* __restrict__ tnode64, int* __restrict__ visit, long long total_leaves,
-                              const long long* __restrict__ leaf_base) {
-  for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < total_leaves;
-       L += (long long)gridDim.x * blockDim.x) {
-    int b = 0;
-    while (b + 1 < nb && leaf_base[b + 1] <= L) b++;
-    const BlockInfo& B = bi[b];
-    int leaf = (int)(L - leaf_base[b]);
-    int j0 = leaf * kLeafCells, j1 = min(j0 + kLeafCells, B.ncells);
-    float lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY, hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
+// Level-by-level refit of the implicit trees: each CTA owns up to 256
+// consecutive nodes of one level of one block and builds the 8 levels above
+// them in shared memory.  Pass 0 starts from the leaves (unions of their
+// cells' boxes); pass p starts from the nodes pass p-1 wrote.
+
+__global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict__ bi,
+                                                     const RefitGroup* __restrict__ groups, int pass0,
+                                                     const float4* __restrict__ cbox,
+                                                     const double* __restrict__ cbox64,
+                                                     float4* __restrict__ tnode, double* __restrict__ tnode64) {
+  __shared__ float s32[256][6];
+  __shared__ double s64[256][6];
+  const RefitGroup G = groups[blockIdx.x];
+  const BlockInfo& B = bi[G.block];
+  const int L = G.level;
+  const int width = min(256, 1 << L);
+  const int t = threadIdx.x;
+  const int lvl_first = (1 << L) - 1;
+  if (t < width) {
+    const int node = lvl_first + G.first + t;
+    float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
     double d[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
-    for (int j = j0; j < j1; j++) {
-      long long s = (long long)B.cell_off + j;
-      float4 a = cbox[2 * s], c = cbox[2 * s + 1];
-      lo0 = fminf(lo0, a.x); lo1 = fminf(lo1, a.y); lo2 = fminf(lo2, a.z);
-      hi0 = fmaxf(hi0, a.w); hi1 = fmaxf(hi1, c.x); hi2 = fmaxf(hi2, c.y);
+    if (pass0) {
+      const int leaf = G.first + t;
+      const int j0 = leaf * kLeafCells, j1 = min(j0 + kLeafCells, B.ncells);
+      for (int j = j0; j < j1; j++) {
+        const long long sidx = (long long)B.cell_off + j;
+        const float4 A = cbox[2 * sidx], C = cbox[2 * sidx + 1];
+        b[0] = fminf(b[0], A.x); b[1] = fminf(b[1], A.y); b[2] = fminf(b[2], A.z);
+        b[3] = fmaxf(b[3], A.w); b[4] = fmaxf(b[4], C.x); b[5] = fmaxf(b[5], C.y);
+        if (tnode64)
+          for (int k = 0; k < 3; k++) {
+            d[k] = dmin(d[k], cbox64[6 * sidx + k]);
+            d[k + 3] = dmax(d[k + 3], cbox64[6 * sidx + k + 3]);
+          }
+      }
+      const long long gn = (long long)B.tree_off + node;
+      tnode[2 * gn] = make_float4(b[0], b[1], b[2], b[3]);
+      tnode[2 * gn + 1] = make_float4(b[4], b[5], 0.f, 0.f);
       if (tnode64)
-        for (int k = 0; k < 3; k++) {
-          d[k] = dmin(d[k], cbox64[6 * s + k]);
-          d[k + 3] = dmax(d[k + 3], cbox64[6 * s + k + 3]);
-        }
-    }
-    int node = B.P - 1 + leaf;
-    long long gn = (long long)B.tree_off + node;
-    tnode[2 * gn] = make_float4(lo0, lo1, lo2, hi0);
-    tnode[2 * gn + 1] = make_float4(hi1, hi2, 0.f, 0.f);
-    if (tnode64)
-      for (int k = 0; k < 6; k++) tnode64[6 * gn + k] = d[k];
-    while (node > 0) {
-      int parent = (node - 1) >> 1;
-      __threadfence();
-      long long gp = (long long)B.tree_off + parent;
-      if (atomicAdd(&visit[gp], 1) == 0) break;  // the sibling builds it
-      long long gl = (long long)B.tree_off + 2 * parent + 1, gr = gl + 1;
-      float4 la = __ldcg(&tnode[2 * gl]), lb = __ldcg(&tnode[2 * gl + 1]);
-      float4 ra = __ldcg(&tnode[2 * gr]), rb = __ldcg(&tnode[2 * gr + 1]);
-      tnode[2 * gp] = make_float4(fminf(la.x, ra.x), fminf(la.y, ra.y), fminf(la.z, ra.z), fmaxf(la.w, ra.w));
-      tnode[2 * gp + 1] = make_float4(fmaxf(lb.x, rb.x), fmaxf(lb.y, rb.y), 0.f, 0.f);
+        for (int k = 0; k < 6; k++) tnode64[6 * gn + k] = d[k];
+    } else {
+      const long long gn = (long long)B.tree_off + node;
+      const float4 A = tnode[2 * gn], C = tnode[2 * gn + 1];
+      b[0] = A.x; b[1] = A.y; b[2] = A.z; b[3] = A.w; b[4] = C.x; b[5] = C.y;
       if (tnode64)
-        for (int k = 0; k < 6; k++) {
-          double u = __ldcg(&tnode64[6 * gl + k]), v = __ldcg(&tnode64[6 * gr + k]);
-          tnode64[6 * gp + k] = (k < 3) ? dmin(u, v) : dmax(u, v);
-        }
-      node = parent;
+        for (int k = 0; k < 6; k++) d[k] = tnode64[6 * gn + k];
     }
+    for (int k = 0; k < 6; k++) {
+      s32[t][k] = b[k];
+      s64[t][k] = d[k];
+    }
+  }
+  __syncthreads();
+  int n = width, lev = L;
+  const int top = max(L - 8, 0);
+  while (lev > top) {
+    const int half = n >> 1;
+    float b[6];
+    double d[6];
+    if (t < half) {
+      for (int k = 0; k < 3; k++) {
+        b[k] = fminf(s32[2 * t][k], s32[2 * t + 1][k]);
+        b[k + 3] = fmaxf(s32[2 * t][k + 3], s32[2 * t + 1][k + 3]);
+        d[k] = dmin(s64[2 * t][k], s64[2 * t + 1][k]);
+        d[k + 3] = dmax(s64[2 * t][k + 3], s64[2 * t + 1][k + 3]);
+      }
+    }
+    __syncthreads();  // every pair is read before any slot is overwritten
+    if (t < half) {
+      for (int k = 0; k < 6; k++) {
+        s32[t][k] = b[k];
+        s64[t][k] = d[k];
+      }
+      const int plev = lev - 1;
+      const int node = (1 << plev) - 1 + (G.first >> (L - plev)) + t;
+      const long long gn = (long long)B.tree_off + node;
+      tnode[2 * gn] = make_float4(b[0], b[1], b[2], b[3]);
+      tnode[2 * gn + 1] = make_float4(b[4], b[5], 0.f, 0.f);
+      if (tnode64)
+        for (int k = 0; k < 6; k++) tnode64[6 * gn + k] = d[k];
+    }
+    __syncthreads();
+    n = half;
+    lev--;
+  }
+}
+
+// Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
+// rounded outward), so the query gathering can skip tiles far from a region.
+__global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
+                                                    int nb, const long long* __restrict__ tile_base,
+                                                    float4* __restrict__ tbox) {
+  __shared__ double sh[6][8];
+  const long long T = blockIdx.x;
+  int b = 0;
+  while (b + 1 < nb && tile_base[b + 1] <= T) b++;
+  const BlockInfo& B = bi[b];
+  const int t0 = (int)(T - tile_base[b]) * kNodeTile;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
+    const double* p = x + 3 * ((long long)B.node_off + i);
+    for (int k = 0; k < 3; k++) {
+      lo[k] = dmin(lo[k], p[k]);
+      hi[k] = dmax(hi[k], p[k]);
+    }
+  }
+  for (int k = 0; k < 3; k++)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; k++) {
+      sh[k][w] = lo[k];
+      sh[k + 3][w] = hi[k];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++)
+      for (int k = 0; k < 3; k++) {
+        sh[k][0] = dmin(sh[k][0], sh[k][ww]);
+        sh[k + 3][0] = dmax(sh[k + 3][0], sh[k + 3][ww]);
+      }
+    tbox[2 * T] = make_float4(f_rd(sh[0][0]), f_rd(sh[1][0]), f_rd(sh[2][0]), f_ru(sh[3][0]));
+    tbox[2 * T + 1] = make_float4(f_ru(sh[4][0]), f_ru(sh[5][0]), 0.f, 0.f);
   }
 }
 
@@ -458,10 +553,21 @@ __device__ __forceinline__ bool in_region(const double* p, const Obb& r) {
   return fabs(xd[0]) <= r.dxc[0] && fabs(xd[1]) <= r.dxc[1] && fabs(xd[2]) <= r.dxc[2];
 }
 
+// A tile is skipped when its box misses the region's world box (the region
+// is an oriented box inside it), so only tiles that may hold a query point are
+// tested node by node.
+__device__ __forceinline__ bool tile_may_hit(const float4* __restrict__ tbox, long long T, const PairInfo& P) {
+  const float4 A = tbox[2 * T], C = tbox[2 * T + 1];
+  return !((double)A.x > P.wbox[3] || (double)A.y > P.wbox[4] || (double)A.z > P.wbox[5] ||
+           (double)A.w < P.wbox[0] || (double)C.x < P.wbox[1] || (double)C.y < P.wbox[2]);
+}
+
 __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restrict__ x,
                                                            const BlockInfo* __restrict__ bi,
                                                            const PairInfo* __restrict__ pairs, int tiles_x,
-                                                           int tile, int* __restrict__ tile_cnt) {
+                                                           int tile, int* __restrict__ tile_cnt,
+                                                           const float4* __restrict__ tbox,
+                                                           const long long* __restrict__ tile_base) {
   const int p = blockIdx.y;
   const PairInfo& P = pairs[p];
   const BlockInfo& R = bi[P.rec];
@@ -470,6 +576,10 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
   for (int t = blockIdx.x; t < tiles_x; t += gridDim.x) {
     int n0 = t * tile;
     cnt = 0;
+    if (n0 < R.nnodes && !tile_may_hit(tbox, tile_base[P.rec] + t, P)) {
+      if (threadIdx.x == 0) tile_cnt[(long long)p * tiles_x + t] = 0;
+      continue;
+    }
     for (int k = 0; k < kQItems; k++) {
       int i = n0 + threadIdx.x * kQItems + k;
       if (i < R.nnodes && in_region(x + 3 * ((long long)R.node_off + i), reg)) cnt++;
@@ -494,7 +604,8 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
                                                            int tile, const int* __restrict__ tile_off,
                                                            const double* __restrict__ node_res,
                                                            int* __restrict__ qnode, int* __restrict__ qdon,
-                                                           double* __restrict__ qres) {
+                                                           double* __restrict__ qres, const float4* __restrict__ tbox,
+                                                           const long long* __restrict__ tile_base) {
   typedef cub::BlockScan<int, kQThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
   const int p = blockIdx.y;
@@ -503,6 +614,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
   const Obb reg = P.region;
   for (int t = blockIdx.x; t < tiles_x; t += gridDim.x) {
     int n0 = t * tile;
+    if (n0 >= R.nnodes || !tile_may_hit(tbox, tile_base[P.rec] + t, P)) continue;
     unsigned mask = 0;
     int cnt = 0;
     for (int k = 0; k < kQItems; k++) {
@@ -640,26 +752,47 @@ __device__ __forceinline__ int screen32(const double xv[8][3], const double p[3]
   return interior ? 1 : -1;
 }
 
+// ---------------------------------------------------------------------------
+// Search, stage 1: stack-free traversal of the donor block's tree.  Every
+// cell whose (conservative) box holds the point is appended to the candidate
+// list as (query, sorted cell position).  FORM 0 tests FP64 boxes with the
+// reference's +-TOL (exact candidates); FORM 1 tests FP32 boxes rounded
+// outward with a relative margin (a superset, filtered exactly in stage 2).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void append_candidate(int q, int s, int2* __restrict__ cand, int cap,
+                                                 unsigned* __restrict__ count) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const int rank = __popc(mask & ((1u << lane) - 1u));
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(count, (unsigned)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  const unsigned i = base + rank;
+  if (i < (unsigned)cap) cand[i] = make_int2(q, s);
+}
+
 template <int FORM>
-__global__ void __launch_bounds__(128) k_search(
-    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-    const double* __restrict__ cell_res, const BlockInfo* __restrict__ bi, const int* __restrict__ sorted_cell,
-    const float4* __restrict__ cbox, const double* __restrict__ cbox64, const float4* __restrict__ tnode,
-    const double* __restrict__ tnode64, const int* __restrict__ qnode, const int* __restrict__ qdon,
-    long long nq, int early_exit, int* __restrict__ qcell, unsigned char* __restrict__ qtie,
-    unsigned long long* __restrict__ counters) {
-  unsigned long long my_cand = 0, my_refine = 0, my_tie = 0, my_found = 0, my_verts = 0;
+__global__ void __launch_bounds__(256) k_traverse(
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
+    const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
+    const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int2* __restrict__ cand,
+    int cap, unsigned* __restrict__ count) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
     const int g = qnode[q];
     const int a = qdon[q];
     const int P = bi[a].P, toff = bi[a].tree_off, coff = bi[a].cell_off, nc = bi[a].ncells;
-    const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
-    const float p0 = (float)p[0], p1 = (float)p[1], p2 = (float)p[2];
-    const float e0 = fabsf(p0) * 4.8e-7f + 1e-9f, e1 = fabsf(p1) * 4.8e-7f + 1e-9f,
-                e2 = fabsf(p2) * 4.8e-7f + 1e-9f;
-    int best_clean = 0x7fffffff, best_prov = 0x7fffffff, nacc = 0, nprov = 0;
-    bool stop = false;
+    double p[3];
+    float p32[3], e32[3];
+    p[0] = x[3 * (long long)g];
+    p[1] = x[3 * (long long)g + 1];
+    p[2] = x[3 * (long long)g + 2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      p32[k] = (float)p[k];
+      e32[k] = fabsf(p32[k]) * 4.8e-7f + 1e-9f;
+    }
     int node = 0;
     for (;;) {
       bool hit;
@@ -670,17 +803,16 @@ __global__ void __launch_bounds__(128) k_search(
               p[1] <= b[4] + kTol && p[2] <= b[5] + kTol;
       } else {
         const float4 A = tnode[2 * gn], B = tnode[2 * gn + 1];
-        hit = p0 >= A.x - e0 && p1 >= A.y - e1 && p2 >= A.z - e2 && p0 <= A.w + e0 && p1 <= B.x + e1 &&
-              p2 <= B.y + e2;
+        hit = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
+              p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
       }
       if (hit) {
         if (node < P - 1) {
           node = 2 * node + 1;
           continue;
         }
-        const int leaf = node - (P - 1);
-        const int j0 = leaf * kLeafCells, j1 = min(j0 + kLeafCells, nc);
-        for (int j = j0; j < j1 && !stop; j++) {
+        const int j0 = (node - (P - 1)) * kLeafCells, j1 = min(j0 + kLeafCells, nc);
+        for (int j = j0; j < j1; j++) {
           const long long s = (long long)coff + j;
           bool pass;
           if (FORM == 0) {
@@ -689,89 +821,163 @@ __global__ void __launch_bounds__(128) k_search(
             pass = in_box64(p, lo, hi);
           } else {
             const float4 A = cbox[2 * s], B = cbox[2 * s + 1];
-            pass = p0 >= A.x - e0 && p1 >= A.y - e1 && p2 >= A.z - e2 && p0 <= A.w + e0 && p1 <= B.x + e1 &&
-                   p2 <= B.y + e2;
+            pass = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
+                   p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
           }
-          if (!pass) continue;
-          const int c = sorted_cell[s];
-          const int nv = cell_nv[c];
-          const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c);
-          const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c + 4);
-          const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-          double xv[8][3];
-          gather_vertices(x, cv, nv, xv);
-          if (FORM == 1) {  // exact FP64 element box (searchADTrecursion.C:63-66)
-            double lo[3] = {xv[0][0], xv[0][1], xv[0][2]}, hi[3] = {xv[0][0], xv[0][1], xv[0][2]};
-            for (int m = 1; m < nv; m++)
-              for (int k = 0; k < 3; k++) {
-                lo[k] = dmin(lo[k], xv[m][k]);
-                hi[k] = dmax(hi[k], xv[m][k]);
-              }
-            if (!in_box64(p, lo, hi)) continue;
-          }
-          my_cand++;
-          my_verts += nv;
-          const bool big = cell_res[c] == kBig;
-          int cls = -1;
-          if (FORM == 1 && nv != 4) cls = screen32(xv, p, nv);
-          if (cls < 0) {
-            double frac[8];
-            nodal_weights64(xv, p, frac, nv);
-            cls = classify64(frac, nv, big);
-            if (FORM == 1) my_refine++;
-          } else if (cls == 1 && early_exit) {
-            stop = true;
-          }
-          if (cls == 1) {
-            nacc++;
-            best_clean = min(best_clean, c);
-          } else if (cls == 2) {
-            nacc++;
-            nprov++;
-            best_prov = min(best_prov, c);
-          }
+          if (pass) append_candidate((int)q, (int)s, cand, cap, count);
         }
-        if (stop) break;
       }
       while (node > 0 && !(node & 1)) node = (node - 1) >> 1;
       if (node == 0) break;
       node++;
     }
-    int donor = (best_clean != 0x7fffffff) ? best_clean : ((best_prov != 0x7fffffff) ? best_prov : -1);
-    qcell[q] = donor;
-    unsigned char tie = (unsigned char)((nacc >= 2 ? 1 : 0) | (nprov >= 1 ? 2 : 0));
-    qtie[q] = tie;
-    my_tie += (tie != 0);
-    my_found += (donor >= 0);
   }
-  // counters: 0 candidates, 1 FP64 refinements, 2 ties, 3 found
+}
+
+// The query's outcome is the lowest cell id among clean accepts, else among
+// accepts on a no-donor cell's face: one ordered 64-bit key per query,
+// (face accept) << 32 | cell, merged with atomicMin.  The accept counters
+// (low half: accepts, high half: face accepts) flag order-dependent ties.
+__device__ __forceinline__ void record_accept(int q, int c, int cls, unsigned long long* __restrict__ qkey,
+                                              unsigned* __restrict__ qacc) {
+  if (cls <= 0) return;
+  const unsigned long long key = ((unsigned long long)(cls == 2) << 32) | (unsigned)c;
+  atomicMin(&qkey[q], key);
+  atomicAdd(&qacc[q], cls == 2 ? 0x10001u : 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Search, stage 2: one thread per candidate.  The exact FP64 element box
+// (searchADTrecursion.C:63-66) filters the superset; FORM 1 screens the
+// Newton inversion in FP32 and defers undecided candidates and tets to stage
+// 3; FORM 0 decides everything with the reference's FP64 arithmetic.
+// ---------------------------------------------------------------------------
+template <int FORM>
+__global__ void __launch_bounds__(256) k_candidates(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const double* __restrict__ cell_res, const int* __restrict__ sorted_cell, const int* __restrict__ qnode,
+    const int2* __restrict__ cand, int ncand, unsigned long long* __restrict__ qkey,
+    unsigned* __restrict__ qacc, int* __restrict__ refine, unsigned* __restrict__ nrefine,
+    unsigned long long* __restrict__ counters) {
+  unsigned long long my_cand = 0, my_verts = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
+    const int2 qs = cand[i];
+    const int q = qs.x;
+    const int c = sorted_cell[qs.y];
+    const int nv = cell_nv[c];
+    const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c);
+    const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c + 4);
+    const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    double xv[8][3];
+    gather_vertices(x, cv, nv, xv);
+    const int g = qnode[q];
+    const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
+    if (FORM == 1) {
+      double lo[3] = {xv[0][0], xv[0][1], xv[0][2]}, hi[3] = {xv[0][0], xv[0][1], xv[0][2]};
+      for (int m = 1; m < nv; m++)
+        for (int k = 0; k < 3; k++) {
+          lo[k] = dmin(lo[k], xv[m][k]);
+          hi[k] = dmax(hi[k], xv[m][k]);
+        }
+      if (!in_box64(p, lo, hi)) continue;
+    }
+    my_cand++;
+    my_verts += nv;
+    int cls;
+    if (FORM == 1) {
+      cls = (nv == 4) ? -1 : screen32(xv, p, nv);
+      if (cls < 0) {
+        const unsigned r = atomicAdd(nrefine, 1u);
+        refine[r] = i;  // capacity: one slot per candidate
+        continue;
+      }
+    } else {
+      double frac[8];
+      nodal_weights64(xv, p, frac, nv);
+      cls = classify64(frac, nv, cell_res[c] == kBig);
+    }
+    record_accept(q, c, cls, qkey, qacc);
+  }
   for (int o = 16; o > 0; o >>= 1) {
     my_cand += __shfl_xor_sync(0xffffffffu, my_cand, o);
-    my_refine += __shfl_xor_sync(0xffffffffu, my_refine, o);
-    my_tie += __shfl_xor_sync(0xffffffffu, my_tie, o);
-    my_found += __shfl_xor_sync(0xffffffffu, my_found, o);
     my_verts += __shfl_xor_sync(0xffffffffu, my_verts, o);
   }
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&counters[0], my_cand);
-    atomicAdd(&counters[1], my_refine);
-    atomicAdd(&counters[2], my_tie);
-    atomicAdd(&counters[3], my_found);
     atomicAdd(&counters[6], my_verts);
   }
 }
 
-void launch_search(int form, int blocks, int threads, cudaStream_t st, const double* x, const int* conn8,
-                   const unsigned char* cell_nv, const double* cell_res, const BlockInfo* bi,
-                   const int* sorted_cell, const float4* cbox, const double* cbox64, const float4* tnode,
-                   const double* tnode64, const int* qnode, const int* qdon, long long nq, int early_exit,
-                   int* qcell, unsigned char* qtie, unsigned long long* counters) {
+// Search, stage 3: the reference's FP64 Newton for the deferred candidates.
+__global__ void __launch_bounds__(128) k_refine(const double* __restrict__ x, const int* __restrict__ conn8,
+                                                const unsigned char* __restrict__ cell_nv,
+                                                const double* __restrict__ cell_res,
+                                                const int* __restrict__ sorted_cell, const int* __restrict__ qnode,
+                                                const int2* __restrict__ cand, const int* __restrict__ refine,
+                                                const unsigned* __restrict__ nrefine,
+                                                unsigned long long* __restrict__ qkey, unsigned* __restrict__ qacc) {
+  const int n = (int)*nrefine;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int2 qs = cand[refine[k]];
+    const int q = qs.x;
+    const int c = sorted_cell[qs.y];
+    const int nv = cell_nv[c];
+    double xv[8][3];
+    gather_vertices(x, conn8 + 8 * (long long)c, nv, xv);
+    const int g = qnode[q];
+    const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
+    double frac[8];
+    nodal_weights64(xv, p, frac, nv);
+    record_accept(q, c, classify64(frac, nv, cell_res[c] == kBig), qkey, qacc);
+  }
+}
+
+// Search, stage 4: per query outcome and tie flags.
+__global__ void k_search_finish(const unsigned long long* __restrict__ qkey, const unsigned* __restrict__ qacc,
+                                long long nq, int* __restrict__ qcell, unsigned char* __restrict__ qtie,
+                                unsigned long long* __restrict__ counters) {
+  unsigned long long my_tie = 0, my_found = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long key = qkey[q];
+    const int donor = (key == ~0ull) ? -1 : (int)(key & 0xffffffffull);
+    const unsigned acc = qacc[q];
+    const unsigned nacc = acc & 0xffffu, nprov = acc >> 16;
+    const unsigned char tie = (unsigned char)((nacc >= 2 ? 1 : 0) | (nprov >= 1 ? 2 : 0));
+    qcell[q] = donor;
+    qtie[q] = tie;
+    my_tie += (tie != 0);
+    my_found += (donor >= 0);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    my_tie += __shfl_xor_sync(0xffffffffu, my_tie, o);
+    my_found += __shfl_xor_sync(0xffffffffu, my_found, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&counters[2], my_tie);
+    atomicAdd(&counters[3], my_found);
+  }
+}
+
+void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
+                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const int* qnode, const int* qdon, long long nq, int2* cand, int cap, unsigned* count) {
   if (form == 0)
-    k_search<0><<<blocks, threads, 0, st>>>(x, conn8, cell_nv, cell_res, bi, sorted_cell, cbox, cbox64, tnode,
-                                            tnode64, qnode, qdon, nq, 0, qcell, qtie, counters);
+    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, cand, cap, count);
   else
-    k_search<1><<<blocks, threads, 0, st>>>(x, conn8, cell_nv, cell_res, bi, sorted_cell, cbox, cbox64, tnode,
-                                            tnode64, qnode, qdon, nq, early_exit, qcell, qtie, counters);
+    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, cand, cap, count);
+}
+
+void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,
+                       const unsigned char* cell_nv, const double* cell_res, const int* sorted_cell,
+                       const int* qnode, const int2* cand, int ncand, unsigned long long* qkey, unsigned* qacc,
+                       int* refine, unsigned* nrefine, unsigned long long* counters) {
+  if (form == 0)
+    k_candidates<0><<<blocks, 256, 0, st>>>(x, conn8, cell_nv, cell_res, sorted_cell, qnode, cand, ncand, qkey,
+                                            qacc, refine, nrefine, counters);
+  else
+    k_candidates<1><<<blocks, 256, 0, st>>>(x, conn8, cell_nv, cell_res, sorted_cell, qnode, cand, ncand, qkey,
+                                            qacc, refine, nrefine, counters);
 }
 
 }  // namespace tb

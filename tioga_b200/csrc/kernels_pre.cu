@@ -390,4 +390,10 @@ __global__ void k_morton(const double* __restrict__ x, const int* __restrict__ c
   }
 }
 
+__global__ void k_invert(const int* __restrict__ perm, long long n, int* __restrict__ inv) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x)
+    inv[perm[s]] = (int)s;
+}
+
 }  // namespace tb
