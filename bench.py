@@ -206,9 +206,15 @@ def run_gpu(args, ws, rank, local, dist):
     if lib.lib.tioga_b200_last_error() != 0:
         raise RuntimeError("connectivity failed")
 
+    # device-resident forms keep iblank in HBM too (a GPU solver's arrays)
+    d_ibl = [torch.ones(b.nnodes, dtype=torch.int32, device="cuda") for b in system.blocks]
+
     def timed(precision, resident, steps, warmup, clocks=None):
         tb.set_int(lib.lib, "tioga_b200_set_precision_", precision)
         tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", resident)
+        for b, d in zip(system.blocks, d_ibl):
+            lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)),
+                                                       C.c_void_p(d.data_ptr() if resident else 0))
         for _ in range(warmup):
             lib.performconnectivity()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]

@@ -137,7 +137,8 @@ int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights,
 /* Device time (ms) of the last connectivity call per phase: [0] coordinate
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,
- * [8] total. */
+ * [8] total; inside the search: [9] traversal, [10] candidate screen,
+ * [11] FP64 refinement. */
 void tioga_b200_timing_(float out[16]);
 
 #ifdef __cplusplus

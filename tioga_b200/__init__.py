@@ -49,7 +49,7 @@ def timing(lib: C.CDLL) -> dict:
     out = (C.c_float * 16)()
     lib.tioga_b200_timing_(out)
     keys = ["upload", "holemap", "boxes_refit", "query", "search", "donors", "celliblank",
-            "download", "total"]
+            "download", "total", "search_traverse", "search_candidates", "search_refine"]
     return {k: float(out[i]) for i, k in enumerate(keys)}
 
 

@@ -235,6 +235,9 @@ void tioga_b200_timing_(float out[16]) {
   out[6] = t.celliblank;
   out[7] = t.download;
   out[8] = t.total;
+  out[9] = t.traverse;
+  out[10] = t.candidates;
+  out[11] = t.refine;
 }
 
 }  // extern "C"

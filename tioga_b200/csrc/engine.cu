@@ -50,11 +50,13 @@ Engine::Engine() {
   cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking);
   stream_ = own_stream_;
   for (auto& e : ev_) cudaEventCreate(&e);
+  for (auto& e : sev_) cudaEventCreate(&e);
 }
 
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& e : ev_) cudaEventDestroy(e);
+  for (auto& e : sev_) cudaEventDestroy(e);
   x_.release(); node_res_.release(); cell_res_.release(); iblank_.release(); iblank_cell_.release();
   conn8_.release(); node_blk_.release(); cell_blk_.release(); cell_nv_.release(); wallf_.release();
   obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
@@ -351,7 +353,7 @@ int Engine::compute_obbs() {
 
 int Engine::build_tree_topology() {
   // Morton order of the cell centroids per block (block id in the key's
-  // high word), leaves of kLeafCells consecutive cells, one implicit tree per
+  // high word), leaves of consecutive cells, one implicit 4-ary tree per
   // block.  Rebuilt only when the registration changes; every connectivity
   // call refits the boxes to the current coordinates.
   TB_CUDA(mkey_.ensure(ctot_));
@@ -367,37 +369,56 @@ int Engine::build_tree_topology() {
   TB_CUDA(cub_tmp_.ensure(tmp));
   cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
                                   (int)ctot_, 0, 40, stream_);
+  // Morton order of each block's nodes: the order query points are gathered in
+  TB_CUDA(node_order_.ensure(ntot_));
+  {
+    DBuf<unsigned long long> k0, k1;
+    DBuf<int> v0;
+    TB_CUDA(k0.ensure(ntot_));
+    TB_CUDA(k1.ensure(ntot_));
+    TB_CUDA(v0.ensure(ntot_));
+    k_morton_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, k0.p, v0.p);
+    TB_LAUNCHED("k_morton_nodes");
+    size_t tmpn = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, 40, stream_);
+    TB_CUDA(cub_tmp_.ensure(tmpn));
+    cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, 40, stream_);
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    k0.release();
+    k1.release();
+    v0.release();
+  }
   TB_CUDA(inv_sorted_.ensure(ctot_));
   k_invert<<<grid_for(ctot_, kT), kT, 0, stream_>>>(sorted_cell_.p, ctot_, inv_sorted_.p);
   TB_LAUNCHED("k_invert");
+  // one 4-ary tree per block: leaves of at most kMaxLeafCells consecutive
+  // cells in Morton order; node i of a block sits in slot tree_off + 3 + i
   long long off = 0;
-  int maxlev = 0;
-  std::vector<int> lev(bi_.size());
+  int maxdepth = 0;
   for (size_t b = 0; b < bi_.size(); b++) {
     BlockInfo& B = bi_[b];
-    long long nleaf = std::max(1ll, ((long long)B.ncells + kLeafCells - 1) / kLeafCells);
-    long long P = 1;
-    int L = 0;
-    while (P < nleaf) {
-      P <<= 1;
-      L++;
-    }
-    B.P = (int)P;
+    // leaves of kMaxLeafCells consecutive Morton cells (a 2x2x2 group on a
+    // structured grid), as many leaves as the cells need
+    int D = 0;
+    while ((1ll << (2 * D)) * kMaxLeafCells < (long long)B.ncells) D++;
+    B.depth = D;
+    B.leaf_first = (int)level_first(D);
+    B.leaf_cells = kMaxLeafCells;
     B.tree_off = (int)off;
-    off += 2 * P - 1;
-    lev[b] = L;
-    maxlev = std::max(maxlev, L);
+    off += (3 + level_first(D + 1) + 3) / 4 * 4;
+    maxdepth = std::max(maxdepth, D);
   }
   tree_nodes_ = off;
-  // refit groups: pass p starts at level L-8p of each block and climbs 8 levels
+  // refit groups: pass p starts at depth D-4p of each block and climbs 4 levels
   std::vector<RefitGroup> groups;
   refit_pass_off_.assign(1, 0);
-  for (int pass = 0; 8 * pass <= maxlev; pass++) {
+  for (int pass = 0; 4 * pass <= maxdepth; pass++) {
     for (size_t b = 0; b < bi_.size(); b++) {
-      const int L = lev[b] - 8 * pass;
-      if (L < 0 || (pass > 0 && L == 0 && lev[b] - 8 * (pass - 1) <= 8)) continue;
-      if (pass > 0 && lev[b] - 8 * (pass - 1) <= 8) continue;  // reached the root already
-      const long long width = 1ll << L;
+      const int D = bi_[b].depth;
+      const int L = D - 4 * pass;
+      if (L < 0) continue;
+      if (pass > 0 && D - 4 * (pass - 1) <= 4) continue;  // the previous pass reached the root
+      const long long width = 1ll << (2 * L);
       for (long long f = 0; f < width; f += 256) groups.push_back(RefitGroup{(int)b, L, (int)f});
     }
     refit_pass_off_.push_back((int)groups.size());
@@ -621,7 +642,8 @@ int Engine::run_pairs_and_refit() {
     TB_LAUNCHED("k_tree_levels");
   }
   if (h_tile_base_.back() > 0) {
-    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p);
+    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
+                                                                      node_order_.p);
     TB_LAUNCHED("k_node_tiles");
   }
   k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
@@ -641,7 +663,7 @@ int Engine::run_queries() {
   TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
   dim3 grid(std::min(tiles_x, 148 * 8), npairs_);
   k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_cnt_.p, tbox_.p,
-                                           tile_base_.p);
+                                           tile_base_.p, node_order_.p);
   TB_LAUNCHED("k_query_count");
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
@@ -659,7 +681,8 @@ int Engine::run_queries() {
   TB_CUDA(interp2rec_.ensure(nq));
   if (nq > 0) {
     k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_off_.p,
-                                             node_res_.p, qnode_.p, qdon_.p, qres_.p, tbox_.p, tile_base_.p);
+                                             node_res_.p, qnode_.p, qdon_.p, qres_.p, tbox_.p, tile_base_.p,
+                                             node_order_.p);
     TB_LAUNCHED("k_query_write");
   }
   return 0;
@@ -678,31 +701,46 @@ int Engine::run_search() {
   TB_CUDA(qacc_.ensure(nq_));
   TB_CUDA(cudaMemsetAsync(qkey_.p, 0xff, nq_ * sizeof(unsigned long long), stream_));
   TB_CUDA(cudaMemsetAsync(qacc_.p, 0, nq_ * sizeof(unsigned), stream_));
-  long long cap = std::max<long long>(cand_cap_, std::max<long long>(4 * nq_, 1 << 16));
-  unsigned count = 0;
+  TB_CUDA(slots_.ensure((size_t)nq_ * kSlots));
+  TB_CUDA(ncand_q_.ensure(nq_ + 1));
+  TB_CUDA(cand_off_.ensure(nq_ + 1));
+  TB_CUDA(cudaMemsetAsync(ncand_q_.p + nq_, 0, sizeof(int), stream_));
+  long long ovf_cap = std::max<long long>(cand_cap_, std::max<long long>(nq_ / 8, 1 << 16));
+  unsigned count = 0, novf = 0;
+  TB_CUDA(cudaEventRecord(sev_[0], stream_));
   for (int attempt = 0; attempt < 2; attempt++) {
-    if (cap >= (1ll << 31)) {
-      fprintf(stderr, "#tioga_b200: more than 2^31 search candidates\n");
-      return -1;
-    }
-    TB_CUDA(cand_.ensure(cap));
+    TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq_, 256), stream_, x_.p, d_bi_.p, cbox_.p, form == 0 ? cbox64_.p : nullptr,
-                    tnode_.p, form == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p, nq_, cand_.p, (int)cap,
-                    scount_.p);
+    launch_traverse(form, grid_for(nq_, 256, 148 * 64), stream_, x_.p, d_bi_.p, cbox_.p,
+                    form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p,
+                    nq_, slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
     TB_LAUNCHED("k_traverse");
-    TB_CUDA(cudaMemcpyAsync(&count, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
-    cand_cap_ = cap;
-    if ((long long)count <= cap) break;
-    cap = (long long)count + count / 4 + 1024;  // grow and traverse again
+    cand_cap_ = ovf_cap;
+    if ((long long)novf <= ovf_cap) break;
+    ovf_cap = (long long)novf + novf / 4 + 1024;  // grow the overflow list and traverse again
   }
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncand_q_.p, cand_off_.p, (int)(nq_ + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, ncand_q_.p, cand_off_.p, (int)(nq_ + 1), stream_);
+  TB_CUDA(cudaMemcpyAsync(&count, cand_off_.p + nq_, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
   ncand_ = count;
+  TB_CUDA(cand_.ensure(std::max(1u, count)));
+  if (count > 0) {
+    k_gather_candidates<<<grid_for(nq_, kT), kT, 0, stream_>>>(slots_.p, ncand_q_.p, cand_off_.p, nq_, ovf_.p,
+                                                               scount_.p, (int)ovf_cap, cand_.p);
+    TB_LAUNCHED("k_gather_candidates");
+  }
+  TB_CUDA(cudaEventRecord(sev_[1], stream_));
   if (count > 0) {
     TB_CUDA(refine_.ensure(count));
     launch_candidates(form, grid_for(count, 256), stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p, sorted_cell_.p,
                       qnode_.p, cand_.p, (int)count, qkey_.p, qacc_.p, refine_.p, scount_.p + 1, counters_.p);
     TB_LAUNCHED("k_candidates");
+    TB_CUDA(cudaEventRecord(sev_[2], stream_));
     if (form == 1) {
       k_refine<<<grid_for(count / 4 + 1, 128), 128, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_res_.p,
                                                                   sorted_cell_.p, qnode_.p, cand_.p, refine_.p,
@@ -710,8 +748,11 @@ int Engine::run_search() {
       TB_LAUNCHED("k_refine");
     }
   }
+  if (count == 0) TB_CUDA(cudaEventRecord(sev_[2], stream_));
+  TB_CUDA(cudaEventRecord(sev_[3], stream_));
   k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, qcell_.p, qtie_.p, counters_.p);
   TB_LAUNCHED("k_search_finish");
+  search_timed_ = true;
   return 0;
 }
 
@@ -837,6 +878,7 @@ int Engine::connectivity() {
   }
   stats_ = Stats{};
   nlaunch_ = 0;
+  search_timed_ = false;
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   if (!coords_resident_) TB_TRY(upload_coords());
@@ -899,6 +941,12 @@ int Engine::connectivity() {
   timing_.celliblank = ms[7];
   timing_.download = ms[8];
   cudaEventElapsedTime(&timing_.total, ev_[0], ev_[8]);
+  timing_.traverse = timing_.candidates = timing_.refine = 0;
+  if (search_timed_) {
+    cudaEventElapsedTime(&timing_.traverse, sev_[0], sev_[1]);
+    cudaEventElapsedTime(&timing_.candidates, sev_[1], sev_[2]);
+    cudaEventElapsedTime(&timing_.refine, sev_[2], sev_[3]);
+  }
   if (err & kErrWeightRange)
     fprintf(stderr, "#tioga_b200: an interpolation weight fell outside [-0.2,1.2] (the reference aborts)\n");
   if (err & kErrFloodFillBound) fprintf(stderr, "#tioga_b200: hole-map fill hit its round limit\n");

@@ -20,8 +20,9 @@
 
 namespace tb {
 
-constexpr int kLeafCells = 4;   // cells per BVH leaf
+constexpr int kMaxLeafCells = 8; // cells per tree leaf at most (per-block leaf size 1..8)
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
+constexpr int kSlots = 8;       // inline search candidates per query
 constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
 
 template <class T>
@@ -56,8 +57,10 @@ struct BlockInfo {
   int nwbc, wall_off;  // wall nodes in the global wall list
   int nobc, obc_off;
   int nfringe;         // snapshot taken at preprocess (tioga.C:95-110)
-  int tree_off;        // first tree node in the node pool
-  int P;               // padded leaf count (power of two)
+  int tree_off;        // first slot of the block's 4-ary tree in the node pool (multiple of 4)
+  int depth;           // leaves are at this depth (root = 0)
+  int leaf_first;      // heap index of the first leaf, (4^depth - 1) / 3
+  int leaf_cells;      // cells per leaf
   int has_user_res;
   Obb obb;
   float bb_lo[3], bb_hi[3];  // block box for the Morton keys
@@ -116,6 +119,7 @@ struct Stats {
 struct Timing {
   float holemap = 0, boxes = 0, refit = 0, query = 0, search = 0, donors = 0, celliblank = 0,
         total = 0, upload = 0, download = 0;
+  float traverse = 0, candidates = 0, refine = 0;  // stages of the search
 };
 
 class Engine {
@@ -192,6 +196,7 @@ class Engine {
   DBuf<int2> cand_;
   DBuf<int> refine_;
   long long cand_cap_ = 0, ncand_ = 0;
+  bool search_timed_ = false;
   // tree refit and query tiles
   DBuf<int> inv_sorted_;
   DBuf<RefitGroup> refit_groups_;
@@ -199,12 +204,16 @@ class Engine {
   DBuf<long long> tile_base_;
   std::vector<long long> h_tile_base_;
   DBuf<float4> tbox_;
+  DBuf<int> node_order_;    // Morton order of each block's nodes
+  DBuf<int> slots_, ncand_q_, cand_off_;
+  DBuf<int3> ovf_;
   long long ntot_ = 0, ctot_ = 0, inc_tot_ = 0;
   int last_error_ = 0;
   cudaStream_t stream_ = nullptr;
   cudaStream_t own_stream_ = nullptr;
   long long nlaunch_ = 0;
   cudaEvent_t ev_[12];
+  cudaEvent_t sev_[4];
 
   // flat device arrays
   DBuf<double> x_, node_res_, cell_res_;

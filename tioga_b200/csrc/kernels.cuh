@@ -8,6 +8,11 @@
 
 namespace tb {
 
+// Node i of a block's 4-ary tree lives in slot tree_off + 3 + i, so the four
+// children 4n+1..4n+4 of any node share one aligned 128-byte line.
+__host__ __device__ __forceinline__ long long tslot(int tree_off, long long i) { return (long long)tree_off + 3 + i; }
+__host__ __device__ __forceinline__ long long level_first(int l) { return ((1ll << (2 * l)) - 1) / 3; }
+
 __device__ __forceinline__ void gather_vertices(const double* __restrict__ x, const int* __restrict__ cv,
                                                 int nv, double xv[8][3]) {
 #pragma unroll
@@ -85,19 +90,25 @@ __global__ void k_cell_pass(const double* x, const int* conn8, const unsigned ch
 __global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, int pass0, const float4* cbox,
                               const double* cbox64, float4* tnode, double* tnode64);
 __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
-                             float4* tbox);
+                             float4* tbox, const int* node_order);
+__global__ void k_morton_nodes(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
+                               long long ntot, unsigned long long* key, int* val);
 __global__ void k_invert(const int* perm, long long n, int* inv);
 __global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs,
-                              int tiles_x, int tile, int* tile_cnt, const float4* tbox, const long long* tile_base);
+                              int tiles_x, int tile, int* tile_cnt, const float4* tbox, const long long* tile_base,
+                              const int* node_order);
 __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs,
                               int tiles_x, int tile, const int* tile_off, const double* node_res,
                               int* qnode, int* qdon, double* qres, const float4* tbox,
-                              const long long* tile_base);
+                              const long long* tile_base, const int* node_order);
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
-                     const int* qnode, const int* qdon, long long nq, int2* cand, int cap, unsigned* count);
+                     const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
+                     int ovf_cap, unsigned* novf);
+__global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,
+                                    const int3* ovf, const unsigned* novf, int ovf_cap, int2* cand);
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const double* cell_res, const int* sorted_cell,
                        const int* qnode, const int2* cand, int ncand, unsigned long long* qkey, unsigned* qacc,

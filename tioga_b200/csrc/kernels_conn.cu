@@ -297,8 +297,8 @@ __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __rest
 }
 
 // ===========================================================================
-// bounding-volume tree: cell boxes in Morton order, leaves of kLeafCells
-// cells, implicit complete binary tree (heap order) per block
+// bounding-volume tree: cell boxes in Morton order, leaves of up to
+// kMaxLeafCells cells, implicit complete 4-ary tree (heap order) per block
 // ===========================================================================
 __device__ __forceinline__ float f_rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float f_ru(double v) { return __double2float_ru(v); }
@@ -421,17 +421,17 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
   const RefitGroup G = groups[blockIdx.x];
   const BlockInfo& B = bi[G.block];
   const int L = G.level;
-  const int width = min(256, 1 << L);
+  const int width = (int)min(256ll, 1ll << (2 * L));
   const int t = threadIdx.x;
-  const int lvl_first = (1 << L) - 1;
   if (t < width) {
-    const int node = lvl_first + G.first + t;
+    const long long node = level_first(L) + G.first + t;
+    const long long sl = tslot(B.tree_off, node);
     float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
     double d[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
     if (pass0) {
-      const int leaf = G.first + t;
-      const int j0 = leaf * kLeafCells, j1 = min(j0 + kLeafCells, B.ncells);
-      for (int j = j0; j < j1; j++) {
+      const long long j0 = (long long)(G.first + t) * B.leaf_cells;
+      const long long j1 = min(j0 + B.leaf_cells, (long long)B.ncells);
+      for (long long j = j0; j < j1; j++) {
         const long long sidx = (long long)B.cell_off + j;
         const float4 A = cbox[2 * sidx], C = cbox[2 * sidx + 1];
         b[0] = fminf(b[0], A.x); b[1] = fminf(b[1], A.y); b[2] = fminf(b[2], A.z);
@@ -442,17 +442,15 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
             d[k + 3] = dmax(d[k + 3], cbox64[6 * sidx + k + 3]);
           }
       }
-      const long long gn = (long long)B.tree_off + node;
-      tnode[2 * gn] = make_float4(b[0], b[1], b[2], b[3]);
-      tnode[2 * gn + 1] = make_float4(b[4], b[5], 0.f, 0.f);
+      tnode[2 * sl] = make_float4(b[0], b[1], b[2], b[3]);
+      tnode[2 * sl + 1] = make_float4(b[4], b[5], 0.f, 0.f);
       if (tnode64)
-        for (int k = 0; k < 6; k++) tnode64[6 * gn + k] = d[k];
+        for (int k = 0; k < 6; k++) tnode64[6 * sl + k] = d[k];
     } else {
-      const long long gn = (long long)B.tree_off + node;
-      const float4 A = tnode[2 * gn], C = tnode[2 * gn + 1];
+      const float4 A = tnode[2 * sl], C = tnode[2 * sl + 1];
       b[0] = A.x; b[1] = A.y; b[2] = A.z; b[3] = A.w; b[4] = C.x; b[5] = C.y;
       if (tnode64)
-        for (int k = 0; k < 6; k++) d[k] = tnode64[6 * gn + k];
+        for (int k = 0; k < 6; k++) d[k] = tnode64[6 * sl + k];
     }
     for (int k = 0; k < 6; k++) {
       s32[t][k] = b[k];
@@ -461,35 +459,37 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
   }
   __syncthreads();
   int n = width, lev = L;
-  const int top = max(L - 8, 0);
+  const int top = max(L - 4, 0);
   while (lev > top) {
-    const int half = n >> 1;
+    const int quarter = n >> 2;
     float b[6];
     double d[6];
-    if (t < half) {
+    if (t < quarter) {
       for (int k = 0; k < 3; k++) {
-        b[k] = fminf(s32[2 * t][k], s32[2 * t + 1][k]);
-        b[k + 3] = fmaxf(s32[2 * t][k + 3], s32[2 * t + 1][k + 3]);
-        d[k] = dmin(s64[2 * t][k], s64[2 * t + 1][k]);
-        d[k + 3] = dmax(s64[2 * t][k + 3], s64[2 * t + 1][k + 3]);
+        b[k] = fminf(fminf(s32[4 * t][k], s32[4 * t + 1][k]), fminf(s32[4 * t + 2][k], s32[4 * t + 3][k]));
+        b[k + 3] = fmaxf(fmaxf(s32[4 * t][k + 3], s32[4 * t + 1][k + 3]),
+                         fmaxf(s32[4 * t + 2][k + 3], s32[4 * t + 3][k + 3]));
+        d[k] = dmin(dmin(s64[4 * t][k], s64[4 * t + 1][k]), dmin(s64[4 * t + 2][k], s64[4 * t + 3][k]));
+        d[k + 3] = dmax(dmax(s64[4 * t][k + 3], s64[4 * t + 1][k + 3]),
+                        dmax(s64[4 * t + 2][k + 3], s64[4 * t + 3][k + 3]));
       }
     }
-    __syncthreads();  // every pair is read before any slot is overwritten
-    if (t < half) {
+    __syncthreads();  // every group of four is read before any slot is overwritten
+    if (t < quarter) {
       for (int k = 0; k < 6; k++) {
         s32[t][k] = b[k];
         s64[t][k] = d[k];
       }
       const int plev = lev - 1;
-      const int node = (1 << plev) - 1 + (G.first >> (L - plev)) + t;
-      const long long gn = (long long)B.tree_off + node;
-      tnode[2 * gn] = make_float4(b[0], b[1], b[2], b[3]);
-      tnode[2 * gn + 1] = make_float4(b[4], b[5], 0.f, 0.f);
+      const long long node = level_first(plev) + (G.first >> (2 * (L - plev))) + t;
+      const long long sl = tslot(B.tree_off, node);
+      tnode[2 * sl] = make_float4(b[0], b[1], b[2], b[3]);
+      tnode[2 * sl + 1] = make_float4(b[4], b[5], 0.f, 0.f);
       if (tnode64)
-        for (int k = 0; k < 6; k++) tnode64[6 * gn + k] = d[k];
+        for (int k = 0; k < 6; k++) tnode64[6 * sl + k] = d[k];
     }
     __syncthreads();
-    n = half;
+    n = quarter;
     lev--;
   }
 }
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
 // rounded outward), so the query gathering can skip tiles far from a region.
 __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
                                                     int nb, const long long* __restrict__ tile_base,
-                                                    float4* __restrict__ tbox) {
+                                                    float4* __restrict__ tbox, const int* __restrict__ node_order) {
   __shared__ double sh[6][8];
   const long long T = blockIdx.x;
   int b = 0;
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
-    const double* p = x + 3 * ((long long)B.node_off + i);
+    const double* p = x + 3 * (long long)node_order[B.node_off + i];
     for (int k = 0; k < 3; k++) {
       lo[k] = dmin(lo[k], p[k]);
       hi[k] = dmax(hi[k], p[k]);
@@ -567,7 +567,8 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
                                                            const PairInfo* __restrict__ pairs, int tiles_x,
                                                            int tile, int* __restrict__ tile_cnt,
                                                            const float4* __restrict__ tbox,
-                                                           const long long* __restrict__ tile_base) {
+                                                           const long long* __restrict__ tile_base,
+                                                           const int* __restrict__ node_order) {
   const int p = blockIdx.y;
   const PairInfo& P = pairs[p];
   const BlockInfo& R = bi[P.rec];
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
     }
     for (int k = 0; k < kQItems; k++) {
       int i = n0 + threadIdx.x * kQItems + k;
-      if (i < R.nnodes && in_region(x + 3 * ((long long)R.node_off + i), reg)) cnt++;
+      if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) cnt++;
     }
     __shared__ int sh[kQThreads / 32];
     int w = cnt;
@@ -605,7 +606,8 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
                                                            const double* __restrict__ node_res,
                                                            int* __restrict__ qnode, int* __restrict__ qdon,
                                                            double* __restrict__ qres, const float4* __restrict__ tbox,
-                                                           const long long* __restrict__ tile_base) {
+                                                           const long long* __restrict__ tile_base,
+                                                           const int* __restrict__ node_order) {
   typedef cub::BlockScan<int, kQThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
   const int p = blockIdx.y;
@@ -619,7 +621,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
     int cnt = 0;
     for (int k = 0; k < kQItems; k++) {
       int i = n0 + threadIdx.x * kQItems + k;
-      if (i < R.nnodes && in_region(x + 3 * ((long long)R.node_off + i), reg)) {
+      if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) {
         mask |= 1u << k;
         cnt++;
       }
@@ -629,7 +631,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
     long long o = (long long)tile_off[(long long)p * tiles_x + t] + pos;
     for (int k = 0; k < kQItems; k++) {
       if (mask & (1u << k)) {
-        int g = R.node_off + n0 + threadIdx.x * kQItems + k;
+        int g = node_order[R.node_off + n0 + threadIdx.x * kQItems + k];
         qnode[o] = g;
         qdon[o] = P.don;
         qres[o] = node_res[g];
@@ -646,16 +648,9 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
 // FP32 screen of the Newton inversion (hex 8, prism 6, pyramid 5) on
 // coordinates relative to vertex 0.  Returns 0 reject, 1 clean interior
 // accept, -1 undecided (the FP64 path decides).
-__device__ __forceinline__ int screen32(const double xv[8][3], const double p[3], int nv) {
+// FP32 core on vertex offsets y[m] = x_m - x_0 and point offset yp = p - x_0.
+__device__ __forceinline__ int screen32f(const float y[8][3], const float yp[3], int nv) {
   constexpr float kEps = 2e-3f;
-  float y[8][3], yp[3];
-#pragma unroll
-  for (int m = 0; m < 8; m++)
-    if (m < nv)
-#pragma unroll
-      for (int j = 0; j < 3; j++) y[m][j] = (float)(xv[m][j] - xv[0][j]);
-#pragma unroll
-  for (int j = 0; j < 3; j++) yp[j] = (float)(p[j] - xv[0][j]);
   float f[8][3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
@@ -752,6 +747,18 @@ __device__ __forceinline__ int screen32(const double xv[8][3], const double p[3]
   return interior ? 1 : -1;
 }
 
+__device__ __forceinline__ int screen32(const double xv[8][3], const double p[3], int nv) {
+  float y[8][3], yp[3];
+#pragma unroll
+  for (int m = 0; m < 8; m++)
+    if (m < nv)
+#pragma unroll
+      for (int j = 0; j < 3; j++) y[m][j] = (float)(xv[m][j] - xv[0][j]);
+#pragma unroll
+  for (int j = 0; j < 3; j++) yp[j] = (float)(p[j] - xv[0][j]);
+  return screen32f(y, yp, nv);
+}
+
 // ---------------------------------------------------------------------------
 // Search, stage 1: stack-free traversal of the donor block's tree.  Every
 // cell whose (conservative) box holds the point is appended to the candidate
@@ -759,30 +766,49 @@ __device__ __forceinline__ int screen32(const double xv[8][3], const double p[3]
 // reference's +-TOL (exact candidates); FORM 1 tests FP32 boxes rounded
 // outward with a relative margin (a superset, filtered exactly in stage 2).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void append_candidate(int q, int s, int2* __restrict__ cand, int cap,
-                                                 unsigned* __restrict__ count) {
-  const unsigned mask = __activemask();
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  const int rank = __popc(mask & ((1u << lane) - 1u));
-  unsigned base = 0;
-  if (lane == leader) base = atomicAdd(count, (unsigned)__popc(mask));
-  base = __shfl_sync(mask, base, leader);
-  const unsigned i = base + rank;
-  if (i < (unsigned)cap) cand[i] = make_int2(q, s);
+// Candidates of a query go to kSlots inline slots of that query; the rare
+// extra ones (thin cells crowding a pole axis) go to an overflow list.  No
+// global counter is touched for the common case.
+__device__ __forceinline__ void add_candidate(int q, int s, int& n, int* __restrict__ slots,
+                                              int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf) {
+  if (n < kSlots) {
+    slots[(long long)q * kSlots + n] = s;
+  } else {
+    const unsigned i = atomicAdd(novf, 1u);
+    if (i < (unsigned)ovf_cap) ovf[i] = make_int3(q, s, n);
+  }
+  n++;
 }
 
+__device__ __forceinline__ bool hit32(const float4* __restrict__ tn, long long slot, const float* p,
+                                      const float* e) {
+  const float4 A = tn[2 * slot], B = tn[2 * slot + 1];
+  return p[0] >= A.x - e[0] && p[1] >= A.y - e[1] && p[2] >= A.z - e[2] && p[0] <= A.w + e[0] &&
+         p[1] <= B.x + e[1] && p[2] <= B.y + e[2];
+}
+__device__ __forceinline__ bool hit64(const double* __restrict__ tn, long long slot, const double* p) {
+  const double* b = tn + 6 * slot;
+  return p[0] >= b[0] - kTol && p[1] >= b[1] - kTol && p[2] >= b[2] - kTol && p[0] <= b[3] + kTol &&
+         p[1] <= b[4] + kTol && p[2] <= b[5] + kTol;
+}
+
+// Depth-first walk of the 4-ary tree without a stack: the four children of a
+// node are tested together (one 128-byte line) and the hits not yet visited
+// are kept as a 4-bit mask per depth in `trail`.
 template <int FORM>
 __global__ void __launch_bounds__(256) k_traverse(
     const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
-    const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int2* __restrict__ cand,
-    int cap, unsigned* __restrict__ count) {
+    const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
+    int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
+    int n = 0;
     const int g = qnode[q];
     const int a = qdon[q];
-    const int P = bi[a].P, toff = bi[a].tree_off, coff = bi[a].cell_off, nc = bi[a].ncells;
+    const int D = bi[a].depth, toff = bi[a].tree_off, coff = bi[a].cell_off, nc = bi[a].ncells;
+    const int Lc = bi[a].leaf_cells;
+    const long long leaf0 = bi[a].leaf_first;
     double p[3];
     float p32[3], e32[3];
     p[0] = x[3 * (long long)g];
@@ -793,44 +819,87 @@ __global__ void __launch_bounds__(256) k_traverse(
       p32[k] = (float)p[k];
       e32[k] = fabsf(p32[k]) * 4.8e-7f + 1e-9f;
     }
-    int node = 0;
-    for (;;) {
-      bool hit;
-      const long long gn = (long long)toff + node;
-      if (FORM == 0) {
-        const double* b = tnode64 + 6 * gn;
-        hit = p[0] >= b[0] - kTol && p[1] >= b[1] - kTol && p[2] >= b[2] - kTol && p[0] <= b[3] + kTol &&
-              p[1] <= b[4] + kTol && p[2] <= b[5] + kTol;
-      } else {
-        const float4 A = tnode[2 * gn], B = tnode[2 * gn + 1];
-        hit = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
-              p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
-      }
-      if (hit) {
-        if (node < P - 1) {
-          node = 2 * node + 1;
-          continue;
-        }
-        const int j0 = (node - (P - 1)) * kLeafCells, j1 = min(j0 + kLeafCells, nc);
-        for (int j = j0; j < j1; j++) {
-          const long long s = (long long)coff + j;
-          bool pass;
-          if (FORM == 0) {
-            const double* b = cbox64 + 6 * s;
-            const double lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
-            pass = in_box64(p, lo, hi);
-          } else {
-            const float4 A = cbox[2 * s], B = cbox[2 * s + 1];
-            pass = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
-                   p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
+    const bool root = (FORM == 0) ? hit64(tnode64, tslot(toff, 0), p) : hit32(tnode, tslot(toff, 0), p32, e32);
+    if (root) {
+      long long node = 0;
+      int depth = 0;
+      unsigned long long trail = 0;
+      for (;;) {
+        bool descended = false;
+        if (depth < D) {
+          const long long c0 = 4 * node + 1;
+          unsigned m = 0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const bool h = (FORM == 0) ? hit64(tnode64, tslot(toff, c0 + k), p)
+                                       : hit32(tnode, tslot(toff, c0 + k), p32, e32);
+            m |= (unsigned)h << k;
           }
-          if (pass) append_candidate((int)q, (int)s, cand, cap, count);
+          if (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1;
+            trail |= (unsigned long long)m << (4 * depth);
+            node = c0 + c;
+            depth++;
+            descended = true;
+          }
+        } else {
+          const long long j0 = (node - leaf0) * Lc;
+          const long long j1 = min(j0 + Lc, (long long)nc);
+          for (long long j = j0; j < j1; j++) {
+            const long long s = (long long)coff + j;
+            bool pass;
+            if (FORM == 0) {
+              const double* bb = cbox64 + 6 * s;
+              const double lo[3] = {bb[0], bb[1], bb[2]}, hi[3] = {bb[3], bb[4], bb[5]};
+              pass = in_box64(p, lo, hi);
+            } else {
+              const float4 A = cbox[2 * s], B = cbox[2 * s + 1];
+              pass = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
+                     p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
+            }
+            if (pass) add_candidate((int)q, (int)s, n, slots, ovf, ovf_cap, novf);
+          }
         }
+        if (descended) continue;
+        // back up to the deepest node with children still to visit
+        bool more = false;
+        while (depth > 0) {
+          depth--;
+          node = (node - 1) >> 2;
+          unsigned m = (unsigned)(trail >> (4 * depth)) & 0xFu;
+          if (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1;
+            trail = (trail & ~(0xFull << (4 * depth))) | ((unsigned long long)m << (4 * depth));
+            node = 4 * node + 1 + c;
+            depth++;
+            more = true;
+            break;
+          }
+        }
+        if (!more) break;
       }
-      while (node > 0 && !(node & 1)) node = (node - 1) >> 1;
-      if (node == 0) break;
-      node++;
     }
+    ncand_q[q] = n;
+  }
+}
+
+// Dense, query-ordered candidate list from the slots and the overflow list
+// (off = exclusive scan of the per-query counts).
+__global__ void k_gather_candidates(const int* __restrict__ slots, const int* __restrict__ ncand_q,
+                                    const int* __restrict__ off, long long nq, const int3* __restrict__ ovf,
+                                    const unsigned* __restrict__ novf, int ovf_cap, int2* __restrict__ cand) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int n = min(ncand_q[q], kSlots);
+    const int o = off[q];
+    for (int k = 0; k < n; k++) cand[o + k] = make_int2((int)q, slots[q * kSlots + k]);
+  }
+  const int no = min((int)*novf, ovf_cap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < no; i += gridDim.x * blockDim.x) {
+    const int3 e = ovf[i];
+    cand[off[e.x] + e.z] = make_int2(e.x, e.y);
   }
 }
 
@@ -853,7 +922,7 @@ __device__ __forceinline__ void record_accept(int q, int c, int cls, unsigned lo
 // 3; FORM 0 decides everything with the reference's FP64 arithmetic.
 // ---------------------------------------------------------------------------
 template <int FORM>
-__global__ void __launch_bounds__(256) k_candidates(
+__global__ void __launch_bounds__(256, 2) k_candidates(
     const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
     const double* __restrict__ cell_res, const int* __restrict__ sorted_cell, const int* __restrict__ qnode,
     const int2* __restrict__ cand, int ncand, unsigned long long* __restrict__ qkey,
@@ -868,30 +937,45 @@ __global__ void __launch_bounds__(256) k_candidates(
     const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c);
     const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c + 4);
     const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    double xv[8][3];
-    gather_vertices(x, cv, nv, xv);
     const int g = qnode[q];
     const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
-    if (FORM == 1) {
-      double lo[3] = {xv[0][0], xv[0][1], xv[0][2]}, hi[3] = {xv[0][0], xv[0][1], xv[0][2]};
-      for (int m = 1; m < nv; m++)
-        for (int k = 0; k < 3; k++) {
-          lo[k] = dmin(lo[k], xv[m][k]);
-          hi[k] = dmax(hi[k], xv[m][k]);
-        }
-      if (!in_box64(p, lo, hi)) continue;
-    }
-    my_cand++;
-    my_verts += nv;
     int cls;
     if (FORM == 1) {
-      cls = (nv == 4) ? -1 : screen32(xv, p, nv);
+      // exact FP64 element box while streaming the vertices; keep only the
+      // FP32 offsets from vertex 0 for the screen
+      const double* v0p = x + 3 * (long long)cv[0];
+      const double v0[3] = {v0p[0], v0p[1], v0p[2]};
+      double lo[3] = {v0[0], v0[1], v0[2]}, hi[3] = {v0[0], v0[1], v0[2]};
+      float y[8][3];
+      y[0][0] = y[0][1] = y[0][2] = 0.f;
+#pragma unroll
+      for (int m = 1; m < 8; m++) {
+        if (m < nv) {
+          const double* vp = x + 3 * (long long)cv[m];
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const double v = vp[k];
+            lo[k] = dmin(lo[k], v);
+            hi[k] = dmax(hi[k], v);
+            y[m][k] = (float)(v - v0[k]);
+          }
+        }
+      }
+      if (!in_box64(p, lo, hi)) continue;
+      my_cand++;
+      my_verts += nv;
+      const float yp[3] = {(float)(p[0] - v0[0]), (float)(p[1] - v0[1]), (float)(p[2] - v0[2])};
+      cls = (nv == 4) ? -1 : screen32f(y, yp, nv);
       if (cls < 0) {
         const unsigned r = atomicAdd(nrefine, 1u);
         refine[r] = i;  // capacity: one slot per candidate
         continue;
       }
     } else {
+      double xv[8][3];
+      gather_vertices(x, cv, nv, xv);
+      my_cand++;
+      my_verts += nv;
       double frac[8];
       nodal_weights64(xv, p, frac, nv);
       cls = classify64(frac, nv, cell_res[c] == kBig);
@@ -961,11 +1045,14 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
-                     const int* qnode, const int* qdon, long long nq, int2* cand, int cap, unsigned* count) {
+                     const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
+                     int ovf_cap, unsigned* novf) {
   if (form == 0)
-    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, cand, cap, count);
+    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+                                          ovf, ovf_cap, novf);
   else
-    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, cand, cap, count);
+    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+                                          ovf, ovf_cap, novf);
 }
 
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,

@@ -390,6 +390,26 @@ __global__ void k_morton(const double* __restrict__ x, const int* __restrict__ c
   }
 }
 
+// Morton keys of node positions, block id in the high word (the order in
+// which query points are gathered, so a warp's queries are neighbours)
+__global__ void k_morton_nodes(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+                               const BlockInfo* __restrict__ bi, long long ntot, unsigned long long* __restrict__ key,
+                               int* __restrict__ val) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int b = node_blk[g];
+    unsigned code = 0;
+    for (int j = 0; j < 3; j++) {
+      float lo = bi[b].bb_lo[j], hi = bi[b].bb_hi[j];
+      float t = (hi > lo) ? (float)(x[3 * g + j] - lo) / (hi - lo) : 0.f;
+      t = fminf(fmaxf(t, 0.f), 1.f);
+      code |= spread10((unsigned)(t * 1023.f)) << j;
+    }
+    key[g] = ((unsigned long long)b << 32) | code;
+    val[g] = (int)g;
+  }
+}
+
 __global__ void k_invert(const int* __restrict__ perm, long long n, int* __restrict__ inv) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x)
