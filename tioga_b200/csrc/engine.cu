@@ -369,6 +369,30 @@ int Engine::build_tree_topology() {
   TB_CUDA(cub_tmp_.ensure(tmp));
   cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
                                   (int)ctot_, 0, 40, stream_);
+  // From here on every cell array is in storage (Morton) order; sorted_cell_
+  // maps a storage position to the caller's cell id and inv_sorted_ back.
+  TB_CUDA(inv_sorted_.ensure(ctot_));
+  k_invert<<<grid_for(ctot_, kT), kT, 0, stream_>>>(sorted_cell_.p, ctot_, inv_sorted_.p);
+  TB_LAUNCHED("k_invert");
+  {
+    DBuf<int> conn2;
+    DBuf<unsigned char> nv2, blk2;
+    TB_CUDA(conn2.ensure(8 * ctot_));
+    TB_CUDA(nv2.ensure(ctot_));
+    TB_CUDA(blk2.ensure(ctot_));
+    k_permute_cells<<<grid_for(ctot_, kT), kT, 0, stream_>>>(sorted_cell_.p, ctot_, conn8_.p, cell_nv_.p,
+                                                              cell_blk_.p, conn2.p, nv2.p, blk2.p);
+    TB_LAUNCHED("k_permute_cells");
+    std::swap(conn8_, conn2);
+    std::swap(cell_nv_, nv2);
+    std::swap(cell_blk_, blk2);
+    k_remap<<<grid_for(inc_tot_, kT), kT, 0, stream_>>>(csr_cell_.p, inc_tot_, inv_sorted_.p);
+    TB_LAUNCHED("k_remap");
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    conn2.release();
+    nv2.release();
+    blk2.release();
+  }
   // Morton order of each block's nodes: the order query points are gathered in
   TB_CUDA(node_order_.ensure(ntot_));
   {
@@ -388,9 +412,6 @@ int Engine::build_tree_topology() {
     k1.release();
     v0.release();
   }
-  TB_CUDA(inv_sorted_.ensure(ctot_));
-  k_invert<<<grid_for(ctot_, kT), kT, 0, stream_>>>(sorted_cell_.p, ctot_, inv_sorted_.p);
-  TB_LAUNCHED("k_invert");
   // one 4-ary tree per block: leaves of at most kMaxLeafCells consecutive
   // cells in Morton order; node i of a block sits in slot tree_off + 3 + i
   long long off = 0;
@@ -455,13 +476,29 @@ int Engine::preprocess() {
   TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
                           stream_));
   TB_TRY(upload_coords());
+  TB_TRY(compute_obbs());
+  // keep the OBBs and block boxes on the host too
+  TB_CUDA(cudaMemcpyAsync(bi_.data(), d_bi_.p, bi_.size() * sizeof(BlockInfo), cudaMemcpyDeviceToHost,
+                          stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (fresh || tree_nodes_ == 0) {
+    TB_TRY(build_tree_topology());  // also puts the cell arrays in storage order
+    TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
+                            stream_));
+  }
   for (size_t b = 0; b < hb_.size(); b++) {
     const HostBlock& H = hb_[b];
     if (!bi_[b].has_user_res) continue;
     TB_CUDA(cudaMemcpyAsync(node_res_.p + bi_[b].node_off, H.user_nres, H.nnodes * sizeof(double),
                             cudaMemcpyHostToDevice, stream_));
-    TB_CUDA(cudaMemcpyAsync(cell_res_.p + bi_[b].cell_off, H.user_cres, H.ncells * sizeof(double),
-                            cudaMemcpyHostToDevice, stream_));
+    DBuf<double> stage;
+    TB_CUDA(stage.ensure(H.ncells));
+    TB_CUDA(cudaMemcpyAsync(stage.p, H.user_cres, H.ncells * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    k_scatter_f64<<<grid_for(H.ncells, kT), kT, 0, stream_>>>(stage.p, H.ncells, inv_sorted_.p, bi_[b].cell_off,
+                                                               cell_res_.p);
+    TB_LAUNCHED("k_scatter_f64");
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    stage.release();
   }
   k_cell_volume<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p,
                                                           ctot_, cell_res_.p);
@@ -469,7 +506,6 @@ int Engine::preprocess() {
   k_node_res<<<grid_for(ntot_, kT), kT, 0, stream_>>>(csr_off_.p, csr_cell_.p, cell_res_.p, node_blk_.p,
                                                        d_bi_.p, ntot_, node_res_.p);
   TB_LAUNCHED("k_node_res");
-  TB_TRY(compute_obbs());
   TB_CUDA(cudaMemsetAsync(ex0_.p, 0, ntot_, stream_));
   TB_CUDA(cudaMemsetAsync(ex1_.p, 0, ntot_, stream_));
   k_mandatory<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, obcf_.p, node_res_.p,
@@ -484,15 +520,6 @@ int Engine::preprocess() {
   }
   k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, 1, ntot_);
   TB_LAUNCHED("k_fill_int");
-  // keep the OBBs and block boxes on the host too
-  TB_CUDA(cudaMemcpyAsync(bi_.data(), d_bi_.p, bi_.size() * sizeof(BlockInfo), cudaMemcpyDeviceToHost,
-                          stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
-  if (fresh || tree_nodes_ == 0) {
-    TB_TRY(build_tree_topology());
-    TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
-                            stream_));
-  }
   for (size_t b = 0; b < hb_.size(); b++) {  // preprocess sets iblank = 1 (MeshBlock.C:80)
     HostBlock& H = hb_[b];
     if (H.dibl)
@@ -630,8 +657,7 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  k_cell_pass<<<grid_for(ctot_, 256), 256, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, inv_sorted_.p,
-                                                         ctot_, d_bi_.p, d_pairs_.p, npairs_, cbox_.p,
+  k_cell_pass<<<grid_for(ctot_, 256), 256, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, ctot_, d_bi_.p, d_pairs_.p, npairs_, cbox_.p,
                                                          fp64 ? cbox64_.p : nullptr, pair_acc_.p);
   TB_LAUNCHED("k_cell_pass");
   for (size_t pass = 0; pass + 1 < refit_pass_off_.size(); pass++) {
@@ -750,7 +776,8 @@ int Engine::run_search() {
   }
   if (count == 0) TB_CUDA(cudaEventRecord(sev_[2], stream_));
   TB_CUDA(cudaEventRecord(sev_[3], stream_));
-  k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, qcell_.p, qtie_.p, counters_.p);
+  k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, inv_sorted_.p, qcell_.p, qtie_.p,
+                                                         counters_.p);
   TB_LAUNCHED("k_search_finish");
   search_timed_ = true;
   return 0;
@@ -831,7 +858,8 @@ int Engine::run_donors() {
     TB_LAUNCHED("k_interp_marks");
     k_interp<<<grid_for(R, 128), 128, 0, stream_>>>(x_.p, rkey_.p, rval_.p, rcount_.p, qcell_.p, conn8_.p,
                                                      cell_nv_.p, node_blk_.p, d_bi_.p, iblank_.p, node_res_.p,
-                                                     reset_t_.p, it_node_.p, it_w_.p, it_rec_.p, it_don_.p,
+                                                     reset_t_.p, sorted_cell_.p, it_node_.p, it_w_.p, it_rec_.p,
+                                                     it_don_.p,
                                                      it_nv_.p, it_cancel_.p, rres_.p, interp2rec_.p, err_.p);
     TB_LAUNCHED("k_interp");
     k_cancel<<<grid_for(ntot_, kT), kT, 0, stream_>>>(cmark_.p, ntot_, slot_.p, K_, qcell_.p, cell_res_.p,
@@ -848,7 +876,7 @@ int Engine::run_donors() {
 }
 
 int Engine::run_celliblank() {
-  k_cell_iblank<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, iblank_.p,
+  k_cell_iblank<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, iblank_.p, sorted_cell_.p,
                                                           iblank_cell_.p);
   TB_LAUNCHED("k_cell_iblank");
   k_count_iblank<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, ntot_, counters_.p);
@@ -864,9 +892,16 @@ int Engine::download_iblank() {
     else
       TB_CUDA(cudaMemcpyAsync(hb_[b].hibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
                               cudaMemcpyDeviceToHost, stream_));
-    if (hb_[b].h_iblank_cell)
-      TB_CUDA(cudaMemcpyAsync(hb_[b].h_iblank_cell, iblank_cell_.p + bi_[b].cell_off,
-                              hb_[b].ncells * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    if (hb_[b].h_iblank_cell) {
+      TB_CUDA(cell_stage_.ensure(hb_[b].ncells));
+      k_gather_cells_i32<<<grid_for(hb_[b].ncells, kT), kT, 0, stream_>>>(iblank_cell_.p, inv_sorted_.p,
+                                                                          bi_[b].cell_off, hb_[b].ncells,
+                                                                          cell_stage_.p);
+      TB_LAUNCHED("k_gather_cells_i32");
+      TB_CUDA(cudaMemcpyAsync(hb_[b].h_iblank_cell, cell_stage_.p, hb_[b].ncells * sizeof(int),
+                              cudaMemcpyDeviceToHost, stream_));
+      TB_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused
+    }
   }
   return 0;
 }
@@ -1023,8 +1058,12 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
 int Engine::cell_iblank(int tag, int* out) {
   int ib = find_tag(tag);
   if (ib < 0 || !connected_) return -1;
-  TB_CUDA(cudaMemcpyAsync(out, iblank_cell_.p + bi_[ib].cell_off, bi_[ib].ncells * sizeof(int),
-                          cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cell_stage_.ensure(bi_[ib].ncells));
+  k_gather_cells_i32<<<grid_for(bi_[ib].ncells, kT), kT, 0, stream_>>>(iblank_cell_.p, inv_sorted_.p,
+                                                                       bi_[ib].cell_off, bi_[ib].ncells,
+                                                                       cell_stage_.p);
+  TB_LAUNCHED("k_gather_cells_i32");
+  TB_CUDA(cudaMemcpyAsync(out, cell_stage_.p, bi_[ib].ncells * sizeof(int), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   return 0;
 }

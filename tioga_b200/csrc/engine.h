@@ -207,6 +207,7 @@ class Engine {
   DBuf<int> node_order_;    // Morton order of each block's nodes
   DBuf<int> slots_, ncand_q_, cand_off_;
   DBuf<int3> ovf_;
+  DBuf<int> cell_stage_;     // one block's cells in the caller's order
   long long ntot_ = 0, ctot_ = 0, inc_tot_ = 0;
   int last_error_ = 0;
   cudaStream_t stream_ = nullptr;

@@ -84,7 +84,7 @@ __global__ void k_pairs(BlockInfo* bi, int nb, PairInfo* pairs, int* npairs);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 __global__ void k_cell_pass(const double* x, const int* conn8, const unsigned char* cell_nv,
-                            const unsigned char* cell_blk, const int* inv_sorted, long long ctot,
+                            const unsigned char* cell_blk, long long ctot,
                             const BlockInfo* bi, const PairInfo* pairs, int npairs, float4* cbox, double* cbox64,
                             unsigned long long* acc);
 __global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, int pass0, const float4* cbox,
@@ -94,6 +94,11 @@ __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const
 __global__ void k_morton_nodes(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);
 __global__ void k_invert(const int* perm, long long n, int* inv);
+__global__ void k_permute_cells(const int* perm, long long n, const int* conn8, const unsigned char* nv,
+                                const unsigned char* blk, int* conn8_out, unsigned char* nv_out,
+                                unsigned char* blk_out);
+__global__ void k_remap(int* idx, long long n, const int* map);
+__global__ void k_scatter_f64(const double* src, long long n, const int* inv, long long base, double* dst);
 __global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs,
                               int tiles_x, int tile, int* tile_cnt, const float4* tbox, const long long* tile_base,
                               const int* node_order);
@@ -116,8 +121,9 @@ void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, c
 __global__ void k_refine(const double* x, const int* conn8, const unsigned char* cell_nv, const double* cell_res,
                          const int* sorted_cell, const int* qnode, const int2* cand, const int* refine,
                          const unsigned* nrefine, unsigned long long* qkey, unsigned* qacc);
-__global__ void k_search_finish(const unsigned long long* qkey, const unsigned* qacc, long long nq, int* qcell,
-                                unsigned char* qtie, unsigned long long* counters);
+__global__ void k_search_finish(const unsigned long long* qkey, const unsigned* qacc, long long nq,
+                                const int* inv_sorted, int* qcell, unsigned char* qtie,
+                                unsigned long long* counters);
 
 // ---- donors (kernels_donor.cu) ----
 __global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
@@ -142,8 +148,8 @@ __global__ void k_interp(const double* x, const unsigned long long* rkey, const 
                          const int* rcount, const int* qcell, const int* conn8,
                          const unsigned char* cell_nv, const unsigned char* node_blk,
                          const BlockInfo* bi, const int* iblank, const double* node_res,
-                         const int* reset_t, int* it_node, double* it_w, int* it_rec, int* it_don,
-                         unsigned char* it_nv, unsigned char* it_cancel, double* rres,
+                         const int* reset_t, const int* orig_cell, int* it_node, double* it_w, int* it_rec,
+                         int* it_don, unsigned char* it_nv, unsigned char* it_cancel, double* rres,
                          int* interp2rec, unsigned* err);
 __global__ void k_cancel(const unsigned char* cmark, long long ntot, const int* slot, int K,
                          const int* qcell, const double* cell_res, const int* interp2rec,
@@ -152,7 +158,8 @@ __global__ void k_iblank_clear(int* iblank, long long ntot);
 __global__ void k_iblank_set(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
                              int* iblank);
 __global__ void k_cell_iblank(const int* conn8, const unsigned char* cell_nv, long long ctot,
-                              const int* iblank, int* iblank_cell);
+                              const int* iblank, const int* orig_cell, int* iblank_cell);
+__global__ void k_gather_cells_i32(const int* src, const int* inv, long long base, int n, int* out);
 __global__ void k_count_iblank(const int* iblank, long long ntot, unsigned long long* counters);
 __global__ void k_interp_gather(const int* it_node, const double* it_w, const int* it_don,
                                 const unsigned char* it_nv, const unsigned char* it_cancel,

@@ -303,16 +303,15 @@ __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __rest
 __device__ __forceinline__ float f_rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float f_ru(double v) { return __double2float_ru(v); }
 
-// One pass over all cells in their natural order (coalesced connectivity):
-// the FP64 element box, stored (FP32, rounded outward) at the cell's
-// position in the tree order, and the reduced-box accumulation of every pair
+// One pass over all cells in storage (tree) order: the FP64 element box,
+// stored in FP32 rounded outward, and the reduced-box accumulation of every pair
 // whose donor is the cell's block (getReducedOBB, MeshBlock.C:774-838).  A
 // cell is projected vertex by vertex only if the projection of its box centre
 // does not already prove every vertex outside the receptor box, so the
 // overlap decision is the reference's exact one.
-__global__ void __launch_bounds__(256) k_cell_pass(
+__global__ void __launch_bounds__(256, 3) k_cell_pass(
     const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-    const unsigned char* __restrict__ cell_blk, const int* __restrict__ inv_sorted, long long ctot,
+    const unsigned char* __restrict__ cell_blk, long long ctot,
     const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs, int npairs,
     float4* __restrict__ cbox, double* __restrict__ cbox64, unsigned long long* __restrict__ acc) {
   const int lane = threadIdx.x & 31;
@@ -336,11 +335,10 @@ __global__ void __launch_bounds__(256) k_cell_pass(
           lo[k] = dmin(lo[k], xv[m][k]);
           hi[k] = dmax(hi[k], xv[m][k]);
         }
-      const long long j = inv_sorted[c];
-      cbox[2 * j] = make_float4(f_rd(lo[0]), f_rd(lo[1]), f_rd(lo[2]), f_ru(hi[0]));
-      cbox[2 * j + 1] = make_float4(f_ru(hi[1]), f_ru(hi[2]), 0.f, 0.f);
+      cbox[2 * c] = make_float4(f_rd(lo[0]), f_rd(lo[1]), f_rd(lo[2]), f_ru(hi[0]));
+      cbox[2 * c + 1] = make_float4(f_ru(hi[1]), f_ru(hi[2]), 0.f, 0.f);
       if (cbox64) {
-        double* o = cbox64 + 6 * j;
+        double* o = cbox64 + 6 * c;
         o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
         o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
       }
@@ -780,11 +778,11 @@ __device__ __forceinline__ void add_candidate(int q, int s, int& n, int* __restr
   n++;
 }
 
-__device__ __forceinline__ bool hit32(const float4* __restrict__ tn, long long slot, const float* p,
-                                      const float* e) {
+// box [A.xyz, (A.w, B.x, B.y)] against the point interval [lo, hi] = p -+ e
+__device__ __forceinline__ bool hit32(const float4* __restrict__ tn, long long slot, const float* lo,
+                                      const float* hi) {
   const float4 A = tn[2 * slot], B = tn[2 * slot + 1];
-  return p[0] >= A.x - e[0] && p[1] >= A.y - e[1] && p[2] >= A.z - e[2] && p[0] <= A.w + e[0] &&
-         p[1] <= B.x + e[1] && p[2] <= B.y + e[2];
+  return A.x <= hi[0] && A.y <= hi[1] && A.z <= hi[2] && A.w >= lo[0] && B.x >= lo[1] && B.y >= lo[2];
 }
 __device__ __forceinline__ bool hit64(const double* __restrict__ tn, long long slot, const double* p) {
   const double* b = tn + 6 * slot;
@@ -810,16 +808,18 @@ __global__ void __launch_bounds__(256) k_traverse(
     const int Lc = bi[a].leaf_cells;
     const long long leaf0 = bi[a].leaf_first;
     double p[3];
-    float p32[3], e32[3];
+    float plo[3], phi[3];  // the point widened by a margin that covers TOL and FP32 rounding
     p[0] = x[3 * (long long)g];
     p[1] = x[3 * (long long)g + 1];
     p[2] = x[3 * (long long)g + 2];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      p32[k] = (float)p[k];
-      e32[k] = fabsf(p32[k]) * 4.8e-7f + 1e-9f;
+      const float p32 = (float)p[k];
+      const float e = fabsf(p32) * 9.6e-7f + 2e-9f;
+      plo[k] = p32 - e;
+      phi[k] = p32 + e;
     }
-    const bool root = (FORM == 0) ? hit64(tnode64, tslot(toff, 0), p) : hit32(tnode, tslot(toff, 0), p32, e32);
+    const bool root = (FORM == 0) ? hit64(tnode64, tslot(toff, 0), p) : hit32(tnode, tslot(toff, 0), plo, phi);
     if (root) {
       long long node = 0;
       int depth = 0;
@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(256) k_traverse(
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const bool h = (FORM == 0) ? hit64(tnode64, tslot(toff, c0 + k), p)
-                                       : hit32(tnode, tslot(toff, c0 + k), p32, e32);
+                                       : hit32(tnode, tslot(toff, c0 + k), plo, phi);
             m |= (unsigned)h << k;
           }
           if (m) {
@@ -854,9 +854,7 @@ __global__ void __launch_bounds__(256) k_traverse(
               const double lo[3] = {bb[0], bb[1], bb[2]}, hi[3] = {bb[3], bb[4], bb[5]};
               pass = in_box64(p, lo, hi);
             } else {
-              const float4 A = cbox[2 * s], B = cbox[2 * s + 1];
-              pass = p32[0] >= A.x - e32[0] && p32[1] >= A.y - e32[1] && p32[2] >= A.z - e32[2] &&
-                     p32[0] <= A.w + e32[0] && p32[1] <= B.x + e32[1] && p32[2] <= B.y + e32[2];
+              pass = hit32(cbox, s, plo, phi);
             }
             if (pass) add_candidate((int)q, (int)s, n, slots, ovf, ovf_cap, novf);
           }
@@ -932,7 +930,7 @@ __global__ void __launch_bounds__(256, 2) k_candidates(
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
     const int2 qs = cand[i];
     const int q = qs.x;
-    const int c = sorted_cell[qs.y];
+    const int c = qs.y;  // storage position; the tie rule uses the registration id
     const int nv = cell_nv[c];
     const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c);
     const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * (long long)c + 4);
@@ -980,7 +978,7 @@ __global__ void __launch_bounds__(256, 2) k_candidates(
       nodal_weights64(xv, p, frac, nv);
       cls = classify64(frac, nv, cell_res[c] == kBig);
     }
-    record_accept(q, c, cls, qkey, qacc);
+    record_accept(q, sorted_cell[c], cls, qkey, qacc);
   }
   for (int o = 16; o > 0; o >>= 1) {
     my_cand += __shfl_xor_sync(0xffffffffu, my_cand, o);
@@ -1004,7 +1002,7 @@ __global__ void __launch_bounds__(128) k_refine(const double* __restrict__ x, co
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int2 qs = cand[refine[k]];
     const int q = qs.x;
-    const int c = sorted_cell[qs.y];
+    const int c = qs.y;
     const int nv = cell_nv[c];
     double xv[8][3];
     gather_vertices(x, conn8 + 8 * (long long)c, nv, xv);
@@ -1012,19 +1010,19 @@ __global__ void __launch_bounds__(128) k_refine(const double* __restrict__ x, co
     const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
     double frac[8];
     nodal_weights64(xv, p, frac, nv);
-    record_accept(q, c, classify64(frac, nv, cell_res[c] == kBig), qkey, qacc);
+    record_accept(q, sorted_cell[c], classify64(frac, nv, cell_res[c] == kBig), qkey, qacc);
   }
 }
 
 // Search, stage 4: per query outcome and tie flags.
 __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, const unsigned* __restrict__ qacc,
-                                long long nq, int* __restrict__ qcell, unsigned char* __restrict__ qtie,
-                                unsigned long long* __restrict__ counters) {
+                                long long nq, const int* __restrict__ inv_sorted, int* __restrict__ qcell,
+                                unsigned char* __restrict__ qtie, unsigned long long* __restrict__ counters) {
   unsigned long long my_tie = 0, my_found = 0;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
     const unsigned long long key = qkey[q];
-    const int donor = (key == ~0ull) ? -1 : (int)(key & 0xffffffffull);
+    const int donor = (key == ~0ull) ? -1 : inv_sorted[(int)(key & 0xffffffffull)];
     const unsigned acc = qacc[q];
     const unsigned nacc = acc & 0xffffu, nprov = acc >> 16;
     const unsigned char tie = (unsigned char)((nacc >= 2 ? 1 : 0) | (nprov >= 1 ? 2 : 0));

@@ -191,7 +191,8 @@ __global__ void k_interp(const double* __restrict__ x, const unsigned long long*
                          const unsigned char* __restrict__ cell_nv, const unsigned char* __restrict__ node_blk,
                          const BlockInfo* __restrict__ bi, const int* __restrict__ iblank,
                          const double* __restrict__ node_res, const int* __restrict__ reset_t,
-                         int* __restrict__ it_node, double* __restrict__ it_w, int* __restrict__ it_rec,
+                         const int* __restrict__ orig_cell, int* __restrict__ it_node,
+                         double* __restrict__ it_w, int* __restrict__ it_rec,
                          int* __restrict__ it_don, unsigned char* __restrict__ it_nv,
                          unsigned char* __restrict__ it_cancel, double* __restrict__ rres_out,
                          int* __restrict__ interp2rec, unsigned* __restrict__ err) {
@@ -236,7 +237,7 @@ __global__ void k_interp(const double* __restrict__ x, const unsigned long long*
       it_w[9 * (long long)r + m] = frac[m];
       if (frac[m] < -0.2 || frac[m] > 1.2) atomicOr(err, kErrWeightRange);
     }
-    it_node[9 * (long long)r + nv] = c - bi[a].cell_off;
+    it_node[9 * (long long)r + nv] = orig_cell[c] - bi[a].cell_off;  // the caller's cell id
     it_w[9 * (long long)r + nv] = 0.0;
     it_nv[r] = (unsigned char)nv;
     it_rec[r] = g;
@@ -279,7 +280,8 @@ __global__ void k_iblank_set(const int* __restrict__ it_rec, const unsigned char
 
 // getCellIblanks (highOrder.C:88-150)
 __global__ void k_cell_iblank(const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-                              long long ctot, const int* __restrict__ iblank, int* __restrict__ iblank_cell) {
+                              long long ctot, const int* __restrict__ iblank, const int* __restrict__ orig_cell,
+                              int* __restrict__ iblank_cell) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
        c += (long long)gridDim.x * blockDim.x) {
     const int nv = cell_nv[c];
@@ -296,6 +298,13 @@ __global__ void k_cell_iblank(const int* __restrict__ conn8, const unsigned char
     if (flag && ncount == nv) v = -1;
     iblank_cell[c] = v;
   }
+}
+
+// cells of one block back in the caller's order: out[i] = src[inv[base + i]]
+__global__ void k_gather_cells_i32(const int* __restrict__ src, const int* __restrict__ inv, long long base,
+                                   int n, int* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = src[inv[base + i]];
 }
 
 __global__ void k_count_iblank(const int* __restrict__ iblank, long long ntot,

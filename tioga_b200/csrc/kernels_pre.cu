@@ -410,6 +410,40 @@ __global__ void k_morton_nodes(const double* __restrict__ x, const unsigned char
   }
 }
 
+// Cell arrays from registration order to storage (Morton) order:
+// dst[s] = src[perm[s]].
+__global__ void k_permute_cells(const int* __restrict__ perm, long long n, const int* __restrict__ conn8,
+                                const unsigned char* __restrict__ nv, const unsigned char* __restrict__ blk,
+                                int* __restrict__ conn8_out, unsigned char* __restrict__ nv_out,
+                                unsigned char* __restrict__ blk_out) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const long long c = perm[s];
+    const int4* src = reinterpret_cast<const int4*>(conn8 + 8 * c);
+    int4* dst = reinterpret_cast<int4*>(conn8_out + 8 * s);
+    dst[0] = src[0];
+    dst[1] = src[1];
+    nv_out[s] = nv[c];
+    blk_out[s] = blk[c];
+  }
+}
+
+// idx[i] = map[idx[i]] (node->cell lists from registration to storage ids;
+// each list keeps its registration order, the order of the reference's sums)
+__global__ void k_remap(int* __restrict__ idx, long long n, const int* __restrict__ map) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    idx[i] = map[idx[i]];
+}
+
+// dst[inv[c]] = src[c] for doubles (user cell resolutions into storage order)
+__global__ void k_scatter_f64(const double* __restrict__ src, long long n, const int* __restrict__ inv,
+                              long long base, double* __restrict__ dst) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x)
+    dst[inv[base + c]] = src[c];
+}
+
 __global__ void k_invert(const int* __restrict__ perm, long long n, int* __restrict__ inv) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x)
