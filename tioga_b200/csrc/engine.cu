@@ -64,6 +64,7 @@ Engine::~Engine() {
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   for (auto& h : hm_state_) h.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
+  xf_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
@@ -416,21 +417,27 @@ int Engine::build_tree_topology() {
   // cells in Morton order; node i of a block sits in slot tree_off + 3 + i
   long long off = 0;
   int maxdepth = 0;
+  nleaf_total_ = 0;
   for (size_t b = 0; b < bi_.size(); b++) {
     BlockInfo& B = bi_[b];
-    // leaves of kMaxLeafCells consecutive Morton cells (a 2x2x2 group on a
-    // structured grid), as many leaves as the cells need
+    // leaves of kMaxLeafCells consecutive Morton cells, as many leaves as
+    // the cells need
     int D = 0;
     while ((1ll << (2 * D)) * kMaxLeafCells < (long long)B.ncells) D++;
     B.depth = D;
     B.leaf_first = (int)level_first(D);
     B.leaf_cells = kMaxLeafCells;
+    B.nleaf = (B.ncells + kMaxLeafCells - 1) / kMaxLeafCells;
+    B.leaf_base = (int)nleaf_total_;
+    nleaf_total_ += B.nleaf;
     B.tree_off = (int)off;
     off += (3 + level_first(D + 1) + 3) / 4 * 4;
     maxdepth = std::max(maxdepth, D);
   }
   tree_nodes_ = off;
-  // refit groups: pass p starts at depth D-4p of each block and climbs 4 levels
+  // refit groups: pass p starts at depth D-4p of each block and climbs 4
+  // levels; only nodes with cells below them are refitted, the others keep
+  // the empty boxes written here once
   std::vector<RefitGroup> groups;
   refit_pass_off_.assign(1, 0);
   for (int pass = 0; 4 * pass <= maxdepth; pass++) {
@@ -439,7 +446,8 @@ int Engine::build_tree_topology() {
       const int L = D - 4 * pass;
       if (L < 0) continue;
       if (pass > 0 && D - 4 * (pass - 1) <= 4) continue;  // the previous pass reached the root
-      const long long width = 1ll << (2 * L);
+      const long long span = 1ll << (2 * (D - L));  // leaves under a node of level L
+      const long long width = (bi_[b].nleaf + span - 1) / span;
       for (long long f = 0; f < width; f += 256) groups.push_back(RefitGroup{(int)b, L, (int)f});
     }
     refit_pass_off_.push_back((int)groups.size());
@@ -457,6 +465,9 @@ int Engine::build_tree_topology() {
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
   TB_CUDA(cbox_.ensure(2 * ctot_));
   TB_CUDA(tnode_.ensure(2 * tree_nodes_));
+  k_empty_boxes<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(tnode_.p, tree_nodes_, nullptr);
+  TB_LAUNCHED("k_empty_boxes");
+  tnode64_empty_ = false;
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   return 0;
 }
@@ -643,6 +654,11 @@ int Engine::run_pairs_and_refit() {
   if (fp64) {
     TB_CUDA(cbox64_.ensure(6 * ctot_));
     TB_CUDA(tnode64_.ensure(6 * tree_nodes_));
+    if (!tnode64_empty_) {
+      k_empty_boxes<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(nullptr, tree_nodes_, tnode64_.p);
+      TB_LAUNCHED("k_empty_boxes");
+      tnode64_empty_ = true;
+    }
   }
   std::vector<unsigned long long> acc(6 * npairs_);
   for (int p = 0; p < npairs_; p++)
@@ -657,18 +673,29 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  k_cell_pass<<<grid_for(ctot_, 256), 256, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, ctot_, d_bi_.p, d_pairs_.p, npairs_, cbox_.p,
-                                                         fp64 ? cbox64_.p : nullptr, pair_acc_.p);
-  TB_LAUNCHED("k_cell_pass");
+  TB_CUDA(xf_.ensure(ntot_));
+  k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
+  TB_LAUNCHED("k_round_nodes");
+  // pairs in chunks that fit one CTA's shared memory; the first launch also
+  // writes the cell and leaf boxes
+  const int chunk = 256;
+  for (int p0 = 0; p0 < npairs_; p0 += chunk) {
+    const int np = std::min(chunk, npairs_ - p0);
+    const size_t smem = (size_t)np * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
+    launch_cell_pass(fp64, grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3), smem, stream_, x_.p, xf_.p, conn8_.p,
+                     cell_nv_.p, d_bi_.p, nb, nleaf_total_, d_pairs_.p, p0, np, p0 == 0 ? 1 : 0, cbox_.p,
+                     fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, pair_acc_.p);
+    TB_LAUNCHED("k_cell_pass");
+  }
   for (size_t pass = 0; pass + 1 < refit_pass_off_.size(); pass++) {
     const int g0 = refit_pass_off_[pass], g1 = refit_pass_off_[pass + 1];
     if (g1 <= g0) continue;
-    k_tree_levels<<<g1 - g0, 256, 0, stream_>>>(d_bi_.p, refit_groups_.p + g0, pass == 0 ? 1 : 0, cbox_.p,
-                                                fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr);
+    k_tree_levels<<<g1 - g0, 256, 0, stream_>>>(d_bi_.p, refit_groups_.p + g0, tnode_.p,
+                                                fp64 ? tnode64_.p : nullptr);
     TB_LAUNCHED("k_tree_levels");
   }
   if (h_tile_base_.back() > 0) {
-    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
+    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(xf_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
                                                                       node_order_.p);
     TB_LAUNCHED("k_node_tiles");
   }

@@ -20,7 +20,7 @@
 
 namespace tb {
 
-constexpr int kMaxLeafCells = 8; // cells per tree leaf at most (per-block leaf size 1..8)
+constexpr int kMaxLeafCells = 8; // cells per tree leaf (the last leaf of a block may hold fewer)
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kSlots = 8;       // inline search candidates per query
 constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
@@ -61,6 +61,8 @@ struct BlockInfo {
   int depth;           // leaves are at this depth (root = 0)
   int leaf_first;      // heap index of the first leaf, (4^depth - 1) / 3
   int leaf_cells;      // cells per leaf
+  int nleaf;           // leaves holding cells, ceil(ncells / leaf_cells)
+  int leaf_base;       // leaves of the blocks before this one
   int has_user_res;
   Obb obb;
   float bb_lo[3], bb_hi[3];  // block box for the Morton keys
@@ -71,6 +73,19 @@ struct PairInfo {  // one (receptor block, donor block) pair, src/exchangeBoxes.
   double rd[6];    // reduced box accumulator in the donor's OBB frame (ordered bits)
   Obb region;      // donor cells overlapping the receptor OBB, donor axes
   double wbox[6];  // world-axis box holding the region (tile culling)
+};
+
+// Per-pair data of the cell pass's FP32 bounds, kept in shared memory: both
+// boxes' centres in FP64 (so the centre differences are exact to FP32
+// rounding), their axes and the receptor box's half sizes in FP32.
+struct PairCull {
+  double rxc[3];  // receptor box centre
+  double dxc[3];  // donor box centre
+  float rvec[9];  // receptor axes, row j = axis j
+  float rdxc[3];  // receptor half sizes
+  float dvec[9];  // donor axes
+  int don;        // donor block
+  int pair;       // index in the pair list
 };
 
 // one CTA of the level-by-level tree refit: up to 256 nodes of one level
@@ -233,9 +248,12 @@ class Engine {
   DBuf<int> sorted_cell_;
   DBuf<float4> cbox_;      // 2 per sorted cell
   DBuf<float4> tnode_;     // 2 per tree node
+  DBuf<float4> xf_;        // coordinates rounded to FP32, one per node
   DBuf<double> tnode64_;   // 6 per tree node (FP64 form)
   DBuf<double> cbox64_;    // 6 per sorted cell (FP64 form)
   long long tree_nodes_ = 0;
+  long long nleaf_total_ = 0;    // leaves holding cells, all blocks
+  bool tnode64_empty_ = false;   // tnode64_ initialised to empty boxes for this topology
   // queries
   DBuf<int> qnode_, qdon_, qcell_;
   DBuf<double> qres_;

@@ -83,13 +83,14 @@ __global__ void k_holemap_final(unsigned char* sam, const HoleMapInfo* hm);
 __global__ void k_pairs(BlockInfo* bi, int nb, PairInfo* pairs, int* npairs);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-__global__ void k_cell_pass(const double* x, const int* conn8, const unsigned char* cell_nv,
-                            const unsigned char* cell_blk, long long ctot,
-                            const BlockInfo* bi, const PairInfo* pairs, int npairs, float4* cbox, double* cbox64,
-                            unsigned long long* acc);
-__global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, int pass0, const float4* cbox,
-                              const double* cbox64, float4* tnode, double* tnode64);
-__global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
+void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
+                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
+                      long long nleaf_total, const PairInfo* pairs, int p0, int np, int write_boxes, float4* cbox,
+                      double* cbox64, float4* tnode, double* tnode64, unsigned long long* acc);
+__global__ void k_round_nodes(const double* x, long long n, float4* xf);
+__global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, float4* tnode, double* tnode64);
+__global__ void k_empty_boxes(float4* t, long long nnodes, double* t64);
+__global__ void k_node_tiles(const float4* xf, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
 __global__ void k_morton_nodes(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);

@@ -303,92 +303,362 @@ __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __rest
 __device__ __forceinline__ float f_rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float f_ru(double v) { return __double2float_ru(v); }
 
-// One pass over all cells in storage (tree) order: the FP64 element box,
-// stored in FP32 rounded outward, and the reduced-box accumulation of every pair
-// whose donor is the cell's block (getReducedOBB, MeshBlock.C:774-838).  A
-// cell is projected vertex by vertex only if the projection of its box centre
-// does not already prove every vertex outside the receptor box, so the
-// overlap decision is the reference's exact one.
+// Bounds of every double that rounds to nearest onto v: it lies within half
+// an ulp of v, at most 2^-24 |v| (or 2^-150 below the normal range).
+__device__ __forceinline__ float f_down(float v) { return __fsub_rd(__fmaf_rd(fabsf(v), -6.0e-8f, v), 1e-44f); }
+__device__ __forceinline__ float f_up(float v) { return __fadd_ru(__fmaf_ru(fabsf(v), 6.0e-8f, v), 1e-44f); }
+
+// FP32 copy of the coordinates (rounded to nearest), read where a box that
+// holds the vertices is enough: 16 bytes per vertex instead of 24
+__global__ void k_round_nodes(const double* __restrict__ x, long long n, float4* __restrict__ xf) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]),
+                        __double2float_rn(x[3 * i + 2]), 0.f);
+}
+
+// float -> int key with the same order (-0 taken as +0), for shared-memory
+// atomicMin / atomicMax
+__device__ __forceinline__ int fkey(float f) {
+  const int i = __float_as_int(__fadd_rn(f, 0.0f));
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+
+// FP32 bounds [lo_j, hi_j] of the projections onto axes vec (rows) about
+// origin o of every point of the box with centre cc and half sizes hh.  The
+// slack covers, with a wide margin, the rounding of this FP32 arithmetic, of
+// the FP32 axes and half sizes, and of the reference's FP64 projections of the
+// vertices: every error term is below 2^-22 times the magnitudes summed into
+// it (sd, sh, ext, and |cc| for the FP64 centre).
+__device__ __forceinline__ void proj_bounds(const double cc[3], const double o[3], const float vec[9],
+                                            const float hh[3], float sc, const float ext[3], float lo[3],
+                                            float hi[3]) {
+  float dc[3], sd = 0.f;
+  for (int k = 0; k < 3; k++) {
+    dc[k] = (float)(cc[k] - o[k]);
+    sd += fabsf(dc[k]);
+  }
+  const float sh = hh[0] + hh[1] + hh[2];
+  for (int jx = 0; jx < 3; jx++) {
+    float cp = 0.f, rad = 0.f;
+    for (int k = 0; k < 3; k++) {
+      cp = __fmaf_rn(dc[k], vec[3 * jx + k], cp);
+      rad = __fmaf_rn(hh[k], fabsf(vec[3 * jx + k]), rad);
+    }
+    const float slack = 2e-6f * (sd + sh + ext[jx]) + 1e-12f * sc + 1e-30f;
+    lo[jx] = cp - rad - slack;
+    hi[jx] = cp + rad + slack;
+  }
+}
+
+// One pass over all cells, leaf by leaf (32 / kMaxLeafCells leaves of
+// kMaxLeafCells storage-order cells per warp, one lane per cell):
+//  * the FP64 element box, stored in FP32 rounded outward (and exactly for the
+//    FP64 form), and the union of each leaf's eight boxes written straight to
+//    the leaf's tree node, so the refit starts from the leaves;
+//  * the reduced box of every pair whose donor is the cell's block
+//    (getReducedOBB, MeshBlock.C:774-838), exact: the extents are minima and
+//    maxima over the vertices of the donor cells that overlap the receptor
+//    box, projected onto the donor box's axes.
+// FP32 bounds of a cell's vertex projections (box centre and half sizes,
+// widened by far more than their rounding error and the reference's) decide
+// what needs FP64:
+//  * a cell clearly outside the receptor box is skipped, one clearly inside
+//    overlaps it; only cells across its faces get the reference's FP64 test;
+//  * for the extents, each CTA keeps in shared memory an FP32 upper bound of
+//    every axis minimum (the least upper bound of any overlapping cell's
+//    projections seen so far) and a lower bound of every maximum.  A cell
+//    whose projections cannot reach below that bound cannot hold the minimum:
+//    the cell that does hold it always has its lower bound under every such
+//    upper bound, so it is always projected exactly.  The exact extents are
+//    combined per warp, per CTA in shared memory, and flushed once.
+// Pairs p0 .. p0+np-1 are handled; with write_boxes == 0 only their reduced
+// boxes are accumulated (the extra launches when the pairs exceed one CTA's
+// shared memory).
+template <bool F64>
 __global__ void __launch_bounds__(256, 3) k_cell_pass(
-    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-    const unsigned char* __restrict__ cell_blk, long long ctot,
-    const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs, int npairs,
-    float4* __restrict__ cbox, double* __restrict__ cbox64, unsigned long long* __restrict__ acc) {
-  const int lane = threadIdx.x & 31;
-  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long base = warp0 * 32; base < ctot; base += nwarps * 32) {
-    const long long c = base + lane;
-    const bool valid = c < ctot;
-    double xv[8][3];
-    int nv = 0, b = -1;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    if (valid) {
-      nv = cell_nv[c];
-      b = cell_blk[c];
-      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
-      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
-      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-      gather_vertices(x, cv, nv, xv);
-      for (int m = 0; m < nv; m++)
-        for (int k = 0; k < 3; k++) {
-          lo[k] = dmin(lo[k], xv[m][k]);
-          hi[k] = dmax(hi[k], xv[m][k]);
-        }
-      cbox[2 * c] = make_float4(f_rd(lo[0]), f_rd(lo[1]), f_rd(lo[2]), f_ru(hi[0]));
-      cbox[2 * c + 1] = make_float4(f_ru(hi[1]), f_ru(hi[2]), 0.f, 0.f);
-      if (cbox64) {
-        double* o = cbox64 + 6 * c;
-        o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
-        o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+    const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
+    const unsigned char* __restrict__ cell_nv,
+    const BlockInfo* __restrict__ bi, int nb, long long nleaf_total, const PairInfo* __restrict__ pairs, int p0,
+    int np, int write_boxes, float4* __restrict__ cbox, double* __restrict__ cbox64, float4* __restrict__ tnode,
+    double* __restrict__ tnode64, unsigned long long* __restrict__ acc) {
+  extern __shared__ unsigned long long s_dyn[];
+  unsigned long long* s_acc = s_dyn;                                  // 6 per pair, exact extents
+  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * np);        // 1 per pair, by donor block
+  int* s_ext = reinterpret_cast<int*>(s_pc + np);                      // 6 per pair, FP32 bounds
+  __shared__ long long s_lbase[kMaxBlocks + 1];
+  __shared__ int s_coff[kMaxBlocks], s_nc[kMaxBlocks], s_toff[kMaxBlocks], s_lf[kMaxBlocks];
+  __shared__ int s_pf[kMaxBlocks + 1];  // pairs of donor block b: s_pc[s_pf[b] .. s_pf[b+1])
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 6 * np; i += blockDim.x) {
+    s_acc[i] = (i % 6 < 3) ? ~0ull : 0ull;
+    s_ext[i] = (i % 6 < 3) ? 0x7fffffff : (int)0x80000000;
+  }
+  for (int i = tid; i < np; i += blockDim.x) {
+    const PairInfo& P = pairs[p0 + i];
+    int rank = 0;  // position when sorted by donor block, ties by index
+    for (int k = 0; k < np; k++) {
+      const int dk = pairs[p0 + k].don;
+      rank += (dk < P.don) || (dk == P.don && k < i);
+    }
+    const Obb& R = bi[P.rec].obb;
+    const Obb& D = bi[P.don].obb;
+    PairCull q;
+    for (int k = 0; k < 3; k++) {
+      q.rxc[k] = R.xc[k];
+      q.dxc[k] = D.xc[k];
+      q.rdxc[k] = (float)R.dxc[k];
+      for (int j = 0; j < 3; j++) {
+        q.rvec[3 * j + k] = (float)R.vec[j][k];
+        q.dvec[3 * j + k] = (float)D.vec[j][k];
       }
     }
-    for (int p = 0; p < npairs; p++) {
-      const int don = pairs[p].don;
-      bool ov = false;
-      double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
-      if (valid && b == don) {
-        const Obb& R = bi[pairs[p].rec].obb;
-        // centre/half-size bound of the vertex projections onto R's axes
-        bool maybe = true;
-        for (int jx = 0; jx < 3 && maybe; jx++) {
-          double cp = 0, rad = 0;
-          for (int k = 0; k < 3; k++) {
-            cp += (0.5 * (lo[k] + hi[k]) - R.xc[k]) * R.vec[jx][k];
-            rad += 0.5 * (hi[k] - lo[k]) * fabs(R.vec[jx][k]);
+    q.don = P.don;
+    q.pair = p0 + i;
+    s_pc[rank] = q;
+  }
+  for (int b = tid; b <= nb; b += blockDim.x) {
+    int cnt = 0;
+    for (int k = 0; k < np; k++) cnt += pairs[p0 + k].don < b;
+    s_pf[b] = cnt;
+    if (b < nb) {
+      s_lbase[b] = bi[b].leaf_base;
+      s_coff[b] = bi[b].cell_off;
+      s_nc[b] = bi[b].ncells;
+      s_toff[b] = bi[b].tree_off;
+      s_lf[b] = bi[b].leaf_first;
+    }
+  }
+  if (tid == 0) s_lbase[nb] = nleaf_total;
+  __syncthreads();
+  volatile int* v_ext = s_ext;
+  const int lane = tid & 31;
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + tid) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;  // cells per leaf, leaves per warp
+  for (long long base = LPW * warp0; base < nleaf_total; base += LPW * nwarps) {
+    const long long leaf = base + lane / LC;
+    const bool leaf_ok = leaf < nleaf_total;
+    int b = 0;
+    if (leaf_ok)
+      while (b + 1 < nb && leaf >= s_lbase[b + 1]) b++;
+    const long long j = LC * (leaf - s_lbase[b]) + lane % LC;
+    const bool valid = leaf_ok && j < s_nc[b];
+    const long long c = (long long)s_coff[b] + j;
+    int nv = 0;
+    float fb[6];  // FP32 box, rounded outward
+    double cc[3];  // box centre
+    float hh[3];   // half sizes, rounded up
+    if constexpr (F64) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      if (valid) {
+        nv = cell_nv[c];
+        const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+        const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+        const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          if (m < nv) {
+            const double* v = x + 3 * (long long)cv[m];
+            for (int k = 0; k < 3; k++) {
+              const double t = v[k];
+              lo[k] = fmin(lo[k], t);
+              hi[k] = fmax(hi[k], t);
+            }
           }
-          const double slack = 1e-9 * (fabs(cp) + rad + R.dxc[jx]) + 1e-12;
-          if (cp - rad - slack > R.dxc[jx] || cp + rad + slack < -R.dxc[jx]) maybe = false;
         }
-        if (maybe) {
+      }
+      for (int k = 0; k < 3; k++) {
+        fb[k] = valid ? f_rd(lo[k]) : INFINITY;
+        fb[k + 3] = valid ? f_ru(hi[k]) : -INFINITY;
+        cc[k] = 0.5 * (lo[k] + hi[k]);
+        hh[k] = valid ? __double2float_ru(0.5 * (hi[k] - lo[k])) : 0.f;
+      }
+      if (write_boxes) {
+        if (valid) {
+          double* o = cbox64 + 6 * c;
+          o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
+          o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+        }
+        for (int o = 1; o < LC; o <<= 1)
+          for (int k = 0; k < 3; k++) {
+            lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+          }
+        const long long sl = tslot(s_toff[b], s_lf[b] + (leaf - s_lbase[b]));
+        if (leaf_ok && lane % LC == 0)
+          for (int k = 0; k < 3; k++) {
+            tnode64[6 * sl + k] = lo[k];
+            tnode64[6 * sl + k + 3] = hi[k];
+          }
+      }
+    } else {
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      if (valid) {
+        nv = cell_nv[c];
+        const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+        const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+        const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          if (m < nv) {
+            const float4 v = xf[cv[m]];
+            lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+            hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
+          }
+        }
+      }
+      for (int k = 0; k < 3; k++) {
+        fb[k] = valid ? f_down(lo[k]) : INFINITY;
+        fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
+        cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
+        hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
+      }
+    }
+    // leaf box: union over the LC lanes of the leaf
+    float f[6];
+    for (int k = 0; k < 6; k++) f[k] = fb[k];
+    for (int o = 1; o < LC; o <<= 1)
+      for (int k = 0; k < 3; k++) {
+        f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
+        f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
+      }
+    if (write_boxes) {
+      if (valid) {
+        cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
+        cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
+      }
+      const long long sl = tslot(s_toff[b], s_lf[b] + (leaf - s_lbase[b]));
+      if (leaf_ok && lane % LC == 0) {
+        tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
+        tnode[2 * sl + 1] = make_float4(f[4], f[5], 0.f, 0.f);
+      }
+    }
+    // The pairs of the leaf's block are s_pc[qa .. qb).  First every leaf
+    // tests its box against them, lane g of the leaf taking pairs qa+g,
+    // qa+g+LC, ...: a leaf clearly outside a receptor box is done with that
+    // pair; one clearly inside, whose projections cannot reach the current
+    // extents' bounds, tightens them and is done too.  The remaining
+    // (leaf, pair) combinations, bit q-qa of mixed, go cell by cell.
+    const bool leaf_live = leaf_ok && f[0] <= f[3];
+    const int qa = leaf_live ? s_pf[b] : 0, qb = leaf_live ? s_pf[b + 1] : 0;
+    const int g = lane % LC;
+    unsigned mixed = 0u;
+    {
+      const int nqw = __reduce_max_sync(0xffffffffu, qb - qa);
+      if (nqw > 32) {
+        mixed = 0xffffffffu;  // more pairs than mask bits: cell by cell
+      } else if (nqw > 0) {
+        double lc[3];
+        float lh[3], lsc = 0.f;
+        for (int k = 0; k < 3; k++) {
+          lc[k] = 0.5 * ((double)f[k] + (double)f[k + 3]);
+          lh[k] = leaf_live ? __fmul_ru(__fsub_ru(f[k + 3], f[k]), 0.5f) : 0.f;
+          lsc += leaf_live ? fabsf((float)lc[k]) : 0.f;
+        }
+        for (int r = 0; LC * r < nqw; r++) {
+          const int q = qa + g + LC * r;
+          if (q < qb) {
+            const PairCull& Q = s_pc[q];
+            float blo[3], bhi[3];
+            proj_bounds(lc, Q.rxc, Q.rvec, lh, lsc, Q.rdxc, blo, bhi);
+            bool out = false, inside = true;
+            for (int jx = 0; jx < 3; jx++) {
+              out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
+              inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
+            }
+            bool mix = !out && !inside;
+            if (inside) {
+              const float zero[3] = {0.f, 0.f, 0.f};
+              proj_bounds(lc, Q.dxc, Q.dvec, lh, lsc, zero, blo, bhi);
+              for (int jx = 0; jx < 3; jx++) {
+                const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+                const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
+                mix = mix || (kl <= umin) || (ku >= lmax);
+              }
+              if (!mix)
+                for (int jx = 0; jx < 3; jx++) {
+                  const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+                  if (ku < v_ext[6 * q + jx]) atomicMin(&s_ext[6 * q + jx], ku);
+                  if (kl > v_ext[6 * q + 3 + jx]) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+                }
+            }
+            if (mix) mixed |= 1u << (q - qa);
+          }
+        }
+        for (int o = 1; o < LC; o <<= 1) mixed |= __shfl_xor_sync(0xffffffffu, mixed, o);
+      }
+    }
+    float sh = 0.f, sc = 0.f;
+    for (int k = 0; k < 3; k++) {
+      sh += hh[k];
+      sc += valid ? fabsf((float)cc[k]) : 0.f;
+    }
+    const int q0 = __reduce_min_sync(0xffffffffu, (valid && mixed) ? qa : 0x7fffffff);
+    const int q1 = __reduce_max_sync(0xffffffffu, (valid && mixed) ? qb : 0);
+    for (int q = q0; q < q1; q++) {
+      const bool mine = valid && q >= qa && q < qb && ((mixed >> min(q - qa, 31)) & 1u);
+      if (!__any_sync(0xffffffffu, mine)) continue;
+      bool contrib = false;
+      double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+      if (mine) {
+        const PairCull& Q = s_pc[q];
+        float blo[3], bhi[3];
+        proj_bounds(cc, Q.rxc, Q.rvec, hh, sc, Q.rdxc, blo, bhi);
+        bool out = false, inside = true;
+        for (int jx = 0; jx < 3; jx++) {
+          out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
+          inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
+        }
+        bool ov = !out && inside;
+        if (!out && !inside) {  // across a face: the reference's test, MeshBlock.C:800-821
+          const Obb& R = bi[pairs[Q.pair].rec].obb;
           double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
           for (int m = 0; m < nv; m++) {
-            double xd[3];
+            const double* v = x + 3 * (long long)conn8[8 * c + m];
+            const double v0 = v[0], v1 = v[1], v2 = v[2];
             for (int jx = 0; jx < 3; jx++) {
-              xd[jx] = 0;
-              for (int k = 0; k < 3; k++) xd[jx] += (xv[m][k] - R.xc[k]) * R.vec[jx][k];
-            }
-            for (int jx = 0; jx < 3; jx++) {
-              bb[jx] = dmin(bb[jx], xd[jx]);
-              bb[jx + 3] = dmax(bb[jx + 3], xd[jx]);
+              double xd = 0;
+              xd += (v0 - R.xc[0]) * R.vec[jx][0];
+              xd += (v1 - R.xc[1]) * R.vec[jx][1];
+              xd += (v2 - R.xc[2]) * R.vec[jx][2];
+              bb[jx] = dmin(bb[jx], xd);
+              bb[jx + 3] = dmax(bb[jx + 3], xd);
             }
           }
           ov = true;
           for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx] > R.dxc[jx]);
           for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx + 3] < -R.dxc[jx]);
-          if (ov) {
-            const Obb& D = bi[don].obb;
-            for (int m = 0; m < nv; m++)
+        }
+        if (ov) {
+          const float zero[3] = {0.f, 0.f, 0.f};
+          proj_bounds(cc, Q.dxc, Q.dvec, hh, sc, zero, blo, bhi);
+          bool need = false;
+          for (int jx = 0; jx < 3; jx++) {
+            const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+            const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
+            need = need || (kl <= umin) || (ku >= lmax);
+            if (ku < umin) atomicMin(&s_ext[6 * q + jx], ku);
+            if (kl > lmax) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+          }
+          if (need) {  // the reference's projections, MeshBlock.C:822-833
+            const Obb& D = bi[Q.don].obb;
+            for (int m = 0; m < nv; m++) {
+              const double* v = x + 3 * (long long)conn8[8 * c + m];
+              const double v0 = v[0], v1 = v[1], v2 = v[2];
               for (int jx = 0; jx < 3; jx++) {
                 double xd = 0;
-                for (int k = 0; k < 3; k++) xd += (xv[m][k] - D.xc[k]) * D.vec[jx][k];
+                xd += (v0 - D.xc[0]) * D.vec[jx][0];
+                xd += (v1 - D.xc[1]) * D.vec[jx][1];
+                xd += (v2 - D.xc[2]) * D.vec[jx][2];
                 rlo[jx] = dmin(rlo[jx], xd);
                 rhi[jx] = dmax(rhi[jx], xd);
               }
+            }
+            contrib = true;
           }
         }
       }
-      if (__any_sync(0xffffffffu, ov)) {
+      if (__any_sync(0xffffffffu, contrib)) {
         for (int jx = 0; jx < 3; jx++)
           for (int o = 16; o > 0; o >>= 1) {
             rlo[jx] = dmin(rlo[jx], __shfl_xor_sync(0xffffffffu, rlo[jx], o));
@@ -396,23 +666,43 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
           }
         if (lane == 0)
           for (int jx = 0; jx < 3; jx++) {
-            atomicMin(&acc[6 * p + jx], dkey(rlo[jx]));
-            atomicMax(&acc[6 * p + jx + 3], dkey(rhi[jx]));
+            atomicMin(&s_acc[6 * q + jx], dkey(rlo[jx]));
+            atomicMax(&s_acc[6 * q + jx + 3], dkey(rhi[jx]));
           }
       }
     }
   }
+  __syncthreads();
+  for (int i = tid; i < 6 * np; i += blockDim.x) {
+    const unsigned long long v = s_acc[i];
+    unsigned long long* dst = &acc[6 * (long long)s_pc[i / 6].pair + i % 6];
+    if (i % 6 < 3) {
+      if (v != ~0ull) atomicMin(dst, v);
+    } else if (v != 0ull) {
+      atomicMax(dst, v);
+    }
+  }
+}
+
+void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
+                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
+                      long long nleaf_total, const PairInfo* pairs, int p0, int np, int write_boxes, float4* cbox,
+                      double* cbox64, float4* tnode, double* tnode64, unsigned long long* acc) {
+  if (f64)
+    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, nleaf_total, pairs, p0, np,
+                                               write_boxes, cbox, cbox64, tnode, tnode64, acc);
+  else
+    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, nleaf_total, pairs, p0, np,
+                                                write_boxes, cbox, cbox64, tnode, tnode64, acc);
 }
 
 // Level-by-level refit of the implicit trees: each CTA owns up to 256
-// consecutive nodes of one level of one block and builds the 8 levels above
-// them in shared memory.  Pass 0 starts from the leaves (unions of their
-// cells' boxes); pass p starts from the nodes pass p-1 wrote.
+// consecutive nodes of one level of one block and builds the 4 levels above
+// them in shared memory.  Pass 0 starts from the leaves the cell pass wrote;
+// pass p starts from the nodes pass p-1 wrote.
 
 __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict__ bi,
-                                                     const RefitGroup* __restrict__ groups, int pass0,
-                                                     const float4* __restrict__ cbox,
-                                                     const double* __restrict__ cbox64,
+                                                     const RefitGroup* __restrict__ groups,
                                                      float4* __restrict__ tnode, double* __restrict__ tnode64) {
   __shared__ float s32[256][6];
   __shared__ double s64[256][6];
@@ -424,36 +714,10 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
   if (t < width) {
     const long long node = level_first(L) + G.first + t;
     const long long sl = tslot(B.tree_off, node);
-    float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    double d[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
-    if (pass0) {
-      const long long j0 = (long long)(G.first + t) * B.leaf_cells;
-      const long long j1 = min(j0 + B.leaf_cells, (long long)B.ncells);
-      for (long long j = j0; j < j1; j++) {
-        const long long sidx = (long long)B.cell_off + j;
-        const float4 A = cbox[2 * sidx], C = cbox[2 * sidx + 1];
-        b[0] = fminf(b[0], A.x); b[1] = fminf(b[1], A.y); b[2] = fminf(b[2], A.z);
-        b[3] = fmaxf(b[3], A.w); b[4] = fmaxf(b[4], C.x); b[5] = fmaxf(b[5], C.y);
-        if (tnode64)
-          for (int k = 0; k < 3; k++) {
-            d[k] = dmin(d[k], cbox64[6 * sidx + k]);
-            d[k + 3] = dmax(d[k + 3], cbox64[6 * sidx + k + 3]);
-          }
-      }
-      tnode[2 * sl] = make_float4(b[0], b[1], b[2], b[3]);
-      tnode[2 * sl + 1] = make_float4(b[4], b[5], 0.f, 0.f);
-      if (tnode64)
-        for (int k = 0; k < 6; k++) tnode64[6 * sl + k] = d[k];
-    } else {
-      const float4 A = tnode[2 * sl], C = tnode[2 * sl + 1];
-      b[0] = A.x; b[1] = A.y; b[2] = A.z; b[3] = A.w; b[4] = C.x; b[5] = C.y;
-      if (tnode64)
-        for (int k = 0; k < 6; k++) d[k] = tnode64[6 * sl + k];
-    }
-    for (int k = 0; k < 6; k++) {
-      s32[t][k] = b[k];
-      s64[t][k] = d[k];
-    }
+    const float4 A = tnode[2 * sl], C = tnode[2 * sl + 1];
+    const float b[6] = {A.x, A.y, A.z, A.w, C.x, C.y};
+    for (int k = 0; k < 6; k++) s32[t][k] = b[k];
+    for (int k = 0; k < 6; k++) s64[t][k] = tnode64 ? tnode64[6 * sl + k] : 0.0;
   }
   __syncthreads();
   int n = width, lev = L;
@@ -492,29 +756,41 @@ __global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict
   }
 }
 
+// Empty boxes (lo = +inf, hi = -inf) in every tree node: the nodes that no
+// cell reaches keep them, so the traversal never enters them.
+__global__ void k_empty_boxes(float4* __restrict__ t, long long nnodes, double* __restrict__ t64) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nnodes;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (t) {
+      t[2 * i] = make_float4(INFINITY, INFINITY, INFINITY, -INFINITY);
+      t[2 * i + 1] = make_float4(-INFINITY, -INFINITY, 0.f, 0.f);
+    }
+    if (t64)
+      for (int k = 0; k < 6; k++) t64[6 * i + k] = (k < 3) ? 1e300 : -1e300;
+  }
+}
+
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
 // rounded outward), so the query gathering can skip tiles far from a region.
-__global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
+__global__ void __launch_bounds__(256) k_node_tiles(const float4* __restrict__ xf, const BlockInfo* __restrict__ bi,
                                                     int nb, const long long* __restrict__ tile_base,
                                                     float4* __restrict__ tbox, const int* __restrict__ node_order) {
-  __shared__ double sh[6][8];
+  __shared__ float sh[6][8];
   const long long T = blockIdx.x;
   int b = 0;
   while (b + 1 < nb && tile_base[b + 1] <= T) b++;
   const BlockInfo& B = bi[b];
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
-    const double* p = x + 3 * (long long)node_order[B.node_off + i];
-    for (int k = 0; k < 3; k++) {
-      lo[k] = dmin(lo[k], p[k]);
-      hi[k] = dmax(hi[k], p[k]);
-    }
+    const float4 v = xf[node_order[B.node_off + i]];
+    lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+    hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
   }
   for (int k = 0; k < 3; k++)
     for (int o = 16; o > 0; o >>= 1) {
-      lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
-      hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
     }
   const int w = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0)
@@ -526,11 +802,11 @@ __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x
   if (threadIdx.x == 0) {
     for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++)
       for (int k = 0; k < 3; k++) {
-        sh[k][0] = dmin(sh[k][0], sh[k][ww]);
-        sh[k + 3][0] = dmax(sh[k + 3][0], sh[k + 3][ww]);
+        sh[k][0] = fminf(sh[k][0], sh[k][ww]);
+        sh[k + 3][0] = fmaxf(sh[k + 3][0], sh[k + 3][ww]);
       }
-    tbox[2 * T] = make_float4(f_rd(sh[0][0]), f_rd(sh[1][0]), f_rd(sh[2][0]), f_ru(sh[3][0]));
-    tbox[2 * T + 1] = make_float4(f_ru(sh[4][0]), f_ru(sh[5][0]), 0.f, 0.f);
+    tbox[2 * T] = make_float4(f_down(sh[0][0]), f_down(sh[1][0]), f_down(sh[2][0]), f_up(sh[3][0]));
+    tbox[2 * T + 1] = make_float4(f_up(sh[4][0]), f_up(sh[5][0]), 0.f, 0.f);
   }
 }
 
