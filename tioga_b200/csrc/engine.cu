@@ -64,7 +64,7 @@ Engine::~Engine() {
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   for (auto& h : hm_state_) h.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
-  xf_.release();
+  xf_.release(); leaves_.release(); gparent_.release(); gnk_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
@@ -413,48 +413,125 @@ int Engine::build_tree_topology() {
     k1.release();
     v0.release();
   }
-  // one 4-ary tree per block: leaves of at most kMaxLeafCells consecutive
-  // cells in Morton order; node i of a block sits in slot tree_off + 3 + i
-  long long off = 0;
-  int maxdepth = 0;
-  nleaf_total_ = 0;
-  for (size_t b = 0; b < bi_.size(); b++) {
-    BlockInfo& B = bi_[b];
-    // leaves of kMaxLeafCells consecutive Morton cells, as many leaves as
-    // the cells need
-    int D = 0;
-    while ((1ll << (2 * D)) * kMaxLeafCells < (long long)B.ncells) D++;
-    B.depth = D;
-    B.leaf_first = (int)level_first(D);
-    B.leaf_cells = kMaxLeafCells;
-    B.nleaf = (B.ncells + kMaxLeafCells - 1) / kMaxLeafCells;
-    B.leaf_base = (int)nleaf_total_;
-    nleaf_total_ += B.nleaf;
-    B.tree_off = (int)off;
-    off += (3 + level_first(D + 1) + 3) / 4 * 4;
-    maxdepth = std::max(maxdepth, D);
-  }
-  tree_nodes_ = off;
-  // refit groups: pass p starts at depth D-4p of each block and climbs 4
-  // levels; only nodes with cells below them are refitted, the others keep
-  // the empty boxes written here once
-  std::vector<RefitGroup> groups;
-  refit_pass_off_.assign(1, 0);
-  for (int pass = 0; 4 * pass <= maxdepth; pass++) {
-    for (size_t b = 0; b < bi_.size(); b++) {
-      const int D = bi_[b].depth;
-      const int L = D - 4 * pass;
-      if (L < 0) continue;
-      if (pass > 0 && D - 4 * (pass - 1) <= 4) continue;  // the previous pass reached the root
-      const long long span = 1ll << (2 * (D - L));  // leaves under a node of level L
-      const long long width = (bi_[b].nleaf + span - 1) / span;
-      for (long long f = 0; f < width; f += 256) groups.push_back(RefitGroup{(int)b, L, (int)f});
+  // 4-ary radix tree per block over the sorted Morton keys (still in
+  // mkey_alt_), built level by level; group b holds block b's root
+  {
+    const int nb = (int)bi_.size();
+    long long gcap = std::max<long long>(2 * nb, ctot_ / 8 + 16);  // grows if needed
+    DBuf<int2> tlink, kids;
+    DBuf<int> ca, cb, cs, na, nbuf, ns, nk, isint, ioff, koff, leaf_at;
+    TB_CUDA(tlink.ensure(4 * gcap));
+    TB_CUDA(cudaMemsetAsync(tlink.p, 0, 4 * gcap * sizeof(int2), stream_));
+    TB_CUDA(gparent_.ensure(gcap));
+    TB_CUDA(gnk_.ensure(gcap));
+    TB_CUDA(leaf_at.ensure(ctot_));
+    TB_CUDA(cudaMemsetAsync(leaf_at.p, 0xff, ctot_ * sizeof(int), stream_));
+    std::vector<int> h_a, h_b, h_s, h_par(nb, -1), h_nk(nb, 1);
+    for (int b = 0; b < nb; b++) {
+      bi_[b].root = bi_[b].ncells > 0 ? 4 * b : -1;
+      if (bi_[b].ncells > 0) {
+        h_a.push_back(bi_[b].cell_off);
+        h_b.push_back(bi_[b].cell_off + bi_[b].ncells);
+        h_s.push_back(4 * b);
+      }
     }
-    refit_pass_off_.push_back((int)groups.size());
+    TB_CUDA(cudaMemcpyAsync(gparent_.p, h_par.data(), nb * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaMemcpyAsync(gnk_.p, h_nk.data(), nb * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    int n = (int)h_a.size();
+    TB_CUDA(ca.ensure(std::max(n, 1)));
+    TB_CUDA(cb.ensure(std::max(n, 1)));
+    TB_CUDA(cs.ensure(std::max(n, 1)));
+    TB_CUDA(cudaMemcpyAsync(ca.p, h_a.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaMemcpyAsync(cb.p, h_b.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaMemcpyAsync(cs.p, h_s.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));  // host staging vectors go out of scope level by level
+    long long g0 = nb;
+    int depth = 0;
+    level_groups_.assign(1, nb);
+    while (n > 0) {
+      TB_CUDA(kids.ensure(4 * (size_t)n));
+      TB_CUDA(nk.ensure(n + 1));
+      TB_CUDA(isint.ensure(n + 1));
+      TB_CUDA(ioff.ensure(n + 1));
+      TB_CUDA(koff.ensure(n + 1));
+      k_tree_split<<<grid_for(n, kT), kT, 0, stream_>>>(mkey_alt_.p, n, ca.p, cb.p, cs.p, kids.p, nk.p, isint.p,
+                                                        tlink.p, leaf_at.p);
+      TB_LAUNCHED("k_tree_split");
+      TB_CUDA(cudaMemsetAsync(nk.p + n, 0, sizeof(int), stream_));
+      TB_CUDA(cudaMemsetAsync(isint.p + n, 0, sizeof(int), stream_));
+      size_t tmp = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tmp, isint.p, ioff.p, n + 1, stream_);
+      TB_CUDA(cub_tmp_.ensure(tmp));
+      cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, isint.p, ioff.p, n + 1, stream_);
+      cub::DeviceScan::ExclusiveSum(nullptr, tmp, nk.p, koff.p, n + 1, stream_);
+      TB_CUDA(cub_tmp_.ensure(tmp));
+      cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, nk.p, koff.p, n + 1, stream_);
+      int nint = 0, nnext = 0;
+      TB_CUDA(cudaMemcpyAsync(&nint, ioff.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+      TB_CUDA(cudaMemcpyAsync(&nnext, koff.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+      TB_CUDA(cudaStreamSynchronize(stream_));
+      if (nint > 0 && depth >= kMaxTreeDepth) {  // the traversal keeps one entry per internal level
+        fprintf(stderr, "#tioga_b200: cell tree deeper than %d levels\n", kMaxTreeDepth);
+        return -1;
+      }
+      if (g0 + nint > gcap) {  // grow the per-slot and per-group tables, keeping their contents
+        const long long ncap = std::max(2 * gcap, g0 + nint);
+        DBuf<int2> t2;
+        DBuf<int> p2, k2;
+        TB_CUDA(t2.ensure(4 * ncap));
+        TB_CUDA(p2.ensure(ncap));
+        TB_CUDA(k2.ensure(ncap));
+        TB_CUDA(cudaMemsetAsync(t2.p, 0, 4 * ncap * sizeof(int2), stream_));
+        TB_CUDA(cudaMemcpyAsync(t2.p, tlink.p, 4 * gcap * sizeof(int2), cudaMemcpyDeviceToDevice, stream_));
+        TB_CUDA(cudaMemcpyAsync(p2.p, gparent_.p, gcap * sizeof(int), cudaMemcpyDeviceToDevice, stream_));
+        TB_CUDA(cudaMemcpyAsync(k2.p, gnk_.p, gcap * sizeof(int), cudaMemcpyDeviceToDevice, stream_));
+        TB_CUDA(cudaStreamSynchronize(stream_));
+        std::swap(tlink, t2);
+        std::swap(gparent_, p2);
+        std::swap(gnk_, k2);
+        gcap = ncap;
+      }
+      TB_CUDA(na.ensure(std::max(nnext, 1)));
+      TB_CUDA(nbuf.ensure(std::max(nnext, 1)));
+      TB_CUDA(ns.ensure(std::max(nnext, 1)));
+      k_tree_link<<<grid_for(n, kT), kT, 0, stream_>>>(n, cs.p, kids.p, nk.p, isint.p, ioff.p, koff.p, (int)g0,
+                                                       tlink.p, gparent_.p, gnk_.p, na.p, nbuf.p, ns.p);
+      TB_LAUNCHED("k_tree_link");
+      g0 += nint;
+      level_groups_.push_back((int)g0);
+      std::swap(ca, na);
+      std::swap(cb, nbuf);
+      std::swap(cs, ns);
+      n = nnext;
+      if (n > 0) depth++;
+    }
+    tree_depth_ = depth;
+    tree_nodes_ = 4 * g0;
+    TB_CUDA(tnode_.ensure(2 * tree_nodes_));
+    k_tree_init<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(tlink.p, tree_nodes_, tnode_.p);
+    TB_LAUNCHED("k_tree_init");
+    tnode64_empty_ = false;
+    // leaves in storage order
+    DBuf<int> flag, loff;
+    TB_CUDA(flag.ensure(ctot_ + 1));
+    TB_CUDA(loff.ensure(ctot_ + 1));
+    k_leaf_flags<<<grid_for(ctot_, kT), kT, 0, stream_>>>(leaf_at.p, ctot_, flag.p);
+    TB_LAUNCHED("k_leaf_flags");
+    TB_CUDA(cudaMemsetAsync(flag.p + ctot_, 0, sizeof(int), stream_));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag.p, loff.p, (int)(ctot_ + 1), stream_);
+    TB_CUDA(cub_tmp_.ensure(tmp));
+    cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, flag.p, loff.p, (int)(ctot_ + 1), stream_);
+    int nl = 0;
+    TB_CUDA(cudaMemcpyAsync(&nl, loff.p + ctot_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    nleaf_total_ = nl;
+    TB_CUDA(leaves_.ensure(std::max(nl, 1)));
+    k_leaf_list<<<grid_for(ctot_, kT), kT, 0, stream_>>>(leaf_at.p, loff.p, ctot_, tlink.p, cell_blk_.p,
+                                                         leaves_.p);
+    TB_LAUNCHED("k_leaf_list");
+    TB_CUDA(cudaStreamSynchronize(stream_));
   }
-  TB_CUDA(refit_groups_.ensure(groups.size()));
-  TB_CUDA(cudaMemcpyAsync(refit_groups_.p, groups.data(), groups.size() * sizeof(RefitGroup),
-                          cudaMemcpyHostToDevice, stream_));
   // query-gathering tiles of kNodeTile nodes per block
   h_tile_base_.assign(bi_.size() + 1, 0);
   for (size_t b = 0; b < bi_.size(); b++)
@@ -464,10 +541,6 @@ int Engine::build_tree_topology() {
                           cudaMemcpyHostToDevice, stream_));
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
   TB_CUDA(cbox_.ensure(2 * ctot_));
-  TB_CUDA(tnode_.ensure(2 * tree_nodes_));
-  k_empty_boxes<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(tnode_.p, tree_nodes_, nullptr);
-  TB_LAUNCHED("k_empty_boxes");
-  tnode64_empty_ = false;
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   return 0;
 }
@@ -655,8 +728,8 @@ int Engine::run_pairs_and_refit() {
     TB_CUDA(cbox64_.ensure(6 * ctot_));
     TB_CUDA(tnode64_.ensure(6 * tree_nodes_));
     if (!tnode64_empty_) {
-      k_empty_boxes<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(nullptr, tree_nodes_, tnode64_.p);
-      TB_LAUNCHED("k_empty_boxes");
+      k_tree_init64<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(tree_nodes_, tnode64_.p);
+      TB_LAUNCHED("k_tree_init64");
       tnode64_empty_ = true;
     }
   }
@@ -682,17 +755,19 @@ int Engine::run_pairs_and_refit() {
   for (int p0 = 0; p0 < npairs_; p0 += chunk) {
     const int np = std::min(chunk, npairs_ - p0);
     const size_t smem = (size_t)np * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
-    launch_cell_pass(fp64, grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3), smem, stream_, x_.p, xf_.p, conn8_.p,
-                     cell_nv_.p, d_bi_.p, nb, nleaf_total_, d_pairs_.p, p0, np, p0 == 0 ? 1 : 0, cbox_.p,
-                     fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, pair_acc_.p);
+    launch_cell_pass(fp64, grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3), smem, stream_, x_.p, xf_.p,
+                     conn8_.p, cell_nv_.p, d_bi_.p, nb, leaves_.p, nleaf_total_, d_pairs_.p, p0, np,
+                     p0 == 0 ? 1 : 0, cbox_.p, fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr,
+                     pair_acc_.p);
     TB_LAUNCHED("k_cell_pass");
   }
-  for (size_t pass = 0; pass + 1 < refit_pass_off_.size(); pass++) {
-    const int g0 = refit_pass_off_[pass], g1 = refit_pass_off_[pass + 1];
+  // internal nodes, deepest level first, from the leaves the cell pass wrote
+  for (int d = (int)level_groups_.size() - 2; d >= 0; d--) {
+    const int g0 = level_groups_[d], g1 = level_groups_[d + 1];
     if (g1 <= g0) continue;
-    k_tree_levels<<<g1 - g0, 256, 0, stream_>>>(d_bi_.p, refit_groups_.p + g0, tnode_.p,
-                                                fp64 ? tnode64_.p : nullptr);
-    TB_LAUNCHED("k_tree_levels");
+    k_refit_level<<<grid_for(g1 - g0, kT), kT, 0, stream_>>>(g0, g1, gparent_.p, tnode_.p,
+                                                             fp64 ? tnode64_.p : nullptr);
+    TB_LAUNCHED("k_refit_level");
   }
   if (h_tile_base_.back() > 0) {
     k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(xf_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,

@@ -20,7 +20,8 @@
 
 namespace tb {
 
-constexpr int kMaxLeafCells = 8; // cells per tree leaf (the last leaf of a block may hold fewer)
+constexpr int kMaxLeafCells = 8; // cells per tree leaf at most
+constexpr int kMaxTreeDepth = 32; // tree levels below the root at most (30-bit keys: 29 reachable)
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kSlots = 8;       // inline search candidates per query
 constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
@@ -57,12 +58,7 @@ struct BlockInfo {
   int nwbc, wall_off;  // wall nodes in the global wall list
   int nobc, obc_off;
   int nfringe;         // snapshot taken at preprocess (tioga.C:95-110)
-  int tree_off;        // first slot of the block's 4-ary tree in the node pool (multiple of 4)
-  int depth;           // leaves are at this depth (root = 0)
-  int leaf_first;      // heap index of the first leaf, (4^depth - 1) / 3
-  int leaf_cells;      // cells per leaf
-  int nleaf;           // leaves holding cells, ceil(ncells / leaf_cells)
-  int leaf_base;       // leaves of the blocks before this one
+  int root;            // slot of the block's tree root (4 * block), -1 without cells
   int has_user_res;
   Obb obb;
   float bb_lo[3], bb_hi[3];  // block box for the Morton keys
@@ -88,10 +84,6 @@ struct PairCull {
   int pair;       // index in the pair list
 };
 
-// one CTA of the level-by-level tree refit: up to 256 nodes of one level
-struct RefitGroup {
-  int block, level, first;
-};
 
 struct HoleMapInfo {
   int exist;
@@ -214,8 +206,6 @@ class Engine {
   bool search_timed_ = false;
   // tree refit and query tiles
   DBuf<int> inv_sorted_;
-  DBuf<RefitGroup> refit_groups_;
-  std::vector<int> refit_pass_off_;  // first group of each pass, plus the end
   DBuf<long long> tile_base_;
   std::vector<long long> h_tile_base_;
   DBuf<float4> tbox_;
@@ -251,9 +241,13 @@ class Engine {
   DBuf<float4> xf_;        // coordinates rounded to FP32, one per node
   DBuf<double> tnode64_;   // 6 per tree node (FP64 form)
   DBuf<double> cbox64_;    // 6 per sorted cell (FP64 form)
-  long long tree_nodes_ = 0;
-  long long nleaf_total_ = 0;    // leaves holding cells, all blocks
-  bool tnode64_empty_ = false;   // tnode64_ initialised to empty boxes for this topology
+  long long tree_nodes_ = 0;      // slots, four per group
+  long long nleaf_total_ = 0;     // leaves, all blocks
+  int tree_depth_ = 0;            // deepest level below a root
+  bool tnode64_empty_ = false;    // tnode64_ initialised to empty boxes for this topology
+  DBuf<int4> leaves_;             // (first cell, cells, slot, block), storage order
+  DBuf<int> gparent_, gnk_;      // per slot group: parent slot, children
+  std::vector<int> level_groups_; // groups of each depth's children: [level_groups_[d], level_groups_[d+1])
   // queries
   DBuf<int> qnode_, qdon_, qcell_;
   DBuf<double> qres_;

@@ -8,10 +8,6 @@
 
 namespace tb {
 
-// Node i of a block's 4-ary tree lives in slot tree_off + 3 + i, so the four
-// children 4n+1..4n+4 of any node share one aligned 128-byte line.
-__host__ __device__ __forceinline__ long long tslot(int tree_off, long long i) { return (long long)tree_off + 3 + i; }
-__host__ __device__ __forceinline__ long long level_first(int l) { return ((1ll << (2 * l)) - 1) / 3; }
 
 __device__ __forceinline__ void gather_vertices(const double* __restrict__ x, const int* __restrict__ cv,
                                                 int nv, double xv[8][3]) {
@@ -85,11 +81,21 @@ __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
                       const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
-                      long long nleaf_total, const PairInfo* pairs, int p0, int np, int write_boxes, float4* cbox,
-                      double* cbox64, float4* tnode, double* tnode64, unsigned long long* acc);
+                      const int4* leaves, long long nleaf_total, const PairInfo* pairs, int p0, int np,
+                      int write_boxes, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
+                      unsigned long long* acc);
 __global__ void k_round_nodes(const double* x, long long n, float4* xf);
-__global__ void k_tree_levels(const BlockInfo* bi, const RefitGroup* groups, float4* tnode, double* tnode64);
-__global__ void k_empty_boxes(float4* t, long long nnodes, double* t64);
+__global__ void k_tree_split(const unsigned long long* key, int n, const int* ca, const int* cb, const int* cslot,
+                             int2* kids, int* nk, int* isint, int2* tlink, int* leaf_at);
+__global__ void k_tree_link(int n, const int* cslot, const int2* kids, const int* nk, const int* isint,
+                            const int* ioff, const int* koff, int g0, int2* tlink, int* gparent, int* gnk, int* na,
+                            int* nb, int* nslot);
+__global__ void k_tree_init(const int2* tlink, long long nslots, float4* tnode);
+__global__ void k_tree_init64(long long nslots, double* t64);
+__global__ void k_leaf_flags(const int* leaf_at, long long ctot, int* flag);
+__global__ void k_leaf_list(const int* leaf_at, const int* loff, long long ctot, const int2* tlink,
+                            const unsigned char* cell_blk, int4* leaves);
+__global__ void k_refit_level(int g0, int g1, const int* gparent, float4* tnode, double* tnode64);
 __global__ void k_node_tiles(const float4* xf, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
 __global__ void k_morton_nodes(const double* x, const unsigned char* node_blk, const BlockInfo* bi,

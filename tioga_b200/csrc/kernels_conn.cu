@@ -378,15 +378,14 @@ template <bool F64>
 __global__ void __launch_bounds__(256, 3) k_cell_pass(
     const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
     const unsigned char* __restrict__ cell_nv,
-    const BlockInfo* __restrict__ bi, int nb, long long nleaf_total, const PairInfo* __restrict__ pairs, int p0,
-    int np, int write_boxes, float4* __restrict__ cbox, double* __restrict__ cbox64, float4* __restrict__ tnode,
-    double* __restrict__ tnode64, unsigned long long* __restrict__ acc) {
+    const BlockInfo* __restrict__ bi, int nb, const int4* __restrict__ leaves, long long nleaf_total,
+    const PairInfo* __restrict__ pairs, int p0, int np, int write_boxes, float4* __restrict__ cbox,
+    double* __restrict__ cbox64, float4* __restrict__ tnode, double* __restrict__ tnode64,
+    unsigned long long* __restrict__ acc) {
   extern __shared__ unsigned long long s_dyn[];
   unsigned long long* s_acc = s_dyn;                                  // 6 per pair, exact extents
   PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * np);        // 1 per pair, by donor block
   int* s_ext = reinterpret_cast<int*>(s_pc + np);                      // 6 per pair, FP32 bounds
-  __shared__ long long s_lbase[kMaxBlocks + 1];
-  __shared__ int s_coff[kMaxBlocks], s_nc[kMaxBlocks], s_toff[kMaxBlocks], s_lf[kMaxBlocks];
   __shared__ int s_pf[kMaxBlocks + 1];  // pairs of donor block b: s_pc[s_pf[b] .. s_pf[b+1])
   const int tid = threadIdx.x;
   for (int i = tid; i < 6 * np; i += blockDim.x) {
@@ -420,15 +419,7 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
     int cnt = 0;
     for (int k = 0; k < np; k++) cnt += pairs[p0 + k].don < b;
     s_pf[b] = cnt;
-    if (b < nb) {
-      s_lbase[b] = bi[b].leaf_base;
-      s_coff[b] = bi[b].cell_off;
-      s_nc[b] = bi[b].ncells;
-      s_toff[b] = bi[b].tree_off;
-      s_lf[b] = bi[b].leaf_first;
-    }
   }
-  if (tid == 0) s_lbase[nb] = nleaf_total;
   __syncthreads();
   volatile int* v_ext = s_ext;
   const int lane = tid & 31;
@@ -438,12 +429,11 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
   for (long long base = LPW * warp0; base < nleaf_total; base += LPW * nwarps) {
     const long long leaf = base + lane / LC;
     const bool leaf_ok = leaf < nleaf_total;
-    int b = 0;
-    if (leaf_ok)
-      while (b + 1 < nb && leaf >= s_lbase[b + 1]) b++;
-    const long long j = LC * (leaf - s_lbase[b]) + lane % LC;
-    const bool valid = leaf_ok && j < s_nc[b];
-    const long long c = (long long)s_coff[b] + j;
+    const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
+    const int b = L.w;
+    const bool valid = leaf_ok && lane % LC < L.y;
+    const long long c = (long long)L.x + lane % LC;
+    const long long sl = L.z;
     int nv = 0;
     float fb[6];  // FP32 box, rounded outward
     double cc[3];  // box centre
@@ -484,7 +474,6 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
             lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
             hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
           }
-        const long long sl = tslot(s_toff[b], s_lf[b] + (leaf - s_lbase[b]));
         if (leaf_ok && lane % LC == 0)
           for (int k = 0; k < 3; k++) {
             tnode64[6 * sl + k] = lo[k];
@@ -527,10 +516,9 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
         cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
         cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
       }
-      const long long sl = tslot(s_toff[b], s_lf[b] + (leaf - s_lbase[b]));
       if (leaf_ok && lane % LC == 0) {
         tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
-        tnode[2 * sl + 1] = make_float4(f[4], f[5], 0.f, 0.f);
+        *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
       }
     }
     // The pairs of the leaf's block are s_pc[qa .. qb).  First every leaf
@@ -686,88 +674,15 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
 
 void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
                       const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
-                      long long nleaf_total, const PairInfo* pairs, int p0, int np, int write_boxes, float4* cbox,
-                      double* cbox64, float4* tnode, double* tnode64, unsigned long long* acc) {
+                      const int4* leaves, long long nleaf_total, const PairInfo* pairs, int p0, int np,
+                      int write_boxes, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
+                      unsigned long long* acc) {
   if (f64)
-    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, nleaf_total, pairs, p0, np,
+    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, leaves, nleaf_total, pairs, p0, np,
                                                write_boxes, cbox, cbox64, tnode, tnode64, acc);
   else
-    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, nleaf_total, pairs, p0, np,
-                                                write_boxes, cbox, cbox64, tnode, tnode64, acc);
-}
-
-// Level-by-level refit of the implicit trees: each CTA owns up to 256
-// consecutive nodes of one level of one block and builds the 4 levels above
-// them in shared memory.  Pass 0 starts from the leaves the cell pass wrote;
-// pass p starts from the nodes pass p-1 wrote.
-
-__global__ void __launch_bounds__(256) k_tree_levels(const BlockInfo* __restrict__ bi,
-                                                     const RefitGroup* __restrict__ groups,
-                                                     float4* __restrict__ tnode, double* __restrict__ tnode64) {
-  __shared__ float s32[256][6];
-  __shared__ double s64[256][6];
-  const RefitGroup G = groups[blockIdx.x];
-  const BlockInfo& B = bi[G.block];
-  const int L = G.level;
-  const int width = (int)min(256ll, 1ll << (2 * L));
-  const int t = threadIdx.x;
-  if (t < width) {
-    const long long node = level_first(L) + G.first + t;
-    const long long sl = tslot(B.tree_off, node);
-    const float4 A = tnode[2 * sl], C = tnode[2 * sl + 1];
-    const float b[6] = {A.x, A.y, A.z, A.w, C.x, C.y};
-    for (int k = 0; k < 6; k++) s32[t][k] = b[k];
-    for (int k = 0; k < 6; k++) s64[t][k] = tnode64 ? tnode64[6 * sl + k] : 0.0;
-  }
-  __syncthreads();
-  int n = width, lev = L;
-  const int top = max(L - 4, 0);
-  while (lev > top) {
-    const int quarter = n >> 2;
-    float b[6];
-    double d[6];
-    if (t < quarter) {
-      for (int k = 0; k < 3; k++) {
-        b[k] = fminf(fminf(s32[4 * t][k], s32[4 * t + 1][k]), fminf(s32[4 * t + 2][k], s32[4 * t + 3][k]));
-        b[k + 3] = fmaxf(fmaxf(s32[4 * t][k + 3], s32[4 * t + 1][k + 3]),
-                         fmaxf(s32[4 * t + 2][k + 3], s32[4 * t + 3][k + 3]));
-        d[k] = dmin(dmin(s64[4 * t][k], s64[4 * t + 1][k]), dmin(s64[4 * t + 2][k], s64[4 * t + 3][k]));
-        d[k + 3] = dmax(dmax(s64[4 * t][k + 3], s64[4 * t + 1][k + 3]),
-                        dmax(s64[4 * t + 2][k + 3], s64[4 * t + 3][k + 3]));
-      }
-    }
-    __syncthreads();  // every group of four is read before any slot is overwritten
-    if (t < quarter) {
-      for (int k = 0; k < 6; k++) {
-        s32[t][k] = b[k];
-        s64[t][k] = d[k];
-      }
-      const int plev = lev - 1;
-      const long long node = level_first(plev) + (G.first >> (2 * (L - plev))) + t;
-      const long long sl = tslot(B.tree_off, node);
-      tnode[2 * sl] = make_float4(b[0], b[1], b[2], b[3]);
-      tnode[2 * sl + 1] = make_float4(b[4], b[5], 0.f, 0.f);
-      if (tnode64)
-        for (int k = 0; k < 6; k++) tnode64[6 * sl + k] = d[k];
-    }
-    __syncthreads();
-    n = quarter;
-    lev--;
-  }
-}
-
-// Empty boxes (lo = +inf, hi = -inf) in every tree node: the nodes that no
-// cell reaches keep them, so the traversal never enters them.
-__global__ void k_empty_boxes(float4* __restrict__ t, long long nnodes, double* __restrict__ t64) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nnodes;
-       i += (long long)gridDim.x * blockDim.x) {
-    if (t) {
-      t[2 * i] = make_float4(INFINITY, INFINITY, INFINITY, -INFINITY);
-      t[2 * i + 1] = make_float4(-INFINITY, -INFINITY, 0.f, 0.f);
-    }
-    if (t64)
-      for (int k = 0; k < 6; k++) t64[6 * i + k] = (k < 3) ? 1e300 : -1e300;
-  }
+    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, leaves, nleaf_total, pairs, p0,
+                                                np, write_boxes, cbox, cbox64, tnode, tnode64, acc);
 }
 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
@@ -1066,23 +981,34 @@ __device__ __forceinline__ bool hit64(const double* __restrict__ tn, long long s
          p[1] <= b[4] + kTol && p[2] <= b[5] + kTol;
 }
 
-// Depth-first walk of the 4-ary tree without a stack: the four children of a
-// node are tested together (one 128-byte line) and the hits not yet visited
-// are kept as a 4-bit mask per depth in `trail`.
+// FP32 node or cell box [A.xyz, (A.w, B.x, B.y)] against the point interval
+__device__ __forceinline__ bool hit_ab(const float4& A, const float4& B, const float* lo, const float* hi) {
+  return A.x <= hi[0] && A.y <= hi[1] && A.z <= hi[2] && A.w >= lo[0] && B.x >= lo[1] && B.y >= lo[2];
+}
+__device__ __forceinline__ int pick4(int k, int a0, int a1, int a2, int a3) {
+  return k == 0 ? a0 : (k == 1 ? a1 : (k == 2 ? a2 : a3));
+}
+
+// Depth-first walk of the donor block's radix tree.  Every step tests the
+// four slots of one child group (one 128-byte line) against the point; hit
+// leaves have their cells tested at once, the first hit internal child is
+// entered and the other hit ones are kept as a 4-bit mask for the current
+// depth in the trail (two 64-bit words, 32 depths), with the group's base
+// slot in shared memory.  The next node after a subtree is always in the
+// deepest non-empty mask.
 template <int FORM>
 __global__ void __launch_bounds__(256) k_traverse(
     const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
     int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf) {
+  __shared__ int s_base[kMaxTreeDepth][256];
+  const int t = threadIdx.x;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
     int n = 0;
     const int g = qnode[q];
-    const int a = qdon[q];
-    const int D = bi[a].depth, toff = bi[a].tree_off, coff = bi[a].cell_off, nc = bi[a].ncells;
-    const int Lc = bi[a].leaf_cells;
-    const long long leaf0 = bi[a].leaf_first;
+    const int root = bi[qdon[q]].root;
     double p[3];
     float plo[3], phi[3];  // the point widened by a margin that covers TOL and FP32 rounding
     p[0] = x[3 * (long long)g];
@@ -1095,64 +1021,78 @@ __global__ void __launch_bounds__(256) k_traverse(
       plo[k] = p32 - e;
       phi[k] = p32 + e;
     }
-    const bool root = (FORM == 0) ? hit64(tnode64, tslot(toff, 0), p) : hit32(tnode, tslot(toff, 0), plo, phi);
-    if (root) {
-      long long node = 0;
-      int depth = 0;
-      unsigned long long trail = 0;
-      for (;;) {
-        bool descended = false;
-        if (depth < D) {
-          const long long c0 = 4 * node + 1;
-          unsigned m = 0;
+    // cells [c0, c0 + nc) of a hit leaf
+    auto leaf_cells = [&](int c0, int ncell) {
+      for (int j = 0; j < ncell; j++) {
+        const int c = c0 + j;
+        bool pass;
+        if (FORM == 0) {
+          const double* bb = cbox64 + 6 * (long long)c;
+          const double lo[3] = {bb[0], bb[1], bb[2]}, hi[3] = {bb[3], bb[4], bb[5]};
+          pass = in_box64(p, lo, hi);
+        } else {
+          pass = hit_ab(cbox[2 * (long long)c], cbox[2 * (long long)c + 1], plo, phi);
+        }
+        if (pass) add_candidate((int)q, c, n, slots, ovf, ovf_cap, novf);
+      }
+    };
+    if (root >= 0) {
+      const float4 RA = tnode[2 * root], RB = tnode[2 * root + 1];
+      const bool rh = (FORM == 0) ? hit64(tnode64, root, p) : hit_ab(RA, RB, plo, phi);
+      const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
+      if (rh && rcnt > 0) leaf_cells(rlink, rcnt);
+      if (rh && rcnt < 0) {
+        int base = rlink, depth = 0;
+        unsigned long long tr0 = 0, tr1 = 0;  // masks of depths 0-15 and 16-31
+        for (;;) {
+          int lk[4], lc[4];
+          unsigned mi = 0, ml = 0;
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const bool h = (FORM == 0) ? hit64(tnode64, tslot(toff, c0 + k), p)
-                                       : hit32(tnode, tslot(toff, c0 + k), plo, phi);
-            m |= (unsigned)h << k;
-          }
-          if (m) {
-            const int c = __ffs(m) - 1;
-            m &= m - 1;
-            trail |= (unsigned long long)m << (4 * depth);
-            node = c0 + c;
-            depth++;
-            descended = true;
-          }
-        } else {
-          const long long j0 = (node - leaf0) * Lc;
-          const long long j1 = min(j0 + Lc, (long long)nc);
-          for (long long j = j0; j < j1; j++) {
-            const long long s = (long long)coff + j;
-            bool pass;
-            if (FORM == 0) {
-              const double* bb = cbox64 + 6 * s;
-              const double lo[3] = {bb[0], bb[1], bb[2]}, hi[3] = {bb[3], bb[4], bb[5]};
-              pass = in_box64(p, lo, hi);
-            } else {
-              pass = hit32(cbox, s, plo, phi);
+            const long long sl = base + k;
+            const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
+            lk[k] = __float_as_int(B.z);
+            lc[k] = __float_as_int(B.w);
+            const bool h = (FORM == 0) ? (lc[k] != 0 && hit64(tnode64, sl, p)) : hit_ab(A, B, plo, phi);
+            if (h) {
+              if (lc[k] > 0) ml |= 1u << k;
+              else mi |= 1u << k;
             }
-            if (pass) add_candidate((int)q, (int)s, n, slots, ovf, ovf_cap, novf);
           }
-        }
-        if (descended) continue;
-        // back up to the deepest node with children still to visit
-        bool more = false;
-        while (depth > 0) {
-          depth--;
-          node = (node - 1) >> 2;
-          unsigned m = (unsigned)(trail >> (4 * depth)) & 0xFu;
-          if (m) {
-            const int c = __ffs(m) - 1;
-            m &= m - 1;
-            trail = (trail & ~(0xFull << (4 * depth))) | ((unsigned long long)m << (4 * depth));
-            node = 4 * node + 1 + c;
+          while (ml) {
+            const int k = __ffs(ml) - 1;
+            ml &= ml - 1;
+            leaf_cells(pick4(k, lk[0], lk[1], lk[2], lk[3]), pick4(k, lc[0], lc[1], lc[2], lc[3]));
+          }
+          if (mi) {
+            const int c = __ffs(mi) - 1;
+            mi &= mi - 1;
+            if (mi) {
+              if (depth < 16) tr0 |= (unsigned long long)mi << (4 * depth);
+              else tr1 |= (unsigned long long)mi << (4 * (depth - 16));
+              s_base[depth][t] = base;
+            }
+            base = pick4(c, lk[0], lk[1], lk[2], lk[3]);
             depth++;
-            more = true;
+            continue;
+          }
+          int d2;
+          unsigned mm;
+          if (tr1) {
+            d2 = 16 + ((63 - __clzll((long long)tr1)) >> 2);
+            mm = (unsigned)(tr1 >> (4 * (d2 - 16))) & 0xFu;
+            tr1 &= ~(1ull << (4 * (d2 - 16) + __ffs(mm) - 1));
+          } else if (tr0) {
+            d2 = (63 - __clzll((long long)tr0)) >> 2;
+            mm = (unsigned)(tr0 >> (4 * d2)) & 0xFu;
+            tr0 &= ~(1ull << (4 * d2 + __ffs(mm) - 1));
+          } else {
             break;
           }
+          const long long sl = s_base[d2][t] + __ffs(mm) - 1;
+          base = __float_as_int(tnode[2 * sl + 1].z);
+          depth = d2 + 1;
         }
-        if (!more) break;
       }
     }
     ncand_q[q] = n;
