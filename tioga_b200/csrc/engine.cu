@@ -65,6 +65,7 @@ Engine::~Engine() {
   for (auto& h : hm_state_) h.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
   xf_.release(); leaves_.release(); gparent_.release(); gnk_.release();
+  mlist_.release(); cmlist_.release(); dcnt_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
@@ -614,6 +615,7 @@ int Engine::preprocess() {
   }
   TB_CUDA(cudaStreamSynchronize(stream_));
   preprocessed_ = true;
+  donor_rest_ = false;
   connected_ = false;
   interps_fetched_ = false;
   return 0;
@@ -719,6 +721,15 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(h_pairs_.data(), d_pairs_.p, (nb * nb + 1) * sizeof(PairInfo),
                           cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
+  // FP32 coordinates and the node tiles' boxes (query gathering, hole search)
+  TB_CUDA(xf_.ensure(ntot_));
+  k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
+  TB_LAUNCHED("k_round_nodes");
+  if (h_tile_base_.back() > 0) {
+    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(xf_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
+                                                                      node_order_.p);
+    TB_LAUNCHED("k_node_tiles");
+  }
   if (npairs_ == 0) return 0;
   // refit to the current coordinates: one pass over the cells (tree-order
   // cell boxes + reduced boxes of every pair), then the tree levels, then the
@@ -746,9 +757,6 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  TB_CUDA(xf_.ensure(ntot_));
-  k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
-  TB_LAUNCHED("k_round_nodes");
   // pairs in chunks that fit one CTA's shared memory; the first launch also
   // writes the cell and leaf boxes
   const int chunk = 256;
@@ -768,11 +776,6 @@ int Engine::run_pairs_and_refit() {
     k_refit_level<<<grid_for(g1 - g0, kT), kT, 0, stream_>>>(g0, g1, gparent_.p, tnode_.p,
                                                              fp64 ? tnode64_.p : nullptr);
     TB_LAUNCHED("k_refit_level");
-  }
-  if (h_tile_base_.back() > 0) {
-    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(xf_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
-                                                                      node_order_.p);
-    TB_LAUNCHED("k_node_tiles");
   }
   k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
   TB_LAUNCHED("k_pair_finish");
@@ -885,29 +888,69 @@ int Engine::run_search() {
   return 0;
 }
 
-int Engine::run_donors() {
-  // candidate slots: one per (receptor node, donor block)
+// Per-node donor state at rest: iblank 1 (set by preprocess), no marks, no
+// slots, every cell iblank 1.  Each call leaves it so (k_donor_reset at the
+// start undoes the previous call's holes, receptors and layers).
+int Engine::donor_rest_init() {
+  TB_CUDA(mlist_.ensure(ntot_));
+  TB_CUDA(cmlist_.ensure(ntot_));
+  TB_CUDA(dcnt_.ensure(8));
+  TB_CUDA(cudaMemsetAsync(dcnt_.p, 0, 8 * sizeof(int), stream_));
+  TB_CUDA(cudaMemsetAsync(m0_.p, 0, ntot_, stream_));
+  TB_CUDA(cudaMemsetAsync(m1_.p, 0, ntot_ * sizeof(int), stream_));
+  TB_CUDA(cudaMemsetAsync(cmark_.p, 0, ntot_ * sizeof(int), stream_));
   TB_CUDA(cudaMemsetAsync(slot_.p, 0xff, (size_t)ntot_ * K_ * sizeof(int), stream_));
+  k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(reset_t_.p, 0x7fffffff, ntot_);
+  TB_LAUNCHED("k_fill_int");
+  k_fill_int<<<grid_for(ctot_, kT), kT, 0, stream_>>>(iblank_cell_.p, 1, ctot_);
+  TB_LAUNCHED("k_fill_int");
+  prev_nrec_ = 0;
+  donor_rest_ = true;
+  return 0;
+}
+
+int Engine::run_donors() {
+  if (!donor_rest_) TB_TRY(donor_rest_init());
+  // undo the previous call's holes, receptors and layers
+  TB_CUDA(it_rec_.ensure(1));
+  TB_CUDA(it_cancel_.ensure(1));
+  k_donor_reset<<<148 * 16, kT, 0, stream_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p,
+                                                                   prev_nrec_, csr_off_.p, csr_cell_.p, iblank_.p,
+                                                                   m0_.p, m1_.p, iblank_cell_.p);
+  TB_LAUNCHED("k_donor_reset");
+  prev_nrec_ = 0;
+  TB_CUDA(cudaMemsetAsync(dcnt_.p, 0, 8 * sizeof(int), stream_));
+  // candidate slots: one per (receptor node, donor block)
   if (nq_ > 0) {
     k_fill_slots<<<grid_for(nq_, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, qcell_.p, nq_, K_, ntot_, ctot_,
                                                         slot_.p, err_.p);
     TB_LAUNCHED("k_fill_slots");
+    k_classify_queried<<<grid_for(nq_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, slot_.p, K_, qnode_.p,
+                                                              qcell_.p, nq_, qres_.p, d_hmdev_.p, nhm_, iblank_.p,
+                                                              node_res_.p, m0_.p, m1_.p, mlist_.p, dcnt_.p,
+                                                              counters_.p);
+    TB_LAUNCHED("k_classify_queried");
   }
-  k_process_donors<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, slot_.p, K_, qres_.p,
-                                                             d_hmdev_.p, nhm_, ntot_, iblank_.p, node_res_.p,
-                                                             m0_.p, m1_.p);
-  TB_LAUNCHED("k_process_donors");
+  if (nhm_ > 0 && h_tile_base_.back() > 0) {
+    k_classify_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(
+        x_.p, d_bi_.p, (int)hb_.size(), tile_base_.p, tbox_.p, node_order_.p, slot_.p, K_, d_hmdev_.p, nhm_,
+        iblank_.p, m0_.p, m1_.p, mlist_.p, dcnt_.p, counters_.p);
+    TB_LAUNCHED("k_classify_tiles");
+  }
+  // nfringe layers around the holes, then the layers' nodes become mandatory
+  k_front_init<<<1, 1, 0, stream_>>>(dcnt_.p);
+  TB_LAUNCHED("k_front_init");
   int maxfr = 0;
   for (auto& B : bi_) maxfr = std::max(maxfr, B.nfringe);
   for (int it = 0; it < maxfr; it++) {
-    k_dilate<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p, ctot_, it,
-                                                       m0_.p, m1_.p);
-    TB_LAUNCHED("k_dilate");
-    k_copy_u8<<<grid_for(ntot_, kT), kT, 0, stream_>>>(m1_.p, m0_.p, ntot_);
-    TB_LAUNCHED("k_copy_u8");
+    k_dilate_front<<<148 * 16, kT, 0, stream_>>>(it, csr_off_.p, csr_cell_.p, conn8_.p, cell_nv_.p, cell_blk_.p,
+                                                d_bi_.p, m0_.p, m1_.p, mlist_.p, dcnt_.p);
+    TB_LAUNCHED("k_dilate_front");
+    k_front_next<<<148 * 4, kT, 0, stream_>>>(it, m0_.p, mlist_.p, dcnt_.p);
+    TB_LAUNCHED("k_front_next");
   }
-  k_fringe_big<<<grid_for(ntot_, kT), kT, 0, stream_>>>(m1_.p, iblank_.p, ntot_, node_res_.p);
-  TB_LAUNCHED("k_fringe_big");
+  k_fringe_big_list<<<148 * 4, kT, 0, stream_>>>(mlist_.p, dcnt_.p, iblank_.p, node_res_.p);
+  TB_LAUNCHED("k_fringe_big_list");
   // fringe choice -> records keyed (donor block, receptor node)
   TB_CUDA(rcount_.ensure(2));
   TB_CUDA(cudaMemsetAsync(rcount_.p, 0, 2 * sizeof(int), stream_));
@@ -916,13 +959,15 @@ int Engine::run_donors() {
   TB_CUDA(rkey_alt_.ensure(rcap));
   TB_CUDA(rval_.ensure(rcap));
   TB_CUDA(rval_alt_.ensure(rcap));
-  k_select<<<grid_for(ntot_, kT), kT, 0, stream_>>>(node_blk_.p, d_bi_.p, slot_.p, K_, qcell_.p, cell_res_.p,
-                                                     ntot_, iblank_.p, node_res_.p, rkey_alt_.p, rval_alt_.p,
-                                                     rcount_.p, (int)rcap, err_.p);
-  TB_LAUNCHED("k_select");
   int R = 0;
-  TB_CUDA(cudaMemcpyAsync(&R, rcount_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (nq_ > 0) {
+    k_select<<<grid_for(nq_, kT), kT, 0, stream_>>>(node_blk_.p, d_bi_.p, slot_.p, K_, qnode_.p, qcell_.p, nq_,
+                                                    cell_res_.p, iblank_.p, node_res_.p, rkey_alt_.p, rval_alt_.p,
+                                                    rcount_.p, (int)rcap, err_.p);
+    TB_LAUNCHED("k_select");
+    TB_CUDA(cudaMemcpyAsync(&R, rcount_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+  }
   if (R > rcap) {  // cannot happen: one record per receptor node at most
     fprintf(stderr, "#tioga_b200: donor records overflowed their capacity\n");
     R = (int)rcap;
@@ -946,9 +991,6 @@ int Engine::run_donors() {
   TB_CUDA(it_nv_.ensure(std::max(R, 1)));
   TB_CUDA(it_cancel_.ensure(std::max(R, 1)));
   TB_CUDA(rres_.ensure(std::max(R, 1)));
-  TB_CUDA(cudaMemsetAsync(cmark_.p, 0, ntot_, stream_));
-  k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(reset_t_.p, 0x7fffffff, ntot_);
-  TB_LAUNCHED("k_fill_int");
   if (nq_ > 0) {
     k_fill_int<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, -1, nq_);
     TB_LAUNCHED("k_fill_int");
@@ -956,7 +998,7 @@ int Engine::run_donors() {
   if (R > 0) {
     k_interp_marks<<<grid_for(R, kT), kT, 0, stream_>>>(rkey_.p, rval_.p, rcount_.p, qcell_.p, conn8_.p,
                                                          cell_nv_.p, iblank_.p, node_res_.p, cmark_.p,
-                                                         reset_t_.p);
+                                                         reset_t_.p, cmlist_.p, dcnt_.p);
     TB_LAUNCHED("k_interp_marks");
     k_interp<<<grid_for(R, 128), 128, 0, stream_>>>(x_.p, rkey_.p, rval_.p, rcount_.p, qcell_.p, conn8_.p,
                                                      cell_nv_.p, node_blk_.p, d_bi_.p, iblank_.p, node_res_.p,
@@ -964,25 +1006,27 @@ int Engine::run_donors() {
                                                      it_don_.p,
                                                      it_nv_.p, it_cancel_.p, rres_.p, interp2rec_.p, err_.p);
     TB_LAUNCHED("k_interp");
-    k_cancel<<<grid_for(ntot_, kT), kT, 0, stream_>>>(cmark_.p, ntot_, slot_.p, K_, qcell_.p, cell_res_.p,
-                                                       interp2rec_.p, it_cancel_.p);
+    k_cancel<<<148 * 4, kT, 0, stream_>>>(cmlist_.p, dcnt_.p, slot_.p, K_, qcell_.p, cell_res_.p, interp2rec_.p,
+                                           it_cancel_.p);
     TB_LAUNCHED("k_cancel");
+    k_iblank_final<<<grid_for(R, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, iblank_.p,
+                                                        counters_.p);
+    TB_LAUNCHED("k_iblank_final");
   }
-  k_iblank_clear<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, ntot_);
-  TB_LAUNCHED("k_iblank_clear");
-  if (R > 0) {
-    k_iblank_set<<<grid_for(R, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, iblank_.p);
-    TB_LAUNCHED("k_iblank_set");
-  }
+  prev_nrec_ = R;
+  // back to rest for the next call: slots, cancel marks
+  k_donor_clear<<<grid_for(std::max<long long>(nq_, 1), kT), kT, 0, stream_>>>(
+      qnode_.p, qdon_.p, qcell_.p, nq_, K_, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
+  TB_LAUNCHED("k_donor_clear");
   return 0;
 }
 
 int Engine::run_celliblank() {
-  k_cell_iblank<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, ctot_, iblank_.p, sorted_cell_.p,
-                                                          iblank_cell_.p);
-  TB_LAUNCHED("k_cell_iblank");
-  k_count_iblank<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, ntot_, counters_.p);
-  TB_LAUNCHED("k_count_iblank");
+  // cells around the holes and the final receptors (all others are 1)
+  k_cell_iblank_sparse<<<148 * 16, kT, 0, stream_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p, rcount_.p,
+                                                    csr_off_.p, csr_cell_.p, conn8_.p, cell_nv_.p, iblank_.p,
+                                                    iblank_cell_.p);
+  TB_LAUNCHED("k_cell_iblank_sparse");
   return 0;
 }
 
@@ -1034,14 +1078,13 @@ int Engine::connectivity() {
     TB_CUDA(cudaEventRecord(ev_[4], stream_));
     rc = run_search();
     if (rc) return rc;
-    TB_CUDA(cudaEventRecord(ev_[5], stream_));
-    rc = run_donors();
-    if (rc) return rc;
   } else {
     TB_CUDA(cudaEventRecord(ev_[4], stream_));
-    TB_CUDA(cudaEventRecord(ev_[5], stream_));
     TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
   }
+  TB_CUDA(cudaEventRecord(ev_[5], stream_));
+  rc = run_donors();
+  if (rc) return rc;
   TB_CUDA(cudaEventRecord(ev_[6], stream_));
   rc = run_celliblank();
   if (rc) return rc;

@@ -21,6 +21,11 @@
 namespace tb {
 
 constexpr int kMaxLeafCells = 8; // cells per tree leaf at most
+// device counters of the sparse donor phase (dcnt_)
+constexpr int kHoles = 0;        // holes, the first entries of the marked-node list
+constexpr int kMarked = 1;       // holes plus nfringe layers
+constexpr int kCancelMarks = 2;  // nodes marked for cancellation
+constexpr int kSeg = 4;          // two alternating frontier ranges of the marked list (4 ints)
 constexpr int kMaxTreeDepth = 32; // tree levels below the root at most (30-bit keys: 29 reachable)
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kSlots = 8;       // inline search candidates per query
@@ -175,6 +180,7 @@ class Engine {
   int run_queries();
   int run_search();
   int run_donors();
+  int donor_rest_init();
   int run_celliblank();
   int download_iblank();
   int fetch_interps();
@@ -224,7 +230,11 @@ class Engine {
   // flat device arrays
   DBuf<double> x_, node_res_, cell_res_;
   DBuf<int> iblank_, iblank_cell_, conn8_;
-  DBuf<unsigned char> node_blk_, cell_blk_, cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_, m1_, cmark_;
+  DBuf<unsigned char> node_blk_, cell_blk_, cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_;
+  DBuf<int> m1_, cmark_;            // nfringe marks and cancel marks (first marker wins an atomicExch)
+  DBuf<int> mlist_, cmlist_, dcnt_;  // marked nodes (holes first), cancel-marked nodes, their counters
+  int prev_nrec_ = 0;               // records of the previous call (their receptors are reset next call)
+  bool donor_rest_ = false;         // per-node donor state is in its rest state
   DBuf<int> wall_list_, obc_list_;
   DBuf<int> csr_off_, csr_cell_, deg_;
   DBuf<BlockInfo> d_bi_;

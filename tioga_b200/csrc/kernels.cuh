@@ -135,22 +135,31 @@ __global__ void k_search_finish(const unsigned long long* qkey, const unsigned* 
 // ---- donors (kernels_donor.cu) ----
 __global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
                              long long ntot, long long ctot, int* slot, unsigned* err);
-__global__ void k_process_donors(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
-                                 const int* slot, int K, const double* qres,
-                                 const HoleMapDev* hm, int nhm, long long ntot, int* iblank,
-                                 double* node_res, unsigned char* m0, unsigned char* m1);
-__global__ void k_dilate(const int* conn8, const unsigned char* cell_nv, const unsigned char* cell_blk,
-                         const BlockInfo* bi, long long ctot, int iter, const unsigned char* m0,
-                         unsigned char* m1);
-__global__ void k_fringe_big(const unsigned char* m1, const int* iblank, long long ntot, double* node_res);
+__global__ void k_donor_reset(const int* mlist, const int* dcnt, const int* it_rec, const unsigned char* it_cancel,
+                              int prev_R, const int* csr_off, const int* csr_cell, int* iblank, unsigned char* m0,
+                              int* m1, int* iblank_cell);
+__global__ void k_classify_queried(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
+                                   const int* slot, int K, const int* qnode, const int* qcell, long long nq,
+                                   const double* qres, const HoleMapDev* hm, int nhm, int* iblank, double* node_res,
+                                   unsigned char* m0, int* m1, int* mlist, int* dcnt, unsigned long long* counters);
+__global__ void k_classify_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
+                                 const float4* tbox, const int* node_order, const int* slot, int K,
+                                 const HoleMapDev* hm, int nhm, int* iblank, unsigned char* m0, int* m1, int* mlist,
+                                 int* dcnt, unsigned long long* counters);
+__global__ void k_front_init(int* dcnt);
+__global__ void k_dilate_front(int iter, const int* csr_off, const int* csr_cell, const int* conn8,
+                               const unsigned char* cell_nv, const unsigned char* cell_blk, const BlockInfo* bi,
+                               const unsigned char* m0, int* m1, int* mlist, int* dcnt);
+__global__ void k_front_next(int iter, unsigned char* m0, const int* mlist, int* dcnt);
+__global__ void k_fringe_big_list(const int* mlist, const int* dcnt, const int* iblank, double* node_res);
 __global__ void k_select(const unsigned char* node_blk, const BlockInfo* bi, const int* slot, int K,
-                         const int* qcell, const double* cell_res, long long ntot, int* iblank,
-                         const double* node_res, unsigned long long* rkey, int* rval, int* rcount,
-                         int rcap, unsigned* err);
+                         const int* qnode, const int* qcell, long long nq, const double* cell_res, int* iblank,
+                         const double* node_res, unsigned long long* rkey, int* rval, int* rcount, int rcap,
+                         unsigned* err);
 __global__ void k_interp_marks(const unsigned long long* rkey, const int* rval, const int* rcount,
                                const int* qcell, const int* conn8, const unsigned char* cell_nv,
-                               const int* iblank, const double* node_res, unsigned char* cmark,
-                               int* reset_t);
+                               const int* iblank, const double* node_res, int* cmark, int* reset_t, int* cmlist,
+                               int* dcnt);
 __global__ void k_interp(const double* x, const unsigned long long* rkey, const int* rval,
                          const int* rcount, const int* qcell, const int* conn8,
                          const unsigned char* cell_nv, const unsigned char* node_blk,
@@ -158,16 +167,17 @@ __global__ void k_interp(const double* x, const unsigned long long* rkey, const 
                          const int* reset_t, const int* orig_cell, int* it_node, double* it_w, int* it_rec,
                          int* it_don, unsigned char* it_nv, unsigned char* it_cancel, double* rres,
                          int* interp2rec, unsigned* err);
-__global__ void k_cancel(const unsigned char* cmark, long long ntot, const int* slot, int K,
-                         const int* qcell, const double* cell_res, const int* interp2rec,
-                         unsigned char* it_cancel);
-__global__ void k_iblank_clear(int* iblank, long long ntot);
-__global__ void k_iblank_set(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
-                             int* iblank);
-__global__ void k_cell_iblank(const int* conn8, const unsigned char* cell_nv, long long ctot,
-                              const int* iblank, const int* orig_cell, int* iblank_cell);
+__global__ void k_cancel(const int* cmlist, const int* dcnt, const int* slot, int K, const int* qcell,
+                         const double* cell_res, const int* interp2rec, unsigned char* it_cancel);
+__global__ void k_iblank_final(const int* it_rec, const unsigned char* it_cancel, const int* rcount, int* iblank,
+                               unsigned long long* counters);
+__global__ void k_donor_clear(const int* qnode, const int* qdon, const int* qcell, long long nq, int K, int* slot,
+                              const int* cmlist, const int* dcnt, int* cmark, int* reset_t);
+__global__ void k_cell_iblank_sparse(const int* mlist, const int* dcnt, const int* it_rec,
+                                     const unsigned char* it_cancel, const int* rcount, const int* csr_off,
+                                     const int* csr_cell, const int* conn8, const unsigned char* cell_nv,
+                                     const int* iblank, int* iblank_cell);
 __global__ void k_gather_cells_i32(const int* src, const int* inv, long long base, int n, int* out);
-__global__ void k_count_iblank(const int* iblank, long long ntot, unsigned long long* counters);
 __global__ void k_interp_gather(const int* it_node, const double* it_w, const int* it_don,
                                 const unsigned char* it_nv, const unsigned char* it_cancel,
                                 const int* rcount, const BlockInfo* bi, const double* q, int nvar,

@@ -55,93 +55,233 @@ __global__ void k_fill_slots(const int* __restrict__ qnode, const int* __restric
   }
 }
 
-// processDonors first pass (bookKeeping.C:158-237): holes from the hole maps
-// of wall-bearing meshes that supplied no donor, node resolution raised to
-// the candidates' receptor resolutions.
-__global__ void k_process_donors(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
-                                 const BlockInfo* __restrict__ bi, const int* __restrict__ slot, int K,
-                                 const double* __restrict__ qres, const HoleMapDev* __restrict__ hm, int nhm,
-                                 long long ntot, int* __restrict__ iblank, double* __restrict__ node_res,
-                                 unsigned char* __restrict__ m0, unsigned char* __restrict__ m1) {
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
-       g += (long long)gridDim.x * blockDim.x) {
-    const int b = node_blk[g];
-    const int tag = bi[b].tag;
+// ---------------------------------------------------------------------------
+// Sparse donor phase.  Only a small part of the nodes is ever touched: the
+// queried nodes with a donor, the nodes inside a foreign wall mesh's hole
+// map, the nfringe layers around the holes and the donor cells' vertices.
+// Every per-node state array (iblank, m0/m1, slot, cmark, reset_t) is kept in
+// its rest state between calls, and each call undoes exactly what the
+// previous one marked, from its lists.  mlist holds the holes first
+// (dcnt[kHoles] of them) and then the nfringe layers (dcnt[kMarked] in all).
+// ---------------------------------------------------------------------------
+
+// first donor block with a candidate for node g is the node's owner query
+__device__ __forceinline__ bool owner_query(const int* __restrict__ slot, int K, long long g, int q) {
+  for (int a = 0; a < K; a++) {
+    const int s = slot[g * K + a];
+    if (s >= 0) return s == q;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mark_hole(int g, int* __restrict__ iblank, unsigned char* __restrict__ m0,
+                                          int* __restrict__ m1, int* __restrict__ mlist, int* __restrict__ dcnt,
+                                          unsigned long long* __restrict__ counters) {
+  iblank[g] = 0;
+  m0[g] = 1;
+  m1[g] = 1;
+  mlist[atomicAdd(&dcnt[kMarked], 1)] = g;
+  atomicAdd(&counters[4], 1ull);
+}
+
+// Start of a call: back to the rest state from the previous call's lists
+// (holes and kept receptors -> iblank 1 and their cells' iblank 1; marked
+// nodes -> m0 = m1 = 0).  prev_R records of the previous call.
+__global__ void k_donor_reset(const int* __restrict__ mlist, const int* __restrict__ dcnt,
+                              const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                              int prev_R, const int* __restrict__ csr_off, const int* __restrict__ csr_cell,
+                              int* __restrict__ iblank, unsigned char* __restrict__ m0, int* __restrict__ m1,
+                              int* __restrict__ iblank_cell) {
+  const int nh = dcnt[kHoles], nm = dcnt[kMarked];
+  const int n = max(nm, nh + prev_R);
+  const int lane = threadIdx.x & 31;  // a warp per entry, its lanes over the node's cells
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    if (i < nm && lane == 0) {
+      m0[mlist[i]] = 0;
+      m1[mlist[i]] = 0;
+    }
+    int v = -1;  // a node that ended the previous call with iblank 0 or -1
+    if (i < nh) v = mlist[i];
+    else if (i < nh + prev_R && !it_cancel[i - nh]) v = it_rec[i - nh];
+    if (v < 0) continue;
+    if (lane == 0) iblank[v] = 1;
+    for (int k = csr_off[v] + lane; k < csr_off[v + 1]; k += 32) iblank_cell[csr_cell[k]] = 1;
+  }
+}
+
+// processDonors first pass (bookKeeping.C:158-237) for the queried nodes that
+// have donors: holes from the hole maps of wall-bearing meshes that supplied
+// none of them, node resolution raised to the candidates' receptor
+// resolutions.  One thread per node (its owner query).
+__global__ void k_classify_queried(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+                                   const BlockInfo* __restrict__ bi, const int* __restrict__ slot, int K,
+                                   const int* __restrict__ qnode, const int* __restrict__ qcell, long long nq,
+                                   const double* __restrict__ qres, const HoleMapDev* __restrict__ hm, int nhm,
+                                   int* __restrict__ iblank, double* __restrict__ node_res,
+                                   unsigned char* __restrict__ m0, int* __restrict__ m1, int* __restrict__ mlist,
+                                   int* __restrict__ dcnt, unsigned long long* __restrict__ counters) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (qcell[q] < 0) continue;
+    const int g = qnode[q];
+    if (!owner_query(slot, K, g, (int)q)) continue;
+    const int tag = bi[node_blk[g]].tag;
     unsigned long long seen[2] = {0ull, 0ull};
-    int ncand = 0;
     double nres = node_res[g];
     for (int a = 0; a < K; a++) {
-      int q = slot[g * K + a];
-      if (q < 0) continue;
-      ncand++;
-      int t = bi[a].tag - 1;
+      const int s = slot[(long long)g * K + a];
+      if (s < 0) continue;
+      const int t = bi[a].tag - 1;
       seen[t >> 6] |= 1ull << (t & 63);
-      nres = dmax(nres, qres[q]);
+      nres = dmax(nres, qres[s]);
     }
-    int ib = 1;
-    const double p[3] = {x[3 * g], x[3 * g + 1], x[3 * g + 2]};
-    for (int h = 0; h < nhm; h++) {
-      const HoleMapDev& H = hm[h];
-      int ht = H.tagidx;
-      if (ht == tag - 1) continue;
-      if (ncand > 0 && ((seen[ht >> 6] >> (ht & 63)) & 1ull)) continue;
-      if (check_holemap(p, H)) {
-        ib = 0;
-        break;
-      }
+    const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
+    bool hole = false;
+    for (int h = 0; h < nhm && !hole; h++) {
+      const int ht = hm[h].tagidx;
+      if (ht == tag - 1 || ((seen[ht >> 6] >> (ht & 63)) & 1ull)) continue;
+      hole = check_holemap(p, hm[h]) != 0;
     }
-    iblank[g] = ib;
-    if (ncand > 0) node_res[g] = nres;
-    m0[g] = m1[g] = (ib == 0);
+    node_res[g] = nres;
+    if (hole) mark_hole(g, iblank, m0, m1, mlist, dcnt, counters);
   }
+}
+
+// The same pass for nodes without a donor: every foreign wall mesh's hole
+// map applies.  One CTA per tile of kNodeTile Morton-ordered nodes; only
+// tiles whose box meets a foreign hole map's reach are walked.  A point is
+// in a map only if it lies within one map cell beyond the map's extent (the
+// index truncates toward zero), so the reach is the extent widened by one
+// cell and rounded outward.
+__global__ void __launch_bounds__(256) k_classify_tiles(
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, int nb, const long long* __restrict__ tile_base,
+    const float4* __restrict__ tbox, const int* __restrict__ node_order, const int* __restrict__ slot, int K,
+    const HoleMapDev* __restrict__ hm, int nhm, int* __restrict__ iblank, unsigned char* __restrict__ m0,
+    int* __restrict__ m1, int* __restrict__ mlist, int* __restrict__ dcnt, unsigned long long* __restrict__ counters) {
+  __shared__ unsigned s_maps;  // foreign maps that reach the tile (bit h; all bits set past 32 maps)
+  const long long T = blockIdx.x;
+  int b = 0;
+  while (b + 1 < nb && tile_base[b + 1] <= T) b++;
+  const BlockInfo& B = bi[b];
+  if (threadIdx.x == 0) {
+    const float4 A = tbox[2 * T], C = tbox[2 * T + 1];
+    const float lo[3] = {A.x, A.y, A.z}, hi[3] = {A.w, C.x, C.y};
+    unsigned m = 0;
+    for (int h = 0; h < nhm; h++) {
+      if (hm[h].tagidx == B.tag - 1) continue;
+      bool meet = true;
+      for (int k = 0; k < 3; k++) {
+        const double dx = (hm[h].ext[k + 3] - hm[h].ext[k]) / hm[h].nx[k];
+        const double sl = 1e-6 * (fabs(hm[h].ext[k]) + fabs(hm[h].ext[k + 3]) + dx);
+        const float rlo = __double2float_rd(hm[h].ext[k] - dx - sl);
+        const float rhi = __double2float_ru(hm[h].ext[k + 3] + dx + sl);
+        meet = meet && !(hi[k] < rlo) && !(lo[k] > rhi);
+      }
+      if (meet) m |= (h < 32) ? (1u << h) : 0xffffffffu;
+    }
+    s_maps = m;
+  }
+  __syncthreads();
+  const unsigned maps = s_maps;
+  if (!maps) return;
+  const int t0 = (int)(T - tile_base[b]) * kNodeTile;
+  for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
+    const int g = node_order[B.node_off + i];
+    bool has = false;
+    for (int a = 0; a < K && !has; a++) has = slot[(long long)g * K + a] >= 0;
+    if (has) continue;  // classified with its owner query
+    const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
+    bool hole = false;
+    for (int h = 0; h < nhm && !hole; h++) {
+      if (h < 32 && !((maps >> h) & 1u)) continue;
+      if (hm[h].tagidx == B.tag - 1) continue;
+      hole = check_holemap(p, hm[h]) != 0;
+    }
+    if (hole) mark_hole(g, iblank, m0, m1, mlist, dcnt, counters);
+  }
+}
+
+// frontier bounds of the nfringe layers: seg[0..1] and seg[2..3] alternate
+__global__ void k_front_init(int* __restrict__ dcnt) {
+  dcnt[kHoles] = dcnt[kMarked];
+  dcnt[kSeg] = 0;
+  dcnt[kSeg + 1] = dcnt[kMarked];
 }
 
 // one nfringe layer (bookKeeping.C:250-271): every node of a cell that
-// touches the current layer joins the next one
-__global__ void k_dilate(const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-                         const unsigned char* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
-                         long long ctot, int iter, const unsigned char* __restrict__ m0,
-                         unsigned char* __restrict__ m1) {
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
-       c += (long long)gridDim.x * blockDim.x) {
-    if (iter >= bi[cell_blk[c]].nfringe) continue;
-    const int nv = cell_nv[c];
-    const int* cv = conn8 + 8 * c;
-    int hit = 0;
-    for (int m = 0; m < nv; m++) hit |= (m0[cv[m]] == 1);
-    if (!hit) continue;
-    for (int m = 0; m < nv; m++)
-      if (m0[cv[m]] != 1) m1[cv[m]] = 1;
+// touches the previous layer joins the next one.  Only cells around the
+// previous layer's new nodes can add nodes.
+__global__ void k_dilate_front(int iter, const int* __restrict__ csr_off, const int* __restrict__ csr_cell,
+                               const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+                               const unsigned char* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                               const unsigned char* __restrict__ m0, int* __restrict__ m1, int* __restrict__ mlist,
+                               int* __restrict__ dcnt) {
+  const int* seg = dcnt + kSeg + 2 * (iter & 1);
+  const int s0 = seg[0], s1 = seg[1];
+  const int lane = threadIdx.x & 31;  // a warp per frontier node, its lanes over the node's cells
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = s0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < s1; i += nw) {
+    const int u = mlist[i];
+    for (int k = csr_off[u] + lane; k < csr_off[u + 1]; k += 32) {
+      const int c = csr_cell[k];
+      if (iter >= bi[cell_blk[c]].nfringe) continue;
+      const int nv = cell_nv[c];
+      const int* cv = conn8 + 8 * (long long)c;
+      for (int m = 0; m < nv; m++) {
+        const int v = cv[m];
+        if (m0[v] != 1 && atomicExch(&m1[v], 1) == 0) mlist[atomicAdd(&dcnt[kMarked], 1)] = v;
+      }
+    }
   }
 }
 
-__global__ void k_fringe_big(const unsigned char* __restrict__ m1, const int* __restrict__ iblank,
-                             long long ntot, double* __restrict__ node_res) {
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
-       g += (long long)gridDim.x * blockDim.x)
-    if (m1[g] && iblank[g]) node_res[g] = kBig;
+// the new layer joins m0, and it is the next frontier
+__global__ void k_front_next(int iter, unsigned char* __restrict__ m0, const int* __restrict__ mlist,
+                             int* __restrict__ dcnt) {
+  const int* seg = dcnt + kSeg + 2 * (iter & 1);
+  const int s1 = seg[1], e = dcnt[kMarked];
+  for (int i = s1 + blockIdx.x * blockDim.x + threadIdx.x; i < e; i += gridDim.x * blockDim.x) m0[mlist[i]] = 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int* nseg = dcnt + kSeg + 2 * ((iter + 1) & 1);
+    nseg[0] = s1;
+    nseg[1] = e;
+  }
+}
+
+// fringe nodes that are not holes become mandatory receptors (nodeRes = BIG)
+__global__ void k_fringe_big_list(const int* __restrict__ mlist, const int* __restrict__ dcnt,
+                                  const int* __restrict__ iblank, double* __restrict__ node_res) {
+  const int nh = dcnt[kHoles], nm = dcnt[kMarked];
+  for (int i = nh + blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x) {
+    const int v = mlist[i];
+    if (iblank[v]) node_res[v] = kBig;
+  }
 }
 
 // fringe choice (bookKeeping.C:278-352): the first candidate in list order
 // that is finer than the node donates; the record is keyed by (donor block,
-// receptor node), which is the order the donor side processes them in.
+// receptor node), which is the order the donor side processes them in.  One
+// thread per node with donors (its owner query).
 __global__ void k_select(const unsigned char* __restrict__ node_blk, const BlockInfo* __restrict__ bi,
-                         const int* __restrict__ slot, int K, const int* __restrict__ qcell,
-                         const double* __restrict__ cell_res, long long ntot, int* __restrict__ iblank,
-                         const double* __restrict__ node_res, unsigned long long* __restrict__ rkey,
-                         int* __restrict__ rval, int* __restrict__ rcount, int rcap,
-                         unsigned* __restrict__ err) {
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
-       g += (long long)gridDim.x * blockDim.x) {
+                         const int* __restrict__ slot, int K, const int* __restrict__ qnode,
+                         const int* __restrict__ qcell, long long nq, const double* __restrict__ cell_res,
+                         int* __restrict__ iblank, const double* __restrict__ node_res,
+                         unsigned long long* __restrict__ rkey, int* __restrict__ rval, int* __restrict__ rcount,
+                         int rcap, unsigned* __restrict__ err) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (qcell[q] < 0) continue;
+    const int g = qnode[q];
+    if (!owner_query(slot, K, g, (int)q)) continue;
     if (iblank[g] == 0) continue;
     Cand L[kMaxK];
-    int n = donor_list(g, slot, K, qcell, cell_res, L);
-    if (n == 0) continue;
+    const int n = donor_list(g, slot, K, qcell, cell_res, L);
     const double nres = node_res[g];
     for (int k = 0; k < n; k++) {
       if (L[k].dres < nres) {
         iblank[g] = -bi[L[k].a].tag;
-        int r = atomicAdd(rcount, 1);
+        const int r = atomicAdd(rcount, 1);
         if (r >= rcap) {
           atomicOr(err, kErrCapacity);
           break;
@@ -162,7 +302,8 @@ __global__ void k_interp_marks(const unsigned long long* __restrict__ rkey, cons
                                const int* __restrict__ rcount, const int* __restrict__ qcell,
                                const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
                                const int* __restrict__ iblank, const double* __restrict__ node_res,
-                               unsigned char* __restrict__ cmark, int* __restrict__ reset_t) {
+                               int* __restrict__ cmark, int* __restrict__ reset_t, int* __restrict__ cmlist,
+                               int* __restrict__ dcnt) {
   const int R = *rcount;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
     const int g = (int)(rkey[r] & 0xffffffffull);
@@ -175,7 +316,7 @@ __global__ void k_interp_marks(const unsigned long long* __restrict__ rkey, cons
     for (int m = 0; m < nv; m++) {
       const int v = cv[m];
       if (iblank[v] <= 0 && node_res[v] != kBig) {
-        cmark[v] = 1;
+        if (atomicExch(&cmark[v], 1) == 0) cmlist[atomicAdd(&dcnt[kCancelMarks], 1)] = v;
         if (iblank[v] < 0) atomicMin(&reset_t[v], r);
       }
     }
@@ -250,53 +391,88 @@ __global__ void k_interp(const double* __restrict__ x, const unsigned long long*
 
 // getCancellationData + cancelDonor (bookKeeping.C:542-570): each marked
 // node cancels the interpolation of the head of its own donor list
-__global__ void k_cancel(const unsigned char* __restrict__ cmark, long long ntot, const int* __restrict__ slot,
+__global__ void k_cancel(const int* __restrict__ cmlist, const int* __restrict__ dcnt, const int* __restrict__ slot,
                          int K, const int* __restrict__ qcell, const double* __restrict__ cell_res,
                          const int* __restrict__ interp2rec, unsigned char* __restrict__ it_cancel) {
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < ntot;
-       v += (long long)gridDim.x * blockDim.x) {
-    if (!cmark[v]) continue;
+  const int n = dcnt[kCancelMarks];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = cmlist[i];
     Cand L[kMaxK];
-    int n = donor_list(v, slot, K, qcell, cell_res, L);
-    if (n == 0) continue;
-    int r = interp2rec[L[0].q];
+    const int nl = donor_list(v, slot, K, qcell, cell_res, L);
+    if (nl == 0) continue;
+    const int r = interp2rec[L[0].q];
     if (r >= 0) it_cancel[r] = 1;
   }
 }
 
-// clearIblanks + setIblanks (bookKeeping.C:615-648)
-__global__ void k_iblank_clear(int* __restrict__ iblank, long long ntot) {
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
-       g += (long long)gridDim.x * blockDim.x)
-    if (iblank[g] < 0) iblank[g] = 1;
+// clearIblanks + setIblanks (bookKeeping.C:615-648): the only negative
+// iblanks are the records' receptors (-meshtag); they end as -1, or 1 when
+// cancelled
+__global__ void k_iblank_final(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                               const int* __restrict__ rcount, int* __restrict__ iblank,
+                               unsigned long long* __restrict__ counters) {
+  const int R = *rcount;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    const bool keep = !it_cancel[r];
+    iblank[it_rec[r]] = keep ? -1 : 1;
+    if (keep) atomicAdd(&counters[5], 1ull);
+  }
 }
 
-__global__ void k_iblank_set(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
-                             const int* __restrict__ rcount, int* __restrict__ iblank) {
-  const int R = *rcount;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x)
-    if (!it_cancel[r]) iblank[it_rec[r]] = -1;
+// End of a call: back to the rest state for the next one (slots of the
+// queries with a donor, cancel marks and their reset times).
+__global__ void k_donor_clear(const int* __restrict__ qnode, const int* __restrict__ qdon,
+                              const int* __restrict__ qcell, long long nq, int K, int* __restrict__ slot,
+                              const int* __restrict__ cmlist, const int* __restrict__ dcnt, int* __restrict__ cmark,
+                              int* __restrict__ reset_t) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += stride)
+    if (qcell[q] >= 0) slot[(long long)qnode[q] * K + qdon[q]] = -1;
+  const int n = dcnt[kCancelMarks];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+    cmark[cmlist[i]] = 0;
+    reset_t[cmlist[i]] = 0x7fffffff;
+  }
 }
 
 // getCellIblanks (highOrder.C:88-150)
-__global__ void k_cell_iblank(const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-                              long long ctot, const int* __restrict__ iblank, const int* __restrict__ orig_cell,
-                              int* __restrict__ iblank_cell) {
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int nv = cell_nv[c];
-    const int* cv = conn8 + 8 * c;
-    int v = 1, flag = 1, ncount = 0;
-    for (int m = 0; m < nv && flag; m++) {
-      int ib = iblank[cv[m]];
-      if (ib == 0) {
-        v = 0;
-        flag = 0;
-      }
-      ncount += (ib == -1);
+__device__ __forceinline__ int cell_iblank_of(const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+                                              const int* __restrict__ iblank, long long c) {
+  const int nv = cell_nv[c];
+  const int* cv = conn8 + 8 * c;
+  int v = 1, flag = 1, ncount = 0;
+  for (int m = 0; m < nv && flag; m++) {
+    const int ib = iblank[cv[m]];
+    if (ib == 0) {
+      v = 0;
+      flag = 0;
     }
-    if (flag && ncount == nv) v = -1;
-    iblank_cell[c] = v;
+    ncount += (ib == -1);
+  }
+  if (flag && ncount == nv) v = -1;
+  return v;
+}
+
+// Only cells with a node whose iblank is not 1 can differ from 1: the cells
+// around the holes and the final receptors (every other cell is 1 already).
+__global__ void k_cell_iblank_sparse(const int* __restrict__ mlist, const int* __restrict__ dcnt,
+                                     const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                                     const int* __restrict__ rcount, const int* __restrict__ csr_off,
+                                     const int* __restrict__ csr_cell, const int* __restrict__ conn8,
+                                     const unsigned char* __restrict__ cell_nv, const int* __restrict__ iblank,
+                                     int* __restrict__ iblank_cell) {
+  const int nh = dcnt[kHoles], R = *rcount;
+  const int lane = threadIdx.x & 31;  // a warp per node, its lanes over the node's cells
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh + R; i += nw) {
+    int v;
+    if (i < nh) v = mlist[i];
+    else if (!it_cancel[i - nh]) v = it_rec[i - nh];
+    else continue;
+    for (int k = csr_off[v] + lane; k < csr_off[v + 1]; k += 32) {
+      const int c = csr_cell[k];
+      iblank_cell[c] = cell_iblank_of(conn8, cell_nv, iblank, c);
+    }
   }
 }
 
@@ -305,24 +481,6 @@ __global__ void k_gather_cells_i32(const int* __restrict__ src, const int* __res
                                    int n, int* __restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[i] = src[inv[base + i]];
-}
-
-__global__ void k_count_iblank(const int* __restrict__ iblank, long long ntot,
-                               unsigned long long* __restrict__ counters) {
-  unsigned long long h = 0, r = 0;
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
-       g += (long long)gridDim.x * blockDim.x) {
-    h += (iblank[g] == 0);
-    r += (iblank[g] < 0);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    h += __shfl_xor_sync(0xffffffffu, h, o);
-    r += __shfl_xor_sync(0xffffffffu, r, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&counters[4], h);
-    atomicAdd(&counters[5], r);
-  }
 }
 
 // ---------------------------------------------------------------------------
