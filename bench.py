@@ -47,6 +47,10 @@ WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherica
             "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
+# DRAM bytes (read + write) per cell of one cell-pass launch, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of this workload's
+# geometry at 161^3 / 49x49x97, scaled by the cell count; None until measured.
+CELL_PASS_DRAM_BYTES_PER_CELL = None
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
@@ -258,16 +262,22 @@ def run_gpu(args, ws, rank, local, dist):
         ms_e2e = float("nan")
     h2d = sum(24 * b.nnodes for b in system.blocks)
     d2h = sum(4 * b.nnodes for b in system.blocks)
-    # dominant kernel: the fused search (one launch per step)
-    search_ms = ph["search"]
-    alg_bytes = Q * 37 + st["ncand"] * 41 + st["cand_verts"] * 24
+    # Dominant kernel: the cell pass (one launch per step).  Its compulsory
+    # bytes: connectivity (4 B per vertex reference) and the cell type (1 B)
+    # read, each node's FP32 coordinates read once (16 B), every cell's box
+    # written (24 B), and per leaf its record read (16 B) and box written (24 B).
+    cell_ms = ph["cell_pass"]
+    nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
+    alg_bytes = 4 * nvsum + system.ncells * (1 + 24) + system.nnodes * 16 + st["nleaf"] * (16 + 24)
+    traffic = (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
+               else CELL_PASS_DRAM_BYTES_PER_CELL * system.ncells)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg_bytes / (search_ms * 1e-3) / 1e9
+    achieved = alg_bytes / (cell_ms * 1e-3) / 1e9
     out = {
         "metric": METRIC, "value": ws * Q / (ms_split * 1e-3), "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split, "higher_is_better": True,
@@ -287,9 +297,9 @@ def run_gpu(args, ws, rank, local, dist):
         "speedup_vs_plain": ms_plain / ms_split,
         "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
-        "roofline": {"kernel": "k_search (fused tree traversal + Newton containment)", "bound": "hbm",
+        "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "algorithmic_bytes": alg_bytes, "launch_ms": search_ms,
+                     "traffic": traffic, "algorithmic_bytes": alg_bytes, "launch_ms": cell_ms,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],

@@ -112,7 +112,7 @@ void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
  * a donor, [2] order-dependent ties, [3] Newton candidates, [4] FP64
  * refinements, [5] receptors, [6] holes, [7] donor records, [8] device
  * error bits, [9] pairs of blocks, [10] kernels launched by the library,
- * [11] sum of the candidates' vertex counts. */
+ * [11] sum of the candidates' vertex counts, [12] leaves of the cell trees. */
 void tioga_b200_stats_(long long out[16]);
 /* Run on the caller's CUDA stream (a cudaStream_t; NULL restores the
  * library's own stream), e.g. to time the calls with the caller's events. */
@@ -138,7 +138,8 @@ int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights,
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,
  * [8] total; inside the search: [9] traversal, [10] candidate screen,
- * [11] FP64 refinement. */
+ * [11] FP64 refinement; [12] the cell pass alone (cell and leaf boxes,
+ * reduced boxes), inside [2]. */
 void tioga_b200_timing_(float out[16]);
 
 #ifdef __cplusplus

@@ -216,6 +216,7 @@ void tioga_b200_stats_(long long out[16]) {
   out[9] = s.npairs;
   out[10] = s.launches;
   out[11] = s.cand_verts;
+  out[12] = s.nleaf;
 }
 
 void tioga_b200_set_stream_(void* stream) {
@@ -238,6 +239,7 @@ void tioga_b200_timing_(float out[16]) {
   out[9] = t.traverse;
   out[10] = t.candidates;
   out[11] = t.refine;
+  out[12] = t.cell_pass;
 }
 
 }  // extern "C"

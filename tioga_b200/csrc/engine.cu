@@ -51,12 +51,14 @@ Engine::Engine() {
   stream_ = own_stream_;
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : sev_) cudaEventCreate(&e);
+  for (auto& e : cev_) cudaEventCreate(&e);
 }
 
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& e : ev_) cudaEventDestroy(e);
   for (auto& e : sev_) cudaEventDestroy(e);
+  for (auto& e : cev_) cudaEventDestroy(e);
   x_.release(); node_res_.release(); cell_res_.release(); iblank_.release(); iblank_cell_.release();
   conn8_.release(); node_blk_.release(); cell_blk_.release(); cell_nv_.release(); wallf_.release();
   obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
@@ -757,6 +759,7 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaEventRecord(cev_[0], stream_));
   // pairs in chunks that fit one CTA's shared memory; the first launch also
   // writes the cell and leaf boxes
   const int chunk = 256;
@@ -769,6 +772,8 @@ int Engine::run_pairs_and_refit() {
                      pair_acc_.p);
     TB_LAUNCHED("k_cell_pass");
   }
+  TB_CUDA(cudaEventRecord(cev_[1], stream_));
+  cell_timed_ = true;
   // internal nodes, deepest level first, from the leaves the cell pass wrote
   for (int d = (int)level_groups_.size() - 2; d >= 0; d--) {
     const int g0 = level_groups_[d], g1 = level_groups_[d + 1];
@@ -1060,6 +1065,7 @@ int Engine::connectivity() {
   stats_ = Stats{};
   nlaunch_ = 0;
   search_timed_ = false;
+  cell_timed_ = false;
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   if (!coords_resident_) TB_TRY(upload_coords());
@@ -1106,6 +1112,7 @@ int Engine::connectivity() {
   stats_.nhole = (long long)cnt[4];
   stats_.nreceptor = (long long)cnt[5];
   stats_.nrecords = nrec_;
+  stats_.nleaf = nleaf_total_;
   stats_.npairs = npairs_;
   stats_.launches = nlaunch_;
   stats_.cand_verts = (long long)cnt[6];
@@ -1122,6 +1129,8 @@ int Engine::connectivity() {
   timing_.download = ms[8];
   cudaEventElapsedTime(&timing_.total, ev_[0], ev_[8]);
   timing_.traverse = timing_.candidates = timing_.refine = 0;
+  timing_.cell_pass = 0;
+  if (cell_timed_) cudaEventElapsedTime(&timing_.cell_pass, cev_[0], cev_[1]);
   if (search_timed_) {
     cudaEventElapsedTime(&timing_.traverse, sev_[0], sev_[1]);
     cudaEventElapsedTime(&timing_.candidates, sev_[1], sev_[2]);

@@ -122,6 +122,7 @@ struct Stats {
   long long nreceptor = 0;    // final iblank == -1
   long long nhole = 0;        // final iblank == 0
   long long nrecords = 0;     // chosen donors (before cancellation)
+  long long nleaf = 0;        // tree leaves (the cell pass's units of work, with the cells)
   long long npairs = 0;       // intersecting (receptor, donor) block pairs
   long long launches = 0;     // kernels this library launched in the call
   long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
@@ -132,6 +133,7 @@ struct Timing {
   float holemap = 0, boxes = 0, refit = 0, query = 0, search = 0, donors = 0, celliblank = 0,
         total = 0, upload = 0, download = 0;
   float traverse = 0, candidates = 0, refine = 0;  // stages of the search
+  float cell_pass = 0;                              // the cell pass kernel(s) alone
 };
 
 class Engine {
@@ -226,6 +228,8 @@ class Engine {
   long long nlaunch_ = 0;
   cudaEvent_t ev_[12];
   cudaEvent_t sev_[4];
+  cudaEvent_t cev_[2];  // around the cell pass
+  bool cell_timed_ = false;
 
   // flat device arrays
   DBuf<double> x_, node_res_, cell_res_;
