@@ -47,10 +47,11 @@ WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherica
             "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
-# DRAM bytes (read + write) per cell of one cell-pass launch, from an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum) of this workload's
-# geometry at 161^3 / 49x49x97, scaled by the cell count; None until measured.
-CELL_PASS_DRAM_BYTES_PER_CELL = None
+# DRAM bytes (read + write) of one cell-pass launch on the full workload, from
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of
+# `bench.py --forms split --steps 1 --warmup 1 --no-cpu-baseline`: 1,489,302,528
+# read + 959,081,984 written over 26,961,129 cells; other sizes scale by cells.
+CELL_PASS_DRAM_BYTES_PER_CELL = (1489302528 + 959081984) / 26961129
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "

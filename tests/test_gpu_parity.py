@@ -163,3 +163,62 @@ def test_query_count_matches_oracle(name, oracle_lib):
         assert counts["gpu"] == counts["oracle"], counts
     else:
         assert abs(counts["gpu"] - counts["oracle"]) <= 0.02 * counts["oracle"], counts
+
+
+def _two_calls(lib_path, system, shift, extras_fn, setup=None):
+    """preprocess, connectivity, move the last block by `shift` in the
+    caller's own coordinate array (the library reads it again), connectivity
+    again; returns iblanks, donor info and cell iblanks after each call."""
+    import copy
+    from tioga_b200.capi import TiogaLibrary
+    system = copy.deepcopy(system)  # the library keeps (and this moves) the caller's arrays
+    t = TiogaLibrary(lib_path)
+    t.init()
+    t.register_system(system)
+    if setup is not None:
+        setup(t)
+    t.preprocess_grids()
+    outs = []
+    for call in range(2):
+        if call == 1:
+            x = t.blocks[system.blocks[-1].tag]["x"].reshape(-1, 3)
+            x += np.asarray(shift)
+        t.performconnectivity()
+        out = {"iblank": {}, "donors": {}, "q": {}, "cells": {}}
+        for b in system.blocks:
+            out["iblank"][b.tag] = t.iblank(b.tag).copy()
+            out["donors"][b.tag] = t.getdonorinfo(b.tag)
+            cell = np.zeros(b.ncells, np.int32)
+            extras_fn(t.lib, b.tag, cell)
+            out["cells"][b.tag] = cell
+        outs.append(out)
+    t.delete()
+    return outs
+
+
+@pytest.mark.parametrize("name", ["cfg0-small", "cfg1-small"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_second_call_after_motion(name, precision, oracle_lib):
+    """A second connectivity call after the shell moved (no new preprocess,
+    as a solver between time steps) gives the reference's answer: the holes,
+    receptors and cell iblanks of the first call are undone and rebuilt."""
+    import ctypes as C
+    system = CASES[name]()
+    h = (system.blocks[0].x.max() - system.blocks[0].x.min()) / round(system.blocks[0].nnodes ** (1 / 3))
+    shift = (0.31 * h, -0.17 * h, 0.23 * h)  # a fraction of a background cell
+
+    def oracle_cells(lib, tag, out):
+        lib.tioga_oracle_getcelliblank(C.c_int(tag), out.ctypes.data_as(C.c_void_p))
+
+    def gpu_cells(lib, tag, out):
+        lib.tioga_b200_getcelliblank_(C.byref(C.c_int(tag)), out.ctypes.data_as(C.c_void_p))
+
+    ref = _two_calls(oracle_lib, system, shift, oracle_cells)
+    gpu = _two_calls(tb.library_path(), system, shift, gpu_cells, _gpu_setup(precision))
+    for call in range(2):
+        bad = diff_runs(system, ref[call], gpu[call])
+        assert not bad, (call, bad)
+        for b in system.blocks:
+            np.testing.assert_array_equal(gpu[call]["cells"][b.tag], ref[call]["cells"][b.tag])
+    moved = sum(int((ref[0]["iblank"][b.tag] != ref[1]["iblank"][b.tag]).sum()) for b in system.blocks)
+    assert moved > 0  # the motion changed the answer, so the second call is a real test
