@@ -32,12 +32,24 @@ def user_resolutions(system, seed):
     return {b.tag: (nres, cres)}
 
 
+def shell_resolutions(system, seed):
+    """Seeded user resolutions for every block but the first, spread widely
+    enough that coincident seam nodes differ and their merged (max)
+    resolution changes donor choices."""
+    rng = np.random.default_rng(seed)
+    return {b.tag: (rng.uniform(0.02, 0.6, b.nnodes), rng.uniform(0.02, 0.6, b.ncells))
+            for b in system.blocks[1:]}
+
+
 # name -> (system factory, settings, nvar, itype, field seed)
 CASES = {
     "cfg0_small_s0": (lambda: cases.small_config0(0), {}, 5, "row", 11),
     "cfg1_small_s1": (lambda: cases.small_config1(1), {}, 5, "row", 12),
     "cfg0_small_s1_opts": (lambda: cases.small_config0(1), dict(isym=0, nfringe=2, mexclude=1), 3, "column", 13),
     "cfg1_small_s2_userres": (lambda: cases.small_config1(2), "userres", 2, "row", 14),
+    # duplicated phi seams: coincident query points, merged by uniqNodesTree
+    "cfg1_small_s1_seam": (lambda: cases.small_config1_seam(1), {}, 5, "row", 15),
+    "cfg0_small_s2_seam_shellres": (lambda: cases.small_config0_seam(2), "shellres", 4, "row", 16),
 }
 
 
@@ -57,6 +69,8 @@ def settings_for(name, system):
     s = CASES[name][1]
     if s == "userres":
         return {"resolutions": user_resolutions(system, 99)}
+    if s == "shellres":
+        return {"resolutions": shell_resolutions(system, 98)}
     return dict(s)
 
 
@@ -87,7 +101,7 @@ if __name__ == "__main__":
     lib = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
     if not os.path.exists(lib):
         sys.exit("build the compiled reference first: make -C oracle ref")
-    for name in CASES:
+    for name in (sys.argv[1:] or CASES):
         system, q, out = run_case(lib, name)
         save(name, system, q, out)
         print(name, "saved")

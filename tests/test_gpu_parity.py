@@ -24,6 +24,8 @@ CASES = {
     "cfg1-small": lambda: cases.small_config1(1),
     "cfg1-small-seed3": lambda: cases.small_config1(3),
     "cfg0": lambda: cases.config0(0),
+    "cfg0-small-seam": lambda: cases.small_config0_seam(0),
+    "cfg1-small-seam": lambda: cases.small_config1_seam(1),
 }
 
 
@@ -51,6 +53,8 @@ def test_parity_with_oracle(name, precision, oracle_lib):
     assert st["nties"] == 0, st
     problems = diff_runs(system, ref, gpu)
     assert not problems, "\n".join(problems)
+    # the duplicated seams give coincident query points, which must be merged
+    assert (st["nmerged"] > 0) == name.endswith("seam"), st
 
 
 @pytest.mark.parametrize("itype", ["row", "column"])

@@ -129,11 +129,16 @@ def _radii(nr: int, r0: float, r1: float, ratio: float) -> np.ndarray:
 
 def sphere_shell(nr: int, nt: int, nphi: int, r0: float, r1: float,
                  ratio: float = 1.1, center=(0.0, 0.0, 0.0), perturb: float = 0.0,
-                 rng: np.random.Generator | None = None, split_layers: int = 0):
+                 rng: np.random.Generator | None = None, split_layers: int = 0,
+                 seam_copy: bool = False):
     """Structured spherical shell: nr radii x nt polar angles x nphi azimuths.
 
     Poles (t=0, t=nt-1) are single nodes per radius and phi=2*pi is the phi=0
-    seam, so the layer holds 2 + (nt-2)*(nphi-1) distinct nodes.  Cell vertex
+    seam, so the layer holds 2 + (nt-2)*(nphi-1) distinct nodes.  With
+    ``seam_copy`` the phi=2*pi side gets nodes of its own instead (an O-grid
+    with a duplicated seam, appended after each layer's nodes): each lies
+    within about 1e-16 of its phi=0 twin, so the twins are coincident query
+    points for a donor mesh.  Cell vertex
     order maps (u, v, w) to (r, theta, phi), a right-handed frame, so hex
     volumes are positive.  Cells of the first ``split_layers`` radial layers
     that do not touch a pole are split into 5 tets, 2 prisms or 3 pyramids,
@@ -167,12 +172,22 @@ def sphere_shell(nr: int, nt: int, nphi: int, r0: float, r1: float,
             T[sl] += rng.uniform(-perturb, perturb, cnt) * dth
             P[sl] += rng.uniform(-perturb, perturb, cnt) * dph
     c = np.asarray(center, dtype=np.float64)
+    nseam = (nt - 2) if seam_copy else 0
+    if seam_copy:  # the twin of every interior phi=0 node, at phi + 2*pi
+        lay = np.arange(nr * L).reshape(nr, L)
+        twin = lay[:, 1:1 + (nt - 2) * npl].reshape(nr, nt - 2, npl)[:, :, 0]
+        R = np.concatenate([R.reshape(nr, L), R[twin]], axis=1).ravel()
+        T = np.concatenate([T.reshape(nr, L), T[twin]], axis=1).ravel()
+        P = np.concatenate([P.reshape(nr, L), P[twin] + 2.0 * np.pi], axis=1).ravel()
+    Lx = L + nseam
     st = np.sin(T)
     x = np.stack([R * st * np.cos(P), R * st * np.sin(P), R * np.cos(T)], axis=1) + c
 
     def nid(i, t, p):
-        base = i * L
+        base = i * Lx
         out = base + 1 + (t - 1) * npl + (p % npl)
+        if seam_copy:
+            out = np.where(p == npl, base + L + (t - 1), out)
         out = np.where(t == 0, base, out)
         out = np.where(t == nt - 1, base + L - 1, out)
         return out.astype(np.int32)
@@ -182,8 +197,8 @@ def sphere_shell(nr: int, nt: int, nphi: int, r0: float, r1: float,
     v = [nid(i, t, p), nid(i + 1, t, p), nid(i + 1, t + 1, p), nid(i, t + 1, p),
          nid(i, t, p + 1), nid(i + 1, t, p + 1), nid(i + 1, t + 1, p + 1), nid(i, t + 1, p + 1)]
     hexes = np.stack(v, axis=1)
-    wall = np.arange(0, L, dtype=np.int32)
-    outer = np.arange((nr - 1) * L, nr * L, dtype=np.int32)
+    wall = np.arange(0, Lx, dtype=np.int32)
+    outer = np.arange((nr - 1) * Lx, nr * Lx, dtype=np.int32)
     kind = np.zeros(hexes.shape[0], dtype=np.int8)
     if split_layers <= 0:
         return x, [(NV_HEX, hexes)], wall, outer, kind
@@ -213,13 +228,14 @@ def _empty_i32():
 
 
 def config0(seed: int = 0, nbg: int = 65, nr: int = 33, nt: int = 33, nphi: int = 65,
-            perturb: float = 0.05) -> System:
+            perturb: float = 0.05, seam_copy: bool = False) -> System:
     """Plain all-hex case: 65^3 background box on [-5,5]^3 plus one shell
     (r 0.5 -> 2.0, radial ratio 1.1) at the origin; interior nodes jittered
     by +-5% of the local spacing."""
     rng = np.random.default_rng(seed)
     xb, cb = hex_box(nbg, -5.0, 5.0, perturb, rng)
-    xs, cs, wall, outer, _ = sphere_shell(nr, nt, nphi, 0.5, 2.0, 1.1, (0.0, 0.0, 0.0), perturb, rng)
+    xs, cs, wall, outer, _ = sphere_shell(nr, nt, nphi, 0.5, 2.0, 1.1, (0.0, 0.0, 0.0), perturb, rng,
+                                          seam_copy=seam_copy)
     bg = Block(1, xb, cb, _empty_i32(), _empty_i32(), name="background")
     sh = Block(2, xs, cs, wall, outer, name="shell")
     return System([bg, sh], name=f"cfg0(nbg={nbg},shell={nr}x{nt}x{nphi},seed={seed})",
@@ -251,7 +267,7 @@ def shell_centres(rng: np.random.Generator, nshell: int, rwall: np.ndarray, rout
 
 
 def config1(seed: int = 1, nbg: int = 257, nshell: int = 3, nr: int = 65, nt: int = 65,
-            nphi: int = 129, split_layers: int = 4) -> System:
+            nphi: int = 129, split_layers: int = 4, seam_copy: bool = False) -> System:
     """Mixed-element case: 257^3 background whose z<0 hexes are split into
     two prisms each, plus three shells (wall radius U(0.3,0.6), outer radius
     4x wall) at random centres within |x|<=3, 65x65x129 nodes each, whose
@@ -265,7 +281,7 @@ def config1(seed: int = 1, nbg: int = 257, nshell: int = 3, nr: int = 65, nt: in
     centres = shell_centres(rng, nshell, rwall, router)
     for s in range(nshell):
         xs, cs, wall, outer, _ = sphere_shell(nr, nt, nphi, rwall[s], router[s], 1.1,
-                                              centres[s], 0.0, rng, split_layers)
+                                              centres[s], 0.0, rng, split_layers, seam_copy)
         blocks.append(Block(2 + s, xs, cs, wall, outer, name=f"shell{s}"))
     return System(blocks, name=f"cfg1(nbg={nbg},{nshell}x{nr}x{nt}x{nphi},seed={seed})",
                   meta={"seed": seed, "centres": centres.tolist(), "rwall": rwall.tolist()})
@@ -296,6 +312,16 @@ CONFIGS = {
 def small_config0(seed: int = 0) -> System:
     """cfg0 geometry at test size (17^3 box, 9x9x17 shell)."""
     return config0(seed, nbg=17, nr=9, nt=9, nphi=17)
+
+
+def small_config0_seam(seed: int = 0) -> System:
+    """small_config0 with the shell's phi seam duplicated (coincident query points)."""
+    return config0(seed, nbg=17, nr=9, nt=9, nphi=17, seam_copy=True)
+
+
+def small_config1_seam(seed: int = 1) -> System:
+    """small_config1 with every shell's phi seam duplicated (coincident query points)."""
+    return config1(seed, nbg=33, nshell=3, nr=9, nt=9, nphi=17, split_layers=2, seam_copy=True)
 
 
 def small_config1(seed: int = 1) -> System:

@@ -217,6 +217,7 @@ void tioga_b200_stats_(long long out[16]) {
   out[10] = s.launches;
   out[11] = s.cand_verts;
   out[12] = s.nleaf;
+  out[13] = s.nmerged;
 }
 
 void tioga_b200_set_stream_(void* stream) {

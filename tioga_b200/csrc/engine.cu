@@ -67,7 +67,7 @@ Engine::~Engine() {
   for (auto& h : hm_state_) h.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
   xf_.release(); leaves_.release(); gparent_.release(); gnk_.release();
-  mlist_.release(); cmlist_.release(); dcnt_.release();
+  mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
@@ -573,6 +573,7 @@ int Engine::preprocess() {
     TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
                             stream_));
   }
+  TB_TRY(dedup_gate());
   for (size_t b = 0; b < hb_.size(); b++) {
     const HostBlock& H = hb_[b];
     if (!bi_[b].has_user_res) continue;
@@ -821,13 +822,14 @@ int Engine::run_queries() {
                                              node_order_.p);
     TB_LAUNCHED("k_query_write");
   }
+  dedup_ran_ = false;
+  if (dedup_active_ && nq > 0) TB_TRY(run_dedup(tiles_x));
   return 0;
 }
 
 // search in four stages: traversal -> candidate list -> one thread per
 // candidate (exact box test, FP32 screen) -> FP64 refinement -> outcome
 int Engine::run_search() {
-  TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
   TB_CUDA(scount_.ensure(2));
   TB_CUDA(cudaMemsetAsync(scount_.p, 0, 2 * sizeof(unsigned), stream_));
   ncand_ = 0;
@@ -889,7 +891,235 @@ int Engine::run_search() {
   k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, inv_sorted_.p, qcell_.p, qtie_.p,
                                                          counters_.p);
   TB_LAUNCHED("k_search_finish");
+  if (dedup_ran_) {  // merged coincident points take their representative's donor
+    k_dedup_copy<<<grid_for(nq_, kT), kT, 0, stream_>>>(q_rep_.p, nq_, qcell_.p, qtie_.p);
+    TB_LAUNCHED("k_dedup_copy");
+  }
   search_timed_ = true;
+  return 0;
+}
+
+// Coincident query points.  At preprocess: every node's OBB bin (the order in
+// which the reference lists a receptor block's query points) and whether any
+// block holds two nodes closer than the gate distance (a per-block grid of
+// 2^18 cells per axis, distance a quarter cell, never below 10 TOL).  Blocks
+// without such nodes cannot produce query points within TOL of each other,
+// and the per-call merge is skipped.  Nodes farther apart than the gate
+// distance at preprocess that later move within TOL of each other are not
+// merged until the next preprocess.
+int Engine::dedup_gate() {
+  dedup_active_ = false;
+  TB_CUDA(node_bin_.ensure(ntot_));
+  k_node_bins<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, node_bin_.p);
+  TB_LAUNCHED("k_node_bins");
+  DBuf<int> cnt, off, v0, v1;
+  DBuf<unsigned long long> k0, k1;
+  DBuf<unsigned> flag;
+  TB_CUDA(cnt.ensure(ntot_ + 1));
+  TB_CUDA(off.ensure(ntot_ + 1));
+  k_coin_count<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, cnt.p);
+  TB_LAUNCHED("k_coin_count");
+  TB_CUDA(cudaMemsetAsync(cnt.p + ntot_, 0, sizeof(int), stream_));
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, (int)(ntot_ + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, cnt.p, off.p, (int)(ntot_ + 1), stream_);
+  int total = 0;
+  TB_CUDA(cudaMemcpyAsync(&total, off.p + ntot_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (total < 2) return 0;
+  TB_CUDA(k0.ensure(total));
+  TB_CUDA(k1.ensure(total));
+  TB_CUDA(v0.ensure(total));
+  TB_CUDA(v1.ensure(total));
+  TB_CUDA(flag.ensure(1));
+  TB_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(unsigned), stream_));
+  k_coin_fill<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, off.p, k0.p, v0.p);
+  TB_LAUNCHED("k_coin_fill");
+  tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 62, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 62, stream_);
+  k_coin_check<<<grid_for(total, kT), kT, 0, stream_>>>(k1.p, v1.p, total, x_.p, node_blk_.p, d_bi_.p, flag.p);
+  TB_LAUNCHED("k_coin_check");
+  unsigned f = 0;
+  TB_CUDA(cudaMemcpyAsync(&f, flag.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  dedup_active_ = f != 0;
+  return 0;
+}
+
+// The per-call merge (uniqNodesTree): donor-list order, octree subsets level
+// by level, the pairwise loop per leaf, then xtag / representative / merged
+// resolution per query.
+int Engine::run_dedup(int tiles_x) {
+  const long long n = nq_;
+  const int np = npairs_;
+  // queries of pair p are [qoff[p], qoff[p+1]); rank of p among its donor's pairs
+  std::vector<int> h_toff((size_t)tiles_x * np + 1);
+  TB_CUDA(cudaMemcpyAsync(h_toff.data(), tile_off_.p, h_toff.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                          stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<int> qoff(np + 1), prank(np);
+  for (int p = 0; p < np; p++) qoff[p] = h_toff[(size_t)p * tiles_x];
+  qoff[np] = (int)n;
+  const int nb = (int)hb_.size();
+  std::vector<long long> dcount(nb, 0);
+  std::vector<int> seen(nb, 0);
+  for (int p = 0; p < np; p++) {
+    prank[p] = seen[h_pairs_[p].don]++;
+    dcount[h_pairs_[p].don] += qoff[p + 1] - qoff[p];
+  }
+  TB_CUDA(dd_pqoff_.ensure(np + 1));
+  TB_CUDA(dd_prank_.ensure(np));
+  TB_CUDA(cudaMemcpyAsync(dd_pqoff_.p, qoff.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaMemcpyAsync(dd_prank_.p, prank.data(), np * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(dd_key_.ensure(n));
+  TB_CUDA(dd_key2_.ensure(n));
+  TB_CUDA(dd_perm_.ensure(n));
+  TB_CUDA(dd_perm2_.ensure(n));
+  TB_CUDA(dd_refq_.ensure(n));
+  TB_CUDA(dd_x_.ensure(3 * n));
+  TB_CUDA(dd_mtag_.ensure(n));
+  TB_CUDA(dd_rtag_.ensure(n));
+  TB_CUDA(dd_itag_.ensure(n));
+  TB_CUDA(dd_seg_.ensure(n));
+  TB_CUDA(dd_oct_.ensure(n));
+  TB_CUDA(q_gpos_.ensure(n));
+  TB_CUDA(q_xt_.ensure(n));
+  TB_CUDA(q_rep_.ensure(n));
+  k_dedup_keys<<<grid_for(n, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, n, dd_pqoff_.p, np, dd_prank_.p,
+                                                    node_bin_.p, dd_key_.p, dd_perm_.p);
+  TB_LAUNCHED("k_dedup_keys");
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64,
+                                  stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64,
+                                  stream_);
+  k_dedup_gather<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, qnode_.p, qres_.p, x_.p, node_blk_.p, d_bi_.p,
+                                                      dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p, dd_perm_.p,
+                                                      q_gpos_.p);
+  TB_LAUNCHED("k_dedup_gather");
+  // subsets: (start, count, splits so far); the donors' lists to begin with
+  struct Seg {
+    int start, len, depth;
+  };
+  std::vector<Seg> segs, next;
+  std::vector<int4> leaves;
+  long long pos = 0;
+  for (int d = 0; d < nb; d++) {
+    if (dcount[d] > 0) segs.push_back(Seg{(int)pos, (int)dcount[d], 0});
+    pos += dcount[d];
+  }
+  constexpr int kChunk = 4096;
+  auto chunks_of = [&](const std::vector<Seg>& v, std::vector<int4>& ch, std::vector<int>& starts) {
+    ch.clear();
+    starts.clear();
+    for (size_t a = 0; a < v.size(); a++) {
+      starts.push_back(v[a].start);
+      for (int c = 0; c < v[a].len; c += kChunk)
+        ch.push_back(make_int4((int)a, v[a].start + c, std::min(kChunk, v[a].len - c), 0));
+    }
+  };
+  std::vector<int4> ch;
+  std::vector<int> starts;
+  chunks_of(segs, ch, starts);
+  if (!ch.empty()) {
+    TB_CUDA(dd_chunks_.ensure(ch.size()));
+    TB_CUDA(dd_starts_.ensure(starts.size()));
+    TB_CUDA(cudaMemcpyAsync(dd_chunks_.p, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaMemcpyAsync(dd_starts_.p, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            stream_));
+    k_dedup_segfill<<<(unsigned)ch.size(), 256, 0, stream_>>>(dd_chunks_.p, dd_starts_.p, dd_seg_.p);
+    TB_LAUNCHED("k_dedup_segfill");
+  }
+  for (int level = 0; level < 128 && !segs.empty(); level++) {
+    std::vector<Seg> act;
+    for (const Seg& g : segs) {
+      if (g.len > kDedupLeaf) act.push_back(g);
+      else leaves.push_back(make_int4(g.start, g.len, g.depth, 0));
+    }
+    if (act.empty()) break;
+    chunks_of(act, ch, starts);
+    const int na = (int)act.size();
+    TB_CUDA(dd_chunks_.ensure(ch.size()));
+    TB_CUDA(cudaMemcpyAsync(dd_chunks_.p, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, stream_));
+    std::vector<unsigned long long> box(6 * (size_t)na);
+    for (int a = 0; a < na; a++)
+      for (int k = 0; k < 3; k++) {
+        box[6 * a + k] = ~0ull;
+        box[6 * a + k + 3] = 0ull;
+      }
+    TB_CUDA(dd_box_.ensure(box.size()));
+    TB_CUDA(cudaMemcpyAsync(dd_box_.p, box.data(), box.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                            stream_));
+    TB_CUDA(dd_cnt_.ensure(8 * (size_t)na));
+    TB_CUDA(cudaMemsetAsync(dd_cnt_.p, 0, 8 * (size_t)na * sizeof(int), stream_));
+    TB_CUDA(cudaMemsetAsync(dd_oct_.p, 0, n, stream_));
+    k_dedup_box<<<(unsigned)ch.size(), 256, 0, stream_>>>(dd_chunks_.p, dd_perm_.p, dd_x_.p, dd_box_.p);
+    TB_LAUNCHED("k_dedup_box");
+    k_dedup_octant<<<(unsigned)ch.size(), 256, 0, stream_>>>(dd_chunks_.p, dd_perm_.p, dd_x_.p, dd_box_.p,
+                                                             dd_oct_.p, dd_cnt_.p);
+    TB_LAUNCHED("k_dedup_octant");
+    std::vector<int> cnt(8 * (size_t)na);
+    TB_CUDA(cudaMemcpyAsync(cnt.data(), dd_cnt_.p, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    next.clear();
+    for (int a = 0; a < na; a++) {
+      bool one = false;  // every point in one octant: compared as it is (icheck)
+      for (int j = 0; j < 8; j++) one = one || cnt[8 * a + j] == act[a].len;
+      if (one) {
+        leaves.push_back(make_int4(act[a].start, act[a].len, act[a].depth, 0));
+        continue;
+      }
+      int c = act[a].start;
+      for (int j = 0; j < 8; j++) {
+        const int m = cnt[8 * a + j];
+        if (m > 0) next.push_back(Seg{c, m, act[a].depth + 1});
+        c += m;
+      }
+    }
+    // stable partition of every splitting subset by octant (the others have
+    // one octant, or none, and keep their order)
+    int bits = 3;
+    while ((1ll << (bits - 3)) <= n) bits++;
+    k_dedup_pkeys<<<grid_for(n, kT), kT, 0, stream_>>>(dd_seg_.p, dd_oct_.p, n, dd_key_.p);
+    TB_LAUNCHED("k_dedup_pkeys");
+    tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_perm2_.p, (int)n, 0, bits,
+                                    stream_);
+    TB_CUDA(cub_tmp_.ensure(tmp));
+    cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_perm2_.p, (int)n, 0,
+                                    bits, stream_);
+    std::swap(dd_perm_, dd_perm2_);
+    chunks_of(next, ch, starts);
+    if (!ch.empty()) {
+      TB_CUDA(dd_chunks_.ensure(ch.size()));
+      TB_CUDA(dd_starts_.ensure(starts.size()));
+      TB_CUDA(cudaMemcpyAsync(dd_chunks_.p, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, stream_));
+      TB_CUDA(cudaMemcpyAsync(dd_starts_.p, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              stream_));
+      k_dedup_segfill<<<(unsigned)ch.size(), 256, 0, stream_>>>(dd_chunks_.p, dd_starts_.p, dd_seg_.p);
+      TB_LAUNCHED("k_dedup_segfill");
+    }
+    segs.swap(next);
+    TB_CUDA(cudaStreamSynchronize(stream_));  // host tables are reused next level
+  }
+  for (const Seg& g : segs) leaves.push_back(make_int4(g.start, g.len, g.depth, 0));
+  if (!leaves.empty()) {
+    TB_CUDA(dd_leaves_.ensure(leaves.size()));
+    TB_CUDA(cudaMemcpyAsync(dd_leaves_.p, leaves.data(), leaves.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                            stream_));
+    k_dedup_leaves<<<grid_for((long long)leaves.size(), 128), 128, 0, stream_>>>(
+        dd_leaves_.p, (int)leaves.size(), dd_perm_.p, dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p);
+    TB_LAUNCHED("k_dedup_leaves");
+  }
+  k_dedup_apply<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, dd_itag_.p, dd_rtag_.p, qres_.p, q_xt_.p,
+                                                     q_rep_.p, err_.p, counters_.p);
+  TB_LAUNCHED("k_dedup_apply");
+  TB_CUDA(cudaStreamSynchronize(stream_));  // host staging vectors go out of scope
+  dedup_ran_ = true;
   return 0;
 }
 
@@ -1014,6 +1244,17 @@ int Engine::run_donors() {
     k_cancel<<<148 * 4, kT, 0, stream_>>>(cmlist_.p, dcnt_.p, slot_.p, K_, qcell_.p, cell_res_.p, interp2rec_.p,
                                            it_cancel_.p);
     TB_LAUNCHED("k_cancel");
+    if (dedup_ran_) {  // resetCoincident
+      TB_CUDA(dd_ireset_.ensure(nq_));
+      k_fill_int<<<grid_for(nq_, kT), kT, 0, stream_>>>(dd_ireset_.p, 1, nq_);
+      TB_LAUNCHED("k_fill_int");
+      k_reset_coincident_min<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, q_xt_.p, nq_, it_cancel_.p,
+                                                                    dd_ireset_.p);
+      TB_LAUNCHED("k_reset_coincident_min");
+      k_reset_coincident_set<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, q_xt_.p, nq_, dd_ireset_.p,
+                                                                    it_cancel_.p);
+      TB_LAUNCHED("k_reset_coincident_set");
+    }
     k_iblank_final<<<grid_for(R, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, iblank_.p,
                                                         counters_.p);
     TB_LAUNCHED("k_iblank_final");
@@ -1068,6 +1309,7 @@ int Engine::connectivity() {
   cell_timed_ = false;
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
+  TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
   if (!coords_resident_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
   int rc = run_holemaps();
@@ -1086,7 +1328,6 @@ int Engine::connectivity() {
     if (rc) return rc;
   } else {
     TB_CUDA(cudaEventRecord(ev_[4], stream_));
-    TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
   }
   TB_CUDA(cudaEventRecord(ev_[5], stream_));
   rc = run_donors();
@@ -1113,6 +1354,7 @@ int Engine::connectivity() {
   stats_.nreceptor = (long long)cnt[5];
   stats_.nrecords = nrec_;
   stats_.nleaf = nleaf_total_;
+  stats_.nmerged = (long long)cnt[7];
   stats_.npairs = npairs_;
   stats_.launches = nlaunch_;
   stats_.cand_verts = (long long)cnt[6];

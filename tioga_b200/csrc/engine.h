@@ -26,6 +26,7 @@ constexpr int kHoles = 0;        // holes, the first entries of the marked-node 
 constexpr int kMarked = 1;       // holes plus nfringe layers
 constexpr int kCancelMarks = 2;  // nodes marked for cancellation
 constexpr int kSeg = 4;          // two alternating frontier ranges of the marked list (4 ints)
+constexpr int kDedupLeaf = 20;   // uniqNodesTree compares subsets of at most 20 points pairwise
 constexpr int kMaxTreeDepth = 32; // tree levels below the root at most (30-bit keys: 29 reachable)
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kSlots = 8;       // inline search candidates per query
@@ -123,6 +124,7 @@ struct Stats {
   long long nhole = 0;        // final iblank == 0
   long long nrecords = 0;     // chosen donors (before cancellation)
   long long nleaf = 0;        // tree leaves (the cell pass's units of work, with the cells)
+  long long nmerged = 0;      // query points merged into a coincident one (not searched themselves)
   long long npairs = 0;       // intersecting (receptor, donor) block pairs
   long long launches = 0;     // kernels this library launched in the call
   long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
@@ -183,6 +185,8 @@ class Engine {
   int run_search();
   int run_donors();
   int donor_rest_init();
+  int dedup_gate();
+  int run_dedup(int tiles_x);
   int run_celliblank();
   int download_iblank();
   int fetch_interps();
@@ -237,6 +241,16 @@ class Engine {
   DBuf<unsigned char> node_blk_, cell_blk_, cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_;
   DBuf<int> m1_, cmark_;            // nfringe marks and cancel marks (first marker wins an atomicExch)
   DBuf<int> mlist_, cmlist_, dcnt_;  // marked nodes (holes first), cancel-marked nodes, their counters
+  // coincident query points (uniqNodesTree)
+  DBuf<short> node_bin_;            // 10x10x10 OBB bin of every node (donor-list order)
+  bool dedup_active_ = false;       // some block has nodes within the gate's distance
+  bool dedup_ran_ = false;          // this call merged coincident query points
+  DBuf<int> q_xt_, q_rep_, q_gpos_, dd_refq_, dd_perm_, dd_perm2_, dd_mtag_, dd_itag_, dd_seg_, dd_cnt_, dd_ireset_;
+  DBuf<double> dd_x_, dd_rtag_;
+  DBuf<unsigned long long> dd_key_, dd_key2_, dd_box_;
+  DBuf<unsigned char> dd_oct_;
+  DBuf<int4> dd_chunks_, dd_leaves_;
+  DBuf<int> dd_starts_, dd_pqoff_, dd_prank_;
   int prev_nrec_ = 0;               // records of the previous call (their receptors are reset next call)
   bool donor_rest_ = false;         // per-node donor state is in its rest state
   DBuf<int> wall_list_, obc_list_;

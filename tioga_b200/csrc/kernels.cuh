@@ -167,6 +167,33 @@ __global__ void k_interp(const double* x, const unsigned long long* rkey, const 
                          const int* reset_t, const int* orig_cell, int* it_node, double* it_w, int* it_rec,
                          int* it_don, unsigned char* it_nv, unsigned char* it_cancel, double* rres,
                          int* interp2rec, unsigned* err);
+__global__ void k_node_bins(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+                            short* node_bin);
+__global__ void k_coin_count(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+                             int* cnt);
+__global__ void k_coin_fill(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+                            const int* off, unsigned long long* key, int* val);
+__global__ void k_coin_check(const unsigned long long* key, const int* val, long long n, const double* x,
+                             const unsigned char* node_blk, const BlockInfo* bi, unsigned* flag);
+__global__ void k_dedup_keys(const int* qnode, const int* qdon, long long nq, const int* pair_qoff, int npairs,
+                             const int* pair_rank, const short* node_bin, unsigned long long* key, int* val);
+__global__ void k_dedup_gather(const int* refq, long long n, const int* qnode, const double* qres, const double* x,
+                               const unsigned char* node_blk, const BlockInfo* bi, double* xg, int* mtag,
+                               double* rtag, int* itag, int* perm, int* gpos_of);
+__global__ void k_dedup_box(const int4* chunks, const int* perm, const double* xg, unsigned long long* box);
+__global__ void k_dedup_octant(const int4* chunks, const int* perm, const double* xg, const unsigned long long* box,
+                               unsigned char* oct, int* cnt);
+__global__ void k_dedup_pkeys(const int* segstart, const unsigned char* oct, long long n, unsigned long long* key);
+__global__ void k_dedup_segfill(const int4* chunks, const int* starts, int* segstart);
+__global__ void k_dedup_leaves(const int4* leaves, int nleaves, const int* perm, const double* xg, const int* mtag,
+                               double* rtag, int* itag);
+__global__ void k_dedup_apply(const int* refq, long long n, const int* itag, const double* rtag, double* qres,
+                              int* q_xt, int* q_rep, unsigned* err, unsigned long long* counters);
+__global__ void k_dedup_copy(const int* q_rep, long long nq, int* qcell, unsigned char* qtie);
+__global__ void k_reset_coincident_min(const int* interp2rec, const int* q_xt, long long nq,
+                                       const unsigned char* it_cancel, int* ireset);
+__global__ void k_reset_coincident_set(const int* interp2rec, const int* q_xt, long long nq, const int* ireset,
+                                       unsigned char* it_cancel);
 __global__ void k_cancel(const int* cmlist, const int* dcnt, const int* slot, int K, const int* qcell,
                          const double* cell_res, const int* interp2rec, unsigned char* it_cancel);
 __global__ void k_iblank_final(const int* it_rec, const unsigned char* it_cancel, const int* rcount, int* iblank,
