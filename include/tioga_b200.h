@@ -73,20 +73,57 @@ void tioga_setmexclude_(int *mexclude);
 /* tiogaInterface.C:317-326 */
 void tioga_delete_(void);
 
-/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
- * p4est, high-order callbacks, fringe reduction, Tecplot output).  They are
- * exported so that existing solvers link; each reports "not supported" and
- * sets the last error. */
+/* tiogaInterface.C:160-163: the high-order connectivity (tioga.C:162-178):
+ * the points of every receptor cell (cell iblank -1 after the last
+ * performconnectivity) are searched in the donor blocks, and points whose
+ * donor is a field cell get interpolation weights.  The following
+ * tioga_dataupdate_mb_ then interpolates at those points (ROW solutions,
+ * element-major DOFs) and updates the receptor cells (highOrder.C:152-566).
+ * Every block's elements must be described with
+ * tioga_b200_set_highorder_lagrange_. */
 void tioga_performconnectivity_highorder_(void);
-void tioga_performconnectivity_amr_(void);
+/* tiogaInterface.C:273-285.  Recorded (it switches the data update to the
+ * point form), but the solver's host callbacks cannot run in the device
+ * search; describe the elements with tioga_b200_set_highorder_lagrange_. */
 void tioga_set_highorder_callback_(void (*f1)(int *, int *), void (*f2)(int *, int *, double *),
                                    void (*f3)(int *, double *, int *, double *),
                                    void (*f4)(int *, double *, int *, int *, double *, double *, int *),
                                    void (*f5)(int *, int *, double *, int *, int *, double *));
+
+/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
+ * p4est, fringe reduction, Tecplot output).  They are exported so that
+ * existing solvers link; each reports "not supported" and sets the last
+ * error. */
+void tioga_performconnectivity_amr_(void);
 void tioga_reduce_fringes_(void);
 void tioga_writeoutputfiles_(int *nvar, char *itype);
 
 /* ---- additions of this library (no counterpart in TIOGA) -------------- */
+
+/* The elements of block btag for the high-order path, in place of the
+ * solver callbacks: Lagrange hexahedra of degree `order` (1..10) with
+ * equispaced nodes.  xdof holds every cell's (order+1)^3 DOF coordinates,
+ * cell after cell in the block's cell order, tensor order within a cell
+ * (node (i, j, k) at ((k (order+1) + j) (order+1) + i), reference point
+ * (i, j, k) / order, i along the cell's first corner edge v0->v1, j along
+ * v0->v3, k along v0->v4).  Caller-owned like the coordinates, read again by
+ * every tioga_performconnectivity_highorder_.  The solution arrays of the
+ * high-order data update are laid out the same way, nvar values per DOF.
+ * What the device computes is what such callbacks would: the cell's DOFs
+ * as its receptor points, Newton inversion of the element map from the
+ * centre (|update| < 1e-14 within 50 steps) as the inclusion test with
+ * r, s, t in [-1e-10, 1 + 1e-10], the basis at the inverted point as the
+ * weights, and nodal values written back unchanged. */
+void tioga_b200_set_highorder_lagrange_(int *btag, int *order, double *xdof);
+/* Point donors of donor block btag after the high-order connectivity, in
+ * its list order: out[4 i ..] = (receptor block index, point index in that
+ * block, donor cell, weight count), w[1331 i ..] = weights.  Returns the
+ * count; out or w may be NULL. */
+int tioga_b200_pointdonors_(int *btag, int *out, double *w);
+/* High-order counters: [0] query points, [1] with a donor, [2] ties,
+ * [3] interpolation records, [4] coincident points merged, [5] receptor
+ * cells changed by the orphan rule in the last data update. */
+void tioga_b200_highorder_stats_(long long out[8]);
 
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);

@@ -98,6 +98,13 @@ typedef struct {
   int ncancel;
   int *cancel_nodes;
   int cancel_cap;
+  /* high-order path (highOrder.C): receptor cells, their points, point donors */
+  int nrc, ntp;
+  int *ctag, *ppc;
+  double *rxyz, *rst;
+  int ninterp2;
+  int *i2_inode0, *i2_nw, *i2_rinfo; /* rinfo: point id, receptor block */
+  double *i2_w;                      /* NFRAC per record */
 } block_t;
 
 static struct {
@@ -112,7 +119,22 @@ static struct {
   obb_t *pair_obb;
   int nsend; /* 1 when any pair exists (self-message map), else 0 */
   double **qblock;
+  /* high-order callbacks (src/MeshBlock.h:79-83) */
+  int ihigh, ihighGlobal, ihigh_search;
+  void (*get_nodes_per_cell)(int *, int *);
+  void (*get_receptor_nodes)(int *, int *, double *);
+  void (*donor_inclusion_test)(int *, double *, int *, double *);
+  void (*donor_frac)(int *, double *, int *, int *, double *, double *, int *);
+  void (*convert_to_modal)(int *, int *, double *, int *, int *, double *);
+  void (*block_hook)(int); /* oracle only: names the block before callbacks */
+  double *search_rst;      /* rst of the query being searched */
 } G;
+
+#define NFRAC 1331
+static void data_update_points(int nvar, int itype);
+static void ho_hook(int ib) {
+  if (G.block_hook) G.block_hook(ib);
+}
 
 static int find_tag(int tag) {
   for (int i = 0; i < G.nblocks; i++)
@@ -1004,6 +1026,14 @@ static void adt_build(block_t *b) {
  * for an accept on a face (|frac|<TOL) of a no-donor (BIG) cell */
 static void check_containment(block_t *b, int *cellIndex, int elem, const double *xs) {
   int icell = b->elementList[elem], n, i;
+  if (G.ihigh_search) { /* checkContainment.C:86-94 */
+    int icell1 = icell + 1, pass = 0;
+    cellIndex[0] = -1;
+    cellIndex[1] = 0;
+    G.donor_inclusion_test(&icell1, (double *)xs, &pass, G.search_rst);
+    if (pass) cellIndex[0] = icell;
+    return;
+  }
   double xv[8][3], frac[8];
   int inode[8];
   cell_type(b, icell, &n, &i);
@@ -1196,6 +1226,7 @@ static void search_block(block_t *b) {
   for (int i = 0; i < b->nsearch; i++) {
     if (b->xtag[i] == i) {
       int ci[2];
+      G.search_rst = b->rst ? b->rst + 3 * i : NULL;
       adt_search(b, ci, b->xsearch + 3 * i);
       b->donorId[i] = ci[0];
     } else {
@@ -1494,6 +1525,8 @@ static void free_block(block_t *b) {
   free(b->donorId); free(b->xtag); free(b->elementList); free(b->elementBbox);
   free(b->adtInt); free(b->adtReal); free(b->dl_cnt); free(b->dl_off); free(b->dl);
   free(b->interp); free(b->interp2donor); free(b->cancel_nodes);
+  free(b->ctag); free(b->ppc); free(b->rxyz); free(b->rst);
+  free(b->i2_inode0); free(b->i2_nw); free(b->i2_rinfo); free(b->i2_w);
   if (b->own_iblank_cell) free(b->iblank_cell);
   free(b);
 }
@@ -1580,6 +1613,7 @@ void tioga_performconnectivity_(void) {
     search_block(G.b[ib]);
   }
   exchange_donors();
+  G.ihighGlobal = G.ihigh; /* tioga.C:138 */
   for (int ib = 0; ib < G.nblocks; ib++) cell_iblanks(G.b[ib]);
   free(G.qblock);
   G.qblock = (double **)calloc(G.nblocks ? G.nblocks : 1, sizeof(double *));
@@ -1650,7 +1684,8 @@ void tioga_dataupdate_mb_(int *nvar, char *itype) {
     printf("#tiogaInterface.C:dataupdate_:unknown data orientation\n");
     return;
   }
-  data_update(*nvar, t);
+  if (G.ihighGlobal) data_update_points(*nvar, t); /* tiogaInterface.C:194-214 */
+  else data_update(*nvar, t);
 }
 
 /* The reference looks up mesh tag 0 here, which never exists (undefined
@@ -1728,6 +1763,244 @@ void tioga_delete_(void) {
   free(G.pair_obb);
   free(G.qblock);
   memset(&G, 0, sizeof(G));
+}
+
+/* ======================================================================= */
+/* high-order path: tioga.C:162-178, highOrder.C:152-566, exchangeSearchData  */
+/* ======================================================================= */
+void tioga_set_highorder_callback_(void (*f1)(int *, int *), void (*f2)(int *, int *, double *),
+                                   void (*f3)(int *, double *, int *, double *),
+                                   void (*f4)(int *, double *, int *, int *, double *, double *, int *),
+                                   void (*f5)(int *, int *, double *, int *, int *, double *)) {
+  G.get_nodes_per_cell = f1;
+  G.get_receptor_nodes = f2;
+  G.donor_inclusion_test = f3;
+  G.donor_frac = f4;
+  G.convert_to_modal = f5;
+  G.ihigh = 1; /* tioga.h:211-223 */
+}
+
+/* oracle only: fn(block index) is called before the callbacks of a block */
+void tioga_oracle_set_block_hook(void (*fn)(int)) { G.block_hook = fn; }
+
+/* highOrder.C:208-247: receptor cells (iblank_cell == -1) and their points */
+static void get_internal_nodes(int ib) {
+  block_t *b = G.b[ib];
+  free(b->ctag);
+  b->ctag = (int *)malloc(sizeof(int) * (b->ncells ? b->ncells : 1));
+  b->nrc = 0;
+  for (int i = 0; i < b->ncells; i++)
+    if (b->iblank_cell[i] == -1) b->ctag[b->nrc++] = i + 1;
+  free(b->ppc);
+  b->ppc = (int *)malloc(sizeof(int) * (b->nrc ? b->nrc : 1));
+  b->ntp = 0;
+  ho_hook(ib);
+  for (int i = 0; i < b->nrc; i++) {
+    G.get_nodes_per_cell(&b->ctag[i], &b->ppc[i]);
+    b->ntp += b->ppc[i];
+  }
+  free(b->rxyz);
+  b->rxyz = (double *)malloc(sizeof(double) * 3 * (b->ntp ? b->ntp : 1));
+  for (int i = 0, m = 0; i < b->nrc; i++) {
+    G.get_receptor_nodes(&b->ctag[i], &b->ppc[i], b->rxyz + m);
+    m += 3 * b->ppc[i];
+  }
+}
+
+/* exchangeSearchData(at_points = 1) + getExtraQueryPoints (highOrder.C:272-319):
+ * every receptor point inside the pair's box, in point order, res = BIG */
+static void exchange_search_points(void) {
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *b = G.b[ib];
+    b->nsearch = 0;
+    free(b->xsearch); b->xsearch = NULL;
+    free(b->isearch); b->isearch = NULL;
+    free(b->tagsearch); b->tagsearch = NULL;
+    free(b->donorId); b->donorId = NULL;
+    free(b->res_search); b->res_search = NULL;
+    free(b->rst); b->rst = NULL;
+  }
+  int **lists = (int **)malloc(sizeof(int *) * (G.npairs + 1));
+  int *counts = (int *)calloc(G.npairs + 1, sizeof(int));
+  for (int p = 0; p < G.npairs; p++) {
+    block_t *rec = G.b[G.pair_ib[p]];
+    const obb_t *o = &G.pair_obb[p];
+    lists[p] = (int *)malloc(sizeof(int) * (rec->ntp ? rec->ntp : 1));
+    for (int i = 0; i < rec->ntp; i++) {
+      double xd[3];
+      for (int j = 0; j < 3; j++) xd[j] = 0;
+      for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++) xd[j] += (rec->rxyz[3 * i + k] - o->xc[k]) * o->vec[j][k];
+      if (fabs(xd[0]) <= o->dxc[0] && fabs(xd[1]) <= o->dxc[1] && fabs(xd[2]) <= o->dxc[2])
+        lists[p][counts[p]++] = i;
+    }
+    G.b[G.pair_ob[p]]->nsearch += counts[p];
+  }
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *b = G.b[ib];
+    if (b->nsearch < 1) continue;
+    b->xsearch = (double *)malloc(sizeof(double) * 3 * b->nsearch);
+    b->res_search = (double *)malloc(sizeof(double) * b->nsearch);
+    b->isearch = (int *)malloc(sizeof(int) * 3 * b->nsearch);
+    b->tagsearch = (int *)malloc(sizeof(int) * b->nsearch);
+    b->donorId = (int *)malloc(sizeof(int) * b->nsearch);
+    b->rst = (double *)calloc(3 * (size_t)b->nsearch, sizeof(double));
+  }
+  int *fill = (int *)calloc(G.nblocks, sizeof(int));
+  for (int p = 0; p < G.npairs; p++) {
+    block_t *rec = G.b[G.pair_ib[p]], *don = G.b[G.pair_ob[p]];
+    int ob = G.pair_ob[p];
+    for (int j = 0; j < counts[p]; j++) {
+      int pt = lists[p][j], q = fill[ob]++;
+      don->isearch[3 * q] = 0;
+      don->isearch[3 * q + 1] = pt;
+      don->isearch[3 * q + 2] = G.pair_ib[p];
+      don->tagsearch[q] = rec->tag;
+      for (int k = 0; k < 3; k++) don->xsearch[3 * q + k] = rec->rxyz[3 * pt + k];
+      don->res_search[q] = BIGVALUE;
+    }
+    free(lists[p]);
+  }
+  free(fill);
+  free(lists);
+  free(counts);
+}
+
+/* highOrder.C:321-419 (ihigh branch): point donors that are field cells */
+static void process_point_donors(int ib) {
+  block_t *b = G.b[ib];
+  free(b->i2_inode0); free(b->i2_nw); free(b->i2_rinfo); free(b->i2_w);
+  b->ninterp2 = 0;
+  for (int i = 0; i < b->nsearch; i++)
+    if (b->donorId[i] > -1 && b->iblank_cell[b->donorId[i]] == 1) b->ninterp2++;
+  const int n = b->ninterp2 ? b->ninterp2 : 1;
+  b->i2_inode0 = (int *)malloc(sizeof(int) * n);
+  b->i2_nw = (int *)malloc(sizeof(int) * n);
+  b->i2_rinfo = (int *)malloc(sizeof(int) * 2 * n);
+  b->i2_w = (double *)malloc(sizeof(double) * NFRAC * (size_t)n);
+  ho_hook(ib);
+  for (int i = 0, m = 0; i < b->nsearch; i++) {
+    if (b->donorId[i] > -1 && b->iblank_cell[b->donorId[i]] == 1) {
+      int icell = b->donorId[i] + 1, ndim = NFRAC;
+      b->i2_nw[m] = 0;
+      G.donor_frac(&icell, b->xsearch + 3 * i, &b->i2_nw[m], &b->i2_inode0[m], b->i2_w + (size_t)NFRAC * m,
+                   b->rst + 3 * i, &ndim);
+      b->i2_rinfo[2 * m] = b->isearch[3 * i + 1];
+      b->i2_rinfo[2 * m + 1] = b->isearch[3 * i + 2];
+      m++;
+    }
+  }
+}
+
+void tioga_performconnectivity_highorder_(void) {
+  if (!G.ihigh) {
+    fprintf(stderr, "#tioga_oracle: performconnectivity_highorder without callbacks is not restated\n");
+    return;
+  }
+  for (int ib = 0; ib < G.nblocks; ib++) get_internal_nodes(ib);
+  exchange_search_points();
+  G.ihigh_search = 1;
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    ho_hook(ib);
+    search_block(G.b[ib]);
+    process_point_donors(ib);
+  }
+  G.ihigh_search = 0;
+}
+
+/* tioga.C:336-524 with at_points = 1, ROW (getInterpolatedSolutionAtPoints
+ * ihigh branch, highOrder.C:421-477; receptor side, clearOrphans 152-205,
+ * updatePointData 479-566).  A point reached by several donors keeps the
+ * last one in packet order (donor blocks in order, then list order). */
+static void data_update_points(int nvar, int itype) {
+  for (int ib = 0; ib < G.nblocks; ib++)
+    if (G.qblock == NULL || G.qblock[ib] == NULL) {
+      printf("Solution data not set, cannot update \n");
+      return;
+    }
+  if (!G.nsend) return;
+  if (itype != 0) {
+    fprintf(stderr, "#tioga_oracle: high-order data update is ROW only (highOrder.C:474)\n");
+    return;
+  }
+  double **qtmp = (double **)malloc(sizeof(double *) * G.nblocks);
+  int **itmp = (int **)malloc(sizeof(int *) * G.nblocks);
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *b = G.b[ib];
+    qtmp[ib] = (double *)calloc((size_t)(b->ntp ? b->ntp : 1) * nvar, sizeof(double));
+    itmp[ib] = (int *)calloc(b->ntp ? b->ntp : 1, sizeof(int));
+  }
+  double *qq = (double *)malloc(sizeof(double) * nvar);
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *d = G.b[ib];
+    const double *q = G.qblock[ib];
+    for (int i = 0; i < d->ninterp2; i++) {
+      for (int k = 0; k < nvar; k++) qq[k] = 0;
+      const int inode = d->i2_inode0[i] - 1;
+      for (int m = 0; m < d->i2_nw[i]; m++) {
+        const double w = d->i2_w[(size_t)NFRAC * i + m];
+        for (int k = 0; k < nvar; k++) qq[k] += q[inode + m * nvar + k] * w;
+      }
+      const int pt = d->i2_rinfo[2 * i], rb = d->i2_rinfo[2 * i + 1];
+      for (int k = 0; k < nvar; k++) qtmp[rb][(size_t)pt * nvar + k] = qq[k];
+      itmp[rb][pt] = 1;
+    }
+  }
+  free(qq);
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *b = G.b[ib];
+    /* clearOrphans: the last orphan point of a cell decides */
+    for (int i = 0, m = 0; i < b->nrc; i++) {
+      int reject = 0;
+      for (int j = 0; j < b->ppc[i]; j++, m++) {
+        if (itmp[ib][m] == 0) {
+          reject = 2;
+          for (int k = 0; k < G.nmesh; k++)
+            if (k != b->tag - 1 && G.hm[k].exist && check_holemap(b->rxyz + 3 * m, &G.hm[k])) {
+              reject = 1;
+              break;
+            }
+        }
+      }
+      if (reject == 1) b->iblank_cell[b->ctag[i] - 1] = 0;
+      else if (reject == 2) b->iblank_cell[b->ctag[i] - 1] = 1;
+    }
+    /* updatePointData */
+    double *qout = (double *)malloc(sizeof(double) * (size_t)nvar * NFRAC);
+    ho_hook(ib);
+    for (int i = 0, m = 0; i < b->nrc; i++) {
+      if (b->iblank_cell[b->ctag[i] - 1] == -1) {
+        int npts = NFRAC, index_out = 0;
+        G.convert_to_modal(&b->ctag[i], &b->ppc[i], qtmp[ib] + m, &npts, &index_out, qout);
+        index_out -= 1;
+        for (int j = 0, k = 0; j < npts; j++)
+          for (int n = 0; n < nvar; n++, k++) G.qblock[ib][index_out + j * nvar + n] = qout[k];
+      }
+      m += b->ppc[i] * nvar;
+    }
+    free(qout);
+    free(qtmp[ib]);
+    free(itmp[ib]);
+  }
+  free(qtmp);
+  free(itmp);
+}
+
+/* oracle only: point donors of block btag's list, in list order: for each
+ * record (receptor block, point id, donor cell 0-based, weights count) */
+int tioga_oracle_pointdonors(int btag, int *out, double *w) {
+  int ib = find_tag(btag);
+  if (ib < 0) return 0;
+  block_t *b = G.b[ib];
+  if (out)
+    for (int i = 0; i < b->ninterp2; i++) {
+      out[4 * i] = b->i2_rinfo[2 * i + 1];
+      out[4 * i + 1] = b->i2_rinfo[2 * i];
+      out[4 * i + 2] = b->i2_inode0[i];
+      out[4 * i + 3] = b->i2_nw[i];
+      if (w) memcpy(w + (size_t)NFRAC * i, b->i2_w + (size_t)NFRAC * i, sizeof(double) * b->i2_nw[i]);
+    }
+  return b->ninterp2;
 }
 
 /* ---- oracle-only diagnostics for the tests ---------------------------- */

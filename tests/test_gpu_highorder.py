@@ -1,0 +1,51 @@
+"""The high-order path on the GPU (tioga_performconnectivity_highorder_ and
+the point data update) against the oracle's restatement driven by the
+Lagrange-hex callbacks: iblanks, point donors and their FP64 weights, the
+receptor cells after the orphan rule, and the updated DOF values, bit for
+bit."""
+import numpy as np
+import pytest
+
+import tioga_b200 as tb
+from tioga_b200 import cases
+from tests.ho_harness import run_highorder, diff_highorder
+
+pytestmark = pytest.mark.gpu
+
+
+def _mex1(t):
+    t.setmexclude(1)
+
+
+def _both_ways():
+    """Receptor cells in both blocks: a coarse background, a fine cubic
+    shell (user resolutions), caps that are not overset boundaries."""
+    system, ho = cases.config4(4, nbg=33, ne_r=6, ne_t=8, ne_p=16, p=3, cap_obc=False)
+    bg, sh = system.blocks
+    res = {bg.tag: (np.full(bg.nnodes, 10.0), np.full(bg.ncells, 10.0)),
+           sh.tag: (np.full(sh.nnodes, 1e-3), np.full(sh.ncells, 1e-3))}
+    return system, ho, res, _mex1
+
+
+CASES = {
+    "small": lambda: cases.small_config4(4) + (None, None),
+    "both-ways": _both_ways,
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_highorder_matches_oracle(name, oracle_lib):
+    system, ho, res, setup = CASES[name]()
+    nvar = 3
+    q = cases.dof_fields(ho, nvar, seed=21)
+    ref = run_highorder(oracle_lib, system, ho, nvar, q, "hook", resolutions=res, setup=setup)
+    gpu = run_highorder(tb.library_path(), system, ho, nvar, q, "gpu", resolutions=res, setup=setup)
+    problems = diff_highorder(system, ref, gpu)
+    assert not problems, "\n".join(problems)
+    st = gpu["stats"]
+    assert st[2] == 0, st            # no order-dependent ties
+    assert st[3] > 0 and st[4] > 0   # records, and coincident points merged
+    changed = sum(int((gpu["q"][b.tag] != q[i]).sum()) for i, b in enumerate(system.blocks))
+    assert changed > 0
+    if name == "both-ways":  # cubic donors reached background points
+        assert ref["points"][system.blocks[1].tag][0].shape[0] > 0

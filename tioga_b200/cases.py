@@ -287,6 +287,122 @@ def config1(seed: int = 1, nbg: int = 257, nshell: int = 3, nr: int = 65, nt: in
                   meta={"seed": seed, "centres": centres.tolist(), "rwall": rwall.tolist()})
 
 
+# ---------------------------------------------------------------------------
+# High-order workload: Lagrange hexahedra described by their degrees of
+# freedom (element-major, tensor order i fastest, reference cube [0,1]^3 with
+# node (i, j, k) at (i/p, j/p, k/p)), registered through their corners
+# ---------------------------------------------------------------------------
+@dataclass
+class HighOrder:
+    """Degree and DOF coordinates (ncells, (p+1)^3, 3) of one block's cells."""
+
+    p: int
+    xdof: np.ndarray
+
+
+HEX_TO_TENSOR = [0, 1, 3, 2, 4, 5, 7, 6]  # hex vertex order -> tensor (i fastest) order
+
+
+def shell_q(ne_r: int, ne_t: int, ne_p: int, p: int, r0: float, r1: float, ratio: float,
+            theta0: float, theta1: float, center, perturb: float, rng: np.random.Generator,
+            cap_obc: bool = True):
+    """Curved band of a spherical shell, theta in [theta0, theta1], phi periodic,
+    as ne_r x ne_t x ne_p Lagrange hexahedra of degree p.  Every DOF is a point
+    of one global (ne_r p + 1) x (ne_t p + 1) x (ne_p p) lattice in (r, theta,
+    phi), so neighbouring elements share their face DOFs bit for bit; DOFs
+    inside an element are moved by +-``perturb`` of the local lattice spacing.
+    Returns (corner coordinates, hex cells, wall nodes, overset-boundary nodes,
+    DOF coordinates (ncells, (p+1)^3, 3))."""
+    nr, nt, npp = ne_r * p + 1, ne_t * p + 1, ne_p * p
+    # element corner radii graded by `ratio`; the DOF radii equispaced inside each element
+    rc = _radii(ne_r + 1, r0, r1, ratio)
+    r = np.concatenate([rc[e] + (rc[e + 1] - rc[e]) * np.arange(p) / p for e in range(ne_r)] + [rc[-1:]])
+    th = np.linspace(theta0, theta1, nt)
+    ph = np.linspace(0.0, 2.0 * np.pi, npp + 1)[:-1]
+    c = np.asarray(center, dtype=np.float64)
+
+    def xyz(R, T, P):
+        st = np.sin(T)
+        return np.stack([R * st * np.cos(P), R * st * np.sin(P), R * np.cos(T)], axis=-1) + c
+
+    # element (a, b, d) = (r, theta, phi) index; DOF (i, j, k) along (r, theta, phi)
+    a, b, d = np.meshgrid(np.arange(ne_r), np.arange(ne_t), np.arange(ne_p), indexing="ij")
+    a = a.ravel(); b = b.ravel(); d = d.ravel()
+    n1 = p + 1
+    k, j, i = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")
+    i = i.ravel(); j = j.ravel(); k = k.ravel()
+    ri = a[:, None] * p + i[None, :]
+    ti = b[:, None] * p + j[None, :]
+    pi = (d[:, None] * p + k[None, :]) % npp
+    R = r[ri].copy(); T = th[ti].copy(); P = ph[pi].copy()
+    if perturb > 0.0:
+        inner = ((i > 0) & (i < p) & (j > 0) & (j < p) & (k > 0) & (k < p))[None, :].repeat(len(a), 0)
+        dr = (r[np.minimum(ri + 1, nr - 1)] - r[np.maximum(ri - 1, 0)]) * 0.5
+        R[inner] += rng.uniform(-perturb, perturb, int(inner.sum())) * dr[inner]
+        T[inner] += rng.uniform(-perturb, perturb, int(inner.sum())) * (th[1] - th[0])
+        P[inner] += rng.uniform(-perturb, perturb, int(inner.sum())) * (ph[1] - ph[0])
+    xdof = xyz(R, T, P)
+    # registered corner mesh: lattice points with indices multiple of p
+    nrc, ntc, npc = ne_r + 1, ne_t + 1, ne_p
+
+    def nid(ia, ib, id_):
+        return ((id_ % npc) * ntc + ib) * nrc + ia
+
+    ia, ib, id_ = np.meshgrid(np.arange(nrc), np.arange(ntc), np.arange(npc), indexing="ij")
+    corner = np.zeros((nrc * ntc * npc, 3))
+    corner[nid(ia, ib, id_).ravel()] = xyz(r[ia.ravel() * p], th[ib.ravel() * p], ph[id_.ravel() * p])
+    # hex vertex order (u, v, w) = (r, theta, phi): right-handed, positive volume
+    tensor = np.stack([nid(a + di, b + dj, d + dk) for dk in (0, 1) for dj in (0, 1) for di in (0, 1)], axis=1)
+    hexes = tensor[:, [0, 1, 3, 2, 4, 5, 7, 6]].astype(np.int32)
+    wall = np.flatnonzero(np.isin(np.arange(len(corner)), nid(0, ib, id_).ravel())).astype(np.int32)
+    rim = np.zeros(len(corner), bool)
+    edge = (ia.ravel() == nrc - 1)
+    if cap_obc:  # the theta caps are overset boundaries too
+        edge = edge | (ib.ravel() == 0) | (ib.ravel() == ntc - 1)
+    rim[nid(ia, ib, id_).ravel()[edge]] = True
+    return corner, [(NV_HEX, hexes)], wall, np.flatnonzero(rim).astype(np.int32), xdof
+
+
+def config4(seed: int = 4, nbg: int = 97, ne_r: int = 24, ne_t: int = 24, ne_p: int = 48, p: int = 3,
+            perturb: float = 0.02, wall: bool = True, cap_obc: bool = True):
+    """High-order case: a degree-1 background box (nbg^3 nodes on [-5,5]^3)
+    and a curved band of a spherical shell (r 0.5 -> 2.0, theta in
+    [pi/4, 3pi/4]) of ne_r x ne_t x ne_p degree-p Lagrange hexahedra whose
+    inner DOFs are moved by +-2% of the spacing.  Returns the System of the
+    registered corner meshes and each block's HighOrder description."""
+    rng = np.random.default_rng(seed)
+    xb, cb = hex_box(nbg, -5.0, 5.0, 0.0, None)
+    hx = cb[0][1]
+    bg_dof = xb[hx[:, HEX_TO_TENSOR]]                       # (ncells, 8, 3)
+    xs, cs, wn, on, sh_dof = shell_q(ne_r, ne_t, ne_p, p, 0.5, 2.0, 1.1, np.pi / 4, 3 * np.pi / 4,
+                                     (0.1, -0.2, 0.05), perturb, rng, cap_obc)
+    bg = Block(1, xb, cb, _empty_i32(), _empty_i32(), name="background")
+    sh = Block(2, xs, cs, wn if wall else _empty_i32(), on, name=f"shell-q{p}")
+    system = System([bg, sh], name=f"cfg4(nbg={nbg},q{p} {ne_r}x{ne_t}x{ne_p},seed={seed})", meta={"seed": seed})
+    return system, [HighOrder(1, bg_dof), HighOrder(p, sh_dof)]
+
+
+def small_config4(seed: int = 4, wall: bool = True):
+    """config4 geometry at test size (17^3 box, 2 x 4 x 8 cubic elements)."""
+    return config4(seed, nbg=17, ne_r=2, ne_t=4, ne_p=8, p=3, wall=wall)
+
+
+def dof_fields(ho: list, nvar: int, seed: int = 5) -> list:
+    """Element-major DOF values (ncells * (p+1)^3 * nvar, ROW) of a seeded
+    cubic polynomial in x, y, z per variable."""
+    rng = np.random.default_rng(seed)
+    out = []
+    coef = rng.uniform(-1.0, 1.0, (nvar, 20))
+    for h in ho:
+        X = h.xdof.reshape(-1, 3)
+        x, y, z = X[:, 0], X[:, 1], X[:, 2]
+        mono = np.stack([np.ones_like(x), x, y, z, x * x, y * y, z * z, x * y, y * z, z * x,
+                         x ** 3, y ** 3, z ** 3, x * x * y, x * x * z, y * y * x, y * y * z, z * z * x,
+                         z * z * y, x * y * z], axis=1)
+        out.append((mono @ coef.T).reshape(-1).astype(np.float64))
+    return out
+
+
 def fields(system: System, nvar: int = 5, seed: int = 7) -> list:
     """Per-block solution arrays q (ROW layout, nnodes*nvar) ~ U(-1, 1)."""
     rng = np.random.default_rng(seed)

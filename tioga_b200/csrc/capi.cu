@@ -117,7 +117,9 @@ void tioga_dataupdate_mb_(int* nvar, char* itype) {
     printf("#tiogaInterface.C:dataupdate_:unknown data orientation\n");
     return;
   }
-  set_rc(g_tg->dataupdate(*nvar, t));
+  // after high-order registration the update goes to the points (tiogaInterface.C:194-214)
+  if (g_tg->ihigh_global()) set_rc(g_tg->dataupdate_highorder(*nvar, t));
+  else set_rc(g_tg->dataupdate(*nvar, t));
 }
 
 void tioga_dataupdate_(double* q, int* nvar, char* itype) {
@@ -170,13 +172,36 @@ void tioga_delete_(void) {
   g_tg = nullptr;
 }
 
-void tioga_performconnectivity_highorder_(void) { unsupported("tioga_performconnectivity_highorder_"); }
+void tioga_performconnectivity_highorder_(void) {
+  if (ready("tioga_performconnectivity_highorder_")) set_rc(g_tg->connectivity_highorder());
+}
 void tioga_performconnectivity_amr_(void) { unsupported("tioga_performconnectivity_amr_"); }
+// The callbacks are recorded (they switch the data update to the point
+// form, as in tioga.h:211-223), but a device search cannot call host code:
+// the elements must also be described with tioga_b200_set_highorder_lagrange_.
 void tioga_set_highorder_callback_(void (*)(int*, int*), void (*)(int*, int*, double*),
                                    void (*)(int*, double*, int*, double*),
                                    void (*)(int*, double*, int*, int*, double*, double*, int*),
                                    void (*)(int*, int*, double*, int*, int*, double*)) {
-  unsupported("tioga_set_highorder_callback_");
+  if (ready("tioga_set_highorder_callback_")) g_tg->set_highorder_callbacks();
+}
+void tioga_b200_set_highorder_lagrange_(int* btag, int* order, double* xdof) {
+  if (ready("tioga_b200_set_highorder_lagrange_")) set_rc(g_tg->set_highorder(*btag, *order, xdof));
+}
+int tioga_b200_pointdonors_(int* btag, int* out, double* w) {
+  if (!ready("tioga_b200_pointdonors_")) return 0;
+  return g_tg->point_donors(*btag, out, w);
+}
+void tioga_b200_highorder_stats_(long long out[8]) {
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  if (!g_tg) return;
+  const tb::HoStats& s = g_tg->ho_stats();
+  out[0] = s.npoints;
+  out[1] = s.ndonor;
+  out[2] = s.nties;
+  out[3] = s.nrecords;
+  out[4] = s.nmerged;
+  out[5] = s.norphan_cells;
 }
 void tioga_reduce_fringes_(void) { unsupported("tioga_reduce_fringes_"); }
 void tioga_writeoutputfiles_(int*, char*) { unsupported("tioga_writeoutputfiles_"); }

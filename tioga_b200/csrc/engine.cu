@@ -1,12 +1,9 @@
 // Host orchestration of the B200 connectivity path: preprocess, connectivity,
 // data update and the donor queries, all on one CUDA stream.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
-
 #include <algorithm>
 #include <cstring>
 
-#include "kernels.cuh"
+#include "engine_impl.cuh"
 
 namespace tb {
 
@@ -16,12 +13,7 @@ int fail(cudaError_t e) {
   return -(int)e - 1000;
 }
 
-static const int kT = 256;
-
-// After every launch: a launch error is reported at once; with
-// TIOGA_B200_CHECK=1 in the environment the stream is also synchronised so a
-// fault is attributed to the kernel that caused it.
-static int sync_check() {
+int sync_check() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("TIOGA_B200_CHECK");
@@ -29,22 +21,6 @@ static int sync_check() {
   }
   return v;
 }
-#define TB_LAUNCHED(name)                                                              \
-  do {                                                                                 \
-    nlaunch_++;                                                                        \
-    cudaError_t le_ = cudaGetLastError();                                              \
-    if (le_ == cudaSuccess && sync_check()) le_ = cudaStreamSynchronize(stream_);      \
-    if (le_ != cudaSuccess) {                                                          \
-      fprintf(stderr, "#tioga_b200: kernel %s failed: %s\n", name, cudaGetErrorString(le_)); \
-      return tb::fail(le_);                                                            \
-    }                                                                                  \
-  } while (0)
-
-#define TB_TRY(call)      \
-  do {                    \
-    int rc_ = (call);     \
-    if (rc_) return rc_;  \
-  } while (0)
 
 Engine::Engine() {
   cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking);
@@ -839,39 +815,10 @@ int Engine::run_search() {
   TB_CUDA(qacc_.ensure(nq_));
   TB_CUDA(cudaMemsetAsync(qkey_.p, 0xff, nq_ * sizeof(unsigned long long), stream_));
   TB_CUDA(cudaMemsetAsync(qacc_.p, 0, nq_ * sizeof(unsigned), stream_));
-  TB_CUDA(slots_.ensure((size_t)nq_ * kSlots));
-  TB_CUDA(ncand_q_.ensure(nq_ + 1));
-  TB_CUDA(cand_off_.ensure(nq_ + 1));
-  TB_CUDA(cudaMemsetAsync(ncand_q_.p + nq_, 0, sizeof(int), stream_));
-  long long ovf_cap = std::max<long long>(cand_cap_, std::max<long long>(nq_ / 8, 1 << 16));
-  unsigned count = 0, novf = 0;
+  unsigned count = 0;
   TB_CUDA(cudaEventRecord(sev_[0], stream_));
-  for (int attempt = 0; attempt < 2; attempt++) {
-    TB_CUDA(ovf_.ensure(ovf_cap));
-    TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq_, 256, 148 * 64), stream_, x_.p, d_bi_.p, cbox_.p,
-                    form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qnode_.p, qdon_.p,
-                    nq_, slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
-    TB_LAUNCHED("k_traverse");
-    TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-    TB_CUDA(cudaStreamSynchronize(stream_));
-    cand_cap_ = ovf_cap;
-    if ((long long)novf <= ovf_cap) break;
-    ovf_cap = (long long)novf + novf / 4 + 1024;  // grow the overflow list and traverse again
-  }
-  size_t tmp = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncand_q_.p, cand_off_.p, (int)(nq_ + 1), stream_);
-  TB_CUDA(cub_tmp_.ensure(tmp));
-  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, ncand_q_.p, cand_off_.p, (int)(nq_ + 1), stream_);
-  TB_CUDA(cudaMemcpyAsync(&count, cand_off_.p + nq_, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
+  TB_TRY(traverse_and_gather(x_.p, qnode_.p, qdon_.p, nq_, count));
   ncand_ = count;
-  TB_CUDA(cand_.ensure(std::max(1u, count)));
-  if (count > 0) {
-    k_gather_candidates<<<grid_for(nq_, kT), kT, 0, stream_>>>(slots_.p, ncand_q_.p, cand_off_.p, nq_, ovf_.p,
-                                                               scount_.p, (int)ovf_cap, cand_.p);
-    TB_LAUNCHED("k_gather_candidates");
-  }
   TB_CUDA(cudaEventRecord(sev_[1], stream_));
   if (count > 0) {
     TB_CUDA(refine_.ensure(count));
@@ -896,6 +843,50 @@ int Engine::run_search() {
     TB_LAUNCHED("k_dedup_copy");
   }
   search_timed_ = true;
+  return 0;
+}
+
+// Candidate cells of every query point (point qn[i] of xq, donor block
+// qd[i]): stack-free traversal of the donor's tree into per-query slots and
+// an overflow list, then one dense query-ordered list in cand_.  The FP32
+// form of the tree is used unless the FP64 form is selected.
+int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count) {
+  const int form = (precision_ == 0) ? 0 : 1;
+  TB_CUDA(slots_.ensure((size_t)nq * kSlots));
+  TB_CUDA(ncand_q_.ensure(nq + 1));
+  TB_CUDA(cand_off_.ensure(nq + 1));
+  TB_CUDA(scount_.ensure(2));
+  TB_CUDA(cudaMemsetAsync(ncand_q_.p + nq, 0, sizeof(int), stream_));
+  long long ovf_cap = std::max<long long>(cand_cap_, std::max<long long>(nq / 8, 1 << 16));
+  unsigned novf = 0;
+  count = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    TB_CUDA(ovf_.ensure(ovf_cap));
+    TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
+    launch_traverse(form, grid_for(nq, 256, 148 * 64), stream_, xq, d_bi_.p, cbox_.p,
+                    form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
+                    slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
+    TB_LAUNCHED("k_traverse");
+    TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    cand_cap_ = ovf_cap;
+    if ((long long)novf <= ovf_cap) break;
+    ovf_cap = (long long)novf + novf / 4 + 1024;  // grow the overflow list and traverse again
+  }
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
+  TB_CUDA(cudaMemcpyAsync(&count, cand_off_.p + nq, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  TB_CUDA(cand_.ensure(std::max(1u, count)));
+  if (count > 0) {
+    k_gather_candidates<<<grid_for(nq, kT), kT, 0, stream_>>>(slots_.p, ncand_q_.p, cand_off_.p, nq, ovf_.p,
+                                                              scount_.p, (int)ovf_cap, cand_.p);
+    TB_LAUNCHED("k_gather_candidates");
+  }
+  // the overflow counter's word is reused by the refinement count
+  TB_CUDA(cudaMemsetAsync(scount_.p + 1, 0, sizeof(unsigned), stream_));
   return 0;
 }
 
@@ -953,16 +944,26 @@ int Engine::dedup_gate() {
 // by level, the pairwise loop per leaf, then xtag / representative / merged
 // resolution per query.
 int Engine::run_dedup(int tiles_x) {
-  const long long n = nq_;
-  const int np = npairs_;
-  // queries of pair p are [qoff[p], qoff[p+1]); rank of p among its donor's pairs
-  std::vector<int> h_toff((size_t)tiles_x * np + 1);
+  // queries of pair p are [qoff[p], qoff[p+1])
+  std::vector<int> h_toff((size_t)tiles_x * npairs_ + 1);
   TB_CUDA(cudaMemcpyAsync(h_toff.data(), tile_off_.p, h_toff.size() * sizeof(int), cudaMemcpyDeviceToHost,
                           stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
-  std::vector<int> qoff(np + 1), prank(np);
-  for (int p = 0; p < np; p++) qoff[p] = h_toff[(size_t)p * tiles_x];
-  qoff[np] = (int)n;
+  std::vector<int> qoff(npairs_ + 1);
+  for (int p = 0; p < npairs_; p++) qoff[p] = h_toff[(size_t)p * tiles_x];
+  qoff[npairs_] = (int)nq_;
+  DedupQueries Q{nq_, qnode_.p, qdon_.p, nullptr, nullptr, qres_.p, x_.p, node_blk_.p};
+  TB_TRY(dedup_merge(Q, qoff));
+  dedup_ran_ = true;
+  return 0;
+}
+
+// The merge over any query list that is pair-major: node queries (keys from
+// the OBB bins) or the high-order path's points (keys from the point order).
+int Engine::dedup_merge(const DedupQueries& Qd, const std::vector<int>& qoff) {
+  const long long n = Qd.n;
+  const int np = npairs_;
+  std::vector<int> prank(np);
   const int nb = (int)hb_.size();
   std::vector<long long> dcount(nb, 0);
   std::vector<int> seen(nb, 0);
@@ -988,18 +989,24 @@ int Engine::run_dedup(int tiles_x) {
   TB_CUDA(q_gpos_.ensure(n));
   TB_CUDA(q_xt_.ensure(n));
   TB_CUDA(q_rep_.ensure(n));
-  k_dedup_keys<<<grid_for(n, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, n, dd_pqoff_.p, np, dd_prank_.p,
-                                                    node_bin_.p, dd_key_.p, dd_perm_.p);
-  TB_LAUNCHED("k_dedup_keys");
+  if (Qd.qpt_local) {
+    k_dedup_keys_pts<<<grid_for(n, kT), kT, 0, stream_>>>(Qd.qpt_local, Qd.qdon, n, dd_pqoff_.p, np, dd_prank_.p,
+                                                          dd_key_.p, dd_perm_.p);
+    TB_LAUNCHED("k_dedup_keys_pts");
+  } else {
+    k_dedup_keys<<<grid_for(n, kT), kT, 0, stream_>>>(Qd.qid, Qd.qdon, n, dd_pqoff_.p, np, dd_prank_.p,
+                                                      node_bin_.p, dd_key_.p, dd_perm_.p);
+    TB_LAUNCHED("k_dedup_keys");
+  }
   size_t tmp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64,
                                   stream_);
   TB_CUDA(cub_tmp_.ensure(tmp));
   cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64,
                                   stream_);
-  k_dedup_gather<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, qnode_.p, qres_.p, x_.p, node_blk_.p, d_bi_.p,
-                                                      dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p, dd_perm_.p,
-                                                      q_gpos_.p);
+  k_dedup_gather<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, Qd.qid, Qd.qres, Qd.coords, Qd.node_blk,
+                                                      Qd.qrec, d_bi_.p, dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p,
+                                                      dd_perm_.p, q_gpos_.p);
   TB_LAUNCHED("k_dedup_gather");
   // subsets: (start, count, splits so far); the donors' lists to begin with
   struct Seg {
@@ -1115,11 +1122,10 @@ int Engine::run_dedup(int tiles_x) {
         dd_leaves_.p, (int)leaves.size(), dd_perm_.p, dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p);
     TB_LAUNCHED("k_dedup_leaves");
   }
-  k_dedup_apply<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, dd_itag_.p, dd_rtag_.p, qres_.p, q_xt_.p,
-                                                     q_rep_.p, err_.p, counters_.p);
+  k_dedup_apply<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, dd_itag_.p, dd_rtag_.p, (double*)Qd.qres,
+                                                     q_xt_.p, q_rep_.p, err_.p, counters_.p);
   TB_LAUNCHED("k_dedup_apply");
   TB_CUDA(cudaStreamSynchronize(stream_));  // host staging vectors go out of scope
-  dedup_ran_ = true;
   return 0;
 }
 
@@ -1382,6 +1388,8 @@ int Engine::connectivity() {
     fprintf(stderr, "#tioga_b200: an interpolation weight fell outside [-0.2,1.2] (the reference aborts)\n");
   if (err & kErrFloodFillBound) fprintf(stderr, "#tioga_b200: hole-map fill hit its round limit\n");
   connected_ = true;
+  ihigh_global_ = ihigh_;  // tioga.C:138
+  ho_done_ = false;
   return 0;
 }
 

@@ -97,6 +97,35 @@ struct HoleMapInfo {
   double ext[6];
 };
 
+// High-order elements of one block: Lagrange hexahedra of degree p, DOF
+// coordinates element-major (caller-owned, re-read at every high-order call)
+struct HoBlockDesc {
+  int p = 0, npts = 0;
+  const double* hxdof = nullptr;
+};
+struct HoDev {  // per block, on the device
+  int p, npts;
+  long long dof_off;  // first DOF of the block in the concatenated DOF array
+};
+struct HoStats {
+  long long npoints = 0, ndonor = 0, nties = 0, nrecords = 0, nmerged = 0, norphan_cells = 0;
+};
+
+// A pair-major query list for the coincident-point merge: query q is point
+// qid[q] of `coords` with donor block qdon[q]; node queries give node_blk
+// (receptor block per node), point queries give qpt_local (the point's index
+// in its receptor block, the list order) and qrec (receptor block per query).
+struct DedupQueries {
+  long long n;
+  const int* qid;
+  const int* qdon;
+  const int* qpt_local;
+  const int* qrec;
+  const double* qres;
+  const double* coords;
+  const unsigned char* node_blk;
+};
+
 struct HostBlock {
   int tag = 0, nnodes = 0, ncells = 0, ntypes = 0;
   int nv[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
@@ -140,6 +169,14 @@ struct Timing {
 
 class Engine {
  public:
+  // high-order path
+  int set_highorder(int tag, int p, const double* xdof);
+  void set_highorder_callbacks() { ihigh_ = true; }
+  int connectivity_highorder();
+  int dataupdate_highorder(int nvar, int interptype);
+  int point_donors(int tag, int* out, double* w);
+  bool ihigh_global() const { return ihigh_global_; }
+  const HoStats& ho_stats() const { return ho_stats_; }
   Engine();
   ~Engine();
 
@@ -187,6 +224,8 @@ class Engine {
   int donor_rest_init();
   int dedup_gate();
   int run_dedup(int tiles_x);
+  int dedup_merge(const DedupQueries& Q, const std::vector<int>& qoff);
+  int traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count);
   int run_celliblank();
   int download_iblank();
   int fetch_interps();
@@ -251,6 +290,18 @@ class Engine {
   DBuf<unsigned char> dd_oct_;
   DBuf<int4> dd_chunks_, dd_leaves_;
   DBuf<int> dd_starts_, dd_pqoff_, dd_prank_;
+  // high-order path
+  std::vector<HoBlockDesc> ho_;
+  bool ihigh_ = false, ihigh_global_ = false, ho_done_ = false;
+  DBuf<HoDev> ho_dev_;
+  DBuf<double> ho_xdof_, ho_pts_, ho_qres_, ho_w_, ho_q_, ho_qtmp_;
+  DBuf<int> ho_ctag_, ho_rcblk_, ho_qpt_, ho_qloc_, ho_qdon_, ho_qrec_, ho_qbest_, ho_npass_, ho_qcell_, ho_win_;
+  DBuf<long long> ho_rcoff_d_, ho_ptoff_d_, ho_qoff_d_;
+  DBuf<int4> ho_rec_;
+  std::vector<long long> ho_rc_off_, ho_pt_off_;
+  long long ho_nrc_ = 0, ho_nq_ = 0, ho_nrecs_ = 0, ho_qcap_ = 0;
+  int ho_wstride_ = 1;
+  HoStats ho_stats_;
   int prev_nrec_ = 0;               // records of the previous call (their receptors are reset next call)
   bool donor_rest_ = false;         // per-node donor state is in its rest state
   DBuf<int> wall_list_, obc_list_;

@@ -1,0 +1,111 @@
+// Lagrange hexahedra of degree p with equispaced nodes: the element
+// arithmetic of the high-order path on the device.
+//
+// An element's (p+1)^3 degrees of freedom are stored element-major in
+// tensor order (node (i, j, k) at ((k (p+1) + j) (p+1) + i), i fastest),
+// with reference coordinates (r, s, t) in [0, 1]^3 and node (i, j, k) at
+// (i/p, j/p, k/p).  The inclusion test is Newton's method on the
+// isoparametric map from the element centre; the weights are the basis
+// functions at the inverted point.  Every operation is written out in a
+// fixed order (compiled without contraction), so the FP64 results are the
+// same bits as a host implementation of the same expressions.
+#pragma once
+
+namespace tb {
+
+constexpr int kHoMaxN = 11;          // (p+1) per axis at most: NFRAC = 1331 = 11^3 weights
+constexpr double kHoTol = 1e-10;     // inclusion tolerance in reference coordinates
+
+// 1-D Lagrange basis on the nodes i/p and its derivative
+__device__ inline void ho_basis1(int p, double r, double* l, double* dl) {
+  for (int i = 0; i <= p; i++) {
+    const double xi = (double)i / p;
+    double v = 1.0, d = 0.0;
+    for (int m = 0; m <= p; m++) {
+      if (m == i) continue;
+      const double xm = (double)m / p;
+      const double den = xi - xm;
+      d = d * ((r - xm) / den) + v / den;
+      v = v * ((r - xm) / den);
+    }
+    l[i] = v;
+    dl[i] = d;
+  }
+}
+
+// map and Jacobian of the element with DOF coordinates X at u
+__device__ inline void ho_map(int p, const double* __restrict__ X, const double u[3], double x[3],
+                              double J[3][3]) {
+  const int n1 = p + 1;
+  double lr[kHoMaxN], ls[kHoMaxN], lt[kHoMaxN], dr[kHoMaxN], ds[kHoMaxN], dt[kHoMaxN];
+  ho_basis1(p, u[0], lr, dr);
+  ho_basis1(p, u[1], ls, ds);
+  ho_basis1(p, u[2], lt, dt);
+  for (int a = 0; a < 3; a++) {
+    x[a] = 0.0;
+    J[a][0] = J[a][1] = J[a][2] = 0.0;
+  }
+  for (int k = 0; k < n1; k++)
+    for (int j = 0; j < n1; j++)
+      for (int i = 0; i < n1; i++) {
+        const double* P = X + 3 * ((k * n1 + j) * n1 + i);
+        const double w = (lr[i] * ls[j]) * lt[k];
+        const double wr = (dr[i] * ls[j]) * lt[k];
+        const double ws = (lr[i] * ds[j]) * lt[k];
+        const double wt = (lr[i] * ls[j]) * dt[k];
+        for (int a = 0; a < 3; a++) {
+          x[a] = x[a] + w * P[a];
+          J[a][0] = J[a][0] + wr * P[a];
+          J[a][1] = J[a][1] + ws * P[a];
+          J[a][2] = J[a][2] + wt * P[a];
+        }
+      }
+}
+
+// Newton inversion from the element centre; true when the update fell below
+// 1e-14 (sum of magnitudes) within 50 steps
+__device__ inline bool ho_invert(int p, const double* __restrict__ X, const double* xp, double u[3]) {
+  u[0] = u[1] = u[2] = 0.5;
+  for (int it = 0; it < 50; it++) {
+    double x[3], J[3][3];
+    ho_map(p, X, u, x, J);
+    const double f0 = xp[0] - x[0], f1 = xp[1] - x[1], f2 = xp[2] - x[2];
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    if (!(fabs(det) > 1e-300)) return false;
+    // Cramer's rule: du = J^-1 f
+    const double d0 = (f0 * c00 + f1 * (J[0][2] * J[2][1] - J[0][1] * J[2][2]) +
+                       f2 * (J[0][1] * J[1][2] - J[0][2] * J[1][1])) / det;
+    const double d1 = (f0 * c01 + f1 * (J[0][0] * J[2][2] - J[0][2] * J[2][0]) +
+                       f2 * (J[0][2] * J[1][0] - J[0][0] * J[1][2])) / det;
+    const double d2 = (f0 * c02 + f1 * (J[0][1] * J[2][0] - J[0][0] * J[2][1]) +
+                       f2 * (J[0][0] * J[1][1] - J[0][1] * J[1][0])) / det;
+    u[0] = u[0] + d0;
+    u[1] = u[1] + d1;
+    u[2] = u[2] + d2;
+    if (fabs(d0) + fabs(d1) + fabs(d2) < 1e-14) return true;
+  }
+  return false;
+}
+
+__device__ inline bool ho_inside(const double u[3]) {
+  return u[0] >= -kHoTol && u[0] <= 1.0 + kHoTol && u[1] >= -kHoTol && u[1] <= 1.0 + kHoTol &&
+         u[2] >= -kHoTol && u[2] <= 1.0 + kHoTol;
+}
+
+// the (p+1)^3 weights at u, tensor order
+__device__ inline void ho_weights(int p, const double u[3], double* w) {
+  const int n1 = p + 1;
+  double lr[kHoMaxN], ls[kHoMaxN], lt[kHoMaxN], d[kHoMaxN];
+  ho_basis1(p, u[0], lr, d);
+  ho_basis1(p, u[1], ls, d);
+  ho_basis1(p, u[2], lt, d);
+  int m = 0;
+  for (int k = 0; k < n1; k++)
+    for (int j = 0; j < n1; j++)
+      for (int i = 0; i < n1; i++, m++) w[m] = (lr[i] * ls[j]) * lt[k];
+}
+
+}  // namespace tb

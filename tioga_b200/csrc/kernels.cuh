@@ -177,9 +177,11 @@ __global__ void k_coin_check(const unsigned long long* key, const int* val, long
                              const unsigned char* node_blk, const BlockInfo* bi, unsigned* flag);
 __global__ void k_dedup_keys(const int* qnode, const int* qdon, long long nq, const int* pair_qoff, int npairs,
                              const int* pair_rank, const short* node_bin, unsigned long long* key, int* val);
+__global__ void k_dedup_keys_pts(const int* qpt_local, const int* qdon, long long nq, const int* pair_qoff,
+                                 int npairs, const int* pair_rank, unsigned long long* key, int* val);
 __global__ void k_dedup_gather(const int* refq, long long n, const int* qnode, const double* qres, const double* x,
-                               const unsigned char* node_blk, const BlockInfo* bi, double* xg, int* mtag,
-                               double* rtag, int* itag, int* perm, int* gpos_of);
+                               const unsigned char* node_blk, const int* qrec, const BlockInfo* bi, double* xg,
+                               int* mtag, double* rtag, int* itag, int* perm, int* gpos_of);
 __global__ void k_dedup_box(const int4* chunks, const int* perm, const double* xg, unsigned long long* box);
 __global__ void k_dedup_octant(const int4* chunks, const int* perm, const double* xg, const unsigned long long* box,
                                unsigned char* oct, int* cnt);

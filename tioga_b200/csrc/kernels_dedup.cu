@@ -157,18 +157,40 @@ __global__ void k_dedup_keys(const int* __restrict__ qnode, const int* __restric
   }
 }
 
+// the same for the high-order path's receptor points: within a pair the
+// donor list holds them in point order (getExtraQueryPoints, highOrder.C:272-319)
+__global__ void k_dedup_keys_pts(const int* __restrict__ qpt_local, const int* __restrict__ qdon, long long nq,
+                                 const int* __restrict__ pair_qoff, int npairs, const int* __restrict__ pair_rank,
+                                 unsigned long long* __restrict__ key, int* __restrict__ val) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
+       q += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = npairs - 1;
+    while (lo < hi) {
+      const int m = (lo + hi + 1) >> 1;
+      if (pair_qoff[m] <= q) lo = m;
+      else hi = m - 1;
+    }
+    key[q] = ((unsigned long long)qdon[q] << 56) | ((unsigned long long)pair_rank[lo] << 48) |
+             (unsigned long long)qpt_local[q];
+    val[q] = (int)q;
+  }
+}
+
 // gpos-indexed copies: point, receptor mesh tag, resolution, xtag = self
+// (query q is point qnode[q] of x; its receptor block is node_blk[qnode[q]],
+// or qrec[q] when node_blk is null)
 __global__ void k_dedup_gather(const int* __restrict__ refq, long long n, const int* __restrict__ qnode,
                                const double* __restrict__ qres, const double* __restrict__ x,
-                               const unsigned char* __restrict__ node_blk, const BlockInfo* __restrict__ bi,
-                               double* __restrict__ xg, int* __restrict__ mtag, double* __restrict__ rtag,
-                               int* __restrict__ itag, int* __restrict__ perm, int* __restrict__ gpos_of) {
+                               const unsigned char* __restrict__ node_blk, const int* __restrict__ qrec,
+                               const BlockInfo* __restrict__ bi, double* __restrict__ xg, int* __restrict__ mtag,
+                               double* __restrict__ rtag, int* __restrict__ itag, int* __restrict__ perm,
+                               int* __restrict__ gpos_of) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int q = refq[i];
     const int g = qnode[q];
     for (int k = 0; k < 3; k++) xg[3 * i + k] = x[3ll * g + k];
-    mtag[i] = bi[node_blk[g]].tag;
+    mtag[i] = bi[node_blk ? node_blk[g] : qrec[q]].tag;
     rtag[i] = qres[q];
     itag[i] = (int)i;
     perm[i] = (int)i;
