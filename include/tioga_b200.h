@@ -125,6 +125,26 @@ int tioga_b200_pointdonors_(int *btag, int *out, double *w);
  * cells changed by the orphan rule in the last data update. */
 void tioga_b200_highorder_stats_(long long out[8]);
 
+/* Batched form: the blocks of many independent overset systems in one
+ * instance, in place of the reference's one system per init ... delete
+ * sequence (driver/poisson_mms.f90:111-253 re-initialises per system).
+ * Registers a block of system *sys (>= 0) with the arguments of
+ * tioga_registergrid_data_ (src/tiogaInterface.C:84-105, cell types as the
+ * trailing varargs triples).  Each system has its own mesh tags and is
+ * connected exactly as if it were alone (pairs, hole maps, donor lists and
+ * iblank -meshtag values never cross systems), while every stage of
+ * preprocess, connectivity and data update is one launch over all systems.
+ * At most 16 blocks per system and 8192 in all; the high-order path takes
+ * one system per instance. */
+void tioga_b200_registergrid_sys_(int *sys, int *btag, int *nnodes, double *xyz, int *ibl, int *nwbc,
+                                  int *nobc, int *wbcnode, int *obcnode, int *ntypes, ...);
+/* The system whose mesh tags the tag-based calls (registergrid_data_,
+ * registersolution_, setresolutions_multi_, getdonorcount_/getdonorinfo_,
+ * the tioga_b200_ block calls) address from now on; 0 by default. */
+void tioga_b200_select_system_(int *sys);
+/* Systems registered in the instance. */
+int tioga_b200_nsystems_(void);
+
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);
 /* 1 when a CUDA device is present and the library initialised it. */

@@ -85,6 +85,38 @@ class TiogaLibrary:
         if block.tag not in self._order:
             self._order.append(block.tag)
 
+    def registergrid_sys(self, sys: int, bid: int, block):
+        """Register one cases.Block as block ``bid`` of overset system ``sys``
+        (tioga_b200_registergrid_sys_, the batched form)."""
+        x = np.ascontiguousarray(block.x, dtype=np.float64).reshape(-1)
+        ibl = np.ones(block.nnodes, dtype=np.int32)
+        wbc = np.ascontiguousarray(block.wbc, dtype=np.int32) + 1
+        obc = np.ascontiguousarray(block.obc, dtype=np.int32) + 1
+        args = []
+        for nv, conn in block.cells:
+            c1 = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1) + 1
+            nvc, ncc = C.c_int(int(nv)), C.c_int(int(conn.shape[0]))
+            self._keep += [nvc, ncc, c1]
+            args += [C.byref(nvc), C.byref(ncc), _ptr(c1)]
+        scalars = [C.c_int(sys), C.c_int(block.tag), C.c_int(block.nnodes), C.c_int(len(wbc)),
+                   C.c_int(len(obc)), C.c_int(len(block.cells))]
+        self._keep += [x, ibl, wbc, obc] + scalars
+        cs, ct, cn, cw, co, cty = scalars
+        self.lib.tioga_b200_registergrid_sys_(
+            C.byref(cs), C.byref(ct), C.byref(cn), _ptr(x), _ptr(ibl), C.byref(cw), C.byref(co), _ptr(wbc),
+            _ptr(obc), C.byref(cty), *args)
+        self.blocks[(sys, block.tag)] = {"x": x, "iblank": ibl, "nnodes": block.nnodes,
+                                         "ncells": block.ncells, "bid": bid}
+
+    def register_batch(self, systems):
+        """Every system of a batch, system k under id k."""
+        for k, system in enumerate(systems):
+            for bid, b in enumerate(system.blocks, start=1):
+                self.registergrid_sys(k, bid, b)
+
+    def select_system(self, sys: int):
+        self.lib.tioga_b200_select_system_(_iref(sys))
+
     def register_system(self, system, iblanks=None):
         for bid, b in enumerate(system.blocks, start=1):
             self.registergrid_data_mb(bid, b, None if iblanks is None else iblanks[bid - 1])
@@ -182,3 +214,39 @@ def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str =
             out["q"][b.tag] = q
     t.delete()
     return out
+
+
+def run_batch(lib_path: str, systems, q_sets=None, nvar: int = 5, itype: str = "row", setup=None):
+    """The batched form: every system registered in one instance
+    (tioga_b200_registergrid_sys_), one preprocess, one connectivity and one
+    data update for all of them.  Returns one result per system in the
+    layout of ``run_system``."""
+    t = TiogaLibrary(lib_path)
+    t.init()
+    t.register_batch(systems)
+    if setup is not None:
+        setup(t)
+    t.preprocess_grids()
+    t.performconnectivity()
+    outs = []
+    for k, system in enumerate(systems):
+        t.select_system(k)
+        out = {"iblank": {}, "donors": {}, "q": {}}
+        for b in system.blocks:
+            out["iblank"][b.tag] = t.blocks[(k, b.tag)]["iblank"].copy()
+            out["donors"][b.tag] = t.getdonorinfo(b.tag)
+        outs.append(out)
+    if q_sets is not None:
+        qs = []
+        for k, system in enumerate(systems):
+            t.select_system(k)
+            qk = [np.array(q, dtype=np.float64, copy=True) for q in q_sets[k]]
+            for b, q in zip(system.blocks, qk):
+                t.registersolution(b.tag, q)
+            qs.append(qk)
+        t.dataupdate_mb(nvar, itype)
+        for k, system in enumerate(systems):
+            for b, q in zip(system.blocks, qs[k]):
+                outs[k]["q"][b.tag] = q
+    t.delete()
+    return outs

@@ -419,6 +419,53 @@ def linear_fields(system: System, nvar: int = 5) -> list:
     return out
 
 
+def batch_system(rng: np.random.Generator, nnodes: float, nshell: int, mixed: bool, name: str = "") -> System:
+    """One system of the batched workload: a background box on [-5,5]^3 plus
+    ``nshell`` shells built as in config0 (radial ratio 1.1, outer radius 4x
+    the wall radius U(0.3, 0.6), centres within |x|<=3), about ``nnodes``
+    nodes in all (60% background, the rest shared by the shells).  All-hex
+    systems get config0's +-5% jitter; mixed-element ones split the
+    background's z<0 hexes into prisms and the shells' first radial layers
+    into tets, prisms or pyramids (config1), without jitter."""
+    nbg = max(9, int(round((0.6 * nnodes) ** (1.0 / 3.0))))
+    nt = max(5, int(round((0.4 * nnodes / nshell / 2.0) ** (1.0 / 3.0))))
+    nr, nphi = nt, 2 * nt - 1
+    perturb = 0.0 if mixed else 0.05
+    xb, cb = hex_box(nbg, -5.0, 5.0, perturb, rng if perturb > 0 else None, split_prism_zneg=mixed)
+    blocks = [Block(1, xb, cb, _empty_i32(), _empty_i32(), name="background")]
+    rwall = rng.uniform(0.3, 0.6, nshell)
+    router = 4.0 * rwall
+    centres = shell_centres(rng, nshell, rwall, router)
+    split = min(4, max(1, nr // 4)) if mixed else 0
+    for a in range(nshell):
+        xs, cs, wall, outer, _ = sphere_shell(nr, nt, nphi, rwall[a], router[a], 1.1, centres[a], perturb, rng,
+                                              split)
+        blocks.append(Block(2 + a, xs, cs, wall, outer, name=f"shell{a}"))
+    return System(blocks, name=name or f"batch(nbg={nbg},{nshell}x{nr}x{nt}x{nphi},mixed={mixed})",
+                  meta={"centres": centres.tolist(), "rwall": rwall.tolist(), "mixed": mixed})
+
+
+def config2(seed: int = 2, nsys: int = 64, nmin: float = 5e4, nmax: float = 2e6) -> list:
+    """Batched workload: ``nsys`` independent overset systems, each a
+    background box plus 1-4 shells (batch_system), with node counts drawn
+    log-uniformly in [nmin, nmax] and all-hex or mixed-element with
+    probability 0.5, from one seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(nsys):
+        n = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        nshell = int(rng.integers(1, 5))
+        mixed = bool(rng.uniform() < 0.5)
+        out.append(batch_system(rng, n, nshell, mixed, name=f"cfg2[{k}](n~{int(n)},{nshell} shells,"
+                                f"{'mixed' if mixed else 'hex'})"))
+    return out
+
+
+def small_config2(seed: int = 2, nsys: int = 6) -> list:
+    """The batched workload at test size: systems of 3e3 to 2e4 nodes."""
+    return config2(seed, nsys=nsys, nmin=3e3, nmax=2e4)
+
+
 CONFIGS = {
     "cfg0": config0,
     "cfg1": config1,

@@ -52,7 +52,8 @@ void register_va(int btag, int nnodes, double* xyz, int* ibl, int nwbc, int nobc
     nc[i] = *va_arg(ap, int*);
     conn[i] = va_arg(ap, int*);
   }
-  set_rc(g_tg->register_block(btag, nnodes, xyz, ibl, nwbc, nobc, wbc, obc, ntypes, nv, nc, conn));
+  set_rc(g_tg->register_block_sys(g_tg->selected_system(), btag, nnodes, xyz, ibl, nwbc, nobc, wbc, obc, ntypes,
+                                  nv, nc, conn));
 }
 
 void unsupported(const char* fn) {
@@ -95,6 +96,22 @@ void tioga_registergrid_data_mb_(int* bid, int* btag, int* nnodes, double* xyz, 
   register_va(*btag, *nnodes, xyz, ibl, *nwbc, *nobc, wbcnode, obcnode, *ntypes, ap);
   va_end(ap);
 }
+
+void tioga_b200_registergrid_sys_(int* sys, int* btag, int* nnodes, double* xyz, int* ibl, int* nwbc, int* nobc,
+                                  int* wbcnode, int* obcnode, int* ntypes, ...) {
+  if (!ready("tioga_b200_registergrid_sys_")) return;
+  g_tg->select_system(*sys);
+  va_list ap;
+  va_start(ap, ntypes);
+  register_va(*btag, *nnodes, xyz, ibl, *nwbc, *nobc, wbcnode, obcnode, *ntypes, ap);
+  va_end(ap);
+}
+
+void tioga_b200_select_system_(int* sys) {
+  if (ready("tioga_b200_select_system_")) g_tg->select_system(*sys);
+}
+
+int tioga_b200_nsystems_(void) { return g_tg ? g_tg->nsystems() : 0; }
 
 void tioga_preprocess_grids_(void) {
   if (ready("tioga_preprocess_grids_")) set_rc(g_tg->preprocess());

@@ -19,6 +19,7 @@ constexpr double kTol = 1.0e-10;      // TOL, src/codetypes.h:54
 constexpr int kHoleMapSize = 192;     // HOLEMAPSIZE, src/codetypes.h:55
 constexpr int kBigInt = 2147483647;   // BIGINT, src/codetypes.h:53
 constexpr int kMaxNv = 8;
+typedef unsigned short blk_t;        // block index of a node or cell
 
 // error word bits (device-side failures are reported, never trapped)
 enum : unsigned {

@@ -40,7 +40,7 @@ Engine::~Engine() {
   obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
   wall_list_.release(); obc_list_.release(); csr_off_.release(); csr_cell_.release(); deg_.release();
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
-  for (auto& h : hm_state_) h.release();
+  hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
   xf_.release(); leaves_.release(); gparent_.release(); gnk_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
@@ -51,6 +51,8 @@ Engine::~Engine() {
   it_don_.release(); it_nv_.release(); it_cancel_.release(); rres_.release(); q_.release();
   qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
+  d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
+  d_wall_.release();
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -60,16 +62,31 @@ void Engine::set_stream(cudaStream_t s) {
   stream_ = s ? s : own_stream_;
 }
 
-int Engine::find_tag(int tag) const {
-  auto it = tag2idx_.find(tag);
+int Engine::find_tag(int tag) const { return find_block(cur_sys_, tag); }
+
+int Engine::nsystems() const {
+  int n = 0;
+  for (size_t b = 0; b < hb_.size(); b++) n += (b == 0 || hb_[b].sys != hb_[b - 1].sys);
+  return n;
+}
+
+int Engine::find_block(int sys, int tag) const {
+  auto it = tag2idx_.find(((long long)sys << 32) | (unsigned)tag);
   return it == tag2idx_.end() ? -1 : it->second;
 }
 
 // src/tioga.C:64-86 + MeshBlock.C:37-72: one block per mesh tag; a second
 // registration of a tag replaces that block's data.  Pointers stay the
-// caller's.
+// caller's.  Blocks of several independent overset systems may share one
+// engine (system ids >= 0, each with its own tags); the blocks are kept
+// grouped by system, in registration order within a system.
 int Engine::register_block(int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
                            int* obc, int ntypes, const int* nv, const int* nc, int** conn) {
+  return register_block_sys(0, tag, nnodes, x, ibl, nwbc, nobc, wbc, obc, ntypes, nv, nc, conn);
+}
+
+int Engine::register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
+                               int* obc, int ntypes, const int* nv, const int* nc, int** conn) {
   if (ntypes < 1 || ntypes > 4) {
     fprintf(stderr, "#tioga_b200: %d cell types given, 1..4 supported\n", ntypes);
     return -1;
@@ -83,17 +100,35 @@ int Engine::register_block(int tag, int nnodes, double* x, int* ibl, int nwbc, i
     fprintf(stderr, "#tioga_b200: mesh tags must lie in 1..128 (got %d)\n", tag);
     return -1;
   }
-  int ib = find_tag(tag);
+  if (sys < 0) {
+    fprintf(stderr, "#tioga_b200: system ids must be >= 0 (got %d)\n", sys);
+    return -1;
+  }
+  int ib = find_block(sys, tag);
   if (ib < 0) {
-    if ((int)hb_.size() >= 16) {
-      fprintf(stderr, "#tioga_b200: at most 16 blocks per instance\n");
+    int in_sys = 0;
+    for (const HostBlock& H : hb_) in_sys += (H.sys == sys);
+    if (in_sys >= kMaxSysBlocks) {
+      fprintf(stderr, "#tioga_b200: at most %d blocks per system\n", kMaxSysBlocks);
       return -1;
     }
-    hb_.emplace_back();
-    ib = (int)hb_.size() - 1;
-    tag2idx_[tag] = ib;
+    if ((int)hb_.size() >= kMaxEngineBlocks) {
+      fprintf(stderr, "#tioga_b200: at most %d blocks per instance\n", kMaxEngineBlocks);
+      return -1;
+    }
+    // after the last block of a system with an id <= sys
+    int pos = (int)hb_.size();
+    while (pos > 0 && hb_[pos - 1].sys > sys) pos--;
+    hb_.insert(hb_.begin() + pos, HostBlock{});
+    if (pos < (int)ho_.size()) ho_.insert(ho_.begin() + pos, HoBlockDesc{});
+    tag2idx_.clear();
+    for (int b = 0; b < (int)hb_.size(); b++)
+      if (b != pos) tag2idx_[((long long)hb_[b].sys << 32) | (unsigned)hb_[b].tag] = b;
+    tag2idx_[((long long)sys << 32) | (unsigned)tag] = pos;
+    ib = pos;
   }
   HostBlock& b = hb_[ib];
+  b.sys = sys;
   b.tag = tag;
   b.nnodes = nnodes;
   b.hx = x;
@@ -188,11 +223,29 @@ int Engine::upload_topology() {
     nobcn += H.nobc;
     maxtag_ = std::max(maxtag_, H.tag);
   }
+  // systems: consecutive block ranges; one hole map per wall-bearing block,
+  // numbered in block order so that a system's maps are consecutive too
+  nhm_all_ = 0;
+  K_ = 1;
+  for (int b = 0; b < nb;) {
+    int e = b;
+    while (e < nb && hb_[e].sys == hb_[b].sys) e++;
+    const int lo = nhm_all_;
+    for (int k = b; k < e; k++) bi_[k].hm = hb_[k].nwbc > 0 ? nhm_all_++ : -1;
+    for (int k = b; k < e; k++) {
+      bi_[k].sys = hb_[k].sys;
+      bi_[k].sblk0 = b;
+      bi_[k].snb = e - b;
+      bi_[k].hm_lo = lo;
+      bi_[k].hm_hi = nhm_all_;
+    }
+    K_ = std::max(K_, e - b);
+    b = e;
+  }
   if (ntot_ >= (1ll << 31) || ctot_ >= (1ll << 31)) {
     fprintf(stderr, "#tioga_b200: more than 2^31 nodes or cells\n");
     return -1;
   }
-  K_ = nb;
   TB_CUDA(x_.ensure(3 * ntot_));
   TB_CUDA(node_res_.ensure(ntot_));
   TB_CUDA(iblank_.ensure(ntot_));
@@ -260,18 +313,31 @@ int Engine::upload_topology() {
   }
   stg.release();
   TB_TRY(build_csr());
-  // hole map state buffers for every wall-bearing tag
-  hm_state_.resize(maxtag_);
-  std::vector<HoleMapDev> hmd;
-  for (int b = 0; b < nb; b++) {
-    if (hb_[b].nwbc <= 0) continue;
-    int t = hb_[b].tag - 1;
-    const size_t cap = 197ull * 197ull * 197ull;
-    TB_CUDA(hm_state_[t].ensure(cap));
-  }
-  TB_CUDA(d_hm_.ensure(maxtag_));
-  TB_CUDA(wall_bb_.ensure(6 * maxtag_));
-  TB_CUDA(d_hmdev_.ensure(maxtag_));
+  // block pairs that may intersect: different mesh tags of one system, donor
+  // outer, receptor inner (exchangeBoxes.C:133-160)
+  std::vector<int2> cand;
+  for (int ob = 0; ob < nb; ob++)
+    for (int ib = bi_[ob].sblk0; ib < bi_[ob].sblk0 + bi_[ob].snb; ib++)
+      if (hb_[ib].tag != hb_[ob].tag) cand.push_back(make_int2(ob, ib));
+  npcand_ = (int)cand.size();
+  TB_CUDA(d_pcand_.ensure(std::max(npcand_, 1)));
+  if (npcand_ > 0)
+    TB_CUDA(cudaMemcpyAsync(d_pcand_.p, cand.data(), cand.size() * sizeof(int2), cudaMemcpyHostToDevice, stream_));
+  // wall-bearing blocks
+  h_wall_.clear();
+  for (int b = 0; b < nb; b++)
+    if (bi_[b].hm >= 0)
+      h_wall_.push_back(WallBlock{bi_[b].wall_off, bi_[b].nwbc, bi_[b].cell_off, bi_[b].ncells, bi_[b].hm});
+  TB_CUDA(d_wall_.ensure(std::max<size_t>(h_wall_.size(), 1)));
+  if (!h_wall_.empty())
+    TB_CUDA(cudaMemcpyAsync(d_wall_.p, h_wall_.data(), h_wall_.size() * sizeof(WallBlock), cudaMemcpyHostToDevice,
+                            stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above go out of scope
+  // hole map state: one fixed-size slab per wall-bearing block
+  if (nhm_all_ > 0) TB_CUDA(hm_state_.ensure((size_t)nhm_all_ * kHoleMapCap));
+  TB_CUDA(d_hm_.ensure(std::max(nhm_all_, 1)));
+  TB_CUDA(wall_bb_.ensure(6 * std::max(nhm_all_, 1)));
+  TB_CUDA(d_hmdev_.ensure(std::max(nhm_all_, 1)));
   topo_dirty_ = false;
   interps_fetched_ = false;
   return 0;
@@ -309,24 +375,17 @@ int Engine::upload_coords() {
 }
 
 int Engine::compute_obbs() {
+  // every block at once: 148 CTAs per block, three passes (sums, covariance,
+  // projections), each finished by one thread per block
   const int nparts = 148;
-  TB_CUDA(red_.ensure(12 * nparts));
-  for (size_t b = 0; b < hb_.size(); b++) {
-    const BlockInfo& B = bi_[b];
-    Obb* dobb = &d_bi_.p[b].obb;
-    int n = B.nnodes;
-    if (n == 0) continue;
-    for (int pass = 0; pass < 3; pass++) {
-      if (pass == 1 && n < 4) break;
-      k_obb_partial<<<nparts, 256, 0, stream_>>>(x_.p, B.node_off, n, pass, dobb, red_.p);
-      TB_LAUNCHED("k_obb_partial");
-      k_obb_finish<<<1, 1, 0, stream_>>>(red_.p, nparts, n, pass, x_.p, B.node_off, dobb, &d_bi_.p[b]);
-      TB_LAUNCHED("k_obb_finish");
-    }
-    if (n < 4) {  // the raw box is still needed for the Morton keys
-      k_obb_partial<<<nparts, 256, 0, stream_>>>(x_.p, B.node_off, n, 2, dobb, red_.p);
-      TB_LAUNCHED("k_obb_partial");
-    }
+  const int nb = (int)hb_.size();
+  if (nb == 0) return 0;
+  TB_CUDA(red_.ensure(12 * (size_t)nparts * nb));
+  for (int pass = 0; pass < 3; pass++) {
+    k_obb_partial<<<dim3(nparts, nb), 256, 0, stream_>>>(x_.p, d_bi_.p, pass, red_.p);
+    TB_LAUNCHED("k_obb_partial");
+    k_obb_finish<<<(nb + 127) / 128, 128, 0, stream_>>>(red_.p, nparts, pass, x_.p, d_bi_.p, nb);
+    TB_LAUNCHED("k_obb_finish");
   }
   return 0;
 }
@@ -344,11 +403,13 @@ int Engine::build_tree_topology() {
                                                     ctot_, mkey_.p, mval_alt_.p);
   TB_LAUNCHED("k_morton");
   size_t tmp = 0;
+  int key_bits = 32;  // 30-bit Morton code, block id from bit 32
+  while ((1ll << (key_bits - 32)) < (long long)bi_.size()) key_bits++;
   cub::DeviceRadixSort::SortPairs(nullptr, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
-                                  (int)ctot_, 0, 40, stream_);
+                                  (int)ctot_, 0, key_bits, stream_);
   TB_CUDA(cub_tmp_.ensure(tmp));
   cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, mkey_.p, mkey_alt_.p, mval_alt_.p, sorted_cell_.p,
-                                  (int)ctot_, 0, 40, stream_);
+                                  (int)ctot_, 0, key_bits, stream_);
   // From here on every cell array is in storage (Morton) order; sorted_cell_
   // maps a storage position to the caller's cell id and inv_sorted_ back.
   TB_CUDA(inv_sorted_.ensure(ctot_));
@@ -356,7 +417,8 @@ int Engine::build_tree_topology() {
   TB_LAUNCHED("k_invert");
   {
     DBuf<int> conn2;
-    DBuf<unsigned char> nv2, blk2;
+    DBuf<unsigned char> nv2;
+    DBuf<blk_t> blk2;
     TB_CUDA(conn2.ensure(8 * ctot_));
     TB_CUDA(nv2.ensure(ctot_));
     TB_CUDA(blk2.ensure(ctot_));
@@ -384,9 +446,11 @@ int Engine::build_tree_topology() {
     k_morton_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, k0.p, v0.p);
     TB_LAUNCHED("k_morton_nodes");
     size_t tmpn = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, 40, stream_);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, key_bits,
+                                    stream_);
     TB_CUDA(cub_tmp_.ensure(tmpn));
-    cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, 40, stream_);
+    cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmpn, k0.p, k1.p, v0.p, node_order_.p, (int)ntot_, 0, key_bits,
+                                    stream_);
     TB_CUDA(cudaStreamSynchronize(stream_));
     k0.release();
     k1.release();
@@ -509,7 +573,19 @@ int Engine::build_tree_topology() {
     k_leaf_list<<<grid_for(ctot_, kT), kT, 0, stream_>>>(leaf_at.p, loff.p, ctot_, tlink.p, cell_blk_.p,
                                                          leaves_.p);
     TB_LAUNCHED("k_leaf_list");
+    // leaves of block b: [blk_leaf_[b], blk_leaf_[b + 1])
+    DBuf<int> first;
+    TB_CUDA(first.ensure(nb));
+    TB_CUDA(cudaMemsetAsync(first.p, 0xff, nb * sizeof(int), stream_));
+    if (nl > 0) {
+      k_block_leaves<<<grid_for(nl, kT), kT, 0, stream_>>>(leaves_.p, nl, first.p);
+      TB_LAUNCHED("k_block_leaves");
+    }
+    h_blk_leaf_.assign(nb + 1, nl);
+    TB_CUDA(cudaMemcpyAsync(h_blk_leaf_.data(), first.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
+    for (int b = nb - 1; b >= 0; b--)
+      if (h_blk_leaf_[b] < 0) h_blk_leaf_[b] = h_blk_leaf_[b + 1];
   }
   // query-gathering tiles of kNodeTile nodes per block
   h_tile_base_.assign(bi_.size() + 1, 0);
@@ -604,101 +680,104 @@ int Engine::preprocess() {
 // connectivity (src/tioga.C:112-160)
 // ---------------------------------------------------------------------------
 int Engine::run_holemaps() {
-  // wall bounds per mesh tag -> extents and sizes -> mark -> fill
-  std::vector<unsigned long long> init(6 * maxtag_);
-  for (int t = 0; t < maxtag_; t++)
-    for (int j = 0; j < 6; j++) init[6 * t + j] = 0;
-  for (int t = 0; t < maxtag_; t++) {
-    // identity elements of min (all ones) and max (zero) over ordered keys
-    for (int j = 0; j < 3; j++) init[6 * t + j] = ~0ull;
-  }
+  // every wall-bearing block's map at once: wall bounds -> extents and sizes
+  // -> mark -> fill -> final
+  const int nh = nhm_all_;
+  nhm_ = 0;
+  if (nh == 0) return 0;
+  std::vector<unsigned long long> init(6 * (size_t)nh);
+  for (int t = 0; t < nh; t++)
+    for (int j = 0; j < 3; j++) {  // identity elements of min (all ones) and max (zero) over ordered keys
+      init[6 * t + j] = ~0ull;
+      init[6 * t + j + 3] = 0ull;
+    }
   TB_CUDA(cudaMemcpyAsync(wall_bb_.p, init.data(), init.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  std::vector<HoleMapInfo> hinfo(maxtag_);
-  for (auto& h : hinfo) h.exist = 0;
-  TB_CUDA(cudaMemcpyAsync(d_hm_.p, hinfo.data(), maxtag_ * sizeof(HoleMapInfo), cudaMemcpyHostToDevice,
-                          stream_));
-  std::vector<HoleMapDev> hdev;
-  for (size_t b = 0; b < hb_.size(); b++) {
-    const BlockInfo& B = bi_[b];
-    if (B.nwbc <= 0) continue;
-    int t = B.tag - 1;
-    k_wall_bounds<<<grid_for(B.nwbc, kT, 148), kT, 0, stream_>>>(x_.p, wall_list_.p, B.wall_off, B.nwbc,
-                                                                 wall_bb_.p + 6 * t);
-    TB_LAUNCHED("k_wall_bounds");
+  const unsigned nw = (unsigned)h_wall_.size();
+  int maxw = 1, maxc = 1;
+  for (const WallBlock& W : h_wall_) {
+    maxw = std::max(maxw, W.nwall);
+    maxc = std::max(maxc, W.ncells);
   }
-  for (size_t b = 0; b < hb_.size(); b++) {
-    const BlockInfo& B = bi_[b];
-    if (B.nwbc <= 0) continue;
-    int t = B.tag - 1;
-    k_holemap_setup<<<1, 1, 0, stream_>>>(wall_bb_.p, d_hm_.p, t);
-    TB_LAUNCHED("k_holemap_setup");
-    TB_CUDA(cudaMemsetAsync(hm_state_[t].p, 0, hm_state_[t].n, stream_));
-    k_holemap_mark<<<grid_for(B.ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, B.cell_off,
-                                                               B.ncells, wallf_.p, d_hm_.p + t,
-                                                               hm_state_[t].p);
-    TB_LAUNCHED("k_holemap_mark");
-  }
-  TB_CUDA(cudaMemcpyAsync(hinfo.data(), d_hm_.p, maxtag_ * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost,
-                          stream_));
+  k_wall_bounds<<<dim3(grid_for(maxw, kT, 148), nw), kT, 0, stream_>>>(x_.p, wall_list_.p, d_wall_.p, wall_bb_.p);
+  TB_LAUNCHED("k_wall_bounds");
+  k_holemap_setup<<<(nh + 127) / 128, 128, 0, stream_>>>(wall_bb_.p, d_hm_.p, nh);
+  TB_LAUNCHED("k_holemap_setup");
+  TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nh * kHoleMapCap, stream_));
+  k_holemap_mark<<<dim3(grid_for(maxc, kT), nw), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, d_wall_.p, wallf_.p,
+                                                                 d_hm_.p, hm_state_.p, kHoleMapCap);
+  TB_LAUNCHED("k_holemap_mark");
+  std::vector<HoleMapInfo> hinfo(nh);
+  TB_CUDA(cudaMemcpyAsync(hinfo.data(), d_hm_.p, nh * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
-  for (int t = 0; t < maxtag_; t++) {
+  const int isym = isym_;
+  const bool planar = (isym == 1 || isym == 2 || isym == 3);
+  const int pa = (isym == 1) ? 0 : (isym == 2) ? 1 : 2;
+  const int a0 = (pa == 0) ? 1 : 0, a1 = (pa == 2) ? 1 : 2;
+  int maxpl = 1;
+  size_t smem = 1;
+  long long maxcells = 1;
+  for (int t = 0; t < nh; t++) {
     const HoleMapInfo& h = hinfo[t];
-    if (!h.exist) continue;
     if (h.nx[0] > 197 || h.nx[1] > 197 || h.nx[2] > 197 || h.nx[0] < 1 || h.nx[1] < 1 || h.nx[2] < 1) {
-      fprintf(stderr, "#tioga_b200: hole map of mesh %d has an unexpected size\n", t + 1);
+      fprintf(stderr, "#tioga_b200: hole map %d has an unexpected size\n", t);
       return -1;
     }
-    int isym = isym_;
-    bool planar = (isym == 1 || isym == 2 || isym == 3);
-    int pa = (isym == 1) ? 0 : (isym == 2) ? 1 : 2;
-    int a0 = (pa == 0) ? 1 : 0, a1 = (pa == 2) ? 1 : 2;
-    size_t smem = (size_t)h.nx[a0] * h.nx[a1];
-    k_holemap_fill_planes<<<std::min(h.nx[pa], 148 * 4), 256, smem, stream_>>>(
-        hm_state_[t].p, d_hm_.p + t, planar ? isym : 3, planar ? 0 : 1, nullptr, err_.p);
-    TB_LAUNCHED("k_holemap_fill_planes");
-    if (!planar) {  // 6-neighbour fill: line sweeps over the three axes
-      unsigned* d_changed = err_.p + 1;
-      for (int round = 0; round < 4 * (h.nx[0] + h.nx[1] + h.nx[2]); round++) {
-        TB_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(unsigned), stream_));
-        for (int axis = 0; axis < 3; axis++) {
-          k_holemap_lines<<<grid_for((long long)h.nx[0] * h.nx[1] * h.nx[2] / 64 + 1, kT), kT, 0,
-                            stream_>>>(hm_state_[t].p, d_hm_.p + t, axis, d_changed);
-          TB_LAUNCHED("k_holemap_lines");
-        }
-        unsigned ch = 0;
-        TB_CUDA(cudaMemcpyAsync(&ch, d_changed, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-        TB_CUDA(cudaStreamSynchronize(stream_));
-        if (!ch) break;
-      }
-    }
-    k_holemap_final<<<grid_for((long long)h.nx[0] * h.nx[1] * h.nx[2], kT), kT, 0, stream_>>>(
-        hm_state_[t].p, d_hm_.p + t);
-    TB_LAUNCHED("k_holemap_final");
-    HoleMapDev d;
-    d.tagidx = t;
-    for (int j = 0; j < 3; j++) d.nx[j] = h.nx[j];
-    for (int j = 0; j < 6; j++) d.ext[j] = h.ext[j];
-    d.hole = hm_state_[t].p;
-    hdev.push_back(d);
+    maxpl = std::max(maxpl, h.nx[pa]);
+    smem = std::max(smem, (size_t)h.nx[a0] * h.nx[a1]);
+    maxcells = std::max(maxcells, (long long)h.nx[0] * h.nx[1] * h.nx[2]);
   }
-  nhm_ = (int)hdev.size();
-  if (nhm_ > 0)
-    TB_CUDA(cudaMemcpyAsync(d_hmdev_.p, hdev.data(), nhm_ * sizeof(HoleMapDev), cudaMemcpyHostToDevice,
-                            stream_));
+  k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, stream_>>>(
+      hm_state_.p, d_hm_.p, kHoleMapCap, planar ? isym : 3, planar ? 0 : 1, err_.p);
+  TB_LAUNCHED("k_holemap_fill_planes");
+  if (!planar) {  // 6-neighbour fill: line sweeps over the three axes until no map changes
+    unsigned* d_changed = err_.p + 1;
+    int maxsum = 0;
+    for (const HoleMapInfo& h : hinfo) maxsum = std::max(maxsum, h.nx[0] + h.nx[1] + h.nx[2]);
+    for (int round = 0; round < 4 * maxsum; round++) {
+      TB_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(unsigned), stream_));
+      for (int axis = 0; axis < 3; axis++) {
+        k_holemap_lines<<<dim3(grid_for(maxcells / 64 + 1, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p,
+                                                                                      kHoleMapCap, axis, d_changed);
+        TB_LAUNCHED("k_holemap_lines");
+      }
+      unsigned ch = 0;
+      TB_CUDA(cudaMemcpyAsync(&ch, d_changed, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      TB_CUDA(cudaStreamSynchronize(stream_));
+      if (!ch) break;
+    }
+  }
+  k_holemap_final<<<dim3(grid_for(maxcells, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p, kHoleMapCap);
+  TB_LAUNCHED("k_holemap_final");
+  std::vector<HoleMapDev> hdev(nh);
+  for (int b = 0; b < (int)bi_.size(); b++) {
+    const int t = bi_[b].hm;
+    if (t < 0) continue;
+    HoleMapDev& d = hdev[t];
+    d.tagidx = bi_[b].tag - 1;
+    for (int j = 0; j < 3; j++) d.nx[j] = hinfo[t].nx[j];
+    for (int j = 0; j < 6; j++) d.ext[j] = hinfo[t].ext[j];
+    d.hole = hm_state_.p + (size_t)t * kHoleMapCap;
+  }
+  nhm_ = nh;
+  TB_CUDA(cudaMemcpyAsync(d_hmdev_.p, hdev.data(), nh * sizeof(HoleMapDev), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));  // host tables go out of scope
   return 0;
 }
 
 int Engine::run_pairs_and_refit() {
   const int nb = (int)hb_.size();
-  TB_CUDA(d_pairs_.ensure(nb * nb + 1));
+  TB_CUDA(d_pairs_.ensure(npcand_ + 1));
   TB_CUDA(d_npairs_.ensure(1));
-  k_pairs<<<1, 1, 0, stream_>>>(d_bi_.p, nb, d_pairs_.p, d_npairs_.p);
+  TB_CUDA(d_pfirst_.ensure(nb + 1));
+  k_pairs<<<1, 1024, 0, stream_>>>(d_bi_.p, nb, d_pcand_.p, npcand_, d_pairs_.p, d_npairs_.p, d_pfirst_.p);
   TB_LAUNCHED("k_pairs");
   TB_CUDA(cudaMemcpyAsync(&npairs_, d_npairs_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
-  h_pairs_.resize(nb * nb + 1);
-  TB_CUDA(cudaMemcpyAsync(h_pairs_.data(), d_pairs_.p, (nb * nb + 1) * sizeof(PairInfo),
-                          cudaMemcpyDeviceToHost, stream_));
+  h_pairs_.resize(npcand_ + 1);
+  h_pfirst_.resize(nb + 1);
+  TB_CUDA(cudaMemcpyAsync(h_pairs_.data(), d_pairs_.p, (npcand_ + 1) * sizeof(PairInfo), cudaMemcpyDeviceToHost,
+                          stream_));
+  TB_CUDA(cudaMemcpyAsync(h_pfirst_.data(), d_pfirst_.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   // FP32 coordinates and the node tiles' boxes (query gathering, hole search)
   TB_CUDA(xf_.ensure(ntot_));
@@ -736,19 +815,36 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
-  TB_CUDA(cudaEventRecord(cev_[0], stream_));
-  // pairs in chunks that fit one CTA's shared memory; the first launch also
-  // writes the cell and leaf boxes
-  const int chunk = 256;
-  for (int p0 = 0; p0 < npairs_; p0 += chunk) {
-    const int np = std::min(chunk, npairs_ - p0);
-    const size_t smem = (size_t)np * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
-    launch_cell_pass(fp64, grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3), smem, stream_, x_.p, xf_.p,
-                     conn8_.p, cell_nv_.p, d_bi_.p, nb, leaves_.p, nleaf_total_, d_pairs_.p, p0, np,
-                     p0 == 0 ? 1 : 0, cbox_.p, fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr,
-                     pair_acc_.p);
-    TB_LAUNCHED("k_cell_pass");
+  // chunks of consecutive blocks whose pairs fit one CTA's shared memory;
+  // the CTAs of one launch are split among the chunks by leaf count
+  constexpr int kChunkPairs = 128;
+  std::vector<int4> chunks;
+  for (int b = 0; b < nb;) {
+    int e = b + 1;
+    while (e < nb && h_pfirst_[e + 1] - h_pfirst_[b] <= kChunkPairs) e++;
+    chunks.push_back(make_int4(h_blk_leaf_[b], h_blk_leaf_[e], h_pfirst_[b], h_pfirst_[e] - h_pfirst_[b]));
+    b = e;
   }
+  const long long want = grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3);
+  std::vector<int> ccta(chunks.size() + 1, 0);
+  int maxnp = 1;
+  for (size_t k = 0; k < chunks.size(); k++) {
+    const long long nl = chunks[k].y - chunks[k].x;
+    long long n = nleaf_total_ > 0 ? (want * nl + nleaf_total_ - 1) / nleaf_total_ : 1;
+    n = std::max(1ll, std::min(n, (nl * kMaxLeafCells + 255) / 256));
+    ccta[k + 1] = ccta[k] + (int)n;
+    maxnp = std::max(maxnp, chunks[k].w);
+  }
+  TB_CUDA(d_chunks_.ensure(chunks.size()));
+  TB_CUDA(d_chunk_cta_.ensure(ccta.size()));
+  TB_CUDA(cudaMemcpyAsync(d_chunks_.p, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaMemcpyAsync(d_chunk_cta_.p, ccta.data(), ccta.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaEventRecord(cev_[0], stream_));
+  const size_t smem = (size_t)maxnp * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
+  launch_cell_pass(fp64, ccta.back(), smem, stream_, x_.p, xf_.p, conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p,
+                   d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
+                   fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, pair_acc_.p);
+  TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
   // internal nodes, deepest level first, from the leaves the cell pass wrote
@@ -765,18 +861,22 @@ int Engine::run_pairs_and_refit() {
 }
 
 int Engine::run_queries() {
-  // ordered compaction of each pair's receptor nodes inside the donor region
-  int maxn = 0;
-  for (int p = 0; p < npairs_; p++) maxn = std::max(maxn, bi_[h_pairs_[p].rec].nnodes);
+  // ordered compaction of each pair's receptor nodes inside the donor region,
+  // over one list of every pair's node tiles
   const int tile = kNodeTile;  // 256 threads x 8 nodes, one node tile
-  const int tiles_x = std::max(1, (maxn + tile - 1) / tile);
-  const long long ntiles = (long long)tiles_x * npairs_;
+  h_pair_t0_.assign(npairs_ + 1, 0);
+  for (int p = 0; p < npairs_; p++)
+    h_pair_t0_[p + 1] = h_pair_t0_[p] + (bi_[h_pairs_[p].rec].nnodes + tile - 1) / tile;
+  const long long ntiles = h_pair_t0_[npairs_];
+  TB_CUDA(d_pair_t0_.ensure(npairs_ + 1));
+  TB_CUDA(cudaMemcpyAsync(d_pair_t0_.p, h_pair_t0_.data(), (npairs_ + 1) * sizeof(long long), cudaMemcpyHostToDevice,
+                          stream_));
   TB_CUDA(tile_cnt_.ensure(ntiles + 1));
   TB_CUDA(tile_off_.ensure(ntiles + 1));
   TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
-  dim3 grid(std::min(tiles_x, 148 * 8), npairs_);
-  k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_cnt_.p, tbox_.p,
-                                           tile_base_.p, node_order_.p);
+  const unsigned grid = (unsigned)std::max(1ll, std::min(ntiles, 148ll * 16));
+  k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_cnt_.p,
+                                           tbox_.p, tile_base_.p, node_order_.p);
   TB_LAUNCHED("k_query_count");
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
@@ -793,13 +893,13 @@ int Engine::run_queries() {
   TB_CUDA(qtie_.ensure(nq));
   TB_CUDA(interp2rec_.ensure(nq));
   if (nq > 0) {
-    k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, tiles_x, tile, tile_off_.p,
+    k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_off_.p,
                                              node_res_.p, qnode_.p, qdon_.p, qres_.p, tbox_.p, tile_base_.p,
                                              node_order_.p);
     TB_LAUNCHED("k_query_write");
   }
   dedup_ran_ = false;
-  if (dedup_active_ && nq > 0) TB_TRY(run_dedup(tiles_x));
+  if (dedup_active_ && nq > 0) TB_TRY(run_dedup());
   return 0;
 }
 
@@ -928,9 +1028,9 @@ int Engine::dedup_gate() {
   k_coin_fill<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, off.p, k0.p, v0.p);
   TB_LAUNCHED("k_coin_fill");
   tmp = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 62, stream_);
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 64, stream_);
   TB_CUDA(cub_tmp_.ensure(tmp));
-  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 62, stream_);
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, k0.p, k1.p, v0.p, v1.p, total, 0, 64, stream_);
   k_coin_check<<<grid_for(total, kT), kT, 0, stream_>>>(k1.p, v1.p, total, x_.p, node_blk_.p, d_bi_.p, flag.p);
   TB_LAUNCHED("k_coin_check");
   unsigned f = 0;
@@ -943,14 +1043,14 @@ int Engine::dedup_gate() {
 // The per-call merge (uniqNodesTree): donor-list order, octree subsets level
 // by level, the pairwise loop per leaf, then xtag / representative / merged
 // resolution per query.
-int Engine::run_dedup(int tiles_x) {
+int Engine::run_dedup() {
   // queries of pair p are [qoff[p], qoff[p+1])
-  std::vector<int> h_toff((size_t)tiles_x * npairs_ + 1);
+  std::vector<int> h_toff(h_pair_t0_.back() + 1);
   TB_CUDA(cudaMemcpyAsync(h_toff.data(), tile_off_.p, h_toff.size() * sizeof(int), cudaMemcpyDeviceToHost,
                           stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   std::vector<int> qoff(npairs_ + 1);
-  for (int p = 0; p < npairs_; p++) qoff[p] = h_toff[(size_t)p * tiles_x];
+  for (int p = 0; p < npairs_; p++) qoff[p] = h_toff[h_pair_t0_[p]];
   qoff[npairs_] = (int)nq_;
   DedupQueries Q{nq_, qnode_.p, qdon_.p, nullptr, nullptr, qres_.p, x_.p, node_blk_.p};
   TB_TRY(dedup_merge(Q, qoff));
@@ -1164,7 +1264,7 @@ int Engine::run_donors() {
   // candidate slots: one per (receptor node, donor block)
   if (nq_ > 0) {
     k_fill_slots<<<grid_for(nq_, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, qcell_.p, nq_, K_, ntot_, ctot_,
-                                                        slot_.p, err_.p);
+                                                        d_bi_.p, (int)hb_.size(), slot_.p, err_.p);
     TB_LAUNCHED("k_fill_slots");
     k_classify_queried<<<grid_for(nq_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, slot_.p, K_, qnode_.p,
                                                               qcell_.p, nq_, qres_.p, d_hmdev_.p, nhm_, iblank_.p,
@@ -1217,8 +1317,8 @@ int Engine::run_donors() {
   nrec_ = R;
   if (R > 0) {
     size_t tmp = 0;
-    int hi_bit = 32;
-    while ((1ll << (hi_bit - 32)) < K_) hi_bit++;
+    int hi_bit = 32;  // receptor node below, donor block from bit 32
+    while ((1ll << (hi_bit - 32)) < (long long)hb_.size()) hi_bit++;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp, rkey_alt_.p, rkey_.p, rval_alt_.p, rval_.p, R, 0, hi_bit,
                                     stream_);
     TB_CUDA(cub_tmp_.ensure(tmp));
@@ -1268,7 +1368,7 @@ int Engine::run_donors() {
   prev_nrec_ = R;
   // back to rest for the next call: slots, cancel marks
   k_donor_clear<<<grid_for(std::max<long long>(nq_, 1), kT), kT, 0, stream_>>>(
-      qnode_.p, qdon_.p, qcell_.p, nq_, K_, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
+      qnode_.p, qdon_.p, qcell_.p, nq_, K_, d_bi_.p, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
   TB_LAUNCHED("k_donor_clear");
   return 0;
 }
@@ -1439,6 +1539,8 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
   if (ib < 0) return -1;
   int rc = fetch_interps();
   if (rc) return rc;
+  std::vector<int> first(bi_.size());
+  for (size_t b = 0; b < bi_.size(); b++) first[b] = bi_[b].node_off;
   long long j = 0, k = 0;
   for (long long r = 0; r < nrec_; r++) {
     if (h_it_don_[r] != ib || h_it_cancel_[r]) continue;
@@ -1449,11 +1551,10 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
       j++;
     }
     const int g = h_it_rec_[r];
-    int rb = 0;
-    while (rb + 1 < (int)bi_.size() && bi_[rb + 1].node_off <= g) rb++;
+    const int rb = (int)(std::upper_bound(first.begin(), first.end(), g) - first.begin()) - 1;
     receptors[k++] = 0;  // rank of the receptor: the only one
     receptors[k++] = g - bi_[rb].node_off;
-    receptors[k++] = rb;
+    receptors[k++] = rb - bi_[rb].sblk0;  // the receptor block's index within its system
     receptors[k++] = nv;
   }
   return 0;
@@ -1521,11 +1622,13 @@ int Engine::dataupdate(int nvar, int interptype) {
                             stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
     // scatter into the caller's arrays (updateSolnData, dataUpdate.C:105-119)
+    std::vector<int> first(bi_.size());
+    for (size_t b = 0; b < bi_.size(); b++) first[b] = bi_[b].node_off;
     for (long long r = 0; r < nrec_; r++) {
       if (h_it_cancel_[r]) continue;
       const int g = h_it_rec_[r];
-      int rb = 0;
-      while (rb + 1 < (int)bi_.size() && bi_[rb + 1].node_off <= g) rb++;
+      // the last block whose first node is <= g (empty blocks share an offset with the next one)
+      const int rb = (int)(std::upper_bound(first.begin(), first.end(), g) - first.begin()) - 1;
       const int local = g - bi_[rb].node_off;
       double* q = hb_[rb].hq;
       for (int k = 0; k < nvar; k++) {

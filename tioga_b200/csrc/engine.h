@@ -31,6 +31,9 @@ constexpr int kMaxTreeDepth = 32; // tree levels below the root at most (30-bit 
 constexpr int kNodeTile = 2048; // nodes per query-gathering tile
 constexpr int kSlots = 8;       // inline search candidates per query
 constexpr int kMaxBlocks = 100; // MAXBLOCKS, src/globals.h:29
+constexpr int kMaxSysBlocks = 16;      // blocks of one overset system (donor lists per node)
+constexpr int kMaxEngineBlocks = 8192;
+constexpr size_t kHoleMapCap = 197ull * 197ull * 197ull;  // bytes of one hole map at most // blocks of all systems of one engine (16-bit block ids)
 
 template <class T>
 struct DBuf {
@@ -66,6 +69,12 @@ struct BlockInfo {
   int nfringe;         // snapshot taken at preprocess (tioga.C:95-110)
   int root;            // slot of the block's tree root (4 * block), -1 without cells
   int has_user_res;
+  // overset system of the block: every system is connected on its own (pairs,
+  // hole maps and donor lists never cross systems); its blocks are
+  // consecutive, sblk0 .. sblk0 + snb - 1, in registration order
+  int sys, sblk0, snb;
+  int hm_lo, hm_hi;    // the system's hole maps: d_hmdev_[hm_lo .. hm_hi)
+  int hm;              // the block's own hole map (wall-bearing blocks), else -1
   Obb obb;
   float bb_lo[3], bb_hi[3];  // block box for the Morton keys
 };
@@ -90,6 +99,12 @@ struct PairCull {
   int pair;       // index in the pair list
 };
 
+
+// one wall-bearing block: its wall nodes in the global wall list, its cells,
+// its hole map
+struct WallBlock {
+  int wall_off, nwall, cell_off, ncells, hm;
+};
 
 struct HoleMapInfo {
   int exist;
@@ -123,10 +138,11 @@ struct DedupQueries {
   const int* qrec;
   const double* qres;
   const double* coords;
-  const unsigned char* node_blk;
+  const blk_t* node_blk;
 };
 
 struct HostBlock {
+  int sys = 0;
   int tag = 0, nnodes = 0, ncells = 0, ntypes = 0;
   int nv[4] = {0, 0, 0, 0}, nc[4] = {0, 0, 0, 0};
   double* hx = nullptr;
@@ -183,6 +199,12 @@ class Engine {
   // registration / settings (src/tioga.C:64-93, tioga.h:181-205)
   int register_block(int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
                      int* obc, int ntypes, const int* nv, const int* nc, int** conn);
+  int register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl, int nwbc, int nobc, int* wbc,
+                         int* obc, int ntypes, const int* nv, const int* nc, int** conn);
+  int find_block(int sys, int tag) const;
+  int nsystems() const;
+  void select_system(int sys) { cur_sys_ = sys; }
+  int selected_system() const { return cur_sys_; }
   void set_symmetry(int s) { isym_ = s; }
   void set_nfringe(int n) { nfringe_ = n; }
   void set_mexclude(int m) { mexclude_ = m; }
@@ -223,7 +245,7 @@ class Engine {
   int run_donors();
   int donor_rest_init();
   int dedup_gate();
-  int run_dedup(int tiles_x);
+  int run_dedup();
   int dedup_merge(const DedupQueries& Q, const std::vector<int>& qoff);
   int traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count);
   int run_celliblank();
@@ -233,7 +255,7 @@ class Engine {
 
   std::vector<HostBlock> hb_;
   std::vector<BlockInfo> bi_;
-  std::map<int, int> tag2idx_;
+  std::map<long long, int> tag2idx_;  // (system << 32 | tag) -> block
   int isym_ = 3, nfringe_ = 1, mexclude_ = 3;
   int precision_ = 1;        // 0 = FP64 throughout, 1 = FP32 screen + FP64 refine
   int coords_resident_ = 0;  // 1: the caller promises x has not moved
@@ -242,6 +264,7 @@ class Engine {
   bool connected_ = false;
   int npairs_ = 0;
   int maxtag_ = 0;
+  int cur_sys_ = 0;               // system whose tags the tag-based calls address
   int nhm_ = 0;
   long long nq_ = 0;
   std::vector<PairInfo> h_pairs_;
@@ -277,7 +300,8 @@ class Engine {
   // flat device arrays
   DBuf<double> x_, node_res_, cell_res_;
   DBuf<int> iblank_, iblank_cell_, conn8_;
-  DBuf<unsigned char> node_blk_, cell_blk_, cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_;
+  DBuf<blk_t> node_blk_, cell_blk_;
+  DBuf<unsigned char> cell_nv_, wallf_, obcf_, ex0_, ex1_, m0_;
   DBuf<int> m1_, cmark_;            // nfringe marks and cancel marks (first marker wins an atomicExch)
   DBuf<int> mlist_, cmlist_, dcnt_;  // marked nodes (holes first), cancel-marked nodes, their counters
   // coincident query points (uniqNodesTree)
@@ -308,10 +332,22 @@ class Engine {
   DBuf<int> csr_off_, csr_cell_, deg_;
   DBuf<BlockInfo> d_bi_;
   DBuf<PairInfo> d_pairs_;
+  DBuf<int2> d_pcand_;              // (donor, receptor) blocks that may pair, donor-major
+  int npcand_ = 0;
+  DBuf<int> d_pfirst_;              // first pair of every donor block (nb + 1)
+  std::vector<int> h_pfirst_;
+  DBuf<int4> d_chunks_;             // cell pass: (first leaf, end leaf, first pair, pairs) per chunk
+  DBuf<int> d_chunk_cta_;
+  std::vector<int> h_blk_leaf_;     // leaves of block b: [h_blk_leaf_[b], h_blk_leaf_[b + 1])
+  DBuf<long long> d_pair_t0_;       // query tiles of pair p: [pair_t0[p], pair_t0[p + 1])
+  std::vector<long long> h_pair_t0_;
+  std::vector<WallBlock> h_wall_;
+  DBuf<WallBlock> d_wall_;
   DBuf<int> d_npairs_;
   DBuf<HoleMapInfo> d_hm_;
   DBuf<HoleMapDev> d_hmdev_;
-  std::vector<DBuf<unsigned char>> hm_state_;
+  DBuf<unsigned char> hm_state_;  // kHoleMapCap bytes per hole map
+  int nhm_all_ = 0;               // wall-bearing blocks (hole maps) of all systems
   DBuf<unsigned long long> wall_bb_;
   // tree
   DBuf<int> sorted_cell_;

@@ -228,7 +228,7 @@ __global__ void k_ho_orphans(const int* __restrict__ ctag, const int* __restrict
     for (int j = 0; j < npts; j++) {
       if (win[p0 + j] >= 0) continue;
       reject = 2;
-      for (int k = 0; k < nhm; k++)
+      for (int k = bi[b].hm_lo; k < bi[b].hm_hi; k++)
         if (hm[k].tagidx != bi[b].tag - 1 && check_holemap(pts + 3 * (p0 + j), hm[k])) {
           reject = 1;
           break;
@@ -278,6 +278,10 @@ int Engine::set_highorder(int tag, int p, const double* xdof) {
 int Engine::connectivity_highorder() {
   if (!connected_) {
     fprintf(stderr, "#tioga_b200: performconnectivity_highorder needs performconnectivity first\n");
+    return -1;
+  }
+  if (nsystems() > 1) {
+    fprintf(stderr, "#tioga_b200: the high-order path takes one overset system per instance\n");
     return -1;
   }
   const int nb = (int)hb_.size();

@@ -35,10 +35,21 @@ __host__ __device__ inline double dkey_inv(unsigned long long k) {
   return d;
 }
 
+// the last block whose first node tile is <= T (tile_base[b] = first tile of block b)
+__device__ __forceinline__ int block_of_tile(const long long* __restrict__ tile_base, int nb, long long T) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (tile_base[m] <= T) lo = m;
+    else hi = m - 1;
+  }
+  return lo;
+}
+
 // ---- preprocess (kernels_pre.cu) ----
 __global__ void k_conn_convert(const int* raw, int nc, int nv, int node_off, int cell_base, int blk,
-                               int* conn8, unsigned char* cell_nv, unsigned char* cell_blk);
-__global__ void k_node_blk(int node_off, int nnodes, int blk, unsigned char* node_blk);
+                               int* conn8, unsigned char* cell_nv, blk_t* cell_blk);
+__global__ void k_node_blk(int node_off, int nnodes, int blk, blk_t* node_blk);
 __global__ void k_mark_list(const int* list, int n, int node_off, int* glist, int goff,
                             unsigned char* flag);
 __global__ void k_csr_count(const int* conn8, const unsigned char* cell_nv, long long ctot, int* deg);
@@ -46,10 +57,10 @@ __global__ void k_csr_fill(const int* conn8, const unsigned char* cell_nv, long 
                            const int* off, int* cursor, int* cells);
 __global__ void k_csr_sort(const int* off, long long ntot, int* cells);
 __global__ void k_cell_volume(const double* x, const int* conn8, const unsigned char* cell_nv,
-                              const unsigned char* cell_blk, const BlockInfo* bi, long long ctot,
+                              const blk_t* cell_blk, const BlockInfo* bi, long long ctot,
                               double* cell_res);
 __global__ void k_node_res(const int* off, const int* cells, const double* cell_res,
-                           const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+                           const blk_t* node_blk, const BlockInfo* bi, long long ntot,
                            double* node_res);
 __global__ void k_mandatory(const int* conn8, const unsigned char* cell_nv, long long ctot,
                             const unsigned char* obcf, double* node_res, unsigned char* ex0,
@@ -58,31 +69,29 @@ __global__ void k_mexclude(const int* conn8, const unsigned char* cell_nv, long 
                            const unsigned char* ex0, unsigned char* ex1, double* cell_res);
 __global__ void k_copy_u8(const unsigned char* a, unsigned char* b, long long n);
 __global__ void k_fill_int(int* a, int v, long long n);
-__global__ void k_obb_partial(const double* x, int off, int n, int pass, const Obb* obb, double* part);
-__global__ void k_obb_finish(const double* part, int nparts, int n, int pass, const double* x, int off,
-                             Obb* obb, BlockInfo* bi);
+__global__ void k_obb_partial(const double* x, const BlockInfo* bi, int pass, double* part);
+__global__ void k_obb_finish(const double* part, int nparts, int pass, const double* x, BlockInfo* bi, int nb);
 __global__ void k_morton(const double* x, const int* conn8, const unsigned char* cell_nv,
-                         const unsigned char* cell_blk, const BlockInfo* bi, long long ctot,
+                         const blk_t* cell_blk, const BlockInfo* bi, long long ctot,
                          unsigned long long* key, int* val);
 
 // ---- connectivity (kernels_conn.cu) ----
-__global__ void k_wall_bounds(const double* x, const int* wall_list, int off, int n,
-                              unsigned long long* bb);
-__global__ void k_holemap_setup(const unsigned long long* bb, HoleMapInfo* hm, int tag0);
-__global__ void k_holemap_mark(const double* x, const int* conn8, const unsigned char* cell_nv,
-                               int cell_off, int ncells, const unsigned char* wallf,
-                               const HoleMapInfo* hm, unsigned char* sam);
-__global__ void k_holemap_fill_planes(unsigned char* sam, const HoleMapInfo* hm, int isym,
-                                      int seed, unsigned* changed, unsigned* err);
-__global__ void k_holemap_lines(unsigned char* sam, const HoleMapInfo* hm, int axis, unsigned* changed);
-__global__ void k_holemap_final(unsigned char* sam, const HoleMapInfo* hm);
-__global__ void k_pairs(BlockInfo* bi, int nb, PairInfo* pairs, int* npairs);
+__global__ void k_wall_bounds(const double* x, const int* wall_list, const WallBlock* wt, unsigned long long* bb);
+__global__ void k_holemap_setup(const unsigned long long* bb, HoleMapInfo* hm, int nhm);
+__global__ void k_holemap_mark(const double* x, const int* conn8, const unsigned char* cell_nv, const WallBlock* wt,
+                               const unsigned char* wallf, const HoleMapInfo* hm, unsigned char* sam, size_t cap);
+__global__ void k_holemap_fill_planes(unsigned char* sam, const HoleMapInfo* hm, size_t cap, int isym, int seed,
+                                      unsigned* err);
+__global__ void k_holemap_lines(unsigned char* sam, const HoleMapInfo* hm, size_t cap, int axis, unsigned* changed);
+__global__ void k_holemap_final(unsigned char* sam, const HoleMapInfo* hm, size_t cap);
+__global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand, PairInfo* pairs, int* npairs,
+                        int* pfirst);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
-                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
-                      const int4* leaves, long long nleaf_total, const PairInfo* pairs, int p0, int np,
-                      int write_boxes, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
+                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
+                      const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
+                      const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
                       unsigned long long* acc);
 __global__ void k_round_nodes(const double* x, long long n, float4* xf);
 __global__ void k_tree_split(const unsigned long long* key, int n, const int* ca, const int* cb, const int* cslot,
@@ -94,23 +103,24 @@ __global__ void k_tree_init(const int2* tlink, long long nslots, float4* tnode);
 __global__ void k_tree_init64(long long nslots, double* t64);
 __global__ void k_leaf_flags(const int* leaf_at, long long ctot, int* flag);
 __global__ void k_leaf_list(const int* leaf_at, const int* loff, long long ctot, const int2* tlink,
-                            const unsigned char* cell_blk, int4* leaves);
+                            const blk_t* cell_blk, int4* leaves);
+__global__ void k_block_leaves(const int4* leaves, long long nleaf, int* first);
 __global__ void k_refit_level(int g0, int g1, const int* gparent, float4* tnode, double* tnode64);
 __global__ void k_node_tiles(const float4* xf, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
-__global__ void k_morton_nodes(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
+__global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);
 __global__ void k_invert(const int* perm, long long n, int* inv);
 __global__ void k_permute_cells(const int* perm, long long n, const int* conn8, const unsigned char* nv,
-                                const unsigned char* blk, int* conn8_out, unsigned char* nv_out,
-                                unsigned char* blk_out);
+                                const blk_t* blk, int* conn8_out, unsigned char* nv_out,
+                                blk_t* blk_out);
 __global__ void k_remap(int* idx, long long n, const int* map);
 __global__ void k_scatter_f64(const double* src, long long n, const int* inv, long long base, double* dst);
-__global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs,
-                              int tiles_x, int tile, int* tile_cnt, const float4* tbox, const long long* tile_base,
-                              const int* node_order);
-__global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs,
-                              int tiles_x, int tile, const int* tile_off, const double* node_res,
+__global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs, int npairs,
+                              const long long* pair_t0, int tile, int* tile_cnt, const float4* tbox,
+                              const long long* tile_base, const int* node_order);
+__global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs, int npairs,
+                              const long long* pair_t0, int tile, const int* tile_off, const double* node_res,
                               int* qnode, int* qdon, double* qres, const float4* tbox,
                               const long long* tile_base, const int* node_order);
 // host launchers of the templated search stages (same translation unit as
@@ -134,11 +144,11 @@ __global__ void k_search_finish(const unsigned long long* qkey, const unsigned* 
 
 // ---- donors (kernels_donor.cu) ----
 __global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
-                             long long ntot, long long ctot, int* slot, unsigned* err);
+                             long long ntot, long long ctot, const BlockInfo* bi, int nb, int* slot, unsigned* err);
 __global__ void k_donor_reset(const int* mlist, const int* dcnt, const int* it_rec, const unsigned char* it_cancel,
                               int prev_R, const int* csr_off, const int* csr_cell, int* iblank, unsigned char* m0,
                               int* m1, int* iblank_cell);
-__global__ void k_classify_queried(const double* x, const unsigned char* node_blk, const BlockInfo* bi,
+__global__ void k_classify_queried(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                    const int* slot, int K, const int* qnode, const int* qcell, long long nq,
                                    const double* qres, const HoleMapDev* hm, int nhm, int* iblank, double* node_res,
                                    unsigned char* m0, int* m1, int* mlist, int* dcnt, unsigned long long* counters);
@@ -148,11 +158,11 @@ __global__ void k_classify_tiles(const double* x, const BlockInfo* bi, int nb, c
                                  int* dcnt, unsigned long long* counters);
 __global__ void k_front_init(int* dcnt);
 __global__ void k_dilate_front(int iter, const int* csr_off, const int* csr_cell, const int* conn8,
-                               const unsigned char* cell_nv, const unsigned char* cell_blk, const BlockInfo* bi,
+                               const unsigned char* cell_nv, const blk_t* cell_blk, const BlockInfo* bi,
                                const unsigned char* m0, int* m1, int* mlist, int* dcnt);
 __global__ void k_front_next(int iter, unsigned char* m0, const int* mlist, int* dcnt);
 __global__ void k_fringe_big_list(const int* mlist, const int* dcnt, const int* iblank, double* node_res);
-__global__ void k_select(const unsigned char* node_blk, const BlockInfo* bi, const int* slot, int K,
+__global__ void k_select(const blk_t* node_blk, const BlockInfo* bi, const int* slot, int K,
                          const int* qnode, const int* qcell, long long nq, const double* cell_res, int* iblank,
                          const double* node_res, unsigned long long* rkey, int* rval, int* rcount, int rcap,
                          unsigned* err);
@@ -162,25 +172,25 @@ __global__ void k_interp_marks(const unsigned long long* rkey, const int* rval, 
                                int* dcnt);
 __global__ void k_interp(const double* x, const unsigned long long* rkey, const int* rval,
                          const int* rcount, const int* qcell, const int* conn8,
-                         const unsigned char* cell_nv, const unsigned char* node_blk,
+                         const unsigned char* cell_nv, const blk_t* node_blk,
                          const BlockInfo* bi, const int* iblank, const double* node_res,
                          const int* reset_t, const int* orig_cell, int* it_node, double* it_w, int* it_rec,
                          int* it_don, unsigned char* it_nv, unsigned char* it_cancel, double* rres,
                          int* interp2rec, unsigned* err);
-__global__ void k_node_bins(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+__global__ void k_node_bins(const double* x, const blk_t* node_blk, const BlockInfo* bi, long long ntot,
                             short* node_bin);
-__global__ void k_coin_count(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+__global__ void k_coin_count(const double* x, const blk_t* node_blk, const BlockInfo* bi, long long ntot,
                              int* cnt);
-__global__ void k_coin_fill(const double* x, const unsigned char* node_blk, const BlockInfo* bi, long long ntot,
+__global__ void k_coin_fill(const double* x, const blk_t* node_blk, const BlockInfo* bi, long long ntot,
                             const int* off, unsigned long long* key, int* val);
 __global__ void k_coin_check(const unsigned long long* key, const int* val, long long n, const double* x,
-                             const unsigned char* node_blk, const BlockInfo* bi, unsigned* flag);
+                             const blk_t* node_blk, const BlockInfo* bi, unsigned* flag);
 __global__ void k_dedup_keys(const int* qnode, const int* qdon, long long nq, const int* pair_qoff, int npairs,
                              const int* pair_rank, const short* node_bin, unsigned long long* key, int* val);
 __global__ void k_dedup_keys_pts(const int* qpt_local, const int* qdon, long long nq, const int* pair_qoff,
                                  int npairs, const int* pair_rank, unsigned long long* key, int* val);
 __global__ void k_dedup_gather(const int* refq, long long n, const int* qnode, const double* qres, const double* x,
-                               const unsigned char* node_blk, const int* qrec, const BlockInfo* bi, double* xg,
+                               const blk_t* node_blk, const int* qrec, const BlockInfo* bi, double* xg,
                                int* mtag, double* rtag, int* itag, int* perm, int* gpos_of);
 __global__ void k_dedup_box(const int4* chunks, const int* perm, const double* xg, unsigned long long* box);
 __global__ void k_dedup_octant(const int4* chunks, const int* perm, const double* xg, const unsigned long long* box,
@@ -200,8 +210,9 @@ __global__ void k_cancel(const int* cmlist, const int* dcnt, const int* slot, in
                          const double* cell_res, const int* interp2rec, unsigned char* it_cancel);
 __global__ void k_iblank_final(const int* it_rec, const unsigned char* it_cancel, const int* rcount, int* iblank,
                                unsigned long long* counters);
-__global__ void k_donor_clear(const int* qnode, const int* qdon, const int* qcell, long long nq, int K, int* slot,
-                              const int* cmlist, const int* dcnt, int* cmark, int* reset_t);
+__global__ void k_donor_clear(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
+                              const BlockInfo* bi, int* slot, const int* cmlist, const int* dcnt, int* cmark,
+                              int* reset_t);
 __global__ void k_cell_iblank_sparse(const int* mlist, const int* dcnt, const int* it_rec,
                                      const unsigned char* it_cancel, const int* rcount, const int* csr_off,
                                      const int* csr_cell, const int* conn8, const unsigned char* cell_nv,
@@ -212,7 +223,7 @@ __global__ void k_interp_gather(const int* it_node, const double* it_w, const in
                                 const int* rcount, const BlockInfo* bi, const double* q, int nvar,
                                 int interptype, double* vals);
 __global__ void k_interp_scatter(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
-                                 const unsigned char* node_blk, const BlockInfo* bi, const double* vals,
+                                 const blk_t* node_blk, const BlockInfo* bi, const double* vals,
                                  int nvar, int interptype, double* q);
 
 }  // namespace tb

@@ -13,11 +13,15 @@ namespace tb {
 // ===========================================================================
 // hole maps
 // ===========================================================================
-__global__ void k_wall_bounds(const double* __restrict__ x, const int* __restrict__ wall_list, int off,
-                              int n, unsigned long long* __restrict__ bb) {
+// Wall-node bounds of every wall-bearing block: blockIdx.y indexes the wall
+// table (first wall node, wall nodes, cells: first, count; hole map index)
+__global__ void k_wall_bounds(const double* __restrict__ x, const int* __restrict__ wall_list,
+                              const WallBlock* __restrict__ wt, unsigned long long* __restrict__ bb_all) {
+  const WallBlock W = wt[blockIdx.y];
+  unsigned long long* bb = bb_all + 6 * W.hm;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double* p = x + 3 * (long long)wall_list[off + i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.nwall; i += gridDim.x * blockDim.x) {
+    const double* p = x + 3 * (long long)wall_list[W.wall_off + i];
     for (int j = 0; j < 3; j++) {
       lo[j] = dmin(lo[j], p[j]);
       hi[j] = dmax(hi[j], p[j]);
@@ -37,10 +41,10 @@ __global__ void k_wall_bounds(const double* __restrict__ x, const int* __restric
   }
 }
 
-// extents and sizes exactly as holeMap.C:118-140
-__global__ void k_holemap_setup(const unsigned long long* __restrict__ bb, HoleMapInfo* __restrict__ hm,
-                                int t) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// extents and sizes exactly as holeMap.C:118-140, one thread per hole map
+__global__ void k_holemap_setup(const unsigned long long* __restrict__ bb, HoleMapInfo* __restrict__ hm, int nhm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nhm) return;
   HoleMapInfo& h = hm[t];
   double ds[3];
   for (int j = 0; j < 3; j++) {
@@ -59,15 +63,21 @@ __global__ void k_holemap_setup(const unsigned long long* __restrict__ bb, HoleM
   h.exist = 1;
 }
 
+// wall-touching cells mark their index box with 2 (MeshBlock.C:666-772);
+// blockIdx.y indexes the wall table.  Sizes past the slab are left alone (the
+// host rejects such a map before it is used).
 __global__ void k_holemap_mark(const double* __restrict__ x, const int* __restrict__ conn8,
-                               const unsigned char* __restrict__ cell_nv, int cell_off, int ncells,
-                               const unsigned char* __restrict__ wallf, const HoleMapInfo* __restrict__ hmp,
-                               unsigned char* __restrict__ sam) {
-  const HoleMapInfo h = *hmp;
+                               const unsigned char* __restrict__ cell_nv, const WallBlock* __restrict__ wt,
+                               const unsigned char* __restrict__ wallf, const HoleMapInfo* __restrict__ hm_all,
+                               unsigned char* __restrict__ sam_all, size_t cap) {
+  const WallBlock W = wt[blockIdx.y];
+  const HoleMapInfo h = hm_all[W.hm];
+  if ((size_t)h.nx[0] * h.nx[1] * h.nx[2] > cap) return;
+  unsigned char* __restrict__ sam = sam_all + (size_t)W.hm * cap;
   double ds[3];
   for (int k = 0; k < 3; k++) ds[k] = (h.ext[k + 3] - h.ext[k]) / h.nx[k];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncells; i += gridDim.x * blockDim.x) {
-    long long c = (long long)cell_off + i;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.ncells; i += gridDim.x * blockDim.x) {
+    long long c = (long long)W.cell_off + i;
     int nv = cell_nv[c];
     const int* cv = conn8 + 8 * c;
     int wall = 0;
@@ -101,11 +111,11 @@ __global__ void k_holemap_mark(const double* __restrict__ x, const int* __restri
 // the reference's Gauss-Seidel sweeps (utils.c:227-290), which is
 // independent of the visiting order.  With seed == 2 (6-neighbour mode) the
 // kernel only seeds the faces.
-__global__ void k_holemap_fill_planes(unsigned char* __restrict__ sam, const HoleMapInfo* __restrict__ hmp,
-                                      int isym, int seed_only, unsigned* __restrict__ changed,
-                                      unsigned* __restrict__ err) {
+__global__ void k_holemap_fill_planes(unsigned char* __restrict__ sam_all, const HoleMapInfo* __restrict__ hm_all,
+                                      size_t cap, int isym, int seed_only, unsigned* __restrict__ err) {
   extern __shared__ unsigned char s[];
-  const HoleMapInfo h = *hmp;
+  const HoleMapInfo h = hm_all[blockIdx.y];
+  unsigned char* __restrict__ sam = sam_all + (size_t)blockIdx.y * cap;
   const int n[3] = {h.nx[0], h.nx[1], h.nx[2]};
   const long long st[3] = {1, n[0], (long long)n[0] * n[1]};
   int pa, a0, a1;  // plane-normal axis and the two in-plane axes
@@ -158,14 +168,14 @@ __global__ void k_holemap_fill_planes(unsigned char* __restrict__ sam, const Hol
     }
     __syncthreads();
   }
-  (void)changed;
 }
 
 // 6-neighbour mode: one forward and one backward sweep along `axis` for every
 // line of interior cells; repeated over the three axes until no change.
-__global__ void k_holemap_lines(unsigned char* __restrict__ sam, const HoleMapInfo* __restrict__ hmp,
-                                int axis, unsigned* __restrict__ changed) {
-  const HoleMapInfo h = *hmp;
+__global__ void k_holemap_lines(unsigned char* __restrict__ sam_all, const HoleMapInfo* __restrict__ hm_all,
+                                size_t cap, int axis, unsigned* __restrict__ changed) {
+  const HoleMapInfo h = hm_all[blockIdx.y];
+  unsigned char* __restrict__ sam = sam_all + (size_t)blockIdx.y * cap;
   const int n[3] = {h.nx[0], h.nx[1], h.nx[2]};
   const long long st[3] = {1, n[0], (long long)n[0] * n[1]};
   int b0 = (axis == 0) ? 1 : 0, b1 = (axis == 2) ? 1 : 2;
@@ -186,8 +196,10 @@ __global__ void k_holemap_lines(unsigned char* __restrict__ sam, const HoleMapIn
 }
 
 // hole = unreached or wall-marked (utils.c:291-294)
-__global__ void k_holemap_final(unsigned char* __restrict__ sam, const HoleMapInfo* __restrict__ hmp) {
-  const HoleMapInfo h = *hmp;
+__global__ void k_holemap_final(unsigned char* __restrict__ sam_all, const HoleMapInfo* __restrict__ hm_all,
+                                size_t cap) {
+  const HoleMapInfo h = hm_all[blockIdx.y];
+  unsigned char* __restrict__ sam = sam_all + (size_t)blockIdx.y * cap;
   long long n = (long long)h.nx[0] * h.nx[1] * h.nx[2];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -249,24 +261,54 @@ __device__ int obb_intersect(const double vA[3][3], const double xA[3], const do
   return 1;
 }
 
-// pairs listed donor-outer, receptor-inner as in exchangeBoxes.C:133-160
-__global__ void k_pairs(BlockInfo* __restrict__ bi, int nb, PairInfo* __restrict__ pairs,
-                        int* __restrict__ npairs) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int np = 0;
-  for (int ob = 0; ob < nb; ob++)
-    for (int ib = 0; ib < nb; ib++) {
+// pairs listed donor-outer, receptor-inner as in exchangeBoxes.C:133-160:
+// the candidates (donor, receptor) of different mesh tags within a system
+// come in that order, and one CTA keeps those whose boxes intersect, in
+// order.  pfirst[b] = first pair whose donor is block b (pairs are sorted by
+// donor), pfirst[nb] = the pair count.
+constexpr int kPairThreads = 1024;
+__global__ void __launch_bounds__(kPairThreads) k_pairs(const BlockInfo* __restrict__ bi, int nb,
+                                                        const int2* __restrict__ cand, int ncand,
+                                                        PairInfo* __restrict__ pairs, int* __restrict__ npairs,
+                                                        int* __restrict__ pfirst) {
+  typedef cub::BlockScan<int, kPairThreads> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ int s_base;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < ncand; c0 += kPairThreads) {
+    const int i = c0 + threadIdx.x;
+    int hit = 0, ob = 0, ib = 0;
+    if (i < ncand) {
+      ob = cand[i].x;
+      ib = cand[i].y;
       const Obb& a = bi[ib].obb;
       const Obb& o = bi[ob].obb;
-      if (abs(bi[ob].tag) == bi[ib].tag) continue;
-      if (obb_intersect(a.vec, a.xc, a.dxc, o.vec, o.xc, o.dxc) ||
-          obb_intersect(o.vec, o.xc, o.dxc, a.vec, a.xc, a.dxc)) {
-        pairs[np].rec = ib;
-        pairs[np].don = ob;
-        np++;
-      }
+      hit = obb_intersect(a.vec, a.xc, a.dxc, o.vec, o.xc, o.dxc) ||
+            obb_intersect(o.vec, o.xc, o.dxc, a.vec, a.xc, a.dxc);
     }
-  *npairs = np;
+    int pos, total;
+    Scan(tmp).ExclusiveSum(hit, pos, total);
+    const int base = s_base;
+    if (hit) {
+      pairs[base + pos].rec = ib;
+      pairs[base + pos].don = ob;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_base = base + total;
+    __syncthreads();
+  }
+  const int np = s_base;
+  for (int b = threadIdx.x; b <= nb; b += blockDim.x) {
+    int lo = 0, hi = np;  // first pair with donor >= b
+    while (lo < hi) {
+      const int m = (lo + hi) >> 1;
+      if (pairs[m].don < b) lo = m + 1;
+      else hi = m;
+    }
+    pfirst[b] = lo;
+  }
+  if (threadIdx.x == 0) *npairs = np;
 }
 
 __global__ void k_pair_finish(const BlockInfo* __restrict__ bi, PairInfo* __restrict__ pairs, int npairs,
@@ -371,22 +413,34 @@ __device__ __forceinline__ void proj_bounds(const double cc[3], const double o[3
 //    the cell that does hold it always has its lower bound under every such
 //    upper bound, so it is always projected exactly.  The exact extents are
 //    combined per warp, per CTA in shared memory, and flushed once.
-// Pairs p0 .. p0+np-1 are handled; with write_boxes == 0 only their reduced
-// boxes are accumulated (the extra launches when the pairs exceed one CTA's
-// shared memory).
+// Work comes in chunks of consecutive blocks (chunk = leaves [x, y), pairs
+// z .. z+w-1: all the pairs whose donor is one of the chunk's blocks, as the
+// pairs are sorted by donor); CTAs chunk_cta[k] .. chunk_cta[k+1]-1 share
+// chunk k, whose pairs sit in their shared memory.
 template <bool F64>
 __global__ void __launch_bounds__(256, 3) k_cell_pass(
     const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
-    const unsigned char* __restrict__ cell_nv,
-    const BlockInfo* __restrict__ bi, int nb, const int4* __restrict__ leaves, long long nleaf_total,
-    const PairInfo* __restrict__ pairs, int p0, int np, int write_boxes, float4* __restrict__ cbox,
-    double* __restrict__ cbox64, float4* __restrict__ tnode, double* __restrict__ tnode64,
-    unsigned long long* __restrict__ acc) {
+    const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves,
+    const int4* __restrict__ chunks, const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, double* __restrict__ cbox64,
+    float4* __restrict__ tnode, double* __restrict__ tnode64, unsigned long long* __restrict__ acc) {
   extern __shared__ unsigned long long s_dyn[];
+  int kc = 0;  // this CTA's chunk: the last one whose first CTA is <= blockIdx.x
+  {
+    int hi = nchunks - 1;
+    while (kc < hi) {
+      const int m = (kc + hi + 1) >> 1;
+      if (chunk_cta[m] <= (int)blockIdx.x) kc = m;
+      else hi = m - 1;
+    }
+  }
+  const int4 CH = chunks[kc];
+  const long long leaf_lo = CH.x, leaf_hi = CH.y;
+  const int p0 = CH.z, np = CH.w;
+  const int cta = (int)blockIdx.x - chunk_cta[kc], ncta = chunk_cta[kc + 1] - chunk_cta[kc];
   unsigned long long* s_acc = s_dyn;                                  // 6 per pair, exact extents
   PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * np);        // 1 per pair, by donor block
   int* s_ext = reinterpret_cast<int*>(s_pc + np);                      // 6 per pair, FP32 bounds
-  __shared__ int s_pf[kMaxBlocks + 1];  // pairs of donor block b: s_pc[s_pf[b] .. s_pf[b+1])
   const int tid = threadIdx.x;
   for (int i = tid; i < 6 * np; i += blockDim.x) {
     s_acc[i] = (i % 6 < 3) ? ~0ull : 0ull;
@@ -394,11 +448,6 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
   }
   for (int i = tid; i < np; i += blockDim.x) {
     const PairInfo& P = pairs[p0 + i];
-    int rank = 0;  // position when sorted by donor block, ties by index
-    for (int k = 0; k < np; k++) {
-      const int dk = pairs[p0 + k].don;
-      rank += (dk < P.don) || (dk == P.don && k < i);
-    }
     const Obb& R = bi[P.rec].obb;
     const Obb& D = bi[P.don].obb;
     PairCull q;
@@ -413,22 +462,17 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
     }
     q.don = P.don;
     q.pair = p0 + i;
-    s_pc[rank] = q;
-  }
-  for (int b = tid; b <= nb; b += blockDim.x) {
-    int cnt = 0;
-    for (int k = 0; k < np; k++) cnt += pairs[p0 + k].don < b;
-    s_pf[b] = cnt;
+    s_pc[i] = q;
   }
   __syncthreads();
   volatile int* v_ext = s_ext;
   const int lane = tid & 31;
-  const long long warp0 = (blockIdx.x * (long long)blockDim.x + tid) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
+  const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
   constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;  // cells per leaf, leaves per warp
-  for (long long base = LPW * warp0; base < nleaf_total; base += LPW * nwarps) {
+  for (long long base = leaf_lo + LPW * warp0; base < leaf_hi; base += LPW * nwarps) {
     const long long leaf = base + lane / LC;
-    const bool leaf_ok = leaf < nleaf_total;
+    const bool leaf_ok = leaf < leaf_hi;
     const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
     const int b = L.w;
     const bool valid = leaf_ok && lane % LC < L.y;
@@ -463,7 +507,7 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
         cc[k] = 0.5 * (lo[k] + hi[k]);
         hh[k] = valid ? __double2float_ru(0.5 * (hi[k] - lo[k])) : 0.f;
       }
-      if (write_boxes) {
+      {
         if (valid) {
           double* o = cbox64 + 6 * c;
           o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
@@ -511,7 +555,7 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
         f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
         f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
       }
-    if (write_boxes) {
+    {
       if (valid) {
         cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
         cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
@@ -528,7 +572,7 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
     // extents' bounds, tightens them and is done too.  The remaining
     // (leaf, pair) combinations, bit q-qa of mixed, go cell by cell.
     const bool leaf_live = leaf_ok && f[0] <= f[3];
-    const int qa = leaf_live ? s_pf[b] : 0, qb = leaf_live ? s_pf[b + 1] : 0;
+    const int qa = leaf_live ? pfirst[b] - p0 : 0, qb = leaf_live ? pfirst[b + 1] - p0 : 0;
     const int g = lane % LC;
     unsigned mixed = 0u;
     {
@@ -663,7 +707,7 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
   __syncthreads();
   for (int i = tid; i < 6 * np; i += blockDim.x) {
     const unsigned long long v = s_acc[i];
-    unsigned long long* dst = &acc[6 * (long long)s_pc[i / 6].pair + i % 6];
+    unsigned long long* dst = &acc[6 * (long long)(p0 + i / 6) + i % 6];
     if (i % 6 < 3) {
       if (v != ~0ull) atomicMin(dst, v);
     } else if (v != 0ull) {
@@ -673,16 +717,16 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
 }
 
 void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
-                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, int nb,
-                      const int4* leaves, long long nleaf_total, const PairInfo* pairs, int p0, int np,
-                      int write_boxes, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
+                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
+                      const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
+                      const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
                       unsigned long long* acc) {
   if (f64)
-    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, leaves, nleaf_total, pairs, p0, np,
-                                               write_boxes, cbox, cbox64, tnode, tnode64, acc);
+    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
+                                               pairs, cbox, cbox64, tnode, tnode64, acc);
   else
-    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, nb, leaves, nleaf_total, pairs, p0,
-                                                np, write_boxes, cbox, cbox64, tnode, tnode64, acc);
+    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
+                                                pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
 }
 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
@@ -692,8 +736,7 @@ __global__ void __launch_bounds__(256) k_node_tiles(const float4* __restrict__ x
                                                     float4* __restrict__ tbox, const int* __restrict__ node_order) {
   __shared__ float sh[6][8];
   const long long T = blockIdx.x;
-  int b = 0;
-  while (b + 1 < nb && tile_base[b + 1] <= T) b++;
+  const int b = block_of_tile(tile_base, nb, T);
   const BlockInfo& B = bi[b];
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -751,30 +794,45 @@ __device__ __forceinline__ bool tile_may_hit(const float4* __restrict__ tbox, lo
            (double)A.w < P.wbox[0] || (double)C.x < P.wbox[1] || (double)C.y < P.wbox[2]);
 }
 
+// Tiles of all pairs in one list: pair p owns tiles pair_t0[p] .. pair_t0[p+1]-1
+// (its receptor block's node tiles), so a launch covers every pair whatever
+// the sizes of their receptor blocks.
+__device__ __forceinline__ int pair_of_tile(const long long* __restrict__ pair_t0, int npairs, long long T) {
+  int lo = 0, hi = npairs - 1;  // the last pair whose first tile is <= T
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (pair_t0[m] <= T) lo = m;
+    else hi = m - 1;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restrict__ x,
                                                            const BlockInfo* __restrict__ bi,
-                                                           const PairInfo* __restrict__ pairs, int tiles_x,
-                                                           int tile, int* __restrict__ tile_cnt,
+                                                           const PairInfo* __restrict__ pairs, int npairs,
+                                                           const long long* __restrict__ pair_t0, int tile,
+                                                           int* __restrict__ tile_cnt,
                                                            const float4* __restrict__ tbox,
                                                            const long long* __restrict__ tile_base,
                                                            const int* __restrict__ node_order) {
-  const int p = blockIdx.y;
-  const PairInfo& P = pairs[p];
-  const BlockInfo& R = bi[P.rec];
-  const Obb reg = P.region;
-  int cnt = 0;
-  for (int t = blockIdx.x; t < tiles_x; t += gridDim.x) {
-    int n0 = t * tile;
-    cnt = 0;
-    if (n0 < R.nnodes && !tile_may_hit(tbox, tile_base[P.rec] + t, P)) {
-      if (threadIdx.x == 0) tile_cnt[(long long)p * tiles_x + t] = 0;
+  __shared__ int sh[kQThreads / 32];
+  const long long ntiles = pair_t0[npairs];
+  for (long long T = blockIdx.x; T < ntiles; T += gridDim.x) {
+    const int p = pair_of_tile(pair_t0, npairs, T);
+    const int t = (int)(T - pair_t0[p]);
+    const PairInfo& P = pairs[p];
+    const BlockInfo& R = bi[P.rec];
+    const int n0 = t * tile;
+    if (!tile_may_hit(tbox, tile_base[P.rec] + t, P)) {
+      if (threadIdx.x == 0) tile_cnt[T] = 0;
       continue;
     }
+    const Obb reg = P.region;
+    int cnt = 0;
     for (int k = 0; k < kQItems; k++) {
       int i = n0 + threadIdx.x * kQItems + k;
       if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) cnt++;
     }
-    __shared__ int sh[kQThreads / 32];
     int w = cnt;
     for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = w;
@@ -782,7 +840,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
     if (threadIdx.x == 0) {
       int s = 0;
       for (int k = 0; k < kQThreads / 32; k++) s += sh[k];
-      tile_cnt[(long long)p * tiles_x + t] = s;
+      tile_cnt[T] = s;
     }
     __syncthreads();
   }
@@ -790,8 +848,9 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
 
 __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restrict__ x,
                                                            const BlockInfo* __restrict__ bi,
-                                                           const PairInfo* __restrict__ pairs, int tiles_x,
-                                                           int tile, const int* __restrict__ tile_off,
+                                                           const PairInfo* __restrict__ pairs, int npairs,
+                                                           const long long* __restrict__ pair_t0, int tile,
+                                                           const int* __restrict__ tile_off,
                                                            const double* __restrict__ node_res,
                                                            int* __restrict__ qnode, int* __restrict__ qdon,
                                                            double* __restrict__ qres, const float4* __restrict__ tbox,
@@ -799,13 +858,15 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
                                                            const int* __restrict__ node_order) {
   typedef cub::BlockScan<int, kQThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
-  const int p = blockIdx.y;
-  const PairInfo& P = pairs[p];
-  const BlockInfo& R = bi[P.rec];
-  const Obb reg = P.region;
-  for (int t = blockIdx.x; t < tiles_x; t += gridDim.x) {
-    int n0 = t * tile;
-    if (n0 >= R.nnodes || !tile_may_hit(tbox, tile_base[P.rec] + t, P)) continue;
+  const long long ntiles = pair_t0[npairs];
+  for (long long T = blockIdx.x; T < ntiles; T += gridDim.x) {
+    const int p = pair_of_tile(pair_t0, npairs, T);
+    const int t = (int)(T - pair_t0[p]);
+    const PairInfo& P = pairs[p];
+    const BlockInfo& R = bi[P.rec];
+    const int n0 = t * tile;
+    if (!tile_may_hit(tbox, tile_base[P.rec] + t, P)) continue;
+    const Obb reg = P.region;
     unsigned mask = 0;
     int cnt = 0;
     for (int k = 0; k < kQItems; k++) {
@@ -817,7 +878,7 @@ __global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restr
     }
     int pos;
     Scan(tmp).ExclusiveSum(cnt, pos);
-    long long o = (long long)tile_off[(long long)p * tiles_x + t] + pos;
+    long long o = (long long)tile_off[T] + pos;
     for (int k = 0; k < kQItems; k++) {
       if (mask & (1u << k)) {
         int g = node_order[R.node_off + n0 + threadIdx.x * kQItems + k];

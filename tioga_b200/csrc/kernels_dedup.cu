@@ -29,7 +29,7 @@
 namespace tb {
 
 // the 10x10x10 bin of every node in its block's OBB frame (MeshBlock.C:171-224)
-__global__ void k_node_bins(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+__global__ void k_node_bins(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                             const BlockInfo* __restrict__ bi, long long ntot, short* __restrict__ node_bin) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
        g += (long long)gridDim.x * blockDim.x) {
@@ -52,7 +52,7 @@ __global__ void k_node_bins(const double* __restrict__ x, const unsigned char* _
 // delta-box touches (one cell, rarely two per axis), so two such nodes always
 // share a key; runs of equal keys are then compared pairwise.
 // ---------------------------------------------------------------------------
-constexpr int kCoinBits = 18;  // grid cells per axis: 2^18
+constexpr int kCoinBits = 17;  // grid cells per axis: 2^17 (block id in the key's top 13 bits)
 
 __device__ __forceinline__ void coin_frame(const BlockInfo& B, double& s, double& delta) {
   double ext = 0;
@@ -71,7 +71,7 @@ __device__ __forceinline__ void coin_axis(double p, double lo, double s, double 
   n = max(b, c) - c0 + 1;
 }
 
-__global__ void k_coin_count(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+__global__ void k_coin_count(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                              const BlockInfo* __restrict__ bi, long long ntot, int* __restrict__ cnt) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
        g += (long long)gridDim.x * blockDim.x) {
@@ -88,7 +88,7 @@ __global__ void k_coin_count(const double* __restrict__ x, const unsigned char* 
   }
 }
 
-__global__ void k_coin_fill(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+__global__ void k_coin_fill(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                             const BlockInfo* __restrict__ bi, long long ntot, const int* __restrict__ off,
                             unsigned long long* __restrict__ key, int* __restrict__ val) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
@@ -103,8 +103,8 @@ __global__ void k_coin_fill(const double* __restrict__ x, const unsigned char* _
     for (int i = 0; i < n[0]; i++)
       for (int j = 0; j < n[1]; j++)
         for (int k = 0; k < n[2]; k++) {
-          key[o] = ((unsigned long long)b << 54) | ((unsigned long long)(c0[0] + i) << 36) |
-                   ((unsigned long long)(c0[1] + j) << 18) | (unsigned long long)(c0[2] + k);
+          key[o] = ((unsigned long long)b << 51) | ((unsigned long long)(c0[0] + i) << 34) |
+                   ((unsigned long long)(c0[1] + j) << 17) | (unsigned long long)(c0[2] + k);
           val[o] = (int)g;
           o++;
         }
@@ -112,7 +112,7 @@ __global__ void k_coin_fill(const double* __restrict__ x, const unsigned char* _
 }
 
 __global__ void k_coin_check(const unsigned long long* __restrict__ key, const int* __restrict__ val, long long n,
-                             const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+                             const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                              const BlockInfo* __restrict__ bi, unsigned* __restrict__ flag) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x + 1; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -135,9 +135,10 @@ __global__ void k_coin_check(const unsigned long long* __restrict__ key, const i
 // ---------------------------------------------------------------------------
 // Per call: donor-list order of every query, then the octree emulation.
 // ---------------------------------------------------------------------------
-// key = donor block | pair's rank among the donor's pairs | receptor bin |
-// descending node id; sorting the queries by it gives every donor's list in
-// the reference's order (gpos = position in that sorted order)
+// key = pair | receptor bin | descending node id (the pairs are sorted by
+// donor block, so a donor's pairs are consecutive and in list order); sorting
+// the queries by it gives every donor's list in the reference's order (gpos =
+// position in that sorted order)
 __global__ void k_dedup_keys(const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq,
                              const int* __restrict__ pair_qoff, int npairs, const int* __restrict__ pair_rank,
                              const short* __restrict__ node_bin, unsigned long long* __restrict__ key,
@@ -151,8 +152,8 @@ __global__ void k_dedup_keys(const int* __restrict__ qnode, const int* __restric
       else hi = m - 1;
     }
     const int g = qnode[q];
-    key[q] = ((unsigned long long)qdon[q] << 56) | ((unsigned long long)pair_rank[lo] << 48) |
-             ((unsigned long long)node_bin[g] << 31) | (unsigned long long)(0x7fffffff - g);
+    key[q] = ((unsigned long long)lo << 41) | ((unsigned long long)node_bin[g] << 31) |
+             (unsigned long long)(0x7fffffff - g);
     val[q] = (int)q;
   }
 }
@@ -170,8 +171,7 @@ __global__ void k_dedup_keys_pts(const int* __restrict__ qpt_local, const int* _
       if (pair_qoff[m] <= q) lo = m;
       else hi = m - 1;
     }
-    key[q] = ((unsigned long long)qdon[q] << 56) | ((unsigned long long)pair_rank[lo] << 48) |
-             (unsigned long long)qpt_local[q];
+    key[q] = ((unsigned long long)lo << 40) | (unsigned long long)qpt_local[q];
     val[q] = (int)q;
   }
 }
@@ -181,7 +181,7 @@ __global__ void k_dedup_keys_pts(const int* __restrict__ qpt_local, const int* _
 // or qrec[q] when node_blk is null)
 __global__ void k_dedup_gather(const int* __restrict__ refq, long long n, const int* __restrict__ qnode,
                                const double* __restrict__ qres, const double* __restrict__ x,
-                               const unsigned char* __restrict__ node_blk, const int* __restrict__ qrec,
+                               const blk_t* __restrict__ node_blk, const int* __restrict__ qrec,
                                const BlockInfo* __restrict__ bi, double* __restrict__ xg, int* __restrict__ mtag,
                                double* __restrict__ rtag, int* __restrict__ itag, int* __restrict__ perm,
                                int* __restrict__ gpos_of) {

@@ -41,12 +41,14 @@ __device__ __forceinline__ int donor_list(long long g, const int* __restrict__ s
 
 __global__ void k_fill_slots(const int* __restrict__ qnode, const int* __restrict__ qdon,
                              const int* __restrict__ qcell, long long nq, int K, long long ntot,
-                             long long ctot, int* __restrict__ slot, unsigned* __restrict__ err) {
+                             long long ctot, const BlockInfo* __restrict__ bi, int nb, int* __restrict__ slot,
+                             unsigned* __restrict__ err) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
        q += (long long)gridDim.x * blockDim.x) {
     const int c = qcell[q];
     if (c < 0) continue;
-    const int g = qnode[q], a = qdon[q];
+    const int g = qnode[q], d = qdon[q];
+    const int a = (d >= 0 && d < nb) ? d - bi[d].sblk0 : -1;  // the donor's index within its system
     if (c >= ctot || g < 0 || g >= ntot || a < 0 || a >= K) {
       atomicOr(err, kErrBadIndex);
       continue;
@@ -114,7 +116,7 @@ __global__ void k_donor_reset(const int* __restrict__ mlist, const int* __restri
 // have donors: holes from the hole maps of wall-bearing meshes that supplied
 // none of them, node resolution raised to the candidates' receptor
 // resolutions.  One thread per node (its owner query).
-__global__ void k_classify_queried(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+__global__ void k_classify_queried(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                                    const BlockInfo* __restrict__ bi, const int* __restrict__ slot, int K,
                                    const int* __restrict__ qnode, const int* __restrict__ qcell, long long nq,
                                    const double* __restrict__ qres, const HoleMapDev* __restrict__ hm, int nhm,
@@ -126,19 +128,20 @@ __global__ void k_classify_queried(const double* __restrict__ x, const unsigned 
     if (qcell[q] < 0) continue;
     const int g = qnode[q];
     if (!owner_query(slot, K, g, (int)q)) continue;
-    const int tag = bi[node_blk[g]].tag;
+    const BlockInfo& B = bi[node_blk[g]];
+    const int tag = B.tag;
     unsigned long long seen[2] = {0ull, 0ull};
     double nres = node_res[g];
     for (int a = 0; a < K; a++) {
       const int s = slot[(long long)g * K + a];
       if (s < 0) continue;
-      const int t = bi[a].tag - 1;
+      const int t = bi[B.sblk0 + a].tag - 1;
       seen[t >> 6] |= 1ull << (t & 63);
       nres = dmax(nres, qres[s]);
     }
     const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
     bool hole = false;
-    for (int h = 0; h < nhm && !hole; h++) {
+    for (int h = B.hm_lo; h < B.hm_hi && !hole; h++) {
       const int ht = hm[h].tagidx;
       if (ht == tag - 1 || ((seen[ht >> 6] >> (ht & 63)) & 1ull)) continue;
       hole = check_holemap(p, hm[h]) != 0;
@@ -161,14 +164,13 @@ __global__ void __launch_bounds__(256) k_classify_tiles(
     int* __restrict__ m1, int* __restrict__ mlist, int* __restrict__ dcnt, unsigned long long* __restrict__ counters) {
   __shared__ unsigned s_maps;  // foreign maps that reach the tile (bit h; all bits set past 32 maps)
   const long long T = blockIdx.x;
-  int b = 0;
-  while (b + 1 < nb && tile_base[b + 1] <= T) b++;
+  const int b = block_of_tile(tile_base, nb, T);
   const BlockInfo& B = bi[b];
   if (threadIdx.x == 0) {
     const float4 A = tbox[2 * T], C = tbox[2 * T + 1];
     const float lo[3] = {A.x, A.y, A.z}, hi[3] = {A.w, C.x, C.y};
     unsigned m = 0;
-    for (int h = 0; h < nhm; h++) {
+    for (int h = B.hm_lo; h < B.hm_hi; h++) {
       if (hm[h].tagidx == B.tag - 1) continue;
       bool meet = true;
       for (int k = 0; k < 3; k++) {
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(256) k_classify_tiles(
         const float rhi = __double2float_ru(hm[h].ext[k + 3] + dx + sl);
         meet = meet && !(hi[k] < rlo) && !(lo[k] > rhi);
       }
-      if (meet) m |= (h < 32) ? (1u << h) : 0xffffffffu;
+      if (meet) m |= (h - B.hm_lo < 32) ? (1u << (h - B.hm_lo)) : 0xffffffffu;
     }
     s_maps = m;
   }
@@ -193,8 +195,8 @@ __global__ void __launch_bounds__(256) k_classify_tiles(
     if (has) continue;  // classified with its owner query
     const double p[3] = {x[3 * (long long)g], x[3 * (long long)g + 1], x[3 * (long long)g + 2]};
     bool hole = false;
-    for (int h = 0; h < nhm && !hole; h++) {
-      if (h < 32 && !((maps >> h) & 1u)) continue;
+    for (int h = B.hm_lo; h < B.hm_hi && !hole; h++) {
+      if (h - B.hm_lo < 32 && !((maps >> (h - B.hm_lo)) & 1u)) continue;
       if (hm[h].tagidx == B.tag - 1) continue;
       hole = check_holemap(p, hm[h]) != 0;
     }
@@ -214,7 +216,7 @@ __global__ void k_front_init(int* __restrict__ dcnt) {
 // previous layer's new nodes can add nodes.
 __global__ void k_dilate_front(int iter, const int* __restrict__ csr_off, const int* __restrict__ csr_cell,
                                const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-                               const unsigned char* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                               const blk_t* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
                                const unsigned char* __restrict__ m0, int* __restrict__ m1, int* __restrict__ mlist,
                                int* __restrict__ dcnt) {
   const int* seg = dcnt + kSeg + 2 * (iter & 1);
@@ -263,7 +265,7 @@ __global__ void k_fringe_big_list(const int* __restrict__ mlist, const int* __re
 // that is finer than the node donates; the record is keyed by (donor block,
 // receptor node), which is the order the donor side processes them in.  One
 // thread per node with donors (its owner query).
-__global__ void k_select(const unsigned char* __restrict__ node_blk, const BlockInfo* __restrict__ bi,
+__global__ void k_select(const blk_t* __restrict__ node_blk, const BlockInfo* __restrict__ bi,
                          const int* __restrict__ slot, int K, const int* __restrict__ qnode,
                          const int* __restrict__ qcell, long long nq, const double* __restrict__ cell_res,
                          int* __restrict__ iblank, const double* __restrict__ node_res,
@@ -278,15 +280,16 @@ __global__ void k_select(const unsigned char* __restrict__ node_blk, const Block
     Cand L[kMaxK];
     const int n = donor_list(g, slot, K, qcell, cell_res, L);
     const double nres = node_res[g];
+    const int b0 = bi[node_blk[g]].sblk0;  // donor indices are system-local
     for (int k = 0; k < n; k++) {
       if (L[k].dres < nres) {
-        iblank[g] = -bi[L[k].a].tag;
+        iblank[g] = -bi[b0 + L[k].a].tag;
         const int r = atomicAdd(rcount, 1);
         if (r >= rcap) {
           atomicOr(err, kErrCapacity);
           break;
         }
-        rkey[r] = ((unsigned long long)L[k].a << 32) | (unsigned long long)g;
+        rkey[r] = ((unsigned long long)(b0 + L[k].a) << 32) | (unsigned long long)g;
         rval[r] = L[k].q;
         break;
       }
@@ -329,7 +332,7 @@ __global__ void k_interp_marks(const unsigned long long* __restrict__ rkey, cons
 __global__ void k_interp(const double* __restrict__ x, const unsigned long long* __restrict__ rkey,
                          const int* __restrict__ rval, const int* __restrict__ rcount,
                          const int* __restrict__ qcell, const int* __restrict__ conn8,
-                         const unsigned char* __restrict__ cell_nv, const unsigned char* __restrict__ node_blk,
+                         const unsigned char* __restrict__ cell_nv, const blk_t* __restrict__ node_blk,
                          const BlockInfo* __restrict__ bi, const int* __restrict__ iblank,
                          const double* __restrict__ node_res, const int* __restrict__ reset_t,
                          const int* __restrict__ orig_cell, int* __restrict__ it_node,
@@ -422,12 +425,12 @@ __global__ void k_iblank_final(const int* __restrict__ it_rec, const unsigned ch
 // End of a call: back to the rest state for the next one (slots of the
 // queries with a donor, cancel marks and their reset times).
 __global__ void k_donor_clear(const int* __restrict__ qnode, const int* __restrict__ qdon,
-                              const int* __restrict__ qcell, long long nq, int K, int* __restrict__ slot,
-                              const int* __restrict__ cmlist, const int* __restrict__ dcnt, int* __restrict__ cmark,
-                              int* __restrict__ reset_t) {
+                              const int* __restrict__ qcell, long long nq, int K, const BlockInfo* __restrict__ bi,
+                              int* __restrict__ slot, const int* __restrict__ cmlist, const int* __restrict__ dcnt,
+                              int* __restrict__ cmark, int* __restrict__ reset_t) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += stride)
-    if (qcell[q] >= 0) slot[(long long)qnode[q] * K + qdon[q]] = -1;
+    if (qcell[q] >= 0) slot[(long long)qnode[q] * K + qdon[q] - bi[qdon[q]].sblk0] = -1;
   const int n = dcnt[kCancelMarks];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
     cmark[cmlist[i]] = 0;
@@ -522,7 +525,7 @@ __global__ void k_interp_gather(const int* __restrict__ it_node, const double* _
 }
 
 __global__ void k_interp_scatter(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
-                                 const int* __restrict__ rcount, const unsigned char* __restrict__ node_blk,
+                                 const int* __restrict__ rcount, const blk_t* __restrict__ node_blk,
                                  const BlockInfo* __restrict__ bi, const double* __restrict__ vals, int nvar,
                                  int interptype, double* __restrict__ q) {
   const int R = *rcount;

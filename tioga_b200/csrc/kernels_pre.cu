@@ -10,7 +10,7 @@ namespace tb {
 // ---------------------------------------------------------------------------
 __global__ void k_conn_convert(const int* __restrict__ raw, int nc, int nv, int node_off,
                                int cell_base, int blk, int* __restrict__ conn8,
-                               unsigned char* __restrict__ cell_nv, unsigned char* __restrict__ cell_blk) {
+                               unsigned char* __restrict__ cell_nv, blk_t* __restrict__ cell_blk) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc;
        i += (long long)gridDim.x * blockDim.x) {
     long long c = cell_base + i;
@@ -21,14 +21,14 @@ __global__ void k_conn_convert(const int* __restrict__ raw, int nc, int nv, int 
     dst[0] = make_int4(v[0], v[1], v[2], v[3]);
     dst[1] = make_int4(v[4], v[5], v[6], v[7]);
     cell_nv[c] = (unsigned char)nv;
-    cell_blk[c] = (unsigned char)blk;
+    cell_blk[c] = (blk_t)blk;
   }
 }
 
-__global__ void k_node_blk(int node_off, int nnodes, int blk, unsigned char* node_blk) {
+__global__ void k_node_blk(int node_off, int nnodes, int blk, blk_t* node_blk) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nnodes;
        i += (long long)gridDim.x * blockDim.x)
-    node_blk[node_off + i] = (unsigned char)blk;
+    node_blk[node_off + i] = (blk_t)blk;
 }
 
 __global__ void k_mark_list(const int* __restrict__ list, int n, int node_off, int* __restrict__ glist,
@@ -89,7 +89,7 @@ __global__ void k_csr_sort(const int* __restrict__ off, long long ntot, int* __r
 // ---------------------------------------------------------------------------
 __global__ void k_cell_volume(const double* __restrict__ x, const int* __restrict__ conn8,
                               const unsigned char* __restrict__ cell_nv,
-                              const unsigned char* __restrict__ cell_blk,
+                              const blk_t* __restrict__ cell_blk,
                               const BlockInfo* __restrict__ bi, long long ctot,
                               double* __restrict__ cell_res) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
@@ -103,7 +103,7 @@ __global__ void k_cell_volume(const double* __restrict__ x, const int* __restric
 }
 
 __global__ void k_node_res(const int* __restrict__ off, const int* __restrict__ cells,
-                           const double* __restrict__ cell_res, const unsigned char* __restrict__ node_blk,
+                           const double* __restrict__ cell_res, const blk_t* __restrict__ node_blk,
                            const BlockInfo* __restrict__ bi, long long ntot, double* __restrict__ node_res) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
        g += (long long)gridDim.x * blockDim.x) {
@@ -173,10 +173,18 @@ __global__ void k_fill_int(int* __restrict__ a, int v, long long n) {
 // reference sums sequentially; the box only culls, so the rounding of its
 // last bits cannot change a result).
 // ---------------------------------------------------------------------------
-__global__ void k_obb_partial(const double* __restrict__ x, int off, int n, int pass,
-                              const Obb* __restrict__ obb, double* __restrict__ part) {
+// Every block at once: blockIdx.y is the block, gridDim.x CTAs share its
+// nodes (the same split for any number of blocks, so a block's box does not
+// depend on the others).
+__global__ void k_obb_partial(const double* __restrict__ x, const BlockInfo* __restrict__ bi, int pass,
+                              double* __restrict__ part_all) {
   // pass 0: sums of x; pass 1: covariance; pass 2: min/max of the projections
   // and of the raw coordinates
+  const BlockInfo& B = bi[blockIdx.y];
+  const int off = B.node_off, n = B.nnodes;
+  if (n == 0 || (pass == 1 && n < 4)) return;
+  const Obb* __restrict__ obb = &B.obb;
+  double* __restrict__ part = part_all + 12 * (size_t)gridDim.x * blockIdx.y;
   double acc[12];
   for (int k = 0; k < 12; k++) acc[k] = (pass == 2) ? ((k % 2 == 0) ? 1e300 : -1e300) : 0.0;
   double xc0 = 0, xc1 = 0, xc2 = 0;
@@ -294,10 +302,15 @@ __device__ void kaiser3(double* a, double* eigenv) {
 #undef A_
 }
 
-__global__ void k_obb_finish(const double* __restrict__ part, int nparts, int n, int pass,
-                             const double* __restrict__ x, int off, Obb* __restrict__ obb,
-                             BlockInfo* __restrict__ bi) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void k_obb_finish(const double* __restrict__ part_all, int nparts, int pass, const double* __restrict__ x,
+                             BlockInfo* __restrict__ bi_all, int nb) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  BlockInfo* __restrict__ bi = bi_all + b;
+  const int off = bi->node_off, n = bi->nnodes;
+  if (n == 0 || (pass == 1 && n < 4)) return;
+  const double* __restrict__ part = part_all + 12 * (size_t)nparts * b;
+  Obb* __restrict__ obb = &bi->obb;
   double r[12];
   for (int k = 0; k < 12; k++) r[k] = part[k];
   for (int t = 1; t < nparts; t++)
@@ -338,6 +351,12 @@ __global__ void k_obb_finish(const double* __restrict__ part, int nparts, int n,
     kaiser3(aa, eig);
     for (int i = 0, m = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) o.vec[i][j] = aa[m++];
+  } else if (n < 4) {  // the box stays as set from the points; the raw box feeds the Morton keys
+    for (int j = 0; j < 3; j++) {
+      bi->bb_lo[j] = (float)r[6 + 2 * j];
+      bi->bb_hi[j] = (float)r[6 + 2 * j + 1];
+    }
+    return;
   } else {
     double xd[3];
     for (int j = 0; j < 3; j++) {
@@ -368,7 +387,7 @@ __device__ inline unsigned spread10(unsigned v) {
 
 __global__ void k_morton(const double* __restrict__ x, const int* __restrict__ conn8,
                          const unsigned char* __restrict__ cell_nv,
-                         const unsigned char* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                         const blk_t* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
                          long long ctot, unsigned long long* __restrict__ key, int* __restrict__ val) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
        c += (long long)gridDim.x * blockDim.x) {
@@ -392,7 +411,7 @@ __global__ void k_morton(const double* __restrict__ x, const int* __restrict__ c
 
 // Morton keys of node positions, block id in the high word (the order in
 // which query points are gathered, so a warp's queries are neighbours)
-__global__ void k_morton_nodes(const double* __restrict__ x, const unsigned char* __restrict__ node_blk,
+__global__ void k_morton_nodes(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                                const BlockInfo* __restrict__ bi, long long ntot, unsigned long long* __restrict__ key,
                                int* __restrict__ val) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
@@ -413,9 +432,9 @@ __global__ void k_morton_nodes(const double* __restrict__ x, const unsigned char
 // Cell arrays from registration order to storage (Morton) order:
 // dst[s] = src[perm[s]].
 __global__ void k_permute_cells(const int* __restrict__ perm, long long n, const int* __restrict__ conn8,
-                                const unsigned char* __restrict__ nv, const unsigned char* __restrict__ blk,
+                                const unsigned char* __restrict__ nv, const blk_t* __restrict__ blk,
                                 int* __restrict__ conn8_out, unsigned char* __restrict__ nv_out,
-                                unsigned char* __restrict__ blk_out) {
+                                blk_t* __restrict__ blk_out) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
        s += (long long)gridDim.x * blockDim.x) {
     const long long c = perm[s];

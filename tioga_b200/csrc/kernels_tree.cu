@@ -120,7 +120,7 @@ __global__ void k_leaf_flags(const int* __restrict__ leaf_at, long long ctot, in
 }
 
 __global__ void k_leaf_list(const int* __restrict__ leaf_at, const int* __restrict__ loff, long long ctot,
-                            const int2* __restrict__ tlink, const unsigned char* __restrict__ cell_blk,
+                            const int2* __restrict__ tlink, const blk_t* __restrict__ cell_blk,
                             int4* __restrict__ leaves) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
        c += (long long)gridDim.x * blockDim.x) {
@@ -156,6 +156,16 @@ __global__ void k_refit_level(int g0, int g1, const int* __restrict__ gparent, f
       }
       for (int j = 0; j < 6; j++) tnode64[6 * (long long)p + j] = d[j];
     }
+  }
+}
+
+// first leaf of every block that has leaves (leaves are in storage order,
+// which is block-major)
+__global__ void k_block_leaves(const int4* __restrict__ leaves, long long nleaf, int* __restrict__ first) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nleaf;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int b = leaves[i].w;
+    if (i == 0 || leaves[i - 1].w != b) first[b] = (int)i;
   }
 }
 
