@@ -69,6 +69,8 @@ def parse():
     p.add_argument("--cpu-reps", type=int, default=3)
     p.add_argument("--size", default="full", choices=["full", "medium", "small"],
                    help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
+    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2"],
+                   help="cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems")
     p.add_argument("--forms", default="split,plain,e2e",
                    help="comma list of measured forms (the first one gives `value`)")
     return p.parse_args()
@@ -315,6 +317,161 @@ def run_gpu(args, ws, rank, local, dist):
 
 
 # ---------------------------------------------------------------------------
+# batched form: 64 independent systems in one instance
+# ---------------------------------------------------------------------------
+WORKLOAD2 = ("cfg2: 64 independent overset systems (background box + 1-4 spherical shells, node counts "
+             "log-uniform in [5e4, 2e6], all-hex or mixed-element with p=0.5), seed 2, one instance")
+
+
+def batch_systems(args):
+    if args.size == "small":
+        return cases.config2(2, nsys=8, nmin=5e3, nmax=5e4)
+    if args.size == "medium":
+        return cases.config2(2, nsys=16, nmin=2e4, nmax=5e5)
+    return cases.config2(2)
+
+
+def run_gpu_batch(args, ws, rank, local, dist):
+    """The batched form against the plain form on the same systems: every
+    system in one instance (one launch per stage over all of them) versus one
+    system per instance, one after another (the reference's way of running
+    independent systems)."""
+    import torch
+
+    import tioga_b200 as tb
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    systems = batch_systems(args)
+    pinned = [pinned_copy(s) for s in systems]
+    lib = TiogaLibrary(tb.library_path())
+    tb.extras(lib.lib)
+    lib.lib.tioga_b200_nsystems_.restype = C.c_int
+
+    def events_time(steps, warmup, clocks=None):
+        for _ in range(warmup):
+            lib.performconnectivity()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        phases, launches = [], 0
+        dist.barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        ev[0].record(stream)
+        for k in range(steps):
+            lib.performconnectivity()
+            ev[k + 1].record(stream)
+            phases.append(tb.timing(lib.lib))
+            launches += tb.stats(lib.lib)["launches"]
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        dist.barrier()
+        if lib.lib.tioga_b200_last_error() != 0:
+            raise RuntimeError("connectivity failed during timing")
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        avg = {k: float(np.mean([p[k] for p in phases])) for k in phases[0]}
+        return ev[0].elapsed_time(ev[steps]) / steps, per, tb.stats(lib.lib), avg, launches, clk
+
+    # plain form: one system per instance, one after another
+    plain_ms = {0: 0.0, 1: 0.0}
+    plain_q = 0
+    for (psys, ibls, _keep) in pinned:
+        lib.init()
+        lib.register_system(psys, ibls)
+        lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
+        tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
+        lib.preprocess_grids()
+        for prec in (1, 0):
+            tb.set_int(lib.lib, "tioga_b200_set_precision_", prec)
+            ms, _, st, _, _, _ = events_time(max(1, args.steps // 2), 1)
+            plain_ms[prec] += ms
+        plain_q += st["nquery"]
+        lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
+        lib.delete()
+    # batched form
+    lib.init()
+    for k, (psys, ibls, _keep) in enumerate(pinned):
+        for bid, (b, ib) in enumerate(zip(psys.blocks, ibls), start=1):
+            lib.select_system(k)
+            lib.registergrid_data_mb(bid, b, ib)
+    assert lib.lib.tioga_b200_nsystems_() == len(systems)
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+    lib.preprocess_grids()
+    d_ibl = []
+    for k, s in enumerate(systems):
+        lib.select_system(k)
+        for b in s.blocks:
+            d = torch.ones(b.nnodes, dtype=torch.int32, device="cuda")
+            d_ibl.append(d)
+            lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(d.data_ptr()))
+    tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = Clocks(vis.split(",")[local] if vis else str(local))
+    ms_b, per_b, st, ph, launches, clk = events_time(args.steps, args.warmup, clocks)
+    Q = st["nquery"]
+    assert Q == plain_q, (Q, plain_q)
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 0)
+    ms_b64, _, st64, _, _, _ = events_time(max(1, args.steps // 2), 1)
+    assert st64["nquery"] == Q
+    # end to end: host coordinates in, host iblanks out, every step
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+    tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 0)
+    for k, s in enumerate(systems):
+        lib.select_system(k)
+        for b in s.blocks:
+            lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(0))
+    ms_e2e, _, st_e, _, _, _ = events_time(args.steps, args.warmup)
+    assert st_e["nquery"] == Q
+    nodes = sum(s.nnodes for s in systems)
+    cells = sum(s.ncells for s in systems)
+    h2d, d2h = 24 * nodes, 4 * nodes
+    cell_ms = ph["cell_pass"]
+    nvsum = sum(nv * conn.shape[0] for s in systems for b in s.blocks for nv, conn in b.cells)
+    alg_bytes = 4 * nvsum + cells * (1 + 24) + nodes * 16 + st["nleaf"] * (16 + 24)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (cell_ms * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": ws * Q / (ms_b * 1e-3), "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator tioga_b200.cases.config2)",
+        "config": {"workload": WORKLOAD2 if args.size == "full" else f"cfg2 distribution, {args.size} size",
+                   "systems": len(systems), "nodes": nodes, "cells": cells,
+                   "blocks": sum(len(s.blocks) for s in systems), "query_points": Q,
+                   "receptors": st["nreceptor"], "holes": st["nhole"],
+                   "precision": "fp32 Newton screen + fp64 refinement", "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (coordinates %.0f MB)" % (h2d / 1e6)},
+        "latency_ms": {"p50": float(np.percentile(per_b, 50)), "p99": float(np.percentile(per_b, 99)),
+                       "max": float(np.max(per_b))},
+        "plain": {"value": ws * Q / (plain_ms[0] * 1e-3), "ms_per_step": plain_ms[0],
+                  "form": "one system per instance, one after another, fp64 throughout"},
+        "plain_split": {"value": ws * Q / (plain_ms[1] * 1e-3), "ms_per_step": plain_ms[1],
+                        "form": "one system per instance, one after another, split precision"},
+        "batched_fp64": {"value": ws * Q / (ms_b64 * 1e-3), "ms_per_step": ms_b64},
+        "speedup_vs_plain": plain_ms[0] / ms_b,
+        "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+        "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": CELL_PASS_DRAM_BYTES_PER_CELL * cells, "algorithmic_bytes": alg_bytes,
+                     "launch_ms": cell_ms, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "phases_ms": ph,
+        "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
+                   "donors": st["ndonor"]},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
+    lib.delete()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # CPU: the compiled reference (or the C restatement) on a bounded sample
 # ---------------------------------------------------------------------------
 def sample_query_count(sample):
@@ -383,7 +540,7 @@ def main():
         if ws > 1:
             import torch
             torch.cuda.set_device(local)
-        out = run_gpu(args, ws, rank, local, dist)
+        out = (run_gpu_batch if args.workload == "cfg2" else run_gpu)(args, ws, rank, local, dist)
     finally:
         dist.close()
     if rank == 0:

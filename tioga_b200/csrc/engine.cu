@@ -334,7 +334,10 @@ int Engine::upload_topology() {
                             stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above go out of scope
   // hole map state: one fixed-size slab per wall-bearing block
-  if (nhm_all_ > 0) TB_CUDA(hm_state_.ensure((size_t)nhm_all_ * kHoleMapCap));
+  if (nhm_all_ > 0) {  // no stale wall marks (2) in a fresh map: the plane fill treats the rest as unmarked
+    TB_CUDA(hm_state_.ensure((size_t)nhm_all_ * kHoleMapCap));
+    TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nhm_all_ * kHoleMapCap, stream_));
+  }
   TB_CUDA(d_hm_.ensure(std::max(nhm_all_, 1)));
   TB_CUDA(wall_bb_.ensure(6 * std::max(nhm_all_, 1)));
   TB_CUDA(d_hmdev_.ensure(std::max(nhm_all_, 1)));
@@ -587,6 +590,46 @@ int Engine::build_tree_topology() {
     for (int b = nb - 1; b >= 0; b--)
       if (h_blk_leaf_[b] < 0) h_blk_leaf_[b] = h_blk_leaf_[b + 1];
   }
+  // cells (storage order) that mark their wall-bearing block's hole map
+  {
+    DBuf<int> flag, off;
+    TB_CUDA(flag.ensure(ctot_ + 1));
+    TB_CUDA(off.ensure(ctot_ + 1));
+    k_wall_cell_flags<<<grid_for(ctot_, kT), kT, 0, stream_>>>(conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p, wallf_.p,
+                                                               ctot_, flag.p);
+    TB_LAUNCHED("k_wall_cell_flags");
+    TB_CUDA(cudaMemsetAsync(flag.p + ctot_, 0, sizeof(int), stream_));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag.p, off.p, (int)(ctot_ + 1), stream_);
+    TB_CUDA(cub_tmp_.ensure(tmp));
+    cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, flag.p, off.p, (int)(ctot_ + 1), stream_);
+    int nwc = 0;
+    TB_CUDA(cudaMemcpyAsync(&nwc, off.p + ctot_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    nwall_cells_ = nwc;
+    TB_CUDA(wall_cells_.ensure(std::max(nwc, 1)));
+    const int nh = std::max(nhm_all_, 1);
+    TB_CUDA(wall_box_first_.ensure(nh + 1));
+    TB_CUDA(wall_box_.ensure(std::max(nwc, 1)));
+    TB_CUDA(cudaMemsetAsync(wall_box_first_.p, 0xff, (nh + 1) * sizeof(int), stream_));
+    if (nwc > 0) {
+      k_wall_cell_list<<<grid_for(ctot_, kT), kT, 0, stream_>>>(flag.p, off.p, ctot_, wall_cells_.p);
+      TB_LAUNCHED("k_wall_cell_list");
+      k_wall_map_first<<<grid_for(nwc, kT), kT, 0, stream_>>>(wall_cells_.p, nwc, cell_blk_.p, d_bi_.p,
+                                                              wall_box_first_.p);
+      TB_LAUNCHED("k_wall_map_first");
+    }
+    // wall cells of map t: [first[t], first[t + 1]) (maps without any: empty)
+    std::vector<int> first(nh + 1);
+    TB_CUDA(cudaMemcpyAsync(first.data(), wall_box_first_.p, nh * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    first[nh] = nwc;
+    for (int t = nh - 1; t >= 0; t--)
+      if (first[t] < 0) first[t] = first[t + 1];
+    TB_CUDA(cudaMemcpyAsync(wall_box_first_.p, first.data(), (nh + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                            stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+  }
   // query-gathering tiles of kNodeTile nodes per block
   h_tile_base_.assign(bi_.size() + 1, 0);
   for (size_t b = 0; b < bi_.size(); b++)
@@ -703,15 +746,25 @@ int Engine::run_holemaps() {
   TB_LAUNCHED("k_wall_bounds");
   k_holemap_setup<<<(nh + 127) / 128, 128, 0, stream_>>>(wall_bb_.p, d_hm_.p, nh);
   TB_LAUNCHED("k_holemap_setup");
-  TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nh * kHoleMapCap, stream_));
-  k_holemap_mark<<<dim3(grid_for(maxc, kT), nw), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, d_wall_.p, wallf_.p,
-                                                                 d_hm_.p, hm_state_.p, kHoleMapCap);
-  TB_LAUNCHED("k_holemap_mark");
+  const bool planar = (isym_ == 1 || isym_ == 2 || isym_ == 3);
+  // the plane fill rewrites every cell of its map, so only this call's marks
+  // (2) count there; the 6-neighbour fill reads the map as it is
+  if (!planar) TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nh * kHoleMapCap, stream_));
+  if (nwall_cells_ > 0 && planar) {  // the boxes the plane fill marks in shared memory
+    k_holemap_boxes<<<grid_for(nwall_cells_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
+                                                                    nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
+                                                                    wall_box_.p);
+    TB_LAUNCHED("k_holemap_boxes");
+  } else if (nwall_cells_ > 0) {
+    k_holemap_mark<<<grid_for(nwall_cells_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
+                                                                   nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
+                                                                   hm_state_.p, kHoleMapCap);
+    TB_LAUNCHED("k_holemap_mark");
+  }
   std::vector<HoleMapInfo> hinfo(nh);
   TB_CUDA(cudaMemcpyAsync(hinfo.data(), d_hm_.p, nh * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   const int isym = isym_;
-  const bool planar = (isym == 1 || isym == 2 || isym == 3);
   const int pa = (isym == 1) ? 0 : (isym == 2) ? 1 : 2;
   const int a0 = (pa == 0) ? 1 : 0, a1 = (pa == 2) ? 1 : 2;
   int maxpl = 1;
@@ -727,10 +780,14 @@ int Engine::run_holemaps() {
     smem = std::max(smem, (size_t)h.nx[a0] * h.nx[a1]);
     maxcells = std::max(maxcells, (long long)h.nx[0] * h.nx[1] * h.nx[2]);
   }
-  k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, stream_>>>(
-      hm_state_.p, d_hm_.p, kHoleMapCap, planar ? isym : 3, planar ? 0 : 1, err_.p);
-  TB_LAUNCHED("k_holemap_fill_planes");
-  if (!planar) {  // 6-neighbour fill: line sweeps over the three axes until no map changes
+  if (planar) {  // fill and final map in one pass
+    k_holemap_fill_bits<<<dim3(std::min(maxpl, 148 * 4), nh), 256, 0, stream_>>>(
+        hm_state_.p, d_hm_.p, kHoleMapCap, wall_box_.p, wall_box_first_.p, isym, err_.p);
+    TB_LAUNCHED("k_holemap_fill_bits");
+  } else {
+    k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, stream_>>>(hm_state_.p, d_hm_.p,
+                                                                                     kHoleMapCap, 3, 1, err_.p);
+    TB_LAUNCHED("k_holemap_fill_planes");  // 6-neighbour fill: line sweeps over the three axes until no map changes
     unsigned* d_changed = err_.p + 1;
     int maxsum = 0;
     for (const HoleMapInfo& h : hinfo) maxsum = std::max(maxsum, h.nx[0] + h.nx[1] + h.nx[2]);
@@ -746,9 +803,9 @@ int Engine::run_holemaps() {
       TB_CUDA(cudaStreamSynchronize(stream_));
       if (!ch) break;
     }
+    k_holemap_final<<<dim3(grid_for(maxcells, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p, kHoleMapCap);
+    TB_LAUNCHED("k_holemap_final");
   }
-  k_holemap_final<<<dim3(grid_for(maxcells, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p, kHoleMapCap);
-  TB_LAUNCHED("k_holemap_final");
   std::vector<HoleMapDev> hdev(nh);
   for (int b = 0; b < (int)bi_.size(); b++) {
     const int t = bi_[b].hm;

@@ -342,6 +342,10 @@ class Engine {
   DBuf<long long> d_pair_t0_;       // query tiles of pair p: [pair_t0[p], pair_t0[p + 1])
   std::vector<long long> h_pair_t0_;
   std::vector<WallBlock> h_wall_;
+  DBuf<int> wall_cells_;            // cells touching a wall node, storage order (hole-map marking)
+  int nwall_cells_ = 0;
+  DBuf<unsigned long long> wall_box_;  // each wall cell's marked index box this call (packed)
+  DBuf<int> wall_box_first_;        // wall cells of hole map t: [first[t], first[t + 1])
   DBuf<WallBlock> d_wall_;
   DBuf<int> d_npairs_;
   DBuf<HoleMapInfo> d_hm_;

@@ -78,8 +78,19 @@ __global__ void k_morton(const double* x, const int* conn8, const unsigned char*
 // ---- connectivity (kernels_conn.cu) ----
 __global__ void k_wall_bounds(const double* x, const int* wall_list, const WallBlock* wt, unsigned long long* bb);
 __global__ void k_holemap_setup(const unsigned long long* bb, HoleMapInfo* hm, int nhm);
-__global__ void k_holemap_mark(const double* x, const int* conn8, const unsigned char* cell_nv, const WallBlock* wt,
-                               const unsigned char* wallf, const HoleMapInfo* hm, unsigned char* sam, size_t cap);
+__global__ void k_holemap_mark(const double* x, const int* conn8, const unsigned char* cell_nv, const int* wall_cells,
+                               int nwc, const blk_t* cell_blk, const BlockInfo* bi, const HoleMapInfo* hm,
+                               unsigned char* sam, size_t cap);
+__global__ void k_wall_cell_flags(const int* conn8, const unsigned char* cell_nv, const blk_t* cell_blk,
+                                  const BlockInfo* bi, const unsigned char* wallf, long long ctot, int* flag);
+__global__ void k_wall_cell_list(const int* flag, const int* off, long long ctot, int* list);
+__global__ void k_holemap_fill_bits(unsigned char* sam, const HoleMapInfo* hm, size_t cap, const unsigned long long* box,
+                                    const int* box_first, int isym, unsigned* err);
+__global__ void k_wall_map_first(const int* wall_cells, int nwc, const blk_t* cell_blk, const BlockInfo* bi,
+                                 int* first);
+__global__ void k_holemap_boxes(const double* x, const int* conn8, const unsigned char* cell_nv, const int* wall_cells,
+                                int nwc, const blk_t* cell_blk, const BlockInfo* bi, const HoleMapInfo* hm,
+                                unsigned long long* box);
 __global__ void k_holemap_fill_planes(unsigned char* sam, const HoleMapInfo* hm, size_t cap, int isym, int seed,
                                       unsigned* err);
 __global__ void k_holemap_lines(unsigned char* sam, const HoleMapInfo* hm, size_t cap, int axis, unsigned* changed);

@@ -63,26 +63,25 @@ __global__ void k_holemap_setup(const unsigned long long* __restrict__ bb, HoleM
   h.exist = 1;
 }
 
-// wall-touching cells mark their index box with 2 (MeshBlock.C:666-772);
-// blockIdx.y indexes the wall table.  Sizes past the slab are left alone (the
-// host rejects such a map before it is used).
+// wall-touching cells mark their index box with 2 (MeshBlock.C:666-772):
+// one thread per cell of the wall-cell list (cells of wall-bearing blocks
+// with a wall node).  Maps past the slab are left alone (the host rejects
+// such a map before it is used).
 __global__ void k_holemap_mark(const double* __restrict__ x, const int* __restrict__ conn8,
-                               const unsigned char* __restrict__ cell_nv, const WallBlock* __restrict__ wt,
-                               const unsigned char* __restrict__ wallf, const HoleMapInfo* __restrict__ hm_all,
-                               unsigned char* __restrict__ sam_all, size_t cap) {
-  const WallBlock W = wt[blockIdx.y];
-  const HoleMapInfo h = hm_all[W.hm];
-  if ((size_t)h.nx[0] * h.nx[1] * h.nx[2] > cap) return;
-  unsigned char* __restrict__ sam = sam_all + (size_t)W.hm * cap;
-  double ds[3];
-  for (int k = 0; k < 3; k++) ds[k] = (h.ext[k + 3] - h.ext[k]) / h.nx[k];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.ncells; i += gridDim.x * blockDim.x) {
-    long long c = (long long)W.cell_off + i;
-    int nv = cell_nv[c];
+                               const unsigned char* __restrict__ cell_nv, const int* __restrict__ wall_cells,
+                               int nwc, const blk_t* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                               const HoleMapInfo* __restrict__ hm_all, unsigned char* __restrict__ sam_all,
+                               size_t cap) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwc; i += gridDim.x * blockDim.x) {
+    const long long c = wall_cells[i];
+    const int t = bi[cell_blk[c]].hm;
+    const HoleMapInfo h = hm_all[t];
+    if ((size_t)h.nx[0] * h.nx[1] * h.nx[2] > cap) continue;
+    unsigned char* __restrict__ sam = sam_all + (size_t)t * cap;
+    double ds[3];
+    for (int k = 0; k < 3; k++) ds[k] = (h.ext[k + 3] - h.ext[k]) / h.nx[k];
+    const int nv = cell_nv[c];
     const int* cv = conn8 + 8 * c;
-    int wall = 0;
-    for (int m = 0; m < nv; m++) wall |= wallf[cv[m]];
-    if (!wall) continue;
     int imin[3] = {kBigInt, kBigInt, kBigInt}, imax[3] = {-kBigInt, -kBigInt, -kBigInt};
     for (int m = 0; m < nv; m++) {
       const double* p = x + 3 * (long long)cv[m];
@@ -100,6 +99,252 @@ __global__ void k_holemap_mark(const double* __restrict__ x, const int* __restri
       for (int jj = imin[1]; jj < imax[1] + 1; jj++)
         for (int ii = imin[0]; ii < imax[0] + 1; ii++)
           sam[(size_t)kk * h.nx[1] * h.nx[0] + (size_t)jj * h.nx[0] + ii] = 2;
+  }
+}
+
+// cells of wall-bearing blocks that touch a wall node
+__global__ void k_wall_cell_flags(const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+                                  const blk_t* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                                  const unsigned char* __restrict__ wallf, long long ctot, int* __restrict__ flag) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
+       c += (long long)gridDim.x * blockDim.x) {
+    int w = 0;
+    if (bi[cell_blk[c]].hm >= 0) {
+      const int nv = cell_nv[c];
+      for (int m = 0; m < nv; m++) w |= wallf[conn8[8 * c + m]];
+    }
+    flag[c] = w ? 1 : 0;
+  }
+}
+
+__global__ void k_wall_cell_list(const int* __restrict__ flag, const int* __restrict__ off, long long ctot,
+                                 int* __restrict__ list) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ctot;
+       c += (long long)gridDim.x * blockDim.x)
+    if (flag[c]) list[off[c]] = (int)c;
+}
+
+// first wall cell of every hole map (the list is block-major, and maps are
+// numbered in block order)
+__global__ void k_wall_map_first(const int* __restrict__ wall_cells, int nwc, const blk_t* __restrict__ cell_blk,
+                                 const BlockInfo* __restrict__ bi, int* __restrict__ first) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwc; i += gridDim.x * blockDim.x) {
+    const int t = bi[cell_blk[wall_cells[i]]].hm;
+    if (i == 0 || bi[cell_blk[wall_cells[i - 1]]].hm != t) first[t] = i;
+  }
+}
+
+// The index box every wall cell marks (MeshBlock.C:666-772, the same
+// floor((x - lo) / ds) per vertex, clamped to the map), packed into 48 bits:
+// imin x, y, z | imax x, y, z, a byte each (maps have at most 197 cells per
+// axis).  An empty box gets imin z = 255, imax z = 0.
+__global__ void k_holemap_boxes(const double* __restrict__ x, const int* __restrict__ conn8,
+                                const unsigned char* __restrict__ cell_nv, const int* __restrict__ wall_cells, int nwc,
+                                const blk_t* __restrict__ cell_blk, const BlockInfo* __restrict__ bi,
+                                const HoleMapInfo* __restrict__ hm_all, unsigned long long* __restrict__ box) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwc; i += gridDim.x * blockDim.x) {
+    const long long c = wall_cells[i];
+    const HoleMapInfo h = hm_all[bi[cell_blk[c]].hm];
+    double ds[3];
+    for (int k = 0; k < 3; k++) ds[k] = (h.ext[k + 3] - h.ext[k]) / h.nx[k];
+    const int nv = cell_nv[c];
+    const int* cv = conn8 + 8 * c;
+    int imin[3] = {kBigInt, kBigInt, kBigInt}, imax[3] = {-kBigInt, -kBigInt, -kBigInt};
+    for (int m = 0; m < nv; m++) {
+      const double* p = x + 3 * (long long)cv[m];
+      for (int k = 0; k < 3; k++) {
+        int iv = (int)floor((p[k] - h.ext[k]) / ds[k]);
+        imin[k] = min(imin[k], iv);
+        imax[k] = max(imax[k], iv);
+      }
+    }
+    bool empty = false;
+    for (int j = 0; j < 3; j++) {
+      imin[j] = max(imin[j], 0);
+      imax[j] = min(imax[j], h.nx[j] - 1);
+      empty = empty || imin[j] > imax[j] || h.nx[j] > 255;
+    }
+    unsigned long long v = 0;
+    if (empty) {
+      v = 255ull << 16;
+    } else {
+      for (int j = 0; j < 3; j++)
+        v |= ((unsigned long long)imin[j] << (8 * j)) | ((unsigned long long)imax[j] << (24 + 8 * j));
+    }
+    box[i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bit-parallel plane fill for isym = 1, 2, 3 (utils.c:192-295 with the
+// in-plane 4-neighbour sweeps): one CTA per plane normal to the symmetry
+// axis.  Every line of the plane is a 224-bit mask (7 words): passable cells
+// (not wall-marked, or seeded) and filled cells (seeds: the six box faces,
+// utils.c:206-226).  A line is filled in one step: adding the seeds to the
+// passable mask carries through each run of passable cells above its lowest
+// seed, and the same on the bit-reversed line covers the run below its
+// highest seed, so every run holding a seed becomes filled.  Rows and columns
+// alternate (a shuffle bit transpose between them) until a round changes
+// nothing: the closure of the seeds through unmarked cells, the fixed point
+// of the reference's Gauss-Seidel sweeps.  The plane is written back as the
+// final map (1 = hole: wall-marked or unreached), so no separate pass is
+// needed, and cells that are not marked 2 by this call count as unmarked
+// whatever the map held before.
+// ---------------------------------------------------------------------------
+constexpr int kHW = 7;            // words per line: 224 >= 197 cells
+constexpr int kHL = 32 * kHW;     // lines per plane at most (row and column tables)
+
+__device__ __forceinline__ bool line_fill(unsigned* __restrict__ F, const unsigned* __restrict__ M) {
+  unsigned S[kHW], U[kHW], Mr[kHW], Sr[kHW];
+#pragma unroll
+  for (int w = 0; w < kHW; w++) S[w] = F[w] & M[w];
+  unsigned long long c = 0;
+#pragma unroll
+  for (int w = 0; w < kHW; w++) {  // upwards from the lowest seed of every run
+    const unsigned long long t = (unsigned long long)M[w] + S[w] + c;
+    U[w] = (((unsigned)t ^ M[w]) & M[w]) | S[w];
+    c = t >> 32;
+  }
+#pragma unroll
+  for (int w = 0; w < kHW; w++) {
+    Mr[w] = __brev(M[kHW - 1 - w]);
+    Sr[w] = __brev(S[kHW - 1 - w]);
+  }
+  c = 0;
+  bool ch = false;
+#pragma unroll
+  for (int w = 0; w < kHW; w++) {  // downwards from the highest seed (on the reversed line)
+    const unsigned long long t = (unsigned long long)Mr[w] + Sr[w] + c;
+    Sr[w] = (((unsigned)t ^ Mr[w]) & Mr[w]) | Sr[w];
+    c = t >> 32;
+  }
+#pragma unroll
+  for (int w = 0; w < kHW; w++) {
+    const unsigned v = U[w] | __brev(Sr[kHW - 1 - w]);
+    ch = ch || (v != F[w]);
+    F[w] = v;
+  }
+  return ch;
+}
+
+// dst[c][w'] bit b' = src[32 w' + b'][w] bit (c - 32 w) for source lines <
+// nsrc and destination lines < ndst: one warp per 32x32 tile, transposed in
+// five shuffle stages (off-diagonal half blocks swapped, then recursively).
+__device__ __forceinline__ void bit_transpose(const unsigned (*__restrict__ src)[kHW], int nsrc,
+                                              unsigned (*__restrict__ dst)[kHW], int ndst) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int wmax = (ndst + 31) >> 5, lmax = (nsrc + 31) >> 5;  // tiles that hold any line
+  for (int t = warp; t < wmax * lmax; t += nwarps) {
+    const int w = t % wmax, wp = t / wmax;  // source word, source line block
+    const int r = 32 * wp + lane;
+    unsigned x = (r < nsrc) ? src[r][w] : 0u;
+#pragma unroll
+    for (int j = 16, m = 0x0000ffff; j > 0; j >>= 1, m ^= (m << j)) {
+      const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
+      x = (lane & j) ? ((x & ~(unsigned)m) | ((y & ~(unsigned)m) >> j)) : ((x & (unsigned)m) | ((y & (unsigned)m) << j));
+    }
+    if (32 * w + lane < ndst) dst[32 * w + lane][wp] = x;
+  }
+}
+
+__global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __restrict__ sam_all,
+                                                           const HoleMapInfo* __restrict__ hm_all, size_t cap,
+                                                           const unsigned long long* __restrict__ box,
+                                                           const int* __restrict__ box_first, int isym,
+                                                           unsigned* __restrict__ err) {
+  __shared__ unsigned pr[kHL][kHW], fr[kHL][kHW], pc[kHL][kHW], fc[kHL][kHW];
+  const HoleMapInfo h = hm_all[blockIdx.y];
+  unsigned char* __restrict__ sam = sam_all + (size_t)blockIdx.y * cap;
+  const int b0 = box_first[blockIdx.y], b1 = box_first[blockIdx.y + 1];
+  const int n[3] = {h.nx[0], h.nx[1], h.nx[2]};
+  const long long st[3] = {1, n[0], (long long)n[0] * n[1]};
+  int pa, a0, a1;  // plane-normal axis and the two in-plane axes
+  if (isym == 1) { pa = 0; a0 = 1; a1 = 2; }
+  else if (isym == 2) { pa = 1; a0 = 0; a1 = 2; }
+  else { pa = 2; a0 = 0; a1 = 1; }
+  const int n0 = n[a0], n1 = n[a1];
+  if (n0 > kHL || n1 > kHL) {
+    if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int plane = blockIdx.x; plane < n[pa]; plane += gridDim.x) {
+    const bool face_plane = (plane == 0 || plane == n[pa] - 1);
+    const long long base = plane * st[pa];
+    // rows (lines along a0): every cell passable, the box faces seeded
+    for (int r = threadIdx.x; r < n1; r += blockDim.x)
+      for (int w = 0; w < kHW; w++) {
+        const int lo = 32 * w, hi = min(32 * w + 32, n0);  // cells [lo, hi) of this word
+        const unsigned all = (hi <= lo) ? 0u : (hi - lo == 32 ? 0xffffffffu : ((1u << (hi - lo)) - 1u));
+        unsigned seed = 0u;
+        if (face_plane || r == 0 || r == n1 - 1) seed = all;
+        else {
+          if (lo == 0 && hi > 0) seed |= 1u;                                 // i0 = 0
+          if (n0 - 1 >= lo && n0 - 1 < hi) seed |= 1u << (n0 - 1 - lo);     // i0 = n0 - 1
+        }
+        pr[r][w] = all;
+        fr[r][w] = seed;
+      }
+    __syncthreads();
+    // wall-marked cells of this plane: the boxes that reach it, cleared
+    // from the passable masks (utils.c:192-205 marks them 2)
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+      const unsigned long long v = box[i];
+      int lo3[3], hi3[3];
+      for (int j = 0; j < 3; j++) {
+        lo3[j] = (int)((v >> (8 * j)) & 255u);
+        hi3[j] = (int)((v >> (24 + 8 * j)) & 255u);
+      }
+      if (plane < lo3[pa] || plane > hi3[pa]) continue;
+      const int c0 = lo3[a0], c1 = hi3[a0];
+      for (int r = lo3[a1]; r <= hi3[a1]; r++)
+        for (int w = c0 >> 5; w <= (c1 >> 5); w++) {
+          const int lo = max(c0, 32 * w) - 32 * w, hi = min(c1, 32 * w + 31) - 32 * w;  // bits [lo, hi]
+          const unsigned m = (hi - lo == 31) ? 0xffffffffu : (((1u << (hi - lo + 1)) - 1u) << lo);
+          atomicAnd(&pr[r][w], ~m);
+        }
+    }
+    __syncthreads();
+    // seeds overwrite wall marks on the box faces (utils.c:206-226)
+    for (int r = threadIdx.x; r < n1; r += blockDim.x)
+      for (int w = 0; w < kHW; w++) pr[r][w] |= fr[r][w];
+    __syncthreads();
+    bit_transpose(pr, n1, pc, n0);
+    __syncthreads();
+    int rounds = 0;
+    const int max_rounds = n0 * n1 + 2;
+    for (;;) {
+      bool ch = false;
+      // rows, then columns: every run of passable cells that holds a filled
+      // cell fills
+      for (int r = threadIdx.x; r < n1; r += blockDim.x) ch = line_fill(fr[r], pr[r]) || ch;
+      __syncthreads();
+      bit_transpose(fr, n1, fc, n0);
+      __syncthreads();
+      for (int c = threadIdx.x; c < n0; c += blockDim.x) ch = line_fill(fc[c], pc[c]) || ch;
+      __syncthreads();
+      bit_transpose(fc, n0, fr, n1);
+      const int any = __syncthreads_or(ch);
+      if (!any) break;
+      if (++rounds > max_rounds) {
+        if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
+        break;
+      }
+    }
+    // final map: hole = wall-marked or unreached (utils.c:291-294)
+    for (int r = warp; r < n1; r += nwarps) {
+      if (pa == 2) {  // rows are contiguous
+        unsigned char* __restrict__ row = sam + base + (size_t)r * n0;
+        for (int w = 0; w < kHW && 32 * w < n0; w++)
+          if (32 * w + lane < n0) row[32 * w + lane] = ((fr[r][w] >> lane) & 1u) ? 0 : 1;
+      } else {
+        for (int w = 0; w < kHW; w++) {
+          const int i0 = 32 * w + lane;
+          if (i0 < n0) sam[base + i0 * st[a0] + r * st[a1]] = ((fr[r][w] >> lane) & 1u) ? 0 : 1;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
