@@ -145,6 +145,47 @@ void tioga_b200_select_system_(int *sys);
 /* Systems registered in the instance. */
 int tioga_b200_nsystems_(void);
 
+/* Serving form: a request loop over many resident systems, each request
+ * one time step of one system (the per-step sequence preprocess ->
+ * performconnectivity -> dataupdate of src/tiogaInterface.C:150-216 for that
+ * system alone).  Independent of the global instance above; thread-safe.
+ * `nslots` requests run at once (each on its own CUDA stream), taken in
+ * arrival order as slots free up; a system is made resident (its topology,
+ * cell trees, hole maps and coordinates kept on the device between its
+ * requests) when it fits `hbm_budget_bytes` and at most `max_resident`
+ * systems are resident; idle systems are evicted least recently used first
+ * (their device coordinates written back to the caller's xyz arrays).
+ * Requests of one system run in submission order, one at a time.  Returns
+ * NULL without a CUDA device. */
+void *tioga_b200_server_create(long long hbm_budget_bytes, int nslots, int max_resident);
+void tioga_b200_server_destroy(void *srv);
+/* A block of system `sys`, with tioga_registergrid_data_'s arguments by
+ * value (vconn[t]: the t-th cell type's 1-based connectivity).  The arrays
+ * stay the caller's and must outlive the server; blocks are added before
+ * the system's first request. */
+int tioga_b200_server_add_block(void *srv, int sys, int btag, int nnodes, double *xyz, int *ibl, int nwbc, int nobc,
+                                int *wbcnode, int *obcnode, int ntypes, const int *nv, const int *nc,
+                                int *const *vconn);
+/* One time step of system `sys`: the rigid motions x <- A x + b of the
+ * blocks move_tags[0..nmoves) (moves[12 m ..]: A row-major, then b; applied
+ * on the device to the resident coordinates, each component evaluated as
+ * ((A[k][0] x + A[k][1] y) + A[k][2] z) + b[k]), then preprocess,
+ * connectivity, and, when q is given, the data update of nvar fields in
+ * the ROW layout into q[block] (blocks in the order they were added).
+ * iblank goes to ibl_out[block] when given, else to the arrays given at
+ * add_block.  The arrays must stay untouched until the request is waited
+ * for.  Returns a ticket (> 0) or -1. */
+long long tioga_b200_server_submit(void *srv, int sys, int nmoves, const int *move_tags, const double *moves,
+                                   int nvar, double *const *q, int *const *ibl_out);
+/* Blocks until the request is done: times_ms = (submit -> done, submit ->
+ * start, start -> done), counts = (query points, receptors, holes, status).
+ * Returns the request's status (0 = success). */
+int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[3], long long counts[4]);
+/* [0] resident systems, [1] device bytes they hold, [2] admissions,
+ * [3] evictions, [4] completed requests, [5] queued requests, [6] budget,
+ * [7] peak device bytes held. */
+void tioga_b200_server_stats(void *srv, long long out[16]);
+
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);
 /* 1 when a CUDA device is present and the library initialised it. */

@@ -8,6 +8,7 @@
 namespace tb {
 
 static int g_last_cuda_error = 0;
+thread_local long long* g_dbuf_account = nullptr;
 int fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
   return -(int)e - 1000;
@@ -52,7 +53,9 @@ Engine::~Engine() {
   qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
   d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
-  d_wall_.release();
+  d_wall_.release(); wall_cells_.release(); wall_box_.release(); wall_box_first_.release();
+  cg_cnt_.release(); cg_off_.release(); cg_v0_.release(); cg_v1_.release(); cg_k0_.release(); cg_k1_.release();
+  cg_flag_.release();
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -146,6 +149,7 @@ int Engine::register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl
     b.ncells += b.nc[t];
   }
   topo_dirty_ = true;
+  coords_on_device_ = false;
   preprocessed_ = false;
   connected_ = false;
   return 0;
@@ -374,6 +378,33 @@ int Engine::upload_coords() {
   for (size_t b = 0; b < hb_.size(); b++)
     TB_CUDA(cudaMemcpyAsync(x_.p + 3 * (long long)bi_[b].node_off, hb_[b].hx,
                             3 * (size_t)hb_[b].nnodes * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  coords_on_device_ = true;
+  return 0;
+}
+
+// device coordinates -> the caller's arrays (after rigid motions on the device)
+int Engine::download_coords() {
+  if (!coords_on_device_) return 0;
+  for (size_t b = 0; b < hb_.size(); b++)
+    TB_CUDA(cudaMemcpyAsync(hb_[b].hx, x_.p + 3 * (long long)bi_[b].node_off,
+                            3 * (size_t)hb_[b].nnodes * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  return 0;
+}
+
+int Engine::apply_rigid(int block, const double* A, const double* b) {
+  if (block < 0 || block >= (int)hb_.size() || topo_dirty_ || !coords_on_device_) {
+    fprintf(stderr, "#tioga_b200: rigid motion needs a preprocessed block with device coordinates\n");
+    return -1;
+  }
+  Rigid m;
+  for (int k = 0; k < 9; k++) m.a[k] = A[k];
+  for (int k = 0; k < 3; k++) m.b[k] = b[k];
+  const int n = hb_[block].nnodes;
+  if (n > 0) {
+    k_rigid<<<grid_for(n, kT), kT, 0, stream_>>>(x_.p + 3 * (long long)bi_[block].node_off, n, m);
+    TB_LAUNCHED("k_rigid");
+  }
   return 0;
 }
 
@@ -657,7 +688,7 @@ int Engine::preprocess() {
   for (size_t b = 0; b < hb_.size(); b++) bi_[b].has_user_res = (hb_[b].user_nres || hb_[b].user_cres);
   TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
                           stream_));
-  TB_TRY(upload_coords());
+  if (!coords_resident_ || !coords_on_device_ || fresh) TB_TRY(upload_coords());
   TB_TRY(compute_obbs());
   // keep the OBBs and block boxes on the host too
   TB_CUDA(cudaMemcpyAsync(bi_.data(), d_bi_.p, bi_.size() * sizeof(BlockInfo), cudaMemcpyDeviceToHost,
@@ -708,7 +739,7 @@ int Engine::preprocess() {
     if (H.dibl)
       TB_CUDA(cudaMemcpyAsync(H.dibl, iblank_.p + bi_[b].node_off, H.nnodes * sizeof(int),
                               cudaMemcpyDeviceToDevice, stream_));
-    else
+    else if (!serving_)
       for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;
   }
   TB_CUDA(cudaStreamSynchronize(stream_));
@@ -1060,9 +1091,13 @@ int Engine::dedup_gate() {
   TB_CUDA(node_bin_.ensure(ntot_));
   k_node_bins<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, node_bin_.p);
   TB_LAUNCHED("k_node_bins");
-  DBuf<int> cnt, off, v0, v1;
-  DBuf<unsigned long long> k0, k1;
-  DBuf<unsigned> flag;
+  DBuf<int>& cnt = cg_cnt_;
+  DBuf<int>& off = cg_off_;
+  DBuf<int>& v0 = cg_v0_;
+  DBuf<int>& v1 = cg_v1_;
+  DBuf<unsigned long long>& k0 = cg_k0_;
+  DBuf<unsigned long long>& k1 = cg_k1_;
+  DBuf<unsigned>& flag = cg_flag_;
   TB_CUDA(cnt.ensure(ntot_ + 1));
   TB_CUDA(off.ensure(ntot_ + 1));
   k_coin_count<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, ntot_, cnt.p);
@@ -1473,7 +1508,7 @@ int Engine::connectivity() {
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
-  if (!coords_resident_) TB_TRY(upload_coords());
+  if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
   int rc = run_holemaps();
   if (rc) return rc;

@@ -35,24 +35,40 @@ constexpr int kMaxSysBlocks = 16;      // blocks of one overset system (donor li
 constexpr int kMaxEngineBlocks = 8192;
 constexpr size_t kHoleMapCap = 197ull * 197ull * 197ull;  // bytes of one hole map at most // blocks of all systems of one engine (16-bit block ids)
 
+// Device bytes of the engine whose calls this thread is running (the
+// serving form's admission accounting); null: not counted.
+extern thread_local long long* g_dbuf_account;
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  long long* acct = nullptr;  // where this allocation is counted
   cudaError_t ensure(size_t count) {
     if (count <= n && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    size_t c = count ? count : 1;
+    // a buffer that has to grow again gets a quarter more, so slowly growing
+    // sizes (moving meshes) do not reallocate every call
+    const size_t grow = (p && count) ? count / 4 : 0;
+    release();
+    size_t c = count ? count + grow : 1;
     cudaError_t e = cudaMalloc(&p, c * sizeof(T));
-    if (e == cudaSuccess) n = c;
+    if (e == cudaSuccess) {
+      n = c;
+      acct = g_dbuf_account;
+      if (acct) *acct += (long long)(c * sizeof(T));
+    } else {
+      p = nullptr;
+    }
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      if (acct) *acct -= (long long)(n * sizeof(T));
+    }
     p = nullptr;
     n = 0;
+    acct = nullptr;
   }
 };
 
@@ -99,6 +115,11 @@ struct PairCull {
   int pair;       // index in the pair list
 };
 
+
+// rigid motion x <- a x + b (a row-major)
+struct Rigid {
+  double a[9], b[3];
+};
 
 // one wall-bearing block: its wall nodes in the global wall list, its cells,
 // its hole map
@@ -214,6 +235,17 @@ class Engine {
   int register_iblank_device(int tag, int* d_ibl);
   void set_precision(int p) { precision_ = p; }
   void set_coords_resident(int r) { coords_resident_ = r; }
+  // serving form: rigid motion of a block's device coordinates (x <- A x + b,
+  // A row-major), the caller's iblank array of a block, the device
+  // coordinates written back to the caller's arrays, device bytes held
+  int apply_rigid(int block, const double* A, const double* b);
+  void set_host_iblank(int block, int* ibl) { hb_[block].hibl = ibl; }
+  int download_coords();
+  long long* byte_counter() { return &dev_bytes_; }
+  // serving: preprocess leaves the caller's iblank alone (connectivity
+  // rewrites all of it)
+  void set_serving(bool v) { serving_ = v; }
+  long long device_bytes() const { return dev_bytes_; }
   void set_stream(cudaStream_t s);
 
   // the path
@@ -259,6 +291,9 @@ class Engine {
   int isym_ = 3, nfringe_ = 1, mexclude_ = 3;
   int precision_ = 1;        // 0 = FP64 throughout, 1 = FP32 screen + FP64 refine
   int coords_resident_ = 0;  // 1: the caller promises x has not moved
+  bool coords_on_device_ = false;  // x_ holds the registered blocks' coordinates
+  long long dev_bytes_ = 0;        // device bytes of this engine's buffers (when counted)
+  bool serving_ = false;
   bool topo_dirty_ = true;
   bool preprocessed_ = false;
   bool connected_ = false;
@@ -312,6 +347,9 @@ class Engine {
   DBuf<double> dd_x_, dd_rtag_;
   DBuf<unsigned long long> dd_key_, dd_key2_, dd_box_;
   DBuf<unsigned char> dd_oct_;
+  DBuf<int> cg_cnt_, cg_off_, cg_v0_, cg_v1_;   // preprocess gate scratch
+  DBuf<unsigned long long> cg_k0_, cg_k1_;
+  DBuf<unsigned> cg_flag_;
   DBuf<int4> dd_chunks_, dd_leaves_;
   DBuf<int> dd_starts_, dd_pqoff_, dd_prank_;
   // high-order path

@@ -69,6 +69,7 @@ __global__ void k_mexclude(const int* conn8, const unsigned char* cell_nv, long 
                            const unsigned char* ex0, unsigned char* ex1, double* cell_res);
 __global__ void k_copy_u8(const unsigned char* a, unsigned char* b, long long n);
 __global__ void k_fill_int(int* a, int v, long long n);
+__global__ void k_rigid(double* x, int n, Rigid m);
 __global__ void k_obb_partial(const double* x, const BlockInfo* bi, int pass, double* part);
 __global__ void k_obb_finish(const double* part, int nparts, int pass, const double* x, BlockInfo* bi, int nb);
 __global__ void k_morton(const double* x, const int* conn8, const unsigned char* cell_nv,

@@ -469,4 +469,14 @@ __global__ void k_invert(const int* __restrict__ perm, long long n, int* __restr
     inv[perm[s]] = (int)s;
 }
 
+// x <- a x + b for n nodes, each product and sum in a fixed order (the same
+// bits as the same expression evaluated on the host without contraction)
+__global__ void k_rigid(double* __restrict__ x, int n, Rigid m) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double* p = x + 3 * (long long)i;
+    const double x0 = p[0], x1 = p[1], x2 = p[2];
+    for (int k = 0; k < 3; k++) p[k] = ((m.a[3 * k] * x0 + m.a[3 * k + 1] * x1) + m.a[3 * k + 2] * x2) + m.b[k];
+  }
+}
+
 }  // namespace tb

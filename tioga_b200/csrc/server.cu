@@ -1,0 +1,418 @@
+// Serving form: a request loop over many resident overset systems.
+//
+// Each request is one time step of one system: rigid motions of some of its
+// blocks, then preprocess, connectivity and (optionally) the data update, the
+// reference's per-step call sequence (src/tiogaInterface.C:150-216) for that
+// system alone.  Systems stay resident between their requests (their
+// engine: topology, cell trees, hole-map slabs, donor rest state and
+// coordinates on the device; a step refits the tree boxes to the moved
+// coordinates instead of rebuilding the trees).
+//
+// Scheduling is continuous: `nslots` workers take requests in arrival order
+// as soon as a slot is free, so requests that arrive while others run are
+// admitted at once and their kernels overlap on the GPU (every engine has its
+// own stream).  A system is made resident when it fits the HBM budget (its
+// bytes measured by the engine's own allocations, estimated before its first
+// step); otherwise idle resident systems without pending requests are
+// evicted, least recently used first (their device coordinates are written
+// back to the caller's arrays first), and a request that still does not fit
+// waits.  Requests of one system run one at a time and in order, so each
+// result is the one the system would get alone.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+
+namespace tb {
+
+namespace {
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+struct SrvBlock {
+  int tag, nnodes, ncells, nwbc, nobc, ntypes;
+  double* x;
+  int* ibl;
+  int* wbc;
+  int* obc;
+  int nv[4], nc[4];
+  int* conn[4];
+};
+
+struct SrvRequest {
+  long long ticket = 0;
+  int sys = 0;
+  std::vector<int> move_tag;
+  std::vector<double> moves;  // 12 per move: a (row-major 3x3), b
+  int nvar = 0;
+  std::vector<double*> q;     // per block, or empty (no data update)
+  std::vector<int*> ibl;      // per block iblank destination, or empty (the registered arrays)
+  double t_submit = 0, t_start = 0, t_done = 0;
+  long long nquery = 0, nreceptor = 0, nhole = 0;
+  int rc = 0;
+  bool done = false;
+};
+
+struct SrvSystem {
+  std::vector<SrvBlock> blocks;
+  Engine* eng = nullptr;
+  long long bytes = 0;       // device bytes held (resident) or reserved (being admitted)
+  long long last_bytes = 0;  // bytes when it was last resident
+  bool busy = false;         // a request (or its eviction) is running
+  double last_used = 0;
+  int pending = 0;           // queued requests
+};
+
+class Server {
+ public:
+  Server(long long budget, int nslots, int max_resident)
+      : budget_(budget), nslots_(std::max(1, nslots)), max_resident_(std::max(1, max_resident)) {
+    cudaGetDevice(&device_);
+    for (int i = 0; i < nslots_; i++) workers_.emplace_back([this] { work(); });
+  }
+  ~Server() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (auto& t : workers_) t.join();
+    for (auto& kv : sys_) {
+      if (kv.second.eng) {
+        g_dbuf_account = &kv.second.bytes;
+        delete kv.second.eng;
+        g_dbuf_account = nullptr;
+      }
+    }
+    for (auto& kv : req_) delete kv.second;
+  }
+
+  int add_block(int sys, const SrvBlock& b) {
+    std::lock_guard<std::mutex> g(mu_);
+    SrvSystem& S = sys_[sys];
+    if (S.eng || S.busy || S.pending) {
+      fprintf(stderr, "#tioga_b200: server: blocks are added before a system's first request\n");
+      return -1;
+    }
+    for (const SrvBlock& o : S.blocks)
+      if (o.tag == b.tag) {
+        fprintf(stderr, "#tioga_b200: server: system %d already has mesh tag %d\n", sys, b.tag);
+        return -1;
+      }
+    S.blocks.push_back(b);
+    return 0;
+  }
+
+  long long submit(SrvRequest* r) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = sys_.find(r->sys);
+    if (it == sys_.end() || it->second.blocks.empty()) {
+      fprintf(stderr, "#tioga_b200: server: unknown system %d\n", r->sys);
+      delete r;
+      return -1;
+    }
+    const size_t nb = it->second.blocks.size();
+    if ((!r->q.empty() && r->q.size() != nb) || (!r->ibl.empty() && r->ibl.size() != nb)) {
+      delete r;
+      return -1;
+    }
+    r->ticket = next_ticket_++;
+    r->t_submit = now_ms();
+    it->second.pending++;
+    queue_.push_back(r);
+    req_[r->ticket] = r;
+    cv_work_.notify_one();
+    return r->ticket;
+  }
+
+  int wait(long long ticket, double times[3], long long counts[4]) {
+    std::unique_lock<std::mutex> l(mu_);
+    auto it = req_.find(ticket);
+    if (it == req_.end()) return -1;
+    SrvRequest* r = it->second;
+    cv_done_.wait(l, [&] { return r->done; });
+    if (times) {
+      times[0] = r->t_done - r->t_submit;
+      times[1] = r->t_start - r->t_submit;
+      times[2] = r->t_done - r->t_start;
+    }
+    if (counts) {
+      counts[0] = r->nquery;
+      counts[1] = r->nreceptor;
+      counts[2] = r->nhole;
+      counts[3] = r->rc;
+    }
+    const int rc = r->rc;
+    req_.erase(it);
+    delete r;
+    return rc;
+  }
+
+  int nblocks(int sys) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = sys_.find(sys);
+    return it == sys_.end() ? -1 : (int)it->second.blocks.size();
+  }
+
+  void stats(long long out[16]) {
+    std::lock_guard<std::mutex> g(mu_);
+    for (int i = 0; i < 16; i++) out[i] = 0;
+    int res = 0;
+    for (auto& kv : sys_) res += kv.second.eng ? 1 : 0;
+    out[0] = res;
+    out[1] = used_;
+    out[2] = admissions_;
+    out[3] = evictions_;
+    out[4] = completed_;
+    out[5] = (long long)queue_.size();
+    out[6] = budget_;
+    out[7] = peak_used_;
+  }
+
+ private:
+  // bytes a system needs before it has been resident once: per node, per
+  // cell and per hole-map slab, with headroom
+  static long long estimate(const SrvSystem& S) {
+    long long n = 0, c = 0, w = 0;
+    for (const SrvBlock& b : S.blocks) {
+      n += b.nnodes;
+      c += b.ncells;
+      w += b.nwbc > 0;
+    }
+    return 320 * n + 320 * c + (long long)kHoleMapCap * w + (16ll << 20);
+  }
+
+  // under the lock: the first queued request that can run now, with the
+  // systems to evict for it (marked busy)
+  SrvRequest* pick(std::vector<int>& evict) {
+    std::map<int, bool> blocked;  // a system whose earlier request waits keeps its order
+    for (auto it = queue_.begin(); it != queue_.end(); ++it) {
+      SrvRequest* r = *it;
+      if (blocked.count(r->sys)) continue;
+      SrvSystem& S = sys_[r->sys];
+      if (S.busy) {
+        blocked[r->sys] = true;
+        continue;
+      }
+      if (!S.eng) {
+        // a system larger than the whole budget runs once every other one is evicted
+        const long long need = std::min(budget_, S.last_bytes > 0 ? S.last_bytes : estimate(S));
+        int res = 0;
+        for (auto& kv : sys_) res += (kv.second.eng != nullptr || kv.second.bytes > 0) ? 1 : 0;
+        long long freed = 0;
+        std::vector<std::pair<double, int>> idle;
+        for (auto& kv : sys_)
+          if (kv.second.eng && !kv.second.busy && kv.second.pending == 0)
+            idle.push_back({kv.second.last_used, kv.first});
+        std::sort(idle.begin(), idle.end());
+        std::vector<int> ev;
+        size_t k = 0;
+        while ((used_ - freed + need > budget_ || res - (int)ev.size() + 1 > max_resident_) && k < idle.size()) {
+          ev.push_back(idle[k].second);
+          freed += sys_[idle[k].second].bytes;
+          k++;
+        }
+        if (used_ - freed + need > budget_ || res - (int)ev.size() + 1 > max_resident_) {
+          blocked[r->sys] = true;  // waits for memory
+          continue;
+        }
+        for (int e : ev) sys_[e].busy = true;
+        evict = ev;
+        S.bytes = need;  // reserved until its engine reports its own bytes
+        used_ += need;
+        admissions_++;
+      }
+      S.busy = true;
+      S.pending--;
+      queue_.erase(it);
+      return r;
+    }
+    return nullptr;
+  }
+
+  void work() {
+    cudaSetDevice(device_);
+    std::unique_lock<std::mutex> l(mu_);
+    for (;;) {
+      std::vector<int> evict;
+      SrvRequest* r = nullptr;
+      while (!stop_ && !(r = pick(evict))) cv_work_.wait(l);
+      if (stop_ && !r) return;
+      l.unlock();
+      for (int e : evict) {  // write the coordinates back, free the device memory
+        SrvSystem& E = sys_.at(e);
+        g_dbuf_account = &E.bytes;
+        E.eng->download_coords();
+        delete E.eng;
+        g_dbuf_account = nullptr;
+        l.lock();
+        used_ -= E.last_bytes;  // what it held at its last step
+        E.bytes = 0;
+        E.eng = nullptr;
+        E.busy = false;
+        evictions_++;
+        l.unlock();
+      }
+      SrvSystem& S = sys_.at(r->sys);
+      r->t_start = now_ms();
+      run(S, r);
+      r->t_done = now_ms();
+      l.lock();
+      if (S.eng) {
+        used_ += S.eng->device_bytes() - S.bytes;
+        S.bytes = S.eng->device_bytes();
+        S.last_bytes = S.bytes;
+      } else {
+        used_ -= S.bytes;
+        S.bytes = 0;
+      }
+      peak_used_ = std::max(peak_used_, used_);
+      S.busy = false;
+      S.last_used = r->t_done;
+      r->done = true;
+      completed_++;
+      cv_done_.notify_all();
+      cv_work_.notify_all();
+    }
+  }
+
+  void run(SrvSystem& S, SrvRequest* r) {
+    int rc = 0;
+    bool fresh = false;
+    if (!S.eng) {  // admission: the system's engine, its topology and coordinates
+      S.eng = new Engine();
+      g_dbuf_account = S.eng->byte_counter();
+      for (const SrvBlock& b : S.blocks) {
+        rc = S.eng->register_block(b.tag, b.nnodes, b.x, b.ibl, b.nwbc, b.nobc, b.wbc, b.obc, b.ntypes, b.nv, b.nc,
+                                   const_cast<int**>(b.conn));
+        if (rc) break;
+      }
+      S.eng->set_coords_resident(1);
+      S.eng->set_serving(true);
+      fresh = true;
+    }
+    Engine& E = *S.eng;
+    g_dbuf_account = E.byte_counter();
+    if (!rc && fresh && !r->move_tag.empty()) rc = E.preprocess();  // coordinates on the device first
+    for (size_t m = 0; !rc && m < r->move_tag.size(); m++) {
+      const int b = E.find_block(0, r->move_tag[m]);
+      rc = (b < 0) ? -1 : E.apply_rigid(b, &r->moves[12 * m], &r->moves[12 * m + 9]);
+    }
+    for (size_t b = 0; b < S.blocks.size(); b++) E.set_host_iblank((int)b, r->ibl.empty() ? S.blocks[b].ibl : r->ibl[b]);
+    if (!rc) rc = E.preprocess();
+    if (!rc) rc = E.connectivity();
+    if (!rc && !r->q.empty()) {
+      for (size_t b = 0; b < S.blocks.size() && !rc; b++) rc = E.register_solution(S.blocks[b].tag, r->q[b], false);
+      if (!rc) rc = E.dataupdate(r->nvar, 0);
+    }
+    const Stats& st = E.stats();
+    r->nquery = st.nquery;
+    r->nreceptor = st.nreceptor;
+    r->nhole = st.nhole;
+    r->rc = rc ? rc : (st.error ? -(int)st.error : 0);
+    g_dbuf_account = nullptr;
+  }
+
+  long long budget_;
+  int nslots_, max_resident_;
+  int device_ = 0;
+  std::mutex mu_;
+  std::condition_variable cv_work_, cv_done_;
+  std::map<int, SrvSystem> sys_;
+  std::deque<SrvRequest*> queue_;
+  std::map<long long, SrvRequest*> req_;
+  long long next_ticket_ = 1, used_ = 0, peak_used_ = 0, admissions_ = 0, evictions_ = 0, completed_ = 0;
+  bool stop_ = false;
+  std::vector<std::thread> workers_;
+};
+
+}  // namespace tb
+
+#pragma GCC visibility push(default)
+#include "../../include/tioga_b200.h"
+
+extern "C" {
+
+void* tioga_b200_server_create(long long hbm_budget_bytes, int nslots, int max_resident) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+    fprintf(stderr, "#tioga_b200: no CUDA device; the serving form cannot run\n");
+    return nullptr;
+  }
+  return new tb::Server(hbm_budget_bytes, nslots, max_resident);
+}
+
+void tioga_b200_server_destroy(void* srv) { delete static_cast<tb::Server*>(srv); }
+
+int tioga_b200_server_add_block(void* srv, int sys, int btag, int nnodes, double* xyz, int* ibl, int nwbc, int nobc,
+                                int* wbcnode, int* obcnode, int ntypes, const int* nv, const int* nc,
+                                int* const* vconn) {
+  if (!srv || ntypes < 1 || ntypes > 4) return -1;
+  tb::SrvBlock b{};
+  b.tag = btag;
+  b.nnodes = nnodes;
+  b.x = xyz;
+  b.ibl = ibl;
+  b.nwbc = nwbc;
+  b.nobc = nobc;
+  b.wbc = wbcnode;
+  b.obc = obcnode;
+  b.ntypes = ntypes;
+  b.ncells = 0;
+  for (int t = 0; t < 4; t++) {
+    b.nv[t] = t < ntypes ? nv[t] : 0;
+    b.nc[t] = t < ntypes ? nc[t] : 0;
+    b.conn[t] = t < ntypes ? vconn[t] : nullptr;
+    b.ncells += b.nc[t];
+  }
+  return static_cast<tb::Server*>(srv)->add_block(sys, b);
+}
+
+long long tioga_b200_server_submit(void* srv, int sys, int nmoves, const int* move_tags, const double* moves,
+                                   int nvar, double* const* q, int* const* ibl_out) {
+  if (!srv || nmoves < 0 || (nmoves > 0 && (!move_tags || !moves))) return -1;
+  auto* r = new tb::SrvRequest();
+  r->sys = sys;
+  r->move_tag.assign(move_tags, move_tags + nmoves);
+  r->moves.assign(moves, moves + 12 * (size_t)nmoves);
+  r->nvar = nvar;
+  auto* s = static_cast<tb::Server*>(srv);
+  // per-block pointer lists: their length is the system's block count,
+  // which the server checks
+  if (q || ibl_out) {
+    const int nb = s->nblocks(sys);
+    if (nb <= 0) {
+      delete r;
+      return -1;
+    }
+    if (q) r->q.assign(q, q + nb);
+    if (ibl_out) r->ibl.assign(ibl_out, ibl_out + nb);
+  }
+  return s->submit(r);
+}
+
+int tioga_b200_server_wait(void* srv, long long ticket, double times_ms[3], long long counts[4]) {
+  if (!srv) return -1;
+  return static_cast<tb::Server*>(srv)->wait(ticket, times_ms, counts);
+}
+
+void tioga_b200_server_stats(void* srv, long long out[16]) {
+  if (!srv) {
+    for (int i = 0; i < 16; i++) out[i] = 0;
+    return;
+  }
+  static_cast<tb::Server*>(srv)->stats(out);
+}
+
+}  // extern "C"
+
+#pragma GCC visibility pop
