@@ -69,8 +69,17 @@ def parse():
     p.add_argument("--cpu-reps", type=int, default=3)
     p.add_argument("--size", default="full", choices=["full", "medium", "small"],
                    help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
-    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2"],
-                   help="cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems")
+    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg3"],
+                   help="cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems; "
+                        "cfg3: the serving form, Poisson requests over resident moving systems")
+    p.add_argument("--rates", default="",
+                   help="cfg3: comma-separated arrival rates (requests/s); default: a sweep around capacity")
+    p.add_argument("--seconds", type=float, default=6.0, help="cfg3: arrival window per rate")
+    p.add_argument("--slots", type=int, default=8, help="cfg3: concurrent requests")
+    p.add_argument("--nsys", type=int, default=200, help="cfg3: systems")
+    p.add_argument("--budget-gb", type=float, default=120.0, help="cfg3: HBM admission budget")
+    p.add_argument("--no-forms", action="store_true",
+                   help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
     p.add_argument("--forms", default="split,plain,e2e",
                    help="comma list of measured forms (the first one gives `value`)")
     return p.parse_args()
@@ -472,6 +481,148 @@ def run_gpu_batch(args, ws, rank, local, dist):
 
 
 # ---------------------------------------------------------------------------
+# serving form: Poisson requests over resident moving systems
+# ---------------------------------------------------------------------------
+WORKLOAD3 = ("cfg3: Poisson request stream over {n} resident systems from the cfg2 distribution (seed 3); each "
+             "request one time step of one system: every shell rotated U(0,2) degrees about a random axis and "
+             "moved by <= 0.5 wall-layer cell widths, then preprocess, connectivity and a 5-field data update")
+
+
+def serving_systems(args):
+    n = args.nsys
+    if args.size == "small":
+        return cases.config2(3, nsys=min(n, 16), nmin=5e3, nmax=5e4)
+    if args.size == "medium":
+        return cases.config2(3, nsys=min(n, 48), nmin=2e4, nmax=5e5)
+    return cases.config2(3, nsys=n)
+
+
+def wall_cell_width(block) -> float:
+    """The smallest edge of the cells that touch the block's wall."""
+    wall = np.zeros(block.nnodes, dtype=bool)
+    wall[block.wbc] = True
+    best = np.inf
+    for nv, conn in block.cells:
+        c = conn[wall[conn].any(axis=1)]
+        if len(c) == 0:
+            continue
+        p = block.x[c]
+        e = np.linalg.norm(p[:, 1:, :] - p[:, :1, :], axis=2)
+        e = e[e > 0]
+        if e.size:
+            best = min(best, float(e.min()))
+    return best if np.isfinite(best) else 0.0
+
+
+def run_gpu_serving(args, ws, rank, local, dist):
+    import torch
+
+    from tioga_b200.serving import Server, rigid
+    torch.cuda.set_device(local)
+    systems = serving_systems(args)
+    nvar = 5
+    rng = np.random.default_rng(33)
+    pinned, keep = [], []
+    for s in systems:  # the solver's arrays in pinned host memory
+        xs, ibs, qs = [], [], []
+        for b in s.blocks:
+            xt = torch.empty((b.nnodes, 3), dtype=torch.float64, pin_memory=True)
+            xt.numpy()[:] = b.x
+            it = torch.ones(b.nnodes, dtype=torch.int32, pin_memory=True)
+            qt = torch.empty(b.nnodes * nvar, dtype=torch.float64, pin_memory=True)
+            qt.numpy()[:] = rng.uniform(-1.0, 1.0, b.nnodes * nvar)
+            keep += [xt, it, qt]
+            xs.append(xt.numpy())
+            ibs.append(it.numpy())
+            qs.append(qt.numpy())
+        pinned.append((xs, ibs, qs))
+    shift = [[0.5 * wall_cell_width(b) for b in s.blocks] for s in systems]
+    srv = Server(budget_bytes=int(args.budget_gb * (1 << 30)), nslots=args.slots, max_resident=200)
+    for k, s in enumerate(systems):
+        srv.add_system(k, s, x_arrays=pinned[k][0], ibl_arrays=pinned[k][1])
+
+    def moves_for(k):
+        s = systems[k]
+        xs = pinned[k][0]
+        return [(b.tag, *rigid(rng, xs[i][:: max(1, b.nnodes // 64)].mean(axis=0), 2.0, shift[k][i]))
+                for i, b in enumerate(s.blocks) if i > 0]
+
+    # admission: one step of every system (topology upload, trees, hole maps)
+    t0 = time.perf_counter()
+    ts = [srv.submit(k, moves_for(k), q=pinned[k][2], nvar=nvar) for k in range(len(systems))]
+    first = [srv.wait(t) for t in ts]
+    admit_s = time.perf_counter() - t0
+    assert all(f["rc"] == 0 for f in first), [f for f in first if f["rc"]][:3]
+    # a closed loop with all slots busy measures the capacity
+    t0 = time.perf_counter()
+    ts = [srv.submit(k % len(systems), moves_for(k % len(systems)), q=pinned[k % len(systems)][2], nvar=nvar)
+          for k in range(2 * len(systems))]
+    sat = [srv.wait(t) for t in ts]
+    sat_s = time.perf_counter() - t0
+    cap = len(ts) / sat_s
+    rates = [float(r) for r in args.rates.split(",")] if args.rates else [0.25 * cap, 0.5 * cap, 0.75 * cap,
+                                                                          0.9 * cap]
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = Clocks(vis.split(",")[local] if vis else str(local))
+    sweep = []
+    for ri, rate in enumerate(rates):
+        n = max(8, int(rate * args.seconds))
+        arr = np.cumsum(rng.exponential(1.0 / rate, n))
+        who = rng.integers(0, len(systems), n)
+        mv = [moves_for(int(k)) for k in who]
+        if ri == len(rates) - 1:
+            clocks.start()
+        tickets = []
+        t0 = time.perf_counter()
+        for i in range(n):  # submit at the arrival times
+            d = t0 + arr[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(int(who[i]), mv[i], q=pinned[int(who[i])][2], nvar=nvar))
+        res = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        clk = clocks.stop() if ri == len(rates) - 1 else None
+        assert all(r["rc"] == 0 for r in res)
+        lat = np.array([r["latency_ms"] for r in res])
+        Q = sum(r["nquery"] for r in res)
+        sweep.append({"rate_rps": rate, "requests": n, "seconds": wall, "receptors_per_s": Q / wall,
+                      "requests_per_s": n / wall, "query_points": Q,
+                      "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                     "p99.9": float(np.percentile(lat, 99.9)), "max": float(lat.max())},
+                      "queue_ms_p50": float(np.median([r["queue_ms"] for r in res])),
+                      "service_ms_p50": float(np.median([r["service_ms"] for r in res])),
+                      "calls_ms_p50": {k: float(np.median([r[k + "_ms"] for r in res]))
+                                       for k in ("preprocess", "connectivity", "dataupdate")}})
+    st = srv.stats()
+    srv.close()
+    top = sweep[-1]
+    nodes = sum(s.nnodes for s in systems)
+    out = {
+        "metric": METRIC, "value": top["receptors_per_s"], "unit": UNIT, "n_gpus": ws, "steps": top["requests"],
+        "warmup": len(systems), "ms_per_step": 1e3 * top["seconds"] / top["requests"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator tioga_b200.cases.config2, seeded rigid motions)",
+        "config": {"workload": WORKLOAD3.format(n=len(systems)) if args.size == "full" else
+                   f"cfg3 stream, {args.size} systems", "systems": len(systems), "nodes": nodes,
+                   "slots": args.slots, "budget_gb": args.budget_gb, "arrivals": "Poisson",
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (all systems' coordinates %.0f MB)" % (24 * nodes / 1e6)},
+        "latency_ms": top["latency_ms"],
+        "serving": {"capacity_rps": cap, "capacity_receptors_per_s": sum(r["nquery"] for r in sat) / sat_s,
+                    "admission_s": admit_s, "sweep": sweep, "server": st},
+        "e2e": {"value": top["receptors_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": int(np.mean([8 * nvar * s.nnodes for s in systems])),
+                "d2h_bytes_per_step": int(np.mean([(4 + 8 * nvar) * s.nnodes for s in systems])),
+                "note": "requests through the serving C ABI with host arrays; every request uploads its "
+                        "system's fields and downloads its iblanks"},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    del keep
+    return out
+
+
+# ---------------------------------------------------------------------------
 # CPU: the compiled reference (or the C restatement) on a bounded sample
 # ---------------------------------------------------------------------------
 def sample_query_count(sample):
@@ -540,9 +691,25 @@ def main():
         if ws > 1:
             import torch
             torch.cuda.set_device(local)
-        out = (run_gpu_batch if args.workload == "cfg2" else run_gpu)(args, ws, rank, local, dist)
+        out = {"cfg2": run_gpu_batch, "cfg3": run_gpu_serving}.get(args.workload, run_gpu)(args, ws, rank, local,
+                                                                                           dist)
     finally:
         dist.close()
+    if rank == 0 and ws == 1 and args.workload == "cfg1" and not args.no_forms:
+        # the other two forms on their own workloads, summarised in the same line
+        import copy
+        a2 = copy.copy(args)
+        a2.steps, a2.warmup = max(3, min(args.steps, 6)), max(3, min(args.warmup, 3))
+        b = run_gpu_batch(a2, ws, rank, local, Dist(1, None))
+        out["batched"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain", "latency_ms",
+                                            "plain", "plain_split", "batched_fp64", "e2e", "phases_ms", "roofline",
+                                            "gpu_launches", "clocks")}
+        out["batched"]["config"] = b["config"]
+        a3 = copy.copy(args)
+        a3.size, a3.seconds, a3.slots, a3.rates = "medium", 3.0, 16, ""
+        sv = run_gpu_serving(a3, ws, rank, local, Dist(1, None))
+        out["served"] = {k: sv[k] for k in ("value", "unit", "latency_ms", "serving", "e2e", "clocks")}
+        out["served"]["config"] = sv["config"]
     if rank == 0:
         if ws == 1 and not args.no_cpu_baseline:
             res, why = cpu_reference(args.cpu_reps)

@@ -178,9 +178,10 @@ int tioga_b200_server_add_block(void *srv, int sys, int btag, int nnodes, double
 long long tioga_b200_server_submit(void *srv, int sys, int nmoves, const int *move_tags, const double *moves,
                                    int nvar, double *const *q, int *const *ibl_out);
 /* Blocks until the request is done: times_ms = (submit -> done, submit ->
- * start, start -> done), counts = (query points, receptors, holes, status).
+ * start, start -> done, then the host time of its preprocess, connectivity
+ * and data update), counts = (query points, receptors, holes, status).
  * Returns the request's status (0 = success). */
-int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[3], long long counts[4]);
+int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[6], long long counts[4]);
 /* [0] resident systems, [1] device bytes they hold, [2] admissions,
  * [3] evictions, [4] completed requests, [5] queued requests, [6] budget,
  * [7] peak device bytes held. */

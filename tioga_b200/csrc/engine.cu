@@ -9,6 +9,7 @@ namespace tb {
 
 static int g_last_cuda_error = 0;
 thread_local long long* g_dbuf_account = nullptr;
+thread_local cudaStream_t g_dbuf_stream = nullptr;
 int fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
   return -(int)e - 1000;
@@ -150,6 +151,7 @@ int Engine::register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl
   }
   topo_dirty_ = true;
   coords_on_device_ = false;
+  gate_valid_ = false;
   preprocessed_ = false;
   connected_ = false;
   return 0;
@@ -379,6 +381,7 @@ int Engine::upload_coords() {
     TB_CUDA(cudaMemcpyAsync(x_.p + 3 * (long long)bi_[b].node_off, hb_[b].hx,
                             3 * (size_t)hb_[b].nnodes * sizeof(double), cudaMemcpyHostToDevice, stream_));
   coords_on_device_ = true;
+  gate_valid_ = false;  // the caller may have moved the nodes any way
   return 0;
 }
 
@@ -699,7 +702,10 @@ int Engine::preprocess() {
     TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice,
                             stream_));
   }
-  TB_TRY(dedup_gate());
+  // rigid motions keep every distance (to rounding far below the gate's
+  // distance), so the gate of the last preprocess still holds after them
+  if (!gate_valid_) TB_TRY(dedup_gate());
+  gate_valid_ = true;
   for (size_t b = 0; b < hb_.size(); b++) {
     const HostBlock& H = hb_[b];
     if (!bi_[b].has_user_res) continue;

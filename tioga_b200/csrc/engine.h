@@ -38,12 +38,18 @@ constexpr size_t kHoleMapCap = 197ull * 197ull * 197ull;  // bytes of one hole m
 // Device bytes of the engine whose calls this thread is running (the
 // serving form's admission accounting); null: not counted.
 extern thread_local long long* g_dbuf_account;
+// When set, buffers are allocated and freed stream-ordered on this stream
+// (cudaMallocAsync / cudaFreeAsync), so engines that run side by side on their
+// own streams never wait for each other's frees; null: cudaMalloc / cudaFree.
+extern thread_local cudaStream_t g_dbuf_stream;
 
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
   long long* acct = nullptr;  // where this allocation is counted
+  cudaStream_t st = nullptr;  // stream-ordered allocation: its stream
+  bool async = false;
   cudaError_t ensure(size_t count) {
     if (count <= n && p) return cudaSuccess;
     // a buffer that has to grow again gets a quarter more, so slowly growing
@@ -51,7 +57,9 @@ struct DBuf {
     const size_t grow = (p && count) ? count / 4 : 0;
     release();
     size_t c = count ? count + grow : 1;
-    cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+    async = g_dbuf_stream != nullptr;
+    st = g_dbuf_stream;
+    cudaError_t e = async ? cudaMallocAsync((void**)&p, c * sizeof(T), st) : cudaMalloc(&p, c * sizeof(T));
     if (e == cudaSuccess) {
       n = c;
       acct = g_dbuf_account;
@@ -63,12 +71,15 @@ struct DBuf {
   }
   void release() {
     if (p) {
-      cudaFree(p);
+      if (async) cudaFreeAsync(p, st);
+      else cudaFree(p);
       if (acct) *acct -= (long long)(n * sizeof(T));
     }
     p = nullptr;
     n = 0;
     acct = nullptr;
+    async = false;
+    st = nullptr;
   }
 };
 
@@ -342,6 +353,7 @@ class Engine {
   // coincident query points (uniqNodesTree)
   DBuf<short> node_bin_;            // 10x10x10 OBB bin of every node (donor-list order)
   bool dedup_active_ = false;       // some block has nodes within the gate's distance
+  bool gate_valid_ = false;         // the gate holds for the device coordinates (moved rigidly since)
   bool dedup_ran_ = false;          // this call merged coincident query points
   DBuf<int> q_xt_, q_rep_, q_gpos_, dd_refq_, dd_perm_, dd_perm2_, dd_mtag_, dd_itag_, dd_seg_, dd_cnt_, dd_ireset_;
   DBuf<double> dd_x_, dd_rtag_;

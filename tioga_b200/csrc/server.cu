@@ -57,6 +57,7 @@ struct SrvRequest {
   std::vector<double*> q;     // per block, or empty (no data update)
   std::vector<int*> ibl;      // per block iblank destination, or empty (the registered arrays)
   double t_submit = 0, t_start = 0, t_done = 0;
+  double t_pre = 0, t_conn = 0, t_upd = 0;  // host time of the three calls
   long long nquery = 0, nreceptor = 0, nhole = 0;
   int rc = 0;
   bool done = false;
@@ -88,9 +89,9 @@ class Server {
     for (auto& t : workers_) t.join();
     for (auto& kv : sys_) {
       if (kv.second.eng) {
-        g_dbuf_account = &kv.second.bytes;
+        g_dbuf_stream = kv.second.eng->stream();
         delete kv.second.eng;
-        g_dbuf_account = nullptr;
+        g_dbuf_stream = nullptr;
       }
     }
     for (auto& kv : req_) delete kv.second;
@@ -134,7 +135,7 @@ class Server {
     return r->ticket;
   }
 
-  int wait(long long ticket, double times[3], long long counts[4]) {
+  int wait(long long ticket, double times[6], long long counts[4]) {
     std::unique_lock<std::mutex> l(mu_);
     auto it = req_.find(ticket);
     if (it == req_.end()) return -1;
@@ -144,6 +145,9 @@ class Server {
       times[0] = r->t_done - r->t_submit;
       times[1] = r->t_start - r->t_submit;
       times[2] = r->t_done - r->t_start;
+      times[3] = r->t_pre;
+      times[4] = r->t_conn;
+      times[5] = r->t_upd;
     }
     if (counts) {
       counts[0] = r->nquery;
@@ -241,6 +245,13 @@ class Server {
 
   void work() {
     cudaSetDevice(device_);
+    {  // freed buffers stay in the device's pool for the next allocation
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+    }
     std::unique_lock<std::mutex> l(mu_);
     for (;;) {
       std::vector<int> evict;
@@ -251,9 +262,11 @@ class Server {
       for (int e : evict) {  // write the coordinates back, free the device memory
         SrvSystem& E = sys_.at(e);
         g_dbuf_account = &E.bytes;
+        g_dbuf_stream = E.eng->stream();
         E.eng->download_coords();
         delete E.eng;
         g_dbuf_account = nullptr;
+        g_dbuf_stream = nullptr;
         l.lock();
         used_ -= E.last_bytes;  // what it held at its last step
         E.bytes = 0;
@@ -291,6 +304,7 @@ class Server {
     if (!S.eng) {  // admission: the system's engine, its topology and coordinates
       S.eng = new Engine();
       g_dbuf_account = S.eng->byte_counter();
+      g_dbuf_stream = S.eng->stream();
       for (const SrvBlock& b : S.blocks) {
         rc = S.eng->register_block(b.tag, b.nnodes, b.x, b.ibl, b.nwbc, b.nobc, b.wbc, b.obc, b.ntypes, b.nv, b.nc,
                                    const_cast<int**>(b.conn));
@@ -302,24 +316,32 @@ class Server {
     }
     Engine& E = *S.eng;
     g_dbuf_account = E.byte_counter();
+    g_dbuf_stream = E.stream();
     if (!rc && fresh && !r->move_tag.empty()) rc = E.preprocess();  // coordinates on the device first
     for (size_t m = 0; !rc && m < r->move_tag.size(); m++) {
       const int b = E.find_block(0, r->move_tag[m]);
       rc = (b < 0) ? -1 : E.apply_rigid(b, &r->moves[12 * m], &r->moves[12 * m + 9]);
     }
     for (size_t b = 0; b < S.blocks.size(); b++) E.set_host_iblank((int)b, r->ibl.empty() ? S.blocks[b].ibl : r->ibl[b]);
+    double t = now_ms();
     if (!rc) rc = E.preprocess();
+    r->t_pre = now_ms() - t;
+    t = now_ms();
     if (!rc) rc = E.connectivity();
+    r->t_conn = now_ms() - t;
+    t = now_ms();
     if (!rc && !r->q.empty()) {
       for (size_t b = 0; b < S.blocks.size() && !rc; b++) rc = E.register_solution(S.blocks[b].tag, r->q[b], false);
       if (!rc) rc = E.dataupdate(r->nvar, 0);
     }
+    r->t_upd = now_ms() - t;
     const Stats& st = E.stats();
     r->nquery = st.nquery;
     r->nreceptor = st.nreceptor;
     r->nhole = st.nhole;
     r->rc = rc ? rc : (st.error ? -(int)st.error : 0);
     g_dbuf_account = nullptr;
+    g_dbuf_stream = nullptr;
   }
 
   long long budget_;
@@ -400,7 +422,7 @@ long long tioga_b200_server_submit(void* srv, int sys, int nmoves, const int* mo
   return s->submit(r);
 }
 
-int tioga_b200_server_wait(void* srv, long long ticket, double times_ms[3], long long counts[4]) {
+int tioga_b200_server_wait(void* srv, long long ticket, double times_ms[6], long long counts[4]) {
   if (!srv) return -1;
   return static_cast<tb::Server*>(srv)->wait(ticket, times_ms, counts);
 }

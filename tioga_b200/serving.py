@@ -122,11 +122,12 @@ class Server:
         return t
 
     def wait(self, ticket: int) -> dict:
-        times = (C.c_double * 3)()
+        times = (C.c_double * 6)()
         counts = (C.c_longlong * 4)()
         rc = self.lib.tioga_b200_server_wait(self.h, C.c_longlong(ticket), C.cast(times, _P), C.cast(counts, _P))
         self._keep.pop(ticket, None)
         return {"rc": rc, "latency_ms": times[0], "queue_ms": times[1], "service_ms": times[2],
+                "preprocess_ms": times[3], "connectivity_ms": times[4], "dataupdate_ms": times[5],
                 "nquery": counts[0], "nreceptor": counts[1], "nhole": counts[2]}
 
     def stats(self) -> dict:
