@@ -196,6 +196,19 @@ def pinned_copy(system):
     return cases.System(blocks, system.name, system.meta), ibls, keep
 
 
+def autotune(lib, tb, reps: int = 2) -> dict:
+    """The library's autotuner (tioga_b200_autotune_) on the loaded workload;
+    returns the launch shapes it chose."""
+    tb.set_int(lib.lib, "tioga_b200_autotune_", reps)
+    if lib.lib.tioga_b200_last_error() != 0:
+        raise RuntimeError("autotune failed")
+    out = (C.c_int * 8)()
+    lib.lib.tioga_b200_tuning_(out)
+    keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
+            "candidate_ctas_per_sm"]
+    return {k: int(out[i]) for i, k in enumerate(keys)}
+
+
 def run_gpu(args, ws, rank, local, dist):
     import torch
 
@@ -221,6 +234,7 @@ def run_gpu(args, ws, rank, local, dist):
     lib.performconnectivity()
     if lib.lib.tioga_b200_last_error() != 0:
         raise RuntimeError("connectivity failed")
+    tuning = autotune(lib, tb)
 
     # device-resident forms keep iblank in HBM too (a GPU solver's arrays)
     d_ibl = [torch.ones(b.nnodes, dtype=torch.int32, device="cuda") for b in system.blocks]
@@ -316,6 +330,7 @@ def run_gpu(args, ws, rank, local, dist):
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
                    "donors": st["ndonor"]},
+        "tuning": tuning,
         "gpu_launches": launches,
         "clocks": clk,
     }
@@ -414,6 +429,7 @@ def run_gpu_batch(args, ws, rank, local, dist):
             d_ibl.append(d)
             lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(d.data_ptr()))
     tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
+    tuning = autotune(lib, tb)
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = Clocks(vis.split(",")[local] if vis else str(local))
     ms_b, per_b, st, ph, launches, clk = events_time(args.steps, args.warmup, clocks)
@@ -472,6 +488,7 @@ def run_gpu_batch(args, ws, rank, local, dist):
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
                    "donors": st["ndonor"]},
+        "tuning": tuning,
         "gpu_launches": launches,
         "clocks": clk,
     }
@@ -703,7 +720,7 @@ def main():
         b = run_gpu_batch(a2, ws, rank, local, Dist(1, None))
         out["batched"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain", "latency_ms",
                                             "plain", "plain_split", "batched_fp64", "e2e", "phases_ms", "roofline",
-                                            "gpu_launches", "clocks")}
+                                            "tuning", "gpu_launches", "clocks")}
         out["batched"]["config"] = b["config"]
         a3 = copy.copy(args)
         a3.size, a3.seconds, a3.slots, a3.rates = "medium", 3.0, 16, ""

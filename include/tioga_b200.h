@@ -187,6 +187,17 @@ int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[6], long
  * [7] peak device bytes held. */
 void tioga_b200_server_stats(void *srv, long long out[16]);
 
+/* Autotuner: after tioga_preprocess_grids_, times every launch shape of the
+ * tuned kernels (CTAs per SM of the cell pass, the query gathering, the
+ * traversal and the candidate screen; pairs per cell-pass CTA) over *reps
+ * connectivity calls each, one knob after the other, and keeps the fastest
+ * for the instance's later calls.  The results of a call do not depend on
+ * the shapes; the instance ends with a connectivity call's results. */
+void tioga_b200_autotune_(int *reps);
+/* The shapes in use: [0] cell-pass CTAs per SM, [1] pairs per cell-pass CTA,
+ * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM. */
+void tioga_b200_tuning_(int out[8]);
+
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);
 /* 1 when a CUDA device is present and the library initialised it. */

@@ -226,3 +226,31 @@ def test_second_call_after_motion(name, precision, oracle_lib):
             np.testing.assert_array_equal(gpu[call]["cells"][b.tag], ref[call]["cells"][b.tag])
     moved = sum(int((ref[0]["iblank"][b.tag] != ref[1]["iblank"][b.tag]).sum()) for b in system.blocks)
     assert moved > 0  # the motion changed the answer, so the second call is a real test
+
+
+def test_autotune_keeps_results():
+    """The autotuner only changes launch shapes: after it the connectivity
+    results are the same bits, and the chosen shapes are among its choices."""
+    import ctypes as C
+    from tioga_b200.capi import TiogaLibrary
+    system = cases.small_config1(3)
+    t = TiogaLibrary(tb.library_path())
+    tb.extras(t.lib)
+    t.init()
+    t.register_system(system)
+    t.preprocess_grids()
+    t.performconnectivity()
+    before = {b.tag: (t.iblank(b.tag).copy(), t.getdonorinfo(b.tag)) for b in system.blocks}
+    tb.set_int(t.lib, "tioga_b200_autotune_", 1)
+    assert t.lib.tioga_b200_last_error() == 0
+    out = (C.c_int * 8)()
+    t.lib.tioga_b200_tuning_(out)
+    assert out[0] in (1, 2, 3, 4, 6) and out[1] in (32, 64, 128) and out[2] in (4, 8, 16, 32, 64)
+    assert out[3] in (16, 32, 64, 128) and out[4] in (8, 16, 32, 64)
+    for b in system.blocks:
+        ib, (r, i, f) = before[b.tag]
+        r2, i2, f2 = t.getdonorinfo(b.tag)
+        assert np.array_equal(ib, t.iblank(b.tag))
+        assert np.array_equal(r, r2) and np.array_equal(i, i2)
+        assert np.array_equal(f.view(np.int64), f2.view(np.int64))
+    t.delete()

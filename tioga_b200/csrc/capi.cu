@@ -262,6 +262,21 @@ void tioga_b200_stats_(long long out[16]) {
   out[13] = s.nmerged;
 }
 
+void tioga_b200_autotune_(int* reps) {
+  if (ready("tioga_b200_autotune_")) set_rc(g_tg->autotune(*reps));
+}
+
+void tioga_b200_tuning_(int out[8]) {
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  if (!g_tg) return;
+  const tb::Tuning& t = g_tg->tuning();
+  out[0] = t.cell_pass_per_sm;
+  out[1] = t.chunk_pairs;
+  out[2] = t.query_per_sm;
+  out[3] = t.traverse_per_sm;
+  out[4] = t.candidates_per_sm;
+}
+
 void tioga_b200_set_stream_(void* stream) {
   if (ready("tioga_b200_set_stream_")) g_tg->set_stream((cudaStream_t)stream);
 }

@@ -911,7 +911,7 @@ int Engine::run_pairs_and_refit() {
                           cudaMemcpyHostToDevice, stream_));
   // chunks of consecutive blocks whose pairs fit one CTA's shared memory;
   // the CTAs of one launch are split among the chunks by leaf count
-  constexpr int kChunkPairs = 128;
+  const int kChunkPairs = std::max(16, std::min(128, tune_.chunk_pairs));
   std::vector<int4> chunks;
   for (int b = 0; b < nb;) {
     int e = b + 1;
@@ -919,7 +919,7 @@ int Engine::run_pairs_and_refit() {
     chunks.push_back(make_int4(h_blk_leaf_[b], h_blk_leaf_[e], h_pfirst_[b], h_pfirst_[e] - h_pfirst_[b]));
     b = e;
   }
-  const long long want = grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * 3);
+  const long long want = grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * tune_.cell_pass_per_sm);
   std::vector<int> ccta(chunks.size() + 1, 0);
   int maxnp = 1;
   for (size_t k = 0; k < chunks.size(); k++) {
@@ -968,7 +968,7 @@ int Engine::run_queries() {
   TB_CUDA(tile_cnt_.ensure(ntiles + 1));
   TB_CUDA(tile_off_.ensure(ntiles + 1));
   TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
-  const unsigned grid = (unsigned)std::max(1ll, std::min(ntiles, 148ll * 16));
+  const unsigned grid = (unsigned)std::max(1ll, std::min(ntiles, 148ll * tune_.query_per_sm));
   k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_cnt_.p,
                                            tbox_.p, tile_base_.p, node_order_.p);
   TB_LAUNCHED("k_query_count");
@@ -1016,7 +1016,7 @@ int Engine::run_search() {
   TB_CUDA(cudaEventRecord(sev_[1], stream_));
   if (count > 0) {
     TB_CUDA(refine_.ensure(count));
-    launch_candidates(form, grid_for(count, 256), stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p, sorted_cell_.p,
+    launch_candidates(form, grid_for(count, 256, 148 * tune_.candidates_per_sm), stream_, x_.p, conn8_.p, cell_nv_.p, cell_res_.p, sorted_cell_.p,
                       qnode_.p, cand_.p, (int)count, qkey_.p, qacc_.p, refine_.p, scount_.p + 1, counters_.p);
     TB_LAUNCHED("k_candidates");
     TB_CUDA(cudaEventRecord(sev_[2], stream_));
@@ -1057,7 +1057,7 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq, 256, 148 * 64), stream_, xq, d_bi_.p, cbox_.p,
+    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, cbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
     TB_LAUNCHED("k_traverse");
@@ -1500,6 +1500,44 @@ int Engine::download_iblank() {
     }
   }
   return 0;
+}
+
+int Engine::autotune(int reps) {
+  if (!preprocessed_) {
+    fprintf(stderr, "#tioga_b200: autotune needs preprocess_grids first\n");
+    return -1;
+  }
+  struct Knob {
+    int* v;
+    std::vector<int> cand;
+    float Timing::*phase;
+  };
+  const Knob knobs[] = {
+      {&tune_.cell_pass_per_sm, {1, 2, 3, 4, 6}, &Timing::cell_pass},
+      {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
+      {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
+      {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},
+      {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
+  };
+  reps = std::max(1, reps);
+  for (const Knob& k : knobs) {
+    int best = *k.v;
+    float tbest = 1e30f;
+    for (int c : k.cand) {
+      *k.v = c;
+      float t = 1e30f;
+      for (int r = 0; r < reps; r++) {
+        TB_TRY(connectivity());
+        t = std::min(t, timing_.*k.phase);
+      }
+      if (t < tbest) {
+        tbest = t;
+        best = c;
+      }
+    }
+    *k.v = best;
+  }
+  return connectivity();  // leave the instance with results of the chosen shapes
 }
 
 int Engine::connectivity() {

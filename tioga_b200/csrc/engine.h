@@ -208,6 +208,13 @@ struct Stats {
   unsigned error = 0;
 };
 
+// Launch shapes the autotuner chooses among (results never depend on them):
+// CTAs per SM of the cell pass, the query gathering, the traversal and the
+// candidate screen, and the pairs one cell-pass CTA holds in shared memory.
+struct Tuning {
+  int cell_pass_per_sm = 3, query_per_sm = 16, traverse_per_sm = 64, candidates_per_sm = 16, chunk_pairs = 128;
+};
+
 struct Timing {
   float holemap = 0, boxes = 0, refit = 0, query = 0, search = 0, donors = 0, celliblank = 0,
         total = 0, upload = 0, download = 0;
@@ -262,6 +269,11 @@ class Engine {
   // the path
   int preprocess();
   int connectivity();
+  // times each launch shape of every tuned kernel over `reps` connectivity
+  // calls (coordinate descent, one knob after the other) and keeps the
+  // fastest; needs a preprocessed instance
+  int autotune(int reps);
+  const Tuning& tuning() const { return tune_; }
   int dataupdate(int nvar, int interptype);
 
   // queries (src/dataUpdate.C:121-159, tioga.C:533-570)
@@ -457,6 +469,7 @@ class Engine {
 
   Stats stats_;
   Timing timing_;
+  Tuning tune_;
 };
 
 }  // namespace tb
