@@ -69,15 +69,17 @@ def parse():
     p.add_argument("--cpu-reps", type=int, default=3)
     p.add_argument("--size", default="full", choices=["full", "medium", "small"],
                    help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
-    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg3"],
+    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg3", "cfg4"],
                    help="cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems; "
-                        "cfg3: the serving form, Poisson requests over resident moving systems")
+                        "cfg3: the serving form, Poisson requests over resident moving systems; "
+                        "cfg4: the high-order path, degree-3 Lagrange shell over a degree-1 background")
     p.add_argument("--rates", default="",
                    help="cfg3: comma-separated arrival rates (requests/s); default: a sweep around capacity")
     p.add_argument("--seconds", type=float, default=6.0, help="cfg3: arrival window per rate")
     p.add_argument("--slots", type=int, default=8, help="cfg3: concurrent requests")
     p.add_argument("--nsys", type=int, default=200, help="cfg3: systems")
     p.add_argument("--budget-gb", type=float, default=120.0, help="cfg3: HBM admission budget")
+    p.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
     p.add_argument("--forms", default="split,plain,e2e",
@@ -234,7 +236,7 @@ def run_gpu(args, ws, rank, local, dist):
     lib.performconnectivity()
     if lib.lib.tioga_b200_last_error() != 0:
         raise RuntimeError("connectivity failed")
-    tuning = autotune(lib, tb)
+    tuning = None if args.no_tune else autotune(lib, tb)
 
     # device-resident forms keep iblank in HBM too (a GPU solver's arrays)
     d_ibl = [torch.ones(b.nnodes, dtype=torch.int32, device="cuda") for b in system.blocks]
@@ -396,9 +398,12 @@ def run_gpu_batch(args, ws, rank, local, dist):
         return ev[0].elapsed_time(ev[steps]) / steps, per, tb.stats(lib.lib), avg, launches, clk
 
     # plain form: one system per instance, one after another
-    plain_ms = {0: 0.0, 1: 0.0}
-    plain_q = 0
-    for (psys, ibls, _keep) in pinned:
+    forms = args.forms.split(",")
+    plain_ms = {0: float("nan"), 1: float("nan")}
+    plain_q = None
+    for (psys, ibls, _keep) in (pinned if "plain" in forms else []):
+        if plain_q is None:
+            plain_ms, plain_q = {0: 0.0, 1: 0.0}, 0
         lib.init()
         lib.register_system(psys, ibls)
         lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
@@ -429,24 +434,27 @@ def run_gpu_batch(args, ws, rank, local, dist):
             d_ibl.append(d)
             lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(d.data_ptr()))
     tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
-    tuning = autotune(lib, tb)
+    tuning = None if args.no_tune else autotune(lib, tb)
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = Clocks(vis.split(",")[local] if vis else str(local))
     ms_b, per_b, st, ph, launches, clk = events_time(args.steps, args.warmup, clocks)
     Q = st["nquery"]
-    assert Q == plain_q, (Q, plain_q)
-    tb.set_int(lib.lib, "tioga_b200_set_precision_", 0)
-    ms_b64, _, st64, _, _, _ = events_time(max(1, args.steps // 2), 1)
-    assert st64["nquery"] == Q
+    assert plain_q is None or Q == plain_q, (Q, plain_q)
+    ms_b64 = ms_e2e = float("nan")
+    if "plain" in forms:
+        tb.set_int(lib.lib, "tioga_b200_set_precision_", 0)
+        ms_b64, _, st64, _, _, _ = events_time(max(1, args.steps // 2), 1)
+        assert st64["nquery"] == Q
     # end to end: host coordinates in, host iblanks out, every step
-    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
-    tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 0)
-    for k, s in enumerate(systems):
-        lib.select_system(k)
-        for b in s.blocks:
-            lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(0))
-    ms_e2e, _, st_e, _, _, _ = events_time(args.steps, args.warmup)
-    assert st_e["nquery"] == Q
+    if "e2e" in forms:
+        tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+        tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 0)
+        for k, s in enumerate(systems):
+            lib.select_system(k)
+            for b in s.blocks:
+                lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(0))
+        ms_e2e, _, st_e, _, _, _ = events_time(args.steps, args.warmup)
+        assert st_e["nquery"] == Q
     nodes = sum(s.nnodes for s in systems)
     cells = sum(s.ncells for s in systems)
     h2d, d2h = 24 * nodes, 4 * nodes
@@ -640,6 +648,135 @@ def run_gpu_serving(args, ws, rank, local, dist):
 
 
 # ---------------------------------------------------------------------------
+# high-order path: degree-3 Lagrange shell over a degree-1 background
+# ---------------------------------------------------------------------------
+WORKLOAD4 = ("cfg4: 97^3 degree-1 background + a curved spherical-shell band of 24x24x48 degree-3 Lagrange "
+             "hexahedra (64 DOFs each), interior DOFs perturbed +-2%, seed 4; one step = performconnectivity + "
+             "performconnectivity_highorder; a seeded cubic field (5 variables) for the data update")
+
+
+def run_gpu_highorder(args, ws, rank, local, dist):
+    import torch
+
+    import tioga_b200 as tb
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    if args.size == "small":
+        system, ho = cases.config4(4, nbg=33, ne_r=6, ne_t=8, ne_p=16)
+    elif args.size == "medium":
+        system, ho = cases.config4(4, nbg=65, ne_r=12, ne_t=12, ne_p=24)
+    else:
+        system, ho = cases.config4(4)
+    nvar = 5
+    lib = TiogaLibrary(tb.library_path())
+    tb.extras(lib.lib)
+    lib.init()
+    lib.register_system(system)
+    xd = [np.ascontiguousarray(h.xdof, dtype=np.float64) for h in ho]
+    for b, h, x in zip(system.blocks, ho, xd):
+        lib.lib.tioga_b200_set_highorder_lagrange_(C.byref(C.c_int(b.tag)), C.byref(C.c_int(h.p)),
+                                                   x.ctypes.data_as(C.c_void_p))
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
+    tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
+    lib.preprocess_grids()
+
+    def hostats():
+        st = (C.c_longlong * 8)()
+        lib.lib.tioga_b200_highorder_stats_(st)
+        return list(st)
+
+    def timed(prec, steps, warmup, resident=1):
+        tb.set_int(lib.lib, "tioga_b200_set_precision_", prec)
+        tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", resident)
+        for _ in range(warmup):
+            lib.performconnectivity()
+            lib.lib.tioga_performconnectivity_highorder_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for k in range(steps):
+            lib.performconnectivity()
+            lib.lib.tioga_performconnectivity_highorder_()
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+        if lib.lib.tioga_b200_last_error() != 0:
+            raise RuntimeError("high-order connectivity failed")
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        return ev[0].elapsed_time(ev[steps]) / steps, per, hostats()
+
+    def update():
+        q0 = cases.dof_fields(ho, nvar, seed=5)  # the cubic at every DOF
+        q = [a.copy() for a in q0]
+        for b, a in zip(system.blocks, q):
+            lib.registersolution(b.tag, a)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib.dataupdate_mb(nvar, "row")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return q0, q, e0.elapsed_time(e1)
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    clocks = Clocks(vis.split(",")[local] if vis else str(local))
+    clocks.start()
+    ms_split, per_split, st_split = timed(1, args.steps, args.warmup)
+    clk = clocks.stop()
+    q0, q_split, upd_ms = update()
+    forms = args.forms.split(",")
+    if "plain" in forms:
+        ms_fp64, per_fp64, st_fp64 = timed(0, max(2, args.steps // 2), 1)
+        _, q_fp64, _ = update()
+        ms_scr, _, st_scr = timed(2, max(2, args.steps // 2), 1)
+        _, q_scr, _ = update()
+        scr_vs_fp64 = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(q_scr, q_fp64))
+    else:
+        ms_fp64, st_fp64, q_fp64, ms_scr, st_scr, scr_vs_fp64 = float("nan"), st_split, q_split, float("nan"), \
+            st_split, float("nan")
+    ms_e2e = timed(1, max(2, args.steps // 2), 1, resident=0)[0] if "e2e" in forms else float("nan")
+    h2d = 24 * system.nnodes + sum(24 * h.xdof.shape[0] * h.xdof.shape[1] for h in ho)
+    Q = st_split[0]
+    assert st_fp64[0] == Q
+    changed = np.concatenate([(a != b) for a, b in zip(q_split, q0)])
+    split_vs_fp64 = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(q_split, q_fp64))
+    interp_err = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(q_split, q0))
+    out = {
+        "metric": METRIC, "value": ws * Q / (ms_split * 1e-3), "unit": UNIT + " (high-order query points)",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded mesh generator tioga_b200.cases.config4, seeded cubic field)",
+        "config": {"workload": WORKLOAD4 if args.size == "full" else f"cfg4 geometry, {args.size} size",
+                   "nodes": system.nnodes, "cells": system.ncells,
+                   "shell_elements": int(ho[1].xdof.shape[0]), "dofs_per_element": int(ho[1].xdof.shape[1]),
+                   "highorder_query_points": Q, "parallelism": f"replicas x{ws}"},
+        "latency_ms": {"p50": float(np.percentile(per_split, 50)), "p99": float(np.percentile(per_split, 99))},
+        "plain": {"value": ws * Q / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64, "precision": "fp64 throughout"},
+        "speedup_vs_plain": ms_fp64 / ms_split,
+        "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 4 * system.nnodes,
+                "note": "corner and DOF coordinates uploaded from the caller's arrays every step"},
+        "inclusion_tests": {"split": {"tests": st_split[6], "fp64_decided": st_split[7]},
+                            "fp64": {"tests": st_fp64[6], "fp64_decided": st_fp64[7]},
+                            "fp32_screen": {"tests": st_scr[6], "fp64_decided": st_scr[7], "ms_per_step": ms_scr,
+                                            "max_abs_vs_fp64": scr_vs_fp64}},
+        "point_donors": st_split[1], "ties": st_split[2], "records": st_split[3],
+        "dataupdate": {"ms": upd_ms, "updated_values": int(changed.sum())},
+        "errors": {"split_vs_fp64_max_abs": split_vs_fp64,
+                   "note": "the FP64 form is bit-identical to the oracle (tests/test_gpu_highorder.py), so "
+                           "split_vs_fp64 is the error against the FP64 oracle",
+                   "cubic_field_max_abs": interp_err,
+                   "cubic_note": "updated DOF values against the cubic they sample: the interpolation error of "
+                                 "the donors (curved isoparametric and trilinear elements do not reproduce a "
+                                 "cubic in x, y, z exactly)"},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
+    lib.delete()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # CPU: the compiled reference (or the C restatement) on a bounded sample
 # ---------------------------------------------------------------------------
 def sample_query_count(sample):
@@ -708,8 +845,8 @@ def main():
         if ws > 1:
             import torch
             torch.cuda.set_device(local)
-        out = {"cfg2": run_gpu_batch, "cfg3": run_gpu_serving}.get(args.workload, run_gpu)(args, ws, rank, local,
-                                                                                           dist)
+        out = {"cfg2": run_gpu_batch, "cfg3": run_gpu_serving,
+               "cfg4": run_gpu_highorder}.get(args.workload, run_gpu)(args, ws, rank, local, dist)
     finally:
         dist.close()
     if rank == 0 and ws == 1 and args.workload == "cfg1" and not args.no_forms:

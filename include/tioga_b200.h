@@ -122,7 +122,10 @@ void tioga_b200_set_highorder_lagrange_(int *btag, int *order, double *xdof);
 int tioga_b200_pointdonors_(int *btag, int *out, double *w);
 /* High-order counters: [0] query points, [1] with a donor, [2] ties,
  * [3] interpolation records, [4] coincident points merged, [5] receptor
- * cells changed by the orphan rule in the last data update. */
+ * cells changed by the orphan rule in the last data update, [6] inclusion
+ * tests (candidates whose box holds the point), [7] of those decided by the
+ * FP64 Newton (all of them in the FP64 form; in the split form the rest are
+ * clear cases of an FP32 Newton). */
 void tioga_b200_highorder_stats_(long long out[8]);
 
 /* Batched form: the blocks of many independent overset systems in one
@@ -202,9 +205,13 @@ void tioga_b200_tuning_(int out[8]);
 int tioga_b200_last_error(void);
 /* 1 when a CUDA device is present and the library initialised it. */
 int tioga_b200_device_ok(void);
-/* Search arithmetic: 0 = FP64 throughout; 1 (default) = FP32 screen of the
- * Newton inversion with FP64 refinement of every undecided candidate.
- * Results are identical (every accept/reject near the TOL band is FP64). */
+/* Search arithmetic: 0 = FP64 throughout; 1 (default) = FP32 tree boxes and
+ * an FP32 screen of the Newton inversion with FP64 refinement of every
+ * undecided candidate; 2 = as 1, and the high-order inclusion test also
+ * screened in FP32 (clear outsiders rejected; every other candidate still
+ * takes the FP64 test, whose fixed 1e-14 stopping rule must be replayed, so
+ * on meshes whose candidates mostly pass this costs more than it saves).
+ * Results are identical in every mode. */
 void tioga_b200_set_precision_(int *mode);
 /* 1: the coordinates have not moved since the last call, so connectivity
  * skips their upload.  Default 0 (TIOGA re-reads x at every call). */

@@ -33,13 +33,20 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("precision", [0, 1, 2], ids=["fp64", "split", "split-ho-screen"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_highorder_matches_oracle(name, oracle_lib):
+def test_highorder_matches_oracle(name, precision, oracle_lib):
     system, ho, res, setup = CASES[name]()
     nvar = 3
     q = cases.dof_fields(ho, nvar, seed=21)
     ref = run_highorder(oracle_lib, system, ho, nvar, q, "hook", resolutions=res, setup=setup)
-    gpu = run_highorder(tb.library_path(), system, ho, nvar, q, "gpu", resolutions=res, setup=setup)
+
+    def gsetup(t):
+        tb.set_int(t.lib, "tioga_b200_set_precision_", precision)
+        if setup is not None:
+            setup(t)
+
+    gpu = run_highorder(tb.library_path(), system, ho, nvar, q, "gpu", resolutions=res, setup=gsetup)
     problems = diff_highorder(system, ref, gpu)
     assert not problems, "\n".join(problems)
     st = gpu["stats"]
@@ -49,3 +56,7 @@ def test_highorder_matches_oracle(name, oracle_lib):
     assert changed > 0
     if name == "both-ways":  # cubic donors reached background points
         assert ref["points"][system.blocks[1].tag][0].shape[0] > 0
+    # inclusion tests, and those left to the FP64 Newton: all of them unless
+    # the high-order screen runs, then the candidates not clearly outside
+    assert st[6] > 0
+    assert (st[7] == st[6]) if precision < 2 else (st[7] <= st[6]), st

@@ -219,6 +219,8 @@ void tioga_b200_highorder_stats_(long long out[8]) {
   out[3] = s.nrecords;
   out[4] = s.nmerged;
   out[5] = s.norphan_cells;
+  out[6] = s.ncand;
+  out[7] = s.nrefine;
 }
 void tioga_reduce_fringes_(void) { unsupported("tioga_reduce_fringes_"); }
 void tioga_writeoutputfiles_(int*, char*) { unsupported("tioga_writeoutputfiles_"); }

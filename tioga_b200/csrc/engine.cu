@@ -152,6 +152,7 @@ int Engine::register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl
   topo_dirty_ = true;
   coords_on_device_ = false;
   gate_valid_ = false;
+  ho_dof_on_device_ = false;
   preprocessed_ = false;
   connected_ = false;
   return 0;

@@ -156,6 +156,7 @@ struct HoDev {  // per block, on the device
 };
 struct HoStats {
   long long npoints = 0, ndonor = 0, nties = 0, nrecords = 0, nmerged = 0, norphan_cells = 0;
+  long long ncand = 0, nrefine = 0;  // inclusion tests of in-box candidates, and those decided in FP64
 };
 
 // A pair-major query list for the coincident-point merge: query q is point
@@ -379,6 +380,7 @@ class Engine {
   // high-order path
   std::vector<HoBlockDesc> ho_;
   bool ihigh_ = false, ihigh_global_ = false, ho_done_ = false;
+  bool ho_dof_on_device_ = false;  // ho_xdof_ holds the registered DOF coordinates
   DBuf<HoDev> ho_dev_;
   DBuf<double> ho_xdof_, ho_pts_, ho_qres_, ho_w_, ho_q_, ho_qtmp_;
   DBuf<int> ho_ctag_, ho_rcblk_, ho_qpt_, ho_qloc_, ho_qdon_, ho_qrec_, ho_qbest_, ho_npass_, ho_qcell_, ho_win_;

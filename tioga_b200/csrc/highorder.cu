@@ -95,7 +95,8 @@ __global__ void k_ho_candidates(const double* __restrict__ pts, const double* __
                                 const int* __restrict__ sorted_cell, const BlockInfo* __restrict__ bi,
                                 const HoDev* __restrict__ hd, const double* __restrict__ xdof,
                                 const int* __restrict__ qpt, const int* __restrict__ qdon, const int2* __restrict__ cand,
-                                long long ncand, int* __restrict__ qbest, int* __restrict__ npass) {
+                                long long ncand, int form, int* __restrict__ qbest, int* __restrict__ npass,
+                                unsigned long long* __restrict__ counters) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncand;
        i += (long long)gridDim.x * blockDim.x) {
     const int2 cq = cand[i];
@@ -115,9 +116,20 @@ __global__ void k_ho_candidates(const double* __restrict__ pts, const double* __
     const int a = qdon[q];
     const int lc = sorted_cell[s] - bi[a].cell_off;
     const HoDev h = hd[a];
-    double u[3];
-    const bool ok = ho_invert(h.p, xdof + 3 * (h.dof_off + (long long)lc * h.npts), xp, u);
-    if (ok && ho_inside(u)) {
+    const double* X = xdof + 3 * (h.dof_off + (long long)lc * h.npts);
+    // split form: an FP32 Newton rejects the clear outsiders; every other
+    // candidate takes the FP64 test, accepts included, since its fixed 1e-14
+    // stopping rule can fail to converge inside an element (the update cannot
+    // always get below 1e-14 in FP64), and that failure rejects the point
+    const int screen = form ? ho_screen32(h.p, X, xp) : -1;
+    bool pass = false;
+    if (screen != 0) {
+      double u[3];
+      pass = ho_invert(h.p, X, xp, u) && ho_inside(u);
+      atomicAdd(&counters[9], 1ull);
+    }
+    atomicAdd(&counters[10], 1ull);
+    if (pass) {
       atomicMin(&qbest[q], lc);
       atomicAdd(&npass[q], 1);
     }
@@ -271,6 +283,7 @@ int Engine::set_highorder(int tag, int p, const double* xdof) {
   ho_[ib].p = p;
   ho_[ib].npts = (p + 1) * (p + 1) * (p + 1);
   ho_[ib].hxdof = xdof;
+  ho_dof_on_device_ = false;
   ihigh_ = true;
   return 0;
 }
@@ -303,11 +316,15 @@ int Engine::connectivity_highorder() {
   }
   TB_CUDA(ho_dev_.ensure(nb));
   TB_CUDA(cudaMemcpyAsync(ho_dev_.p, hd.data(), nb * sizeof(HoDev), cudaMemcpyHostToDevice, stream_));
-  TB_CUDA(ho_xdof_.ensure(3 * std::max(1ll, ndof)));
-  for (int b = 0; b < nb; b++)
-    TB_CUDA(cudaMemcpyAsync(ho_xdof_.p + 3 * hd[b].dof_off, ho_[b].hxdof,
-                            3 * (size_t)hb_[b].ncells * ho_[b].npts * sizeof(double), cudaMemcpyHostToDevice,
-                            stream_));
+  // (kept on the device when the caller declares its coordinates unmoved)
+  if (!(coords_resident_ && ho_dof_on_device_ && ho_xdof_.n >= 3 * (size_t)std::max(1ll, ndof))) {
+    TB_CUDA(ho_xdof_.ensure(3 * std::max(1ll, ndof)));
+    for (int b = 0; b < nb; b++)
+      TB_CUDA(cudaMemcpyAsync(ho_xdof_.p + 3 * hd[b].dof_off, ho_[b].hxdof,
+                              3 * (size_t)hb_[b].ncells * ho_[b].npts * sizeof(double), cudaMemcpyHostToDevice,
+                              stream_));
+    ho_dof_on_device_ = true;
+  }
   // receptor cells (getInternalNodes, highOrder.C:208-247)
   DBuf<int> flag, off;
   TB_CUDA(flag.ensure(ctot_ + 1));
@@ -430,7 +447,7 @@ int Engine::connectivity_highorder() {
   if (count > 0) {
     k_ho_candidates<<<grid_for(count, 128), 128, 0, stream_>>>(
         ho_pts_.p, x_.p, conn8_.p, cell_nv_.p, sorted_cell_.p, d_bi_.p, ho_dev_.p, ho_xdof_.p, ho_qpt_.p,
-        ho_qdon_.p, cand_.p, count, ho_qbest_.p, ho_npass_.p);
+        ho_qdon_.p, cand_.p, count, precision_ == 2 ? 1 : 0, ho_qbest_.p, ho_npass_.p, counters_.p);
     TB_LAUNCHED("k_ho_candidates");
   }
   k_ho_finish<<<grid_for(nq, kT), kT, 0, stream_>>>(ho_qbest_.p, ho_npass_.p, nq, ho_qcell_.p, counters_.p);
@@ -465,7 +482,8 @@ int Engine::connectivity_highorder() {
   unsigned long long cnt[16];
   TB_CUDA(cudaMemcpyAsync(cnt, counters_.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
-  ho_stats_ = {nq, (long long)cnt[3], (long long)cnt[2], (long long)nr, (long long)cnt[7], 0};
+  ho_stats_ = {nq, (long long)cnt[3], (long long)cnt[2], (long long)nr, (long long)cnt[7], 0, (long long)cnt[10],
+               (long long)cnt[9]};
   ho_done_ = true;
   return 0;
 }

@@ -108,4 +108,90 @@ __device__ inline void ho_weights(int p, const double u[3], double* w) {
       for (int i = 0; i < n1; i++, m++) w[m] = (lr[i] * ls[j]) * lt[k];
 }
 
+// FP32 screen of the inclusion test for the split-precision form: Newton on
+// the element map in FP32, on offsets from the element's first DOF (so the
+// coordinates' common part does not cost precision).  Returns 1 when it
+// converged clearly inside (every reference coordinate within [1e-3,
+// 1 - 1e-3]), 0 clearly outside (one below -1e-3 or above 1 + 1e-3), -1
+// otherwise (near a face, no convergence in 20 steps, a near-singular map).
+// Both iterate from the same centre and converge to the same point to about
+// 1e-6, so a clear outside is the FP64 test's reject; a clear inside is not
+// enough for an accept, which also needs the FP64 update to fall below 1e-14.
+__device__ inline void ho_basis1f(int p, float r, float* l, float* dl) {
+  for (int i = 0; i <= p; i++) {
+    const float xi = (float)i / p;
+    float v = 1.f, d = 0.f;
+    for (int m = 0; m <= p; m++) {
+      if (m == i) continue;
+      const float xm = (float)m / p;
+      const float den = xi - xm;
+      d = d * ((r - xm) / den) + v / den;
+      v = v * ((r - xm) / den);
+    }
+    l[i] = v;
+    dl[i] = d;
+  }
+}
+
+__device__ inline int ho_screen32(int p, const double* __restrict__ X, const double* xp) {
+  const int n1 = p + 1;
+  const double x0[3] = {X[0], X[1], X[2]};
+  const float fp[3] = {(float)(xp[0] - x0[0]), (float)(xp[1] - x0[1]), (float)(xp[2] - x0[2])};
+  float u[3] = {0.5f, 0.5f, 0.5f};
+  for (int it = 0; it < 20; it++) {
+    float lr[kHoMaxN], ls[kHoMaxN], lt[kHoMaxN], dr[kHoMaxN], ds[kHoMaxN], dt[kHoMaxN];
+    ho_basis1f(p, u[0], lr, dr);
+    ho_basis1f(p, u[1], ls, ds);
+    ho_basis1f(p, u[2], lt, dt);
+    float x[3] = {0.f, 0.f, 0.f}, J[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    for (int k = 0; k < n1; k++)
+      for (int j = 0; j < n1; j++)
+        for (int i = 0; i < n1; i++) {
+          const double* P = X + 3 * ((k * n1 + j) * n1 + i);
+          const float w = (lr[i] * ls[j]) * lt[k];
+          const float wr = (dr[i] * ls[j]) * lt[k];
+          const float ws = (lr[i] * ds[j]) * lt[k];
+          const float wt = (lr[i] * ls[j]) * dt[k];
+          for (int a = 0; a < 3; a++) {
+            const float pa = (float)(P[a] - x0[a]);
+            x[a] = __fmaf_rn(w, pa, x[a]);
+            J[a][0] = __fmaf_rn(wr, pa, J[a][0]);
+            J[a][1] = __fmaf_rn(ws, pa, J[a][1]);
+            J[a][2] = __fmaf_rn(wt, pa, J[a][2]);
+          }
+        }
+    const float f0 = fp[0] - x[0], f1 = fp[1] - x[1], f2 = fp[2] - x[2];
+    const float c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const float c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const float c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const float det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const float n0 = sqrtf(J[0][0] * J[0][0] + J[1][0] * J[1][0] + J[2][0] * J[2][0]);
+    const float nn1 = sqrtf(J[0][1] * J[0][1] + J[1][1] * J[1][1] + J[2][1] * J[2][1]);
+    const float n2 = sqrtf(J[0][2] * J[0][2] + J[1][2] * J[1][2] + J[2][2] * J[2][2]);
+    const float scale = n0 * nn1 * n2;
+    if (!(scale > 0.f) || !(fabsf(det) > 1e-3f * scale)) return -1;
+    const float id = 1.f / det;
+    const float d0 = (f0 * c00 + f1 * (J[0][2] * J[2][1] - J[0][1] * J[2][2]) +
+                      f2 * (J[0][1] * J[1][2] - J[0][2] * J[1][1])) * id;
+    const float d1 = (f0 * c01 + f1 * (J[0][0] * J[2][2] - J[0][2] * J[2][0]) +
+                      f2 * (J[0][2] * J[1][0] - J[0][0] * J[1][2])) * id;
+    const float d2 = (f0 * c02 + f1 * (J[0][1] * J[2][0] - J[0][0] * J[2][1]) +
+                      f2 * (J[0][0] * J[1][1] - J[0][1] * J[1][0])) * id;
+    u[0] += d0;
+    u[1] += d1;
+    u[2] += d2;
+    if (!(fabsf(u[0]) < 1e3f && fabsf(u[1]) < 1e3f && fabsf(u[2]) < 1e3f)) return -1;
+    if (fabsf(d0) + fabsf(d1) + fabsf(d2) < 1e-5f) {
+      constexpr float e = 1e-3f;
+      bool in = true;
+      for (int k = 0; k < 3; k++) {
+        if (u[k] < -e || u[k] > 1.f + e) return 0;
+        in = in && u[k] >= e && u[k] <= 1.f - e;
+      }
+      return in ? 1 : -1;
+    }
+  }
+  return -1;
+}
+
 }  // namespace tb
