@@ -90,12 +90,17 @@ void tioga_set_highorder_callback_(void (*f1)(int *, int *), void (*f2)(int *, i
                                    void (*f4)(int *, double *, int *, int *, double *, double *, int *),
                                    void (*f5)(int *, int *, double *, int *, int *, double *));
 
-/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
- * p4est, fringe reduction, Tecplot output).  They are exported so that
- * existing solvers link; each reports "not supported" and sets the last
- * error. */
-void tioga_performconnectivity_amr_(void);
+/* tiogaInterface.C:302-305 -- after performconnectivity: keep only the
+ * receptors within nfringe+1 layers of the field nodes (tioga.C:737-885,
+ * bookKeeping.C:650-760); the others' interpolations are cancelled and
+ * they become holes.  ibl[] is rewritten; the cell iblanks stay as the
+ * connectivity call left them, as in TIOGA. */
 void tioga_reduce_fringes_(void);
+
+/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
+ * p4est, Tecplot output).  They are exported so that existing solvers link;
+ * each reports "not supported" and sets the last error. */
+void tioga_performconnectivity_amr_(void);
 void tioga_writeoutputfiles_(int *nvar, char *itype);
 
 /* ---- additions of this library (no counterpart in TIOGA) -------------- */

@@ -1765,6 +1765,87 @@ void tioga_delete_(void) {
   memset(&G, 0, sizeof(G));
 }
 
+/* tioga::reduce_fringes (src/tioga.C:737-885) with MeshBlock::reduce_fringes
+ * (src/bookKeeping.C:650-760): keep only the receptors within nfringe+1
+ * layers of the field, cancel the others through their head donor
+ * (getCancellationData, cancelDonor: bookKeeping.C:542-570), resetCoincident,
+ * then clearIblanks (receptors -> 1, nodes outside the reduced set -> 0,
+ * bookKeeping.C:615-625) and setIblanks for the surviving interpolations. */
+void tioga_reduce_fringes_(void) {
+  int **red = (int **)calloc(G.nblocks ? G.nblocks : 1, sizeof(int *));
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *r = G.b[ib];
+    int nn = r->nnodes;
+    red[ib] = (int *)malloc(sizeof(int) * (nn ? nn : 1));
+    int *tmp = (int *)malloc(sizeof(int) * (nn ? nn : 1));
+    for (int i = 0; i < nn; i++) red[ib][i] = r->iblank[i] > 0 ? r->iblank[i] : 0;
+    for (int i = 0; i < nn; i++) tmp[i] = red[ib][i];
+    for (int iter = 0; iter < r->nfringe + 1; iter++) {
+      for (int n = 0; n < r->ntypes; n++) {
+        int nvert = r->nv[n];
+        for (int i = 0; i < r->nc[n]; i++) {
+          const int *cv = r->vconn[n] + nvert * i;
+          int ncount = 0;
+          for (int m = 0; m < nvert; m++) {
+            int v = cv[m] - 1;
+            ncount = ncount + (red[ib][v] == 1 || red[ib][v] < 0);
+          }
+          if (ncount > 0 && ncount < nvert)
+            for (int m = 0; m < nvert; m++) {
+              int v = cv[m] - 1;
+              if (tmp[v] == 0 && r->iblank[v] < 0) tmp[v] = r->iblank[v];
+            }
+        }
+      }
+      for (int i = 0; i < nn; i++) red[ib][i] = tmp[i];
+    }
+    free(tmp);
+  }
+  /* cancellations through each cancelled node's head donor, node order */
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *r = G.b[ib];
+    for (int v = 0; v < r->nnodes; v++) {
+      if (!(r->iblank[v] < 0 && red[ib][v] == 0)) continue;
+      if (r->dl_cnt == NULL || r->dl_cnt[v] == 0) continue;
+      const cand_t *h = &r->dl[r->dl_off[v]];
+      block_t *dd = G.b[find_tag(h->mtag)];
+      int ip = dd->interp2donor[h->remote];
+      if (ip > -1) dd->interp[ip].cancel = 1;
+    }
+  }
+  /* resetCoincident (bookKeeping.C:572-597) */
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *d = G.b[ib];
+    if (d->interp2donor == NULL) continue;
+    int *reset = (int *)malloc(sizeof(int) * (d->nsearch ? d->nsearch : 1));
+    for (int q = 0; q < d->nsearch; q++) reset[q] = 1;
+    for (int q = 0; q < d->nsearch; q++) {
+      int ip = d->interp2donor[q];
+      if (ip > -1 && d->interp[ip].cancel < reset[d->xtag[q]]) reset[d->xtag[q]] = d->interp[ip].cancel;
+    }
+    for (int q = 0; q < d->nsearch; q++) {
+      int ip = d->interp2donor[q];
+      if (ip > -1 && d->interp[ip].cancel == 1) d->interp[ip].cancel = reset[d->xtag[q]];
+    }
+    free(reset);
+  }
+  /* clearIblanks, then setIblanks for the surviving interpolations */
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *r = G.b[ib];
+    for (int i = 0; i < r->nnodes; i++)
+      if (r->iblank[i] < 0) r->iblank[i] = 1;
+    for (int i = 0; i < r->nnodes; i++)
+      if (red[ib][i] == 0) r->iblank[i] = 0;
+    free(red[ib]);
+  }
+  free(red);
+  for (int ib = 0; ib < G.nblocks; ib++) {
+    block_t *d = G.b[ib];
+    for (int k = 0; k < d->ninterp; k++)
+      if (!d->interp[k].cancel) G.b[d->interp[k].rinfo[2]]->iblank[d->interp[k].rinfo[1]] = -1;
+  }
+}
+
 /* ======================================================================= */
 /* high-order path: tioga.C:162-178, highOrder.C:152-566, exchangeSearchData  */
 /* ======================================================================= */

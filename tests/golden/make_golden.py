@@ -50,7 +50,15 @@ CASES = {
     # duplicated phi seams: coincident query points, merged by uniqNodesTree
     "cfg1_small_s1_seam": (lambda: cases.small_config1_seam(1), {}, 5, "row", 15),
     "cfg0_small_s2_seam_shellres": (lambda: cases.small_config0_seam(2), "shellres", 4, "row", 16),
+    # tioga_reduce_fringes_ after the connectivity (tioga.C:737-885)
+    "cfg0_small_s0_reduce": (lambda: cases.small_config0(0), "reduce", 5, "row", 17),
+    "cfg1_small_s1_reduce_nf2": (lambda: cases.small_config1(1), "reduce_nf2", 5, "row", 18),
+    "cfg1_small_s1_seam_reduce": (lambda: cases.small_config1_seam(1), "reduce", 5, "row", 19),
 }
+
+
+def _reduce(t):
+    t.lib.tioga_reduce_fringes_()
 
 
 def digest(system):
@@ -71,6 +79,10 @@ def settings_for(name, system):
         return {"resolutions": user_resolutions(system, 99)}
     if s == "shellres":
         return {"resolutions": shell_resolutions(system, 98)}
+    if s == "reduce":
+        return {"after": _reduce}
+    if s == "reduce_nf2":
+        return {"after": _reduce, "nfringe": 2}
     return dict(s)
 
 

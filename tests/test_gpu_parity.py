@@ -93,7 +93,8 @@ def test_linear_field_exact():
 
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "split"])
 @pytest.mark.parametrize("name", ["cfg0_small_s0", "cfg1_small_s1", "cfg0_small_s1_opts",
-                                  "cfg1_small_s2_userres"])
+                                  "cfg1_small_s2_userres", "cfg0_small_s0_reduce", "cfg1_small_s1_reduce_nf2",
+                                  "cfg1_small_s1_seam_reduce"])
 def test_gpu_matches_reference_fixtures(name, precision):
     """The GPU library against the compiled reference's own outputs."""
     from tests.golden import make_golden as mg
@@ -254,3 +255,61 @@ def test_autotune_keeps_results():
         assert np.array_equal(r, r2) and np.array_equal(i, i2)
         assert np.array_equal(f.view(np.int64), f2.view(np.int64))
     t.delete()
+
+
+def _reduce(t):
+    t.lib.tioga_reduce_fringes_()
+
+
+@pytest.mark.parametrize("name,nfringe", [("cfg0", 1), ("cfg0", 3), ("cfg1-small-seed3", 2)])
+def test_reduce_fringes_matches_oracle(name, nfringe, oracle_lib):
+    """tioga_reduce_fringes_ after connectivity: iblanks (deep receptors become
+    holes), surviving donor lists and the data update, against the oracle."""
+    system = CASES[name]()
+    q = cases.fields(system, nvar=5, seed=31)
+    ref = run_system(oracle_lib, system, q_blocks=q, nfringe=nfringe, after=_reduce)
+    gpu = run_system(tb.library_path(), system, q_blocks=q, nfringe=nfringe, setup=_gpu_setup(1), after=_reduce)
+    problems = diff_runs(system, ref, gpu)
+    assert not problems, "\n".join(problems)
+
+
+def test_connectivity_after_reduce_fringes(oracle_lib):
+    """A connectivity call after tioga_reduce_fringes_ (the shells moved in
+    between) equals a fresh run: the holes the reduction made are undone."""
+    import copy
+    import ctypes as C
+    from tioga_b200.capi import TiogaLibrary
+    system = cases.config0(0)
+    moved = copy.deepcopy(system)
+    moved.blocks[1].x[:] = moved.blocks[1].x + np.array([0.031, -0.017, 0.022])
+    t = TiogaLibrary(tb.library_path())
+    t.init()
+    t.register_system(copy.deepcopy(system))
+    t.setnfringe(3)
+    t.preprocess_grids()
+    t.performconnectivity()
+    t.lib.tioga_reduce_fringes_()
+    for b in moved.blocks:
+        t.blocks[b.tag]["x"][:] = b.x.reshape(-1)
+    t.preprocess_grids()
+    t.performconnectivity()
+    got = {"iblank": {b.tag: t.iblank(b.tag).copy() for b in moved.blocks},
+           "donors": {b.tag: t.getdonorinfo(b.tag) for b in moved.blocks}, "q": {}}
+    cells = {}
+    for b in moved.blocks:
+        c = np.zeros(b.ncells, np.int32)
+        t.lib.tioga_b200_getcelliblank_(C.byref(C.c_int(b.tag)), c.ctypes.data_as(C.c_void_p))
+        cells[b.tag] = c
+    t.delete()
+    ref = run_system(oracle_lib, moved, nfringe=3)
+    problems = diff_runs(moved, ref, got)
+    assert not problems, "\n".join(problems)
+    # cell iblanks of the new call, from its node iblanks (getCellIblanks,
+    # highOrder.C:88-150): nothing left over from the reduction
+    for b in moved.blocks:
+        ib = got["iblank"][b.tag]
+        want = []
+        for nv, conn in b.cells:
+            v = ib[conn]
+            want.append(np.where((v == 0).any(axis=1), 0, np.where((v == -1).all(axis=1), -1, 1)))
+        np.testing.assert_array_equal(cells[b.tag], np.concatenate(want))

@@ -222,7 +222,9 @@ void tioga_b200_highorder_stats_(long long out[8]) {
   out[6] = s.ncand;
   out[7] = s.nrefine;
 }
-void tioga_reduce_fringes_(void) { unsupported("tioga_reduce_fringes_"); }
+void tioga_reduce_fringes_(void) {
+  if (ready("tioga_reduce_fringes_")) set_rc(g_tg->reduce_fringes());
+}
 void tioga_writeoutputfiles_(int*, char*) { unsupported("tioga_writeoutputfiles_"); }
 
 int tioga_b200_last_error(void) { return g_err; }

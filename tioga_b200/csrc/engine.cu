@@ -54,6 +54,7 @@ Engine::~Engine() {
   qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
   d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
+  rf_red_.release(); rf_tmp_.release(); rf_was_.release();
   d_wall_.release(); wall_cells_.release(); wall_box_.release(); wall_box_first_.release();
   cg_cnt_.release(); cg_off_.release(); cg_v0_.release(); cg_v1_.release(); cg_k0_.release(); cg_k1_.release();
   cg_flag_.release();
@@ -1469,6 +1470,57 @@ int Engine::run_donors() {
   k_donor_clear<<<grid_for(std::max<long long>(nq_, 1), kT), kT, 0, stream_>>>(
       qnode_.p, qdon_.p, qcell_.p, nq_, K_, d_bi_.p, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
   TB_LAUNCHED("k_donor_clear");
+  return 0;
+}
+
+// tioga_reduce_fringes_ (tioga.C:737-885): on the last connectivity call's
+// results; the cell iblanks are left as that call computed them, as the
+// reference does
+int Engine::reduce_fringes() {
+  if (!connected_) {
+    fprintf(stderr, "#tioga_b200: reduce_fringes needs performconnectivity first\n");
+    return -1;
+  }
+  TB_CUDA(rf_red_.ensure(std::max(1ll, ntot_)));
+  TB_CUDA(rf_tmp_.ensure(std::max(1ll, ntot_)));
+  TB_CUDA(rf_was_.ensure(std::max(1ll, nrec_)));
+  k_rf_init<<<grid_for(std::max(1ll, ntot_), kT), kT, 0, stream_>>>(iblank_.p, ntot_, rf_red_.p, rf_tmp_.p);
+  TB_LAUNCHED("k_rf_init");
+  TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
+  if (nrec_ > 0) {
+    int layers = 0;
+    for (const BlockInfo& B : bi_) layers = std::max(layers, B.nfringe + 1);
+    for (int it = 0; it < layers; it++) {
+      k_rf_layer<<<148 * 16, kT, 0, stream_>>>(it, it_rec_.p, it_cancel_.p, rcount_.p, csr_off_.p, csr_cell_.p,
+                                               conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p, iblank_.p, rf_red_.p,
+                                               rf_tmp_.p);
+      TB_LAUNCHED("k_rf_layer");
+      k_rf_copy<<<grid_for(nrec_, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, rf_tmp_.p, rf_red_.p);
+      TB_LAUNCHED("k_rf_copy");
+    }
+    k_rf_cancel<<<grid_for(nrec_, kT), kT, 0, stream_>>>(it_rec_.p, rcount_.p, rf_red_.p, it_cancel_.p, rf_was_.p);
+    TB_LAUNCHED("k_rf_cancel");
+    if (dedup_ran_) {  // resetCoincident (bookKeeping.C:572-597) again
+      k_fill_int<<<grid_for(nq_, kT), kT, 0, stream_>>>(dd_ireset_.p, 1, nq_);
+      TB_LAUNCHED("k_fill_int");
+      k_reset_coincident_min<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, q_xt_.p, nq_, it_cancel_.p,
+                                                                    dd_ireset_.p);
+      TB_LAUNCHED("k_reset_coincident_min");
+      k_reset_coincident_set<<<grid_for(nq_, kT), kT, 0, stream_>>>(interp2rec_.p, q_xt_.p, nq_, dd_ireset_.p,
+                                                                    it_cancel_.p);
+      TB_LAUNCHED("k_reset_coincident_set");
+    }
+    k_rf_iblank<<<grid_for(nrec_, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rf_was_.p, rcount_.p, rf_red_.p,
+                                                         iblank_.p, counters_.p);
+    TB_LAUNCHED("k_rf_iblank");
+  }
+  TB_TRY(download_iblank());
+  unsigned long long cnt[16];
+  TB_CUDA(cudaMemcpyAsync(cnt, counters_.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  stats_.nreceptor = (long long)cnt[5];
+  stats_.nhole += (long long)cnt[4];
+  interps_fetched_ = false;
   return 0;
 }
 

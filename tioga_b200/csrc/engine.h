@@ -274,6 +274,9 @@ class Engine {
   // calls (coordinate descent, one knob after the other) and keeps the
   // fastest; needs a preprocessed instance
   int autotune(int reps);
+  // tioga_reduce_fringes_: keep the receptors within nfringe+1 layers of the
+  // field, hole the others (after connectivity)
+  int reduce_fringes();
   const Tuning& tuning() const { return tune_; }
   int dataupdate(int nvar, int interptype);
 
@@ -452,6 +455,8 @@ class Engine {
   DBuf<int> it_don_;        // donor block per record
   DBuf<unsigned char> it_nv_, it_cancel_;
   DBuf<double> rres_;       // receptor resolution per record
+  DBuf<int> rf_red_, rf_tmp_;        // reduce_fringes: reduced iblank and its next layer, per node
+  DBuf<unsigned char> rf_was_;      // reduce_fringes: records live before it
   long long nrec_ = 0;
   // data update
   DBuf<double> q_, qvals_;

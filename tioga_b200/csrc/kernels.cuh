@@ -225,6 +225,16 @@ __global__ void k_iblank_final(const int* it_rec, const unsigned char* it_cancel
 __global__ void k_donor_clear(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,
                               const BlockInfo* bi, int* slot, const int* cmlist, const int* dcnt, int* cmark,
                               int* reset_t);
+__global__ void k_rf_init(const int* iblank, long long n, int* red, int* tmp);
+__global__ void k_rf_layer(int iter, const int* it_rec, const unsigned char* it_cancel, const int* rcount,
+                           const int* csr_off, const int* csr_cell, const int* conn8, const unsigned char* cell_nv,
+                           const blk_t* cell_blk, const BlockInfo* bi, const int* iblank, const int* red, int* tmp);
+__global__ void k_rf_copy(const int* it_rec, const unsigned char* it_cancel, const int* rcount, const int* tmp,
+                          int* red);
+__global__ void k_rf_cancel(const int* it_rec, const int* rcount, const int* red, unsigned char* it_cancel,
+                            unsigned char* was);
+__global__ void k_rf_iblank(const int* it_rec, const unsigned char* it_cancel, const unsigned char* was,
+                            const int* rcount, const int* red, int* iblank, unsigned long long* counters);
 __global__ void k_cell_iblank_sparse(const int* mlist, const int* dcnt, const int* it_rec,
                                      const unsigned char* it_cancel, const int* rcount, const int* csr_off,
                                      const int* csr_cell, const int* conn8, const unsigned char* cell_nv,

@@ -105,7 +105,7 @@ __global__ void k_donor_reset(const int* __restrict__ mlist, const int* __restri
     }
     int v = -1;  // a node that ended the previous call with iblank 0 or -1
     if (i < nh) v = mlist[i];
-    else if (i < nh + prev_R && !it_cancel[i - nh]) v = it_rec[i - nh];
+    else if (i < nh + prev_R) v = it_rec[i - nh];  // cancelled ones too (reduce_fringes may have holed them)
     if (v < 0) continue;
     if (lane == 0) iblank[v] = 1;
     for (int k = csr_off[v] + lane; k < csr_off[v + 1]; k += 32) iblank_cell[csr_cell[k]] = 1;
@@ -538,6 +538,94 @@ __global__ void k_interp_scatter(const int* __restrict__ it_rec, const unsigned 
     for (int k = 0; k < nvar; k++) {
       if (interptype == 0) qb[(long long)local * nvar + k] = vals[(long long)r * nvar + k];
       else qb[(long long)k * B.nnodes + local] = vals[(long long)r * nvar + k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tioga::reduce_fringes (tioga.C:737-885, bookKeeping.C:650-760), on the
+// records of the last connectivity call.  Only cells around a receptor node
+// can change anything (a cell only restores receptor nodes), so the layers
+// are grown over the receptors' cells.
+// ---------------------------------------------------------------------------
+__global__ void k_rf_init(const int* __restrict__ iblank, long long n, int* __restrict__ red, int* __restrict__ tmp) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int v = iblank[i] > 0 ? iblank[i] : 0;
+    red[i] = v;
+    tmp[i] = v;
+  }
+}
+
+// one layer: a cell with some but not all nodes in the reduced set (1 or
+// restored -1) restores its receptor nodes; a warp per receptor, its lanes
+// over the receptor's cells
+__global__ void k_rf_layer(int iter, const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                           const int* __restrict__ rcount, const int* __restrict__ csr_off,
+                           const int* __restrict__ csr_cell, const int* __restrict__ conn8,
+                           const unsigned char* __restrict__ cell_nv, const blk_t* __restrict__ cell_blk,
+                           const BlockInfo* __restrict__ bi, const int* __restrict__ iblank,
+                           const int* __restrict__ red, int* __restrict__ tmp) {
+  const int R = *rcount;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += nw) {
+    if (it_cancel[r]) continue;
+    const int g = it_rec[r];
+    for (int k = csr_off[g] + lane; k < csr_off[g + 1]; k += 32) {
+      const int c = csr_cell[k];
+      if (iter >= bi[cell_blk[c]].nfringe + 1) continue;
+      const int nv = cell_nv[c];
+      const int* cv = conn8 + 8 * (long long)c;
+      int ncount = 0;
+      for (int m = 0; m < nv; m++) {
+        const int v = red[cv[m]];
+        ncount += (v == 1 || v < 0);
+      }
+      if (ncount > 0 && ncount < nv)
+        for (int m = 0; m < nv; m++) {
+          const int v = cv[m];
+          if (tmp[v] == 0 && iblank[v] < 0) tmp[v] = iblank[v];  // every writer writes the same value
+        }
+    }
+  }
+}
+
+__global__ void k_rf_copy(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                          const int* __restrict__ rcount, const int* __restrict__ tmp, int* __restrict__ red) {
+  const int R = *rcount;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x)
+    if (!it_cancel[r]) red[it_rec[r]] = tmp[it_rec[r]];
+}
+
+// receptors outside the reduced set cancel the interpolation of the head of
+// their donor list, which is their own record (getCancellationData,
+// cancelDonor); `was` keeps which records were live before
+__global__ void k_rf_cancel(const int* __restrict__ it_rec, const int* __restrict__ rcount, const int* __restrict__ red,
+                            unsigned char* __restrict__ it_cancel, unsigned char* __restrict__ was) {
+  const int R = *rcount;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    was[r] = !it_cancel[r];
+    if (!it_cancel[r] && red[it_rec[r]] == 0) it_cancel[r] = 1;
+  }
+}
+
+// clearIblanks + setIblanks (bookKeeping.C:615-648): the receptors of the
+// live records become -1 if their record survived, else 0 when outside the
+// reduced set (1 otherwise); holes stay 0
+__global__ void k_rf_iblank(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
+                            const unsigned char* __restrict__ was, const int* __restrict__ rcount,
+                            const int* __restrict__ red, int* __restrict__ iblank,
+                            unsigned long long* __restrict__ counters) {
+  const int R = *rcount;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    if (!was[r]) continue;
+    const int g = it_rec[r];
+    if (!it_cancel[r]) {
+      iblank[g] = -1;
+      atomicAdd(&counters[5], 1ull);
+    } else {
+      iblank[g] = red[g] == 0 ? 0 : 1;
+      if (red[g] == 0) atomicAdd(&counters[4], 1ull);
     }
   }
 }
