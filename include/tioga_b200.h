@@ -97,11 +97,17 @@ void tioga_set_highorder_callback_(void (*f1)(int *, int *), void (*f2)(int *, i
  * connectivity call left them, as in TIOGA. */
 void tioga_reduce_fringes_(void);
 
-/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
- * p4est, Tecplot output).  They are exported so that existing solvers link;
- * each reports "not supported" and sets the last error. */
-void tioga_performconnectivity_amr_(void);
+/* tiogaInterface.C:226-243 -- one Tecplot file per block, flowNNNNN.dat by
+ * block index (tioga.C:526-531, MeshBlock.C:510-635): coordinates, iblank,
+ * mesh tag and the registered solution per node, then the cells as bricks
+ * and the wall and overset-boundary node lists; same formats as TIOGA.
+ * Every block's solution must be registered. */
 void tioga_writeoutputfiles_(int *nvar, char *itype);
+
+/* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
+ * p4est).  They are exported so that existing solvers link; each reports
+ * "not supported" and sets the last error. */
+void tioga_performconnectivity_amr_(void);
 
 /* ---- additions of this library (no counterpart in TIOGA) -------------- */
 

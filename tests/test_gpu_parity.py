@@ -8,6 +8,8 @@ reference's operation order, compiled without FMA contraction).  The only
 allowed difference is a donor that depends on the reference's tree visiting
 order (several cells accept the point, or a point on the face of a no-donor
 cell); the library counts those, and these inputs have none."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -313,3 +315,40 @@ def test_connectivity_after_reduce_fringes(oracle_lib):
             v = ib[conn]
             want.append(np.where((v == 0).any(axis=1), 0, np.where((v == -1).all(axis=1), -1, 1)))
         np.testing.assert_array_equal(cells[b.tag], np.concatenate(want))
+
+
+@pytest.mark.parametrize("itype", ["row", "column"])
+def test_writeoutputfiles_match_reference(itype, tmp_path, monkeypatch):
+    """tioga_writeoutputfiles_ after the data update: the same flow files, byte
+    for byte, as the compiled reference writes (tioga.C:526-531,
+    MeshBlock.C:510-635)."""
+    import os
+    from tioga_b200.capi import TiogaLibrary
+    from tests.conftest import REF_LIB
+    if not os.path.exists(REF_LIB):
+        pytest.skip("the compiled reference is not built here")
+    system = cases.small_config1(1)
+    q = cases.fields(system, nvar=3, seed=41)
+    if itype == "column":
+        q = [a.reshape(-1, 3).T.copy().reshape(-1) for a in q]
+    files = {}
+    for name, path in (("ref", REF_LIB), ("gpu", tb.library_path())):
+        d = tmp_path / name
+        d.mkdir()
+        monkeypatch.chdir(d)
+        t = TiogaLibrary(path)
+        t.init()
+        t.register_system(system)
+        t.preprocess_grids()
+        t.performconnectivity()
+        qs = [a.copy() for a in q]
+        for b, a in zip(system.blocks, qs):
+            t.registersolution(b.tag, a)
+        t.dataupdate_mb(3, itype)
+        s = C.create_string_buffer(itype.encode())
+        t.lib.tioga_writeoutputfiles_(C.byref(C.c_int(3)), s)
+        t.delete()
+        files[name] = {p.name: p.read_bytes() for p in sorted(d.iterdir())}
+    assert sorted(files["gpu"]) == sorted(files["ref"]) == [f"flow{i:05d}.dat" for i in range(len(system.blocks))]
+    for f in files["ref"]:
+        assert files["gpu"][f] == files["ref"][f], f

@@ -225,7 +225,17 @@ void tioga_b200_highorder_stats_(long long out[8]) {
 void tioga_reduce_fringes_(void) {
   if (ready("tioga_reduce_fringes_")) set_rc(g_tg->reduce_fringes());
 }
-void tioga_writeoutputfiles_(int*, char*) { unsupported("tioga_writeoutputfiles_"); }
+void tioga_writeoutputfiles_(int* nvar, char* itype) {
+  if (!ready("tioga_writeoutputfiles_")) return;
+  int t;
+  if (strstr(itype, "row")) t = 0;
+  else if (strstr(itype, "column")) t = 1;
+  else {
+    printf("#tiogaInterface.C:dataupdate_:unknown data orientation\n");
+    return;
+  }
+  set_rc(g_tg->write_output(*nvar, t));
+}
 
 int tioga_b200_last_error(void) { return g_err; }
 int tioga_b200_device_ok(void) { return device_ok() ? 1 : 0; }

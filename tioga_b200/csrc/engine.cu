@@ -1473,6 +1473,80 @@ int Engine::run_donors() {
   return 0;
 }
 
+// tioga_writeoutputfiles_ -> tioga::writeData (tioga.C:526-531) ->
+// MeshBlock::writeFlowFile (MeshBlock.C:510-635): one Tecplot FEPOINT file
+// per block, flow%05d.dat by block index, with the same fields and formats
+// (coordinates, iblank, mesh tag, the registered solution, bricks, wall and
+// overset-boundary node lists), written from the caller's arrays.
+int Engine::write_output(int nvar, int interptype) {
+  if (!connected_) {
+    fprintf(stderr, "#tioga_b200: writeoutputfiles needs performconnectivity first\n");
+    return -1;
+  }
+  for (size_t ib = 0; ib < hb_.size(); ib++) {
+    const HostBlock& H = hb_[ib];
+    if (!H.hq && !H.dq) {
+      fprintf(stderr, "#tioga_b200: writeoutputfiles: block %d has no registered solution\n", H.tag);
+      return -1;
+    }
+    std::vector<int> ibl_h;
+    const int* ibl = H.hibl;
+    if (H.dibl) {
+      ibl_h.resize(H.nnodes);
+      TB_CUDA(cudaMemcpyAsync(ibl_h.data(), H.dibl, H.nnodes * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+      ibl = ibl_h.data();
+    }
+    std::vector<double> q_h;
+    const double* q = H.hq;
+    if (!q) {
+      q_h.resize((size_t)H.nnodes * nvar);
+      TB_CUDA(cudaMemcpyAsync(q_h.data(), H.dq, q_h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      q = q_h.data();
+    }
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    char intstring[16], fname[32];
+    snprintf(intstring, sizeof(intstring), "%d", 100000 + (int)ib);
+    snprintf(fname, sizeof(fname), "flow%s.dat", intstring + 1);
+    FILE* fp = fopen(fname, "w");
+    if (!fp) {
+      fprintf(stderr, "#tioga_b200: writeoutputfiles: cannot open %s\n", fname);
+      return -1;
+    }
+    fprintf(fp, "TITLE =\"Tioga output\"\n");
+    fprintf(fp, "VARIABLES=\"X\",\"Y\",\"Z\",\"IBLANK\",\"BTAG\" ");
+    for (int i = 0; i < nvar; i++) fprintf(fp, "\"Q%d\",", i);
+    fprintf(fp, "\n");
+    fprintf(fp, "ZONE T=\"VOL_MIXED\",N=%d E=%d ET=BRICK, F=FEPOINT\n", H.nnodes, H.ncells);
+    for (int i = 0; i < H.nnodes; i++) {
+      fprintf(fp, "%lf %lf %lf %d %d ", H.hx[3 * i], H.hx[3 * i + 1], H.hx[3 * i + 2], ibl[i], H.tag);
+      for (int j = 0; j < nvar; j++)
+        fprintf(fp, "%lf ", interptype == 0 ? q[(size_t)i * nvar + j] : q[(size_t)j * H.nnodes + i]);
+      fprintf(fp, "\n");
+    }
+    // bricks: tets, pyramids and prisms with repeated corners (1-based as given)
+    static const int kBrick[4][8] = {{0, 1, 2, 2, 3, 3, 3, 3},   // 4 vertices
+                                     {0, 1, 2, 3, 4, 4, 4, 4},   // 5
+                                     {0, 1, 2, 2, 3, 4, 5, 5},   // 6
+                                     {0, 1, 2, 3, 4, 5, 6, 7}};  // 8
+    for (int n = 0; n < H.ntypes; n++) {
+      const int nvert = H.nv[n];
+      const int* pat = kBrick[nvert == 4 ? 0 : nvert == 5 ? 1 : nvert == 6 ? 2 : 3];
+      const int* cv = H.hconn[n];
+      for (int i = 0; i < H.nc[n]; i++) {
+        const int* c = cv + (size_t)nvert * i;
+        fprintf(fp, "%d %d %d %d %d %d %d %d\n", c[pat[0]], c[pat[1]], c[pat[2]], c[pat[3]], c[pat[4]], c[pat[5]],
+                c[pat[6]], c[pat[7]]);
+      }
+    }
+    fprintf(fp, "%d\n", H.nwbc);
+    for (int i = 0; i < H.nwbc; i++) fprintf(fp, "%d\n", H.hwbc[i]);
+    fprintf(fp, "%d\n", H.nobc);
+    for (int i = 0; i < H.nobc; i++) fprintf(fp, "%d\n", H.hobc[i]);
+    fclose(fp);
+  }
+  return 0;
+}
+
 // tioga_reduce_fringes_ (tioga.C:737-885): on the last connectivity call's
 // results; the cell iblanks are left as that call computed them, as the
 // reference does

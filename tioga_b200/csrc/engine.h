@@ -277,6 +277,8 @@ class Engine {
   // tioga_reduce_fringes_: keep the receptors within nfringe+1 layers of the
   // field, hole the others (after connectivity)
   int reduce_fringes();
+  // tioga_writeoutputfiles_: the Tecplot flow files of every block
+  int write_output(int nvar, int interptype);
   const Tuning& tuning() const { return tune_; }
   int dataupdate(int nvar, int interptype);
 
