@@ -311,22 +311,22 @@ __global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __r
     __syncthreads();
     bit_transpose(pr, n1, pc, n0);
     __syncthreads();
-    int rounds = 0;
-    const int max_rounds = n0 * n1 + 2;
-    for (;;) {
+    // rows, then columns, alternately: every run of passable cells that holds
+    // a filled cell fills.  A pass that changes nothing ends the fill (the
+    // state is then a fixed point of both, a fill being idempotent); the
+    // row masks hold the state when it ends.
+    for (int rounds = 0;; rounds++) {
       bool ch = false;
-      // rows, then columns: every run of passable cells that holds a filled
-      // cell fills
       for (int r = threadIdx.x; r < n1; r += blockDim.x) ch = line_fill(fr[r], pr[r]) || ch;
-      __syncthreads();
+      if (!__syncthreads_or(ch) && rounds > 0) break;
       bit_transpose(fr, n1, fc, n0);
       __syncthreads();
+      ch = false;
       for (int c = threadIdx.x; c < n0; c += blockDim.x) ch = line_fill(fc[c], pc[c]) || ch;
-      __syncthreads();
+      if (!__syncthreads_or(ch)) break;  // fr already holds this state
       bit_transpose(fc, n0, fr, n1);
-      const int any = __syncthreads_or(ch);
-      if (!any) break;
-      if (++rounds > max_rounds) {
+      __syncthreads();
+      if (rounds > n0 * n1 + 2) {
         if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
         break;
       }
