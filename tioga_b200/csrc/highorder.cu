@@ -125,7 +125,7 @@ __global__ void k_ho_candidates(const double* __restrict__ pts, const double* __
     bool pass = false;
     if (screen != 0) {
       double u[3];
-      pass = ho_invert(h.p, X, xp, u) && ho_inside(u);
+      pass = ho_invert_any(h.p, X, xp, u) && ho_inside(u);
       atomicAdd(&counters[9], 1ull);
     }
     atomicAdd(&counters[10], 1ull);
@@ -186,8 +186,8 @@ __global__ void k_ho_records(const int* __restrict__ flag, const int* __restrict
     rec[r] = make_int4(qrec[q], qloc[q], a, c);
     const HoDev h = hd[a];
     double u[3];
-    ho_invert(h.p, xdof + 3 * (h.dof_off + (long long)c * h.npts), pts + 3ll * qpt[q], u);
-    ho_weights(h.p, u, w + r * wstride);
+    ho_invert_any(h.p, xdof + 3 * (h.dof_off + (long long)c * h.npts), pts + 3ll * qpt[q], u);
+    ho_weights_any(h.p, u, w + r * wstride);
   }
 }
 

@@ -108,6 +108,125 @@ __device__ inline void ho_weights(int p, const double u[3], double* w) {
       for (int i = 0; i < n1; i++, m++) w[m] = (lr[i] * ls[j]) * lt[k];
 }
 
+// The same three functions for a degree known at compile time: the loops
+// unroll and the basis values stay in registers.  Every operation is the one
+// of the generic form above, in the same order (a constant divisor is still
+// an IEEE division), so the results are the same bits.
+template <int P>
+__device__ __forceinline__ void ho_basis1_t(double r, double* l, double* dl) {
+#pragma unroll
+  for (int i = 0; i <= P; i++) {
+    const double xi = (double)i / P;
+    double v = 1.0, d = 0.0;
+#pragma unroll
+    for (int m = 0; m <= P; m++) {
+      if (m == i) continue;
+      const double xm = (double)m / P;
+      const double den = xi - xm;
+      d = d * ((r - xm) / den) + v / den;
+      v = v * ((r - xm) / den);
+    }
+    l[i] = v;
+    dl[i] = d;
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void ho_map_t(const double* __restrict__ X, const double u[3], double x[3],
+                                         double J[3][3]) {
+  constexpr int n1 = P + 1;
+  double lr[n1], ls[n1], lt[n1], dr[n1], ds[n1], dt[n1];
+  ho_basis1_t<P>(u[0], lr, dr);
+  ho_basis1_t<P>(u[1], ls, ds);
+  ho_basis1_t<P>(u[2], lt, dt);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    x[a] = 0.0;
+    J[a][0] = J[a][1] = J[a][2] = 0.0;
+  }
+#pragma unroll 1
+  for (int k = 0; k < n1; k++)
+#pragma unroll 1
+    for (int j = 0; j < n1; j++) {
+      const double lsj = ls[j], dsj = ds[j], ltk = lt[k], dtk = dt[k];
+      const double* Pj = X + 3 * ((k * n1 + j) * n1);
+#pragma unroll
+      for (int i = 0; i < n1; i++) {
+        const double* Pp = Pj + 3 * i;
+        const double w = (lr[i] * lsj) * ltk;
+        const double wr = (dr[i] * lsj) * ltk;
+        const double ws = (lr[i] * dsj) * ltk;
+        const double wt = (lr[i] * lsj) * dtk;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          x[a] = x[a] + w * Pp[a];
+          J[a][0] = J[a][0] + wr * Pp[a];
+          J[a][1] = J[a][1] + ws * Pp[a];
+          J[a][2] = J[a][2] + wt * Pp[a];
+        }
+      }
+    }
+}
+
+template <int P>
+__device__ inline bool ho_invert_t(const double* __restrict__ X, const double* xp, double u[3]) {
+  u[0] = u[1] = u[2] = 0.5;
+  for (int it = 0; it < 50; it++) {
+    double x[3], J[3][3];
+    ho_map_t<P>(X, u, x, J);
+    const double f0 = xp[0] - x[0], f1 = xp[1] - x[1], f2 = xp[2] - x[2];
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    if (!(fabs(det) > 1e-300)) return false;
+    const double d0 = (f0 * c00 + f1 * (J[0][2] * J[2][1] - J[0][1] * J[2][2]) +
+                       f2 * (J[0][1] * J[1][2] - J[0][2] * J[1][1])) / det;
+    const double d1 = (f0 * c01 + f1 * (J[0][0] * J[2][2] - J[0][2] * J[2][0]) +
+                       f2 * (J[0][2] * J[1][0] - J[0][0] * J[1][2])) / det;
+    const double d2 = (f0 * c02 + f1 * (J[0][1] * J[2][0] - J[0][0] * J[2][1]) +
+                       f2 * (J[0][0] * J[1][1] - J[0][1] * J[1][0])) / det;
+    u[0] = u[0] + d0;
+    u[1] = u[1] + d1;
+    u[2] = u[2] + d2;
+    if (fabs(d0) + fabs(d1) + fabs(d2) < 1e-14) return true;
+  }
+  return false;
+}
+
+template <int P>
+__device__ __forceinline__ void ho_weights_t(const double u[3], double* w) {
+  constexpr int n1 = P + 1;
+  double lr[n1], ls[n1], lt[n1], d[n1];
+  ho_basis1_t<P>(u[0], lr, d);
+  ho_basis1_t<P>(u[1], ls, d);
+  ho_basis1_t<P>(u[2], lt, d);
+#pragma unroll
+  for (int k = 0; k < n1; k++)
+#pragma unroll
+    for (int j = 0; j < n1; j++)
+#pragma unroll
+      for (int i = 0; i < n1; i++) w[(k * n1 + j) * n1 + i] = (lr[i] * ls[j]) * lt[k];
+}
+
+// degree dispatch: the common degrees take the unrolled forms
+__device__ inline bool ho_invert_any(int p, const double* __restrict__ X, const double* xp, double u[3]) {
+  switch (p) {
+    case 1: return ho_invert_t<1>(X, xp, u);
+    case 2: return ho_invert_t<2>(X, xp, u);
+    case 3: return ho_invert_t<3>(X, xp, u);
+    default: return ho_invert(p, X, xp, u);
+  }
+}
+__device__ inline void ho_weights_any(int p, const double u[3], double* w) {
+  switch (p) {
+    case 1: ho_weights_t<1>(u, w); break;
+    case 2: ho_weights_t<2>(u, w); break;
+    case 3: ho_weights_t<3>(u, w); break;
+    default: ho_weights(p, u, w);
+  }
+}
+
 // FP32 screen of the inclusion test for the split-precision form: Newton on
 // the element map in FP32, on offsets from the element's first DOF (so the
 // coordinates' common part does not cost precision).  Returns 1 when it
