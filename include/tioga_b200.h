@@ -202,8 +202,9 @@ int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[6], long
 void tioga_b200_server_stats(void *srv, long long out[16]);
 
 /* Autotuner: after tioga_preprocess_grids_, times every launch shape of the
- * tuned kernels (CTAs per SM of the cell pass, the query gathering, the
- * traversal and the candidate screen; pairs per cell-pass CTA) over *reps
+ * tuned kernels (CTAs per SM of the cell pass, with its register budget cut
+ * to match; of the query gathering, the traversal and the candidate
+ * screen; pairs per cell-pass CTA) over *reps
  * connectivity calls each, one knob after the other, and keeps the fastest
  * for the instance's later calls.  The results of a call do not depend on
  * the shapes; the instance ends with a connectivity call's results. */

@@ -937,7 +937,7 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(d_chunk_cta_.p, ccta.data(), ccta.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
   TB_CUDA(cudaEventRecord(cev_[0], stream_));
   const size_t smem = (size_t)maxnp * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
-  launch_cell_pass(fp64, ccta.back(), smem, stream_, x_.p, xf_.p, conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p,
+  launch_cell_pass(fp64, tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, xf_.p, conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p,
                    d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
                    fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, pair_acc_.p);
   TB_LAUNCHED("k_cell_pass");
@@ -1640,7 +1640,7 @@ int Engine::autotune(int reps) {
     float Timing::*phase;
   };
   const Knob knobs[] = {
-      {&tune_.cell_pass_per_sm, {1, 2, 3, 4, 6}, &Timing::cell_pass},
+      {&tune_.cell_pass_per_sm, {2, 3, 4}, &Timing::cell_pass},
       {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
       {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
       {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},

@@ -100,7 +100,7 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
                         int* pfirst);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
+void launch_cell_pass(bool f64, int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
                       const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
                       const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
                       const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,

@@ -662,8 +662,8 @@ __device__ __forceinline__ void proj_bounds(const double cc[3], const double o[3
 // z .. z+w-1: all the pairs whose donor is one of the chunk's blocks, as the
 // pairs are sorted by donor); CTAs chunk_cta[k] .. chunk_cta[k+1]-1 share
 // chunk k, whose pairs sit in their shared memory.
-template <bool F64>
-__global__ void __launch_bounds__(256, 3) k_cell_pass(
+template <bool F64, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_pass(
     const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
     const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves,
     const int4* __restrict__ chunks, const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
@@ -961,17 +961,36 @@ __global__ void __launch_bounds__(256, 3) k_cell_pass(
   }
 }
 
-void launch_cell_pass(bool f64, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
+// minb: CTAs per SM the kernel's register budget is cut for (2, 3 or 4;
+// more CTAs hide more gather latency, fewer keep more values in registers)
+template <bool F64>
+static void launch_cell_pass_t(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
+                               const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
+                               const int4* leaves, const int4* chunks, const int* chunk_cta, int nchunks,
+                               const int* pfirst, const PairInfo* pairs, float4* cbox, double* cbox64,
+                               float4* tnode, double* tnode64, unsigned long long* acc) {
+  if (minb <= 2)
+    k_cell_pass<F64, 2><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
+                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
+  else if (minb == 3)
+    k_cell_pass<F64, 3><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
+                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
+  else
+    k_cell_pass<F64, 4><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
+                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
+}
+
+void launch_cell_pass(bool f64, int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
                       const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
                       const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
                       const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
                       unsigned long long* acc) {
   if (f64)
-    k_cell_pass<true><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
-                                               pairs, cbox, cbox64, tnode, tnode64, acc);
+    launch_cell_pass_t<true>(minb, grid, smem, st, x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
+                             pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
   else
-    k_cell_pass<false><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
-                                                pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
+    launch_cell_pass_t<false>(minb, grid, smem, st, x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
+                              pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
 }
 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
