@@ -49,9 +49,10 @@ REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 # DRAM bytes (read + write) of one cell-pass launch on the full workload, from
 # an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of
-# `bench.py --forms split --steps 1 --warmup 1 --no-cpu-baseline`: 1,489,302,528
-# read + 959,081,984 written over 26,961,129 cells; other sizes scale by cells.
-CELL_PASS_DRAM_BYTES_PER_CELL = (1489302528 + 959081984) / 26961129
+# `bench.py --forms split --no-tune --no-forms --steps 1 --warmup 1
+# --no-cpu-baseline`: 1,495,505,408 read + 956,761,856 written over 26,961,129
+# cells; other sizes scale by cells.
+CELL_PASS_DRAM_BYTES_PER_CELL = (1495505408 + 956761856) / 26961129
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
