@@ -776,11 +776,8 @@ int Engine::run_holemaps() {
   TB_CUDA(cudaMemcpyAsync(wall_bb_.p, init.data(), init.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
   const unsigned nw = (unsigned)h_wall_.size();
-  int maxw = 1, maxc = 1;
-  for (const WallBlock& W : h_wall_) {
-    maxw = std::max(maxw, W.nwall);
-    maxc = std::max(maxc, W.ncells);
-  }
+  int maxw = 1;
+  for (const WallBlock& W : h_wall_) maxw = std::max(maxw, W.nwall);
   k_wall_bounds<<<dim3(grid_for(maxw, kT, 148), nw), kT, 0, stream_>>>(x_.p, wall_list_.p, d_wall_.p, wall_bb_.p);
   TB_LAUNCHED("k_wall_bounds");
   k_holemap_setup<<<(nh + 127) / 128, 128, 0, stream_>>>(wall_bb_.p, d_hm_.p, nh);
@@ -1367,14 +1364,14 @@ int Engine::run_donors() {
                                                         d_bi_.p, (int)hb_.size(), slot_.p, err_.p);
     TB_LAUNCHED("k_fill_slots");
     k_classify_queried<<<grid_for(nq_, kT), kT, 0, stream_>>>(x_.p, node_blk_.p, d_bi_.p, slot_.p, K_, qnode_.p,
-                                                              qcell_.p, nq_, qres_.p, d_hmdev_.p, nhm_, iblank_.p,
+                                                              qcell_.p, nq_, qres_.p, d_hmdev_.p, iblank_.p,
                                                               node_res_.p, m0_.p, m1_.p, mlist_.p, dcnt_.p,
                                                               counters_.p);
     TB_LAUNCHED("k_classify_queried");
   }
   if (nhm_ > 0 && h_tile_base_.back() > 0) {
     k_classify_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(
-        x_.p, d_bi_.p, (int)hb_.size(), tile_base_.p, tbox_.p, node_order_.p, slot_.p, K_, d_hmdev_.p, nhm_,
+        x_.p, d_bi_.p, (int)hb_.size(), tile_base_.p, tbox_.p, node_order_.p, slot_.p, K_, d_hmdev_.p,
         iblank_.p, m0_.p, m1_.p, mlist_.p, dcnt_.p, counters_.p);
     TB_LAUNCHED("k_classify_tiles");
   }

@@ -162,11 +162,11 @@ __global__ void k_donor_reset(const int* mlist, const int* dcnt, const int* it_r
                               int* m1, int* iblank_cell);
 __global__ void k_classify_queried(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                    const int* slot, int K, const int* qnode, const int* qcell, long long nq,
-                                   const double* qres, const HoleMapDev* hm, int nhm, int* iblank, double* node_res,
+                                   const double* qres, const HoleMapDev* hm, int* iblank, double* node_res,
                                    unsigned char* m0, int* m1, int* mlist, int* dcnt, unsigned long long* counters);
 __global__ void k_classify_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
                                  const float4* tbox, const int* node_order, const int* slot, int K,
-                                 const HoleMapDev* hm, int nhm, int* iblank, unsigned char* m0, int* m1, int* mlist,
+                                 const HoleMapDev* hm, int* iblank, unsigned char* m0, int* m1, int* mlist,
                                  int* dcnt, unsigned long long* counters);
 __global__ void k_front_init(int* dcnt);
 __global__ void k_dilate_front(int iter, const int* csr_off, const int* csr_cell, const int* conn8,

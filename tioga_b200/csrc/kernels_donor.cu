@@ -119,7 +119,7 @@ __global__ void k_donor_reset(const int* __restrict__ mlist, const int* __restri
 __global__ void k_classify_queried(const double* __restrict__ x, const blk_t* __restrict__ node_blk,
                                    const BlockInfo* __restrict__ bi, const int* __restrict__ slot, int K,
                                    const int* __restrict__ qnode, const int* __restrict__ qcell, long long nq,
-                                   const double* __restrict__ qres, const HoleMapDev* __restrict__ hm, int nhm,
+                                   const double* __restrict__ qres, const HoleMapDev* __restrict__ hm,
                                    int* __restrict__ iblank, double* __restrict__ node_res,
                                    unsigned char* __restrict__ m0, int* __restrict__ m1, int* __restrict__ mlist,
                                    int* __restrict__ dcnt, unsigned long long* __restrict__ counters) {
@@ -160,7 +160,7 @@ __global__ void k_classify_queried(const double* __restrict__ x, const blk_t* __
 __global__ void __launch_bounds__(256) k_classify_tiles(
     const double* __restrict__ x, const BlockInfo* __restrict__ bi, int nb, const long long* __restrict__ tile_base,
     const float4* __restrict__ tbox, const int* __restrict__ node_order, const int* __restrict__ slot, int K,
-    const HoleMapDev* __restrict__ hm, int nhm, int* __restrict__ iblank, unsigned char* __restrict__ m0,
+    const HoleMapDev* __restrict__ hm, int* __restrict__ iblank, unsigned char* __restrict__ m0,
     int* __restrict__ m1, int* __restrict__ mlist, int* __restrict__ dcnt, unsigned long long* __restrict__ counters) {
   __shared__ unsigned s_maps;  // foreign maps that reach the tile (bit h; all bits set past 32 maps)
   const long long T = blockIdx.x;
