@@ -80,6 +80,8 @@ def parse():
     p.add_argument("--slots", type=int, default=8, help="cfg3: concurrent requests")
     p.add_argument("--nsys", type=int, default=200, help="cfg3: systems")
     p.add_argument("--budget-gb", type=float, default=120.0, help="cfg3: HBM admission budget")
+    p.add_argument("--fields", default="host", choices=["host", "device"],
+                   help="cfg3: the requests' 5 fields in pinned host memory or on the device")
     p.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
@@ -580,15 +582,21 @@ def run_gpu_serving(args, ws, rank, local, dist):
             it = torch.ones(b.nnodes, dtype=torch.int32, pin_memory=True)
             qt = torch.empty(b.nnodes * nvar, dtype=torch.float64, pin_memory=True)
             qt.numpy()[:] = rng.uniform(-1.0, 1.0, b.nnodes * nvar)
+            if args.fields == "device":
+                qt = qt.cuda()
             keep += [xt, it, qt]
             xs.append(xt.numpy())
             ibs.append(it.numpy())
-            qs.append(qt.numpy())
+            qs.append(qt if args.fields == "device" else qt.numpy())
         pinned.append((xs, ibs, qs))
     shift = [[0.5 * wall_cell_width(b) for b in s.blocks] for s in systems]
     srv = Server(budget_bytes=int(args.budget_gb * (1 << 30)), nslots=args.slots, max_resident=200)
     for k, s in enumerate(systems):
         srv.add_system(k, s, x_arrays=pinned[k][0], ibl_arrays=pinned[k][1])
+
+    def fields(k):
+        key = "q_device" if args.fields == "device" else "q"
+        return {key: pinned[k][2], "nvar": nvar}
 
     def moves_for(k):
         s = systems[k]
@@ -598,13 +606,13 @@ def run_gpu_serving(args, ws, rank, local, dist):
 
     # admission: one step of every system (topology upload, trees, hole maps)
     t0 = time.perf_counter()
-    ts = [srv.submit(k, moves_for(k), q=pinned[k][2], nvar=nvar) for k in range(len(systems))]
+    ts = [srv.submit(k, moves_for(k), **fields(k)) for k in range(len(systems))]
     first = [srv.wait(t) for t in ts]
     admit_s = time.perf_counter() - t0
     assert all(f["rc"] == 0 for f in first), [f for f in first if f["rc"]][:3]
     # a closed loop with all slots busy measures the capacity
     t0 = time.perf_counter()
-    ts = [srv.submit(k % len(systems), moves_for(k % len(systems)), q=pinned[k % len(systems)][2], nvar=nvar)
+    ts = [srv.submit(k % len(systems), moves_for(k % len(systems)), **fields(k % len(systems)))
           for k in range(2 * len(systems))]
     sat = [srv.wait(t) for t in ts]
     sat_s = time.perf_counter() - t0
@@ -627,7 +635,7 @@ def run_gpu_serving(args, ws, rank, local, dist):
             d = t0 + arr[i] - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            tickets.append(srv.submit(int(who[i]), mv[i], q=pinned[int(who[i])][2], nvar=nvar))
+            tickets.append(srv.submit(int(who[i]), mv[i], **fields(int(who[i]))))
         res = [srv.wait(t) for t in tickets]
         wall = time.perf_counter() - t0
         clk = clocks.stop() if ri == len(rates) - 1 else None
@@ -654,16 +662,19 @@ def run_gpu_serving(args, ws, rank, local, dist):
         "config": {"workload": WORKLOAD3.format(n=len(systems)) if args.size == "full" else
                    f"cfg3 stream, {args.size} systems", "systems": len(systems), "nodes": nodes,
                    "slots": args.slots, "budget_gb": args.budget_gb, "arrivals": "Poisson",
+                   "fields": args.fields,
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (all systems' coordinates %.0f MB)" % (24 * nodes / 1e6)},
         "latency_ms": top["latency_ms"],
         "serving": {"capacity_rps": cap, "capacity_receptors_per_s": sum(r["nquery"] for r in sat) / sat_s,
                     "admission_s": admit_s, "sweep": sweep, "server": st},
         "e2e": {"value": top["receptors_per_s"], "unit": UNIT,
-                "h2d_bytes_per_step": int(np.mean([8 * nvar * s.nnodes for s in systems])),
-                "d2h_bytes_per_step": int(np.mean([(4 + 8 * nvar) * s.nnodes for s in systems])),
-                "note": "requests through the serving C ABI with host arrays; every request uploads its "
-                        "system's fields and downloads its iblanks"},
+                "h2d_bytes_per_step": 0 if args.fields == "device" else int(np.mean([8 * nvar * s.nnodes
+                                                                                      for s in systems])),
+                "d2h_bytes_per_step": int(np.mean([(4 + (0 if args.fields == "device" else 8 * nvar)) * s.nnodes
+                                                   for s in systems])),
+                "note": "requests through the serving C ABI; every request downloads its system's iblanks "
+                        "and, with host fields, uploads its fields and downloads the interpolated values"},
         "gpu_launches": None,
         "clocks": clk,
     }

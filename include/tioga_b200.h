@@ -191,6 +191,11 @@ int tioga_b200_server_add_block(void *srv, int sys, int btag, int nnodes, double
  * for.  Returns a ticket (> 0) or -1. */
 long long tioga_b200_server_submit(void *srv, int sys, int nmoves, const int *move_tags, const double *moves,
                                    int nvar, double *const *q, int *const *ibl_out);
+/* The same with the fields on the device when q_on_device is 1 (a GPU
+ * solver's arrays, same layout): the data update then reads and writes them
+ * in place, with no host copies. */
+long long tioga_b200_server_submit_fields(void *srv, int sys, int nmoves, const int *move_tags, const double *moves,
+                                          int nvar, double *const *q, int q_on_device, int *const *ibl_out);
 /* Blocks until the request is done: times_ms = (submit -> done, submit ->
  * start, start -> done, then the host time of its preprocess, connectivity
  * and data update), counts = (query points, receptors, holes, status).

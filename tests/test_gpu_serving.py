@@ -100,3 +100,36 @@ def test_same_alone_and_in_the_mix(oracle_lib):
                "donors": ref["donors"], "q": {b.tag: q[i] for i, b in enumerate(sysm.blocks)}}
         problems = diff_runs(moved, ref, got)
         assert not problems, f"system {s}:\n" + "\n".join(problems)
+
+
+@pytest.mark.timeout(300)
+def test_device_fields_equal_host_fields():
+    """A request whose fields live on the device (a GPU solver's arrays)
+    updates them exactly as the host form updates host arrays."""
+    import torch
+    systems, steps = _workload()
+    s, sysm = 1, systems[1]
+    out = {}
+    for form in ("host", "device"):
+        srv = Server(budget_bytes=8 << 30, nslots=1)
+        srv.add_system(s, sysm)
+        res = []
+        for k in range(NSTEPS):
+            q = [a.copy() for a in _fields(sysm, s, k)]
+            ibl = [np.zeros(b.nnodes, dtype=np.int32) for b in sysm.blocks]
+            if form == "host":
+                info = srv.wait(srv.submit(s, steps[s][k], q=q, nvar=NVAR, ibl_out=ibl))
+            else:
+                dq = [torch.from_numpy(a).cuda() for a in q]
+                info = srv.wait(srv.submit(s, steps[s][k], q_device=dq, nvar=NVAR, ibl_out=ibl))
+                torch.cuda.synchronize()
+                q = [t.cpu().numpy() for t in dq]
+            assert info["rc"] == 0, info
+            res.append((ibl, q))
+        srv.close()
+        out[form] = res
+    for (ia, qa), (ib, qb) in zip(out["host"], out["device"]):
+        for a, b in zip(ia, ib):
+            assert np.array_equal(a, b)
+        for a, b in zip(qa, qb):
+            assert np.array_equal(a.view(np.int64), b.view(np.int64))

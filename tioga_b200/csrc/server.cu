@@ -55,6 +55,7 @@ struct SrvRequest {
   std::vector<double> moves;  // 12 per move: a (row-major 3x3), b
   int nvar = 0;
   std::vector<double*> q;     // per block, or empty (no data update)
+  bool q_device = false;      // q points to device arrays (a GPU solver's fields)
   std::vector<int*> ibl;      // per block iblank destination, or empty (the registered arrays)
   double t_submit = 0, t_start = 0, t_done = 0;
   double t_pre = 0, t_conn = 0, t_upd = 0;  // host time of the three calls
@@ -331,7 +332,8 @@ class Server {
     r->t_conn = now_ms() - t;
     t = now_ms();
     if (!rc && !r->q.empty()) {
-      for (size_t b = 0; b < S.blocks.size() && !rc; b++) rc = E.register_solution(S.blocks[b].tag, r->q[b], false);
+      for (size_t b = 0; b < S.blocks.size() && !rc; b++)
+        rc = E.register_solution(S.blocks[b].tag, r->q[b], r->q_device);
       if (!rc) rc = E.dataupdate(r->nvar, 0);
     }
     r->t_upd = now_ms() - t;
@@ -401,8 +403,14 @@ int tioga_b200_server_add_block(void* srv, int sys, int btag, int nnodes, double
 
 long long tioga_b200_server_submit(void* srv, int sys, int nmoves, const int* move_tags, const double* moves,
                                    int nvar, double* const* q, int* const* ibl_out) {
+  return tioga_b200_server_submit_fields(srv, sys, nmoves, move_tags, moves, nvar, q, 0, ibl_out);
+}
+
+long long tioga_b200_server_submit_fields(void* srv, int sys, int nmoves, const int* move_tags, const double* moves,
+                                          int nvar, double* const* q, int q_on_device, int* const* ibl_out) {
   if (!srv || nmoves < 0 || (nmoves > 0 && (!move_tags || !moves))) return -1;
   auto* r = new tb::SrvRequest();
+  r->q_device = q_on_device != 0;
   r->sys = sys;
   r->move_tag.assign(move_tags, move_tags + nmoves);
   r->moves.assign(moves, moves + 12 * (size_t)nmoves);

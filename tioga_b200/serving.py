@@ -57,8 +57,8 @@ class Server:
         L.tioga_b200_server_add_block.restype = C.c_int
         L.tioga_b200_server_add_block.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, _P, C.c_int, C.c_int, _P, _P,
                                                   C.c_int, _P, _P, _P]
-        L.tioga_b200_server_submit.restype = C.c_longlong
-        L.tioga_b200_server_submit.argtypes = [_P, C.c_int, C.c_int, _P, _P, C.c_int, _P, _P]
+        L.tioga_b200_server_submit_fields.restype = C.c_longlong
+        L.tioga_b200_server_submit_fields.argtypes = [_P, C.c_int, C.c_int, _P, _P, C.c_int, _P, C.c_int, _P]
         L.tioga_b200_server_wait.restype = C.c_int
         L.tioga_b200_server_wait.argtypes = [_P, C.c_longlong, _P, _P]
         L.tioga_b200_server_stats.argtypes = [_P, _P]
@@ -91,10 +91,11 @@ class Server:
                            "nnodes": b.nnodes})
         self.systems[sys_id] = blocks
 
-    def submit(self, sys_id: int, moves=(), q=None, nvar: int = 5, ibl_out=None) -> int:
+    def submit(self, sys_id: int, moves=(), q=None, nvar: int = 5, ibl_out=None, q_device=None) -> int:
         """moves: [(tag, A (3, 3), b (3,))]; q: per-block ROW solutions
         (float64, nnodes*nvar, updated in place) or None; ibl_out: per-block
-        int32 arrays for this request's iblank, or None."""
+        int32 arrays for this request's iblank, or None.  q_device: per-block
+        float64 CUDA tensors (or device pointers) instead of host q."""
         tags = np.array([m[0] for m in moves], dtype=np.int32)
         mv = np.zeros((max(len(moves), 1), 12), dtype=np.float64)
         for i, (_, A, b) in enumerate(moves):
@@ -102,7 +103,11 @@ class Server:
             mv[i, 9:] = np.asarray(b, dtype=np.float64)
         keep = [tags, mv]
         qp = None
-        if q is not None:
+        if q_device is not None:
+            ptrs = [a if isinstance(a, int) else a.data_ptr() for a in q_device]
+            qp = (_P * len(ptrs))(*ptrs)
+            keep += [qp, list(q_device)]
+        elif q is not None:
             for a in q:
                 assert a.dtype == np.float64 and a.flags.c_contiguous
             qp = (_P * len(q))(*[a.ctypes.data for a in q])
@@ -113,9 +118,10 @@ class Server:
                 assert a.dtype == np.int32 and a.flags.c_contiguous
             ip = (_P * len(ibl_out))(*[a.ctypes.data for a in ibl_out])
             keep += [ip, list(ibl_out)]
-        t = self.lib.tioga_b200_server_submit(self.h, int(sys_id), len(moves), tags.ctypes.data, mv.ctypes.data,
-                                              int(nvar), None if qp is None else C.cast(qp, _P),
-                                              None if ip is None else C.cast(ip, _P))
+        t = self.lib.tioga_b200_server_submit_fields(self.h, int(sys_id), len(moves), tags.ctypes.data,
+                                                     mv.ctypes.data, int(nvar), None if qp is None else C.cast(qp, _P),
+                                                     1 if q_device is not None else 0,
+                                                     None if ip is None else C.cast(ip, _P))
         if t <= 0:
             raise RuntimeError(f"server_submit failed for system {sys_id}")
         self._keep[t] = keep
