@@ -114,7 +114,8 @@ class Dist:
 
     def barrier(self):
         if self.pg:
-            self.pg.barrier()
+            import torch
+            self.pg.barrier(device_ids=[torch.cuda.current_device()])
 
     def max(self, v: float) -> float:
         if not self.pg:
@@ -654,8 +655,10 @@ def run_gpu_serving(args, ws, rank, local, dist):
     srv.close()
     top = sweep[-1]
     nodes = sum(s.nnodes for s in systems)
+    # on N GPUs every rank serves its own stream of requests: the rates add up
+    job_rate = dist.sum(top["receptors_per_s"])
     out = {
-        "metric": METRIC, "value": top["receptors_per_s"], "unit": UNIT, "n_gpus": ws, "steps": top["requests"],
+        "metric": METRIC, "value": job_rate, "unit": UNIT, "n_gpus": ws, "steps": top["requests"],
         "warmup": len(systems), "ms_per_step": 1e3 * top["seconds"] / top["requests"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded mesh generator tioga_b200.cases.config2, seeded rigid motions)",
@@ -775,8 +778,9 @@ def run_gpu_highorder(args, ws, rank, local, dist):
     changed = np.concatenate([(a != b) for a, b in zip(q_split, q0)])
     split_vs_fp64 = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(q_split, q_fp64))
     interp_err = max(float(np.max(np.abs(a - b))) if a.size else 0.0 for a, b in zip(q_split, q0))
+    ms_job = dist.max(ms_split)  # replicas: every rank runs the whole workload
     out = {
-        "metric": METRIC, "value": ws * Q / (ms_split * 1e-3), "unit": UNIT + " (high-order query points)",
+        "metric": METRIC, "value": ws * Q / (ms_job * 1e-3), "unit": UNIT + " (high-order query points)",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded mesh generator tioga_b200.cases.config4, seeded cubic field)",
@@ -875,11 +879,13 @@ def main():
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
-    dist = Dist(ws, None)
+    dev = None
+    if ws > 1:  # one GPU per rank, set before the process group binds it
+        import torch
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+    dist = Dist(ws, dev)
     try:
-        if ws > 1:
-            import torch
-            torch.cuda.set_device(local)
         out = {"cfg2": run_gpu_batch, "cfg3": run_gpu_serving,
                "cfg4": run_gpu_highorder}.get(args.workload, run_gpu)(args, ws, rank, local, dist)
     finally:
