@@ -34,6 +34,7 @@ Engine::Engine() {
 
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (pre_exec_) cudaGraphExecDestroy(pre_exec_);
   for (auto& e : ev_) cudaEventDestroy(e);
   for (auto& e : sev_) cudaEventDestroy(e);
   for (auto& e : cev_) cudaEventDestroy(e);
@@ -351,6 +352,7 @@ int Engine::upload_topology() {
   TB_CUDA(d_hmdev_.ensure(std::max(nhm_all_, 1)));
   topo_dirty_ = false;
   interps_fetched_ = false;
+  topo_gen_++;
   return 0;
 }
 
@@ -676,6 +678,7 @@ int Engine::build_tree_topology() {
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
   TB_CUDA(cbox_.ensure(2 * ctot_));
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
+  topo_gen_++;  // the cell arrays were replaced by their storage-order copies
   return 0;
 }
 
@@ -722,6 +725,64 @@ int Engine::preprocess() {
     TB_CUDA(cudaStreamSynchronize(stream_));
     stage.release();
   }
+  bool user_res = false;
+  for (const BlockInfo& B : bi_) user_res = user_res || B.has_user_res;
+  bool ran = false;
+  if (use_graphs_ && stream_ == own_stream_ && !sync_check() && !user_res) {
+    // the resolution and iblank stage is the same launches for a topology:
+    // captured once into a CUDA graph and replayed by every later preprocess
+    // (the serving form's time steps).  Any capture failure falls back to
+    // plain launches for good.
+    const long long key = topo_gen_ * 64 + mexclude_;
+    if (!pre_exec_ || pre_key_ != key) {
+      if (pre_exec_) cudaGraphExecDestroy(pre_exec_);
+      pre_exec_ = nullptr;
+      const long long n0 = nlaunch_;
+      cudaGraph_t g = nullptr;
+      if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int rc = preprocess_resolutions();
+        const cudaError_t e = cudaStreamEndCapture(stream_, &g);
+        if (rc == 0 && e == cudaSuccess && g && cudaGraphInstantiate(&pre_exec_, g, 0) == cudaSuccess) {
+          pre_key_ = key;
+          pre_nlaunch_ = nlaunch_ - n0;
+        } else {
+          pre_exec_ = nullptr;
+          use_graphs_ = false;
+        }
+        if (g) cudaGraphDestroy(g);
+      } else {
+        use_graphs_ = false;
+      }
+      cudaGetLastError();  // a failed capture leaves no sticky error
+      nlaunch_ = n0;
+    }
+    if (pre_exec_) {
+      TB_CUDA(cudaGraphLaunch(pre_exec_, stream_));
+      nlaunch_ += pre_nlaunch_;
+      ran = true;
+    }
+  }
+  if (!ran) TB_TRY(preprocess_resolutions());
+  for (size_t b = 0; b < hb_.size(); b++) {  // preprocess sets iblank = 1 (MeshBlock.C:80)
+    HostBlock& H = hb_[b];
+    if (H.dibl)
+      TB_CUDA(cudaMemcpyAsync(H.dibl, iblank_.p + bi_[b].node_off, H.nnodes * sizeof(int),
+                              cudaMemcpyDeviceToDevice, stream_));
+    else if (!serving_)
+      for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;
+  }
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  preprocessed_ = true;
+  donor_rest_ = false;
+  connected_ = false;
+  interps_fetched_ = false;
+  return 0;
+}
+
+// Cell volumes and node resolutions (tagBoundary, MeshBlock.C:94-339), the
+// mandatory receptors and mexclude rounds, and iblank = 1: launches only, on
+// buffers fixed by the topology (a CUDA graph can hold them).
+int Engine::preprocess_resolutions() {
   k_cell_volume<<<grid_for(ctot_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, cell_blk_.p, d_bi_.p,
                                                           ctot_, cell_res_.p);
   TB_LAUNCHED("k_cell_volume");
@@ -742,19 +803,6 @@ int Engine::preprocess() {
   }
   k_fill_int<<<grid_for(ntot_, kT), kT, 0, stream_>>>(iblank_.p, 1, ntot_);
   TB_LAUNCHED("k_fill_int");
-  for (size_t b = 0; b < hb_.size(); b++) {  // preprocess sets iblank = 1 (MeshBlock.C:80)
-    HostBlock& H = hb_[b];
-    if (H.dibl)
-      TB_CUDA(cudaMemcpyAsync(H.dibl, iblank_.p + bi_[b].node_off, H.nnodes * sizeof(int),
-                              cudaMemcpyDeviceToDevice, stream_));
-    else if (!serving_)
-      for (int i = 0; i < H.nnodes; i++) H.hibl[i] = 1;
-  }
-  TB_CUDA(cudaStreamSynchronize(stream_));
-  preprocessed_ = true;
-  donor_rest_ = false;
-  connected_ = false;
-  interps_fetched_ = false;
   return 0;
 }
 

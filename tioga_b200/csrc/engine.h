@@ -300,6 +300,7 @@ class Engine {
   int build_tree_topology();
   int upload_coords();
   int run_holemaps();
+  int preprocess_resolutions();
   int run_pairs_and_refit();
   int run_queries();
   int run_search();
@@ -323,6 +324,10 @@ class Engine {
   bool coords_on_device_ = false;  // x_ holds the registered blocks' coordinates
   long long dev_bytes_ = 0;        // device bytes of this engine's buffers (when counted)
   bool serving_ = false;
+  long long topo_gen_ = 0;             // bumped whenever the topology buffers are replaced
+  cudaGraphExec_t pre_exec_ = nullptr;  // preprocess_resolutions as a graph, for topology pre_key_
+  long long pre_key_ = -1, pre_nlaunch_ = 0;
+  bool use_graphs_ = true;
   bool topo_dirty_ = true;
   bool preprocessed_ = false;
   bool connected_ = false;
