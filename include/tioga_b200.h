@@ -169,7 +169,10 @@ int tioga_b200_nsystems_(void);
  * requests) when it fits `hbm_budget_bytes` and at most `max_resident`
  * systems are resident; idle systems are evicted least recently used first
  * (their device coordinates written back to the caller's xyz arrays).
- * Requests of one system run in submission order, one at a time.  Returns
+ * Requests of one system run in submission order, one at a time.  Device
+ * buffers come from the server's own stream-ordered memory pool, which
+ * reserves min(hbm_budget_bytes, free device memory - 2 GiB) at creation
+ * and keeps what is freed, so requests do not wait on pool growth.  Returns
  * NULL without a CUDA device. */
 void *tioga_b200_server_create(long long hbm_budget_bytes, int nslots, int max_resident);
 void tioga_b200_server_destroy(void *srv);
@@ -203,7 +206,8 @@ long long tioga_b200_server_submit_fields(void *srv, int sys, int nmoves, const 
 int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[6], long long counts[4]);
 /* [0] resident systems, [1] device bytes they hold, [2] admissions,
  * [3] evictions, [4] completed requests, [5] queued requests, [6] budget,
- * [7] peak device bytes held. */
+ * [7] peak device bytes held, [8] bytes reserved in the server's memory
+ * pool at creation, [9] bytes the pool holds now. */
 void tioga_b200_server_stats(void *srv, long long out[16]);
 
 /* Autotuner: after tioga_preprocess_grids_, times every launch shape of the

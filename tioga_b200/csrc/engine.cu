@@ -10,6 +10,7 @@ namespace tb {
 static int g_last_cuda_error = 0;
 thread_local long long* g_dbuf_account = nullptr;
 thread_local cudaStream_t g_dbuf_stream = nullptr;
+thread_local cudaMemPool_t g_dbuf_pool = nullptr;
 int fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
   return -(int)e - 1000;

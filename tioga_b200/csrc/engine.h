@@ -42,6 +42,9 @@ extern thread_local long long* g_dbuf_account;
 // (cudaMallocAsync / cudaFreeAsync), so engines that run side by side on their
 // own streams never wait for each other's frees; null: cudaMalloc / cudaFree.
 extern thread_local cudaStream_t g_dbuf_stream;
+// With g_dbuf_stream: the pool the stream-ordered allocations come from
+// (null: the device's current pool).
+extern thread_local cudaMemPool_t g_dbuf_pool;
 
 template <class T>
 struct DBuf {
@@ -59,7 +62,9 @@ struct DBuf {
     size_t c = count ? count + grow : 1;
     async = g_dbuf_stream != nullptr;
     st = g_dbuf_stream;
-    cudaError_t e = async ? cudaMallocAsync((void**)&p, c * sizeof(T), st) : cudaMalloc(&p, c * sizeof(T));
+    cudaError_t e = !async ? cudaMalloc(&p, c * sizeof(T))
+                    : g_dbuf_pool ? cudaMallocFromPoolAsync((void**)&p, c * sizeof(T), g_dbuf_pool, st)
+                                  : cudaMallocAsync((void**)&p, c * sizeof(T), st);
     if (e == cudaSuccess) {
       n = c;
       acct = g_dbuf_account;

@@ -18,6 +18,13 @@
 // back to the caller's arrays first), and a request that still does not fit
 // waits.  Requests of one system run one at a time and in order, so each
 // result is the one the system would get alone.
+//
+// Device buffers come stream-ordered from the server's own memory pool,
+// reserved up front to the budget (less what the device has free).  Growing
+// a pool maps new memory under a lock that every allocating thread waits for
+// (30-70 ms per growth on B200), so a pool that grew whenever a moving mesh
+// pushed a buffer past its last size stalled every slot at once; the
+// reserved pool serves those growths from memory it already holds.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -79,6 +86,7 @@ class Server {
   Server(long long budget, int nslots, int max_resident)
       : budget_(budget), nslots_(std::max(1, nslots)), max_resident_(std::max(1, max_resident)) {
     cudaGetDevice(&device_);
+    make_pool();
     for (int i = 0; i < nslots_; i++) workers_.emplace_back([this] { work(); });
   }
   ~Server() {
@@ -96,6 +104,10 @@ class Server {
       }
     }
     for (auto& kv : req_) delete kv.second;
+    if (pool_) {  // its memory goes back to the device once the frees above complete
+      cudaDeviceSynchronize();
+      cudaMemPoolDestroy(pool_);
+    }
   }
 
   int add_block(int sys, const SrvBlock& b) {
@@ -181,6 +193,12 @@ class Server {
     out[5] = (long long)queue_.size();
     out[6] = budget_;
     out[7] = peak_used_;
+    out[8] = reserved_;
+    cudaMemPool_t pool = pool_;
+    if (!pool) cudaDeviceGetDefaultMemPool(&pool, device_);
+    unsigned long long v = 0;
+    if (pool && cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v) == cudaSuccess)
+      out[9] = (long long)v;
   }
 
  private:
@@ -244,15 +262,51 @@ class Server {
     return nullptr;
   }
 
+  // The server's pool: freed buffers stay in it for the next allocation, and
+  // min(budget, free device memory - 2 GiB) is reserved at once by one
+  // allocation freed at the end of its stream.  Without a pool of its own
+  // (creation failed) the device's default pool is used the same way.
+  void make_pool() {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_;
+    if (cudaMemPoolCreate(&pool_, &props) != cudaSuccess) {
+      cudaGetLastError();
+      pool_ = nullptr;
+      if (cudaDeviceGetDefaultMemPool(&def_pool_, device_) != cudaSuccess) def_pool_ = nullptr;
+    }
+    cudaMemPool_t pool = pool_ ? pool_ : def_pool_;
+    if (!pool) return;
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    const long long want = std::min(budget_, (long long)free_b - (2ll << 30)) & ~((2ll << 20) - 1);
+    if (want < (64ll << 20)) return;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, (size_t)want, pool, s) == cudaSuccess) {
+      cudaFreeAsync(p, s);
+      reserved_ = want;
+    } else {
+      cudaGetLastError();  // no reservation: the pool grows on demand
+    }
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+
   void work() {
     cudaSetDevice(device_);
-    {  // freed buffers stay in the device's pool for the next allocation
-      cudaMemPool_t pool;
-      if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
-        unsigned long long keep = ~0ull;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-      }
-    }
+    g_dbuf_pool = pool_;  // null: cudaMallocAsync from the default pool
     std::unique_lock<std::mutex> l(mu_);
     for (;;) {
       std::vector<int> evict;
@@ -356,6 +410,8 @@ class Server {
   std::map<long long, SrvRequest*> req_;
   long long next_ticket_ = 1, used_ = 0, peak_used_ = 0, admissions_ = 0, evictions_ = 0, completed_ = 0;
   bool stop_ = false;
+  cudaMemPool_t pool_ = nullptr, def_pool_ = nullptr;
+  long long reserved_ = 0;  // bytes reserved in the pool at creation
   std::vector<std::thread> workers_;
 };
 

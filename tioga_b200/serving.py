@@ -139,7 +139,8 @@ class Server:
     def stats(self) -> dict:
         out = (C.c_longlong * 16)()
         self.lib.tioga_b200_server_stats(self.h, C.cast(out, _P))
-        keys = ["resident", "bytes", "admissions", "evictions", "completed", "queued", "budget", "peak_bytes"]
+        keys = ["resident", "bytes", "admissions", "evictions", "completed", "queued", "budget", "peak_bytes",
+                "pool_reserved_at_create", "pool_bytes"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def close(self):
