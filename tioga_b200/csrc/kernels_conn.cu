@@ -776,13 +776,13 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass(
         const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
         const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
         const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        // slots past nv read vertex 0 again (a no-op for the box), so the
+        // eight gathers are unconditional and all in flight at once
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-          if (m < nv) {
-            const float4 v = xf[cv[m]];
-            lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
-            hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
-          }
+          const float4 v = xf[m < nv ? cv[m] : cv[0]];
+          lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+          hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
         }
       }
       for (int k = 0; k < 3; k++) {
@@ -1346,19 +1346,34 @@ __global__ void __launch_bounds__(256) k_traverse(
       plo[k] = p32 - e;
       phi[k] = p32 + e;
     }
-    // cells [c0, c0 + nc) of a hit leaf
+    // cells [c0, c0 + nc) of a hit leaf (1 <= nc <= kMaxLeafCells).  FP32
+    // boxes: the loop is unrolled and every slot reads a cell of the leaf
+    // (the last one again past nc), so all the box loads are issued before
+    // the first test, one memory round trip per leaf.  Hits are added in
+    // cell order.
     auto leaf_cells = [&](int c0, int ncell) {
-      for (int j = 0; j < ncell; j++) {
-        const int c = c0 + j;
-        bool pass;
-        if (FORM == 0) {
-          const double* bb = cbox64 + 6 * (long long)c;
+      unsigned hit = 0;
+      if (FORM == 0) {  // (FP64 boxes: 48 B a cell, tested one at a time)
+        for (int j = 0; j < ncell; j++) {
+          const double* bb = cbox64 + 6 * (long long)(c0 + j);
           const double lo[3] = {bb[0], bb[1], bb[2]}, hi[3] = {bb[3], bb[4], bb[5]};
-          pass = in_box64(p, lo, hi);
-        } else {
-          pass = hit_ab(cbox[2 * (long long)c], cbox[2 * (long long)c + 1], plo, phi);
+          hit |= (unsigned)in_box64(p, lo, hi) << j;
         }
-        if (pass) add_candidate((int)q, c, n, slots, ovf, ovf_cap, novf);
+      } else {
+        float4 A[kMaxLeafCells], B[kMaxLeafCells];
+#pragma unroll
+        for (int j = 0; j < kMaxLeafCells; j++) {
+          const long long c = c0 + min(j, ncell - 1);
+          A[j] = cbox[2 * c];
+          B[j] = cbox[2 * c + 1];
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxLeafCells; j++) hit |= (unsigned)(hit_ab(A[j], B[j], plo, phi) && j < ncell) << j;
+      }
+      while (hit) {
+        const int j = __ffs(hit) - 1;
+        hit &= hit - 1;
+        add_candidate((int)q, c0 + j, n, slots, ovf, ovf_cap, novf);
       }
     };
     if (root >= 0) {
@@ -1481,7 +1496,9 @@ __global__ void __launch_bounds__(256, 2) k_candidates(
     int cls;
     if (FORM == 1) {
       // exact FP64 element box while streaming the vertices; keep only the
-      // FP32 offsets from vertex 0 for the screen
+      // FP32 offsets from vertex 0 for the screen.  Slots past nv read
+      // vertex 0 again (a no-op for the box, offsets unused), so every load
+      // is unconditional and all of them are in flight at once.
       const double* v0p = x + 3 * (long long)cv[0];
       const double v0[3] = {v0p[0], v0p[1], v0p[2]};
       double lo[3] = {v0[0], v0[1], v0[2]}, hi[3] = {v0[0], v0[1], v0[2]};
@@ -1489,15 +1506,13 @@ __global__ void __launch_bounds__(256, 2) k_candidates(
       y[0][0] = y[0][1] = y[0][2] = 0.f;
 #pragma unroll
       for (int m = 1; m < 8; m++) {
-        if (m < nv) {
-          const double* vp = x + 3 * (long long)cv[m];
+        const double* vp = x + 3 * (long long)(m < nv ? cv[m] : cv[0]);
 #pragma unroll
-          for (int k = 0; k < 3; k++) {
-            const double v = vp[k];
-            lo[k] = dmin(lo[k], v);
-            hi[k] = dmax(hi[k], v);
-            y[m][k] = (float)(v - v0[k]);
-          }
+        for (int k = 0; k < 3; k++) {
+          const double v = vp[k];
+          lo[k] = dmin(lo[k], v);
+          hi[k] = dmax(hi[k], v);
+          y[m][k] = (float)(v - v0[k]);
         }
       }
       if (!in_box64(p, lo, hi)) continue;
