@@ -133,3 +133,24 @@ def test_device_fields_equal_host_fields():
             assert np.array_equal(a, b)
         for a, b in zip(qa, qb):
             assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+@pytest.mark.timeout(300)
+def test_pool_reserved_and_not_grown():
+    """The server's memory pool is reserved at creation and serves every
+    request of a moving-mesh stream without growing (a growth holds the
+    pool's lock and stalls every slot)."""
+    systems, steps = _workload()
+    srv = Server(budget_bytes=4 << 30, nslots=3)
+    for s, sysm in enumerate(systems):
+        srv.add_system(s, sysm)
+    st0 = srv.stats()
+    assert st0["pool_reserved_at_create"] > 0
+    assert st0["pool_bytes"] >= st0["pool_reserved_at_create"]
+    order = [(s, k) for k in range(NSTEPS) for s in range(len(systems))]
+    _run(srv, systems, steps, order)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(order)
+    assert st["peak_bytes"] <= st["pool_reserved_at_create"]
+    assert st["pool_bytes"] == st0["pool_bytes"], (st0, st)
