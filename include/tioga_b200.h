@@ -159,6 +159,24 @@ void tioga_b200_select_system_(int *sys);
 /* Systems registered in the instance. */
 int tioga_b200_nsystems_(void);
 
+/* Cell global ids of block btag: one uint64_t per cell in registration
+ * order, the cell_gid argument of the C++ tioga::registerGridData
+ * (src/tioga.h:121-123, kept by MeshBlock::setData, src/MeshBlock.C:60),
+ * which the C API does not pass.  The array stays the caller's; registering
+ * the block again clears it, as registerGridData without ids does. */
+void tioga_b200_registercellgid_(int *btag, uint64_t *cell_gid);
+/* tioga::getReceptorInfo (src/tioga.C:572-671) of the selected system, for
+ * C callers: the count of receptors it returns, then their records, four
+ * ints each.  Donor blocks come in registration order and each block's live
+ * interpolation records in list order (MeshBlock::getReceptorInfo,
+ * src/dataUpdate.C:161-178): receptor node (0-based), mesh tag of the
+ * receptor block, and the donor cell's global id as two ints (its eight
+ * bytes copied, low word first on a little-endian host).  A donating block
+ * without cell ids is an error (tioga_b200_last_error() != 0); the reference
+ * reads through a null pointer there. */
+void tioga_b200_getreceptorcount_(int *nreceptors);
+void tioga_b200_getreceptorinfo_(int *receptors);
+
 /* Serving form: a request loop over many resident systems, each request
  * one time step of one system (the per-step sequence preprocess ->
  * performconnectivity -> dataupdate of src/tiogaInterface.C:150-216 for that

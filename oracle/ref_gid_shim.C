@@ -1,0 +1,64 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY.
+//
+// Two entry points linked into _ref/libtioga_ref.so, so that the tests can
+// drive the reference's cell-global-id path, which only its C++ class offers,
+// through ctypes:
+//   refshim_registergrid_gid_  the arguments of tioga_registergrid_data_mb_
+//                              (src/tiogaInterface.C:107-129) with the cell
+//                              global ids in front, handed to
+//                              tioga::registerGridData (src/tioga.C:64-85)
+//   refshim_getreceptorinfo_   tioga::getReceptorInfo (src/tioga.C:572-671)
+// The instance is the C API's own (the global `tg` of src/globals.h), so the
+// rest of a test drives the reference through its C API as usual.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "tioga.h"
+
+extern TIOGA::tioga* tg;
+
+namespace {
+struct Registration {  // what the block's MeshBlock keeps pointers to
+  std::vector<int> nv, nc;
+  std::vector<int*> conn;
+};
+Registration g_reg[128];
+std::vector<int> g_receptors;
+}  // namespace
+
+extern "C" {
+
+void refshim_registergrid_gid_(uint64_t* cell_gid, int* bid, int* btag, int* nnodes, double* xyz, int* ibl,
+                               int* nwbc, int* nobc, int* wbcnode, int* obcnode, int* ntypes, ...) {
+  Registration& R = g_reg[*bid - 1];
+  std::vector<int> nv(*ntypes), nc(*ntypes);
+  std::vector<int*> conn(*ntypes);
+  va_list args;
+  va_start(args, ntypes);
+  for (int t = 0; t < *ntypes; t++) {
+    nv[t] = *va_arg(args, int*);
+    nc[t] = *va_arg(args, int*);
+    conn[t] = va_arg(args, int*);
+  }
+  va_end(args);
+  R.nv.swap(nv);
+  R.nc.swap(nc);
+  R.conn.swap(conn);
+  tg->registerGridData(*btag, *nnodes, xyz, ibl, *nwbc, *nobc, wbcnode, obcnode, *ntypes, R.nv.data(), R.nc.data(),
+                       R.conn.data(), cell_gid, nullptr);
+}
+
+// The number of ints getReceptorInfo returns (four per receptor); the first
+// min(count, cap) of them are copied to out when out is not null.
+int refshim_getreceptorinfo_(int* out, int cap) {
+  g_receptors.clear();
+  tg->getReceptorInfo(g_receptors);
+  const int n = (int)g_receptors.size();
+  if (out && n > 0) std::memcpy(out, g_receptors.data(), sizeof(int) * std::min(n, cap));
+  return n;
+}
+
+}  // extern "C"

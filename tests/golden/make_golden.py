@@ -61,6 +61,49 @@ def _reduce(t):
     t.lib.tioga_reduce_fringes_()
 
 
+# cases rerun with cell global ids on every block, for getReceptorInfo
+# (tioga.C:572-671); stored as <name>_gid.npz
+GID_CASES = ("cfg0_small_s0", "cfg1_small_s1", "cfg1_small_s1_reduce_nf2")
+
+
+def cell_gids(system, seed):
+    """Seeded, distinct uint64 cell ids per block, with high words in use."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in system.blocks:
+        perm = rng.permutation(b.ncells).astype(np.uint64)
+        out.append((np.uint64(b.tag) << np.uint64(40)) + perm * np.uint64(1000003) + np.uint64(7))
+    return out
+
+
+def receptor_info_from_donors(system, donors, gids):
+    """getReceptorInfo restated from getDonorInfo's lists (dataUpdate.C:121-178):
+    per donor block in registration order, per live record, (receptor node,
+    mesh tag of the receptor block, donor cell id's global id as two int32
+    words, low first)."""
+    tags = [b.tag for b in system.blocks]
+    rows = []
+    for k, b in enumerate(system.blocks):
+        rec, ind, _ = donors[b.tag]
+        pos = 0
+        for r in rec:
+            nw = int(r[3])
+            cell = int(ind[pos + nw])
+            pos += nw + 1
+            g = int(gids[k][cell])
+            rows.append([int(r[1]), tags[int(r[2])], np.int64(g & 0xffffffff).astype(np.int32),
+                         np.int64(g >> 32).astype(np.int32)])
+    return np.array(rows, dtype=np.int32).reshape(-1, 4)
+
+
+def run_gid_case(lib, name):
+    fac, _, nvar, itype, fseed = CASES[name]
+    system = fac()
+    gids = cell_gids(system, 500 + fseed)
+    out = run_system(lib, system, nvar=nvar, itype=itype, cell_gids=gids, **settings_for(name, system))
+    return system, gids, out
+
+
 def digest(system):
     h = hashlib.sha256()
     for b in system.blocks:
@@ -113,7 +156,13 @@ if __name__ == "__main__":
     lib = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
     if not os.path.exists(lib):
         sys.exit("build the compiled reference first: make -C oracle ref")
-    for name in (sys.argv[1:] or CASES):
-        system, q, out = run_case(lib, name)
-        save(name, system, q, out)
+    names = sys.argv[1:] or list(CASES) + [n + "_gid" for n in GID_CASES]
+    for name in names:
+        if name.endswith("_gid"):
+            system, gids, out = run_gid_case(lib, name[:-4])
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), digest=np.array(digest(system)),
+                                receptorinfo=out["receptorinfo"])
+        else:
+            system, q, out = run_case(lib, name)
+            save(name, system, q, out)
         print(name, "saved")

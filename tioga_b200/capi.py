@@ -56,9 +56,12 @@ class TiogaLibrary:
         self._order.clear()
 
     # -- registration ------------------------------------------------------
-    def registergrid_data_mb(self, bid: int, block, ibl=None):
+    def registergrid_data_mb(self, bid: int, block, ibl=None, cell_gid=None):
         """Register one cases.Block under block id ``bid`` (1-based).  ``ibl``
-        may supply the iblank array (e.g. pinned host memory)."""
+        may supply the iblank array (e.g. pinned host memory); ``cell_gid``
+        the cells' uint64 global ids (tioga_b200_registercellgid_ here; the
+        compiled reference takes them through its C++ class, by the test shim
+        refshim_registergrid_gid_)."""
         x = np.ascontiguousarray(block.x, dtype=np.float64).reshape(-1)
         if ibl is None:
             ibl = np.ones(block.nnodes, dtype=np.int32)
@@ -77,9 +80,19 @@ class TiogaLibrary:
         cbid, ctag, cnn = C.c_int(bid), C.c_int(block.tag), C.c_int(block.nnodes)
         cnw, cno, cnt = C.c_int(len(wbc)), C.c_int(len(obc)), C.c_int(len(block.cells))
         self._keep += [cbid, ctag, cnn, cnw, cno, cnt]
-        self.lib.tioga_registergrid_data_mb_(
-            C.byref(cbid), C.byref(ctag), C.byref(cnn), _ptr(x), _ptr(ibl),
-            C.byref(cnw), C.byref(cno), _ptr(wbc), _ptr(obc), C.byref(cnt), *args)
+        regargs = (C.byref(cbid), C.byref(ctag), C.byref(cnn), _ptr(x), _ptr(ibl),
+                   C.byref(cnw), C.byref(cno), _ptr(wbc), _ptr(obc), C.byref(cnt), *args)
+        gid = None
+        if cell_gid is not None:
+            gid = np.ascontiguousarray(cell_gid, dtype=np.uint64)
+            assert gid.shape == (block.ncells,)
+            self._keep.append(gid)
+        if gid is not None and hasattr(self.lib, "refshim_registergrid_gid_"):
+            self.lib.refshim_registergrid_gid_(_ptr(gid), *regargs)
+        else:
+            self.lib.tioga_registergrid_data_mb_(*regargs)
+            if gid is not None:
+                self.lib.tioga_b200_registercellgid_(C.byref(ctag), _ptr(gid))
         self.blocks[block.tag] = {"x": x, "iblank": ibl, "nnodes": block.nnodes,
                                   "ncells": block.ncells, "bid": bid}
         if block.tag not in self._order:
@@ -117,9 +130,10 @@ class TiogaLibrary:
     def select_system(self, sys: int):
         self.lib.tioga_b200_select_system_(_iref(sys))
 
-    def register_system(self, system, iblanks=None):
+    def register_system(self, system, iblanks=None, cell_gids=None):
         for bid, b in enumerate(system.blocks, start=1):
-            self.registergrid_data_mb(bid, b, None if iblanks is None else iblanks[bid - 1])
+            self.registergrid_data_mb(bid, b, None if iblanks is None else iblanks[bid - 1],
+                                      None if cell_gids is None else cell_gids[bid - 1])
 
     # -- settings ----------------------------------------------------------
     def setsymmetry(self, isym: int):
@@ -170,6 +184,22 @@ class TiogaLibrary:
             self.lib.tioga_getdonorinfo_(_iref(tag), _ptr(rec), _ptr(ind), _ptr(frac), C.byref(dc))
         return rec[:4 * d].reshape(d, 4), ind[:f], frac[:f]
 
+    def getreceptorinfo(self) -> np.ndarray:
+        """tioga::getReceptorInfo: (n, 4) int32 rows of (receptor node,
+        receptor mesh tag, donor cell global id low word, high word)."""
+        if hasattr(self.lib, "refshim_getreceptorinfo_"):
+            self.lib.refshim_getreceptorinfo_.restype = C.c_int
+            n = self.lib.refshim_getreceptorinfo_(None, C.c_int(0))
+            out = np.zeros(max(n, 1), dtype=np.int32)
+            self.lib.refshim_getreceptorinfo_(_ptr(out), C.c_int(n))
+            return out[:n].reshape(-1, 4)
+        nr = C.c_int(0)
+        self.lib.tioga_b200_getreceptorcount_(C.byref(nr))
+        out = np.zeros(max(4 * nr.value, 1), dtype=np.int32)
+        if nr.value > 0:
+            self.lib.tioga_b200_getreceptorinfo_(_ptr(out))
+        return out[:4 * nr.value].reshape(-1, 4)
+
     def iblank(self, tag: int) -> np.ndarray:
         return self.blocks[tag]["iblank"]
 
@@ -179,13 +209,16 @@ class TiogaLibrary:
 
 
 def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str = "row",
-               isym=None, nfringe=None, mexclude=None, resolutions=None, setup=None, after=None):
+               isym=None, nfringe=None, mexclude=None, resolutions=None, setup=None, after=None,
+               cell_gids=None):
     """Drive one library through the full north-star sequence and collect
     every observable: iblank per block, donor info per block and the updated
-    fields.  ``q_blocks`` are copied (the library updates them in place)."""
+    fields.  ``q_blocks`` are copied (the library updates them in place).
+    With ``cell_gids`` (per block, uint64 per cell) the blocks carry cell
+    global ids and ``out["receptorinfo"]`` is getReceptorInfo's result."""
     t = TiogaLibrary(lib_path)
     t.init()
-    t.register_system(system)
+    t.register_system(system, cell_gids=cell_gids)
     if isym is not None:
         t.setsymmetry(isym)
     if nfringe is not None:
@@ -205,6 +238,8 @@ def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str =
     for b in system.blocks:
         out["iblank"][b.tag] = t.iblank(b.tag).copy()
         out["donors"][b.tag] = t.getdonorinfo(b.tag)
+    if cell_gids is not None:
+        out["receptorinfo"] = t.getreceptorinfo()
     if q_blocks is not None:
         qs = [np.array(q, dtype=np.float64, copy=True) for q in q_blocks]
         for b, q in zip(system.blocks, qs):

@@ -163,6 +163,24 @@ void tioga_getdonorinfo_(int* btag, int* receptors, int* indices, double* frac, 
   if (ready("tioga_getdonorinfo_")) set_rc(g_tg->donor_info(*btag, receptors, indices, frac));
 }
 
+void tioga_b200_registercellgid_(int* btag, uint64_t* cell_gid) {
+  if (ready("tioga_b200_registercellgid_")) set_rc(g_tg->set_cell_gid(*btag, cell_gid));
+}
+
+void tioga_b200_getreceptorcount_(int* nreceptors) {
+  *nreceptors = 0;
+  if (!ready("tioga_b200_getreceptorcount_")) return;
+  const long long n = g_tg->receptor_info(nullptr, 0);
+  set_rc(n < 0 ? -1 : 0);
+  if (n > 0) *nreceptors = (int)(n / 4);
+}
+
+void tioga_b200_getreceptorinfo_(int* receptors) {
+  if (!ready("tioga_b200_getreceptorinfo_")) return;
+  const long long n = g_tg->receptor_info(receptors, 1ll << 62);
+  set_rc(n < 0 ? -1 : 0);
+}
+
 void tioga_setsymmetry_(int* isym) {
   if (ready("tioga_setsymmetry_")) g_tg->set_symmetry(*isym);
 }

@@ -152,6 +152,7 @@ int Engine::register_block_sys(int sys, int tag, int nnodes, double* x, int* ibl
     b.hconn[t] = t < ntypes ? conn[t] : nullptr;
     b.ncells += b.nc[t];
   }
+  b.cell_gid = nullptr;  // registerGridData without cell ids (src/MeshBlock.C:60)
   topo_dirty_ = true;
   coords_on_device_ = false;
   gate_valid_ = false;
@@ -1867,6 +1868,44 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
     receptors[k++] = nv;
   }
   return 0;
+}
+
+int Engine::set_cell_gid(int tag, const uint64_t* gid) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].cell_gid = gid;
+  return 0;
+}
+
+// tioga::getReceptorInfo (src/tioga.C:572-671) on one rank: the donor blocks
+// in registration order, each block's live records in list order
+// (MeshBlock::getReceptorInfo, src/dataUpdate.C:161-178), every record as
+// (receptor node, mesh tag of the receptor block, the donor cell's global id
+// as two ints: its eight bytes copied, low word first on a little-endian host).
+long long Engine::receptor_info(int* out, long long cap) {
+  if (!connected_ || npairs_ == 0) return 0;
+  if (fetch_interps()) return -1;
+  std::vector<int> first(bi_.size());
+  for (size_t b = 0; b < bi_.size(); b++) first[b] = bi_[b].node_off;
+  long long k = 0;
+  for (int ib = 0; ib < (int)hb_.size(); ib++) {
+    if (hb_[ib].sys != cur_sys_) continue;
+    for (long long r = 0; r < nrec_; r++) {
+      if (h_it_don_[r] != ib || h_it_cancel_[r]) continue;
+      if (!hb_[ib].cell_gid) {  // the reference reads through a null pointer here
+        fprintf(stderr, "#tioga_b200: block %d donates but has no cell global ids\n", hb_[ib].tag);
+        return -1;
+      }
+      const int g = h_it_rec_[r];
+      const int rb = (int)(std::upper_bound(first.begin(), first.end(), g) - first.begin()) - 1;
+      const uint64_t gid = hb_[ib].cell_gid[h_it_node_[9 * r + h_it_nv_[r]]];
+      int v[4] = {g - bi_[rb].node_off, hb_[rb].tag, 0, 0};
+      std::memcpy(&v[2], &gid, sizeof(gid));
+      for (int m = 0; m < 4; m++, k++)
+        if (out && k < cap) out[k] = v[m];
+    }
+  }
+  return k;
 }
 
 int Engine::cell_iblank(int tag, int* out) {

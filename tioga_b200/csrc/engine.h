@@ -195,6 +195,7 @@ struct HostBlock {
   double* hq = nullptr;          // registered host solution
   double* dq = nullptr;          // registered device solution
   int* dibl = nullptr;           // caller's device iblank array (optional)
+  const uint64_t* cell_gid = nullptr;  // caller's cell global ids (registerGridData's cell_gid)
 };
 
 struct Stats {
@@ -290,6 +291,11 @@ class Engine {
   // queries (src/dataUpdate.C:121-159, tioga.C:533-570)
   int donor_count(int tag, int* dcount, int* fcount);
   int donor_info(int tag, int* receptors, int* indices, double* frac);
+  int set_cell_gid(int tag, const uint64_t* gid);
+  // tioga::getReceptorInfo: 4 ints per live record of the selected system;
+  // writes min(count, cap) ints to out (may be null) and returns the count,
+  // or < 0 on error
+  long long receptor_info(int* out, long long cap);
   int cell_iblank(int tag, int* out);
   const Stats& stats() const { return stats_; }
   const Timing& timing() const { return timing_; }
