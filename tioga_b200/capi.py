@@ -211,7 +211,7 @@ class TiogaLibrary:
 def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str = "row",
                isym=None, nfringe=None, mexclude=None, resolutions=None, setup=None, after=None,
                cell_gids=None):
-    """Drive one library through the full north-star sequence and collect
+    """Drive one library through the full TIOGA call sequence and collect
     every observable: iblank per block, donor info per block and the updated
     fields.  ``q_blocks`` are copied (the library updates them in place).
     With ``cell_gids`` (per block, uint64 per cell) the blocks carry cell
