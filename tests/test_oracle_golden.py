@@ -52,3 +52,34 @@ def test_fixtures_exercise_every_state():
     assert (ibl == 0).sum() > 0 and (ibl == -1).sum() > 0 and (ibl == 1).sum() > 0
     nw = np.concatenate([g[k][:, 3] for k in g.files if k.startswith("receptors_")])
     assert set(np.unique(nw)) >= {4, 5, 6, 8}
+
+
+# Seeds beyond the fixtures: the restatement against the compiled reference
+# run in the same process, on every observable (CPU, seconds).
+LIVE_CASES = [
+    ("small_config0", 3, {}),
+    ("small_config0", 4, dict(isym=0, nfringe=2)),
+    ("small_config1", 3, {}),
+    ("small_config1", 4, dict(mexclude=1)),
+    ("small_config1_seam", 3, dict(nfringe=2)),
+]
+
+
+@pytest.mark.parametrize("factory,seed,settings", LIVE_CASES)
+def test_oracle_matches_compiled_reference_on_more_seeds(factory, seed, settings, oracle_lib):
+    if not os.path.exists(REF_LIB):
+        pytest.skip("the compiled reference needs the reference sources (make -C oracle ref)")
+    from tioga_b200 import cases
+    from tioga_b200.capi import run_system
+    system = getattr(cases, factory)(seed)
+    q = cases.fields(system, nvar=3, seed=100 + seed)
+    ref = run_system(REF_LIB, system, q_blocks=q, nvar=3, **settings)
+    got = run_system(oracle_lib, system, q_blocks=q, nvar=3, **settings)
+    for b in system.blocks:
+        t = b.tag
+        np.testing.assert_array_equal(got["iblank"][t], ref["iblank"][t])
+        for x, y in zip(got["donors"][t], ref["donors"][t]):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))
+        assert np.array_equal(got["q"][t].view(np.int64), ref["q"][t].view(np.int64))
+    ibl = np.concatenate([ref["iblank"][b.tag] for b in system.blocks])
+    assert (ibl == -1).sum() > 0
