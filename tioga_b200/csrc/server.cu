@@ -357,7 +357,11 @@ class Server {
     int rc = 0;
     bool fresh = false;
     if (!S.eng) {  // admission: the system's engine, its topology and coordinates
-      S.eng = new Engine();
+      Engine* e = new Engine();
+      {  // published under the lock: pick() and stats() read the pointer
+        std::lock_guard<std::mutex> g(mu_);
+        S.eng = e;
+      }
       g_dbuf_account = S.eng->byte_counter();
       g_dbuf_stream = S.eng->stream();
       for (const SrvBlock& b : S.blocks) {
