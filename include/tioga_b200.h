@@ -105,9 +105,18 @@ void tioga_reduce_fringes_(void);
 void tioga_writeoutputfiles_(int *nvar, char *itype);
 
 /* Entry points of TIOGA outside the accelerated path (AMR/Cartesian,
- * p4est).  They are exported so that existing solvers link; each reports
- * "not supported" and sets the last error. */
+ * p4est; tiogaInterface.C:132-148, 287-299, and the AMR connectivity).
+ * They are exported so that existing solvers link; each reports "not
+ * supported" and sets the last error. */
 void tioga_performconnectivity_amr_(void);
+void tioga_register_amr_global_data_(int *nf, int *qstride, double *qnodein, int *idata, double *rdata,
+                                     int *ngridsin, int *qnodesize);
+void tioga_register_amr_patch_count_(int *npatches);
+void tioga_register_amr_local_data_(int *ipatch, int *global_id, int *iblank, double *q);
+void tioga_set_p4est_(void);
+void tioga_set_amr_callback_(void (*f1)(int *, double *, int *, double *));
+void tioga_set_p4est_search_callback_(void (*f1)(double *xsearch, int *process_id, int *cell_id, int *npts),
+                                      void (*f2)(int *pid, int *iflag));
 
 /* ---- additions of this library (no counterpart in TIOGA) -------------- */
 

@@ -59,3 +59,32 @@ def test_reference_symbols_are_a_subset():
             continue
         assert hasattr(ref, n), f"{n} is not a reference symbol"
         assert hasattr(gpu, n)
+
+
+def test_every_reference_entry_point_is_exported():
+    """Drop-in linking: every tioga_* function of the compiled reference's C
+    API is exported by the GPU library (the ones outside the accelerated path
+    as "not supported" stubs)."""
+    if not os.path.exists(REF_LIB):
+        pytest.skip("compiled reference not built here")
+    import subprocess
+    import tioga_b200
+
+    def exported(path):
+        out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True,
+                             check=True).stdout
+        return {ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[-1].startswith("tioga_")}
+
+    missing = sorted(exported(REF_LIB) - exported(tioga_b200.library_path()))
+    assert not missing, missing
+
+
+def test_unsupported_entry_points_report_without_a_gpu():
+    """The AMR and p4est entry points return with an error status."""
+    import tioga_b200
+    lib = tioga_b200.extras(C.CDLL(tioga_b200.library_path()))
+    lib.tioga_set_p4est_()
+    assert lib.tioga_b200_last_error() != 0
+    n = C.c_int(3)
+    lib.tioga_register_amr_patch_count_(C.byref(n))
+    assert lib.tioga_b200_last_error() != 0

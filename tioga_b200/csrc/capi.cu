@@ -211,6 +211,16 @@ void tioga_performconnectivity_highorder_(void) {
   if (ready("tioga_performconnectivity_highorder_")) set_rc(g_tg->connectivity_highorder());
 }
 void tioga_performconnectivity_amr_(void) { unsupported("tioga_performconnectivity_amr_"); }
+void tioga_register_amr_global_data_(int*, int*, double*, int*, double*, int*, int*) {
+  unsupported("tioga_register_amr_global_data_");
+}
+void tioga_register_amr_patch_count_(int*) { unsupported("tioga_register_amr_patch_count_"); }
+void tioga_register_amr_local_data_(int*, int*, int*, double*) { unsupported("tioga_register_amr_local_data_"); }
+void tioga_set_p4est_(void) { unsupported("tioga_set_p4est_"); }
+void tioga_set_amr_callback_(void (*)(int*, double*, int*, double*)) { unsupported("tioga_set_amr_callback_"); }
+void tioga_set_p4est_search_callback_(void (*)(double*, int*, int*, int*), void (*)(int*, int*)) {
+  unsupported("tioga_set_p4est_search_callback_");
+}
 // The callbacks are recorded (they switch the data update to the point
 // form, as in tioga.h:211-223), but a device search cannot call host code:
 // the elements must also be described with tioga_b200_set_highorder_lagrange_.
