@@ -348,10 +348,40 @@ def run_gpu(args, ws, rank, local, dist):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    out["dataupdate"] = time_dataupdate(lib, system, stream, st["nreceptor"], args.steps, args.warmup)
     lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
     lib.delete()
     del keep
     return out
+
+
+def time_dataupdate(lib, system, stream, nreceptor: int, steps: int, warmup: int, nvar: int = 5):
+    """The data update after the last connectivity call, reported on its own
+    as receptor-fields per second: 5 FP64 fields per node in the ROW layout,
+    resident on the device (a GPU solver's arrays), CUDA events around
+    `steps` calls after `warmup` untimed ones."""
+    import torch
+    try:
+        dq = [torch.empty(b.nnodes * nvar, dtype=torch.float64, device="cuda").uniform_(-1.0, 1.0)
+              for b in system.blocks]
+        for b, d in zip(system.blocks, dq):
+            lib.lib.tioga_b200_registersolution_device_(C.byref(C.c_int(b.tag)), C.c_void_p(d.data_ptr()))
+        for _ in range(max(1, warmup)):
+            lib.dataupdate_mb(nvar, "row")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            lib.dataupdate_mb(nvar, "row")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if lib.lib.tioga_b200_last_error() != 0:
+            return {"error": "data update failed"}
+        ms = e0.elapsed_time(e1) / steps
+        return {"ms": ms, "receptors": nreceptor, "nvar": nvar, "layout": "row, fields on the device",
+                "receptor_fields_per_s": nreceptor * nvar / (ms * 1e-3)}
+    except Exception as ex:  # the connectivity line stands without it
+        return {"error": repr(ex)}
 
 
 # ---------------------------------------------------------------------------
