@@ -278,7 +278,8 @@ void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
  * refinements, [5] receptors, [6] holes, [7] donor records, [8] device
  * error bits, [9] pairs of blocks, [10] kernels launched by the library,
  * [11] sum of the candidates' vertex counts, [12] leaves of the cell trees,
- * [13] query points merged into a coincident one (uniqNodesTree). */
+ * [13] query points merged into a coincident one (uniqNodesTree),
+ * [14] leaf groups of the cell pass, [15] their distinct vertex nodes. */
 void tioga_b200_stats_(long long out[16]);
 /* Run on the caller's CUDA stream (a cudaStream_t; NULL restores the
  * library's own stream), e.g. to time the calls with the caller's events. */

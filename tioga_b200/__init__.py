@@ -41,7 +41,7 @@ def stats(lib: C.CDLL) -> dict:
     out = (C.c_longlong * 16)()
     lib.tioga_b200_stats_(out)
     keys = ["nquery", "ndonor", "nties", "ncand", "nrefine", "nreceptor", "nhole", "nrecords",
-            "error", "npairs", "launches", "cand_verts", "nleaf", "nmerged"]
+            "error", "npairs", "launches", "cand_verts", "nleaf", "nmerged", "ngroups", "ngroup_nodes"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 

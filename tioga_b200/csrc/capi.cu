@@ -302,6 +302,8 @@ void tioga_b200_stats_(long long out[16]) {
   out[11] = s.cand_verts;
   out[12] = s.nleaf;
   out[13] = s.nmerged;
+  out[14] = s.ngroups;
+  out[15] = s.ngroup_nodes;
 }
 
 void tioga_b200_autotune_(int* reps) {

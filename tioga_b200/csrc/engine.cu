@@ -45,8 +45,8 @@ Engine::~Engine() {
   wall_list_.release(); obc_list_.release(); csr_off_.release(); csr_cell_.release(); deg_.release();
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   hm_state_.release();
-  wall_bb_.release(); sorted_cell_.release(); cbox_.release(); tnode_.release(); tnode64_.release();
-  xf_.release(); leaves_.release(); gparent_.release(); gnk_.release();
+  wall_bb_.release(); sorted_cell_.release(); qbox_.release(); tnode_.release(); tnode64_.release();
+  grp_.release(); grp_nodes_.release(); cell_lidx_.release(); leaves_.release(); gparent_.release(); gnk_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
@@ -629,6 +629,7 @@ int Engine::build_tree_topology() {
     TB_CUDA(cudaStreamSynchronize(stream_));
     for (int b = nb - 1; b >= 0; b--)
       if (h_blk_leaf_[b] < 0) h_blk_leaf_[b] = h_blk_leaf_[b + 1];
+    TB_TRY(build_leaf_groups());
   }
   // cells (storage order) that mark their wall-bearing block's hole map
   {
@@ -678,7 +679,7 @@ int Engine::build_tree_topology() {
   TB_CUDA(cudaMemcpyAsync(tile_base_.p, h_tile_base_.data(), h_tile_base_.size() * sizeof(long long),
                           cudaMemcpyHostToDevice, stream_));
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
-  TB_CUDA(cbox_.ensure(2 * ctot_));
+  TB_CUDA(qbox_.ensure(ctot_));
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   topo_gen_++;  // the cell arrays were replaced by their storage-order copies
   return 0;
@@ -908,6 +909,51 @@ int Engine::run_holemaps() {
   return 0;
 }
 
+// Leaf groups of kGroupLeaves consecutive leaves of one block (the cell
+// pass's unit of work for one warp) with their distinct vertex nodes and the
+// cells' positions in them (k_group_nodes); once per topology.
+int Engine::build_leaf_groups() {
+  const int nb = (int)bi_.size();
+  std::vector<int2> hg;
+  h_blk_grp_.assign(nb + 1, 0);
+  for (int b = 0; b < nb; b++) {
+    h_blk_grp_[b] = (int)hg.size();
+    for (int l = h_blk_leaf_[b]; l < h_blk_leaf_[b + 1]; l += kGroupLeaves)
+      hg.push_back(make_int2(l, std::min(kGroupLeaves, h_blk_leaf_[b + 1] - l)));
+  }
+  h_blk_grp_[nb] = (int)hg.size();
+  ngrp_ = (long long)hg.size();
+  ngrp_nodes_ = 0;
+  TB_CUDA(grp_.ensure(std::max(1ll, ngrp_)));
+  TB_CUDA(cell_lidx_.ensure(std::max(1ll, ctot_)));
+  if (ngrp_ == 0) return 0;
+  DBuf<int2> gl;
+  DBuf<int> cnt, off;
+  TB_CUDA(gl.ensure(ngrp_));
+  TB_CUDA(cnt.ensure(ngrp_ + 1));
+  TB_CUDA(off.ensure(ngrp_ + 1));
+  TB_CUDA(cudaMemcpyAsync(gl.p, hg.data(), ngrp_ * sizeof(int2), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaMemsetAsync(cnt.p + ngrp_, 0, sizeof(int), stream_));
+  const unsigned grid = (unsigned)std::max(1ll, std::min((ngrp_ + 7) / 8, 148ll * 64));
+  k_group_nodes<false><<<grid, 256, 0, stream_>>>(gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, cnt.p, nullptr,
+                                                  nullptr, nullptr, nullptr);
+  TB_LAUNCHED("k_group_nodes");
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, (int)(ngrp_ + 1), stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, cnt.p, off.p, (int)(ngrp_ + 1), stream_);
+  int total = 0;
+  TB_CUDA(cudaMemcpyAsync(&total, off.p + ngrp_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  TB_CUDA(grp_nodes_.ensure(std::max(1, total)));
+  k_group_nodes<true><<<grid, 256, 0, stream_>>>(gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, nullptr, off.p,
+                                                 grp_nodes_.p, cell_lidx_.p, grp_.p);
+  TB_LAUNCHED("k_group_nodes");
+  TB_CUDA(cudaStreamSynchronize(stream_));  // the host list and the scratch go out of scope
+  ngrp_nodes_ = total;
+  return 0;
+}
+
 int Engine::run_pairs_and_refit() {
   const int nb = (int)hb_.size();
   TB_CUDA(d_pairs_.ensure(npcand_ + 1));
@@ -922,12 +968,9 @@ int Engine::run_pairs_and_refit() {
                           stream_));
   TB_CUDA(cudaMemcpyAsync(h_pfirst_.data(), d_pfirst_.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
-  // FP32 coordinates and the node tiles' boxes (query gathering, hole search)
-  TB_CUDA(xf_.ensure(ntot_));
-  k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
-  TB_LAUNCHED("k_round_nodes");
+  // the node tiles' boxes (query gathering, hole search)
   if (h_tile_base_.back() > 0) {
-    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(xf_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
+    k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
                                                                       node_order_.p);
     TB_LAUNCHED("k_node_tiles");
   }
@@ -959,22 +1002,27 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
   // chunks of consecutive blocks whose pairs fit one CTA's shared memory;
-  // the CTAs of one launch are split among the chunks by leaf count
+  // the CTAs of one launch are split among the chunks by their work items:
+  // leaf groups (one warp each) in the split form, leaves (a quarter warp
+  // each) in the FP64 form
   const int kChunkPairs = std::max(16, std::min(128, tune_.chunk_pairs));
+  const std::vector<int>& item_of_blk = fp64 ? h_blk_leaf_ : h_blk_grp_;
+  const long long nitems = fp64 ? nleaf_total_ : ngrp_;
+  const long long per_cta = fp64 ? 256 / kMaxLeafCells : 256 / 32;  // items a CTA of 256 threads takes at once
   std::vector<int4> chunks;
   for (int b = 0; b < nb;) {
     int e = b + 1;
     while (e < nb && h_pfirst_[e + 1] - h_pfirst_[b] <= kChunkPairs) e++;
-    chunks.push_back(make_int4(h_blk_leaf_[b], h_blk_leaf_[e], h_pfirst_[b], h_pfirst_[e] - h_pfirst_[b]));
+    chunks.push_back(make_int4(item_of_blk[b], item_of_blk[e], h_pfirst_[b], h_pfirst_[e] - h_pfirst_[b]));
     b = e;
   }
-  const long long want = grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * tune_.cell_pass_per_sm);
+  const long long want = grid_for(nitems * (256 / per_cta), 256, 148 * tune_.cell_pass_per_sm);
   std::vector<int> ccta(chunks.size() + 1, 0);
   int maxnp = 1;
   for (size_t k = 0; k < chunks.size(); k++) {
     const long long nl = chunks[k].y - chunks[k].x;
-    long long n = nleaf_total_ > 0 ? (want * nl + nleaf_total_ - 1) / nleaf_total_ : 1;
-    n = std::max(1ll, std::min(n, (nl * kMaxLeafCells + 255) / 256));
+    long long n = nitems > 0 ? (want * nl + nitems - 1) / nitems : 1;
+    n = std::max(1ll, std::min(n, (nl + per_cta - 1) / per_cta));
     ccta[k + 1] = ccta[k] + (int)n;
     maxnp = std::max(maxnp, chunks[k].w);
   }
@@ -984,9 +1032,14 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(d_chunk_cta_.p, ccta.data(), ccta.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
   TB_CUDA(cudaEventRecord(cev_[0], stream_));
   const size_t smem = (size_t)maxnp * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
-  launch_cell_pass(fp64, tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, xf_.p, conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p,
-                   d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
-                   fp64 ? cbox64_.p : nullptr, tnode_.p, fp64 ? tnode64_.p : nullptr, pair_acc_.p);
+  if (fp64)
+    launch_cell_pass64(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
+                       leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p,
+                       cbox64_.p, tnode_.p, tnode64_.p, pair_acc_.p);
+  else
+    launch_cell_pass32(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
+                       leaves_.p, grp_.p, grp_nodes_.p, cell_lidx_.p, d_chunks_.p, d_chunk_cta_.p,
+                       (int)chunks.size(), d_pfirst_.p, d_pairs_.p, qbox_.p, tnode_.p, pair_acc_.p);
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
@@ -1106,7 +1159,7 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, cbox_.p,
+    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
     TB_LAUNCHED("k_traverse");
@@ -1770,6 +1823,8 @@ int Engine::connectivity() {
   stats_.nreceptor = (long long)cnt[5];
   stats_.nrecords = nrec_;
   stats_.nleaf = nleaf_total_;
+  stats_.ngroups = ngrp_;
+  stats_.ngroup_nodes = ngrp_nodes_;
   stats_.nmerged = (long long)cnt[7];
   stats_.npairs = npairs_;
   stats_.launches = nlaunch_;
@@ -1941,25 +1996,23 @@ int Engine::dataupdate(int nvar, int interptype) {
     return -1;
   }
   TB_CUDA(qvals_.ensure((size_t)nrec_ * nvar));
-  double* qdev;
+  // every block's solution on the device: the caller's own arrays (device
+  // solutions, read and written in place), or one upload of the host arrays
+  std::vector<double*> qptr(hb_.size());
   if (host) {
     TB_CUDA(q_.ensure((size_t)ntot_ * nvar));
-    for (size_t b = 0; b < hb_.size(); b++)
-      TB_CUDA(cudaMemcpyAsync(q_.p + (size_t)bi_[b].node_off * nvar, hb_[b].hq,
-                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    qdev = q_.p;
+    for (size_t b = 0; b < hb_.size(); b++) {
+      qptr[b] = q_.p + (size_t)bi_[b].node_off * nvar;
+      TB_CUDA(cudaMemcpyAsync(qptr[b], hb_[b].hq, (size_t)hb_[b].nnodes * nvar * sizeof(double),
+                              cudaMemcpyHostToDevice, stream_));
+    }
   } else {
-    // device solutions: the blocks' arrays must form one flat array in
-    // registration order (the layout tioga_b200_registersolution_device_
-    // documents); a gather keeps it general
-    TB_CUDA(q_.ensure((size_t)ntot_ * nvar));
-    for (size_t b = 0; b < hb_.size(); b++)
-      TB_CUDA(cudaMemcpyAsync(q_.p + (size_t)bi_[b].node_off * nvar, hb_[b].dq,
-                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    qdev = q_.p;
+    for (size_t b = 0; b < hb_.size(); b++) qptr[b] = hb_[b].dq;
   }
+  TB_CUDA(d_qptr_.ensure(hb_.size()));
+  TB_CUDA(cudaMemcpyAsync(d_qptr_.p, qptr.data(), qptr.size() * sizeof(double*), cudaMemcpyHostToDevice, stream_));
   k_interp_gather<<<grid_for(nrec_, 128), 128, 0, stream_>>>(it_node_.p, it_w_.p, it_don_.p, it_nv_.p,
-                                                              it_cancel_.p, rcount_.p, d_bi_.p, qdev, nvar,
+                                                              it_cancel_.p, rcount_.p, d_bi_.p, d_qptr_.p, nvar,
                                                               interptype, qvals_.p);
   TB_LAUNCHED("k_interp_gather");
   if (host) {
@@ -1985,12 +2038,12 @@ int Engine::dataupdate(int nvar, int interptype) {
       }
     }
   } else {
+    // the receptors' values straight into the caller's device arrays; the
+    // gather finished before (same stream), so every value read was the
+    // pre-update one, as with the reference's packet exchange
     k_interp_scatter<<<grid_for(nrec_, kT), kT, 0, stream_>>>(it_rec_.p, it_cancel_.p, rcount_.p, node_blk_.p,
-                                                               d_bi_.p, qvals_.p, nvar, interptype, qdev);
+                                                               d_bi_.p, qvals_.p, nvar, interptype, d_qptr_.p);
     TB_LAUNCHED("k_interp_scatter");
-    for (size_t b = 0; b < hb_.size(); b++)
-      TB_CUDA(cudaMemcpyAsync(hb_[b].dq, q_.p + (size_t)bi_[b].node_off * nvar,
-                              (size_t)hb_[b].nnodes * nvar * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
   }
   return 0;

@@ -21,6 +21,7 @@
 namespace tb {
 
 constexpr int kMaxLeafCells = 8; // cells per tree leaf at most
+constexpr int kGroupLeaves = 4;  // leaves per group, the cell pass's unit of work for one warp
 // device counters of the sparse donor phase (dcnt_)
 constexpr int kHoles = 0;        // holes, the first entries of the marked-node list
 constexpr int kMarked = 1;       // holes plus nfringe layers
@@ -212,6 +213,8 @@ struct Stats {
   long long npairs = 0;       // intersecting (receptor, donor) block pairs
   long long launches = 0;     // kernels this library launched in the call
   long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
+  long long ngroups = 0;      // leaf groups (the split-form cell pass's units of work)
+  long long ngroup_nodes = 0; // distinct vertex nodes summed over the leaf groups
   unsigned error = 0;
 };
 
@@ -313,6 +316,7 @@ class Engine {
   int run_holemaps();
   int preprocess_resolutions();
   int run_pairs_and_refit();
+  int build_leaf_groups();
   int run_queries();
   int run_search();
   int run_donors();
@@ -440,9 +444,13 @@ class Engine {
   DBuf<unsigned long long> wall_bb_;
   // tree
   DBuf<int> sorted_cell_;
-  DBuf<float4> cbox_;      // 2 per sorted cell
+  DBuf<uint2> qbox_;       // split form: 1 per sorted cell, its box coded inside its leaf's box
   DBuf<float4> tnode_;     // 2 per tree node
-  DBuf<float4> xf_;        // coordinates rounded to FP32, one per node
+  DBuf<int4> grp_;         // leaf groups: (first leaf, leaves, first node, nodes)
+  DBuf<int> grp_nodes_;    // each group's distinct vertex nodes, ascending
+  DBuf<uint2> cell_lidx_;  // 1 per sorted cell: its vertices' positions in its group's node list
+  long long ngrp_ = 0, ngrp_nodes_ = 0;
+  std::vector<int> h_blk_grp_;    // groups of block b: [h_blk_grp_[b], h_blk_grp_[b + 1])
   DBuf<double> tnode64_;   // 6 per tree node (FP64 form)
   DBuf<double> cbox64_;    // 6 per sorted cell (FP64 form)
   long long tree_nodes_ = 0;      // slots, four per group
@@ -478,6 +486,7 @@ class Engine {
   long long nrec_ = 0;
   // data update
   DBuf<double> q_, qvals_;
+  DBuf<double*> d_qptr_;   // every block's solution on the device (data update)
   // scratch for CUB and reductions
   DBuf<unsigned char> cub_tmp_;
   DBuf<double> red_;

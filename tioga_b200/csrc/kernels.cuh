@@ -35,6 +35,46 @@ __host__ __device__ inline double dkey_inv(unsigned long long k) {
   return d;
 }
 
+// ---- cell boxes as 8-bit offsets inside their leaf's box (split form) ----
+// A cell's FP32 box [lo, hi] (already rounded outward) is stored per axis as
+// two bytes (qlo, qhi) relative to the leaf box [L, H] of the tree, which is
+// the union of the leaf's cell boxes.  Decoding rounds outward:
+//   lo' = L                          (qlo == 0)   or fma_rd(qlo, sdn, L)
+//   hi' = H                          (qhi == 255) or fma_ru(qhi, sup, L)
+// with sdn <= (H - L) / 255 <= sup.  The encoder picks the tightest codes whose
+// decoded values still hold the box (it evaluates the same decode functions),
+// so lo' <= lo and hi' >= hi always: the traversal never loses a cell that the
+// FP32 box would have kept, and the exact FP64 element-box test that follows
+// decides candidacy.  8 bytes per cell: (qlo.xyz, qhi.xyz, 2 spare bytes).
+constexpr float kInv255Dn = 0.0039215682f;  // <= 1/255
+constexpr float kInv255Up = 0.0039215693f;  // >= 1/255
+__device__ __forceinline__ float qstep_dn(float L, float H) { return __fmul_rd(__fsub_rd(H, L), kInv255Dn); }
+__device__ __forceinline__ float qstep_up(float L, float H) { return __fmul_ru(__fsub_ru(H, L), kInv255Up); }
+__device__ __forceinline__ float qdec_lo(int q, float L, float sdn) {
+  return q == 0 ? L : __fmaf_rd((float)q, sdn, L);
+}
+__device__ __forceinline__ float qdec_hi(int q, float L, float H, float sup) {
+  return q == 255 ? H : __fmaf_ru((float)q, sup, L);
+}
+__device__ __forceinline__ int qenc_lo(float lo, float L, float sdn) {
+  if (!(sdn > 0.f) || !(lo > L)) return 0;
+  const float t = __fdiv_rd(__fsub_rd(lo, L), sdn);
+  int q = t >= 255.f ? 255 : (t > 0.f ? (int)t : 0);
+  for (int k = 0; k < 4 && q > 0 && qdec_lo(q, L, sdn) > lo; k++) q--;
+  if (q > 0 && qdec_lo(q, L, sdn) > lo) q = 0;
+  for (int k = 0; k < 2 && q < 255 && qdec_lo(q + 1, L, sdn) <= lo; k++) q++;
+  return q;
+}
+__device__ __forceinline__ int qenc_hi(float hi, float L, float H, float sup) {
+  if (!(sup > 0.f) || !(hi < H)) return 255;
+  const float t = __fdiv_ru(__fsub_ru(hi, L), sup);
+  int q = t >= 255.f ? 255 : (t > 0.f ? (int)ceilf(t) : 0);
+  for (int k = 0; k < 4 && q < 255 && qdec_hi(q, L, H, sup) < hi; k++) q++;
+  if (q < 255 && qdec_hi(q, L, H, sup) < hi) q = 255;
+  for (int k = 0; k < 2 && q > 0 && qdec_hi(q - 1, L, H, sup) >= hi; k++) q--;
+  return q;
+}
+
 // the last block whose first node tile is <= T (tile_base[b] = first tile of block b)
 __device__ __forceinline__ int block_of_tile(const long long* __restrict__ tile_base, int nb, long long T) {
   int lo = 0, hi = nb - 1;
@@ -100,12 +140,19 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
                         int* pfirst);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-void launch_cell_pass(bool f64, int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
-                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
-                      const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
-                      const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
-                      unsigned long long* acc);
-__global__ void k_round_nodes(const double* x, long long n, float4* xf);
+void launch_cell_pass32(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* grp,
+                        const int* grp_nodes, const uint2* cell_lidx, const int4* chunks, const int* chunk_cta,
+                        int nchunks, const int* pfirst, const PairInfo* pairs, uint2* qbox, float4* tnode,
+                        unsigned long long* acc);
+void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
+                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
+                        float4* tnode, double* tnode64, unsigned long long* acc);
+template <bool FILL>
+__global__ void k_group_nodes(const int2* grp_leaf, long long ngrp, const int4* leaves, const int* conn8,
+                              const unsigned char* cell_nv, int* cnt, const int* off, int* nodes, uint2* lidx,
+                              int4* grp);
 __global__ void k_tree_split(const unsigned long long* key, int n, const int* ca, const int* cb, const int* cslot,
                              int2* kids, int* nk, int* isint, int2* tlink, int* leaf_at);
 __global__ void k_tree_link(int n, const int* cslot, const int2* kids, const int* nk, const int* isint,
@@ -118,7 +165,7 @@ __global__ void k_leaf_list(const int* leaf_at, const int* loff, long long ctot,
                             const blk_t* cell_blk, int4* leaves);
 __global__ void k_block_leaves(const int4* leaves, long long nleaf, int* first);
 __global__ void k_refit_level(int g0, int g1, const int* gparent, float4* tnode, double* tnode64);
-__global__ void k_node_tiles(const float4* xf, const BlockInfo* bi, int nb, const long long* tile_base,
+__global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
 __global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);
@@ -138,7 +185,7 @@ __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairIn
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf);
 __global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,
@@ -242,10 +289,10 @@ __global__ void k_cell_iblank_sparse(const int* mlist, const int* dcnt, const in
 __global__ void k_gather_cells_i32(const int* src, const int* inv, long long base, int n, int* out);
 __global__ void k_interp_gather(const int* it_node, const double* it_w, const int* it_don,
                                 const unsigned char* it_nv, const unsigned char* it_cancel,
-                                const int* rcount, const BlockInfo* bi, const double* q, int nvar,
+                                const int* rcount, const BlockInfo* bi, const double* const* qptr, int nvar,
                                 int interptype, double* vals);
 __global__ void k_interp_scatter(const int* it_rec, const unsigned char* it_cancel, const int* rcount,
                                  const blk_t* node_blk, const BlockInfo* bi, const double* vals,
-                                 int nvar, int interptype, double* q);
+                                 int nvar, int interptype, double* const* qptr);
 
 }  // namespace tb

@@ -595,14 +595,6 @@ __device__ __forceinline__ float f_ru(double v) { return __double2float_ru(v); }
 __device__ __forceinline__ float f_down(float v) { return __fsub_rd(__fmaf_rd(fabsf(v), -6.0e-8f, v), 1e-44f); }
 __device__ __forceinline__ float f_up(float v) { return __fadd_ru(__fmaf_ru(fabsf(v), 6.0e-8f, v), 1e-44f); }
 
-// FP32 copy of the coordinates (rounded to nearest), read where a box that
-// holds the vertices is enough: 16 bytes per vertex instead of 24
-__global__ void k_round_nodes(const double* __restrict__ x, long long n, float4* __restrict__ xf) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]),
-                        __double2float_rn(x[3 * i + 2]), 0.f);
-}
-
 // float -> int key with the same order (-0 taken as +0), for shared-memory
 // atomicMin / atomicMax
 __device__ __forceinline__ int fkey(float f) {
@@ -637,15 +629,28 @@ __device__ __forceinline__ void proj_bounds(const double cc[3], const double o[3
   }
 }
 
-// One pass over all cells, leaf by leaf (32 / kMaxLeafCells leaves of
-// kMaxLeafCells storage-order cells per warp, one lane per cell):
-//  * the FP64 element box, stored in FP32 rounded outward (and exactly for the
-//    FP64 form), and the union of each leaf's eight boxes written straight to
-//    the leaf's tree node, so the refit starts from the leaves;
-//  * the reduced box of every pair whose donor is the cell's block
-//    (getReducedOBB, MeshBlock.C:774-838), exact: the extents are minima and
-//    maxima over the vertices of the donor cells that overlap the receptor
-//    box, projected onto the donor box's axes.
+// Extents of a cell's vertices projected onto a box's axes about its centre,
+// in the reference's FP64 arithmetic and order (MeshBlock.C:800-833): lo/hi
+// of axis j in pb[j], pb[j + 3] (pb holds the start values).
+__device__ __forceinline__ void project_cell64(const double* __restrict__ x, const int* __restrict__ conn8,
+                                               long long c, int nv, const Obb& B, double pb[6]) {
+  for (int m = 0; m < nv; m++) {
+    const double* v = x + 3 * (long long)conn8[8 * c + m];
+    const double v0 = v[0], v1 = v[1], v2 = v[2];
+    for (int jx = 0; jx < 3; jx++) {
+      double xd = 0;
+      xd += (v0 - B.xc[0]) * B.vec[jx][0];
+      xd += (v1 - B.xc[1]) * B.vec[jx][1];
+      xd += (v2 - B.xc[2]) * B.vec[jx][2];
+      pb[jx] = dmin(pb[jx], xd);
+      pb[jx + 3] = dmax(pb[jx + 3], xd);
+    }
+  }
+}
+
+// The reduced boxes (getReducedOBB, MeshBlock.C:774-838) of every pair whose
+// donor is this lane's block, from the lane's cell box.  Shared by both forms
+// of the cell pass; one lane per cell, kMaxLeafCells lanes per leaf.
 // FP32 bounds of a cell's vertex projections (box centre and half sizes,
 // widened by far more than their rounding error and the reference's) decide
 // what needs FP64:
@@ -658,34 +663,154 @@ __device__ __forceinline__ void proj_bounds(const double cc[3], const double o[3
 //    the cell that does hold it always has its lower bound under every such
 //    upper bound, so it is always projected exactly.  The exact extents are
 //    combined per warp, per CTA in shared memory, and flushed once.
-// Work comes in chunks of consecutive blocks (chunk = leaves [x, y), pairs
+// First every leaf tests its box f against the pairs s_pc[qa .. qb), lane g
+// of the leaf taking pairs qa+g, qa+g+LC, ...: a leaf clearly outside a
+// receptor box is done with that pair; one clearly inside, whose projections
+// cannot reach the current extents' bounds, tightens them and is done too.
+// The remaining (leaf, pair) combinations go cell by cell.
+__device__ __forceinline__ void cell_pass_pairs(
+    const double* __restrict__ x, const int* __restrict__ conn8, const BlockInfo* __restrict__ bi,
+    const PairInfo* __restrict__ pairs, const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
+    unsigned long long* __restrict__ s_acc, int lane, bool leaf_ok, bool valid, long long c, int nv, int qa0, int qb0,
+    const float f[6], const double cc[3], const float hh[3]) {
+  constexpr int LC = kMaxLeafCells;
+  volatile int* v_ext = s_ext;
+  const bool leaf_live = leaf_ok && f[0] <= f[3];
+  const int qa = leaf_live ? qa0 : 0, qb = leaf_live ? qb0 : 0;
+  const int g = lane % LC;
+  unsigned mixed = 0u;
+  {
+    const int nqw = __reduce_max_sync(0xffffffffu, qb - qa);
+    if (nqw > 32) {
+      mixed = 0xffffffffu;  // more pairs than mask bits: cell by cell
+    } else if (nqw > 0) {
+      double lc[3];
+      float lh[3], lsc = 0.f;
+      for (int k = 0; k < 3; k++) {
+        lc[k] = 0.5 * ((double)f[k] + (double)f[k + 3]);
+        lh[k] = leaf_live ? __fmul_ru(__fsub_ru(f[k + 3], f[k]), 0.5f) : 0.f;
+        lsc += leaf_live ? fabsf((float)lc[k]) : 0.f;
+      }
+      for (int r = 0; LC * r < nqw; r++) {
+        const int q = qa + g + LC * r;
+        if (q < qb) {
+          const PairCull& Q = s_pc[q];
+          float blo[3], bhi[3];
+          proj_bounds(lc, Q.rxc, Q.rvec, lh, lsc, Q.rdxc, blo, bhi);
+          bool out = false, inside = true;
+          for (int jx = 0; jx < 3; jx++) {
+            out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
+            inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
+          }
+          bool mix = !out && !inside;
+          if (inside) {
+            const float zero[3] = {0.f, 0.f, 0.f};
+            proj_bounds(lc, Q.dxc, Q.dvec, lh, lsc, zero, blo, bhi);
+            for (int jx = 0; jx < 3; jx++) {
+              const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+              const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
+              mix = mix || (kl <= umin) || (ku >= lmax);
+            }
+            if (!mix)
+              for (int jx = 0; jx < 3; jx++) {
+                const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+                if (ku < v_ext[6 * q + jx]) atomicMin(&s_ext[6 * q + jx], ku);
+                if (kl > v_ext[6 * q + 3 + jx]) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+              }
+          }
+          if (mix) mixed |= 1u << (q - qa);
+        }
+      }
+      for (int o = 1; o < LC; o <<= 1) mixed |= __shfl_xor_sync(0xffffffffu, mixed, o);
+    }
+  }
+  float sc = 0.f;
+  for (int k = 0; k < 3; k++) sc += valid ? fabsf((float)cc[k]) : 0.f;
+  const int q0 = __reduce_min_sync(0xffffffffu, (valid && mixed) ? qa : 0x7fffffff);
+  const int q1 = __reduce_max_sync(0xffffffffu, (valid && mixed) ? qb : 0);
+  for (int q = q0; q < q1; q++) {
+    const bool mine = valid && q >= qa && q < qb && ((mixed >> min(q - qa, 31)) & 1u);
+    if (!__any_sync(0xffffffffu, mine)) continue;
+    bool contrib = false;
+    double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+    if (mine) {
+      const PairCull& Q = s_pc[q];
+      float blo[3], bhi[3];
+      proj_bounds(cc, Q.rxc, Q.rvec, hh, sc, Q.rdxc, blo, bhi);
+      bool out = false, inside = true;
+      for (int jx = 0; jx < 3; jx++) {
+        out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
+        inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
+      }
+      bool ov = !out && inside;
+      if (!out && !inside) {  // across a face: the reference's test, MeshBlock.C:800-821
+        const Obb& R = bi[pairs[Q.pair].rec].obb;
+        double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
+        project_cell64(x, conn8, c, nv, R, bb);
+        ov = true;
+        for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx] > R.dxc[jx]);
+        for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx + 3] < -R.dxc[jx]);
+      }
+      if (ov) {
+        const float zero[3] = {0.f, 0.f, 0.f};
+        proj_bounds(cc, Q.dxc, Q.dvec, hh, sc, zero, blo, bhi);
+        bool need = false;
+        for (int jx = 0; jx < 3; jx++) {
+          const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+          const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
+          need = need || (kl <= umin) || (ku >= lmax);
+          if (ku < umin) atomicMin(&s_ext[6 * q + jx], ku);
+          if (kl > lmax) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+        }
+        if (need) {  // the reference's projections, MeshBlock.C:822-833
+          double pb[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+          project_cell64(x, conn8, c, nv, bi[Q.don].obb, pb);
+          for (int jx = 0; jx < 3; jx++) {
+            rlo[jx] = pb[jx];
+            rhi[jx] = pb[jx + 3];
+          }
+          contrib = true;
+        }
+      }
+    }
+    if (__any_sync(0xffffffffu, contrib)) {
+      for (int jx = 0; jx < 3; jx++)
+        for (int o = 16; o > 0; o >>= 1) {
+          rlo[jx] = dmin(rlo[jx], __shfl_xor_sync(0xffffffffu, rlo[jx], o));
+          rhi[jx] = dmax(rhi[jx], __shfl_xor_sync(0xffffffffu, rhi[jx], o));
+        }
+      if (lane == 0)
+        for (int jx = 0; jx < 3; jx++) {
+          atomicMin(&s_acc[6 * q + jx], dkey(rlo[jx]));
+          atomicMax(&s_acc[6 * q + jx + 3], dkey(rhi[jx]));
+        }
+    }
+  }
+}
+
+// this CTA's chunk: the last one whose first CTA is <= blockIdx.x.  Work
+// comes in chunks of consecutive blocks (chunk = work items [x, y), pairs
 // z .. z+w-1: all the pairs whose donor is one of the chunk's blocks, as the
 // pairs are sorted by donor); CTAs chunk_cta[k] .. chunk_cta[k+1]-1 share
 // chunk k, whose pairs sit in their shared memory.
-template <bool F64, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_cell_pass(
-    const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
-    const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves,
-    const int4* __restrict__ chunks, const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, double* __restrict__ cbox64,
-    float4* __restrict__ tnode, double* __restrict__ tnode64, unsigned long long* __restrict__ acc) {
-  extern __shared__ unsigned long long s_dyn[];
-  int kc = 0;  // this CTA's chunk: the last one whose first CTA is <= blockIdx.x
-  {
-    int hi = nchunks - 1;
-    while (kc < hi) {
-      const int m = (kc + hi + 1) >> 1;
-      if (chunk_cta[m] <= (int)blockIdx.x) kc = m;
-      else hi = m - 1;
-    }
+__device__ __forceinline__ int chunk_of_cta(const int* __restrict__ chunk_cta, int nchunks) {
+  int kc = 0, hi = nchunks - 1;
+  while (kc < hi) {
+    const int m = (kc + hi + 1) >> 1;
+    if (chunk_cta[m] <= (int)blockIdx.x) kc = m;
+    else hi = m - 1;
   }
-  const int4 CH = chunks[kc];
-  const long long leaf_lo = CH.x, leaf_hi = CH.y;
+  return kc;
+}
+
+// the chunk's pairs into shared memory, the extents' accumulators cleared
+__device__ __forceinline__ void cell_pass_setup(const int4& CH, int kc, const int* __restrict__ chunk_cta,
+                                                const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs,
+                                                unsigned long long* s_acc, PairCull* s_pc, int* s_ext, int& cta,
+                                                int& ncta) {
   const int p0 = CH.z, np = CH.w;
-  const int cta = (int)blockIdx.x - chunk_cta[kc], ncta = chunk_cta[kc + 1] - chunk_cta[kc];
-  unsigned long long* s_acc = s_dyn;                                  // 6 per pair, exact extents
-  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * np);        // 1 per pair, by donor block
-  int* s_ext = reinterpret_cast<int*>(s_pc + np);                      // 6 per pair, FP32 bounds
+  cta = (int)blockIdx.x - chunk_cta[kc];
+  ncta = chunk_cta[kc + 1] - chunk_cta[kc];
   const int tid = threadIdx.x;
   for (int i = tid; i < 6 * np; i += blockDim.x) {
     s_acc[i] = (i % 6 < 3) ? ~0ull : 0ull;
@@ -710,8 +835,149 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass(
     s_pc[i] = q;
   }
   __syncthreads();
-  volatile int* v_ext = s_ext;
-  const int lane = tid & 31;
+}
+
+// the CTA's exact extents into the pairs' accumulators
+__device__ __forceinline__ void cell_pass_flush(const unsigned long long* s_acc, int p0, int np,
+                                                unsigned long long* __restrict__ acc) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < 6 * np; i += blockDim.x) {
+    const unsigned long long v = s_acc[i];
+    unsigned long long* dst = &acc[6 * (long long)(p0 + i / 6) + i % 6];
+    if (i % 6 < 3) {
+      if (v != ~0ull) atomicMin(dst, v);
+    } else if (v != 0ull) {
+      atomicMax(dst, v);
+    }
+  }
+}
+
+// Cell pass of the split form, one warp per leaf group (up to 4 leaves of one
+// block, one lane per cell; chunk work items are groups):
+//  * the group's distinct nodes are read once, rounded to FP32 and staged in
+//    shared memory; every cell reads its vertices there through its one-byte
+//    positions (k_group_nodes), so a warp issues about 3 coalesced coordinate
+//    loads instead of 8 scattered gathers;
+//  * each cell's box is rounded outward from the FP32 vertices (f_down/f_up
+//    cover every double that rounds onto them), the leaf box (the union of
+//    its cells' boxes) goes to the leaf's tree slot, and each cell box is
+//    stored as 8-bit offsets inside the leaf box (qbox: 8 bytes a cell);
+//  * the reduced boxes of the pairs, exact (cell_pass_pairs).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_pass32(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ grp,
+    const int* __restrict__ grp_nodes, const uint2* __restrict__ cell_lidx, const int4* __restrict__ chunks,
+    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, uint2* __restrict__ qbox, float4* __restrict__ tnode,
+    unsigned long long* __restrict__ acc) {
+  extern __shared__ unsigned long long s_dyn[];
+  __shared__ float4 s_node[8][256];
+  int cta, ncta;
+  const int kc = chunk_of_cta(chunk_cta, nchunks);
+  const int4 CH = chunks[kc];  // first group, end group, first pair, pairs
+  unsigned long long* s_acc = s_dyn;                              // 6 per pair, exact extents
+  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * CH.w);  // 1 per pair
+  int* s_ext = reinterpret_cast<int*>(s_pc + CH.w);                // 6 per pair, FP32 bounds
+  cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta);
+  const long long g_lo = CH.x, g_hi = CH.y;
+  const int p0 = CH.z;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  float4* sn = s_node[w];
+  const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
+  const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
+  constexpr int LC = kMaxLeafCells;
+  int4 Gnext = g_lo + warp0 < g_hi ? grp[g_lo + warp0] : make_int4(0, 0, 0, 0);
+  for (long long gi = g_lo + warp0; gi < g_hi; gi += nwarps) {
+    const int4 G = Gnext;  // first leaf, leaves, first node, nodes
+    if (gi + nwarps < g_hi) Gnext = grp[gi + nwarps];  // the next group's header, in flight meanwhile
+    const int j = lane / LC, ci = lane % LC;
+    const bool leaf_ok = j < G.y;
+    const int4 L = leaf_ok ? leaves[G.x + j] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
+    const bool valid = leaf_ok && ci < L.y;
+    const long long c = (long long)L.x + ci;
+    int nv = 0;
+    uint2 li = make_uint2(0u, 0u);
+    if (valid) {
+      nv = cell_nv[c];
+      li = cell_lidx[c];
+    }
+    for (int i = lane; i < G.w; i += 32) {
+      const double* v = x + 3 * (long long)grp_nodes[G.z + i];
+      sn[i] = make_float4(__double2float_rn(v[0]), __double2float_rn(v[1]), __double2float_rn(v[2]), 0.f);
+    }
+    __syncwarp();
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (valid) {
+#pragma unroll
+      for (int m = 0; m < 8; m++) {
+        const unsigned k = ((m < 4 ? li.x : li.y) >> (8 * (m & 3))) & 255u;
+        const float4 v = sn[k];
+        lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+        hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
+      }
+    }
+    __syncwarp();  // the next group's staging may overwrite sn
+    float fb[6];   // FP32 box, rounded outward
+    double cc[3];  // box centre
+    float hh[3];   // half sizes, rounded up
+    for (int k = 0; k < 3; k++) {
+      fb[k] = valid ? f_down(lo[k]) : INFINITY;
+      fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
+      cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
+      hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
+    }
+    // leaf box: union over the LC lanes of the leaf
+    float f[6];
+    for (int k = 0; k < 6; k++) f[k] = fb[k];
+    for (int o = 1; o < LC; o <<= 1)
+      for (int k = 0; k < 3; k++) {
+        f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
+        f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
+      }
+    if (valid) {
+      unsigned q[6];
+      for (int k = 0; k < 3; k++) {
+        const float sdn = qstep_dn(f[k], f[k + 3]), sup = qstep_up(f[k], f[k + 3]);
+        q[k] = (unsigned)qenc_lo(fb[k], f[k], sdn);
+        q[k + 3] = (unsigned)qenc_hi(fb[k + 3], f[k], f[k + 3], sup);
+      }
+      qbox[c] = make_uint2(q[0] | (q[1] << 8) | (q[2] << 16) | (q[3] << 24), q[4] | (q[5] << 8));
+    }
+    if (leaf_ok && ci == 0) {
+      const long long sl = L.z;
+      tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
+      *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
+    }
+    const int b = L.w;
+    cell_pass_pairs(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, leaf_ok, valid, c, nv,
+                    leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
+  }
+  cell_pass_flush(s_acc, p0, CH.w, acc);
+}
+
+// Cell pass of the FP64 form, leaf by leaf (32 / kMaxLeafCells leaves per
+// warp, one lane per cell; chunk work items are leaves): the FP64 element
+// box of every cell (cbox64, exact) and of every leaf (tnode64), their FP32
+// roundings outward for the leaf slots (links), and the reduced boxes.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_pass64(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ chunks,
+    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, double* __restrict__ cbox64, float4* __restrict__ tnode,
+    double* __restrict__ tnode64, unsigned long long* __restrict__ acc) {
+  extern __shared__ unsigned long long s_dyn[];
+  int cta, ncta;
+  const int kc = chunk_of_cta(chunk_cta, nchunks);
+  const int4 CH = chunks[kc];  // first leaf, end leaf, first pair, pairs
+  unsigned long long* s_acc = s_dyn;
+  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * CH.w);
+  int* s_ext = reinterpret_cast<int*>(s_pc + CH.w);
+  cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta);
+  const long long leaf_lo = CH.x, leaf_hi = CH.y;
+  const int p0 = CH.z;
+  const int tid = threadIdx.x, lane = tid & 31;
   const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
   const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
   constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;  // cells per leaf, leaves per warp
@@ -724,75 +990,48 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass(
     const long long c = (long long)L.x + lane % LC;
     const long long sl = L.z;
     int nv = 0;
-    float fb[6];  // FP32 box, rounded outward
-    double cc[3];  // box centre
-    float hh[3];   // half sizes, rounded up
-    if constexpr (F64) {
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      if (valid) {
-        nv = cell_nv[c];
-        const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
-        const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
-        const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    float fb[6];
+    double cc[3];
+    float hh[3];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    if (valid) {
+      nv = cell_nv[c];
+      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-          if (m < nv) {
-            const double* v = x + 3 * (long long)cv[m];
-            for (int k = 0; k < 3; k++) {
-              const double t = v[k];
-              lo[k] = fmin(lo[k], t);
-              hi[k] = fmax(hi[k], t);
-            }
-          }
-        }
-      }
-      for (int k = 0; k < 3; k++) {
-        fb[k] = valid ? f_rd(lo[k]) : INFINITY;
-        fb[k + 3] = valid ? f_ru(hi[k]) : -INFINITY;
-        cc[k] = 0.5 * (lo[k] + hi[k]);
-        hh[k] = valid ? __double2float_ru(0.5 * (hi[k] - lo[k])) : 0.f;
-      }
-      {
-        if (valid) {
-          double* o = cbox64 + 6 * c;
-          o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
-          o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
-        }
-        for (int o = 1; o < LC; o <<= 1)
+      for (int m = 0; m < 8; m++) {
+        if (m < nv) {
+          const double* v = x + 3 * (long long)cv[m];
           for (int k = 0; k < 3; k++) {
-            lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
-            hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+            const double t = v[k];
+            lo[k] = fmin(lo[k], t);
+            hi[k] = fmax(hi[k], t);
           }
-        if (leaf_ok && lane % LC == 0)
-          for (int k = 0; k < 3; k++) {
-            tnode64[6 * sl + k] = lo[k];
-            tnode64[6 * sl + k + 3] = hi[k];
-          }
-      }
-    } else {
-      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-      if (valid) {
-        nv = cell_nv[c];
-        const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
-        const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
-        const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        // slots past nv read vertex 0 again (a no-op for the box), so the
-        // eight gathers are unconditional and all in flight at once
-#pragma unroll
-        for (int m = 0; m < 8; m++) {
-          const float4 v = xf[m < nv ? cv[m] : cv[0]];
-          lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
-          hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
         }
-      }
-      for (int k = 0; k < 3; k++) {
-        fb[k] = valid ? f_down(lo[k]) : INFINITY;
-        fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
-        cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
-        hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
       }
     }
-    // leaf box: union over the LC lanes of the leaf
+    for (int k = 0; k < 3; k++) {
+      fb[k] = valid ? f_rd(lo[k]) : INFINITY;
+      fb[k + 3] = valid ? f_ru(hi[k]) : -INFINITY;
+      cc[k] = 0.5 * (lo[k] + hi[k]);
+      hh[k] = valid ? __double2float_ru(0.5 * (hi[k] - lo[k])) : 0.f;
+    }
+    if (valid) {
+      double* o = cbox64 + 6 * c;
+      o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2];
+      o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
+    }
+    for (int o = 1; o < LC; o <<= 1)
+      for (int k = 0; k < 3; k++) {
+        lo[k] = dmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+        hi[k] = dmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+      }
+    if (leaf_ok && lane % LC == 0)
+      for (int k = 0; k < 3; k++) {
+        tnode64[6 * sl + k] = lo[k];
+        tnode64[6 * sl + k + 3] = hi[k];
+      }
     float f[6];
     for (int k = 0; k < 6; k++) f[k] = fb[k];
     for (int o = 1; o < LC; o <<= 1)
@@ -800,202 +1039,61 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass(
         f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
         f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
       }
-    {
-      if (valid) {
-        cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
-        cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
-      }
-      if (leaf_ok && lane % LC == 0) {
-        tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
-        *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
-      }
+    if (leaf_ok && lane % LC == 0) {
+      tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
+      *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
     }
-    // The pairs of the leaf's block are s_pc[qa .. qb).  First every leaf
-    // tests its box against them, lane g of the leaf taking pairs qa+g,
-    // qa+g+LC, ...: a leaf clearly outside a receptor box is done with that
-    // pair; one clearly inside, whose projections cannot reach the current
-    // extents' bounds, tightens them and is done too.  The remaining
-    // (leaf, pair) combinations, bit q-qa of mixed, go cell by cell.
-    const bool leaf_live = leaf_ok && f[0] <= f[3];
-    const int qa = leaf_live ? pfirst[b] - p0 : 0, qb = leaf_live ? pfirst[b + 1] - p0 : 0;
-    const int g = lane % LC;
-    unsigned mixed = 0u;
-    {
-      const int nqw = __reduce_max_sync(0xffffffffu, qb - qa);
-      if (nqw > 32) {
-        mixed = 0xffffffffu;  // more pairs than mask bits: cell by cell
-      } else if (nqw > 0) {
-        double lc[3];
-        float lh[3], lsc = 0.f;
-        for (int k = 0; k < 3; k++) {
-          lc[k] = 0.5 * ((double)f[k] + (double)f[k + 3]);
-          lh[k] = leaf_live ? __fmul_ru(__fsub_ru(f[k + 3], f[k]), 0.5f) : 0.f;
-          lsc += leaf_live ? fabsf((float)lc[k]) : 0.f;
-        }
-        for (int r = 0; LC * r < nqw; r++) {
-          const int q = qa + g + LC * r;
-          if (q < qb) {
-            const PairCull& Q = s_pc[q];
-            float blo[3], bhi[3];
-            proj_bounds(lc, Q.rxc, Q.rvec, lh, lsc, Q.rdxc, blo, bhi);
-            bool out = false, inside = true;
-            for (int jx = 0; jx < 3; jx++) {
-              out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
-              inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
-            }
-            bool mix = !out && !inside;
-            if (inside) {
-              const float zero[3] = {0.f, 0.f, 0.f};
-              proj_bounds(lc, Q.dxc, Q.dvec, lh, lsc, zero, blo, bhi);
-              for (int jx = 0; jx < 3; jx++) {
-                const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-                const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
-                mix = mix || (kl <= umin) || (ku >= lmax);
-              }
-              if (!mix)
-                for (int jx = 0; jx < 3; jx++) {
-                  const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-                  if (ku < v_ext[6 * q + jx]) atomicMin(&s_ext[6 * q + jx], ku);
-                  if (kl > v_ext[6 * q + 3 + jx]) atomicMax(&s_ext[6 * q + 3 + jx], kl);
-                }
-            }
-            if (mix) mixed |= 1u << (q - qa);
-          }
-        }
-        for (int o = 1; o < LC; o <<= 1) mixed |= __shfl_xor_sync(0xffffffffu, mixed, o);
-      }
-    }
-    float sh = 0.f, sc = 0.f;
-    for (int k = 0; k < 3; k++) {
-      sh += hh[k];
-      sc += valid ? fabsf((float)cc[k]) : 0.f;
-    }
-    const int q0 = __reduce_min_sync(0xffffffffu, (valid && mixed) ? qa : 0x7fffffff);
-    const int q1 = __reduce_max_sync(0xffffffffu, (valid && mixed) ? qb : 0);
-    for (int q = q0; q < q1; q++) {
-      const bool mine = valid && q >= qa && q < qb && ((mixed >> min(q - qa, 31)) & 1u);
-      if (!__any_sync(0xffffffffu, mine)) continue;
-      bool contrib = false;
-      double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
-      if (mine) {
-        const PairCull& Q = s_pc[q];
-        float blo[3], bhi[3];
-        proj_bounds(cc, Q.rxc, Q.rvec, hh, sc, Q.rdxc, blo, bhi);
-        bool out = false, inside = true;
-        for (int jx = 0; jx < 3; jx++) {
-          out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
-          inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
-        }
-        bool ov = !out && inside;
-        if (!out && !inside) {  // across a face: the reference's test, MeshBlock.C:800-821
-          const Obb& R = bi[pairs[Q.pair].rec].obb;
-          double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
-          for (int m = 0; m < nv; m++) {
-            const double* v = x + 3 * (long long)conn8[8 * c + m];
-            const double v0 = v[0], v1 = v[1], v2 = v[2];
-            for (int jx = 0; jx < 3; jx++) {
-              double xd = 0;
-              xd += (v0 - R.xc[0]) * R.vec[jx][0];
-              xd += (v1 - R.xc[1]) * R.vec[jx][1];
-              xd += (v2 - R.xc[2]) * R.vec[jx][2];
-              bb[jx] = dmin(bb[jx], xd);
-              bb[jx + 3] = dmax(bb[jx + 3], xd);
-            }
-          }
-          ov = true;
-          for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx] > R.dxc[jx]);
-          for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx + 3] < -R.dxc[jx]);
-        }
-        if (ov) {
-          const float zero[3] = {0.f, 0.f, 0.f};
-          proj_bounds(cc, Q.dxc, Q.dvec, hh, sc, zero, blo, bhi);
-          bool need = false;
-          for (int jx = 0; jx < 3; jx++) {
-            const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-            const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
-            need = need || (kl <= umin) || (ku >= lmax);
-            if (ku < umin) atomicMin(&s_ext[6 * q + jx], ku);
-            if (kl > lmax) atomicMax(&s_ext[6 * q + 3 + jx], kl);
-          }
-          if (need) {  // the reference's projections, MeshBlock.C:822-833
-            const Obb& D = bi[Q.don].obb;
-            for (int m = 0; m < nv; m++) {
-              const double* v = x + 3 * (long long)conn8[8 * c + m];
-              const double v0 = v[0], v1 = v[1], v2 = v[2];
-              for (int jx = 0; jx < 3; jx++) {
-                double xd = 0;
-                xd += (v0 - D.xc[0]) * D.vec[jx][0];
-                xd += (v1 - D.xc[1]) * D.vec[jx][1];
-                xd += (v2 - D.xc[2]) * D.vec[jx][2];
-                rlo[jx] = dmin(rlo[jx], xd);
-                rhi[jx] = dmax(rhi[jx], xd);
-              }
-            }
-            contrib = true;
-          }
-        }
-      }
-      if (__any_sync(0xffffffffu, contrib)) {
-        for (int jx = 0; jx < 3; jx++)
-          for (int o = 16; o > 0; o >>= 1) {
-            rlo[jx] = dmin(rlo[jx], __shfl_xor_sync(0xffffffffu, rlo[jx], o));
-            rhi[jx] = dmax(rhi[jx], __shfl_xor_sync(0xffffffffu, rhi[jx], o));
-          }
-        if (lane == 0)
-          for (int jx = 0; jx < 3; jx++) {
-            atomicMin(&s_acc[6 * q + jx], dkey(rlo[jx]));
-            atomicMax(&s_acc[6 * q + jx + 3], dkey(rhi[jx]));
-          }
-      }
-    }
+    cell_pass_pairs(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, leaf_ok, valid, c, nv,
+                    leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
   }
-  __syncthreads();
-  for (int i = tid; i < 6 * np; i += blockDim.x) {
-    const unsigned long long v = s_acc[i];
-    unsigned long long* dst = &acc[6 * (long long)(p0 + i / 6) + i % 6];
-    if (i % 6 < 3) {
-      if (v != ~0ull) atomicMin(dst, v);
-    } else if (v != 0ull) {
-      atomicMax(dst, v);
-    }
-  }
+  cell_pass_flush(s_acc, p0, CH.w, acc);
 }
 
 // minb: CTAs per SM the kernel's register budget is cut for (2, 3 or 4;
-// more CTAs hide more gather latency, fewer keep more values in registers)
-template <bool F64>
-static void launch_cell_pass_t(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
-                               const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
-                               const int4* leaves, const int4* chunks, const int* chunk_cta, int nchunks,
-                               const int* pfirst, const PairInfo* pairs, float4* cbox, double* cbox64,
-                               float4* tnode, double* tnode64, unsigned long long* acc) {
-  if (minb <= 2)
-    k_cell_pass<F64, 2><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
-                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
-  else if (minb == 3)
-    k_cell_pass<F64, 3><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
-                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
-  else
-    k_cell_pass<F64, 4><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst,
-                                                 pairs, cbox, cbox64, tnode, tnode64, acc);
+// more CTAs hide more load latency, fewer keep more values in registers).
+// The dynamic shared memory (the chunk's pairs) may take the static part
+// over 48 KB, so the kernels opt in to the size they are launched with.
+template <class K>
+static void set_smem(K kern, size_t smem) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void launch_cell_pass(bool f64, int minb, int grid, size_t smem, cudaStream_t st, const double* x, const float4* xf,
-                      const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves,
-                      const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
-                      const PairInfo* pairs, float4* cbox, double* cbox64, float4* tnode, double* tnode64,
-                      unsigned long long* acc) {
-  if (f64)
-    launch_cell_pass_t<true>(minb, grid, smem, st, x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
-                             pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
-  else
-    launch_cell_pass_t<false>(minb, grid, smem, st, x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks,
-                              pfirst, pairs, cbox, cbox64, tnode, tnode64, acc);
+void launch_cell_pass32(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* grp,
+                        const int* grp_nodes, const uint2* cell_lidx, const int4* chunks, const int* chunk_cta,
+                        int nchunks, const int* pfirst, const PairInfo* pairs, uint2* qbox, float4* tnode,
+                        unsigned long long* acc) {
+#define TB_CP32(MB)                                                                                              \
+  do {                                                                                                           \
+    set_smem(k_cell_pass32<MB>, smem);                                                                           \
+    k_cell_pass32<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, grp, grp_nodes, cell_lidx, chunks, \
+                                               chunk_cta, nchunks, pfirst, pairs, qbox, tnode, acc);             \
+  } while (0)
+  if (minb <= 2) TB_CP32(2);
+  else if (minb == 3) TB_CP32(3);
+  else TB_CP32(4);
+#undef TB_CP32
+}
+
+void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
+                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
+                        float4* tnode, double* tnode64, unsigned long long* acc) {
+#define TB_CP64(MB)                                                                                       \
+  do {                                                                                                    \
+    set_smem(k_cell_pass64<MB>, smem);                                                                    \
+    k_cell_pass64<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, \
+                                               pfirst, pairs, cbox64, tnode, tnode64, acc);               \
+  } while (0)
+  if (minb <= 2) TB_CP64(2);
+  else if (minb == 3) TB_CP64(3);
+  else TB_CP64(4);
+#undef TB_CP64
 }
 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
 // rounded outward), so the query gathering can skip tiles far from a region.
-__global__ void __launch_bounds__(256) k_node_tiles(const float4* __restrict__ xf, const BlockInfo* __restrict__ bi,
+__global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
                                                     int nb, const long long* __restrict__ tile_base,
                                                     float4* __restrict__ tbox, const int* __restrict__ node_order) {
   __shared__ float sh[6][8];
@@ -1005,7 +1103,8 @@ __global__ void __launch_bounds__(256) k_node_tiles(const float4* __restrict__ x
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
-    const float4 v = xf[node_order[B.node_off + i]];
+    const double* p = x + 3 * (long long)node_order[B.node_off + i];
+    const float4 v = make_float4(__double2float_rn(p[0]), __double2float_rn(p[1]), __double2float_rn(p[2]), 0.f);
     lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
     hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
   }
@@ -1323,7 +1422,7 @@ __device__ __forceinline__ int pick4(int k, int a0, int a1, int a2, int a3) {
 // deepest non-empty mask.
 template <int FORM>
 __global__ void __launch_bounds__(256) k_traverse(
-    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const uint2* __restrict__ qbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
     int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf) {
@@ -1346,12 +1445,12 @@ __global__ void __launch_bounds__(256) k_traverse(
       plo[k] = p32 - e;
       phi[k] = p32 + e;
     }
-    // cells [c0, c0 + nc) of a hit leaf (1 <= nc <= kMaxLeafCells).  FP32
-    // boxes: the loop is unrolled and every slot reads a cell of the leaf
-    // (the last one again past nc), so all the box loads are issued before
-    // the first test, one memory round trip per leaf.  Hits are added in
-    // cell order.
-    auto leaf_cells = [&](int c0, int ncell) {
+    // cells [c0, c0 + nc) of a hit leaf in tree slot sl (1 <= nc <=
+    // kMaxLeafCells).  Split form: 8-byte cell boxes coded inside the leaf's
+    // box; the loop is unrolled and every slot reads a cell of the leaf (the
+    // last one again past nc), so all the loads are issued before the first
+    // test, one memory round trip per leaf.  Hits are added in cell order.
+    auto leaf_cells = [&](int c0, int ncell, long long sl) {
       unsigned hit = 0;
       if (FORM == 0) {  // (FP64 boxes: 48 B a cell, tested one at a time)
         for (int j = 0; j < ncell; j++) {
@@ -1360,15 +1459,27 @@ __global__ void __launch_bounds__(256) k_traverse(
           hit |= (unsigned)in_box64(p, lo, hi) << j;
         }
       } else {
-        float4 A[kMaxLeafCells], B[kMaxLeafCells];
+        uint2 Q[kMaxLeafCells];
 #pragma unroll
-        for (int j = 0; j < kMaxLeafCells; j++) {
-          const long long c = c0 + min(j, ncell - 1);
-          A[j] = cbox[2 * c];
-          B[j] = cbox[2 * c + 1];
+        for (int j = 0; j < kMaxLeafCells; j++) Q[j] = qbox[c0 + min(j, ncell - 1)];
+        const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
+        const float L[3] = {A.x, A.y, A.z}, H[3] = {A.w, B.x, B.y};
+        float sdn[3], sup[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          sdn[k] = qstep_dn(L[k], H[k]);
+          sup[k] = qstep_up(L[k], H[k]);
         }
 #pragma unroll
-        for (int j = 0; j < kMaxLeafCells; j++) hit |= (unsigned)(hit_ab(A[j], B[j], plo, phi) && j < ncell) << j;
+        for (int j = 0; j < kMaxLeafCells; j++) {
+          const unsigned a = Q[j].x, b = Q[j].y;
+          const bool h = qdec_lo(a & 255u, L[0], sdn[0]) <= phi[0] && qdec_lo((a >> 8) & 255u, L[1], sdn[1]) <= phi[1] &&
+                         qdec_lo((a >> 16) & 255u, L[2], sdn[2]) <= phi[2] &&
+                         qdec_hi(a >> 24, L[0], H[0], sup[0]) >= plo[0] &&
+                         qdec_hi(b & 255u, L[1], H[1], sup[1]) >= plo[1] &&
+                         qdec_hi((b >> 8) & 255u, L[2], H[2], sup[2]) >= plo[2];
+          hit |= (unsigned)(h && j < ncell) << j;
+        }
       }
       while (hit) {
         const int j = __ffs(hit) - 1;
@@ -1380,7 +1491,7 @@ __global__ void __launch_bounds__(256) k_traverse(
       const float4 RA = tnode[2 * root], RB = tnode[2 * root + 1];
       const bool rh = (FORM == 0) ? hit64(tnode64, root, p) : hit_ab(RA, RB, plo, phi);
       const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
-      if (rh && rcnt > 0) leaf_cells(rlink, rcnt);
+      if (rh && rcnt > 0) leaf_cells(rlink, rcnt, root);
       if (rh && rcnt < 0) {
         int base = rlink, depth = 0;
         unsigned long long tr0 = 0, tr1 = 0;  // masks of depths 0-15 and 16-31
@@ -1402,7 +1513,7 @@ __global__ void __launch_bounds__(256) k_traverse(
           while (ml) {
             const int k = __ffs(ml) - 1;
             ml &= ml - 1;
-            leaf_cells(pick4(k, lk[0], lk[1], lk[2], lk[3]), pick4(k, lc[0], lc[1], lc[2], lc[3]));
+            leaf_cells(pick4(k, lk[0], lk[1], lk[2], lk[3]), pick4(k, lc[0], lc[1], lc[2], lc[3]), base + k);
           }
           if (mi) {
             const int c = __ffs(mi) - 1;
@@ -1598,14 +1709,14 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 }
 
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf) {
   if (form == 0)
-    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf);
   else
-    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf);
 }
 

@@ -494,13 +494,13 @@ __global__ void k_gather_cells_i32(const int* __restrict__ src, const int* __res
 __global__ void k_interp_gather(const int* __restrict__ it_node, const double* __restrict__ it_w,
                                 const int* __restrict__ it_don, const unsigned char* __restrict__ it_nv,
                                 const unsigned char* __restrict__ it_cancel, const int* __restrict__ rcount,
-                                const BlockInfo* __restrict__ bi, const double* __restrict__ q, int nvar,
+                                const BlockInfo* __restrict__ bi, const double* const* __restrict__ qptr, int nvar,
                                 int interptype, double* __restrict__ vals) {
   const int R = *rcount;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
     if (it_cancel[r]) continue;
     const BlockInfo& D = bi[it_don[r]];
-    const double* qb = q + (long long)D.node_off * nvar;
+    const double* qb = qptr[it_don[r]];
     const int nv = it_nv[r];
     for (int k0 = 0; k0 < nvar; k0 += 8) {
       const int kn = min(8, nvar - k0);
@@ -527,14 +527,15 @@ __global__ void k_interp_gather(const int* __restrict__ it_node, const double* _
 __global__ void k_interp_scatter(const int* __restrict__ it_rec, const unsigned char* __restrict__ it_cancel,
                                  const int* __restrict__ rcount, const blk_t* __restrict__ node_blk,
                                  const BlockInfo* __restrict__ bi, const double* __restrict__ vals, int nvar,
-                                 int interptype, double* __restrict__ q) {
+                                 int interptype, double* const* __restrict__ qptr) {
   const int R = *rcount;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
     if (it_cancel[r]) continue;
     const int g = it_rec[r];
-    const BlockInfo& B = bi[node_blk[g]];
+    const int rb = node_blk[g];
+    const BlockInfo& B = bi[rb];
     const int local = g - B.node_off;
-    double* qb = q + (long long)B.node_off * nvar;
+    double* qb = qptr[rb];
     for (int k = 0; k < nvar; k++) {
       if (interptype == 0) qb[(long long)local * nvar + k] = vals[(long long)r * nvar + k];
       else qb[(long long)k * B.nnodes + local] = vals[(long long)r * nvar + k];
