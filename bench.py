@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--impl", default="tioga_b200", choices=["tioga_b200", "reference"])
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the mismatch count against the compiled reference's digests")
     p.add_argument("--cpu-reps", type=int, default=3)
     p.add_argument("--size", default="full", choices=["full", "medium", "small"],
                    help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
@@ -223,6 +225,52 @@ def autotune(lib, tb, reps: int = 2) -> dict:
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def parity_vs_reference(lib, tb, system, fixture: str, q_seed: int, precisions=(1, 0)):
+    """Mismatches of the timed configuration against the compiled reference's
+    digests (tests/golden/make_digests.py): iblank per node, getdonorinfo
+    records per record, updated fields per 4096 values, for each precision
+    form, after one more connectivity call with the caller's host iblank
+    arrays.  None when no fixture covers this configuration."""
+    from tests.golden import digest
+    path = os.path.join(GOLDEN, fixture + ".npz")
+    if not os.path.exists(path):
+        return None
+    fix = np.load(path)
+    if digest.input_digest(system) != str(fix["input_digest"]):
+        return {"error": "the generated mesh differs from the fixture's"}
+    q0 = cases.fields(system, nvar=5, seed=q_seed)
+    out = {"against": f"compiled reference, digests in tests/golden/{fixture}.npz", "forms": {}}
+    for b in system.blocks:
+        lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(0))
+    total = 0
+    for prec in precisions:
+        tb.set_int(lib.lib, "tioga_b200_set_precision_", prec)
+        lib.performconnectivity()
+        res = {"iblank": {}, "donors": {}, "q": {}}
+        for b in system.blocks:
+            res["iblank"][b.tag] = lib.iblank(b.tag).copy()
+            res["donors"][b.tag] = lib.getdonorinfo(b.tag)
+        qs = [np.array(q, dtype=np.float64, copy=True) for q in q0]
+        for b, q in zip(system.blocks, qs):
+            lib.registersolution(b.tag, q)
+        lib.dataupdate_mb(5, "row")
+        for b, q in zip(system.blocks, qs):
+            res["q"][b.tag] = q
+        c = digest.compare(fix, system, res)
+        st = tb.stats(lib.lib)
+        name = {0: "fp64", 1: "split"}.get(prec, str(prec))
+        out["forms"][name] = {"iblank_mismatches": c["iblank"], "record_mismatches": c["records"],
+                              "records": c["record_total"], "field_chunk_mismatches": c["q_chunks"],
+                              "ties": st["nties"]}
+        total += c["iblank"] + c["records"] + c["q_chunks"]
+    out["mismatches"] = total
+    out["ties"] = max(f["ties"] for f in out["forms"].values())
+    return out
+
+
 def run_gpu(args, ws, rank, local, dist):
     import torch
 
@@ -348,6 +396,9 @@ def run_gpu(args, ws, rank, local, dist):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    # parity of the timed configuration against the compiled reference
+    if args.size == "full" and args.seed == 1 and not args.no_parity:
+        out["parity"] = parity_vs_reference(lib, tb, psys, "cfg1_full", 21)
     out["dataupdate"] = time_dataupdate(lib, system, stream, st["nreceptor"], args.steps, args.warmup)
     lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
     lib.delete()

@@ -290,8 +290,10 @@ void tioga_b200_set_stream_(void *stream);
  * whose time step runs inside a captured CUDA graph (cudaMalloc is not
  * allowed while a stream is captured), or one whose memory pool must not be
  * disturbed by cudaMalloc's device-wide synchronisation.  Stencil r has
- * d_nweights[r] <= 8 entries at d_inode[9r+m] (node index into d_q) with
- * weights d_weights[9r+m], and writes node d_receptor[r]; interptype 0 is
+ * d_nweights[r] entries, 1 to 8 (a record outside that range is ignored and
+ * its receptor keeps its value), at d_inode[9r+m] (node index into d_q) with
+ * weights d_weights[9r+m], and writes node d_receptor[r]; receptors must be
+ * distinct (as getdonorinfo's are), or their writes race; interptype 0 is
  * row layout (q[node*nvar+k]), 1 column (q[k*nnodes+node]).  The
  * gather-to-scatter staging lives in a fixed device array of 2^20 doubles:
  * nrec*nvar above that is rejected (-1).  The first call on a device looks up

@@ -4,7 +4,8 @@ It serves callers that cannot allocate device memory while they update their
 fields -- a solver stepping inside a captured CUDA graph, or one whose memory
 pool must not see cudaMalloc's device-wide synchronisation.  Checked through
 the C ABI against the regular data update (tioga_dataupdate_mb_) on the same
-connectivity, bit for bit, on two updates in a row; the staging array is
+connectivity, bit for bit, on two updates in a row in the row and the column
+layouts; the staging array is
 shared by all calls, so the second call also shows that nothing is left over
 from the first.  The file name sorts last so a stop-at-first-failure run has
 run every other test before this one.
@@ -90,6 +91,29 @@ def test_noalloc_matches_dataupdate_twice():
         torch.cuda.synchronize()
         got = d_q.cpu().numpy()
         assert np.array_equal(got.view(np.int64), expect.view(np.int64))
+    # the column layout (q[k*nnodes+node]) against tioga_dataupdate_mb_'s, twice
+    qc = [np.array(q, copy=True) for q in q0]  # read as column-layout arrays of each block
+    for b, q in zip(system.blocks, qc):
+        t.registersolution(b.tag, q)
+    expect_col = []
+    for _ in range(2):
+        t.dataupdate_mb(nvar, "column")
+        flat = np.zeros(off * nvar)
+        for b, q in zip(system.blocks, qc):
+            for k in range(nvar):
+                flat[k * off + offsets[b.tag]:k * off + offsets[b.tag] + b.nnodes] = q[k * b.nnodes:(k + 1) * b.nnodes]
+        expect_col.append(flat)
+    flat0 = np.zeros(off * nvar)
+    for b, q in zip(system.blocks, q0):
+        for k in range(nvar):
+            flat0[k * off + offsets[b.tag]:k * off + offsets[b.tag] + b.nnodes] = q[k * b.nnodes:(k + 1) * b.nnodes]
+    d_qc = torch.from_numpy(flat0).to(dev)
+    for expect in expect_col:
+        rc = fn(d_inode.data_ptr(), d_w.data_ptr(), d_nw.data_ptr(), d_recv.data_ptr(), nrec,
+                d_qc.data_ptr(), off, nvar, 1, stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(d_qc.cpu().numpy().view(np.int64), expect.view(np.int64))
     # sizes beyond the fixed staging array are refused and leave q untouched
     before = d_q.cpu().numpy().copy()
     big = NOALLOC_MAX_VALUES // nvar + 1

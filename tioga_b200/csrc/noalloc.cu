@@ -17,7 +17,14 @@
 // serialised by the caller, e.g. by issuing them on one stream.  A call fully
 // writes every staging slot it later reads, so nothing is carried over from
 // the previous call and nothing needs clearing.
+//
+// Stencils hold 1 to 8 weights (d_nweights[r]); a record outside that range is
+// ignored (its receptor keeps its value) rather than summed in part.  Receptor
+// entries must be distinct, as tioga_getdonorinfo_'s are: two records that name
+// the same receptor node would race in the scatter.
 #include <stdio.h>
+
+#include <mutex>
 
 #include "common.cuh"
 
@@ -30,8 +37,10 @@ static __device__ __align__(256) double g_noalloc_vals[kNoAllocMaxValues];
 
 // Device address of g_noalloc_vals per device ordinal.  In host code the
 // symbol's name is only a host-side stand-in, so the address is looked up once
-// per device with cudaGetSymbolAddress while that device is current.
+// per device with cudaGetSymbolAddress while that device is current; the
+// mutex makes the first calls of several host threads on one device safe.
 double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
 
 // qq[k] = sum over the stencil of q[donor, k] * w, accumulated from 0 in
 // stencil order (the same order as the reference's getInterpolatedSolution,
@@ -42,9 +51,10 @@ __global__ void k_noalloc_gather(const int* __restrict__ inode, const double* __
                                  long long nnodes, int nvar, int interptype, double* __restrict__ vals) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrec; r += gridDim.x * blockDim.x) {
     const int n = nw[r];
+    if (n < 1 || n > 8) continue;  // ignored record (k_noalloc_scatter skips it too)
     for (int k = 0; k < nvar; k++) {
       double acc = 0;
-      for (int m = 0; m < n && m < 8; m++) {
+      for (int m = 0; m < n; m++) {
         const long long node = inode[9 * (long long)r + m];
         const double qv = (interptype == 0) ? q[node * nvar + k] : q[(long long)k * nnodes + node];
         acc += qv * w[9 * (long long)r + m];
@@ -54,9 +64,11 @@ __global__ void k_noalloc_gather(const int* __restrict__ inode, const double* __
   }
 }
 
-__global__ void k_noalloc_scatter(const int* __restrict__ recv, int nrec, const double* __restrict__ vals,
-                                  long long nnodes, int nvar, int interptype, double* __restrict__ q) {
+__global__ void k_noalloc_scatter(const int* __restrict__ recv, const int* __restrict__ nw, int nrec,
+                                  const double* __restrict__ vals, long long nnodes, int nvar, int interptype,
+                                  double* __restrict__ q) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrec; r += gridDim.x * blockDim.x) {
+    if (nw[r] < 1 || nw[r] > 8) continue;
     const long long node = recv[r];
     for (int k = 0; k < nvar; k++) {
       const double v = vals[(long long)r * nvar + k];
@@ -95,24 +107,36 @@ extern "C" int tioga_b200_interpolate_noalloc_(const int* d_inode, const double*
             cudaGetErrorString(e));
     return -2;
   }
-  if (!g_noalloc_ptr[dev]) {
-    // set-up on the first call on this device (make it before any capture)
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_vals);
-    if (e != cudaSuccess || !p) {
-      fprintf(stderr, "#tioga_b200: interpolate_noalloc: cudaGetSymbolAddress failed: %s\n",
-              cudaGetErrorString(e));
-      return -2;
-    }
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
-  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* vals = nullptr;
+  {
+    // set-up on the first call on this device: make that call before any
+    // stream capture begins
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_vals);
+      if (e != cudaSuccess || !p) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st, &cs);
+        fprintf(stderr, "#tioga_b200: interpolate_noalloc: cudaGetSymbolAddress failed: %s%s\n",
+                cudaGetErrorString(e),
+                cs != cudaStreamCaptureStatusNone
+                    ? " (this was the first call on the device and a stream capture is active: make one call "
+                      "before capturing)"
+                    : "");
+        return -2;
+      }
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    vals = g_noalloc_ptr[dev];
+  }
   const int threads = 128;
   const int blocks = tb::grid_for(nrec, threads);
   k_noalloc_gather<<<blocks, threads, 0, st>>>(d_inode, d_weights, d_nweights, nrec, d_q, nnodes, nvar,
-                                               interptype, g_noalloc_ptr[dev]);
-  k_noalloc_scatter<<<blocks, threads, 0, st>>>(d_receptor, nrec, g_noalloc_ptr[dev], nnodes, nvar,
-                                                interptype, d_q);
+                                               interptype, vals);
+  k_noalloc_scatter<<<blocks, threads, 0, st>>>(d_receptor, d_nweights, nrec, vals, nnodes, nvar, interptype,
+                                                d_q);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     fprintf(stderr, "#tioga_b200: interpolate_noalloc: launch failed: %s\n", cudaGetErrorString(e));
