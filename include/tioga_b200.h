@@ -229,8 +229,17 @@ long long tioga_b200_server_submit_fields(void *srv, int sys, int nmoves, const 
 /* Blocks until the request is done: times_ms = (submit -> done, submit ->
  * start, start -> done, then the host time of its preprocess, connectivity
  * and data update), counts = (query points, receptors, holes, status).
- * Returns the request's status (0 = success). */
+ * Returns the request's status: 0 = success, a negative engine error code,
+ * -3 = the system alone needs more device memory than the budget (refused,
+ * nothing ran), -4 = cancelled before it started; -1 for an unknown ticket. */
 int tioga_b200_server_wait(void *srv, long long ticket, double times_ms[6], long long counts[4]);
+/* tioga_b200_server_wait for at most timeout_ms: -5 when the request is not
+ * done by then (it goes on, and the ticket stays valid for another wait). */
+int tioga_b200_server_wait_timeout(void *srv, long long ticket, double timeout_ms, double times_ms[6],
+                                   long long counts[4]);
+/* Cancel a request that has not started: it completes with status -4.
+ * Returns 0, or -1 when the request is running, done or unknown. */
+int tioga_b200_server_cancel(void *srv, long long ticket);
 /* [0] resident systems, [1] device bytes they hold, [2] admissions,
  * [3] evictions, [4] completed requests, [5] queued requests, [6] budget,
  * [7] peak device bytes held, [8] bytes reserved in the server's memory
@@ -303,6 +312,12 @@ void tioga_b200_set_stream_(void *stream);
 int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights, const int *d_nweights,
                                     const int *d_receptor, int nrec, double *d_q, long long nnodes,
                                     int nvar, int interptype, void *stream);
+/* For tests of the error paths: lower one device bound to *value (0 restores
+ * it).  *which 0 = rounds of a hole-map fill (at the bound the fill stops and
+ * error bit 8 is reported), 1 = donor-record capacity (error bit 2).  The
+ * connectivity call then returns its error bits through
+ * tioga_b200_last_error(); no counterpart in TIOGA. */
+void tioga_b200_set_test_bound_(int *which, int *value);
 /* Device time (ms) of the last connectivity call per phase: [0] coordinate
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,

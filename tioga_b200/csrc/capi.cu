@@ -306,6 +306,10 @@ void tioga_b200_stats_(long long out[16]) {
   out[15] = s.ngroup_nodes;
 }
 
+void tioga_b200_set_test_bound_(int* which, int* value) {
+  if (ready("tioga_b200_set_test_bound_")) set_rc(g_tg->set_test_bound(*which, *value));
+}
+
 void tioga_b200_autotune_(int* reps) {
   if (ready("tioga_b200_autotune_")) set_rc(g_tg->autotune(*reps));
 }

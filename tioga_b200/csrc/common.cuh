@@ -30,7 +30,11 @@ enum : unsigned {
   kErrFloodFillBound = 1u << 3,
   kErrBadCell = 1u << 4,
   kErrBadIndex = 1u << 5,     // an index outside its array (skipped)
+  kErrBadInput = 1u << 6,     // a caller's node index out of range or a non-finite coordinate
 };
+// error bits after which a connectivity result is not the reference's
+constexpr unsigned kErrFatal = kErrTraversalOverflow | kErrCapacity | kErrWeightRange | kErrFloodFillBound |
+                               kErrBadIndex | kErrBadInput;
 
 #define TB_CUDA(call)                                                              \
   do {                                                                             \

@@ -53,7 +53,8 @@ Engine::~Engine() {
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
   reset_t_.release(); interp2rec_.release(); it_node_.release(); it_w_.release(); it_rec_.release();
   it_don_.release(); it_nv_.release(); it_cancel_.release(); rres_.release(); q_.release();
-  qvals_.release(); cub_tmp_.release(); red_.release(); err_.release(); counters_.release();
+  qvals_.release(); d_qptr_.release(); cub_tmp_.release(); red_.release(); err_.release(); coord_err_.release();
+  counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
   d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
   rf_red_.release(); rf_tmp_.release(); rf_was_.release();
@@ -301,28 +302,38 @@ int Engine::upload_topology() {
       size_t n = (size_t)H.nc[t] * H.nv[t];
       if (n == 0) continue;
       TB_CUDA(cudaMemcpyAsync(stg.p, H.hconn[t], n * sizeof(int), cudaMemcpyHostToDevice, stream_));
-      k_conn_convert<<<grid_for(H.nc[t], kT), kT, 0, stream_>>>(stg.p, H.nc[t], H.nv[t], B.node_off,
+      k_conn_convert<<<grid_for(H.nc[t], kT), kT, 0, stream_>>>(stg.p, H.nc[t], H.nv[t], B.node_off, H.nnodes,
                                                                 B.cell_off + B.type_off[t], b, conn8_.p,
-                                                                cell_nv_.p, cell_blk_.p);
+                                                                cell_nv_.p, cell_blk_.p, err_.p);
       TB_LAUNCHED("k_conn_convert");
       TB_CUDA(cudaStreamSynchronize(stream_));  // the staging buffer is reused
     }
     if (H.nwbc > 0) {
       TB_CUDA(cudaMemcpyAsync(stg.p, H.hwbc, H.nwbc * sizeof(int), cudaMemcpyHostToDevice, stream_));
-      k_mark_list<<<grid_for(H.nwbc, kT), kT, 0, stream_>>>(stg.p, H.nwbc, B.node_off, wall_list_.p,
-                                                            B.wall_off, wallf_.p);
+      k_mark_list<<<grid_for(H.nwbc, kT), kT, 0, stream_>>>(stg.p, H.nwbc, B.node_off, H.nnodes, wall_list_.p,
+                                                            B.wall_off, wallf_.p, err_.p);
       TB_LAUNCHED("k_mark_list");
       TB_CUDA(cudaStreamSynchronize(stream_));
     }
     if (H.nobc > 0) {
       TB_CUDA(cudaMemcpyAsync(stg.p, H.hobc, H.nobc * sizeof(int), cudaMemcpyHostToDevice, stream_));
-      k_mark_list<<<grid_for(H.nobc, kT), kT, 0, stream_>>>(stg.p, H.nobc, B.node_off, obc_list_.p,
-                                                            B.obc_off, obcf_.p);
+      k_mark_list<<<grid_for(H.nobc, kT), kT, 0, stream_>>>(stg.p, H.nobc, B.node_off, H.nnodes, obc_list_.p,
+                                                            B.obc_off, obcf_.p, err_.p);
       TB_LAUNCHED("k_mark_list");
       TB_CUDA(cudaStreamSynchronize(stream_));
     }
   }
   stg.release();
+  {
+    unsigned e = 0;
+    TB_CUDA(cudaMemcpyAsync(&e, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    if (e & kErrBadInput) {
+      fprintf(stderr, "#tioga_b200: a connectivity, wall or overset-boundary node index lies outside 1..nnodes\n");
+      TB_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), stream_));
+      return -1;
+    }
+  }
   TB_TRY(build_csr());
   // block pairs that may intersect: different mesh tags of one system, donor
   // outer, receptor inner (exchangeBoxes.C:133-160)
@@ -388,6 +399,26 @@ int Engine::upload_coords() {
                             3 * (size_t)hb_[b].nnodes * sizeof(double), cudaMemcpyHostToDevice, stream_));
   coords_on_device_ = true;
   gate_valid_ = false;  // the caller may have moved the nodes any way
+  return check_coords();
+}
+
+// Refuse non-finite coordinates before any kernel derives an index (hole-map
+// cells, Morton keys) from them.
+int Engine::check_coords() {
+  TB_CUDA(coord_err_.ensure(1));
+  TB_CUDA(cudaMemsetAsync(coord_err_.p, 0, sizeof(unsigned), stream_));
+  if (ntot_ > 0) {
+    k_check_finite<<<grid_for(3 * ntot_, kT), kT, 0, stream_>>>(x_.p, 3 * ntot_, coord_err_.p);
+    TB_LAUNCHED("k_check_finite");
+  }
+  unsigned e = 0;
+  TB_CUDA(cudaMemcpyAsync(&e, coord_err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (e) {
+    fprintf(stderr, "#tioga_b200: a node coordinate is not finite (NaN or infinite)\n");
+    coords_on_device_ = false;
+    return -1;
+  }
   return 0;
 }
 
@@ -869,7 +900,7 @@ int Engine::run_holemaps() {
   }
   if (planar) {  // fill and final map in one pass
     k_holemap_fill_bits<<<dim3(std::min(maxpl, 148 * 4), nh), 256, 0, stream_>>>(
-        hm_state_.p, d_hm_.p, kHoleMapCap, wall_box_.p, wall_box_first_.p, isym, err_.p);
+        hm_state_.p, d_hm_.p, kHoleMapCap, wall_box_.p, wall_box_first_.p, isym, test_fill_rounds_, err_.p);
     TB_LAUNCHED("k_holemap_fill_bits");
   } else {
     k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, stream_>>>(hm_state_.p, d_hm_.p,
@@ -1161,7 +1192,7 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
     launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
-                    slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p);
+                    slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p);
     TB_LAUNCHED("k_traverse");
     TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
@@ -1496,6 +1527,7 @@ int Engine::run_donors() {
   TB_CUDA(rcount_.ensure(2));
   TB_CUDA(cudaMemsetAsync(rcount_.p, 0, 2 * sizeof(int), stream_));
   long long rcap = std::max<long long>(1, std::min<long long>(ntot_, nq_));
+  if (test_rcap_ > 0) rcap = std::min<long long>(rcap, test_rcap_);  // tioga_b200_set_test_bound_
   TB_CUDA(rkey_.ensure(rcap));
   TB_CUDA(rkey_alt_.ensure(rcap));
   TB_CUDA(rval_.ensure(rcap));
@@ -1779,6 +1811,7 @@ int Engine::connectivity() {
   interps_fetched_ = false;
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
+  TB_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), stream_));  // this call's device errors only
   if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
   int rc = run_holemaps();
@@ -1852,10 +1885,15 @@ int Engine::connectivity() {
   if (err & kErrWeightRange)
     fprintf(stderr, "#tioga_b200: an interpolation weight fell outside [-0.2,1.2] (the reference aborts)\n");
   if (err & kErrFloodFillBound) fprintf(stderr, "#tioga_b200: hole-map fill hit its round limit\n");
+  if (err & kErrCapacity) fprintf(stderr, "#tioga_b200: donor records overflowed their capacity\n");
+  if (err & kErrTraversalOverflow) fprintf(stderr, "#tioga_b200: a tree walk went deeper than its stack\n");
+  if (err & kErrBadIndex) fprintf(stderr, "#tioga_b200: an index fell outside its array and was skipped\n");
   connected_ = true;
   ihigh_global_ = ihigh_;  // tioga.C:138
   ho_done_ = false;
-  return 0;
+  // a device bound that ran out or a weight the reference would abort on:
+  // the call completes, its error bits go to tioga_b200_last_error()
+  return (int)(err & kErrFatal);
 }
 
 // ---------------------------------------------------------------------------

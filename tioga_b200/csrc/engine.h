@@ -237,6 +237,14 @@ class Engine {
   // high-order path
   int set_highorder(int tag, int p, const double* xdof);
   void set_highorder_callbacks() { ihigh_ = true; }
+  // Lowered device bounds for tests of the error paths (0 = the normal
+  // bound): which 0 = hole-map fill rounds, 1 = donor-record capacity.
+  int set_test_bound(int which, int value) {
+    if (which == 0) test_fill_rounds_ = value;
+    else if (which == 1) test_rcap_ = value;
+    else return -1;
+    return 0;
+  }
   int connectivity_highorder();
   int dataupdate_highorder(int nvar, int interptype);
   int point_donors(int tag, int* out, double* w);
@@ -313,6 +321,7 @@ class Engine {
   int compute_obbs();
   int build_tree_topology();
   int upload_coords();
+  int check_coords();
   int run_holemaps();
   int preprocess_resolutions();
   int run_pairs_and_refit();
@@ -491,6 +500,8 @@ class Engine {
   DBuf<unsigned char> cub_tmp_;
   DBuf<double> red_;
   DBuf<unsigned> err_;
+  DBuf<unsigned> coord_err_;  // non-finite coordinate flag (check_coords)
+  int test_fill_rounds_ = 0, test_rcap_ = 0;  // set_test_bound
   DBuf<unsigned long long> counters_;
   DBuf<unsigned long long> mkey_, mkey_alt_;
   DBuf<int> mval_alt_;

@@ -87,11 +87,12 @@ __device__ __forceinline__ int block_of_tile(const long long* __restrict__ tile_
 }
 
 // ---- preprocess (kernels_pre.cu) ----
-__global__ void k_conn_convert(const int* raw, int nc, int nv, int node_off, int cell_base, int blk,
-                               int* conn8, unsigned char* cell_nv, blk_t* cell_blk);
+__global__ void k_conn_convert(const int* raw, int nc, int nv, int node_off, int nnodes, int cell_base, int blk,
+                               int* conn8, unsigned char* cell_nv, blk_t* cell_blk, unsigned* err);
+__global__ void k_check_finite(const double* x, long long n, unsigned* err);
 __global__ void k_node_blk(int node_off, int nnodes, int blk, blk_t* node_blk);
-__global__ void k_mark_list(const int* list, int n, int node_off, int* glist, int goff,
-                            unsigned char* flag);
+__global__ void k_mark_list(const int* list, int n, int node_off, int nnodes, int* glist, int goff,
+                            unsigned char* flag, unsigned* err);
 __global__ void k_csr_count(const int* conn8, const unsigned char* cell_nv, long long ctot, int* deg);
 __global__ void k_csr_fill(const int* conn8, const unsigned char* cell_nv, long long ctot,
                            const int* off, int* cursor, int* cells);
@@ -126,7 +127,7 @@ __global__ void k_wall_cell_flags(const int* conn8, const unsigned char* cell_nv
                                   const BlockInfo* bi, const unsigned char* wallf, long long ctot, int* flag);
 __global__ void k_wall_cell_list(const int* flag, const int* off, long long ctot, int* list);
 __global__ void k_holemap_fill_bits(unsigned char* sam, const HoleMapInfo* hm, size_t cap, const unsigned long long* box,
-                                    const int* box_first, int isym, unsigned* err);
+                                    const int* box_first, int isym, int round_cap, unsigned* err);
 __global__ void k_wall_map_first(const int* wall_cells, int nwc, const blk_t* cell_blk, const BlockInfo* bi,
                                  int* first);
 __global__ void k_holemap_boxes(const double* x, const int* conn8, const unsigned char* cell_nv, const int* wall_cells,
@@ -187,7 +188,7 @@ __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairIn
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
-                     int ovf_cap, unsigned* novf);
+                     int ovf_cap, unsigned* novf, unsigned* err);
 __global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,
                                     const int3* ovf, const unsigned* novf, int ovf_cap, int2* cand);
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,

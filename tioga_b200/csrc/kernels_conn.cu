@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __r
                                                            const HoleMapInfo* __restrict__ hm_all, size_t cap,
                                                            const unsigned long long* __restrict__ box,
                                                            const int* __restrict__ box_first, int isym,
-                                                           unsigned* __restrict__ err) {
+                                                           int round_cap, unsigned* __restrict__ err) {
   __shared__ unsigned pr[kHL][kHW], fr[kHL][kHW], pc[kHL][kHW], fc[kHL][kHW];
   const HoleMapInfo h = hm_all[blockIdx.y];
   unsigned char* __restrict__ sam = sam_all + (size_t)blockIdx.y * cap;
@@ -326,7 +326,9 @@ __global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __r
       if (!__syncthreads_or(ch)) break;  // fr already holds this state
       bit_transpose(fc, n0, fr, n1);
       __syncthreads();
-      if (rounds > n0 * n1 + 2) {
+      // a fill needs fewer rounds than the plane has cells; round_cap > 0
+      // lowers the bound to round_cap rounds (tioga_b200_set_test_bound_)
+      if (round_cap > 0 ? rounds + 1 >= round_cap : rounds > n0 * n1 + 2) {
         if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
         break;
       }
@@ -1425,7 +1427,8 @@ __global__ void __launch_bounds__(256) k_traverse(
     const double* __restrict__ x, const BlockInfo* __restrict__ bi, const uint2* __restrict__ qbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
-    int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf) {
+    int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf,
+    unsigned* __restrict__ err) {
   __shared__ int s_base[kMaxTreeDepth][256];
   const int t = threadIdx.x;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
@@ -1524,7 +1527,10 @@ __global__ void __launch_bounds__(256) k_traverse(
               s_base[depth][t] = base;
             }
             base = pick4(c, lk[0], lk[1], lk[2], lk[3]);
-            depth++;
+            if (++depth >= kMaxTreeDepth) {  // deeper than the trail (the build refuses such trees)
+              atomicOr(err, kErrTraversalOverflow);
+              break;
+            }
             continue;
           }
           int d2;
@@ -1711,13 +1717,13 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
-                     int ovf_cap, unsigned* novf) {
+                     int ovf_cap, unsigned* novf, unsigned* err) {
   if (form == 0)
     k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
-                                          ovf, ovf_cap, novf);
+                                          ovf, ovf_cap, novf, err);
   else
     k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
-                                          ovf, ovf_cap, novf);
+                                          ovf, ovf_cap, novf, err);
 }
 
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,

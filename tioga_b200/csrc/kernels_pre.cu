@@ -8,15 +8,26 @@ namespace tb {
 // ---------------------------------------------------------------------------
 // connectivity: 1-based per-type arrays -> padded 8-wide global node ids
 // ---------------------------------------------------------------------------
-__global__ void k_conn_convert(const int* __restrict__ raw, int nc, int nv, int node_off,
+// 1-based caller connectivity -> padded global ids.  An index outside
+// 1..nnodes is replaced by the block's first node and reported (kErrBadInput):
+// the registration then fails before any kernel reads the cell.
+__global__ void k_conn_convert(const int* __restrict__ raw, int nc, int nv, int node_off, int nnodes,
                                int cell_base, int blk, int* __restrict__ conn8,
-                               unsigned char* __restrict__ cell_nv, blk_t* __restrict__ cell_blk) {
+                               unsigned char* __restrict__ cell_nv, blk_t* __restrict__ cell_blk,
+                               unsigned* __restrict__ err) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc;
        i += (long long)gridDim.x * blockDim.x) {
     long long c = cell_base + i;
     int v[8];
 #pragma unroll
-    for (int m = 0; m < 8; m++) v[m] = (m < nv) ? node_off + raw[i * nv + m] - 1 : -1;
+    for (int m = 0; m < 8; m++) {
+      int r = (m < nv) ? raw[i * nv + m] : 1;
+      if (r < 1 || r > nnodes) {
+        atomicOr(err, kErrBadInput);
+        r = 1;
+      }
+      v[m] = (m < nv) ? node_off + r - 1 : -1;
+    }
     int4* dst = reinterpret_cast<int4*>(conn8 + 8 * c);
     dst[0] = make_int4(v[0], v[1], v[2], v[3]);
     dst[1] = make_int4(v[4], v[5], v[6], v[7]);
@@ -25,17 +36,34 @@ __global__ void k_conn_convert(const int* __restrict__ raw, int nc, int nv, int 
   }
 }
 
+// every coordinate finite, else kErrBadInput (the call then stops before any
+// kernel derives an index from a coordinate)
+__global__ void k_check_finite(const double* __restrict__ x, long long n, unsigned* __restrict__ err) {
+  bool bad = false;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    bad = bad || !isfinite(x[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, kErrBadInput);
+}
+
 __global__ void k_node_blk(int node_off, int nnodes, int blk, blk_t* node_blk) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nnodes;
        i += (long long)gridDim.x * blockDim.x)
     node_blk[node_off + i] = (blk_t)blk;
 }
 
-__global__ void k_mark_list(const int* __restrict__ list, int n, int node_off, int* __restrict__ glist,
-                            int goff, unsigned char* __restrict__ flag) {
+// wall or overset-boundary node list (1-based); an index outside 1..nnodes is
+// replaced by the first node and reported (kErrBadInput)
+__global__ void k_mark_list(const int* __restrict__ list, int n, int node_off, int nnodes, int* __restrict__ glist,
+                            int goff, unsigned char* __restrict__ flag, unsigned* __restrict__ err) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    int g = node_off + list[i] - 1;
+    int r = list[i];
+    if (r < 1 || r > nnodes) {
+      atomicOr(err, kErrBadInput);
+      r = 1;
+    }
+    int g = node_off + r - 1;
     glist[goff + i] = g;
     flag[g] = 1;
   }

@@ -45,6 +45,11 @@ double now_ms() {
 }
 }  // namespace
 
+// request statuses besides 0 (success) and the engine's own error codes
+constexpr int kSrvOverBudget = -3;  // the system alone needs more than the HBM budget
+constexpr int kSrvCancelled = -4;   // cancelled before it started
+constexpr int kSrvTimedOut = -5;    // a bounded wait ended first (the request goes on)
+
 struct SrvBlock {
   int tag, nnodes, ncells, nwbc, nobc, ntypes;
   double* x;
@@ -148,12 +153,18 @@ class Server {
     return r->ticket;
   }
 
-  int wait(long long ticket, double times[6], long long counts[4]) {
+  // Blocks until the request is done, or for at most timeout_ms when that is
+  // >= 0: kSrvTimedOut then, and the ticket stays valid for a later wait.
+  int wait(long long ticket, double times[6], long long counts[4], double timeout_ms = -1.0) {
     std::unique_lock<std::mutex> l(mu_);
     auto it = req_.find(ticket);
     if (it == req_.end()) return -1;
     SrvRequest* r = it->second;
-    cv_done_.wait(l, [&] { return r->done; });
+    if (timeout_ms < 0) {
+      cv_done_.wait(l, [&] { return r->done; });
+    } else if (!cv_done_.wait_for(l, std::chrono::duration<double, std::milli>(timeout_ms), [&] { return r->done; })) {
+      return kSrvTimedOut;
+    }
     if (times) {
       times[0] = r->t_done - r->t_submit;
       times[1] = r->t_start - r->t_submit;
@@ -172,6 +183,21 @@ class Server {
     req_.erase(it);
     delete r;
     return rc;
+  }
+
+  // A request that has not started is taken out of the queue and completes
+  // with kSrvCancelled; one that runs or has finished cannot be cancelled.
+  int cancel(long long ticket) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = req_.find(ticket);
+    if (it == req_.end()) return -1;
+    SrvRequest* r = it->second;
+    auto q = std::find(queue_.begin(), queue_.end(), r);
+    if (q == queue_.end()) return -1;
+    queue_.erase(q);
+    sys_[r->sys].pending--;
+    finish_unrun(r, kSrvCancelled);
+    return 0;
   }
 
   int nblocks(int sys) {
@@ -227,8 +253,16 @@ class Server {
         continue;
       }
       if (!S.eng) {
-        // a system larger than the whole budget runs once every other one is evicted
-        const long long need = std::min(budget_, S.last_bytes > 0 ? S.last_bytes : estimate(S));
+        // a system larger than the whole budget is refused (kSrvOverBudget)
+        const long long need = S.last_bytes > 0 ? S.last_bytes : estimate(S);
+        if (need > budget_) {
+          fprintf(stderr, "#tioga_b200: server: system %d needs %lld bytes, over the budget of %lld\n", r->sys,
+                  need, budget_);
+          queue_.erase(it);
+          S.pending--;
+          finish_unrun(r, kSrvOverBudget);
+          return pick(evict);
+        }
         int res = 0;
         for (auto& kv : sys_) res += (kv.second.eng != nullptr || kv.second.bytes > 0) ? 1 : 0;
         long long freed = 0;
@@ -260,6 +294,14 @@ class Server {
       return r;
     }
     return nullptr;
+  }
+
+  // under the lock: a request that will not run completes with status rc
+  void finish_unrun(SrvRequest* r, int rc) {
+    r->rc = rc;
+    r->t_start = r->t_done = now_ms();
+    r->done = true;
+    cv_done_.notify_all();
   }
 
   // The server's pool: freed buffers stay in it for the next allocation, and
@@ -493,6 +535,17 @@ long long tioga_b200_server_submit_fields(void* srv, int sys, int nmoves, const 
 int tioga_b200_server_wait(void* srv, long long ticket, double times_ms[6], long long counts[4]) {
   if (!srv) return -1;
   return static_cast<tb::Server*>(srv)->wait(ticket, times_ms, counts);
+}
+
+int tioga_b200_server_wait_timeout(void* srv, long long ticket, double timeout_ms, double times_ms[6],
+                                   long long counts[4]) {
+  if (!srv) return -1;
+  return static_cast<tb::Server*>(srv)->wait(ticket, times_ms, counts, timeout_ms < 0 ? 0.0 : timeout_ms);
+}
+
+int tioga_b200_server_cancel(void* srv, long long ticket) {
+  if (!srv) return -1;
+  return static_cast<tb::Server*>(srv)->cancel(ticket);
 }
 
 void tioga_b200_server_stats(void* srv, long long out[16]) {

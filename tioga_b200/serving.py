@@ -61,6 +61,10 @@ class Server:
         L.tioga_b200_server_submit_fields.argtypes = [_P, C.c_int, C.c_int, _P, _P, C.c_int, _P, C.c_int, _P]
         L.tioga_b200_server_wait.restype = C.c_int
         L.tioga_b200_server_wait.argtypes = [_P, C.c_longlong, _P, _P]
+        L.tioga_b200_server_wait_timeout.restype = C.c_int
+        L.tioga_b200_server_wait_timeout.argtypes = [_P, C.c_longlong, C.c_double, _P, _P]
+        L.tioga_b200_server_cancel.restype = C.c_int
+        L.tioga_b200_server_cancel.argtypes = [_P, C.c_longlong]
         L.tioga_b200_server_stats.argtypes = [_P, _P]
         self.h = L.tioga_b200_server_create(int(budget_bytes), int(nslots), int(max_resident))
         if not self.h:
@@ -127,14 +131,31 @@ class Server:
         self._keep[t] = keep
         return t
 
-    def wait(self, ticket: int) -> dict:
+    # request statuses besides 0 and the engine's error codes
+    OVER_BUDGET, CANCELLED, TIMED_OUT = -3, -4, -5
+
+    def wait(self, ticket: int, timeout_ms: float | None = None) -> dict:
+        """The request's result; with timeout_ms, rc == TIMED_OUT when it is
+        not done by then (the ticket stays valid)."""
         times = (C.c_double * 6)()
         counts = (C.c_longlong * 4)()
-        rc = self.lib.tioga_b200_server_wait(self.h, C.c_longlong(ticket), C.cast(times, _P), C.cast(counts, _P))
+        if timeout_ms is None:
+            rc = self.lib.tioga_b200_server_wait(self.h, C.c_longlong(ticket), C.cast(times, _P),
+                                                 C.cast(counts, _P))
+        else:
+            rc = self.lib.tioga_b200_server_wait_timeout(self.h, C.c_longlong(ticket), C.c_double(timeout_ms),
+                                                         C.cast(times, _P), C.cast(counts, _P))
+            if rc == self.TIMED_OUT:
+                return {"rc": rc}
         self._keep.pop(ticket, None)
         return {"rc": rc, "latency_ms": times[0], "queue_ms": times[1], "service_ms": times[2],
                 "preprocess_ms": times[3], "connectivity_ms": times[4], "dataupdate_ms": times[5],
                 "nquery": counts[0], "nreceptor": counts[1], "nhole": counts[2]}
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancel a request that has not started (it then completes with
+        rc == CANCELLED); False when it runs or is done."""
+        return self.lib.tioga_b200_server_cancel(self.h, C.c_longlong(ticket)) == 0
 
     def stats(self) -> dict:
         out = (C.c_longlong * 16)()
