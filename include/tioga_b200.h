@@ -312,6 +312,14 @@ void tioga_b200_set_stream_(void *stream);
 int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights, const int *d_nweights,
                                     const int *d_receptor, int nrec, double *d_q, long long nnodes,
                                     int nvar, int interptype, void *stream);
+/* tioga::set_uniform_hex_flag (src/tioga.h:195-201), which the reference
+ * offers through its C++ class only: at the next preprocess, block btag is
+ * tested for a box of identical rectangular hexahedra
+ * (MeshBlock::check_for_uniform_hex, src/MeshBlock.C:1249-1372) and, when it
+ * is one, searched by index lookup in a cell map instead of its tree
+ * (MeshBlock::search_uniform_hex, src/search.C:271-341).  The high-order
+ * point search keeps the tree for such blocks. */
+void tioga_b200_set_uniform_hex_flag_(int *btag, int *flag);
 /* For tests of the error paths: lower one device bound to *value (0 restores
  * it).  *which 0 = rounds of a hole-map fill (at the bound the fill stops and
  * error bit 8 is reported), 1 = donor-record capacity (error bit 2).  The

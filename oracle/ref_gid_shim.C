@@ -8,6 +8,8 @@
 //                              global ids in front, handed to
 //                              tioga::registerGridData (src/tioga.C:64-85)
 //   refshim_getreceptorinfo_   tioga::getReceptorInfo (src/tioga.C:572-671)
+//   refshim_set_uniform_hex_flag_  tioga::set_uniform_hex_flag (src/tioga.h:195-201),
+//                              the uniform-hex search's switch
 // The instance is the C API's own (the global `tg` of src/globals.h), so the
 // rest of a test drives the reference through its C API as usual.
 #include <algorithm>
@@ -60,5 +62,7 @@ int refshim_getreceptorinfo_(int* out, int cap) {
   if (out && n > 0) std::memcpy(out, g_receptors.data(), sizeof(int) * std::min(n, cap));
   return n;
 }
+
+void refshim_set_uniform_hex_flag_(int* btag, int* flag) { tg->set_uniform_hex_flag(*btag, *flag); }
 
 }  // extern "C"

@@ -105,6 +105,13 @@ typedef struct {
   int ninterp2;
   int *i2_inode0, *i2_nw, *i2_rinfo; /* rinfo: point id, receptor block */
   double *i2_w;                      /* NFRAC per record */
+  /* uniform-hex fast path (MeshBlock.h:96-117: check_uniform_hex_flag,
+     uniform_hex, obh, dx, xlow, idims, uindx) */
+  int check_uniform_flag, uniform_hex;
+  obb_t obh;
+  double hdx[3], xlow[3];
+  int idims[3];
+  int *uindx;
 } block_t;
 
 static struct {
@@ -1157,8 +1164,186 @@ static void uniq_tree(const double *coord, int *itag, double *rtag, const int *m
 /* ======================================================================= */
 /* search: src/search.C:78-269                                             */
 /* ======================================================================= */
+/* ----------------------------------------------------------------------- */
+/* uniform-hex fast path: MeshBlock::check_for_uniform_hex (MeshBlock.C:1249-  */
+/* 1372), create_hex_cell_map (:1374-1409), search_uniform_hex (search.C:     */
+/* 271-341)                                                                 */
+/* ----------------------------------------------------------------------- */
+static double tdot(const double a[3], const double b[3], const double c[3]) { /* math.c:331-337 */
+  double dp = 0.0;
+  for (int k = 0; k < 3; k++) dp += ((a[k] - c[k]) * (b[k] - c[k]));
+  return dp;
+}
+
+static void check_for_uniform_hex(block_t *b) {
+  double xv[8][3];
+  int hex_present = 0;
+  if (b->ntypes > 1) return;
+  for (int n = 0; n < b->ntypes; n++) {
+    int nvert = b->nv[n];
+    if (nvert != 8) continue;
+    hex_present = 1;
+    for (int i = 0; i < b->nc[n]; i++) {
+      int vold = -1;
+      for (int m = 0; m < nvert; m++) {
+        if (b->vconn[n][nvert * i + m] == vold) return; /* degenerate hex */
+        vold = b->vconn[n][nvert * i + m];
+        int i3 = 3 * (vold - 1);
+        for (int k = 0; k < 3; k++) xv[m][k] = b->x[i3 + k];
+      }
+      /* rectangular faces at vertex 0 and the corner at vertex 6 */
+      if (fabs(tdot(xv[1], xv[3], xv[0])) > TOLV) return;
+      if (fabs(tdot(xv[1], xv[3], xv[2])) > TOLV) return;
+      if (fabs(tdot(xv[3], xv[4], xv[0])) > TOLV) return;
+      if (fabs(tdot(xv[3], xv[4], xv[7])) > TOLV) return;
+      if (fabs(tdot(xv[4], xv[1], xv[0])) > TOLV) return;
+      if (fabs(tdot(xv[4], xv[1], xv[5])) > TOLV) return;
+      if (fabs(tdot(xv[5], xv[7], xv[6])) > TOLV) return;
+      /* the same squared edge lengths as the first hex */
+      if (i == 0) {
+        b->hdx[0] = tdot(xv[1], xv[1], xv[0]);
+        b->hdx[1] = tdot(xv[3], xv[3], xv[0]);
+        b->hdx[2] = tdot(xv[4], xv[4], xv[0]);
+      } else {
+        if (fabs(b->hdx[0] - tdot(xv[1], xv[1], xv[0])) > TOLV) return;
+        if (fabs(b->hdx[1] - tdot(xv[3], xv[3], xv[0])) > TOLV) return;
+        if (fabs(b->hdx[2] - tdot(xv[4], xv[4], xv[0])) > TOLV) return;
+      }
+    }
+  }
+  if (!hex_present) return;
+  for (int j = 0; j < 3; j++) b->hdx[j] = sqrt(b->hdx[j]);
+  b->uniform_hex = 1;
+  obb_t *o = &b->obh;
+  for (int j = 0; j < 3; j++)
+    for (int k = 0; k < 3; k++) o->vec[j][k] = 0;
+  /* axes from the last hex's edges, lengths from the first hex's */
+  for (int k = 0; k < 3; k++) o->vec[0][k] = (xv[1][k] - xv[0][k]) / b->hdx[0];
+  for (int k = 0; k < 3; k++) o->vec[1][k] = (xv[3][k] - xv[0][k]) / b->hdx[1];
+  for (int k = 0; k < 3; k++) o->vec[2][k] = (xv[4][k] - xv[0][k]) / b->hdx[2];
+  double xd[3], xmax[3] = {-BIGVALUE, -BIGVALUE, -BIGVALUE}, xmin[3] = {BIGVALUE, BIGVALUE, BIGVALUE};
+  for (int i = 0; i < b->nnodes; i++) {
+    for (int j = 0; j < 3; j++) xd[j] = 0;
+    for (int j = 0; j < 3; j++)
+      for (int k = 0; k < 3; k++) xd[j] += b->x[3 * i + k] * o->vec[j][k];
+    for (int j = 0; j < 3; j++) {
+      xmax[j] = dmax(xmax[j], xd[j]);
+      xmin[j] = dmin(xmin[j], xd[j]);
+    }
+  }
+  for (int j = 0; j < 3; j++) {
+    xmax[j] += TOLV;
+    xmin[j] -= TOLV;
+    o->dxc[j] = (xmax[j] - xmin[j]) * 0.5;
+    xd[j] = (xmax[j] + xmin[j]) * 0.5;
+  }
+  for (int j = 0; j < 3; j++) {
+    o->xc[j] = 0.0;
+    for (int k = 0; k < 3; k++) o->xc[j] += (xd[k] * o->vec[k][j]);
+  }
+}
+
+/* The reference writes uindx without a bounds check; a centroid outside the
+   map (which a uniform block cannot have) is skipped here. */
+static void create_hex_cell_map(block_t *b) {
+  const obb_t *o = &b->obh;
+  for (int j = 0; j < 3; j++) {
+    b->xlow[j] = o->xc[j];
+    for (int k = 0; k < 3; k++) b->xlow[j] -= (o->dxc[k] * o->vec[k][j]);
+    b->idims[j] = (int)round(2 * o->dxc[j] / b->hdx[j]);
+    b->hdx[j] = (2 * o->dxc[j]) / b->idims[j];
+  }
+  const long long nmap = (long long)b->idims[0] * b->idims[1] * b->idims[2];
+  free(b->uindx);
+  b->uindx = (int *)malloc(sizeof(int) * (nmap > 0 ? nmap : 1));
+  for (long long i = 0; i < nmap; i++) b->uindx[i] = -1;
+  for (int i = 0; i < b->nc[0]; i++) {
+    double xc[3], xd[3];
+    int idx[3];
+    for (int j = 0; j < 3; j++) {
+      int lnode = b->vconn[0][8 * i] - 1, tnode = b->vconn[0][8 * i + 6] - 1;
+      xc[j] = 0.5 * (b->x[3 * lnode + j] + b->x[3 * tnode + j]);
+    }
+    int ok = 1;
+    for (int j = 0; j < 3; j++) {
+      xd[j] = 0;
+      for (int k = 0; k < 3; k++) xd[j] += (xc[k] - b->xlow[k]) * o->vec[j][k];
+      idx[j] = (int)(xd[j] / b->hdx[j]);
+      ok = ok && idx[j] >= 0 && idx[j] < b->idims[j];
+    }
+    if (ok) b->uindx[(long long)idx[2] * b->idims[1] * b->idims[0] + idx[1] * b->idims[0] + idx[0]] = i;
+  }
+}
+
+/* search.C:271-341.  The reference's loop over the eight corners of a cube
+   of side 4 TOL runs while "dId[0] == -1 || dID[1]", where dId is a freshly
+   malloc'd, never written array (search.C:291, 311); its first word is not -1
+   in practice, so the loop runs while the current pick is missing (-1) or a
+   cell of BIG resolution, as restated here. */
+static void search_uniform_hex(block_t *b) {
+  free(b->xtag);
+  b->xtag = (int *)malloc(sizeof(int) * b->nsearch);
+  {
+    int *avail = (int *)malloc(sizeof(int) * b->nsearch);
+    for (int i = 0; i < b->nsearch; i++) avail[i] = b->xtag[i] = i;
+    uniq_tree(b->xsearch, b->xtag, b->res_search, b->tagsearch, avail, b->nsearch);
+    free(avail);
+  }
+  double xvec[8][3];
+  for (int jj = 0; jj < 8; jj++)
+    for (int k = 0; k < 3; k++) xvec[jj][k] = (2 * ((jj & (1 << k)) >> k) - 1) * 2 * TOLV;
+  const obb_t *o = &b->obh;
+  const int *d = b->idims;
+  for (int i = 0; i < b->nsearch; i++) {
+    if (b->xtag[i] != i) {
+      b->donorId[i] = b->donorId[b->xtag[i]];
+      continue;
+    }
+    double xd[3];
+    int idx[3];
+    for (int j = 0; j < 3; j++) {
+      xd[j] = 0;
+      for (int k = 0; k < 3; k++) xd[j] += (b->xsearch[3 * i + k] - b->xlow[k]) * o->vec[j][k];
+      idx[j] = (int)(xd[j] / b->hdx[j]);
+    }
+    if (xd[0] > -TOLV && xd[0] < d[0] * b->hdx[0] + TOLV && xd[1] > -TOLV && xd[1] < d[1] * b->hdx[1] + TOLV &&
+        xd[2] > -TOLV && xd[2] < d[2] * b->hdx[2] + TOLV) {
+      for (int k = 0; k < 3; k++)
+        if (idx[k] == d[k]) idx[k]--;
+      int id0 = b->uindx[(long long)idx[2] * d[1] * d[0] + idx[1] * d[0] + idx[0]];
+      int big = (id0 > -1) ? (b->cellRes[id0] == BIGVALUE) : 1;
+      for (int jj = 0; jj < 8 && big; jj++) {
+        for (int k = 0; k < 3; k++) {
+          idx[k] = (int)((xd[k] + xvec[jj][k]) / b->hdx[k]);
+          if (idx[k] == d[k]) idx[k]--;
+        }
+        int dtest = b->uindx[(long long)idx[2] * d[1] * d[0] + idx[1] * d[0] + idx[0]];
+        big = (dtest > -1) ? (b->cellRes[dtest] == BIGVALUE) : 1;
+        id0 = (id0 == -1) ? dtest : (!big ? dtest : id0);
+      }
+      b->donorId[i] = id0;
+    } else {
+      b->donorId[i] = -1;
+    }
+  }
+}
+
+int tioga_oracle_uniform_hex(int btag) {
+  int ib = find_tag(btag);
+  return ib >= 0 ? G.b[ib]->uniform_hex : -1;
+}
+
+void tioga_oracle_set_uniform_hex_flag(int btag, int flag) {
+  int ib = find_tag(btag);
+  if (ib >= 0) G.b[ib]->check_uniform_flag = flag;
+}
+
 static void search_block(block_t *b) {
   if (b->nsearch == 0) return;
+  if (b->uniform_hex) {
+    search_uniform_hex(b);
+    return;
+  }
   obb_t q;
   find_obb(b->xsearch, b->nsearch, &q);
   /* cells whose box overlaps the query OBB, pushed LIFO (:123-167) */
@@ -1527,6 +1712,7 @@ static void free_block(block_t *b) {
   free(b->interp); free(b->interp2donor); free(b->cancel_nodes);
   free(b->ctag); free(b->ppc); free(b->rxyz); free(b->rst);
   free(b->i2_inode0); free(b->i2_nw); free(b->i2_rinfo); free(b->i2_w);
+  free(b->uindx);
   if (b->own_iblank_cell) free(b->iblank_cell);
   free(b);
 }
@@ -1599,6 +1785,10 @@ void tioga_preprocess_grids_(void) {
     block_t *b = G.b[ib];
     b->nfringe = G.nfringe;
     for (int i = 0; i < b->nnodes; i++) b->iblank[i] = 1;
+    if (b->check_uniform_flag) { /* MeshBlock.C:84-87 */
+      check_for_uniform_hex(b);
+      if (b->uniform_hex) create_hex_cell_map(b);
+    }
     find_obb(b->x, b->nnodes, &b->obb);
     tag_boundary(b);
   }

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 SOURCES = ["capi.cu", "engine.cu", "kernels_pre.cu", "kernels_conn.cu", "kernels_tree.cu", "kernels_donor.cu",
-           "kernels_dedup.cu", "highorder.cu", "noalloc.cu", "server.cu"]
+           "kernels_dedup.cu", "kernels_uhex.cu", "highorder.cu", "noalloc.cu", "server.cu"]
 
 
 def _compile(src: str, verbose: bool) -> str:

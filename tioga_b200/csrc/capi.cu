@@ -306,6 +306,10 @@ void tioga_b200_stats_(long long out[16]) {
   out[15] = s.ngroup_nodes;
 }
 
+void tioga_b200_set_uniform_hex_flag_(int* btag, int* flag) {
+  if (ready("tioga_b200_set_uniform_hex_flag_")) set_rc(g_tg->set_uniform_hex_flag(*btag, *flag));
+}
+
 void tioga_b200_set_test_bound_(int* which, int* value) {
   if (ready("tioga_b200_set_test_bound_")) set_rc(g_tg->set_test_bound(*which, *value));
 }

@@ -57,7 +57,7 @@ Engine::~Engine() {
   counters_.release();
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
   d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
-  rf_red_.release(); rf_tmp_.release(); rf_was_.release();
+  rf_red_.release(); rf_tmp_.release(); rf_was_.release(); uhex_map_.release(); uhex_red_.release();
   d_wall_.release(); wall_cells_.release(); wall_box_.release(); wall_box_first_.release();
   cg_cnt_.release(); cg_off_.release(); cg_v0_.release(); cg_v1_.release(); cg_k0_.release(); cg_k1_.release();
   cg_flag_.release();
@@ -745,6 +745,7 @@ int Engine::preprocess() {
   // distance), so the gate of the last preprocess still holds after them
   if (!gate_valid_) TB_TRY(dedup_gate());
   gate_valid_ = true;
+  TB_TRY(setup_uniform_hex());
   for (size_t b = 0; b < hb_.size(); b++) {
     const HostBlock& H = hb_[b];
     if (!bi_[b].has_user_res) continue;
@@ -1144,7 +1145,7 @@ int Engine::run_search() {
   TB_CUDA(cudaMemsetAsync(qacc_.p, 0, nq_ * sizeof(unsigned), stream_));
   unsigned count = 0;
   TB_CUDA(cudaEventRecord(sev_[0], stream_));
-  TB_TRY(traverse_and_gather(x_.p, qnode_.p, qdon_.p, nq_, count));
+  TB_TRY(traverse_and_gather(x_.p, qnode_.p, qdon_.p, nq_, count, any_uhex_ ? 1 : 0));
   ncand_ = count;
   TB_CUDA(cudaEventRecord(sev_[1], stream_));
   if (count > 0) {
@@ -1165,6 +1166,11 @@ int Engine::run_search() {
   k_search_finish<<<grid_for(nq_, kT), kT, 0, stream_>>>(qkey_.p, qacc_.p, nq_, inv_sorted_.p, qcell_.p, qtie_.p,
                                                          counters_.p);
   TB_LAUNCHED("k_search_finish");
+  if (any_uhex_) {  // donors that are uniform boxes: the index lookup (search.C:271-341)
+    k_uhex_search<<<grid_for(nq_, kT), kT, 0, stream_>>>(x_.p, qnode_.p, qdon_.p, nq_, d_bi_.p, uhex_map_.p,
+                                                         cell_res_.p, inv_sorted_.p, qcell_.p, qtie_.p);
+    TB_LAUNCHED("k_uhex_search");
+  }
   if (dedup_ran_) {  // merged coincident points take their representative's donor
     k_dedup_copy<<<grid_for(nq_, kT), kT, 0, stream_>>>(q_rep_.p, nq_, qcell_.p, qtie_.p);
     TB_LAUNCHED("k_dedup_copy");
@@ -1177,7 +1183,8 @@ int Engine::run_search() {
 // qd[i]): stack-free traversal of the donor's tree into per-query slots and
 // an overflow list, then one dense query-ordered list in cand_.  The FP32
 // form of the tree is used unless the FP64 form is selected.
-int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count) {
+int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count,
+                                int skip_uhex) {
   const int form = (precision_ == 0) ? 0 : 1;
   TB_CUDA(slots_.ensure((size_t)nq * kSlots));
   TB_CUDA(ncand_q_.ensure(nq + 1));
@@ -1192,7 +1199,7 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
     launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
-                    slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p);
+                    slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p, skip_uhex);
     TB_LAUNCHED("k_traverse");
     TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
@@ -1960,6 +1967,120 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
     receptors[k++] = rb - bi_[rb].sblk0;  // the receptor block's index within its system
     receptors[k++] = nv;
   }
+  return 0;
+}
+
+int Engine::set_uniform_hex_flag(int tag, int flag) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].uniform_flag = flag;
+  return 0;
+}
+
+// The uniform-hex set-up of every flagged block (MeshBlock::preprocess,
+// MeshBlock.C:84-87): check_for_uniform_hex (MeshBlock.C:1249-1372) and
+// create_hex_cell_map (:1374-1409).  The first hex's squared edge lengths
+// and the last hex's edges (the reference's loop leaves them in dx and xv)
+// are read from the caller's arrays; every hex is checked on the device.
+// Deviation: a flagged block that is no longer uniform at a later preprocess
+// goes back to its tree (the reference keeps its stale map).
+int Engine::setup_uniform_hex() {
+  bool any_flag = false;
+  for (const HostBlock& H : hb_) any_flag = any_flag || H.uniform_flag;
+  if (!any_flag && !any_uhex_) return 0;
+  any_uhex_ = false;
+  long long map_total = 0;
+  TB_CUDA(uhex_red_.ensure(8));
+  unsigned* bad = reinterpret_cast<unsigned*>(uhex_red_.p + 6);
+  for (size_t b = 0; b < hb_.size(); b++) {
+    HostBlock& H = hb_[b];
+    BlockInfo& B = bi_[b];
+    B.uhex = 0;
+    H.uniform = 0;
+    if (!H.uniform_flag || H.ntypes != 1 || H.nv[0] != 8 || H.nc[0] < 1) continue;
+    double first[8][3], last[8][3];
+    const int* c0 = H.hconn[0];
+    const int* cl = H.hconn[0] + 8 * (long long)(H.nc[0] - 1);
+    for (int m = 0; m < 8; m++)
+      for (int k = 0; k < 3; k++) {
+        first[m][k] = H.hx[3 * (long long)(c0[m] - 1) + k];
+        last[m][k] = H.hx[3 * (long long)(cl[m] - 1) + k];
+      }
+    auto tdot = [](const double* a, const double* p, const double* c) {
+      double dp = 0.0;
+      for (int k = 0; k < 3; k++) dp += ((a[k] - c[k]) * (p[k] - c[k]));
+      return dp;
+    };
+    double d[3] = {tdot(first[1], first[1], first[0]), tdot(first[3], first[3], first[0]),
+                   tdot(first[4], first[4], first[0])};
+    TB_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), stream_));
+    k_uhex_check<<<grid_for(H.ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, d_bi_.p, (int)b, d[0], d[1], d[2],
+                                                             bad);
+    TB_LAUNCHED("k_uhex_check");
+    unsigned h_bad = 0;
+    TB_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    if (h_bad) continue;
+    double dx[3], vec[3][3];
+    for (int j = 0; j < 3; j++) dx[j] = sqrt(d[j]);
+    for (int k = 0; k < 3; k++) vec[0][k] = (last[1][k] - last[0][k]) / dx[0];
+    for (int k = 0; k < 3; k++) vec[1][k] = (last[3][k] - last[0][k]) / dx[1];
+    for (int k = 0; k < 3; k++) vec[2][k] = (last[4][k] - last[0][k]) / dx[2];
+    unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+    TB_CUDA(cudaMemcpyAsync(uhex_red_.p, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+    UhexAxes A;
+    memcpy(A.vec, vec, sizeof(vec));
+    k_uhex_extent<<<grid_for(H.nnodes, kT), kT, 0, stream_>>>(x_.p, B.node_off, H.nnodes, A, uhex_red_.p);
+    TB_LAUNCHED("k_uhex_extent");
+    unsigned long long red[6];
+    TB_CUDA(cudaMemcpyAsync(red, uhex_red_.p, sizeof(red), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    double xmin[3], xmax[3], dxc[3], xd[3], xc[3];
+    for (int j = 0; j < 3; j++) {
+      xmin[j] = dkey_inv(red[j]) - kTol;
+      xmax[j] = dkey_inv(red[j + 3]) + kTol;
+      dxc[j] = (xmax[j] - xmin[j]) * 0.5;
+      xd[j] = (xmax[j] + xmin[j]) * 0.5;
+    }
+    for (int j = 0; j < 3; j++) {
+      xc[j] = 0.0;
+      for (int k = 0; k < 3; k++) xc[j] += (xd[k] * vec[k][j]);
+    }
+    long long nmap = 1;
+    bool ok = true;
+    for (int j = 0; j < 3; j++) {
+      B.uxlow[j] = xc[j];
+      for (int k = 0; k < 3; k++) B.uxlow[j] -= (dxc[k] * vec[k][j]);
+      const double r = round(2 * dxc[j] / dx[j]);
+      ok = ok && r >= 1 && r < 2147483647.0;
+      B.uidims[j] = ok ? (int)r : 1;
+      B.udx[j] = (2 * dxc[j]) / B.uidims[j];
+      nmap *= B.uidims[j];
+      for (int k = 0; k < 3; k++) B.uvec[j][k] = vec[j][k];
+    }
+    if (!ok || nmap > 4ll * H.ncells + 1024) {  // not the box of its own cells: keep the tree
+      fprintf(stderr, "#tioga_b200: block %d passed the uniform-hex test but its cell map does not fit\n",
+              H.tag);
+      continue;
+    }
+    B.uhex = 1;
+    H.uniform = 1;
+    B.umap_off = map_total;
+    map_total += nmap;
+    any_uhex_ = true;
+  }
+  TB_CUDA(cudaMemcpyAsync(d_bi_.p, bi_.data(), bi_.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice, stream_));
+  if (any_uhex_) {
+    TB_CUDA(uhex_map_.ensure(map_total));
+    TB_CUDA(cudaMemsetAsync(uhex_map_.p, 0xff, map_total * sizeof(int), stream_));
+    for (size_t b = 0; b < hb_.size(); b++)
+      if (bi_[b].uhex) {
+        k_uhex_map<<<grid_for(hb_[b].ncells, kT), kT, 0, stream_>>>(x_.p, conn8_.p, sorted_cell_.p, d_bi_.p,
+                                                                    (int)b, uhex_map_.p);
+        TB_LAUNCHED("k_uhex_map");
+      }
+  }
+  TB_CUDA(cudaStreamSynchronize(stream_));  // the host block table goes on changing
   return 0;
 }
 

@@ -108,6 +108,12 @@ struct BlockInfo {
   int sys, sblk0, snb;
   int hm_lo, hm_hi;    // the system's hole maps: d_hmdev_[hm_lo .. hm_hi)
   int hm;              // the block's own hole map (wall-bearing blocks), else -1
+  // uniform-hex fast path (tioga::set_uniform_hex_flag): a box of identical
+  // rectangular hexahedra searched by index lookup in its cell map
+  int uhex;            // 1: the lookup replaces the tree search for this donor
+  int uidims[3];
+  double uvec[3][3], uxlow[3], udx[3];
+  long long umap_off;  // its map in uhex_map_
   Obb obb;
   float bb_lo[3], bb_hi[3];  // block box for the Morton keys
 };
@@ -132,6 +138,11 @@ struct PairCull {
   int pair;       // index in the pair list
 };
 
+
+// the axes of a uniform-hex block (rows), passed by value to a kernel
+struct UhexAxes {
+  double vec[3][3];
+};
 
 // rigid motion x <- a x + b (a row-major)
 struct Rigid {
@@ -193,6 +204,8 @@ struct HostBlock {
   double* user_nres = nullptr;
   double* user_cres = nullptr;
   int* h_iblank_cell = nullptr;  // caller array (tioga_setcelliblank_)
+  int uniform_flag = 0;          // tioga::set_uniform_hex_flag: check for a uniform box at preprocess
+  int uniform = 0;               // found uniform at the last preprocess
   double* hq = nullptr;          // registered host solution
   double* dq = nullptr;          // registered device solution
   int* dibl = nullptr;           // caller's device iblank array (optional)
@@ -303,6 +316,7 @@ class Engine {
   int donor_count(int tag, int* dcount, int* fcount);
   int donor_info(int tag, int* receptors, int* indices, double* frac);
   int set_cell_gid(int tag, const uint64_t* gid);
+  int set_uniform_hex_flag(int tag, int flag);
   // tioga::getReceptorInfo: 4 ints per live record of the selected system;
   // writes min(count, cap) ints to out (may be null) and returns the count,
   // or < 0 on error
@@ -326,6 +340,7 @@ class Engine {
   int preprocess_resolutions();
   int run_pairs_and_refit();
   int build_leaf_groups();
+  int setup_uniform_hex();
   int run_queries();
   int run_search();
   int run_donors();
@@ -333,7 +348,8 @@ class Engine {
   int dedup_gate();
   int run_dedup();
   int dedup_merge(const DedupQueries& Q, const std::vector<int>& qoff);
-  int traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count);
+  int traverse_and_gather(const double* xq, const int* qn, const int* qd, long long nq, unsigned& count,
+                          int skip_uhex = 0);
   int run_celliblank();
   int download_iblank();
   int fetch_interps();
@@ -502,6 +518,9 @@ class Engine {
   DBuf<unsigned> err_;
   DBuf<unsigned> coord_err_;  // non-finite coordinate flag (check_coords)
   int test_fill_rounds_ = 0, test_rcap_ = 0;  // set_test_bound
+  DBuf<int> uhex_map_;                  // cell maps of the uniform-hex blocks
+  DBuf<unsigned long long> uhex_red_;   // set-up scratch: extents, check flag
+  bool any_uhex_ = false;
   DBuf<unsigned long long> counters_;
   DBuf<unsigned long long> mkey_, mkey_alt_;
   DBuf<int> mval_alt_;

@@ -188,7 +188,7 @@ __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairIn
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
-                     int ovf_cap, unsigned* novf, unsigned* err);
+                     int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex);
 __global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,
                                     const int3* ovf, const unsigned* novf, int ovf_cap, int2* cand);
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,
@@ -201,6 +201,17 @@ __global__ void k_refine(const double* x, const int* conn8, const unsigned char*
 __global__ void k_search_finish(const unsigned long long* qkey, const unsigned* qacc, long long nq,
                                 const int* inv_sorted, int* qcell, unsigned char* qtie,
                                 unsigned long long* counters);
+
+// ---- uniform-hex fast path (kernels_uhex.cu) ----
+__global__ void k_uhex_check(const double* x, const int* conn8, const BlockInfo* bi, int b, double d0, double d1,
+                             double d2, unsigned* bad);
+__global__ void k_uhex_extent(const double* x, long long node_off, long long nnodes, UhexAxes A,
+                              unsigned long long* red);
+__global__ void k_uhex_map(const double* x, const int* conn8, const int* sorted_cell, const BlockInfo* bi, int b,
+                           int* map);
+__global__ void k_uhex_search(const double* x, const int* qnode, const int* qdon, long long nq, const BlockInfo* bi,
+                              const int* map, const double* cell_res, const int* inv_sorted, int* qcell,
+                              unsigned char* qtie);
 
 // ---- donors (kernels_donor.cu) ----
 __global__ void k_fill_slots(const int* qnode, const int* qdon, const int* qcell, long long nq, int K,

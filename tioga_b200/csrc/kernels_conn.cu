@@ -1428,7 +1428,7 @@ __global__ void __launch_bounds__(256) k_traverse(
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
     int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf,
-    unsigned* __restrict__ err) {
+    unsigned* __restrict__ err, int skip_uhex) {
   __shared__ int s_base[kMaxTreeDepth][256];
   const int t = threadIdx.x;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq;
@@ -1436,6 +1436,10 @@ __global__ void __launch_bounds__(256) k_traverse(
     int n = 0;
     const int g = qnode[q];
     const int root = bi[qdon[q]].root;
+    if (skip_uhex && bi[qdon[q]].uhex) {  // searched by k_uhex_search instead
+      ncand_q[q] = 0;
+      continue;
+    }
     double p[3];
     float plo[3], phi[3];  // the point widened by a margin that covers TOL and FP32 rounding
     p[0] = x[3 * (long long)g];
@@ -1717,13 +1721,13 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
-                     int ovf_cap, unsigned* novf, unsigned* err) {
+                     int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex) {
   if (form == 0)
     k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
-                                          ovf, ovf_cap, novf, err);
+                                          ovf, ovf_cap, novf, err, skip_uhex);
   else
     k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
-                                          ovf, ovf_cap, novf, err);
+                                          ovf, ovf_cap, novf, err, skip_uhex);
 }
 
 void launch_candidates(int form, int blocks, cudaStream_t st, const double* x, const int* conn8,
