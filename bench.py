@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--impl", default="tioga_b200", choices=["tioga_b200", "reference"])
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cpu-full", action="store_true",
+                   help="skip the one full-size connectivity call of the compiled reference")
     p.add_argument("--no-parity", action="store_true",
                    help="skip the mismatch count against the compiled reference's digests")
     p.add_argument("--cpu-reps", type=int, default=3)
@@ -399,10 +401,29 @@ def run_gpu(args, ws, rank, local, dist):
     # parity of the timed configuration against the compiled reference
     if args.size == "full" and args.seed == 1 and not args.no_parity:
         out["parity"] = parity_vs_reference(lib, tb, psys, "cfg1_full", 21)
+    # the whole call against its compulsory bytes (B_conn): every array of the
+    # path read or written once -- coordinates, connectivity, cell and node
+    # resolutions, iblanks, cell iblanks, hole maps, query buffers and their
+    # sort keys, donor ids and interpolation records
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+    tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
+    lib.performconnectivity()
+    st2 = (C.c_longlong * 8)()
+    lib.lib.tioga_b200_stats2_(st2)
+    nw1 = sum(int((lib.getdonorinfo(b.tag)[0][:, 3] + 1).sum()) for b in system.blocks)
+    N, Cc, R = system.nnodes, system.ncells, st["nreceptor"]
+    b_conn = (24 * N + 4 * nvsum + 8 * Cc + 8 * N + 4 * N + 4 * Cc + int(st2[0]) + Q * (24 + 8) + Q * (24 + 4)
+              + 4 * R + 12 * nw1)
+    out["roofline"]["call"] = {"algorithmic_bytes": b_conn, "ms": ms_split,
+                               "achieved": b_conn / (ms_split * 1e-3) / 1e9,
+                               "frac": b_conn / (ms_split * 1e-3) / 1e9 / peak,
+                               "note": "the whole connectivity call (split form, resident coordinates) against "
+                                       "its compulsory bytes"}
     out["dataupdate"] = time_dataupdate(lib, system, stream, st["nreceptor"], args.steps, args.warmup)
     lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
     lib.delete()
     del keep
+    out["_system"] = system
     return out
 
 
@@ -940,6 +961,34 @@ def cpu_reference(reps: int, warmup: int = 1):
             "per_step_s": times}, None
 
 
+def cpu_reference_full(system):
+    """One full-size connectivity call of the compiled reference on the timed
+    configuration itself (after its preprocess), on one host core: the rate per
+    query point at full size, beside the bounded sample's."""
+    if not os.path.exists(REF_LIB):
+        return None
+    sys.path.insert(0, ROOT)
+    from tests.golden import digest
+    t = TiogaLibrary(REF_LIB)
+    t.init()
+    t.register_system(system)
+    t0 = time.perf_counter()
+    t.preprocess_grids()
+    t1 = time.perf_counter()
+    t.performconnectivity()
+    t2 = time.perf_counter()
+    t.delete()
+    Q = None
+    fix = os.path.join(GOLDEN, "cfg1_full.npz")
+    if os.path.exists(fix):
+        f = np.load(fix)
+        if digest.input_digest(system) == str(f["input_digest"]):
+            Q = int(f["query_points"][0])
+    return {"preprocess_s": t1 - t0, "connectivity_s": t2 - t1, "query_points": Q,
+            "value": (Q / (t2 - t1)) if Q else None, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": "the full timed configuration, one connectivity call"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -986,11 +1035,33 @@ def main():
         sv = run_gpu_serving(a3, ws, rank, local, Dist(1, None))
         out["served"] = {k: sv[k] for k in ("value", "unit", "latency_ms", "serving", "e2e", "clocks")}
         out["served"]["config"] = sv["config"]
+    system = out.pop("_system", None)
+    if rank == 0 and ws == 1 and args.workload == "cfg1" and "batched" in out and "served" in out:
+        # the north-star comparison as worded: the split-precision batched and
+        # served forms against the plain (FP64, single-system) form at cfg1 scale
+        plain = out["plain"]["value"]
+        best = max(out["batched"]["value"], out["served"]["serving"]["capacity_receptors_per_s"])
+        par = out.get("parity") or {}
+        forms = par.get("forms", {})
+        out["north_star"] = {
+            "plain_fp64_cfg1": plain, "split_cfg1": out["value"], "split_batched_cfg2": out["batched"]["value"],
+            "served_capacity": out["served"]["serving"]["capacity_receptors_per_s"],
+            "served_p99_ms": out["served"]["latency_ms"]["p99"],
+            "ratio_best_vs_plain": best / plain, "target_ratio": 3.0, "met": best / plain >= 3.0,
+            "mismatches": par.get("mismatches"), "ties": par.get("ties"),
+            "max_weight_error_vs_fp64": (0.0 if forms and all(f["record_mismatches"] == 0 and
+                                                             f["field_chunk_mismatches"] == 0
+                                                             for f in forms.values()) else None),
+            "note": "weights and updated fields of both forms equal the reference's digests bit for bit, so the "
+                    "split form's weight error against FP64 is 0"}
     if rank == 0:
         if ws == 1 and not args.no_cpu_baseline:
             res, why = cpu_reference(args.cpu_reps)
             out["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                    if res else {"unavailable": why})
+            if res and system is not None and args.workload == "cfg1" and args.size == "full" \
+                    and not args.no_cpu_full:
+                out["cpu_baseline"]["full_size"] = cpu_reference_full(system)
         else:
             out["cpu_baseline"] = None
         print(json.dumps(out))

@@ -290,6 +290,8 @@ void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
  * [13] query points merged into a coincident one (uniqNodesTree),
  * [14] leaf groups of the cell pass, [15] their distinct vertex nodes. */
 void tioga_b200_stats_(long long out[16]);
+/* More counters of the last connectivity call: [0] cells of its hole maps. */
+void tioga_b200_stats2_(long long out[8]);
 /* Run on the caller's CUDA stream (a cudaStream_t; NULL restores the
  * library's own stream), e.g. to time the calls with the caller's events. */
 void tioga_b200_set_stream_(void *stream);

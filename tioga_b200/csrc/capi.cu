@@ -314,6 +314,12 @@ void tioga_b200_set_test_bound_(int* which, int* value) {
   if (ready("tioga_b200_set_test_bound_")) set_rc(g_tg->set_test_bound(*which, *value));
 }
 
+void tioga_b200_stats2_(long long out[8]) {
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  if (!g_tg) return;
+  out[0] = g_tg->stats().holemap_cells;
+}
+
 void tioga_b200_autotune_(int* reps) {
   if (ready("tioga_b200_autotune_")) set_rc(g_tg->autotune(*reps));
 }

@@ -898,6 +898,7 @@ int Engine::run_holemaps() {
     maxpl = std::max(maxpl, h.nx[pa]);
     smem = std::max(smem, (size_t)h.nx[a0] * h.nx[a1]);
     maxcells = std::max(maxcells, (long long)h.nx[0] * h.nx[1] * h.nx[2]);
+    stats_.holemap_cells += (long long)h.nx[0] * h.nx[1] * h.nx[2];
   }
   if (planar) {  // fill and final map in one pass
     k_holemap_fill_bits<<<dim3(std::min(maxpl, 148 * 4), nh), 256, 0, stream_>>>(

@@ -228,6 +228,7 @@ struct Stats {
   long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
   long long ngroups = 0;      // leaf groups (the split-form cell pass's units of work)
   long long ngroup_nodes = 0; // distinct vertex nodes summed over the leaf groups
+  long long holemap_cells = 0; // cells of this call's hole maps
   unsigned error = 0;
 };
 
