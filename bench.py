@@ -223,7 +223,7 @@ def autotune(lib, tb, reps: int = 2) -> dict:
     out = (C.c_int * 8)()
     lib.lib.tioga_b200_tuning_(out)
     keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
-            "candidate_ctas_per_sm"]
+            "candidate_ctas_per_sm", "traverse_warp_cooperative"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 

@@ -255,7 +255,8 @@ void tioga_b200_server_stats(void *srv, long long out[16]);
  * the shapes; the instance ends with a connectivity call's results. */
 void tioga_b200_autotune_(int *reps);
 /* The shapes in use: [0] cell-pass CTAs per SM, [1] pairs per cell-pass CTA,
- * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM. */
+ * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM,
+ * [5] split-form traversal: 1 warp-cooperative, 0 one walk per query point. */
 void tioga_b200_tuning_(int out[8]);
 
 /* 0 when the last call succeeded, else a negative code. */

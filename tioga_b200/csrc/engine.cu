@@ -1198,7 +1198,8 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
+    const int tform = (form == 1 && tune_.traverse_warp) ? 2 : form;
+    launch_traverse(tform, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p, skip_uhex);
     TB_LAUNCHED("k_traverse");
@@ -1783,6 +1784,7 @@ int Engine::autotune(int reps) {
       {&tune_.cell_pass_per_sm, {2, 3, 4}, &Timing::cell_pass},
       {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
       {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
+      {&tune_.traverse_warp, {1, 0}, &Timing::traverse},
       {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},
       {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
   };

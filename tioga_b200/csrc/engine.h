@@ -237,6 +237,7 @@ struct Stats {
 // candidate screen, and the pairs one cell-pass CTA holds in shared memory.
 struct Tuning {
   int cell_pass_per_sm = 3, query_per_sm = 16, traverse_per_sm = 64, candidates_per_sm = 16, chunk_pairs = 128;
+  int traverse_warp = 1;  // split form: the warp-cooperative walk (1) or one walk per query (0)
 };
 
 struct Timing {

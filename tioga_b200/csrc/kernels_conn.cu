@@ -1560,6 +1560,134 @@ __global__ void __launch_bounds__(256) k_traverse(
   }
 }
 
+// Warp-cooperative walk of the split form.  A warp takes 32 consecutive
+// query points (Morton-coherent tiles of one pair, so mostly one donor block
+// and one neighbourhood) and walks the union of their paths once: each child
+// group (one 128-byte line) is loaded once for the warp, every lane tests its
+// own point against the four boxes, and a child is entered when any lane of
+// the packet hits it; a hit leaf's cell codes are loaded once for the warp
+// and each lane that hit the leaf tests its point.  Every node on a lane's
+// own path is in the union, so each lane gets exactly the candidates a walk
+// of its own finds (in another order, which the screen does not depend on:
+// it keeps the lowest accepting cell id).  Lanes of other donor blocks form
+// packets of their own.  The stack of child groups to visit is in shared
+// memory; a walk deeper than it reports kErrTraversalOverflow.
+constexpr int kWarpStack = 128;  // 3 pending siblings per level of 32 levels, and the root
+__global__ void __launch_bounds__(256) k_traverse_warp(
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const uint2* __restrict__ qbox,
+    const float4* __restrict__ tnode, const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq,
+    int* __restrict__ slots, int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap,
+    unsigned* __restrict__ novf, unsigned* __restrict__ err, int skip_uhex) {
+  __shared__ int s_stack[8][kWarpStack];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* stk = s_stack[w];
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5) * 32;
+  for (long long q0 = ((long long)blockIdx.x * (blockDim.x >> 5) + w) * 32; q0 < nq; q0 += wstride) {
+    const long long q = q0 + lane;
+    const bool inq = q < nq;
+    int root = -1, n = 0;
+    float plo[3] = {0.f, 0.f, 0.f}, phi[3] = {0.f, 0.f, 0.f};
+    if (inq) {
+      const BlockInfo& B = bi[qdon[q]];
+      root = (skip_uhex && B.uhex) ? -1 : B.root;  // uniform boxes: k_uhex_search
+      const double* pp = x + 3 * (long long)qnode[q];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const float p32 = (float)pp[k];
+        const float e = fabsf(p32) * 9.6e-7f + 2e-9f;  // covers TOL and the FP32 roundings
+        plo[k] = p32 - e;
+        phi[k] = p32 + e;
+      }
+    }
+    // the cells of leaf slot sl (link c0, ncell cells) hit by the lanes of `hit`
+    auto leaf_cells = [&](int c0, int ncell, long long sl, bool hit) {
+      uint2 Q[kMaxLeafCells];
+#pragma unroll
+      for (int j = 0; j < kMaxLeafCells; j++) Q[j] = qbox[c0 + min(j, ncell - 1)];
+      if (!hit) return;
+      const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
+      const float L[3] = {A.x, A.y, A.z}, H[3] = {A.w, B.x, B.y};
+      float sdn[3], sup[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        sdn[k] = qstep_dn(L[k], H[k]);
+        sup[k] = qstep_up(L[k], H[k]);
+      }
+      unsigned hm = 0;
+#pragma unroll
+      for (int j = 0; j < kMaxLeafCells; j++) {
+        const unsigned a = Q[j].x, b = Q[j].y;
+        const bool h = qdec_lo(a & 255u, L[0], sdn[0]) <= phi[0] && qdec_lo((a >> 8) & 255u, L[1], sdn[1]) <= phi[1] &&
+                       qdec_lo((a >> 16) & 255u, L[2], sdn[2]) <= phi[2] &&
+                       qdec_hi(a >> 24, L[0], H[0], sup[0]) >= plo[0] &&
+                       qdec_hi(b & 255u, L[1], H[1], sup[1]) >= plo[1] &&
+                       qdec_hi((b >> 8) & 255u, L[2], H[2], sup[2]) >= plo[2];
+        hm |= (unsigned)(h && j < ncell) << j;
+      }
+      while (hm) {
+        const int j = __ffs(hm) - 1;
+        hm &= hm - 1;
+        add_candidate((int)q, c0 + j, n, slots, ovf, ovf_cap, novf);
+      }
+    };
+    unsigned todo = __ballot_sync(0xffffffffu, inq && root >= 0);
+    while (todo) {
+      const int r = __shfl_sync(0xffffffffu, root, __ffs(todo) - 1);
+      const bool mine = ((todo >> lane) & 1u) && root == r;
+      todo &= ~__ballot_sync(0xffffffffu, mine);
+      const float4 RA = tnode[2 * r], RB = tnode[2 * r + 1];
+      const bool rh = mine && hit_ab(RA, RB, plo, phi);
+      if (!__any_sync(0xffffffffu, rh)) continue;
+      const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
+      if (rcnt > 0) {
+        leaf_cells(rlink, rcnt, r, rh);
+        continue;
+      }
+      int top = 0;
+      if (lane == 0) stk[0] = rlink;
+      top = 1;
+      __syncwarp();
+      bool overflow = false;
+      while (top > 0) {
+        const int base = stk[--top];
+        __syncwarp();
+        int lk[4], lc[4];
+        bool hk[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const float4 A = tnode[2 * (long long)(base + k)], B = tnode[2 * (long long)(base + k) + 1];
+          lk[k] = __float_as_int(B.z);
+          lc[k] = __float_as_int(B.w);
+          hk[k] = mine && hit_ab(A, B, plo, phi);  // empty slots hold an empty box
+        }
+        unsigned anyh = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) anyh |= (__any_sync(0xffffffffu, hk[k]) ? 1u : 0u) << k;
+        // internal children onto the stack (the lowest popped first), then the leaves
+#pragma unroll
+        for (int k = 3; k >= 0; k--)
+          if (((anyh >> k) & 1u) && lc[k] < 0) {
+            if (top >= kWarpStack) {
+              overflow = true;
+            } else {
+              if (lane == 0) stk[top] = lk[k];
+              top++;
+            }
+          }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (((anyh >> k) & 1u) && lc[k] > 0) leaf_cells(lk[k], lc[k], base + k, hk[k]);
+        if (overflow) {
+          if (lane == 0) atomicOr(err, kErrTraversalOverflow);
+          break;
+        }
+      }
+    }
+    if (inq) ncand_q[q] = n;
+  }
+}
+
 // Dense, query-ordered candidate list from the slots and the overflow list
 // (off = exclusive scan of the per-query counts).
 __global__ void k_gather_candidates(const int* __restrict__ slots, const int* __restrict__ ncand_q,
@@ -1725,6 +1853,9 @@ void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, con
   if (form == 0)
     k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf, err, skip_uhex);
+  else if (form == 2)  // split form, warp-cooperative
+    k_traverse_warp<<<blocks, 256, 0, st>>>(x, bi, qbox, tnode, qnode, qdon, nq, slots, ncand_q, ovf, ovf_cap, novf,
+                                            err, skip_uhex);
   else
     k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf, err, skip_uhex);
