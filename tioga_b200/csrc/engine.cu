@@ -968,8 +968,8 @@ int Engine::build_leaf_groups() {
   TB_CUDA(cudaMemcpyAsync(gl.p, hg.data(), ngrp_ * sizeof(int2), cudaMemcpyHostToDevice, stream_));
   TB_CUDA(cudaMemsetAsync(cnt.p + ngrp_, 0, sizeof(int), stream_));
   const unsigned grid = (unsigned)std::max(1ll, std::min((ngrp_ + 7) / 8, 148ll * 64));
-  k_group_nodes<false><<<grid, 256, 0, stream_>>>(gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, cnt.p, nullptr,
-                                                  nullptr, nullptr, nullptr);
+  launch_group_nodes(false, grid, stream_, gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, cnt.p, nullptr, nullptr,
+                     nullptr, nullptr);
   TB_LAUNCHED("k_group_nodes");
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, (int)(ngrp_ + 1), stream_);
@@ -979,8 +979,8 @@ int Engine::build_leaf_groups() {
   TB_CUDA(cudaMemcpyAsync(&total, off.p + ngrp_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
   TB_CUDA(cudaStreamSynchronize(stream_));
   TB_CUDA(grp_nodes_.ensure(std::max(1, total)));
-  k_group_nodes<true><<<grid, 256, 0, stream_>>>(gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, nullptr, off.p,
-                                                 grp_nodes_.p, cell_lidx_.p, grp_.p);
+  launch_group_nodes(true, grid, stream_, gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, nullptr, off.p,
+                     grp_nodes_.p, cell_lidx_.p, grp_.p);
   TB_LAUNCHED("k_group_nodes");
   TB_CUDA(cudaStreamSynchronize(stream_));  // the host list and the scratch go out of scope
   ngrp_nodes_ = total;

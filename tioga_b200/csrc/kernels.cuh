@@ -150,10 +150,9 @@ void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const 
                         const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                         const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
                         float4* tnode, double* tnode64, unsigned long long* acc);
-template <bool FILL>
-__global__ void k_group_nodes(const int2* grp_leaf, long long ngrp, const int4* leaves, const int* conn8,
-                              const unsigned char* cell_nv, int* cnt, const int* off, int* nodes, uint2* lidx,
-                              int4* grp);
+void launch_group_nodes(bool fill, unsigned grid, cudaStream_t st, const int2* grp_leaf, long long ngrp,
+                        const int4* leaves, const int* conn8, const unsigned char* cell_nv, int* cnt, const int* off,
+                        int* nodes, uint2* lidx, int4* grp);
 __global__ void k_tree_split(const unsigned long long* key, int n, const int* ca, const int* cb, const int* cslot,
                              int2* kids, int* nk, int* isint, int2* tlink, int* leaf_at);
 __global__ void k_tree_link(int n, const int* cslot, const int2* kids, const int* nk, const int* isint,

@@ -265,10 +265,15 @@ __global__ void __launch_bounds__(256) k_group_nodes(const int2* __restrict__ gr
     __syncwarp();
   }
 }
-template __global__ void k_group_nodes<false>(const int2*, long long, const int4*, const int*, const unsigned char*,
-                                              int*, const int*, int*, uint2*, int4*);
-template __global__ void k_group_nodes<true>(const int2*, long long, const int4*, const int*, const unsigned char*,
-                                             int*, const int*, int*, uint2*, int4*);
+// host launcher (the template's instantiations live in this translation unit)
+void launch_group_nodes(bool fill, unsigned grid, cudaStream_t st, const int2* grp_leaf, long long ngrp,
+                        const int4* leaves, const int* conn8, const unsigned char* cell_nv, int* cnt, const int* off,
+                        int* nodes, uint2* lidx, int4* grp) {
+  if (fill)
+    k_group_nodes<true><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
+  else
+    k_group_nodes<false><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
+}
 
 // first leaf of every block that has leaves (leaves are in storage order,
 // which is block-major)
