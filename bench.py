@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--impl", default="tioga_b200", choices=["tioga_b200", "reference"])
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-systems", type=int, default=16,
+                   help="--impl reference with cfg2/cfg3: systems of the distribution in the CPU sample")
     p.add_argument("--no-cpu-full", action="store_true",
                    help="skip the one full-size connectivity call of the compiled reference")
     p.add_argument("--no-parity", action="store_true",
@@ -989,11 +991,119 @@ def cpu_reference_full(system):
             "sample": "the full timed configuration, one connectivity call"}
 
 
+def _ref_batch_worker(job):
+    """One process of the batched/served CPU baseline: the compiled reference
+    runs its share of the systems one after another (the reference's way of
+    running independent systems, one instance at a time)."""
+    kind, nsys, seed, share, steps, nvar = job
+    sys.path.insert(0, ROOT)
+    from tioga_b200.serving import apply_rigid, rigid
+    systems = cases.config2(seed, nsys=nsys)
+    rng = np.random.default_rng(1000 + share[0] if share else 0)
+    out = []
+    for k in share:
+        s = systems[k]
+        t = TiogaLibrary(REF_LIB)
+        t.init()
+        t.register_system(s)
+        if kind == "cfg2":
+            t0 = time.perf_counter()
+            t.preprocess_grids()
+            t1 = time.perf_counter()
+            t.performconnectivity()
+            t2 = time.perf_counter()
+            out.append({"system": k, "preprocess_s": t1 - t0, "connectivity_s": t2 - t1})
+        else:  # one request = a time step: rigid motions, preprocess, connectivity, data update
+            qs = [rng.uniform(-1.0, 1.0, b.nnodes * nvar) for b in s.blocks]
+            for _ in range(steps):
+                t0 = time.perf_counter()
+                for i, b in enumerate(s.blocks[1:], start=1):
+                    x = t.blocks[b.tag]["x"].reshape(-1, 3)
+                    A, bb = rigid(rng, x[:: max(1, b.nnodes // 64)].mean(axis=0), 2.0, 0.0)
+                    x[:] = apply_rigid(x, A, bb)
+                t.preprocess_grids()
+                t.performconnectivity()
+                for b, q in zip(s.blocks, qs):  # after the connectivity call, as the reference wants
+                    t.registersolution(b.tag, q)
+                t.dataupdate_mb(nvar, "row")
+                out.append({"system": k, "request_s": time.perf_counter() - t0})
+        t.delete()
+    return out
+
+
+def cpu_reference_batch(kind: str, nsys: int = 16, steps: int = 2, procs: int = 0):
+    """The batched (cfg2) or served (cfg3) workload on the CPU: the compiled
+    reference on a sample of `nsys` systems of the distribution, the systems
+    dealt round-robin to P independent processes (P = the host's cores, at
+    most nsys), rates summed: query points over the slowest process's busy
+    time.  Query counts come from the digest fixture of the first 16 cfg2
+    systems (cfg2) or from the oracle's query lists (cfg3)."""
+    import multiprocessing as mp
+    if not os.path.exists(REF_LIB):
+        return None, "the compiled reference is not built (make -C oracle ref)"
+    P = max(1, min(procs or os.cpu_count() or 1, nsys))
+    seed = 2 if kind == "cfg2" else 3
+    jobs = [(kind, nsys, seed, list(range(r, nsys, P)), steps, 5) for r in range(P)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(P) as pool:
+        parts = pool.map(_ref_batch_worker, jobs)
+    wall = time.perf_counter() - t0
+    if kind == "cfg2":
+        fix = np.load(os.path.join(GOLDEN, "cfg2_16.npz"))
+        qp = [int(v) for v in fix["query_points"]]
+        if nsys > len(qp):
+            return None, "query counts are stored for the first 16 systems only"
+        busy = [sum(r["connectivity_s"] for r in part) for part in parts]
+        Q = sum(qp[:nsys])
+        return {"value": Q / max(busy), "unit": UNIT, "cores": P, "kind": "reference",
+                "sample": f"the first {nsys} systems of the cfg2 distribution, one connectivity call each, "
+                          f"dealt to {P} processes (rates summed: all query points over the busiest process's "
+                          f"connectivity time)",
+                "query_points": Q, "busiest_process_s": max(busy), "wall_s": wall,
+                "preprocess_s": sum(r["preprocess_s"] for part in parts for r in part)}, None
+    systems = cases.config2(seed, nsys=nsys)
+    qsys = []
+    for s in systems:  # Q per request (rigid motions change it little; the unmoved count stands in)
+        t = TiogaLibrary(PORT_LIB)
+        t.init()
+        t.register_system(s)
+        t.preprocess_grids()
+        t.performconnectivity()
+        ns, nd, tot = C.c_int(), C.c_int(), 0
+        for b in s.blocks:
+            t.lib.tioga_oracle_searchstats(C.c_int(b.tag), C.byref(ns), C.byref(nd))
+            tot += ns.value
+        t.delete()
+        qsys.append(tot)
+    lat = [r["request_s"] for part in parts for r in part]
+    busy = [sum(r["request_s"] for r in part) for part in parts]
+    Q = sum(qsys[r["system"]] for part in parts for r in part)
+    return {"value": Q / max(busy), "unit": UNIT, "cores": P, "kind": "reference",
+            "sample": f"{nsys} systems of the cfg3 distribution, {steps} requests each (rigid motion, preprocess, "
+                      f"connectivity, 5-field data update), dealt to {P} processes",
+            "requests_per_s": len(lat) / max(busy),
+            "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))},
+            "wall_s": wall}, None
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         if rank != 0:
+            return 0
+        if args.workload in ("cfg2", "cfg3"):
+            res, why = cpu_reference_batch(args.workload, nsys=args.ref_systems, steps=args.steps)
+            if res is None:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+                return 0
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+                              "n_gpus": ws, "higher_is_better": True, "dtype": "f64",
+                              "config": {"workload": WORKLOAD2 if args.workload == "cfg2" else
+                                         WORKLOAD3.format(n=args.ref_systems), "sample": res["sample"]},
+                              "cpu_baseline": res,
+                              "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
             return 0
         res, why = cpu_reference(args.steps, args.warmup)
         if res is None:
