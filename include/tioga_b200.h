@@ -315,6 +315,16 @@ void tioga_b200_set_stream_(void *stream);
 int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights, const int *d_nweights,
                                     const int *d_receptor, int nrec, double *d_q, long long nnodes,
                                     int nvar, int interptype, void *stream);
+/* Node global ids of block btag (nnodes uint64_t; caller-owned, kept like the
+ * other registered arrays): the node_gid of tioga::registerGridData
+ * (src/tioga.C:64-85), which the C API does not pass. */
+void tioga_b200_registernodegid_(int *btag, uint64_t *node_gid);
+/* *on = 1: coincident query points of a donor are merged by node global id
+ * (uniquenode_map, src/search.C:48-74), as the reference built with
+ * TIOGA_HAS_NODEGID does, instead of by the octree over their coordinates;
+ * every block then needs its node ids (tioga_b200_registernodegid_).  The
+ * high-order point search keeps the octree merge. */
+void tioga_b200_set_nodegid_merge_(int *on);
 /* tioga::set_uniform_hex_flag (src/tioga.h:195-201), which the reference
  * offers through its C++ class only: at the next preprocess, block btag is
  * tested for a box of identical rectangular hexahedra

@@ -108,6 +108,10 @@ typedef struct {
   /* uniform-hex fast path (MeshBlock.h:96-117: check_uniform_hex_flag,
      uniform_hex, obh, dx, xlow, idims, uindx) */
   int check_uniform_flag, uniform_hex;
+  /* node global ids (registerGridData's node_gid, MeshBlock.C:61) and, with
+     the node-GID variant, the query points' ids (gid_search) */
+  const uint64_t *node_gid;
+  uint64_t *gid_search;
   obb_t obh;
   double hdx[3], xlow[3];
   int idims[3];
@@ -135,6 +139,7 @@ static struct {
   void (*convert_to_modal)(int *, int *, double *, int *, int *, double *);
   void (*block_hook)(int); /* oracle only: names the block before callbacks */
   double *search_rst;      /* rst of the query being searched */
+  int nodegid;             /* the TIOGA_HAS_NODEGID build's behaviour, switched at run time */
 } G;
 
 #define NFRAC 1331
@@ -918,6 +923,7 @@ static void exchange_search_data(void) {
     free(b->tagsearch); b->tagsearch = NULL;
     free(b->donorId); b->donorId = NULL;
     free(b->res_search); b->res_search = NULL;
+    free(b->gid_search); b->gid_search = NULL;
   }
   int **lists = (int **)malloc(sizeof(int *) * (G.npairs + 1));
   int *counts = (int *)malloc(sizeof(int) * (G.npairs + 1));
@@ -935,6 +941,7 @@ static void exchange_search_data(void) {
     b->isearch = (int *)malloc(sizeof(int) * 3 * b->nsearch);
     b->tagsearch = (int *)malloc(sizeof(int) * b->nsearch);
     b->donorId = (int *)malloc(sizeof(int) * b->nsearch);
+    if (G.nodegid) b->gid_search = (uint64_t *)malloc(sizeof(uint64_t) * b->nsearch);
   }
   int *fill = (int *)calloc(G.nblocks, sizeof(int));
   for (int p = 0; p < G.npairs; p++) {
@@ -948,6 +955,7 @@ static void exchange_search_data(void) {
       don->tagsearch[q] = rec->tag;
       for (int k = 0; k < 3; k++) don->xsearch[3 * q + k] = rec->x[3 * node + k];
       don->res_search[q] = rec->nodeRes[node];
+      if (G.nodegid) don->gid_search[q] = rec->node_gid ? rec->node_gid[node] : 0; /* exchangeSearchData.C:226-231 */
     }
     free(lists[p]);
   }
@@ -1164,6 +1172,60 @@ static void uniq_tree(const double *coord, int *itag, double *rtag, const int *m
 /* ======================================================================= */
 /* search: src/search.C:78-269                                             */
 /* ======================================================================= */
+/* uniquenode_map (search.C:48-74), the TIOGA_HAS_NODEGID build's merge of
+   coincident query points: the first query with a node id is the
+   representative of every later one with that id, its resolution the
+   maximum over them, copied to all of them.  (The reference uses a hash map;
+   a sort by id gives the same first occurrences.) */
+static int cmp_gid_pos(const void *a, const void *b) {
+  const uint64_t *x = (const uint64_t *)a, *y = (const uint64_t *)b;
+  if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+  return x[1] < y[1] ? -1 : (x[1] > y[1]);
+}
+
+static void uniquenode_map(const uint64_t *ids, double *res, int *itag, int n) {
+  uint64_t *kv = (uint64_t *)malloc(sizeof(uint64_t) * 2 * (n ? n : 1));
+  for (int i = 0; i < n; i++) {
+    kv[2 * i] = ids[i];
+    kv[2 * i + 1] = (uint64_t)i;
+  }
+  qsort(kv, n, 2 * sizeof(uint64_t), cmp_gid_pos);
+  for (int s = 0; s < n;) {
+    int e = s + 1;
+    while (e < n && kv[2 * e] == kv[2 * s]) e++;
+    const int first = (int)kv[2 * s + 1];
+    itag[first] = first;
+    for (int k = s + 1; k < e; k++) { /* in index order, as the sequential loop visits them */
+      const int i = (int)kv[2 * k + 1];
+      itag[i] = first;
+      res[first] = (res[first] > res[i]) ? res[first] : res[i];
+    }
+    s = e;
+  }
+  for (int i = 0; i < n; i++) res[i] = res[itag[i]];
+  free(kv);
+}
+
+static void merge_coincident(block_t *b) {
+  free(b->xtag);
+  b->xtag = (int *)malloc(sizeof(int) * b->nsearch);
+  if (G.nodegid) {
+    uniquenode_map(b->gid_search, b->res_search, b->xtag, b->nsearch);
+    return;
+  }
+  int *avail = (int *)malloc(sizeof(int) * b->nsearch);
+  for (int i = 0; i < b->nsearch; i++) avail[i] = b->xtag[i] = i;
+  uniq_tree(b->xsearch, b->xtag, b->res_search, b->tagsearch, avail, b->nsearch);
+  free(avail);
+}
+
+void tioga_oracle_set_node_gid(int btag, const uint64_t *gid) {
+  int ib = find_tag(btag);
+  if (ib >= 0) G.b[ib]->node_gid = gid;
+}
+
+void tioga_oracle_set_nodegid_merge(int on) { G.nodegid = on; }
+
 /* ----------------------------------------------------------------------- */
 /* uniform-hex fast path: MeshBlock::check_for_uniform_hex (MeshBlock.C:1249-  */
 /* 1372), create_hex_cell_map (:1374-1409), search_uniform_hex (search.C:     */
@@ -1281,14 +1343,7 @@ static void create_hex_cell_map(block_t *b) {
    in practice, so the loop runs while the current pick is missing (-1) or a
    cell of BIG resolution, as restated here. */
 static void search_uniform_hex(block_t *b) {
-  free(b->xtag);
-  b->xtag = (int *)malloc(sizeof(int) * b->nsearch);
-  {
-    int *avail = (int *)malloc(sizeof(int) * b->nsearch);
-    for (int i = 0; i < b->nsearch; i++) avail[i] = b->xtag[i] = i;
-    uniq_tree(b->xsearch, b->xtag, b->res_search, b->tagsearch, avail, b->nsearch);
-    free(avail);
-  }
+  merge_coincident(b);
   double xvec[8][3];
   for (int jj = 0; jj < 8; jj++)
     for (int k = 0; k < 3; k++) xvec[jj][k] = (2 * ((jj & (1 << k)) >> k) - 1) * 2 * TOLV;
@@ -1400,14 +1455,7 @@ static void search_block(block_t *b) {
   }
   free(icell);
   adt_build(b);
-  free(b->xtag);
-  b->xtag = (int *)malloc(sizeof(int) * b->nsearch);
-  {
-    int *avail = (int *)malloc(sizeof(int) * b->nsearch);
-    for (int i = 0; i < b->nsearch; i++) avail[i] = b->xtag[i] = i;
-    uniq_tree(b->xsearch, b->xtag, b->res_search, b->tagsearch, avail, b->nsearch);
-    free(avail);
-  }
+  merge_coincident(b);
   for (int i = 0; i < b->nsearch; i++) {
     if (b->xtag[i] == i) {
       int ci[2];
@@ -1712,7 +1760,7 @@ static void free_block(block_t *b) {
   free(b->interp); free(b->interp2donor); free(b->cancel_nodes);
   free(b->ctag); free(b->ppc); free(b->rxyz); free(b->rst);
   free(b->i2_inode0); free(b->i2_nw); free(b->i2_rinfo); free(b->i2_w);
-  free(b->uindx);
+  free(b->uindx); free(b->gid_search);
   if (b->own_iblank_cell) free(b->iblank_cell);
   free(b);
 }

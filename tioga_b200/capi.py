@@ -56,7 +56,7 @@ class TiogaLibrary:
         self._order.clear()
 
     # -- registration ------------------------------------------------------
-    def registergrid_data_mb(self, bid: int, block, ibl=None, cell_gid=None):
+    def registergrid_data_mb(self, bid: int, block, ibl=None, cell_gid=None, node_gid=None):
         """Register one cases.Block under block id ``bid`` (1-based).  ``ibl``
         may supply the iblank array (e.g. pinned host memory); ``cell_gid``
         the cells' uint64 global ids (tioga_b200_registercellgid_ here; the
@@ -87,12 +87,24 @@ class TiogaLibrary:
             gid = np.ascontiguousarray(cell_gid, dtype=np.uint64)
             assert gid.shape == (block.ncells,)
             self._keep.append(gid)
-        if gid is not None and hasattr(self.lib, "refshim_registergrid_gid_"):
+        ngid = None
+        if node_gid is not None:
+            ngid = np.ascontiguousarray(node_gid, dtype=np.uint64)
+            assert ngid.shape == (block.nnodes,)
+            self._keep.append(ngid)
+        if ngid is not None and hasattr(self.lib, "refshim_registergrid_gids_"):
+            self.lib.refshim_registergrid_gids_(None if gid is None else _ptr(gid), _ptr(ngid), *regargs)
+        elif gid is not None and hasattr(self.lib, "refshim_registergrid_gid_"):
             self.lib.refshim_registergrid_gid_(_ptr(gid), *regargs)
         else:
             self.lib.tioga_registergrid_data_mb_(*regargs)
             if gid is not None:
                 self.lib.tioga_b200_registercellgid_(C.byref(ctag), _ptr(gid))
+            if ngid is not None:
+                if hasattr(self.lib, "tioga_oracle_set_node_gid"):
+                    self.lib.tioga_oracle_set_node_gid(C.c_int(block.tag), _ptr(ngid))
+                else:
+                    self.lib.tioga_b200_registernodegid_(C.byref(ctag), _ptr(ngid))
         self.blocks[block.tag] = {"x": x, "iblank": ibl, "nnodes": block.nnodes,
                                   "ncells": block.ncells, "bid": bid}
         if block.tag not in self._order:
@@ -130,10 +142,11 @@ class TiogaLibrary:
     def select_system(self, sys: int):
         self.lib.tioga_b200_select_system_(_iref(sys))
 
-    def register_system(self, system, iblanks=None, cell_gids=None):
+    def register_system(self, system, iblanks=None, cell_gids=None, node_gids=None):
         for bid, b in enumerate(system.blocks, start=1):
             self.registergrid_data_mb(bid, b, None if iblanks is None else iblanks[bid - 1],
-                                      None if cell_gids is None else cell_gids[bid - 1])
+                                      None if cell_gids is None else cell_gids[bid - 1],
+                                      None if node_gids is None else node_gids[bid - 1])
 
     # -- settings ----------------------------------------------------------
     def setsymmetry(self, isym: int):
@@ -210,15 +223,17 @@ class TiogaLibrary:
 
 def run_system(lib_path: str, system, q_blocks=None, nvar: int = 5, itype: str = "row",
                isym=None, nfringe=None, mexclude=None, resolutions=None, setup=None, after=None,
-               cell_gids=None):
+               cell_gids=None, node_gids=None):
     """Drive one library through the full TIOGA call sequence and collect
     every observable: iblank per block, donor info per block and the updated
     fields.  ``q_blocks`` are copied (the library updates them in place).
     With ``cell_gids`` (per block, uint64 per cell) the blocks carry cell
-    global ids and ``out["receptorinfo"]`` is getReceptorInfo's result."""
+    global ids and ``out["receptorinfo"]`` is getReceptorInfo's result; with
+    ``node_gids`` (per block, uint64 per node) the blocks carry node global
+    ids (the node-GID merge of coincident query points uses them)."""
     t = TiogaLibrary(lib_path)
     t.init()
-    t.register_system(system, cell_gids=cell_gids)
+    t.register_system(system, cell_gids=cell_gids, node_gids=node_gids)
     if isym is not None:
         t.setsymmetry(isym)
     if nfringe is not None:

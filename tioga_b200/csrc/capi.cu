@@ -306,6 +306,17 @@ void tioga_b200_stats_(long long out[16]) {
   out[15] = s.ngroup_nodes;
 }
 
+void tioga_b200_registernodegid_(int* btag, uint64_t* node_gid) {
+  if (ready("tioga_b200_registernodegid_")) set_rc(g_tg->set_node_gid(*btag, node_gid));
+}
+
+void tioga_b200_set_nodegid_merge_(int* on) {
+  if (ready("tioga_b200_set_nodegid_merge_")) {
+    g_tg->set_nodegid_merge(*on);
+    set_rc(0);
+  }
+}
+
 void tioga_b200_set_uniform_hex_flag_(int* btag, int* flag) {
   if (ready("tioga_b200_set_uniform_hex_flag_")) set_rc(g_tg->set_uniform_hex_flag(*btag, *flag));
 }

@@ -58,6 +58,8 @@ Engine::~Engine() {
   mkey_.release(); mkey_alt_.release(); mval_alt_.release();
   d_pcand_.release(); d_pfirst_.release(); d_chunks_.release(); d_chunk_cta_.release(); d_pair_t0_.release();
   rf_red_.release(); rf_tmp_.release(); rf_was_.release(); uhex_map_.release(); uhex_red_.release();
+  node_gid_d_.release(); gm_k0_.release(); gm_k1_.release(); gm_max_.release(); gm_a_.release(); gm_b_.release();
+  gm_c_.release(); gm_d_.release();
   d_wall_.release(); wall_cells_.release(); wall_box_.release(); wall_box_first_.release();
   cg_cnt_.release(); cg_off_.release(); cg_v0_.release(); cg_v1_.release(); cg_k0_.release(); cg_k1_.release();
   cg_flag_.release();
@@ -1128,7 +1130,8 @@ int Engine::run_queries() {
     TB_LAUNCHED("k_query_write");
   }
   dedup_ran_ = false;
-  if (dedup_active_ && nq > 0) TB_TRY(run_dedup());
+  if (nodegid_merge_ && nq > 0) TB_TRY(run_gid_merge());
+  else if (dedup_active_ && nq > 0) TB_TRY(run_dedup());
   return 0;
 }
 
@@ -1294,6 +1297,104 @@ int Engine::run_dedup() {
   qoff[npairs_] = (int)nq_;
   DedupQueries Q{nq_, qnode_.p, qdon_.p, nullptr, nullptr, qres_.p, x_.p, node_blk_.p};
   TB_TRY(dedup_merge(Q, qoff));
+  dedup_ran_ = true;
+  return 0;
+}
+
+// The node-global-id merge (the TIOGA_HAS_NODEGID build's uniquenode_map,
+// search.C:48-74) over the node queries: every donor's list in the
+// reference's order (the same keys as the octree merge), then each (donor,
+// node id) run's first entry represents the others and takes their largest
+// resolution.  Every block needs its node ids.
+int Engine::run_gid_merge() {
+  const long long n = nq_;
+  for (const HostBlock& H : hb_)
+    if (!H.node_gid) {
+      fprintf(stderr, "#tioga_b200: the node-id merge needs every block's node ids (tioga_b200_registernodegid_)\n");
+      return -1;
+    }
+  TB_CUDA(node_gid_d_.ensure(ntot_));
+  for (size_t b = 0; b < hb_.size(); b++)
+    TB_CUDA(cudaMemcpyAsync(node_gid_d_.p + bi_[b].node_off, hb_[b].node_gid, hb_[b].nnodes * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, stream_));
+  std::vector<int> h_toff(h_pair_t0_.back() + 1);
+  TB_CUDA(cudaMemcpyAsync(h_toff.data(), tile_off_.p, h_toff.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<int> qoff(npairs_ + 1);
+  for (int p = 0; p < npairs_; p++) qoff[p] = h_toff[h_pair_t0_[p]];
+  qoff[npairs_] = (int)n;
+  // the donors' lists in the reference's order: position i holds query refq[i]
+  const int np = npairs_;
+  std::vector<int> prank(np), seen(hb_.size(), 0);
+  for (int p = 0; p < np; p++) prank[p] = seen[h_pairs_[p].don]++;
+  TB_CUDA(dd_pqoff_.ensure(np + 1));
+  TB_CUDA(dd_prank_.ensure(np));
+  TB_CUDA(cudaMemcpyAsync(dd_pqoff_.p, qoff.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaMemcpyAsync(dd_prank_.p, prank.data(), np * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(dd_key_.ensure(n));
+  TB_CUDA(dd_key2_.ensure(n));
+  TB_CUDA(dd_perm_.ensure(n));
+  TB_CUDA(dd_refq_.ensure(n));
+  TB_CUDA(dd_x_.ensure(3 * n));
+  TB_CUDA(dd_mtag_.ensure(n));
+  TB_CUDA(dd_rtag_.ensure(n));
+  TB_CUDA(dd_itag_.ensure(n));
+  TB_CUDA(q_gpos_.ensure(n));
+  TB_CUDA(q_xt_.ensure(n));
+  TB_CUDA(q_rep_.ensure(n));
+  k_dedup_keys<<<grid_for(n, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, n, dd_pqoff_.p, np, dd_prank_.p, node_bin_.p,
+                                                    dd_key_.p, dd_perm_.p);
+  TB_LAUNCHED("k_dedup_keys");
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, dd_key_.p, dd_key2_.p, dd_perm_.p, dd_refq_.p, (int)n, 0, 64,
+                                  stream_);
+  k_dedup_gather<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, qnode_.p, qres_.p, x_.p, node_blk_.p, nullptr,
+                                                      d_bi_.p, dd_x_.p, dd_mtag_.p, dd_rtag_.p, dd_itag_.p,
+                                                      dd_perm_.p, q_gpos_.p);
+  TB_LAUNCHED("k_dedup_gather");
+  // (donor, node id) runs in position order: stable sorts by id, then by donor
+  TB_CUDA(gm_k0_.ensure(n));
+  TB_CUDA(gm_k1_.ensure(n));
+  TB_CUDA(gm_max_.ensure(n));
+  TB_CUDA(gm_a_.ensure(n));
+  TB_CUDA(gm_b_.ensure(n));
+  TB_CUDA(gm_c_.ensure(n));
+  TB_CUDA(gm_d_.ensure(n));
+  k_gid_keys<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, qnode_.p, qdon_.p, node_gid_d_.p, gm_k0_.p,
+                                                  gm_a_.p, gm_b_.p);  // id, donor, position (by position)
+  TB_LAUNCHED("k_gid_keys");
+  tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, gm_k0_.p, gm_k1_.p, gm_b_.p, gm_c_.p, (int)n, 0, 64, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, gm_k0_.p, gm_k1_.p, gm_b_.p, gm_c_.p, (int)n, 0, 64, stream_);
+  k_gather_i32<<<grid_for(n, kT), kT, 0, stream_>>>(gm_a_.p, gm_c_.p, n, gm_d_.p);  // donors in id order
+  TB_LAUNCHED("k_gather_i32");
+  tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, gm_d_.p, gm_b_.p, gm_c_.p, dd_perm_.p, (int)n, 0, 16, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, gm_d_.p, gm_b_.p, gm_c_.p, dd_perm_.p, (int)n, 0, 16, stream_);
+  // dd_perm_: positions sorted by (donor, id, position); ids and donors by position: gm_k0_ was sorted in
+  // place into gm_k1_, so take the ids again
+  k_gid_keys<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, qnode_.p, qdon_.p, node_gid_d_.p, gm_k0_.p,
+                                                  gm_a_.p, gm_b_.p);
+  TB_LAUNCHED("k_gid_keys");
+  k_gid_heads<<<grid_for(n, kT), kT, 0, stream_>>>(dd_perm_.p, n, gm_k0_.p, gm_a_.p, gm_c_.p);
+  TB_LAUNCHED("k_gid_heads");
+  tmp = 0;
+  cub::DeviceScan::InclusiveScan(nullptr, tmp, gm_c_.p, gm_d_.p, cub::Max(), (int)n, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceScan::InclusiveScan(cub_tmp_.p, tmp, gm_c_.p, gm_d_.p, cub::Max(), (int)n, stream_);
+  TB_CUDA(cudaMemsetAsync(gm_max_.p, 0, n * sizeof(unsigned long long), stream_));
+  k_gid_apply<<<grid_for(n, kT), kT, 0, stream_>>>(dd_perm_.p, gm_d_.p, n, dd_itag_.p, dd_rtag_.p, gm_max_.p);
+  TB_LAUNCHED("k_gid_apply");
+  k_gid_res<<<grid_for(n, kT), kT, 0, stream_>>>(dd_itag_.p, n, gm_max_.p, dd_rtag_.p);
+  TB_LAUNCHED("k_gid_res");
+  k_dedup_apply<<<grid_for(n, kT), kT, 0, stream_>>>(dd_refq_.p, n, dd_itag_.p, dd_rtag_.p, qres_.p, q_xt_.p,
+                                                     q_rep_.p, err_.p, counters_.p);
+  TB_LAUNCHED("k_dedup_apply");
+  TB_CUDA(cudaStreamSynchronize(stream_));  // host staging vectors go out of scope
   dedup_ran_ = true;
   return 0;
 }
@@ -1970,6 +2071,13 @@ int Engine::donor_info(int tag, int* receptors, int* indices, double* frac) {
     receptors[k++] = rb - bi_[rb].sblk0;  // the receptor block's index within its system
     receptors[k++] = nv;
   }
+  return 0;
+}
+
+int Engine::set_node_gid(int tag, const uint64_t* gid) {
+  int ib = find_tag(tag);
+  if (ib < 0) return -1;
+  hb_[ib].node_gid = gid;
   return 0;
 }
 

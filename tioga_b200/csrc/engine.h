@@ -204,6 +204,7 @@ struct HostBlock {
   double* user_nres = nullptr;
   double* user_cres = nullptr;
   int* h_iblank_cell = nullptr;  // caller array (tioga_setcelliblank_)
+  const uint64_t* node_gid = nullptr;  // caller's node global ids (registerGridData's node_gid)
   int uniform_flag = 0;          // tioga::set_uniform_hex_flag: check for a uniform box at preprocess
   int uniform = 0;               // found uniform at the last preprocess
   double* hq = nullptr;          // registered host solution
@@ -319,6 +320,8 @@ class Engine {
   int donor_info(int tag, int* receptors, int* indices, double* frac);
   int set_cell_gid(int tag, const uint64_t* gid);
   int set_uniform_hex_flag(int tag, int flag);
+  int set_node_gid(int tag, const uint64_t* gid);
+  void set_nodegid_merge(int on) { nodegid_merge_ = on != 0; }
   // tioga::getReceptorInfo: 4 ints per live record of the selected system;
   // writes min(count, cap) ints to out (may be null) and returns the count,
   // or < 0 on error
@@ -343,6 +346,7 @@ class Engine {
   int run_pairs_and_refit();
   int build_leaf_groups();
   int setup_uniform_hex();
+  int run_gid_merge();
   int run_queries();
   int run_search();
   int run_donors();
@@ -523,6 +527,9 @@ class Engine {
   DBuf<int> uhex_map_;                  // cell maps of the uniform-hex blocks
   DBuf<unsigned long long> uhex_red_;   // set-up scratch: extents, check flag
   bool any_uhex_ = false;
+  bool nodegid_merge_ = false;         // coincident query points merged by node id (TIOGA_HAS_NODEGID)
+  DBuf<unsigned long long> node_gid_d_, gm_k0_, gm_k1_, gm_max_;
+  DBuf<int> gm_a_, gm_b_, gm_c_, gm_d_;
   DBuf<unsigned long long> counters_;
   DBuf<unsigned long long> mkey_, mkey_alt_;
   DBuf<int> mval_alt_;

@@ -272,6 +272,14 @@ __global__ void k_dedup_leaves(const int4* leaves, int nleaves, const int* perm,
 __global__ void k_dedup_apply(const int* refq, long long n, const int* itag, const double* rtag, double* qres,
                               int* q_xt, int* q_rep, unsigned* err, unsigned long long* counters);
 __global__ void k_dedup_copy(const int* q_rep, long long nq, int* qcell, unsigned char* qtie);
+__global__ void k_gid_keys(const int* refq, long long n, const int* qnode, const int* qdon,
+                           const unsigned long long* node_gid, unsigned long long* gkey, int* dkey16, int* pos);
+__global__ void k_gid_heads(const int* pos, long long n, const unsigned long long* gkey_of_pos, const int* don_of_pos,
+                            int* head);
+__global__ void k_gid_apply(const int* pos, const int* first, long long n, int* itag, const double* rtag,
+                            unsigned long long* rmax);
+__global__ void k_gid_res(const int* itag, long long n, const unsigned long long* rmax, double* rtag);
+__global__ void k_gather_i32(const int* src, const int* idx, long long n, int* out);
 __global__ void k_reset_coincident_min(const int* interp2rec, const int* q_xt, long long nq,
                                        const unsigned char* it_cancel, int* ireset);
 __global__ void k_reset_coincident_set(const int* interp2rec, const int* q_xt, long long nq, const int* ireset,

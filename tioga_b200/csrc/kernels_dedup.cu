@@ -324,6 +324,67 @@ __global__ void k_dedup_apply(const int* __restrict__ refq, long long n, const i
   }
 }
 
+// ---------------------------------------------------------------------------
+// The node-global-id merge (uniquenode_map, search.C:48-74, in the build with
+// TIOGA_HAS_NODEGID): in every donor's list (positions in the reference's
+// order), the first query with a node id represents all later ones with that
+// id and takes their largest resolution.  Positions are sorted stably by id,
+// then by donor block, so each (donor, id) run is in position order.
+// ---------------------------------------------------------------------------
+__global__ void k_gid_keys(const int* __restrict__ refq, long long n, const int* __restrict__ qnode,
+                           const int* __restrict__ qdon, const unsigned long long* __restrict__ node_gid,
+                           unsigned long long* __restrict__ gkey, int* __restrict__ dkey16, int* __restrict__ pos) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int q = refq[i];
+    gkey[i] = node_gid[qnode[q]];
+    dkey16[i] = qdon[q];
+    pos[i] = (int)i;
+  }
+}
+
+// sorted index j: head of its (donor, id) run -> j, else 0 (a max-scan then
+// gives every entry its run's first index)
+__global__ void k_gid_heads(const int* __restrict__ pos, long long n, const unsigned long long* __restrict__ gkey_of_pos,
+                            const int* __restrict__ don_of_pos, int* __restrict__ head) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    bool h = j == 0;
+    if (!h) {
+      const int a = pos[j], b = pos[j - 1];
+      h = gkey_of_pos[a] != gkey_of_pos[b] || don_of_pos[a] != don_of_pos[b];
+    }
+    head[j] = h ? (int)j : 0;
+  }
+}
+
+// itag[position] = its run's first position; the run's largest resolution at
+// that first position (ordered keys, exact)
+__global__ void k_gid_apply(const int* __restrict__ pos, const int* __restrict__ first, long long n,
+                            int* __restrict__ itag, const double* __restrict__ rtag,
+                            unsigned long long* __restrict__ rmax) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int rep = pos[first[j]];
+    itag[pos[j]] = rep;
+    atomicMax(&rmax[rep], dkey(rtag[pos[j]]));
+  }
+}
+
+__global__ void k_gather_i32(const int* __restrict__ src, const int* __restrict__ idx, long long n,
+                             int* __restrict__ out) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x)
+    out[j] = src[idx[j]];
+}
+
+__global__ void k_gid_res(const int* __restrict__ itag, long long n, const unsigned long long* __restrict__ rmax,
+                          double* __restrict__ rtag) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    if (itag[i] == (int)i) rtag[i] = dkey_inv(rmax[i]);
+}
+
 // after the search: a merged query takes its representative's donor
 __global__ void k_dedup_copy(const int* __restrict__ q_rep, long long nq, int* __restrict__ qcell,
                              unsigned char* __restrict__ qtie) {
