@@ -91,7 +91,7 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
-    p.add_argument("--forms", default="split,plain,e2e",
+    p.add_argument("--forms", default="split,plain,e2e,e2e_pageable",
                    help="comma list of measured forms (the first one gives `value`)")
     return p.parse_args()
 
@@ -425,8 +425,48 @@ def run_gpu(args, ws, rank, local, dist):
     lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
     lib.delete()
     del keep
+    if "e2e_pageable" in forms:
+        out["e2e_pageable"] = time_e2e_pageable(system, stream, args.steps, args.warmup, ws)
     out["_system"] = system
     return out
+
+
+def time_e2e_pageable(system, stream, steps: int, warmup: int, ws: int):
+    """e2e with the caller's arrays in ordinary pageable memory (numpy), as a
+    Fortran or C solver would pass them: the library page-locks them at its
+    first preprocess (tioga_b200_set_pin_host_, on by default), so every
+    later call copies at the pinned rate."""
+    import torch
+
+    import tioga_b200 as tb
+    lib = TiogaLibrary(tb.library_path())
+    tb.extras(lib.lib)
+    lib.init()
+    lib.register_system(system)  # numpy arrays: pageable host memory
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(stream.cuda_stream))
+    tb.set_int(lib.lib, "tioga_b200_set_precision_", 1)
+    t0 = time.perf_counter()
+    lib.preprocess_grids()
+    pin_s = time.perf_counter() - t0
+    for _ in range(max(1, warmup)):
+        lib.performconnectivity()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        lib.performconnectivity()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    err = lib.lib.tioga_b200_last_error()
+    Q = tb.stats(lib.lib)["nquery"]
+    lib.lib.tioga_b200_set_stream_(C.c_void_p(0))
+    lib.delete()
+    if err:
+        return {"error": f"connectivity failed ({err})"}
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": ws * Q / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "first_preprocess_s": pin_s,
+            "note": "caller arrays in pageable memory, page-locked by the library at its first preprocess"}
 
 
 def time_dataupdate(lib, system, stream, nreceptor: int, steps: int, warmup: int, nvar: int = 5):

@@ -315,6 +315,12 @@ void tioga_b200_set_stream_(void *stream);
 int tioga_b200_interpolate_noalloc_(const int *d_inode, const double *d_weights, const int *d_nweights,
                                     const int *d_receptor, int nrec, double *d_q, long long nnodes,
                                     int nvar, int interptype, void *stream);
+/* Page-locking of the caller's arrays (on by default): at the next
+ * preprocess that uploads the topology, pageable coordinate and iblank
+ * arrays are registered with cudaHostRegister (they must stay valid anyway,
+ * src/MeshBlock.C:37-72), so the copies of every connectivity call run at the
+ * full PCIe rate; *on = 0 releases them and leaves arrays as they are. */
+void tioga_b200_set_pin_host_(int *on);
 /* Node global ids of block btag (nnodes uint64_t; caller-owned, kept like the
  * other registered arrays): the node_gid of tioga::registerGridData
  * (src/tioga.C:64-85), which the C API does not pass. */

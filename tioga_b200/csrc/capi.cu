@@ -310,6 +310,13 @@ void tioga_b200_registernodegid_(int* btag, uint64_t* node_gid) {
   if (ready("tioga_b200_registernodegid_")) set_rc(g_tg->set_node_gid(*btag, node_gid));
 }
 
+void tioga_b200_set_pin_host_(int* on) {
+  if (ready("tioga_b200_set_pin_host_")) {
+    g_tg->set_pin_host(*on);
+    set_rc(0);
+  }
+}
+
 void tioga_b200_set_nodegid_merge_(int* on) {
   if (ready("tioga_b200_set_nodegid_merge_")) {
     g_tg->set_nodegid_merge(*on);

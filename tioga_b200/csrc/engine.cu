@@ -34,6 +34,7 @@ Engine::Engine() {
 }
 
 Engine::~Engine() {
+  unpin_caller_arrays();
   if (stream_) cudaStreamSynchronize(stream_);
   if (pre_exec_) cudaGraphExecDestroy(pre_exec_);
   for (auto& e : ev_) cudaEventDestroy(e);
@@ -326,6 +327,7 @@ int Engine::upload_topology() {
     }
   }
   stg.release();
+  if (pin_host_) pin_caller_arrays();
   {
     unsigned e = 0;
     TB_CUDA(cudaMemcpyAsync(&e, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
@@ -393,6 +395,38 @@ int Engine::build_csr() {
   k_csr_sort<<<grid_for(ntot_, kT), kT, 0, stream_>>>(csr_off_.p, ntot_, csr_cell_.p);
   TB_LAUNCHED("k_csr_sort");
   return 0;
+}
+
+// The caller's coordinate and iblank arrays stay valid while they are
+// registered (MeshBlock.C:37-72), and every connectivity call copies them to
+// and from the device, so pageable ones are page-locked once per topology:
+// their copies then run at the full PCIe rate instead of through staging
+// buffers.  Arrays that are pinned already, or that cannot be registered,
+// are left as they are.  The registrations end with the topology (a new
+// registration, tioga_delete_).
+void Engine::pin_caller_arrays() {
+  unpin_caller_arrays();
+  auto pin = [&](void* p, size_t bytes) {
+    if (!p || bytes == 0) return;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    if (a.type != cudaMemoryTypeUnregistered) return;
+    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess) pinned_.push_back(p);
+    else cudaGetLastError();
+  };
+  for (const HostBlock& H : hb_) {
+    pin(H.hx, 3 * (size_t)H.nnodes * sizeof(double));
+    pin(H.hibl, (size_t)H.nnodes * sizeof(int));
+  }
+}
+
+void Engine::unpin_caller_arrays() {
+  for (void* p : pinned_) cudaHostUnregister(p);
+  pinned_.clear();
+  cudaGetLastError();
 }
 
 int Engine::upload_coords() {

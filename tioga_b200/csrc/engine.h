@@ -322,6 +322,10 @@ class Engine {
   int set_uniform_hex_flag(int tag, int flag);
   int set_node_gid(int tag, const uint64_t* gid);
   void set_nodegid_merge(int on) { nodegid_merge_ = on != 0; }
+  void set_pin_host(int on) {
+    pin_host_ = on != 0;
+    if (!pin_host_) unpin_caller_arrays();
+  }
   // tioga::getReceptorInfo: 4 ints per live record of the selected system;
   // writes min(count, cap) ints to out (may be null) and returns the count,
   // or < 0 on error
@@ -347,6 +351,8 @@ class Engine {
   int build_leaf_groups();
   int setup_uniform_hex();
   int run_gid_merge();
+  void pin_caller_arrays();
+  void unpin_caller_arrays();
   int run_queries();
   int run_search();
   int run_donors();
@@ -528,6 +534,8 @@ class Engine {
   DBuf<unsigned long long> uhex_red_;   // set-up scratch: extents, check flag
   bool any_uhex_ = false;
   bool nodegid_merge_ = false;         // coincident query points merged by node id (TIOGA_HAS_NODEGID)
+  std::vector<void*> pinned_;          // caller arrays this engine page-locked (cudaHostRegister)
+  bool pin_host_ = true;               // page-lock pageable caller arrays (tioga_b200_set_pin_host_)
   DBuf<unsigned long long> node_gid_d_, gm_k0_, gm_k1_, gm_max_;
   DBuf<int> gm_a_, gm_b_, gm_c_, gm_d_;
   DBuf<unsigned long long> counters_;
