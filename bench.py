@@ -47,12 +47,25 @@ WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherica
             "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
-# DRAM bytes (read + write) of one cell-pass launch on the full workload, from
-# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of
-# `bench.py --forms split --no-tune --no-forms --steps 1 --warmup 1
-# --no-cpu-baseline`: 1,495,505,408 read + 956,761,856 written over 26,961,129
-# cells; other sizes scale by cells.
-CELL_PASS_DRAM_BYTES_PER_CELL = (1495505408 + 956761856) / 26961129
+# DRAM bytes (read + write) of one split-form cell-pass launch per cell, from
+# an ncu capture on the full workload (profiles/k_cell_pass_cfg1.md); None
+# until one is made for the current kernel.
+CELL_PASS_DRAM_BYTES_PER_CELL = None
+
+
+def cell_pass_bytes(system, st):
+    """Compulsory bytes of one split-form cell-pass launch: each leaf group's
+    header (16 B) and node list (4 B a node), each node's FP64 coordinates
+    once (24 B), each cell's vertex positions and type (8 + 1 B) read; each
+    cell's coded box (8 B) written; each leaf's record read (16 B) and box
+    written (24 B).  `reference_layout` is the same work with the reference's
+    connectivity (4 B per vertex reference) and FP32 coordinates and boxes
+    (16 B per node, 24 B per cell box), the figure of the earlier kernel."""
+    nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
+    alg = (16 * st["ngroups"] + 4 * st["ngroup_nodes"] + 24 * system.nnodes + (8 + 1 + 8) * system.ncells
+           + (16 + 24) * st["nleaf"])
+    ref = 4 * nvsum + system.ncells * (1 + 24) + system.nnodes * 16 + st["nleaf"] * (16 + 24)
+    return alg, ref
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
@@ -360,7 +373,7 @@ def run_gpu(args, ws, rank, local, dist):
     # written (24 B), and per leaf its record read (16 B) and box written (24 B).
     cell_ms = ph["cell_pass"]
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
-    alg_bytes = 4 * nvsum + system.ncells * (1 + 24) + system.nnodes * 16 + st["nleaf"] * (16 + 24)
+    alg_bytes, ref_bytes = cell_pass_bytes(system, st)
     traffic = (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
                else CELL_PASS_DRAM_BYTES_PER_CELL * system.ncells)
     peaks = {}
@@ -392,6 +405,8 @@ def run_gpu(args, ws, rank, local, dist):
         "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": alg_bytes, "launch_ms": cell_ms,
+                     "reference_layout_bytes": ref_bytes,
+                     "reference_layout_frac": ref_bytes / (cell_ms * 1e-3) / 1e9 / peak,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
@@ -626,7 +641,7 @@ def run_gpu_batch(args, ws, rank, local, dist):
     h2d, d2h = 24 * nodes, 4 * nodes
     cell_ms = ph["cell_pass"]
     nvsum = sum(nv * conn.shape[0] for s in systems for b in s.blocks for nv, conn in b.cells)
-    alg_bytes = 4 * nvsum + cells * (1 + 24) + nodes * 16 + st["nleaf"] * (16 + 24)
+    alg_bytes, _ = cell_pass_bytes(cases.System([b for sy in systems for b in sy.blocks]), st)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -662,7 +677,8 @@ def run_gpu_batch(args, ws, rank, local, dist):
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
         "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": CELL_PASS_DRAM_BYTES_PER_CELL * cells, "algorithmic_bytes": alg_bytes,
+                     "traffic": (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
+                                 else CELL_PASS_DRAM_BYTES_PER_CELL * cells), "algorithmic_bytes": alg_bytes,
                      "launch_ms": cell_ms, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
