@@ -48,6 +48,7 @@ Engine::~Engine() {
   hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); qbox_.release(); tnode_.release(); tnode64_.release();
   grp_.release(); grp_nodes_.release(); cell_lidx_.release(); leaves_.release(); gparent_.release(); gnk_.release();
+  gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
   qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
@@ -600,7 +601,6 @@ int Engine::build_tree_topology() {
     TB_CUDA(cudaStreamSynchronize(stream_));  // host staging vectors go out of scope level by level
     long long g0 = nb;
     int depth = 0;
-    level_groups_.assign(1, nb);
     while (n > 0) {
       TB_CUDA(kids.ensure(4 * (size_t)n));
       TB_CUDA(nk.ensure(n + 1));
@@ -651,7 +651,6 @@ int Engine::build_tree_topology() {
                                                        tlink.p, gparent_.p, gnk_.p, na.p, nbuf.p, ns.p);
       TB_LAUNCHED("k_tree_link");
       g0 += nint;
-      level_groups_.push_back((int)g0);
       std::swap(ca, na);
       std::swap(cb, nbuf);
       std::swap(cs, ns);
@@ -663,6 +662,22 @@ int Engine::build_tree_topology() {
     TB_CUDA(tnode_.ensure(2 * tree_nodes_));
     k_tree_init<<<grid_for(tree_nodes_, kT), kT, 0, stream_>>>(tlink.p, tree_nodes_, tnode_.p);
     TB_LAUNCHED("k_tree_init");
+    // the one-launch refit's counts and starting groups
+    {
+      const int ng = (int)(tree_nodes_ / 4);
+      TB_CUDA(gnint_.ensure(std::max(ng, 1)));
+      TB_CUDA(refit_start_.ensure(std::max(ng, 1)));
+      TB_CUDA(refit_cnt_.ensure(std::max(ng, 1)));
+      DBuf<int> ns;
+      TB_CUDA(ns.ensure(1));
+      TB_CUDA(cudaMemsetAsync(ns.p, 0, sizeof(int), stream_));
+      if (ng > nb) {
+        k_group_nint<<<grid_for(ng - nb, kT), kT, 0, stream_>>>(tnode_.p, nb, ng, gnint_.p, refit_start_.p, ns.p);
+        TB_LAUNCHED("k_group_nint");
+      }
+      TB_CUDA(cudaMemcpyAsync(&nrefit_start_, ns.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+      TB_CUDA(cudaStreamSynchronize(stream_));
+    }
     tnode64_empty_ = false;
     // leaves in storage order
     DBuf<int> flag, loff;
@@ -1112,13 +1127,12 @@ int Engine::run_pairs_and_refit() {
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
-  // internal nodes, deepest level first, from the leaves the cell pass wrote
-  for (int d = (int)level_groups_.size() - 2; d >= 0; d--) {
-    const int g0 = level_groups_[d], g1 = level_groups_[d + 1];
-    if (g1 <= g0) continue;
-    k_refit_level<<<grid_for(g1 - g0, kT), kT, 0, stream_>>>(g0, g1, gparent_.p, tnode_.p,
-                                                             fp64 ? tnode64_.p : nullptr);
-    TB_LAUNCHED("k_refit_level");
+  if (nrefit_start_ > 0) {  // internal nodes from the leaves the cell pass wrote, in one launch
+    TB_CUDA(cudaMemsetAsync(refit_cnt_.p, 0, (tree_nodes_ / 4) * sizeof(int), stream_));
+    k_refit_fused<<<grid_for(nrefit_start_, kT), kT, 0, stream_>>>(refit_start_.p, nrefit_start_, gparent_.p,
+                                                                   gnint_.p, (int)hb_.size(), refit_cnt_.p, tnode_.p,
+                                                                   fp64 ? tnode64_.p : nullptr);
+    TB_LAUNCHED("k_refit_fused");
   }
   k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
   TB_LAUNCHED("k_pair_finish");

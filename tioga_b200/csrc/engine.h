@@ -496,7 +496,8 @@ class Engine {
   bool tnode64_empty_ = false;    // tnode64_ initialised to empty boxes for this topology
   DBuf<int4> leaves_;             // (first cell, cells, slot, block), storage order
   DBuf<int> gparent_, gnk_;      // per slot group: parent slot, children
-  std::vector<int> level_groups_; // groups of each depth's children: [level_groups_[d], level_groups_[d+1])
+  DBuf<int> gnint_, refit_start_, refit_cnt_;  // one-launch refit: internal children, starting groups, counts
+  int nrefit_start_ = 0;
   // queries
   DBuf<int> qnode_, qdon_, qcell_;
   DBuf<double> qres_;

@@ -164,7 +164,9 @@ __global__ void k_leaf_flags(const int* leaf_at, long long ctot, int* flag);
 __global__ void k_leaf_list(const int* leaf_at, const int* loff, long long ctot, const int2* tlink,
                             const blk_t* cell_blk, int4* leaves);
 __global__ void k_block_leaves(const int4* leaves, long long nleaf, int* first);
-__global__ void k_refit_level(int g0, int g1, const int* gparent, float4* tnode, double* tnode64);
+__global__ void k_group_nint(const float4* tnode, int g_root, int ngroups, int* nint, int* start, int* nstart);
+__global__ void k_refit_fused(const int* start, int nstart, const int* gparent, const int* nint, int g_root,
+                              int* cnt, float4* tnode, double* tnode64);
 __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
 __global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,

@@ -129,36 +129,6 @@ __global__ void k_leaf_list(const int* __restrict__ leaf_at, const int* __restri
   }
 }
 
-// Refit of one level after the cell pass wrote the leaf boxes: child groups
-// [g0, g1) are the children of one depth's internal nodes, refitted deepest
-// level first, so every child is final when its group is read.  Each parent
-// gets the union of its group's four slots (empty slots add nothing).
-__global__ void k_refit_level(int g0, int g1, const int* __restrict__ gparent, float4* __restrict__ tnode,
-                              double* __restrict__ tnode64) {
-  for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < g1; g += gridDim.x * blockDim.x) {
-    const int p = gparent[g];
-    float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    for (int k = 0; k < 4; k++) {
-      const float4 A = tnode[2 * (4ll * g + k)], B = tnode[2 * (4ll * g + k) + 1];
-      b[0] = fminf(b[0], A.x); b[1] = fminf(b[1], A.y); b[2] = fminf(b[2], A.z);
-      b[3] = fmaxf(b[3], A.w); b[4] = fmaxf(b[4], B.x); b[5] = fmaxf(b[5], B.y);
-    }
-    tnode[2 * (long long)p] = make_float4(b[0], b[1], b[2], b[3]);
-    *reinterpret_cast<float2*>(&tnode[2 * (long long)p + 1]) = make_float2(b[4], b[5]);  // keep the link
-    if (tnode64) {
-      double d[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
-      for (int k = 0; k < 4; k++) {
-        const double* c = tnode64 + 6 * (4ll * g + k);
-        for (int j = 0; j < 3; j++) {
-          d[j] = dmin(d[j], c[j]);
-          d[j + 3] = dmax(d[j + 3], c[j + 3]);
-        }
-      }
-      for (int j = 0; j < 6; j++) tnode64[6 * (long long)p + j] = d[j];
-    }
-  }
-}
-
 // Leaf groups, the cell pass's unit of work for one warp: up to kGroupLeaves
 // consecutive leaves of one block (at most 32 cells).  Every group's distinct
 // vertex nodes are listed once, in ascending global id, and every cell gets
@@ -273,6 +243,61 @@ void launch_group_nodes(bool fill, unsigned grid, cudaStream_t st, const int2* g
     k_group_nodes<true><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
   else
     k_group_nodes<false><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
+}
+
+// One-launch refit.  At build time every child group g >= g_root (the root
+// groups hold the blocks' roots and have no parent) counts its internal
+// slots (nint[g]); the groups with none start the refit.  Per call, each
+// starting group writes the union of its four slots into its parent slot,
+// then counts itself done at the parent's group; the child that completes a
+// group (its nint-th) refits that group too, and so on up to a root group.
+// No thread waits for another: the last one to arrive carries on, and the
+// fence before the count makes its children's unions visible to it (the
+// slots are read through L2).
+__global__ void k_group_nint(const float4* __restrict__ tnode, int g_root, int ngroups, int* __restrict__ nint,
+                             int* __restrict__ start, int* __restrict__ nstart) {
+  for (int g = g_root + blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    int n = 0;
+    for (int k = 0; k < 4; k++) n += __float_as_int(tnode[2 * (4ll * g + k) + 1].w) < 0;
+    nint[g] = n;
+    if (n == 0) start[atomicAdd(nstart, 1)] = g;
+  }
+}
+
+__global__ void k_refit_fused(const int* __restrict__ start, int nstart, const int* __restrict__ gparent,
+                              const int* __restrict__ nint, int g_root, int* __restrict__ cnt, float4* tnode,
+                              double* tnode64) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nstart; i += gridDim.x * blockDim.x) {
+    int g = start[i];
+    for (int guard = 0; guard < 64; guard++) {  // at most one step per tree level
+      const int p = gparent[g];
+      float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+      for (int k = 0; k < 4; k++) {
+        const float4 A = __ldcg(&tnode[2 * (4ll * g + k)]), B = __ldcg(&tnode[2 * (4ll * g + k) + 1]);
+        b[0] = fminf(b[0], A.x); b[1] = fminf(b[1], A.y); b[2] = fminf(b[2], A.z);
+        b[3] = fmaxf(b[3], A.w); b[4] = fmaxf(b[4], B.x); b[5] = fmaxf(b[5], B.y);
+      }
+      tnode[2 * (long long)p] = make_float4(b[0], b[1], b[2], b[3]);
+      *reinterpret_cast<float2*>(&tnode[2 * (long long)p + 1]) = make_float2(b[4], b[5]);  // keep the link
+      if (tnode64) {
+        double d[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+        for (int k = 0; k < 4; k++) {
+          const double* c = tnode64 + 6 * (4ll * g + k);
+          for (int j = 0; j < 3; j++) {
+            d[j] = dmin(d[j], __ldcg(c + j));
+            d[j + 3] = dmax(d[j + 3], __ldcg(c + j + 3));
+          }
+        }
+        for (int j = 0; j < 6; j++) tnode64[6 * (long long)p + j] = d[j];
+      }
+      const int G = p >> 2;  // the group holding the parent slot
+      if (G < g_root) break;   // a block's root: done
+      __threadfence();
+      if (atomicAdd(&cnt[G], 1) + 1 != nint[G]) break;  // a sibling subtree is still being refitted
+      __threadfence();
+      g = G;
+    }
+  }
 }
 
 // first leaf of every block that has leaves (leaves are in storage order,
