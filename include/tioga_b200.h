@@ -258,6 +258,9 @@ void tioga_b200_autotune_(int *reps);
  * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM,
  * [5] split-form traversal: 1 warp-cooperative, 0 one walk per query point. */
 void tioga_b200_tuning_(int out[8]);
+/* Set the shapes by hand, in tioga_b200_tuning_'s order [0..5]; values <= 0
+ * keep a shape ([5] takes 0 or 1). */
+void tioga_b200_set_tuning_(const int in[6]);
 
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);

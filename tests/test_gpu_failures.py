@@ -104,10 +104,11 @@ def test_nan_coordinate_then_recovers(oracle_lib):
     x[40] = keep
     t.preprocess_grids()
     assert t.lib.tioga_b200_last_error() == 0
+    keep41 = x[41]
     x[41] = np.inf  # a node moved to infinity before a connectivity call
     t.performconnectivity()
     assert t.lib.tioga_b200_last_error() != 0
-    x[41] = system.blocks[1].x.reshape(-1)[41]
+    x[41] = keep41
     t.performconnectivity()
     assert t.lib.tioga_b200_last_error() == 0
     gpu = {"iblank": {b.tag: t.iblank(b.tag).copy() for b in system.blocks},

@@ -354,6 +354,11 @@ void tioga_b200_tuning_(int out[8]) {
   out[5] = t.traverse_warp;
 }
 
+void tioga_b200_set_tuning_(const int in[6]) {
+  if (!ready("tioga_b200_set_tuning_")) return;
+  set_rc(g_tg->set_tuning(in));
+}
+
 void tioga_b200_set_stream_(void* stream) {
   if (ready("tioga_b200_set_stream_")) g_tg->set_stream((cudaStream_t)stream);
 }

@@ -255,6 +255,16 @@ class Engine {
   void set_highorder_callbacks() { ihigh_ = true; }
   // Lowered device bounds for tests of the error paths (0 = the normal
   // bound): which 0 = hole-map fill rounds, 1 = donor-record capacity.
+  // launch shapes set by hand (the tuning array's order; values <= 0 keep
+  // the current shape, except the traversal choice, which takes 0 too)
+  int set_tuning(const int in[6]) {
+    int* v[6] = {&tune_.cell_pass_per_sm, &tune_.chunk_pairs, &tune_.query_per_sm, &tune_.traverse_per_sm,
+                 &tune_.candidates_per_sm, &tune_.traverse_warp};
+    for (int i = 0; i < 5; i++)
+      if (in[i] > 0) *v[i] = in[i];
+    if (in[5] == 0 || in[5] == 1) tune_.traverse_warp = in[5];
+    return 0;
+  }
   int set_test_bound(int which, int value) {
     if (which == 0) test_fill_rounds_ = value;
     else if (which == 1) test_rcap_ = value;
