@@ -56,9 +56,11 @@ __device__ __forceinline__ float qdec_lo(int q, float L, float sdn) {
 __device__ __forceinline__ float qdec_hi(int q, float L, float H, float sup) {
   return q == 255 ? H : __fmaf_ru((float)q, sup, L);
 }
+// (the estimates below use the fast division: the loops after them test the
+// decoded value itself, so the codes are exact whatever the estimate)
 __device__ __forceinline__ int qenc_lo(float lo, float L, float sdn) {
   if (!(sdn > 0.f) || !(lo > L)) return 0;
-  const float t = __fdiv_rd(__fsub_rd(lo, L), sdn);
+  const float t = __fdividef(lo - L, sdn);
   int q = t >= 255.f ? 255 : (t > 0.f ? (int)t : 0);
   for (int k = 0; k < 4 && q > 0 && qdec_lo(q, L, sdn) > lo; k++) q--;
   if (q > 0 && qdec_lo(q, L, sdn) > lo) q = 0;
@@ -67,7 +69,7 @@ __device__ __forceinline__ int qenc_lo(float lo, float L, float sdn) {
 }
 __device__ __forceinline__ int qenc_hi(float hi, float L, float H, float sup) {
   if (!(sup > 0.f) || !(hi < H)) return 255;
-  const float t = __fdiv_ru(__fsub_ru(hi, L), sup);
+  const float t = __fdividef(hi - L, sup);
   int q = t >= 255.f ? 255 : (t > 0.f ? (int)ceilf(t) : 0);
   for (int k = 0; k < 4 && q < 255 && qdec_hi(q, L, H, sup) < hi; k++) q++;
   if (q < 255 && qdec_hi(q, L, H, sup) < hi) q = 255;
