@@ -53,19 +53,20 @@ PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 CELL_PASS_DRAM_BYTES_PER_CELL = None
 
 
-def cell_pass_bytes(system, st):
-    """Compulsory bytes of one split-form cell-pass launch: each leaf group's
-    header (16 B) and node list (4 B a node), each node's FP64 coordinates
-    once (24 B), each cell's vertex positions and type (8 + 1 B) read; each
-    cell's coded box (8 B) written; each leaf's record read (16 B) and box
-    written (24 B).  `reference_layout` is the same work with the reference's
-    connectivity (4 B per vertex reference) and FP32 coordinates and boxes
-    (16 B per node, 24 B per cell box), the figure of the earlier kernel."""
+def cell_pass_bytes(system, st, variant: int):
+    """Compulsory bytes of one split-form cell-pass launch, each array read or
+    written once.  Both variants read each cell's type (1 B) and write its
+    FP32 box (24 B), read each leaf's record (16 B) and write its box (24 B).
+    Variant 0 reads the padded connectivity as the reference's vertex
+    references (4 B each) and each node's FP32 copy once (16 B; the copy is
+    made by k_round_nodes, outside this launch).  Variant 1 reads each leaf
+    group's header (16 B) and node list (4 B a node), each node's FP64
+    coordinates once (24 B) and each cell's vertex positions (8 B)."""
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
-    alg = (16 * st["ngroups"] + 4 * st["ngroup_nodes"] + 24 * system.nnodes + (8 + 1 + 8) * system.ncells
-           + (16 + 24) * st["nleaf"])
-    ref = 4 * nvsum + system.ncells * (1 + 24) + system.nnodes * 16 + st["nleaf"] * (16 + 24)
-    return alg, ref
+    common = system.ncells * (1 + 24) + st["nleaf"] * (16 + 24)
+    if variant == 1:
+        return 16 * st["ngroups"] + 4 * st["ngroup_nodes"] + 24 * system.nnodes + 8 * system.ncells + common
+    return 4 * nvsum + 16 * system.nnodes + common
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
@@ -238,7 +239,7 @@ def autotune(lib, tb, reps: int = 2) -> dict:
     out = (C.c_int * 8)()
     lib.lib.tioga_b200_tuning_(out)
     keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
-            "candidate_ctas_per_sm", "traverse_warp_cooperative"]
+            "candidate_ctas_per_sm", "cell_pass_variant"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 
@@ -373,7 +374,8 @@ def run_gpu(args, ws, rank, local, dist):
     # written (24 B), and per leaf its record read (16 B) and box written (24 B).
     cell_ms = ph["cell_pass"]
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
-    alg_bytes, ref_bytes = cell_pass_bytes(system, st)
+    variant = (tuning or {}).get("cell_pass_variant", 0)
+    alg_bytes = cell_pass_bytes(system, st, variant)
     traffic = (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
                else CELL_PASS_DRAM_BYTES_PER_CELL * system.ncells)
     peaks = {}
@@ -405,8 +407,7 @@ def run_gpu(args, ws, rank, local, dist):
         "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": alg_bytes, "launch_ms": cell_ms,
-                     "reference_layout_bytes": ref_bytes,
-                     "reference_layout_frac": ref_bytes / (cell_ms * 1e-3) / 1e9 / peak,
+                     "variant": variant,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
@@ -641,7 +642,8 @@ def run_gpu_batch(args, ws, rank, local, dist):
     h2d, d2h = 24 * nodes, 4 * nodes
     cell_ms = ph["cell_pass"]
     nvsum = sum(nv * conn.shape[0] for s in systems for b in s.blocks for nv, conn in b.cells)
-    alg_bytes, _ = cell_pass_bytes(cases.System([b for sy in systems for b in sy.blocks]), st)
+    alg_bytes = cell_pass_bytes(cases.System([b for sy in systems for b in sy.blocks]), st,
+                                (tuning or {}).get("cell_pass_variant", 0))
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))

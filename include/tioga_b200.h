@@ -256,7 +256,8 @@ void tioga_b200_server_stats(void *srv, long long out[16]);
 void tioga_b200_autotune_(int *reps);
 /* The shapes in use: [0] cell-pass CTAs per SM, [1] pairs per cell-pass CTA,
  * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM,
- * [5] split-form traversal: 1 warp-cooperative, 0 one walk per query point. */
+ * [5] split-form cell pass: 0 gathers from an FP32 coordinate copy, 1 leaf
+ * groups with their distinct nodes staged in shared memory. */
 void tioga_b200_tuning_(int out[8]);
 /* Set the shapes by hand, in tioga_b200_tuning_'s order [0..5]; values <= 0
  * keep a shape ([5] takes 0 or 1). */
@@ -343,7 +344,7 @@ void tioga_b200_set_nodegid_merge_(int *on);
  * point search keeps the tree for such blocks. */
 void tioga_b200_set_uniform_hex_flag_(int *btag, int *flag);
 /* For tests of the error paths: lower one device bound to *value (0 restores
- * it).  *which 0 = rounds of a hole-map fill (at the bound the fill stops and
+ * it).  *which 0 = line passes of a hole-map fill (at the bound the fill stops and
  * error bit 8 is reported), 1 = donor-record capacity (error bit 2).  The
  * connectivity call then returns its error bits through
  * tioga_b200_last_error(); no counterpart in TIOGA. */

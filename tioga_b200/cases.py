@@ -228,14 +228,15 @@ def _empty_i32():
 
 
 def config0(seed: int = 0, nbg: int = 65, nr: int = 33, nt: int = 33, nphi: int = 65,
-            perturb: float = 0.05, seam_copy: bool = False, bg_perturb: float | None = None) -> System:
+            perturb: float = 0.05, seam_copy: bool = False, bg_perturb: float | None = None,
+            bg_shift: float = 0.0) -> System:
     """Plain all-hex case: 65^3 background box on [-5,5]^3 plus one shell
     (r 0.5 -> 2.0, radial ratio 1.1) at the origin; interior nodes jittered
     by +-5% of the local spacing (the background by bg_perturb when given:
-    0 leaves it a uniform Cartesian box)."""
+    0 leaves it a uniform Cartesian box, shifted by bg_shift on every axis)."""
     rng = np.random.default_rng(seed)
     pb = perturb if bg_perturb is None else bg_perturb
-    xb, cb = hex_box(nbg, -5.0, 5.0, pb, rng if pb > 0 else None)
+    xb, cb = hex_box(nbg, -5.0 + bg_shift, 5.0 + bg_shift, pb, rng if pb > 0 else None)
     xs, cs, wall, outer, _ = sphere_shell(nr, nt, nphi, 0.5, 2.0, 1.1, (0.0, 0.0, 0.0), perturb, rng,
                                           seam_copy=seam_copy)
     bg = Block(1, xb, cb, _empty_i32(), _empty_i32(), name="background")
@@ -479,10 +480,14 @@ def small_config0(seed: int = 0) -> System:
     return config0(seed, nbg=17, nr=9, nt=9, nphi=17)
 
 
-def small_config0_uniform(seed: int = 0, nbg: int = 17) -> System:
+def small_config0_uniform(seed: int = 0, nbg: int = 17, shift: float = 0.0) -> System:
     """small_config0 with an unjittered background: a uniform Cartesian hex
-    box, the case of the reference's uniform-hex search (search.C:271-341)."""
-    return config0(seed, nbg=nbg, nr=9, nt=9, nphi=17, bg_perturb=0.0)
+    box, the case of the reference's uniform-hex search (search.C:271-341).
+    Unshifted, the box's lattice planes hold the shell's unjittered seam and
+    pole nodes (they lie on box faces, where the lookup and the tree search
+    pick different cells) and its lattice nodes lie on the shell's seam faces
+    (tied shell cells); a shift off the origin removes both."""
+    return config0(seed, nbg=nbg, nr=9, nt=9, nphi=17, bg_perturb=0.0, bg_shift=shift)
 
 
 def small_config0_seam(seed: int = 0) -> System:

@@ -351,7 +351,7 @@ void tioga_b200_tuning_(int out[8]) {
   out[2] = t.query_per_sm;
   out[3] = t.traverse_per_sm;
   out[4] = t.candidates_per_sm;
-  out[5] = t.traverse_warp;
+  out[5] = t.cell_pass_variant;
 }
 
 void tioga_b200_set_tuning_(const int in[6]) {

@@ -46,7 +46,7 @@ Engine::~Engine() {
   wall_list_.release(); obc_list_.release(); csr_off_.release(); csr_cell_.release(); deg_.release();
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   hm_state_.release();
-  wall_bb_.release(); sorted_cell_.release(); qbox_.release(); tnode_.release(); tnode64_.release();
+  wall_bb_.release(); sorted_cell_.release(); cbox_.release(); xf_.release(); tnode_.release(); tnode64_.release();
   grp_.release(); grp_nodes_.release(); cell_lidx_.release(); leaves_.release(); gparent_.release(); gnk_.release();
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
@@ -761,7 +761,7 @@ int Engine::build_tree_topology() {
   TB_CUDA(cudaMemcpyAsync(tile_base_.p, h_tile_base_.data(), h_tile_base_.size() * sizeof(long long),
                           cudaMemcpyHostToDevice, stream_));
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
-  TB_CUDA(qbox_.ensure(ctot_));
+  TB_CUDA(cbox_.ensure(2 * ctot_));
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   topo_gen_++;  // the cell arrays were replaced by their storage-order copies
   return 0;
@@ -1059,6 +1059,11 @@ int Engine::run_pairs_and_refit() {
     TB_LAUNCHED("k_node_tiles");
   }
   if (npairs_ == 0) return 0;
+  if (precision_ != 0 && tune_.cell_pass_variant == 0) {  // FP32 coordinates for the gather variant
+    TB_CUDA(xf_.ensure(ntot_));
+    k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
+    TB_LAUNCHED("k_round_nodes");
+  }
   // refit to the current coordinates: one pass over the cells (tree-order
   // cell boxes + reduced boxes of every pair), then the tree levels, then the
   // node tiles of the query gathering
@@ -1090,9 +1095,10 @@ int Engine::run_pairs_and_refit() {
   // leaf groups (one warp each) in the split form, leaves (a quarter warp
   // each) in the FP64 form
   const int kChunkPairs = std::max(16, std::min(128, tune_.chunk_pairs));
-  const std::vector<int>& item_of_blk = fp64 ? h_blk_leaf_ : h_blk_grp_;
-  const long long nitems = fp64 ? nleaf_total_ : ngrp_;
-  const long long per_cta = fp64 ? 256 / kMaxLeafCells : 256 / 32;  // items a CTA of 256 threads takes at once
+  const bool groups = !fp64 && tune_.cell_pass_variant == 1;
+  const std::vector<int>& item_of_blk = groups ? h_blk_grp_ : h_blk_leaf_;
+  const long long nitems = groups ? ngrp_ : nleaf_total_;
+  const long long per_cta = groups ? 256 / 32 : 256 / kMaxLeafCells;  // items a CTA of 256 threads takes at once
   std::vector<int4> chunks;
   for (int b = 0; b < nb;) {
     int e = b + 1;
@@ -1121,9 +1127,10 @@ int Engine::run_pairs_and_refit() {
                        leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p,
                        cbox64_.p, tnode_.p, tnode64_.p, pair_acc_.p);
   else
-    launch_cell_pass32(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
-                       leaves_.p, grp_.p, grp_nodes_.p, cell_lidx_.p, d_chunks_.p, d_chunk_cta_.p,
-                       (int)chunks.size(), d_pfirst_.p, d_pairs_.p, qbox_.p, tnode_.p, pair_acc_.p);
+    launch_cell_pass32(tune_.cell_pass_variant, tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, xf_.p,
+                       conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p, grp_.p, grp_nodes_.p, cell_lidx_.p, d_chunks_.p,
+                       d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p, tnode_.p,
+                       pair_acc_.p);
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
@@ -1249,8 +1256,7 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    const int tform = (form == 1 && tune_.traverse_warp) ? 2 : form;
-    launch_traverse(tform, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, qbox_.p,
+    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, cbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p, skip_uhex);
     TB_LAUNCHED("k_traverse");
@@ -1933,7 +1939,7 @@ int Engine::autotune(int reps) {
       {&tune_.cell_pass_per_sm, {2, 3, 4}, &Timing::cell_pass},
       {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
       {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
-      {&tune_.traverse_warp, {1, 0}, &Timing::traverse},
+      {&tune_.cell_pass_variant, {0, 1}, &Timing::cell_pass},
       {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},
       {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
   };

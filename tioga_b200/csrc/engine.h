@@ -238,7 +238,7 @@ struct Stats {
 // candidate screen, and the pairs one cell-pass CTA holds in shared memory.
 struct Tuning {
   int cell_pass_per_sm = 3, query_per_sm = 16, traverse_per_sm = 64, candidates_per_sm = 16, chunk_pairs = 128;
-  int traverse_warp = 1;  // split form: the warp-cooperative walk (1) or one walk per query (0)
+  int cell_pass_variant = 0;  // split form: gathers from an FP32 copy (0) or leaf groups staged in shared memory (1)
 };
 
 struct Timing {
@@ -256,13 +256,13 @@ class Engine {
   // Lowered device bounds for tests of the error paths (0 = the normal
   // bound): which 0 = hole-map fill rounds, 1 = donor-record capacity.
   // launch shapes set by hand (the tuning array's order; values <= 0 keep
-  // the current shape, except the traversal choice, which takes 0 too)
+  // the current shape, except the cell-pass variant, which takes 0 too)
   int set_tuning(const int in[6]) {
-    int* v[6] = {&tune_.cell_pass_per_sm, &tune_.chunk_pairs, &tune_.query_per_sm, &tune_.traverse_per_sm,
-                 &tune_.candidates_per_sm, &tune_.traverse_warp};
+    int* v[5] = {&tune_.cell_pass_per_sm, &tune_.chunk_pairs, &tune_.query_per_sm, &tune_.traverse_per_sm,
+                 &tune_.candidates_per_sm};
     for (int i = 0; i < 5; i++)
       if (in[i] > 0) *v[i] = in[i];
-    if (in[5] == 0 || in[5] == 1) tune_.traverse_warp = in[5];
+    if (in[5] == 0 || in[5] == 1) tune_.cell_pass_variant = in[5];
     return 0;
   }
   int set_test_bound(int which, int value) {
@@ -491,7 +491,8 @@ class Engine {
   DBuf<unsigned long long> wall_bb_;
   // tree
   DBuf<int> sorted_cell_;
-  DBuf<uint2> qbox_;       // split form: 1 per sorted cell, its box coded inside its leaf's box
+  DBuf<float4> cbox_;      // split form: 2 per sorted cell (FP32 box rounded outward)
+  DBuf<float4> xf_;        // coordinates rounded to FP32, one per node (the gather variant of the cell pass)
   DBuf<float4> tnode_;     // 2 per tree node
   DBuf<int4> grp_;         // leaf groups: (first leaf, leaves, first node, nodes)
   DBuf<int> grp_nodes_;    // each group's distinct vertex nodes, ascending

@@ -35,48 +35,6 @@ __host__ __device__ inline double dkey_inv(unsigned long long k) {
   return d;
 }
 
-// ---- cell boxes as 8-bit offsets inside their leaf's box (split form) ----
-// A cell's FP32 box [lo, hi] (already rounded outward) is stored per axis as
-// two bytes (qlo, qhi) relative to the leaf box [L, H] of the tree, which is
-// the union of the leaf's cell boxes.  Decoding rounds outward:
-//   lo' = L                          (qlo == 0)   or fma_rd(qlo, sdn, L)
-//   hi' = H                          (qhi == 255) or fma_ru(qhi, sup, L)
-// with sdn <= (H - L) / 255 <= sup.  The encoder picks the tightest codes whose
-// decoded values still hold the box (it evaluates the same decode functions),
-// so lo' <= lo and hi' >= hi always: the traversal never loses a cell that the
-// FP32 box would have kept, and the exact FP64 element-box test that follows
-// decides candidacy.  8 bytes per cell: (qlo.xyz, qhi.xyz, 2 spare bytes).
-constexpr float kInv255Dn = 0.0039215682f;  // <= 1/255
-constexpr float kInv255Up = 0.0039215693f;  // >= 1/255
-__device__ __forceinline__ float qstep_dn(float L, float H) { return __fmul_rd(__fsub_rd(H, L), kInv255Dn); }
-__device__ __forceinline__ float qstep_up(float L, float H) { return __fmul_ru(__fsub_ru(H, L), kInv255Up); }
-__device__ __forceinline__ float qdec_lo(int q, float L, float sdn) {
-  return q == 0 ? L : __fmaf_rd((float)q, sdn, L);
-}
-__device__ __forceinline__ float qdec_hi(int q, float L, float H, float sup) {
-  return q == 255 ? H : __fmaf_ru((float)q, sup, L);
-}
-// (the estimates below use the fast division: the loops after them test the
-// decoded value itself, so the codes are exact whatever the estimate)
-__device__ __forceinline__ int qenc_lo(float lo, float L, float sdn) {
-  if (!(sdn > 0.f) || !(lo > L)) return 0;
-  const float t = __fdividef(lo - L, sdn);
-  int q = t >= 255.f ? 255 : (t > 0.f ? (int)t : 0);
-  for (int k = 0; k < 4 && q > 0 && qdec_lo(q, L, sdn) > lo; k++) q--;
-  if (q > 0 && qdec_lo(q, L, sdn) > lo) q = 0;
-  for (int k = 0; k < 2 && q < 255 && qdec_lo(q + 1, L, sdn) <= lo; k++) q++;
-  return q;
-}
-__device__ __forceinline__ int qenc_hi(float hi, float L, float H, float sup) {
-  if (!(sup > 0.f) || !(hi < H)) return 255;
-  const float t = __fdividef(hi - L, sup);
-  int q = t >= 255.f ? 255 : (t > 0.f ? (int)ceilf(t) : 0);
-  for (int k = 0; k < 4 && q < 255 && qdec_hi(q, L, H, sup) < hi; k++) q++;
-  if (q < 255 && qdec_hi(q, L, H, sup) < hi) q = 255;
-  for (int k = 0; k < 2 && q > 0 && qdec_hi(q - 1, L, H, sup) >= hi; k++) q--;
-  return q;
-}
-
 // the last block whose first node tile is <= T (tile_base[b] = first tile of block b)
 __device__ __forceinline__ int block_of_tile(const long long* __restrict__ tile_base, int nb, long long T) {
   int lo = 0, hi = nb - 1;
@@ -143,11 +101,12 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
                         int* pfirst);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-void launch_cell_pass32(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
-                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* grp,
-                        const int* grp_nodes, const uint2* cell_lidx, const int4* chunks, const int* chunk_cta,
-                        int nchunks, const int* pfirst, const PairInfo* pairs, uint2* qbox, float4* tnode,
-                        unsigned long long* acc);
+void launch_cell_pass32(int variant, int minb, int grid, size_t smem, cudaStream_t st, const double* x,
+                        const float4* xf, const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
+                        const int4* leaves, const int4* grp, const int* grp_nodes, const uint2* cell_lidx,
+                        const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
+                        const PairInfo* pairs, float4* cbox, float4* tnode, unsigned long long* acc);
+__global__ void k_round_nodes(const double* x, long long n, float4* xf);
 void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                         const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                         const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
@@ -189,7 +148,7 @@ __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairIn
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex);
 __global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,

@@ -315,10 +315,18 @@ __global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __r
     // a filled cell fills.  A pass that changes nothing ends the fill (the
     // state is then a fixed point of both, a fill being idempotent); the
     // row masks hold the state when it ends.
+    // A fill needs fewer rounds than the plane has cells; round_cap > 0
+    // lowers the bound to round_cap line passes that change something
+    // (tioga_b200_set_test_bound_).
     for (int rounds = 0;; rounds++) {
       bool ch = false;
       for (int r = threadIdx.x; r < n1; r += blockDim.x) ch = line_fill(fr[r], pr[r]) || ch;
-      if (!__syncthreads_or(ch) && rounds > 0) break;
+      const bool rch = __syncthreads_or(ch);
+      if (!rch && rounds > 0) break;
+      if (round_cap > 0 && rch && 2 * rounds + 1 >= round_cap) {
+        if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
+        break;
+      }
       bit_transpose(fr, n1, fc, n0);
       __syncthreads();
       ch = false;
@@ -326,9 +334,7 @@ __global__ void __launch_bounds__(256, 4) k_holemap_fill_bits(unsigned char* __r
       if (!__syncthreads_or(ch)) break;  // fr already holds this state
       bit_transpose(fc, n0, fr, n1);
       __syncthreads();
-      // a fill needs fewer rounds than the plane has cells; round_cap > 0
-      // lowers the bound to round_cap rounds (tioga_b200_set_test_bound_)
-      if (round_cap > 0 ? rounds + 1 >= round_cap : rounds > n0 * n1 + 2) {
+      if (round_cap > 0 ? 2 * rounds + 2 >= round_cap : rounds > n0 * n1 + 2) {
         if (threadIdx.x == 0) atomicOr(err, kErrFloodFillBound);
         break;
       }
@@ -861,9 +867,8 @@ __device__ __forceinline__ void cell_pass_flush(const unsigned long long* s_acc,
 //    positions (k_group_nodes), so a warp issues about 3 coalesced coordinate
 //    loads instead of 8 scattered gathers;
 //  * each cell's box is rounded outward from the FP32 vertices (f_down/f_up
-//    cover every double that rounds onto them), the leaf box (the union of
-//    its cells' boxes) goes to the leaf's tree slot, and each cell box is
-//    stored as 8-bit offsets inside the leaf box (qbox: 8 bytes a cell);
+//    cover every double that rounds onto them) into cbox, and the leaf box
+//    (the union of its cells' boxes) goes to the leaf's tree slot;
 //  * the reduced boxes of the pairs, exact (cell_pass_pairs).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_pass32(
@@ -871,7 +876,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass32(
     const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ grp,
     const int* __restrict__ grp_nodes, const uint2* __restrict__ cell_lidx, const int4* __restrict__ chunks,
     const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, uint2* __restrict__ qbox, float4* __restrict__ tnode,
+    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, float4* __restrict__ tnode,
     unsigned long long* __restrict__ acc) {
   extern __shared__ unsigned long long s_dyn[];
   __shared__ float4 s_node[8][256];
@@ -938,13 +943,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass32(
         f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
       }
     if (valid) {
-      unsigned q[6];
-      for (int k = 0; k < 3; k++) {
-        const float sdn = qstep_dn(f[k], f[k + 3]), sup = qstep_up(f[k], f[k + 3]);
-        q[k] = (unsigned)qenc_lo(fb[k], f[k], sdn);
-        q[k + 3] = (unsigned)qenc_hi(fb[k + 3], f[k], f[k + 3], sup);
-      }
-      qbox[c] = make_uint2(q[0] | (q[1] << 8) | (q[2] << 16) | (q[3] << 24), q[4] | (q[5] << 8));
+      cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
+      cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
     }
     if (leaf_ok && ci == 0) {
       const long long sl = L.z;
@@ -956,6 +956,93 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass32(
                     leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
   }
   cell_pass_flush(s_acc, p0, CH.w, acc);
+}
+
+// Cell pass of the split form, gather variant: leaf by leaf (32 /
+// kMaxLeafCells leaves per warp, one lane per cell; chunk work items are
+// leaves), each lane gathering its cell's eight FP32 vertices (xf, rounded to
+// nearest by k_round_nodes; slots past the vertex count read vertex 0 again,
+// so the eight loads are unconditional and in flight together).  The boxes,
+// leaf boxes and reduced boxes are those of k_cell_pass32; the autotuner picks
+// the faster variant for the workload.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_pass32g(
+    const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
+    const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves,
+    const int4* __restrict__ chunks, const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, float4* __restrict__ tnode,
+    unsigned long long* __restrict__ acc) {
+  extern __shared__ unsigned long long s_dyn[];
+  int cta, ncta;
+  const int kc = chunk_of_cta(chunk_cta, nchunks);
+  const int4 CH = chunks[kc];  // first leaf, end leaf, first pair, pairs
+  unsigned long long* s_acc = s_dyn;
+  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * CH.w);
+  int* s_ext = reinterpret_cast<int*>(s_pc + CH.w);
+  cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta);
+  const long long leaf_lo = CH.x, leaf_hi = CH.y;
+  const int p0 = CH.z;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
+  const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
+  constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
+  for (long long base = leaf_lo + LPW * warp0; base < leaf_hi; base += LPW * nwarps) {
+    const long long leaf = base + lane / LC;
+    const bool leaf_ok = leaf < leaf_hi;
+    const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
+    const bool valid = leaf_ok && lane % LC < L.y;
+    const long long c = (long long)L.x + lane % LC;
+    int nv = 0;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (valid) {
+      nv = cell_nv[c];
+      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+      for (int m = 0; m < 8; m++) {
+        const float4 v = xf[m < nv ? cv[m] : cv[0]];
+        lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+        hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
+      }
+    }
+    float fb[6];
+    double cc[3];
+    float hh[3];
+    for (int k = 0; k < 3; k++) {
+      fb[k] = valid ? f_down(lo[k]) : INFINITY;
+      fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
+      cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
+      hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
+    }
+    float f[6];
+    for (int k = 0; k < 6; k++) f[k] = fb[k];
+    for (int o = 1; o < LC; o <<= 1)
+      for (int k = 0; k < 3; k++) {
+        f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
+        f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
+      }
+    if (valid) {
+      cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
+      cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
+    }
+    if (leaf_ok && lane % LC == 0) {
+      const long long sl = L.z;
+      tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
+      *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
+    }
+    const int b = L.w;
+    cell_pass_pairs(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, leaf_ok, valid, c, nv,
+                    leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
+  }
+  cell_pass_flush(s_acc, p0, CH.w, acc);
+}
+
+// FP32 copy of the coordinates (rounded to nearest), for the gather variant
+__global__ void k_round_nodes(const double* __restrict__ x, long long n, float4* __restrict__ xf) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]), __double2float_rn(x[3 * i + 2]),
+                        0.f);
 }
 
 // Cell pass of the FP64 form, leaf by leaf (32 / kMaxLeafCells leaves per
@@ -1060,16 +1147,22 @@ static void set_smem(K kern, size_t smem) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void launch_cell_pass32(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
-                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* grp,
-                        const int* grp_nodes, const uint2* cell_lidx, const int4* chunks, const int* chunk_cta,
-                        int nchunks, const int* pfirst, const PairInfo* pairs, uint2* qbox, float4* tnode,
-                        unsigned long long* acc) {
+void launch_cell_pass32(int variant, int minb, int grid, size_t smem, cudaStream_t st, const double* x,
+                        const float4* xf, const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
+                        const int4* leaves, const int4* grp, const int* grp_nodes, const uint2* cell_lidx,
+                        const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
+                        const PairInfo* pairs, float4* cbox, float4* tnode, unsigned long long* acc) {
 #define TB_CP32(MB)                                                                                              \
   do {                                                                                                           \
-    set_smem(k_cell_pass32<MB>, smem);                                                                           \
-    k_cell_pass32<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, grp, grp_nodes, cell_lidx, chunks, \
-                                               chunk_cta, nchunks, pfirst, pairs, qbox, tnode, acc);             \
+    if (variant == 1) {                                                                                          \
+      set_smem(k_cell_pass32<MB>, smem);                                                                         \
+      k_cell_pass32<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, grp, grp_nodes, cell_lidx,       \
+                                                 chunks, chunk_cta, nchunks, pfirst, pairs, cbox, tnode, acc);   \
+    } else {                                                                                                     \
+      set_smem(k_cell_pass32g<MB>, smem);                                                                        \
+      k_cell_pass32g<MB><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, \
+                                                  pfirst, pairs, cbox, tnode, acc);                              \
+    }                                                                                                            \
   } while (0)
   if (minb <= 2) TB_CP32(2);
   else if (minb == 3) TB_CP32(3);
@@ -1424,7 +1517,7 @@ __device__ __forceinline__ int pick4(int k, int a0, int a1, int a2, int a3) {
 // deepest non-empty mask.
 template <int FORM>
 __global__ void __launch_bounds__(256) k_traverse(
-    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const uint2* __restrict__ qbox,
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
     int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf,
@@ -1452,12 +1545,12 @@ __global__ void __launch_bounds__(256) k_traverse(
       plo[k] = p32 - e;
       phi[k] = p32 + e;
     }
-    // cells [c0, c0 + nc) of a hit leaf in tree slot sl (1 <= nc <=
-    // kMaxLeafCells).  Split form: 8-byte cell boxes coded inside the leaf's
-    // box; the loop is unrolled and every slot reads a cell of the leaf (the
-    // last one again past nc), so all the loads are issued before the first
-    // test, one memory round trip per leaf.  Hits are added in cell order.
-    auto leaf_cells = [&](int c0, int ncell, long long sl) {
+    // cells [c0, c0 + nc) of a hit leaf (1 <= nc <= kMaxLeafCells).  FP32
+    // boxes: the loop is unrolled and every slot reads a cell of the leaf
+    // (the last one again past nc), so all the box loads are issued before
+    // the first test, one memory round trip per leaf.  Hits are added in
+    // cell order.
+    auto leaf_cells = [&](int c0, int ncell) {
       unsigned hit = 0;
       if (FORM == 0) {  // (FP64 boxes: 48 B a cell, tested one at a time)
         for (int j = 0; j < ncell; j++) {
@@ -1466,27 +1559,15 @@ __global__ void __launch_bounds__(256) k_traverse(
           hit |= (unsigned)in_box64(p, lo, hi) << j;
         }
       } else {
-        uint2 Q[kMaxLeafCells];
-#pragma unroll
-        for (int j = 0; j < kMaxLeafCells; j++) Q[j] = qbox[c0 + min(j, ncell - 1)];
-        const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
-        const float L[3] = {A.x, A.y, A.z}, H[3] = {A.w, B.x, B.y};
-        float sdn[3], sup[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          sdn[k] = qstep_dn(L[k], H[k]);
-          sup[k] = qstep_up(L[k], H[k]);
-        }
+        float4 A[kMaxLeafCells], B[kMaxLeafCells];
 #pragma unroll
         for (int j = 0; j < kMaxLeafCells; j++) {
-          const unsigned a = Q[j].x, b = Q[j].y;
-          const bool h = qdec_lo(a & 255u, L[0], sdn[0]) <= phi[0] && qdec_lo((a >> 8) & 255u, L[1], sdn[1]) <= phi[1] &&
-                         qdec_lo((a >> 16) & 255u, L[2], sdn[2]) <= phi[2] &&
-                         qdec_hi(a >> 24, L[0], H[0], sup[0]) >= plo[0] &&
-                         qdec_hi(b & 255u, L[1], H[1], sup[1]) >= plo[1] &&
-                         qdec_hi((b >> 8) & 255u, L[2], H[2], sup[2]) >= plo[2];
-          hit |= (unsigned)(h && j < ncell) << j;
+          const long long c = c0 + min(j, ncell - 1);
+          A[j] = cbox[2 * c];
+          B[j] = cbox[2 * c + 1];
         }
+#pragma unroll
+        for (int j = 0; j < kMaxLeafCells; j++) hit |= (unsigned)(hit_ab(A[j], B[j], plo, phi) && j < ncell) << j;
       }
       while (hit) {
         const int j = __ffs(hit) - 1;
@@ -1498,7 +1579,7 @@ __global__ void __launch_bounds__(256) k_traverse(
       const float4 RA = tnode[2 * root], RB = tnode[2 * root + 1];
       const bool rh = (FORM == 0) ? hit64(tnode64, root, p) : hit_ab(RA, RB, plo, phi);
       const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
-      if (rh && rcnt > 0) leaf_cells(rlink, rcnt, root);
+      if (rh && rcnt > 0) leaf_cells(rlink, rcnt);
       if (rh && rcnt < 0) {
         int base = rlink, depth = 0;
         unsigned long long tr0 = 0, tr1 = 0;  // masks of depths 0-15 and 16-31
@@ -1520,7 +1601,7 @@ __global__ void __launch_bounds__(256) k_traverse(
           while (ml) {
             const int k = __ffs(ml) - 1;
             ml &= ml - 1;
-            leaf_cells(pick4(k, lk[0], lk[1], lk[2], lk[3]), pick4(k, lc[0], lc[1], lc[2], lc[3]), base + k);
+            leaf_cells(pick4(k, lk[0], lk[1], lk[2], lk[3]), pick4(k, lc[0], lc[1], lc[2], lc[3]));
           }
           if (mi) {
             const int c = __ffs(mi) - 1;
@@ -1557,134 +1638,6 @@ __global__ void __launch_bounds__(256) k_traverse(
       }
     }
     ncand_q[q] = n;
-  }
-}
-
-// Warp-cooperative walk of the split form.  A warp takes 32 consecutive
-// query points (Morton-coherent tiles of one pair, so mostly one donor block
-// and one neighbourhood) and walks the union of their paths once: each child
-// group (one 128-byte line) is loaded once for the warp, every lane tests its
-// own point against the four boxes, and a child is entered when any lane of
-// the packet hits it; a hit leaf's cell codes are loaded once for the warp
-// and each lane that hit the leaf tests its point.  Every node on a lane's
-// own path is in the union, so each lane gets exactly the candidates a walk
-// of its own finds (in another order, which the screen does not depend on:
-// it keeps the lowest accepting cell id).  Lanes of other donor blocks form
-// packets of their own.  The stack of child groups to visit is in shared
-// memory; a walk deeper than it reports kErrTraversalOverflow.
-constexpr int kWarpStack = 128;  // 3 pending siblings per level of 32 levels, and the root
-__global__ void __launch_bounds__(256) k_traverse_warp(
-    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const uint2* __restrict__ qbox,
-    const float4* __restrict__ tnode, const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq,
-    int* __restrict__ slots, int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap,
-    unsigned* __restrict__ novf, unsigned* __restrict__ err, int skip_uhex) {
-  __shared__ int s_stack[8][kWarpStack];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int* stk = s_stack[w];
-  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5) * 32;
-  for (long long q0 = ((long long)blockIdx.x * (blockDim.x >> 5) + w) * 32; q0 < nq; q0 += wstride) {
-    const long long q = q0 + lane;
-    const bool inq = q < nq;
-    int root = -1, n = 0;
-    float plo[3] = {0.f, 0.f, 0.f}, phi[3] = {0.f, 0.f, 0.f};
-    if (inq) {
-      const BlockInfo& B = bi[qdon[q]];
-      root = (skip_uhex && B.uhex) ? -1 : B.root;  // uniform boxes: k_uhex_search
-      const double* pp = x + 3 * (long long)qnode[q];
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        const float p32 = (float)pp[k];
-        const float e = fabsf(p32) * 9.6e-7f + 2e-9f;  // covers TOL and the FP32 roundings
-        plo[k] = p32 - e;
-        phi[k] = p32 + e;
-      }
-    }
-    // the cells of leaf slot sl (link c0, ncell cells) hit by the lanes of `hit`
-    auto leaf_cells = [&](int c0, int ncell, long long sl, bool hit) {
-      uint2 Q[kMaxLeafCells];
-#pragma unroll
-      for (int j = 0; j < kMaxLeafCells; j++) Q[j] = qbox[c0 + min(j, ncell - 1)];
-      if (!hit) return;
-      const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
-      const float L[3] = {A.x, A.y, A.z}, H[3] = {A.w, B.x, B.y};
-      float sdn[3], sup[3];
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        sdn[k] = qstep_dn(L[k], H[k]);
-        sup[k] = qstep_up(L[k], H[k]);
-      }
-      unsigned hm = 0;
-#pragma unroll
-      for (int j = 0; j < kMaxLeafCells; j++) {
-        const unsigned a = Q[j].x, b = Q[j].y;
-        const bool h = qdec_lo(a & 255u, L[0], sdn[0]) <= phi[0] && qdec_lo((a >> 8) & 255u, L[1], sdn[1]) <= phi[1] &&
-                       qdec_lo((a >> 16) & 255u, L[2], sdn[2]) <= phi[2] &&
-                       qdec_hi(a >> 24, L[0], H[0], sup[0]) >= plo[0] &&
-                       qdec_hi(b & 255u, L[1], H[1], sup[1]) >= plo[1] &&
-                       qdec_hi((b >> 8) & 255u, L[2], H[2], sup[2]) >= plo[2];
-        hm |= (unsigned)(h && j < ncell) << j;
-      }
-      while (hm) {
-        const int j = __ffs(hm) - 1;
-        hm &= hm - 1;
-        add_candidate((int)q, c0 + j, n, slots, ovf, ovf_cap, novf);
-      }
-    };
-    unsigned todo = __ballot_sync(0xffffffffu, inq && root >= 0);
-    while (todo) {
-      const int r = __shfl_sync(0xffffffffu, root, __ffs(todo) - 1);
-      const bool mine = ((todo >> lane) & 1u) && root == r;
-      todo &= ~__ballot_sync(0xffffffffu, mine);
-      const float4 RA = tnode[2 * r], RB = tnode[2 * r + 1];
-      const bool rh = mine && hit_ab(RA, RB, plo, phi);
-      if (!__any_sync(0xffffffffu, rh)) continue;
-      const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
-      if (rcnt > 0) {
-        leaf_cells(rlink, rcnt, r, rh);
-        continue;
-      }
-      int top = 0;
-      if (lane == 0) stk[0] = rlink;
-      top = 1;
-      __syncwarp();
-      bool overflow = false;
-      while (top > 0) {
-        const int base = stk[--top];
-        __syncwarp();
-        int lk[4], lc[4];
-        bool hk[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const float4 A = tnode[2 * (long long)(base + k)], B = tnode[2 * (long long)(base + k) + 1];
-          lk[k] = __float_as_int(B.z);
-          lc[k] = __float_as_int(B.w);
-          hk[k] = mine && hit_ab(A, B, plo, phi);  // empty slots hold an empty box
-        }
-        unsigned anyh = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) anyh |= (__any_sync(0xffffffffu, hk[k]) ? 1u : 0u) << k;
-        // internal children onto the stack (the lowest popped first), then the leaves
-#pragma unroll
-        for (int k = 3; k >= 0; k--)
-          if (((anyh >> k) & 1u) && lc[k] < 0) {
-            if (top >= kWarpStack) {
-              overflow = true;
-            } else {
-              if (lane == 0) stk[top] = lk[k];
-              top++;
-            }
-          }
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-          if (((anyh >> k) & 1u) && lc[k] > 0) leaf_cells(lk[k], lc[k], base + k, hk[k]);
-        if (overflow) {
-          if (lane == 0) atomicOr(err, kErrTraversalOverflow);
-          break;
-        }
-      }
-    }
-    if (inq) ncand_q[q] = n;
   }
 }
 
@@ -1847,17 +1800,14 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 }
 
 void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const uint2* qbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex) {
   if (form == 0)
-    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+    k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf, err, skip_uhex);
-  else if (form == 2)  // split form, warp-cooperative
-    k_traverse_warp<<<blocks, 256, 0, st>>>(x, bi, qbox, tnode, qnode, qdon, nq, slots, ncand_q, ovf, ovf_cap, novf,
-                                            err, skip_uhex);
   else
-    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, qbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
+    k_traverse<1><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf, err, skip_uhex);
 }
 
