@@ -103,6 +103,10 @@ def parse():
     p.add_argument("--fields", default="host", choices=["host", "device"],
                    help="cfg3: the requests' 5 fields in pinned host memory or on the device")
     p.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    p.add_argument("--tuning", default="",
+                   help="launch shapes by hand instead of the autotuner, tioga_b200_tuning_'s order: cell-pass "
+                        "CTAs/SM, pairs per cell-pass CTA, query CTAs/SM, traversal CTAs/SM, candidate CTAs/SM, "
+                        "cell-pass variant (0 gathers, 1 leaf groups); e.g. 3,128,16,64,16,1")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
     p.add_argument("--forms", default="split,plain,e2e,e2e_pageable",
@@ -230,12 +234,23 @@ def pinned_copy(system):
     return cases.System(blocks, system.name, system.meta), ibls, keep
 
 
+def set_tuning(lib, text: str):
+    v = [int(t) for t in text.split(",")]
+    v += [0] * (6 - len(v))
+    lib.lib.tioga_b200_set_tuning_((C.c_int * 6)(*v[:6]))
+
+
 def autotune(lib, tb, reps: int = 2) -> dict:
     """The library's autotuner (tioga_b200_autotune_) on the loaded workload;
     returns the launch shapes it chose."""
     tb.set_int(lib.lib, "tioga_b200_autotune_", reps)
     if lib.lib.tioga_b200_last_error() != 0:
         raise RuntimeError("autotune failed")
+    return read_tuning(lib)
+
+
+def read_tuning(lib) -> dict:
+    """The launch shapes in use (tioga_b200_tuning_)."""
     out = (C.c_int * 8)()
     lib.lib.tioga_b200_tuning_(out)
     keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
@@ -314,7 +329,9 @@ def run_gpu(args, ws, rank, local, dist):
     lib.performconnectivity()
     if lib.lib.tioga_b200_last_error() != 0:
         raise RuntimeError("connectivity failed")
-    tuning = None if args.no_tune else autotune(lib, tb)
+    if args.tuning:
+        set_tuning(lib, args.tuning)
+    tuning = read_tuning(lib) if (args.no_tune or args.tuning) else autotune(lib, tb)
 
     # device-resident forms keep iblank in HBM too (a GPU solver's arrays)
     d_ibl = [torch.ones(b.nnodes, dtype=torch.int32, device="cuda") for b in system.blocks]
@@ -616,7 +633,9 @@ def run_gpu_batch(args, ws, rank, local, dist):
             d_ibl.append(d)
             lib.lib.tioga_b200_registeriblank_device_(C.byref(C.c_int(b.tag)), C.c_void_p(d.data_ptr()))
     tb.set_int(lib.lib, "tioga_b200_set_coords_resident_", 1)
-    tuning = None if args.no_tune else autotune(lib, tb)
+    if args.tuning:
+        set_tuning(lib, args.tuning)
+    tuning = read_tuning(lib) if (args.no_tune or args.tuning) else autotune(lib, tb)
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     clocks = Clocks(vis.split(",")[local] if vis else str(local))
     ms_b, per_b, st, ph, launches, clk = events_time(args.steps, args.warmup, clocks)
