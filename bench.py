@@ -47,26 +47,23 @@ WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherica
             "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
-# DRAM bytes (read + write) of one split-form cell-pass launch per cell, from
-# an ncu capture on the full workload (profiles/k_cell_pass_cfg1.md); None
-# until one is made for the current kernel.
-CELL_PASS_DRAM_BYTES_PER_CELL = None
+# DRAM bytes (read + write) of one k_cell_boxes launch per cell, from an ncu
+# capture on the full workload (profiles/k_cell_boxes_cfg1.md); None until
+# one is made for the current kernel.
+CELL_BOX_DRAM_BYTES_PER_CELL = None
 
 
-def cell_pass_bytes(system, st, variant: int):
-    """Compulsory bytes of one split-form cell-pass launch, each array read or
-    written once.  Both variants read each cell's type (1 B) and write its
-    FP32 box (24 B), read each leaf's record (16 B) and write its box (24 B).
-    Variant 0 reads the padded connectivity as the reference's vertex
-    references (4 B each) and each node's FP32 copy once (16 B; the copy is
-    made by k_round_nodes, outside this launch).  Variant 1 reads each leaf
-    group's header (16 B) and node list (4 B a node), each node's FP64
-    coordinates once (24 B) and each cell's vertex positions (8 B)."""
+def cell_box_bytes(system, st):
+    """Compulsory bytes of one k_cell_boxes launch (the split form's cell and
+    leaf boxes), each array read or written once: per cell its vertex
+    references (4 B each, the reference's connectivity), its type (1 B) read
+    and its FP32 box (24 B) written; per node its FP32 copy (16 B, made by
+    k_round_nodes outside this launch) read once; per leaf its record (16 B)
+    read and its box (24 B) written."""
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
-    common = system.ncells * (1 + 24) + st["nleaf"] * (16 + 24)
-    if variant == 1:
-        return 16 * st["ngroups"] + 4 * st["ngroup_nodes"] + 24 * system.nnodes + 8 * system.ncells + common
-    return 4 * nvsum + 16 * system.nnodes + common
+    return 4 * nvsum + 16 * system.nnodes + system.ncells * (1 + 24) + st["nleaf"] * (16 + 24)
+
+
 # bounded CPU sample: the same geometry at 97^3 background and 25x25x49 shells
 CPU_SAMPLE = dict(nbg=97, nshell=3, nr=25, nt=25, nphi=49, split_layers=4)
 CPU_SAMPLE_TEXT = ("cfg1 geometry at reduced resolution (97^3 background, three 25x25x49 shells, "
@@ -106,7 +103,7 @@ def parse():
     p.add_argument("--tuning", default="",
                    help="launch shapes by hand instead of the autotuner, tioga_b200_tuning_'s order: cell-pass "
                         "CTAs/SM, pairs per cell-pass CTA, query CTAs/SM, traversal CTAs/SM, candidate CTAs/SM, "
-                        "cell-pass variant (0 gathers, 1 leaf groups); e.g. 3,128,16,64,16,1")
+                        "cell-box CTAs/SM; e.g. 3,128,16,64,16,6")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
     p.add_argument("--forms", default="split,plain,e2e,e2e_pageable",
@@ -254,7 +251,7 @@ def read_tuning(lib) -> dict:
     out = (C.c_int * 8)()
     lib.lib.tioga_b200_tuning_(out)
     keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
-            "candidate_ctas_per_sm", "cell_pass_variant"]
+            "candidate_ctas_per_sm", "cell_box_ctas_per_sm"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 
@@ -385,16 +382,13 @@ def run_gpu(args, ws, rank, local, dist):
         ms_e2e = float("nan")
     h2d = sum(24 * b.nnodes for b in system.blocks)
     d2h = sum(4 * b.nnodes for b in system.blocks)
-    # Dominant kernel: the cell pass (one launch per step).  Its compulsory
-    # bytes: connectivity (4 B per vertex reference) and the cell type (1 B)
-    # read, each node's FP32 coordinates read once (16 B), every cell's box
-    # written (24 B), and per leaf its record read (16 B) and box written (24 B).
-    cell_ms = ph["cell_pass"]
+    # Roofline kernel: k_cell_boxes, the cell pass's pass over every cell (one
+    # launch per step; cell_box_bytes gives its compulsory bytes).
+    cell_ms = ph["cell_boxes"]
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
-    variant = (tuning or {}).get("cell_pass_variant", 0)
-    alg_bytes = cell_pass_bytes(system, st, variant)
-    traffic = (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
-               else CELL_PASS_DRAM_BYTES_PER_CELL * system.ncells)
+    alg_bytes = cell_box_bytes(system, st)
+    traffic = (None if CELL_BOX_DRAM_BYTES_PER_CELL is None
+               else CELL_BOX_DRAM_BYTES_PER_CELL * system.ncells)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -421,10 +415,10 @@ def run_gpu(args, ws, rank, local, dist):
         "speedup_vs_plain": ms_plain / ms_split,
         "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
-        "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
+        "roofline": {"kernel": "k_cell_boxes (FP32 cell and leaf boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": alg_bytes, "launch_ms": cell_ms,
-                     "variant": variant,
+                     "pairs_kernel_ms": ph["cell_pass"] - ph["cell_boxes"],
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
@@ -659,10 +653,9 @@ def run_gpu_batch(args, ws, rank, local, dist):
     nodes = sum(s.nnodes for s in systems)
     cells = sum(s.ncells for s in systems)
     h2d, d2h = 24 * nodes, 4 * nodes
-    cell_ms = ph["cell_pass"]
+    cell_ms = ph["cell_boxes"]
     nvsum = sum(nv * conn.shape[0] for s in systems for b in s.blocks for nv, conn in b.cells)
-    alg_bytes = cell_pass_bytes(cases.System([b for sy in systems for b in sy.blocks]), st,
-                                (tuning or {}).get("cell_pass_variant", 0))
+    alg_bytes = cell_box_bytes(cases.System([b for sy in systems for b in sy.blocks]), st)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -696,11 +689,12 @@ def run_gpu_batch(args, ws, rank, local, dist):
         "speedup_vs_plain": plain_ms[0] / ms_b,
         "e2e": {"value": ws * Q / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
-        "roofline": {"kernel": "k_cell_pass (cell and leaf boxes, exact reduced boxes)", "bound": "hbm",
+        "roofline": {"kernel": "k_cell_boxes (FP32 cell and leaf boxes)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (None if CELL_PASS_DRAM_BYTES_PER_CELL is None
-                                 else CELL_PASS_DRAM_BYTES_PER_CELL * cells), "algorithmic_bytes": alg_bytes,
-                     "launch_ms": cell_ms, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+                     "traffic": (None if CELL_BOX_DRAM_BYTES_PER_CELL is None
+                                 else CELL_BOX_DRAM_BYTES_PER_CELL * cells), "algorithmic_bytes": alg_bytes,
+                     "launch_ms": cell_ms, "pairs_kernel_ms": ph["cell_pass"] - ph["cell_boxes"],
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "phases_ms": ph,
         "search": {"candidates": st["ncand"], "fp64_refinements": st["nrefine"], "ties": st["nties"],
                    "donors": st["ndonor"]},

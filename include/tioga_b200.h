@@ -256,11 +256,10 @@ void tioga_b200_server_stats(void *srv, long long out[16]);
 void tioga_b200_autotune_(int *reps);
 /* The shapes in use: [0] cell-pass CTAs per SM, [1] pairs per cell-pass CTA,
  * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM,
- * [5] split-form cell pass: 0 gathers from an FP32 coordinate copy, 1 leaf
- * groups with their distinct nodes staged in shared memory. */
+ * [5] CTAs per SM of the split form's cell-box kernel. */
 void tioga_b200_tuning_(int out[8]);
 /* Set the shapes by hand, in tioga_b200_tuning_'s order [0..5]; values <= 0
- * keep a shape ([5] takes 0 or 1). */
+ * keep a shape. */
 void tioga_b200_set_tuning_(const int in[6]);
 
 /* 0 when the last call succeeded, else a negative code. */
@@ -292,8 +291,7 @@ void tioga_b200_getcelliblank_(int *btag, int *iblank_cell);
  * refinements, [5] receptors, [6] holes, [7] donor records, [8] device
  * error bits, [9] pairs of blocks, [10] kernels launched by the library,
  * [11] sum of the candidates' vertex counts, [12] leaves of the cell trees,
- * [13] query points merged into a coincident one (uniqNodesTree),
- * [14] leaf groups of the cell pass, [15] their distinct vertex nodes. */
+ * [13] query points merged into a coincident one (uniqNodesTree). */
 void tioga_b200_stats_(long long out[16]);
 /* More counters of the last connectivity call: [0] cells of its hole maps. */
 void tioga_b200_stats2_(long long out[8]);
@@ -354,7 +352,8 @@ void tioga_b200_set_test_bound_(int *which, int *value);
  * [4] search, [5] donor bookkeeping, [6] cell iblank, [7] iblank download,
  * [8] total; inside the search: [9] traversal, [10] candidate screen,
  * [11] FP64 refinement; [12] the cell pass alone (cell and leaf boxes,
- * reduced boxes), inside [2]. */
+ * reduced boxes), inside [2]; [13] the split form's cell-box kernel alone,
+ * inside [12]. */
 void tioga_b200_timing_(float out[16]);
 
 #ifdef __cplusplus

@@ -41,7 +41,7 @@ def stats(lib: C.CDLL) -> dict:
     out = (C.c_longlong * 16)()
     lib.tioga_b200_stats_(out)
     keys = ["nquery", "ndonor", "nties", "ncand", "nrefine", "nreceptor", "nhole", "nrecords",
-            "error", "npairs", "launches", "cand_verts", "nleaf", "nmerged", "ngroups", "ngroup_nodes"]
+            "error", "npairs", "launches", "cand_verts", "nleaf", "nmerged"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 
@@ -49,7 +49,8 @@ def timing(lib: C.CDLL) -> dict:
     out = (C.c_float * 16)()
     lib.tioga_b200_timing_(out)
     keys = ["upload", "holemap", "boxes_refit", "query", "search", "donors", "celliblank",
-            "download", "total", "search_traverse", "search_candidates", "search_refine", "cell_pass"]
+            "download", "total", "search_traverse", "search_candidates", "search_refine", "cell_pass",
+            "cell_boxes"]
     return {k: float(out[i]) for i, k in enumerate(keys)}
 
 

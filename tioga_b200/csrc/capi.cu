@@ -302,8 +302,6 @@ void tioga_b200_stats_(long long out[16]) {
   out[11] = s.cand_verts;
   out[12] = s.nleaf;
   out[13] = s.nmerged;
-  out[14] = s.ngroups;
-  out[15] = s.ngroup_nodes;
 }
 
 void tioga_b200_registernodegid_(int* btag, uint64_t* node_gid) {
@@ -351,7 +349,7 @@ void tioga_b200_tuning_(int out[8]) {
   out[2] = t.query_per_sm;
   out[3] = t.traverse_per_sm;
   out[4] = t.candidates_per_sm;
-  out[5] = t.cell_pass_variant;
+  out[5] = t.cell_box_per_sm;
 }
 
 void tioga_b200_set_tuning_(const int in[6]) {
@@ -380,6 +378,7 @@ void tioga_b200_timing_(float out[16]) {
   out[10] = t.candidates;
   out[11] = t.refine;
   out[12] = t.cell_pass;
+  out[13] = t.cell_boxes;
 }
 
 }  // extern "C"

@@ -47,7 +47,7 @@ Engine::~Engine() {
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); xf_.release(); tnode_.release(); tnode64_.release();
-  grp_.release(); grp_nodes_.release(); cell_lidx_.release(); leaves_.release(); gparent_.release(); gnk_.release();
+  leaves_.release(); gparent_.release(); gnk_.release();
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
@@ -711,7 +711,6 @@ int Engine::build_tree_topology() {
     TB_CUDA(cudaStreamSynchronize(stream_));
     for (int b = nb - 1; b >= 0; b--)
       if (h_blk_leaf_[b] < 0) h_blk_leaf_[b] = h_blk_leaf_[b + 1];
-    TB_TRY(build_leaf_groups());
   }
   // cells (storage order) that mark their wall-bearing block's hole map
   {
@@ -993,51 +992,6 @@ int Engine::run_holemaps() {
   return 0;
 }
 
-// Leaf groups of kGroupLeaves consecutive leaves of one block (the cell
-// pass's unit of work for one warp) with their distinct vertex nodes and the
-// cells' positions in them (k_group_nodes); once per topology.
-int Engine::build_leaf_groups() {
-  const int nb = (int)bi_.size();
-  std::vector<int2> hg;
-  h_blk_grp_.assign(nb + 1, 0);
-  for (int b = 0; b < nb; b++) {
-    h_blk_grp_[b] = (int)hg.size();
-    for (int l = h_blk_leaf_[b]; l < h_blk_leaf_[b + 1]; l += kGroupLeaves)
-      hg.push_back(make_int2(l, std::min(kGroupLeaves, h_blk_leaf_[b + 1] - l)));
-  }
-  h_blk_grp_[nb] = (int)hg.size();
-  ngrp_ = (long long)hg.size();
-  ngrp_nodes_ = 0;
-  TB_CUDA(grp_.ensure(std::max(1ll, ngrp_)));
-  TB_CUDA(cell_lidx_.ensure(std::max(1ll, ctot_)));
-  if (ngrp_ == 0) return 0;
-  DBuf<int2> gl;
-  DBuf<int> cnt, off;
-  TB_CUDA(gl.ensure(ngrp_));
-  TB_CUDA(cnt.ensure(ngrp_ + 1));
-  TB_CUDA(off.ensure(ngrp_ + 1));
-  TB_CUDA(cudaMemcpyAsync(gl.p, hg.data(), ngrp_ * sizeof(int2), cudaMemcpyHostToDevice, stream_));
-  TB_CUDA(cudaMemsetAsync(cnt.p + ngrp_, 0, sizeof(int), stream_));
-  const unsigned grid = (unsigned)std::max(1ll, std::min((ngrp_ + 7) / 8, 148ll * 64));
-  launch_group_nodes(false, grid, stream_, gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, cnt.p, nullptr, nullptr,
-                     nullptr, nullptr);
-  TB_LAUNCHED("k_group_nodes");
-  size_t tmp = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, (int)(ngrp_ + 1), stream_);
-  TB_CUDA(cub_tmp_.ensure(tmp));
-  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, cnt.p, off.p, (int)(ngrp_ + 1), stream_);
-  int total = 0;
-  TB_CUDA(cudaMemcpyAsync(&total, off.p + ngrp_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
-  TB_CUDA(grp_nodes_.ensure(std::max(1, total)));
-  launch_group_nodes(true, grid, stream_, gl.p, ngrp_, leaves_.p, conn8_.p, cell_nv_.p, nullptr, off.p,
-                     grp_nodes_.p, cell_lidx_.p, grp_.p);
-  TB_LAUNCHED("k_group_nodes");
-  TB_CUDA(cudaStreamSynchronize(stream_));  // the host list and the scratch go out of scope
-  ngrp_nodes_ = total;
-  return 0;
-}
-
 int Engine::run_pairs_and_refit() {
   const int nb = (int)hb_.size();
   TB_CUDA(d_pairs_.ensure(npcand_ + 1));
@@ -1059,7 +1013,7 @@ int Engine::run_pairs_and_refit() {
     TB_LAUNCHED("k_node_tiles");
   }
   if (npairs_ == 0) return 0;
-  if (precision_ != 0 && tune_.cell_pass_variant == 0) {  // FP32 coordinates for the gather variant
+  if (precision_ != 0) {  // FP32 coordinates for the cell boxes
     TB_CUDA(xf_.ensure(ntot_));
     k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
     TB_LAUNCHED("k_round_nodes");
@@ -1091,19 +1045,24 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
   // chunks of consecutive blocks whose pairs fit one CTA's shared memory;
-  // the CTAs of one launch are split among the chunks by their work items:
-  // leaf groups (one warp each) in the split form, leaves (a quarter warp
-  // each) in the FP64 form
+  // the CTAs of one launch are split among the chunks by leaf count.  The
+  // FP64 kernel writes every cell's box, so its chunks cover every block;
+  // the split form's pair kernel only visits blocks that donate to a pair.
   const int kChunkPairs = std::max(16, std::min(128, tune_.chunk_pairs));
-  const bool groups = !fp64 && tune_.cell_pass_variant == 1;
-  const std::vector<int>& item_of_blk = groups ? h_blk_grp_ : h_blk_leaf_;
-  const long long nitems = groups ? ngrp_ : nleaf_total_;
-  const long long per_cta = groups ? 256 / 32 : 256 / kMaxLeafCells;  // items a CTA of 256 threads takes at once
+  const std::vector<int>& item_of_blk = h_blk_leaf_;
+  const long long per_cta = 256 / kMaxLeafCells;  // leaves a CTA of 256 threads takes at once
+  auto donates = [&](int b) { return fp64 || h_pfirst_[b + 1] > h_pfirst_[b]; };
   std::vector<int4> chunks;
+  long long nitems = 0;
   for (int b = 0; b < nb;) {
+    if (!donates(b)) {
+      b++;
+      continue;
+    }
     int e = b + 1;
-    while (e < nb && h_pfirst_[e + 1] - h_pfirst_[b] <= kChunkPairs) e++;
+    while (e < nb && donates(e) && h_pfirst_[e + 1] - h_pfirst_[b] <= kChunkPairs) e++;
     chunks.push_back(make_int4(item_of_blk[b], item_of_blk[e], h_pfirst_[b], h_pfirst_[e] - h_pfirst_[b]));
+    nitems += item_of_blk[e] - item_of_blk[b];
     b = e;
   }
   const long long want = grid_for(nitems * (256 / per_cta), 256, 148 * tune_.cell_pass_per_sm);
@@ -1122,15 +1081,21 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(d_chunk_cta_.p, ccta.data(), ccta.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
   TB_CUDA(cudaEventRecord(cev_[0], stream_));
   const size_t smem = (size_t)maxnp * (6 * sizeof(unsigned long long) + sizeof(PairCull) + 6 * sizeof(int));
-  if (fp64)
+  if (fp64) {
     launch_cell_pass64(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
                        leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p,
                        cbox64_.p, tnode_.p, tnode64_.p, pair_acc_.p);
-  else
-    launch_cell_pass32(tune_.cell_pass_variant, tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, xf_.p,
-                       conn8_.p, cell_nv_.p, d_bi_.p, leaves_.p, grp_.p, grp_nodes_.p, cell_lidx_.p, d_chunks_.p,
-                       d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p, tnode_.p,
-                       pair_acc_.p);
+    TB_CUDA(cudaEventRecord(cev_[2], stream_));
+  } else {
+    const int mb = tune_.cell_box_per_sm;
+    launch_cell_boxes(mb, (int)grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p,
+                      cell_nv_.p, leaves_.p, nleaf_total_, cbox_.p, tnode_.p);
+    TB_LAUNCHED("k_cell_boxes");
+    TB_CUDA(cudaEventRecord(cev_[2], stream_));
+    launch_cell_pairs(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
+                      leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
+                      tnode_.p, pair_acc_.p);
+  }
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
@@ -1939,7 +1904,7 @@ int Engine::autotune(int reps) {
       {&tune_.cell_pass_per_sm, {2, 3, 4}, &Timing::cell_pass},
       {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
       {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
-      {&tune_.cell_pass_variant, {0, 1}, &Timing::cell_pass},
+      {&tune_.cell_box_per_sm, {4, 6, 8}, &Timing::cell_boxes},
       {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},
       {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
   };
@@ -2021,8 +1986,6 @@ int Engine::connectivity() {
   stats_.nreceptor = (long long)cnt[5];
   stats_.nrecords = nrec_;
   stats_.nleaf = nleaf_total_;
-  stats_.ngroups = ngrp_;
-  stats_.ngroup_nodes = ngrp_nodes_;
   stats_.nmerged = (long long)cnt[7];
   stats_.npairs = npairs_;
   stats_.launches = nlaunch_;
@@ -2041,7 +2004,11 @@ int Engine::connectivity() {
   cudaEventElapsedTime(&timing_.total, ev_[0], ev_[8]);
   timing_.traverse = timing_.candidates = timing_.refine = 0;
   timing_.cell_pass = 0;
-  if (cell_timed_) cudaEventElapsedTime(&timing_.cell_pass, cev_[0], cev_[1]);
+  timing_.cell_boxes = 0;
+  if (cell_timed_) {
+    cudaEventElapsedTime(&timing_.cell_pass, cev_[0], cev_[1]);
+    cudaEventElapsedTime(&timing_.cell_boxes, cev_[0], cev_[2]);
+  }
   if (search_timed_) {
     cudaEventElapsedTime(&timing_.traverse, sev_[0], sev_[1]);
     cudaEventElapsedTime(&timing_.candidates, sev_[1], sev_[2]);

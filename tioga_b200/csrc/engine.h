@@ -21,7 +21,6 @@
 namespace tb {
 
 constexpr int kMaxLeafCells = 8; // cells per tree leaf at most
-constexpr int kGroupLeaves = 4;  // leaves per group, the cell pass's unit of work for one warp
 // device counters of the sparse donor phase (dcnt_)
 constexpr int kHoles = 0;        // holes, the first entries of the marked-node list
 constexpr int kMarked = 1;       // holes plus nfringe layers
@@ -227,8 +226,6 @@ struct Stats {
   long long npairs = 0;       // intersecting (receptor, donor) block pairs
   long long launches = 0;     // kernels this library launched in the call
   long long cand_verts = 0;   // sum of the vertex counts of the Newton candidates
-  long long ngroups = 0;      // leaf groups (the split-form cell pass's units of work)
-  long long ngroup_nodes = 0; // distinct vertex nodes summed over the leaf groups
   long long holemap_cells = 0; // cells of this call's hole maps
   unsigned error = 0;
 };
@@ -238,7 +235,7 @@ struct Stats {
 // candidate screen, and the pairs one cell-pass CTA holds in shared memory.
 struct Tuning {
   int cell_pass_per_sm = 3, query_per_sm = 16, traverse_per_sm = 64, candidates_per_sm = 16, chunk_pairs = 128;
-  int cell_pass_variant = 0;  // split form: gathers from an FP32 copy (0) or leaf groups staged in shared memory (1)
+  int cell_box_per_sm = 6;  // split form: CTAs per SM of the box kernel (4, 6 or 8)
 };
 
 struct Timing {
@@ -246,6 +243,7 @@ struct Timing {
         total = 0, upload = 0, download = 0;
   float traverse = 0, candidates = 0, refine = 0;  // stages of the search
   float cell_pass = 0;                              // the cell pass kernel(s) alone
+  float cell_boxes = 0;                             // split form: its box kernel alone
 };
 
 class Engine {
@@ -256,13 +254,13 @@ class Engine {
   // Lowered device bounds for tests of the error paths (0 = the normal
   // bound): which 0 = hole-map fill rounds, 1 = donor-record capacity.
   // launch shapes set by hand (the tuning array's order; values <= 0 keep
-  // the current shape, except the cell-pass variant, which takes 0 too)
+  // the current shape)
   int set_tuning(const int in[6]) {
     int* v[5] = {&tune_.cell_pass_per_sm, &tune_.chunk_pairs, &tune_.query_per_sm, &tune_.traverse_per_sm,
                  &tune_.candidates_per_sm};
     for (int i = 0; i < 5; i++)
       if (in[i] > 0) *v[i] = in[i];
-    if (in[5] == 0 || in[5] == 1) tune_.cell_pass_variant = in[5];
+    if (in[5] > 0) tune_.cell_box_per_sm = in[5];
     return 0;
   }
   int set_test_bound(int which, int value) {
@@ -358,7 +356,6 @@ class Engine {
   int run_holemaps();
   int preprocess_resolutions();
   int run_pairs_and_refit();
-  int build_leaf_groups();
   int setup_uniform_hex();
   int run_gid_merge();
   void pin_caller_arrays();
@@ -425,7 +422,7 @@ class Engine {
   long long nlaunch_ = 0;
   cudaEvent_t ev_[12];
   cudaEvent_t sev_[4];
-  cudaEvent_t cev_[2];  // around the cell pass
+  cudaEvent_t cev_[3];  // around the cell pass (split form: and between its two kernels)
   bool cell_timed_ = false;
 
   // flat device arrays
@@ -492,13 +489,8 @@ class Engine {
   // tree
   DBuf<int> sorted_cell_;
   DBuf<float4> cbox_;      // split form: 2 per sorted cell (FP32 box rounded outward)
-  DBuf<float4> xf_;        // coordinates rounded to FP32, one per node (the gather variant of the cell pass)
+  DBuf<float4> xf_;        // coordinates rounded to FP32, one per node (split-form cell boxes)
   DBuf<float4> tnode_;     // 2 per tree node
-  DBuf<int4> grp_;         // leaf groups: (first leaf, leaves, first node, nodes)
-  DBuf<int> grp_nodes_;    // each group's distinct vertex nodes, ascending
-  DBuf<uint2> cell_lidx_;  // 1 per sorted cell: its vertices' positions in its group's node list
-  long long ngrp_ = 0, ngrp_nodes_ = 0;
-  std::vector<int> h_blk_grp_;    // groups of block b: [h_blk_grp_[b], h_blk_grp_[b + 1])
   DBuf<double> tnode64_;   // 6 per tree node (FP64 form)
   DBuf<double> cbox64_;    // 6 per sorted cell (FP64 form)
   long long tree_nodes_ = 0;      // slots, four per group

@@ -101,19 +101,17 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
                         int* pfirst);
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
-void launch_cell_pass32(int variant, int minb, int grid, size_t smem, cudaStream_t st, const double* x,
-                        const float4* xf, const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
-                        const int4* leaves, const int4* grp, const int* grp_nodes, const uint2* cell_lidx,
-                        const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
-                        const PairInfo* pairs, float4* cbox, float4* tnode, unsigned long long* acc);
-__global__ void k_round_nodes(const double* x, long long n, float4* xf);
+void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode);
+void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                       const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
+                       const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
+                       const float4* cbox, const float4* tnode, unsigned long long* acc);
 void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                         const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                         const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
                         float4* tnode, double* tnode64, unsigned long long* acc);
-void launch_group_nodes(bool fill, unsigned grid, cudaStream_t st, const int2* grp_leaf, long long ngrp,
-                        const int4* leaves, const int* conn8, const unsigned char* cell_nv, int* cnt, const int* off,
-                        int* nodes, uint2* lidx, int4* grp);
+
 __global__ void k_tree_split(const unsigned long long* key, int n, const int* ca, const int* cb, const int* cslot,
                              int2* kids, int* nk, int* isint, int2* tlink, int* leaf_at);
 __global__ void k_tree_link(int n, const int* cslot, const int2* kids, const int* nk, const int* isint,
@@ -128,6 +126,7 @@ __global__ void k_block_leaves(const int4* leaves, long long nleaf, int* first);
 __global__ void k_group_nint(const float4* tnode, int g_root, int ngroups, int* nint, int* start, int* nstart);
 __global__ void k_refit_fused(const int* start, int nstart, const int* gparent, const int* nint, int g_root,
                               int* cnt, float4* tnode, double* tnode64);
+__global__ void k_round_nodes(const double* x, long long n, float4* xf);
 __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
                              float4* tbox, const int* node_order);
 __global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,

@@ -676,15 +676,18 @@ __device__ __forceinline__ void project_cell64(const double* __restrict__ x, con
 // receptor box is done with that pair; one clearly inside, whose projections
 // cannot reach the current extents' bounds, tightens them and is done too.
 // The remaining (leaf, pair) combinations go cell by cell.
-__device__ __forceinline__ void cell_pass_pairs(
-    const double* __restrict__ x, const int* __restrict__ conn8, const BlockInfo* __restrict__ bi,
-    const PairInfo* __restrict__ pairs, const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
-    unsigned long long* __restrict__ s_acc, int lane, bool leaf_ok, bool valid, long long c, int nv, int qa0, int qb0,
-    const float f[6], const double cc[3], const float hh[3]) {
+// First part: every leaf tests its box f against the pairs of its block,
+// lane g of the leaf taking pairs qa+g, qa+g+LC, ...; returns the mask of
+// pairs (bit q - qa) that need cell-by-cell work, the same in every lane of
+// the leaf, and the pair range [qa, qb) the lane's leaf takes part in.
+__device__ __forceinline__ unsigned leaf_pairs_mixed(const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
+                                                     int lane, bool leaf_ok, int qa0, int qb0, const float f[6],
+                                                     int& qa, int& qb) {
   constexpr int LC = kMaxLeafCells;
   volatile int* v_ext = s_ext;
   const bool leaf_live = leaf_ok && f[0] <= f[3];
-  const int qa = leaf_live ? qa0 : 0, qb = leaf_live ? qb0 : 0;
+  qa = leaf_live ? qa0 : 0;
+  qb = leaf_live ? qb0 : 0;
   const int g = lane % LC;
   unsigned mixed = 0u;
   {
@@ -732,6 +735,18 @@ __device__ __forceinline__ void cell_pass_pairs(
       for (int o = 1; o < LC; o <<= 1) mixed |= __shfl_xor_sync(0xffffffffu, mixed, o);
     }
   }
+  return mixed;
+}
+
+// Second part: the cells of the mixed (leaf, pair) combinations, with the
+// cell's box (centre cc, half sizes hh), exactly as getReducedOBB decides.
+__device__ __forceinline__ void cell_pairs_exact(const double* __restrict__ x, const int* __restrict__ conn8,
+                                                 const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs,
+                                                 const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
+                                                 unsigned long long* __restrict__ s_acc, int lane, bool valid,
+                                                 long long c, int nv, unsigned mixed, int qa, int qb,
+                                                 const double cc[3], const float hh[3]) {
+  volatile int* v_ext = s_ext;
   float sc = 0.f;
   for (int k = 0; k < 3; k++) sc += valid ? fabsf((float)cc[k]) : 0.f;
   const int q0 = __reduce_min_sync(0xffffffffu, (valid && mixed) ? qa : 0x7fffffff);
@@ -794,6 +809,18 @@ __device__ __forceinline__ void cell_pass_pairs(
         }
     }
   }
+}
+
+
+// Both parts, for the kernels that hold every cell's box in registers.
+__device__ __forceinline__ void cell_pass_pairs(
+    const double* __restrict__ x, const int* __restrict__ conn8, const BlockInfo* __restrict__ bi,
+    const PairInfo* __restrict__ pairs, const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
+    unsigned long long* __restrict__ s_acc, int lane, bool leaf_ok, bool valid, long long c, int nv, int qa0, int qb0,
+    const float f[6], const double cc[3], const float hh[3]) {
+  int qa, qb;
+  const unsigned mixed = leaf_pairs_mixed(s_pc, s_ext, lane, leaf_ok, qa0, qb0, f, qa, qb);
+  cell_pairs_exact(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, valid, c, nv, mixed, qa, qb, cc, hh);
 }
 
 // this CTA's chunk: the last one whose first CTA is <= blockIdx.x.  Work
@@ -860,117 +887,79 @@ __device__ __forceinline__ void cell_pass_flush(const unsigned long long* s_acc,
   }
 }
 
-// Cell pass of the split form, one warp per leaf group (up to 4 leaves of one
-// block, one lane per cell; chunk work items are groups):
-//  * the group's distinct nodes are read once, rounded to FP32 and staged in
-//    shared memory; every cell reads its vertices there through its one-byte
-//    positions (k_group_nodes), so a warp issues about 3 coalesced coordinate
-//    loads instead of 8 scattered gathers;
-//  * each cell's box is rounded outward from the FP32 vertices (f_down/f_up
-//    cover every double that rounds onto them) into cbox, and the leaf box
-//    (the union of its cells' boxes) goes to the leaf's tree slot;
-//  * the reduced boxes of the pairs, exact (cell_pass_pairs).
+// Cell pass of the split form, in two kernels.
+//
+// k_cell_boxes: leaf by leaf (32 / kMaxLeafCells leaves per warp, one lane per
+// cell), each lane gathers its cell's eight FP32 vertices (xf, rounded to
+// nearest by k_round_nodes; slots past the vertex count read vertex 0 again,
+// so the eight loads are unconditional and in flight together), rounds the
+// box outward (f_down/f_up cover every double that rounds onto a vertex) into
+// cbox, and the leaf's lanes write the union to the leaf's tree slot.  It
+// holds nothing else, so it runs at a high occupancy that hides the gathers.
 template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_cell_pass32(
-    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ grp,
-    const int* __restrict__ grp_nodes, const uint2* __restrict__ cell_lidx, const int4* __restrict__ chunks,
-    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, float4* __restrict__ tnode,
-    unsigned long long* __restrict__ acc) {
-  extern __shared__ unsigned long long s_dyn[];
-  __shared__ float4 s_node[8][256];
-  int cta, ncta;
-  const int kc = chunk_of_cta(chunk_cta, nchunks);
-  const int4 CH = chunks[kc];  // first group, end group, first pair, pairs
-  unsigned long long* s_acc = s_dyn;                              // 6 per pair, exact extents
-  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * CH.w);  // 1 per pair
-  int* s_ext = reinterpret_cast<int*>(s_pc + CH.w);                // 6 per pair, FP32 bounds
-  cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta);
-  const long long g_lo = CH.x, g_hi = CH.y;
-  const int p0 = CH.z;
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  float4* sn = s_node[w];
-  const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
-  const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
-  constexpr int LC = kMaxLeafCells;
-  int4 Gnext = g_lo + warp0 < g_hi ? grp[g_lo + warp0] : make_int4(0, 0, 0, 0);
-  for (long long gi = g_lo + warp0; gi < g_hi; gi += nwarps) {
-    const int4 G = Gnext;  // first leaf, leaves, first node, nodes
-    if (gi + nwarps < g_hi) Gnext = grp[gi + nwarps];  // the next group's header, in flight meanwhile
-    const int j = lane / LC, ci = lane % LC;
-    const bool leaf_ok = j < G.y;
-    const int4 L = leaf_ok ? leaves[G.x + j] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
-    const bool valid = leaf_ok && ci < L.y;
-    const long long c = (long long)L.x + ci;
-    int nv = 0;
-    uint2 li = make_uint2(0u, 0u);
-    if (valid) {
-      nv = cell_nv[c];
-      li = cell_lidx[c];
-    }
-    for (int i = lane; i < G.w; i += 32) {
-      const double* v = x + 3 * (long long)grp_nodes[G.z + i];
-      sn[i] = make_float4(__double2float_rn(v[0]), __double2float_rn(v[1]), __double2float_rn(v[2]), 0.f);
-    }
-    __syncwarp();
+__global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restrict__ xf,
+                                                          const int* __restrict__ conn8,
+                                                          const unsigned char* __restrict__ cell_nv,
+                                                          const int4* __restrict__ leaves, long long nleaf,
+                                                          float4* __restrict__ cbox, float4* __restrict__ tnode) {
+  constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long base = LPW * warp0; base < nleaf; base += LPW * nwarps) {
+    const long long leaf = base + lane / LC;
+    const bool leaf_ok = leaf < nleaf;
+    const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
+    const bool valid = leaf_ok && lane % LC < L.y;
+    const long long c = (long long)L.x + lane % LC;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     if (valid) {
+      const int nv = cell_nv[c];
+      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
+      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
+      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
       for (int m = 0; m < 8; m++) {
-        const unsigned k = ((m < 4 ? li.x : li.y) >> (8 * (m & 3))) & 255u;
-        const float4 v = sn[k];
+        const float4 v = xf[m < nv ? cv[m] : cv[0]];
         lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
         hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
       }
     }
-    __syncwarp();  // the next group's staging may overwrite sn
-    float fb[6];   // FP32 box, rounded outward
-    double cc[3];  // box centre
-    float hh[3];   // half sizes, rounded up
-    for (int k = 0; k < 3; k++) {
-      fb[k] = valid ? f_down(lo[k]) : INFINITY;
-      fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
-      cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
-      hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
-    }
-    // leaf box: union over the LC lanes of the leaf
     float f[6];
-    for (int k = 0; k < 6; k++) f[k] = fb[k];
+    for (int k = 0; k < 3; k++) {
+      f[k] = valid ? f_down(lo[k]) : INFINITY;
+      f[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
+    }
+    if (valid) {
+      cbox[2 * c] = make_float4(f[0], f[1], f[2], f[3]);
+      cbox[2 * c + 1] = make_float4(f[4], f[5], 0.f, 0.f);
+    }
     for (int o = 1; o < LC; o <<= 1)
       for (int k = 0; k < 3; k++) {
         f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
         f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
       }
-    if (valid) {
-      cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
-      cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
-    }
-    if (leaf_ok && ci == 0) {
+    if (leaf_ok && lane % LC == 0) {
       const long long sl = L.z;
       tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
       *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
     }
-    const int b = L.w;
-    cell_pass_pairs(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, leaf_ok, valid, c, nv,
-                    leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
   }
-  cell_pass_flush(s_acc, p0, CH.w, acc);
 }
 
-// Cell pass of the split form, gather variant: leaf by leaf (32 /
-// kMaxLeafCells leaves per warp, one lane per cell; chunk work items are
-// leaves), each lane gathering its cell's eight FP32 vertices (xf, rounded to
-// nearest by k_round_nodes; slots past the vertex count read vertex 0 again,
-// so the eight loads are unconditional and in flight together).  The boxes,
-// leaf boxes and reduced boxes are those of k_cell_pass32; the autotuner picks
-// the faster variant for the workload.
+// k_cell_pairs: the reduced boxes of the pairs (getReducedOBB,
+// MeshBlock.C:774-838), over the leaves of the blocks that donate to some
+// pair (chunk work items are leaves): each leaf's box from its tree slot is
+// tested against the pairs first (leaf_pairs_mixed); only the leaves with a
+// mixed (leaf, pair) combination read their cells' boxes back from cbox for
+// the exact cell-by-cell work (cell_pairs_exact).  The boxes are the ones
+// k_cell_boxes wrote, so every decision is the one-kernel form's.
 template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_cell_pass32g(
-    const double* __restrict__ x, const float4* __restrict__ xf, const int* __restrict__ conn8,
-    const unsigned char* __restrict__ cell_nv, const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves,
-    const int4* __restrict__ chunks, const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, float4* __restrict__ cbox, float4* __restrict__ tnode,
+__global__ void __launch_bounds__(256, MINB) k_cell_pairs(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ chunks,
+    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, const float4* __restrict__ cbox, const float4* __restrict__ tnode,
     unsigned long long* __restrict__ acc) {
   extern __shared__ unsigned long long s_dyn[];
   int cta, ncta;
@@ -990,55 +979,36 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass32g(
     const long long leaf = base + lane / LC;
     const bool leaf_ok = leaf < leaf_hi;
     const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
+    float f[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    if (leaf_ok) {
+      const float4 A = tnode[2 * (long long)L.z], B = tnode[2 * (long long)L.z + 1];
+      f[0] = A.x; f[1] = A.y; f[2] = A.z; f[3] = A.w; f[4] = B.x; f[5] = B.y;
+    }
+    const int b = L.w;
+    int qa, qb;
+    const unsigned mixed = leaf_pairs_mixed(s_pc, s_ext, lane, leaf_ok, leaf_ok ? pfirst[b] - p0 : 0,
+                                            leaf_ok ? pfirst[b + 1] - p0 : 0, f, qa, qb);
+    if (!__any_sync(0xffffffffu, mixed != 0u)) continue;
     const bool valid = leaf_ok && lane % LC < L.y;
     const long long c = (long long)L.x + lane % LC;
     int nv = 0;
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    if (valid) {
+    double cc[3] = {0.0, 0.0, 0.0};
+    float hh[3] = {0.f, 0.f, 0.f};
+    if (valid && mixed) {
       nv = cell_nv[c];
-      const int4 c0 = *reinterpret_cast<const int4*>(conn8 + 8 * c);
-      const int4 c1 = *reinterpret_cast<const int4*>(conn8 + 8 * c + 4);
-      const int cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-#pragma unroll
-      for (int m = 0; m < 8; m++) {
-        const float4 v = xf[m < nv ? cv[m] : cv[0]];
-        lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
-        hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
-      }
-    }
-    float fb[6];
-    double cc[3];
-    float hh[3];
-    for (int k = 0; k < 3; k++) {
-      fb[k] = valid ? f_down(lo[k]) : INFINITY;
-      fb[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
-      cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
-      hh[k] = valid ? __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f) : 0.f;
-    }
-    float f[6];
-    for (int k = 0; k < 6; k++) f[k] = fb[k];
-    for (int o = 1; o < LC; o <<= 1)
+      const float4 A = cbox[2 * c], B = cbox[2 * c + 1];
+      const float fb[6] = {A.x, A.y, A.z, A.w, B.x, B.y};
       for (int k = 0; k < 3; k++) {
-        f[k] = fminf(f[k], __shfl_xor_sync(0xffffffffu, f[k], o));
-        f[k + 3] = fmaxf(f[k + 3], __shfl_xor_sync(0xffffffffu, f[k + 3], o));
+        cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
+        hh[k] = __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f);
       }
-    if (valid) {
-      cbox[2 * c] = make_float4(fb[0], fb[1], fb[2], fb[3]);
-      cbox[2 * c + 1] = make_float4(fb[4], fb[5], 0.f, 0.f);
     }
-    if (leaf_ok && lane % LC == 0) {
-      const long long sl = L.z;
-      tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
-      *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
-    }
-    const int b = L.w;
-    cell_pass_pairs(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, leaf_ok, valid, c, nv,
-                    leaf_ok ? pfirst[b] - p0 : 0, leaf_ok ? pfirst[b + 1] - p0 : 0, f, cc, hh);
+    cell_pairs_exact(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, valid && mixed, c, nv, mixed, qa, qb, cc, hh);
   }
   cell_pass_flush(s_acc, p0, CH.w, acc);
 }
 
-// FP32 copy of the coordinates (rounded to nearest), for the gather variant
+// FP32 copy of the coordinates (rounded to nearest), for k_cell_boxes
 __global__ void k_round_nodes(const double* __restrict__ x, long long n, float4* __restrict__ xf) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]), __double2float_rn(x[3 * i + 2]),
@@ -1147,27 +1117,27 @@ static void set_smem(K kern, size_t smem) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void launch_cell_pass32(int variant, int minb, int grid, size_t smem, cudaStream_t st, const double* x,
-                        const float4* xf, const int* conn8, const unsigned char* cell_nv, const BlockInfo* bi,
-                        const int4* leaves, const int4* grp, const int* grp_nodes, const uint2* cell_lidx,
-                        const int4* chunks, const int* chunk_cta, int nchunks, const int* pfirst,
-                        const PairInfo* pairs, float4* cbox, float4* tnode, unsigned long long* acc) {
-#define TB_CP32(MB)                                                                                              \
-  do {                                                                                                           \
-    if (variant == 1) {                                                                                          \
-      set_smem(k_cell_pass32<MB>, smem);                                                                         \
-      k_cell_pass32<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, grp, grp_nodes, cell_lidx,       \
-                                                 chunks, chunk_cta, nchunks, pfirst, pairs, cbox, tnode, acc);   \
-    } else {                                                                                                     \
-      set_smem(k_cell_pass32g<MB>, smem);                                                                        \
-      k_cell_pass32g<MB><<<grid, 256, smem, st>>>(x, xf, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, \
-                                                  pfirst, pairs, cbox, tnode, acc);                              \
-    }                                                                                                            \
+void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode) {
+  if (minb <= 4) k_cell_boxes<4><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
+  else if (minb <= 6) k_cell_boxes<6><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
+  else k_cell_boxes<8><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
+}
+
+void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
+                       const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
+                       const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
+                       const float4* cbox, const float4* tnode, unsigned long long* acc) {
+#define TB_CPP(MB)                                                                                           \
+  do {                                                                                                       \
+    set_smem(k_cell_pairs<MB>, smem);                                                                        \
+    k_cell_pairs<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst, \
+                                              pairs, cbox, tnode, acc);                                      \
   } while (0)
-  if (minb <= 2) TB_CP32(2);
-  else if (minb == 3) TB_CP32(3);
-  else TB_CP32(4);
-#undef TB_CP32
+  if (minb <= 2) TB_CPP(2);
+  else if (minb == 3) TB_CPP(3);
+  else TB_CPP(4);
+#undef TB_CPP
 }
 
 void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,

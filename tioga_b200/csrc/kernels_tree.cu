@@ -129,122 +129,6 @@ __global__ void k_leaf_list(const int* __restrict__ leaf_at, const int* __restri
   }
 }
 
-// Leaf groups, the cell pass's unit of work for one warp: up to kGroupLeaves
-// consecutive leaves of one block (at most 32 cells).  Every group's distinct
-// vertex nodes are listed once, in ascending global id, and every cell gets
-// the positions of its vertices in that list, one byte each (slots past the
-// cell's vertex count repeat vertex 0's position).  The cell pass then loads
-// each node once per group into shared memory instead of once per vertex
-// reference (a structured hexahedral group of 32 cells has 75 distinct nodes
-// against 256 references).  Built once per topology.
-// FILL = false: cnt[g] = distinct nodes of group g.  FILL = true: the nodes at
-// off[g], the cells' positions, and grp[g] = (first leaf, leaves, off, count).
-template <bool FILL>
-__global__ void __launch_bounds__(256) k_group_nodes(const int2* __restrict__ grp_leaf, long long ngrp,
-                                                     const int4* __restrict__ leaves, const int* __restrict__ conn8,
-                                                     const unsigned char* __restrict__ cell_nv, int* __restrict__ cnt,
-                                                     const int* __restrict__ off, int* __restrict__ nodes,
-                                                     uint2* __restrict__ lidx, int4* __restrict__ grp) {
-  __shared__ int s_key[8][256];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int* key = s_key[w];
-  for (long long g = blockIdx.x * 8ll + w; g < ngrp; g += gridDim.x * 8ll) {
-    const int2 GL = grp_leaf[g];  // first leaf, leaves
-    const int j = lane >> 3, i = lane & 7;
-    int4 L = make_int4(0, 0, 0, 0);
-    bool valid = false;
-    if (j < GL.y) {
-      L = leaves[GL.x + j];
-      valid = i < L.y;
-    }
-    const long long c = (long long)L.x + i;
-    int nv = 0, cv[8];
-#pragma unroll
-    for (int m = 0; m < 8; m++) cv[m] = 0;
-    if (valid) {
-      nv = cell_nv[c];
-#pragma unroll
-      for (int m = 0; m < 8; m++) cv[m] = conn8[8 * c + m];
-    }
-#pragma unroll
-    for (int m = 0; m < 8; m++) key[8 * lane + m] = (valid && m < nv) ? cv[m] : 0x7fffffff;
-    __syncwarp();
-    // bitonic sort of the group's 256 vertex references, ascending
-    for (int k = 2; k <= 256; k <<= 1)
-      for (int s = k >> 1; s > 0; s >>= 1) {
-        for (int t = lane; t < 128; t += 32) {
-          const int a = 2 * s * (t / s) + (t % s), b = a + s;
-          const int ka = key[a], kb = key[b];
-          if ((ka > kb) == ((a & k) == 0)) {
-            key[a] = kb;
-            key[b] = ka;
-          }
-        }
-        __syncwarp();
-      }
-    // first occurrences, compacted in order
-    int vals[8], nf = 0;
-    unsigned fl = 0u;
-#pragma unroll
-    for (int m = 0; m < 8; m++) {
-      const int p = 8 * lane + m;
-      vals[m] = key[p];
-      if (vals[m] != 0x7fffffff && (p == 0 || key[p - 1] != vals[m])) {
-        fl |= 1u << m;
-        nf++;
-      }
-    }
-    int incl = nf;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    __syncwarp();
-    if (!FILL) {
-      if (lane == 0) cnt[g] = total;
-      continue;
-    }
-    int pos = incl - nf;
-    const int base = off[g];
-#pragma unroll
-    for (int m = 0; m < 8; m++)
-      if ((fl >> m) & 1u) {
-        key[pos] = vals[m];
-        nodes[base + pos] = vals[m];
-        pos++;
-      }
-    __syncwarp();
-    if (valid) {
-      unsigned b[8];
-#pragma unroll
-      for (int m = 0; m < 8; m++) {
-        const int id = m < nv ? cv[m] : cv[0];
-        int lo = 0, hi = total;
-        while (lo < hi) {
-          const int mid = (lo + hi) >> 1;
-          if (key[mid] < id) lo = mid + 1;
-          else hi = mid;
-        }
-        b[m] = (unsigned)lo;
-      }
-      lidx[c] = make_uint2(b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24),
-                           b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24));
-    }
-    if (lane == 0) grp[g] = make_int4(GL.x, GL.y, base, total);
-    __syncwarp();
-  }
-}
-// host launcher (the template's instantiations live in this translation unit)
-void launch_group_nodes(bool fill, unsigned grid, cudaStream_t st, const int2* grp_leaf, long long ngrp,
-                        const int4* leaves, const int* conn8, const unsigned char* cell_nv, int* cnt, const int* off,
-                        int* nodes, uint2* lidx, int4* grp) {
-  if (fill)
-    k_group_nodes<true><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
-  else
-    k_group_nodes<false><<<grid, 256, 0, st>>>(grp_leaf, ngrp, leaves, conn8, cell_nv, cnt, off, nodes, lidx, grp);
-}
-
 // One-launch refit.  At build time every child group g >= g_root (the root
 // groups hold the blocks' roots and have no parent) counts its internal
 // slots (nint[g]); the groups with none start the refit.  Per call, each
