@@ -58,7 +58,7 @@ def cell_box_bytes(system, st):
     leaf boxes), each array read or written once: per cell its vertex
     references (4 B each, the reference's connectivity), its type (1 B) read
     and its FP32 box (24 B) written; per node its FP32 copy (16 B, made by
-    k_round_nodes outside this launch) read once; per leaf its record (16 B)
+    k_node_tiles outside this launch) read once; per leaf its record (16 B)
     read and its box (24 B) written."""
     nvsum = sum(nv * conn.shape[0] for b in system.blocks for nv, conn in b.cells)
     return 4 * nvsum + 16 * system.nnodes + system.ncells * (1 + 24) + st["nleaf"] * (16 + 24)

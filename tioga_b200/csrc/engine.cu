@@ -31,6 +31,7 @@ Engine::Engine() {
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : sev_) cudaEventCreate(&e);
   for (auto& e : cev_) cudaEventCreate(&e);
+  cudaEventCreateWithFlags(&pev_, cudaEventDisableTiming);
 }
 
 Engine::~Engine() {
@@ -40,6 +41,7 @@ Engine::~Engine() {
   for (auto& e : ev_) cudaEventDestroy(e);
   for (auto& e : sev_) cudaEventDestroy(e);
   for (auto& e : cev_) cudaEventDestroy(e);
+  cudaEventDestroy(pev_);
   x_.release(); node_res_.release(); cell_res_.release(); iblank_.release(); iblank_cell_.release();
   conn8_.release(); node_blk_.release(); cell_blk_.release(); cell_nv_.release(); wallf_.release();
   obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
@@ -47,7 +49,7 @@ Engine::~Engine() {
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); xf_.release(); tnode_.release(); tnode64_.release();
-  leaves_.release(); gparent_.release(); gnk_.release();
+  leaves_.release(); lbox_.release(); pair_ext_.release(); gparent_.release(); gnk_.release();
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
@@ -1005,19 +1007,19 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(cudaMemcpyAsync(h_pairs_.data(), d_pairs_.p, (npcand_ + 1) * sizeof(PairInfo), cudaMemcpyDeviceToHost,
                           stream_));
   TB_CUDA(cudaMemcpyAsync(h_pfirst_.data(), d_pfirst_.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
-  // the node tiles' boxes (query gathering, hole search)
+  TB_CUDA(cudaEventRecord(pev_, stream_));
+  // the node tiles' boxes (query gathering, hole search) and, for the split
+  // form's cell boxes, the FP32 copy of the coordinates, while the host
+  // waits for the pairs
+  if (precision_ != 0) TB_CUDA(xf_.ensure(ntot_));
   if (h_tile_base_.back() > 0) {
     k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
-                                                                      node_order_.p);
+                                                                      node_order_.p,
+                                                                      precision_ != 0 ? xf_.p : nullptr);
     TB_LAUNCHED("k_node_tiles");
   }
+  TB_CUDA(cudaEventSynchronize(pev_));
   if (npairs_ == 0) return 0;
-  if (precision_ != 0) {  // FP32 coordinates for the cell boxes
-    TB_CUDA(xf_.ensure(ntot_));
-    k_round_nodes<<<grid_for(ntot_, kT), kT, 0, stream_>>>(x_.p, ntot_, xf_.p);
-    TB_LAUNCHED("k_round_nodes");
-  }
   // refit to the current coordinates: one pass over the cells (tree-order
   // cell boxes + reduced boxes of every pair), then the tree levels, then the
   // node tiles of the query gathering
@@ -1044,13 +1046,21 @@ int Engine::run_pairs_and_refit() {
   TB_CUDA(pair_acc_.ensure(6 * npairs_));
   TB_CUDA(cudaMemcpyAsync(pair_acc_.p, acc.data(), acc.size() * sizeof(unsigned long long),
                           cudaMemcpyHostToDevice, stream_));
+  if (!fp64) {  // the seeds of the extents' bounds start open
+    std::vector<int> ext(6 * npairs_);
+    for (int i = 0; i < 6 * npairs_; i++) ext[i] = (i % 6 < 3) ? 0x7fffffff : (int)0x80000000;
+    TB_CUDA(pair_ext_.ensure(6 * npairs_));
+    TB_CUDA(cudaMemcpyAsync(pair_ext_.p, ext.data(), ext.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+  }
   // chunks of consecutive blocks whose pairs fit one CTA's shared memory;
   // the CTAs of one launch are split among the chunks by leaf count.  The
   // FP64 kernel writes every cell's box, so its chunks cover every block;
   // the split form's pair kernel only visits blocks that donate to a pair.
   const int kChunkPairs = std::max(16, std::min(128, tune_.chunk_pairs));
   const std::vector<int>& item_of_blk = h_blk_leaf_;
-  const long long per_cta = 256 / kMaxLeafCells;  // leaves a CTA of 256 threads takes at once
+  // leaves a CTA of 256 threads takes at once: a lane per cell in the FP64
+  // kernel, a lane per leaf in the split form's scan
+  const long long per_cta = fp64 ? 256 / kMaxLeafCells : 256;
   auto donates = [&](int b) { return fp64 || h_pfirst_[b + 1] > h_pfirst_[b]; };
   std::vector<int4> chunks;
   long long nitems = 0;
@@ -1088,13 +1098,15 @@ int Engine::run_pairs_and_refit() {
     TB_CUDA(cudaEventRecord(cev_[2], stream_));
   } else {
     const int mb = tune_.cell_box_per_sm;
+    TB_CUDA(lbox_.ensure(2 * nleaf_total_));
     launch_cell_boxes(mb, (int)grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p,
-                      cell_nv_.p, leaves_.p, nleaf_total_, cbox_.p, tnode_.p);
+                      cell_nv_.p, leaves_.p, nleaf_total_, cbox_.p, tnode_.p, lbox_.p);
     TB_LAUNCHED("k_cell_boxes");
     TB_CUDA(cudaEventRecord(cev_[2], stream_));
     launch_cell_pairs(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
                       leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
-                      tnode_.p, pair_acc_.p);
+                      lbox_.p, pair_ext_.p, pair_acc_.p);
+    TB_LAUNCHED("k_leaf_seeds");
   }
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));

@@ -423,6 +423,7 @@ class Engine {
   cudaEvent_t ev_[12];
   cudaEvent_t sev_[4];
   cudaEvent_t cev_[3];  // around the cell pass (split form: and between its two kernels)
+  cudaEvent_t pev_;     // the pairs' copy to the host has landed
   bool cell_timed_ = false;
 
   // flat device arrays
@@ -489,6 +490,8 @@ class Engine {
   // tree
   DBuf<int> sorted_cell_;
   DBuf<float4> cbox_;      // split form: 2 per sorted cell (FP32 box rounded outward)
+  DBuf<float4> lbox_;      // split form: 2 per leaf, in leaf order (its box, and its block in the 7th word)
+  DBuf<int> pair_ext_;     // split form: 6 per pair, the seeds of the extents' bounds (fkey order)
   DBuf<float4> xf_;        // coordinates rounded to FP32, one per node (split-form cell boxes)
   DBuf<float4> tnode_;     // 2 per tree node
   DBuf<double> tnode64_;   // 6 per tree node (FP64 form)

@@ -102,11 +102,12 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode);
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode,
+                       float4* lbox);
 void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
-                       const float4* cbox, const float4* tnode, unsigned long long* acc);
+                       const float4* cbox, const float4* lbox, int* ext, unsigned long long* acc);
 void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                         const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                         const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
@@ -126,9 +127,8 @@ __global__ void k_block_leaves(const int4* leaves, long long nleaf, int* first);
 __global__ void k_group_nint(const float4* tnode, int g_root, int ngroups, int* nint, int* start, int* nstart);
 __global__ void k_refit_fused(const int* start, int nstart, const int* gparent, const int* nint, int g_root,
                               int* cnt, float4* tnode, double* tnode64);
-__global__ void k_round_nodes(const double* x, long long n, float4* xf);
 __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
-                             float4* tbox, const int* node_order);
+                             float4* tbox, const int* node_order, float4* xf);
 __global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);
 __global__ void k_invert(const int* perm, long long n, int* inv);

@@ -656,26 +656,53 @@ __device__ __forceinline__ void project_cell64(const double* __restrict__ x, con
   }
 }
 
-// The reduced boxes (getReducedOBB, MeshBlock.C:774-838) of every pair whose
-// donor is this lane's block, from the lane's cell box.  Shared by both forms
-// of the cell pass; one lane per cell, kMaxLeafCells lanes per leaf.
-// FP32 bounds of a cell's vertex projections (box centre and half sizes,
-// widened by far more than their rounding error and the reference's) decide
-// what needs FP64:
-//  * a cell clearly outside the receptor box is skipped, one clearly inside
-//    overlaps it; only cells across its faces get the reference's FP64 test;
-//  * for the extents, each CTA keeps in shared memory an FP32 upper bound of
-//    every axis minimum (the least upper bound of any overlapping cell's
-//    projections seen so far) and a lower bound of every maximum.  A cell
-//    whose projections cannot reach below that bound cannot hold the minimum:
-//    the cell that does hold it always has its lower bound under every such
-//    upper bound, so it is always projected exactly.  The exact extents are
-//    combined per warp, per CTA in shared memory, and flushed once.
-// First every leaf tests its box f against the pairs s_pc[qa .. qb), lane g
-// of the leaf taking pairs qa+g, qa+g+LC, ...: a leaf clearly outside a
-// receptor box is done with that pair; one clearly inside, whose projections
-// cannot reach the current extents' bounds, tightens them and is done too.
-// The remaining (leaf, pair) combinations go cell by cell.
+// The reduced boxes (getReducedOBB, MeshBlock.C:774-838): for every pair,
+// the extents along the donor's axes of the donor's cells that overlap the
+// receptor's box.  FP32 bounds of a cell's or a leaf's projections (box
+// centre and half sizes, widened by far more than their rounding error and
+// the reference's) decide what needs FP64:
+//  * a cell or leaf clearly outside the receptor box is skipped, one clearly
+//    inside overlaps it; only cells across its faces get the reference's
+//    FP64 test;
+//  * for the extents, an FP32 upper bound of every axis minimum (the least
+//    upper bound of the projections of any leaf inside the receptor box, or
+//    the exact minimum of any overlapping cell rounded up) and a lower bound
+//    of every maximum are kept per pair.  A cell or leaf whose
+//    projections lie strictly between them on every axis cannot hold an
+//    extreme, whether it overlaps or not; the cell that does hold one always
+//    has its lower bound under every such upper bound, so it is always
+//    projected exactly.  The exact extents are combined per warp and by
+//    min/max atomics on order-preserving keys, so their order is free.
+// Each CTA keeps the bounds of its chunk's pairs in shared memory; the split
+// form starts them from seeds taken over every leaf inside a receptor box
+// (k_leaf_seeds), the FP64 form (k_cell_pass64) from open bounds.
+// A leaf (centre lc, half sizes lh) that is not outside pair q's receptor
+// box, against the pair's extent bounds (s_ext: per donor axis, in fkey
+// order, an upper bound of the reduced box's minimum and a lower bound of its
+// maximum): true when its projections on the donor's axes reach a bound, so
+// that its cells must be tested one by one.  A leaf whose projections lie
+// strictly between the bounds on every axis cannot hold an extreme, whether
+// its cells take part in the reduced box or not.  Every cell of a leaf
+// inside the receptor box takes part, so such a leaf (`inside`) then
+// tightens the bounds with its own projections (the minimum is at most the
+// leaf's upper bound, the maximum at least its lower bound).
+__device__ __forceinline__ bool leaf_reaches_extents(int* __restrict__ s_ext, int q, const double lc[3],
+                                                     const float lh[3], float lsc, const PairCull& Q, bool inside) {
+  volatile int* v_ext = s_ext;
+  const float zero[3] = {0.f, 0.f, 0.f};
+  float blo[3], bhi[3];
+  proj_bounds(lc, Q.dxc, Q.dvec, lh, lsc, zero, blo, bhi);
+  bool mix = false;
+  for (int jx = 0; jx < 3; jx++) {
+    const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
+    const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
+    mix = mix || (kl <= umin) || (ku >= lmax);
+    if (inside && ku < umin) atomicMin(&s_ext[6 * q + jx], ku);
+    if (inside && kl > lmax) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+  }
+  return mix;
+}
+
 // First part: every leaf tests its box f against the pairs of its block,
 // lane g of the leaf taking pairs qa+g, qa+g+LC, ...; returns the mask of
 // pairs (bit q - qa) that need cell-by-cell work, the same in every lane of
@@ -684,7 +711,6 @@ __device__ __forceinline__ unsigned leaf_pairs_mixed(const PairCull* __restrict_
                                                      int lane, bool leaf_ok, int qa0, int qb0, const float f[6],
                                                      int& qa, int& qb) {
   constexpr int LC = kMaxLeafCells;
-  volatile int* v_ext = s_ext;
   const bool leaf_live = leaf_ok && f[0] <= f[3];
   qa = leaf_live ? qa0 : 0;
   qb = leaf_live ? qb0 : 0;
@@ -713,22 +739,7 @@ __device__ __forceinline__ unsigned leaf_pairs_mixed(const PairCull* __restrict_
             out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
             inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
           }
-          bool mix = !out && !inside;
-          if (inside) {
-            const float zero[3] = {0.f, 0.f, 0.f};
-            proj_bounds(lc, Q.dxc, Q.dvec, lh, lsc, zero, blo, bhi);
-            for (int jx = 0; jx < 3; jx++) {
-              const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-              const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
-              mix = mix || (kl <= umin) || (ku >= lmax);
-            }
-            if (!mix)
-              for (int jx = 0; jx < 3; jx++) {
-                const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-                if (ku < v_ext[6 * q + jx]) atomicMin(&s_ext[6 * q + jx], ku);
-                if (kl > v_ext[6 * q + 3 + jx]) atomicMax(&s_ext[6 * q + 3 + jx], kl);
-              }
-          }
+          const bool mix = !out && leaf_reaches_extents(s_ext, q, lc, lh, lsc, Q, inside);
           if (mix) mixed |= 1u << (q - qa);
         }
       }
@@ -765,8 +776,18 @@ __device__ __forceinline__ void cell_pairs_exact(const double* __restrict__ x, c
         out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
         inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
       }
-      bool ov = !out && inside;
-      if (!out && !inside) {  // across a face: the reference's test, MeshBlock.C:800-821
+      // a cell whose projections on the donor's axes lie strictly between
+      // the extents' bounds cannot hold an extreme: neither its overlap nor
+      // its projections matter
+      bool need = false;
+      if (!out) {
+        const float zero[3] = {0.f, 0.f, 0.f};
+        proj_bounds(cc, Q.dxc, Q.dvec, hh, sc, zero, blo, bhi);
+        for (int jx = 0; jx < 3; jx++)
+          need = need || (fkey(blo[jx]) <= v_ext[6 * q + jx]) || (fkey(bhi[jx]) >= v_ext[6 * q + 3 + jx]);
+      }
+      bool ov = need && inside;
+      if (need && !inside) {  // across a face: the reference's test, MeshBlock.C:800-821
         const Obb& R = bi[pairs[Q.pair].rec].obb;
         double bb[6] = {kBig, kBig, kBig, -kBig, -kBig, -kBig};
         project_cell64(x, conn8, c, nv, R, bb);
@@ -775,25 +796,19 @@ __device__ __forceinline__ void cell_pairs_exact(const double* __restrict__ x, c
         for (int jx = 0; jx < 3; jx++) ov = ov && !(bb[jx + 3] < -R.dxc[jx]);
       }
       if (ov) {
-        const float zero[3] = {0.f, 0.f, 0.f};
-        proj_bounds(cc, Q.dxc, Q.dvec, hh, sc, zero, blo, bhi);
-        bool need = false;
+        double pb[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};  // the reference's projections,
+        project_cell64(x, conn8, c, nv, bi[Q.don].obb, pb);               // MeshBlock.C:822-833
+        for (int jx = 0; jx < 3; jx++) {  // a cell that takes part tightens the bounds with its
+          const int eu = fkey(__double2float_ru(pb[jx]));      // exact extremes, rounded outward
+          const int el = fkey(__double2float_rd(pb[jx + 3]));
+          if (eu < v_ext[6 * q + jx]) atomicMin(&s_ext[6 * q + jx], eu);
+          if (el > v_ext[6 * q + 3 + jx]) atomicMax(&s_ext[6 * q + 3 + jx], el);
+        }
         for (int jx = 0; jx < 3; jx++) {
-          const int kl = fkey(blo[jx]), ku = fkey(bhi[jx]);
-          const int umin = v_ext[6 * q + jx], lmax = v_ext[6 * q + 3 + jx];
-          need = need || (kl <= umin) || (ku >= lmax);
-          if (ku < umin) atomicMin(&s_ext[6 * q + jx], ku);
-          if (kl > lmax) atomicMax(&s_ext[6 * q + 3 + jx], kl);
+          rlo[jx] = pb[jx];
+          rhi[jx] = pb[jx + 3];
         }
-        if (need) {  // the reference's projections, MeshBlock.C:822-833
-          double pb[6] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
-          project_cell64(x, conn8, c, nv, bi[Q.don].obb, pb);
-          for (int jx = 0; jx < 3; jx++) {
-            rlo[jx] = pb[jx];
-            rhi[jx] = pb[jx + 3];
-          }
-          contrib = true;
-        }
+        contrib = true;
       }
     }
     if (__any_sync(0xffffffffu, contrib)) {
@@ -838,18 +853,19 @@ __device__ __forceinline__ int chunk_of_cta(const int* __restrict__ chunk_cta, i
   return kc;
 }
 
-// the chunk's pairs into shared memory, the extents' accumulators cleared
+// the chunk's pairs into shared memory, the extents' accumulators cleared,
+// the extents' bounds from ext (the seeds) or open
 __device__ __forceinline__ void cell_pass_setup(const int4& CH, int kc, const int* __restrict__ chunk_cta,
                                                 const BlockInfo* __restrict__ bi, const PairInfo* __restrict__ pairs,
                                                 unsigned long long* s_acc, PairCull* s_pc, int* s_ext, int& cta,
-                                                int& ncta) {
+                                                int& ncta, const int* __restrict__ ext = nullptr) {
   const int p0 = CH.z, np = CH.w;
   cta = (int)blockIdx.x - chunk_cta[kc];
   ncta = chunk_cta[kc + 1] - chunk_cta[kc];
   const int tid = threadIdx.x;
   for (int i = tid; i < 6 * np; i += blockDim.x) {
     s_acc[i] = (i % 6 < 3) ? ~0ull : 0ull;
-    s_ext[i] = (i % 6 < 3) ? 0x7fffffff : (int)0x80000000;
+    s_ext[i] = ext ? ext[6 * (long long)p0 + i] : ((i % 6 < 3) ? 0x7fffffff : (int)0x80000000);
   }
   for (int i = tid; i < np; i += blockDim.x) {
     const PairInfo& P = pairs[p0 + i];
@@ -887,21 +903,72 @@ __device__ __forceinline__ void cell_pass_flush(const unsigned long long* s_acc,
   }
 }
 
-// Cell pass of the split form, in two kernels.
+// One lane's leaf (box f) against the pairs [qa, qb) of its block, as
+// leaf_pairs_mixed does for a leaf spread over kMaxLeafCells lanes: the mask
+// of pairs (bit q - qa) whose cells need the exact test.
+__device__ __forceinline__ unsigned leaf_lane_mixed(const PairCull* __restrict__ s_pc, int* __restrict__ s_ext,
+                                                    const float f[6], int qa, int qb) {
+  if (qb - qa > 32) return 0xffffffffu;  // more pairs than mask bits: cell by cell
+  unsigned mixed = 0u;
+  if (qb > qa) {
+    double lc[3];
+    float lh[3], lsc = 0.f;
+    for (int k = 0; k < 3; k++) {
+      lc[k] = 0.5 * ((double)f[k] + (double)f[k + 3]);
+      lh[k] = __fmul_ru(__fsub_ru(f[k + 3], f[k]), 0.5f);
+      lsc += fabsf((float)lc[k]);
+    }
+    for (int q = qa; q < qb; q++) {
+      const PairCull& Q = s_pc[q];
+      float blo[3], bhi[3];
+      proj_bounds(lc, Q.rxc, Q.rvec, lh, lsc, Q.rdxc, blo, bhi);
+      bool out = false, inside = true;
+      for (int jx = 0; jx < 3; jx++) {
+        out = out || (blo[jx] > Q.rdxc[jx]) || (bhi[jx] < -Q.rdxc[jx]);
+        inside = inside && (bhi[jx] <= Q.rdxc[jx]) && (blo[jx] >= -Q.rdxc[jx]);
+      }
+      const bool mix = !out && leaf_reaches_extents(s_ext, q, lc, lh, lsc, Q, inside);
+      if (mix) mixed |= 1u << (q - qa);
+    }
+  }
+  return mixed;
+}
+
+// One lane per leaf of the CTA's share of its chunk: the leaf's box and
+// block from lbox (a warp loads 32 consecutive leaves) and its block's pair
+// range within the chunk, [qa, qb); an empty range past the chunk's end.
+__device__ __forceinline__ void leaf_lane_load(const float4* __restrict__ lbox, const int* __restrict__ pfirst,
+                                               long long leaf, long long leaf_hi, int p0, float f[6], int& qa,
+                                               int& qb) {
+  f[0] = f[1] = f[2] = INFINITY;
+  f[3] = f[4] = f[5] = -INFINITY;
+  qa = qb = 0;
+  if (leaf < leaf_hi) {
+    const float4 A = lbox[2 * leaf], B = lbox[2 * leaf + 1];
+    f[0] = A.x; f[1] = A.y; f[2] = A.z; f[3] = A.w; f[4] = B.x; f[5] = B.y;
+    const int b = __float_as_int(B.z);
+    qa = pfirst[b] - p0;
+    qb = pfirst[b + 1] - p0;
+  }
+}
+
+// Cell pass of the split form, in three kernels.
 //
 // k_cell_boxes: leaf by leaf (32 / kMaxLeafCells leaves per warp, one lane per
 // cell), each lane gathers its cell's eight FP32 vertices (xf, rounded to
-// nearest by k_round_nodes; slots past the vertex count read vertex 0 again,
+// nearest by k_node_tiles; slots past the vertex count read vertex 0 again,
 // so the eight loads are unconditional and in flight together), rounds the
 // box outward (f_down/f_up cover every double that rounds onto a vertex) into
-// cbox, and the leaf's lanes write the union to the leaf's tree slot.  It
-// holds nothing else, so it runs at a high occupancy that hides the gathers.
+// cbox, and the leaf's lanes write the union to the leaf's tree slot and,
+// with the leaf's block, to lbox (leaf order).  It holds nothing else, so it
+// runs at a high occupancy that hides the gathers.
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restrict__ xf,
                                                           const int* __restrict__ conn8,
                                                           const unsigned char* __restrict__ cell_nv,
                                                           const int4* __restrict__ leaves, long long nleaf,
-                                                          float4* __restrict__ cbox, float4* __restrict__ tnode) {
+                                                          float4* __restrict__ cbox, float4* __restrict__ tnode,
+                                                          float4* __restrict__ lbox) {
   constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
   const int lane = threadIdx.x & 31;
   const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -943,24 +1010,23 @@ __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restri
       const long long sl = L.z;
       tnode[2 * sl] = make_float4(f[0], f[1], f[2], f[3]);
       *reinterpret_cast<float2*>(&tnode[2 * sl + 1]) = make_float2(f[4], f[5]);  // keep the link
+      lbox[2 * leaf] = make_float4(f[0], f[1], f[2], f[3]);
+      lbox[2 * leaf + 1] = make_float4(f[4], f[5], __int_as_float(L.w), 0.f);
     }
   }
 }
 
-// k_cell_pairs: the reduced boxes of the pairs (getReducedOBB,
-// MeshBlock.C:774-838), over the leaves of the blocks that donate to some
-// pair (chunk work items are leaves): each leaf's box from its tree slot is
-// tested against the pairs first (leaf_pairs_mixed); only the leaves with a
-// mixed (leaf, pair) combination read their cells' boxes back from cbox for
-// the exact cell-by-cell work (cell_pairs_exact).  The boxes are the ones
-// k_cell_boxes wrote, so every decision is the one-kernel form's.
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_cell_pairs(
-    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
-    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ chunks,
-    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, const float4* __restrict__ cbox, const float4* __restrict__ tnode,
-    unsigned long long* __restrict__ acc) {
+// k_leaf_seeds: over the chunks of k_cell_pairs, one lane per leaf tests the
+// leaf against its block's pairs (leaf_lane_mixed) for the bounds alone:
+// each CTA's tightest bounds, merged over the CTAs into ext (fkey order).
+// k_cell_pairs starts every CTA from them, so only the leaves and cells near
+// a pair's extremes are projected one by one, wherever they lie.
+__global__ void __launch_bounds__(256) k_leaf_seeds(const BlockInfo* __restrict__ bi,
+                                                    const int4* __restrict__ chunks,
+                                                    const int* __restrict__ chunk_cta, int nchunks,
+                                                    const int* __restrict__ pfirst,
+                                                    const PairInfo* __restrict__ pairs,
+                                                    const float4* __restrict__ lbox, int* __restrict__ ext) {
   extern __shared__ unsigned long long s_dyn[];
   int cta, ncta;
   const int kc = chunk_of_cta(chunk_cta, nchunks);
@@ -971,48 +1037,94 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pairs(
   cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta);
   const long long leaf_lo = CH.x, leaf_hi = CH.y;
   const int p0 = CH.z;
-  const int tid = threadIdx.x, lane = tid & 31;
-  const long long warp0 = ((long long)cta * blockDim.x + tid) >> 5;
-  const long long nwarps = ((long long)ncta * blockDim.x) >> 5;
-  constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
-  for (long long base = leaf_lo + LPW * warp0; base < leaf_hi; base += LPW * nwarps) {
-    const long long leaf = base + lane / LC;
-    const bool leaf_ok = leaf < leaf_hi;
-    const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
-    float f[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    if (leaf_ok) {
-      const float4 A = tnode[2 * (long long)L.z], B = tnode[2 * (long long)L.z + 1];
-      f[0] = A.x; f[1] = A.y; f[2] = A.z; f[3] = A.w; f[4] = B.x; f[5] = B.y;
-    }
-    const int b = L.w;
+  const long long t0 = (long long)cta * blockDim.x + threadIdx.x;
+  const long long nt = (long long)ncta * blockDim.x;
+  for (long long base = leaf_lo + (t0 & ~31ll); base < leaf_hi; base += nt) {
+    float f[6];
     int qa, qb;
-    const unsigned mixed = leaf_pairs_mixed(s_pc, s_ext, lane, leaf_ok, leaf_ok ? pfirst[b] - p0 : 0,
-                                            leaf_ok ? pfirst[b + 1] - p0 : 0, f, qa, qb);
-    if (!__any_sync(0xffffffffu, mixed != 0u)) continue;
-    const bool valid = leaf_ok && lane % LC < L.y;
-    const long long c = (long long)L.x + lane % LC;
-    int nv = 0;
-    double cc[3] = {0.0, 0.0, 0.0};
-    float hh[3] = {0.f, 0.f, 0.f};
-    if (valid && mixed) {
-      nv = cell_nv[c];
-      const float4 A = cbox[2 * c], B = cbox[2 * c + 1];
-      const float fb[6] = {A.x, A.y, A.z, A.w, B.x, B.y};
-      for (int k = 0; k < 3; k++) {
-        cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
-        hh[k] = __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f);
-      }
-    }
-    cell_pairs_exact(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, valid && mixed, c, nv, mixed, qa, qb, cc, hh);
+    leaf_lane_load(lbox, pfirst, base + (threadIdx.x & 31), leaf_hi, p0, f, qa, qb);
+    leaf_lane_mixed(s_pc, s_ext, f, qa, qb);
   }
-  cell_pass_flush(s_acc, p0, CH.w, acc);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 6 * CH.w; i += blockDim.x) {
+    const int v = s_ext[i];
+    int* dst = &ext[6 * (long long)p0 + i];
+    if (i % 6 < 3) {
+      if (v != 0x7fffffff) atomicMin(dst, v);
+    } else if (v != (int)0x80000000) {
+      atomicMax(dst, v);
+    }
+  }
 }
 
-// FP32 copy of the coordinates (rounded to nearest), for k_cell_boxes
-__global__ void k_round_nodes(const double* __restrict__ x, long long n, float4* __restrict__ xf) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]), __double2float_rn(x[3 * i + 2]),
-                        0.f);
+// k_cell_pairs: over the same chunks, one lane per leaf, the bounds starting
+// from the seeds: each leaf is tested against its block's pairs
+// (leaf_lane_mixed); then the warp's leaves with a (leaf, pair) combination
+// that needs its cells tested, four at a time, a lane per cell: their cells'
+// boxes are read back from cbox for the exact cell-by-cell work
+// (cell_pairs_exact).  The boxes are the ones k_cell_boxes wrote, so every
+// decision is the one-kernel form's.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_pairs(
+    const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
+    const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ chunks,
+    const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
+    const PairInfo* __restrict__ pairs, const float4* __restrict__ cbox, const float4* __restrict__ lbox,
+    const int* __restrict__ ext, unsigned long long* __restrict__ acc) {
+  extern __shared__ unsigned long long s_dyn[];
+  int cta, ncta;
+  const int kc = chunk_of_cta(chunk_cta, nchunks);
+  const int4 CH = chunks[kc];  // first leaf, end leaf, first pair, pairs
+  unsigned long long* s_acc = s_dyn;
+  PairCull* s_pc = reinterpret_cast<PairCull*>(s_dyn + 6 * CH.w);
+  int* s_ext = reinterpret_cast<int*>(s_pc + CH.w);
+  cell_pass_setup(CH, kc, chunk_cta, bi, pairs, s_acc, s_pc, s_ext, cta, ncta, ext);
+  const long long leaf_lo = CH.x, leaf_hi = CH.y;
+  const int p0 = CH.z;
+  const int lane = threadIdx.x & 31;
+  const long long t0 = (long long)cta * blockDim.x + threadIdx.x;
+  const long long nt = (long long)ncta * blockDim.x;
+  constexpr int LC = kMaxLeafCells;
+  for (long long base = leaf_lo + (t0 & ~31ll); base < leaf_hi; base += nt) {
+    float f[6];
+    int qa, qb;
+    leaf_lane_load(lbox, pfirst, base + lane, leaf_hi, p0, f, qa, qb);
+    const unsigned mixed = leaf_lane_mixed(s_pc, s_ext, f, qa, qb);
+    // the mixed leaves, four at a time, a lane per cell
+    unsigned todo = __ballot_sync(0xffffffffu, mixed != 0u);
+    while (todo) {
+      int src = -1;  // the leaf (lane of the scan) this lane's quarter takes
+      unsigned t = todo;
+      for (int j = 0; j < 32 / LC; j++) {
+        const int l = t ? __ffs(t) - 1 : -1;
+        if (j == lane / LC) src = l;
+        if (t) t &= t - 1;
+      }
+      todo = t;
+      const int s_lane = src < 0 ? 0 : src;
+      const unsigned m = __shfl_sync(0xffffffffu, mixed, s_lane);
+      const int sqa = __shfl_sync(0xffffffffu, qa, s_lane), sqb = __shfl_sync(0xffffffffu, qb, s_lane);
+      int4 L = make_int4(0, 0, 0, 0);
+      if (src >= 0) L = leaves[base + src];  // first cell, cells, slot, block
+      const bool valid = src >= 0 && lane % LC < L.y;
+      const long long c = (long long)L.x + lane % LC;
+      int nv = 0;
+      double cc[3] = {0.0, 0.0, 0.0};
+      float hh[3] = {0.f, 0.f, 0.f};
+      if (valid) {
+        nv = cell_nv[c];
+        const float4 A = cbox[2 * c], B = cbox[2 * c + 1];
+        const float fb[6] = {A.x, A.y, A.z, A.w, B.x, B.y};
+        for (int k = 0; k < 3; k++) {
+          cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
+          hh[k] = __fmul_ru(__fsub_ru(fb[k + 3], fb[k]), 0.5f);
+        }
+      }
+      cell_pairs_exact(x, conn8, bi, pairs, s_pc, s_ext, s_acc, lane, valid, c, nv, valid ? m : 0u,
+                       valid ? sqa : 0, valid ? sqb : 0, cc, hh);
+    }
+  }
+  cell_pass_flush(s_acc, p0, CH.w, acc);
 }
 
 // Cell pass of the FP64 form, leaf by leaf (32 / kMaxLeafCells leaves per
@@ -1118,21 +1230,26 @@ static void set_smem(K kern, size_t smem) {
 }
 
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode) {
-  if (minb <= 4) k_cell_boxes<4><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
-  else if (minb <= 6) k_cell_boxes<6><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
-  else k_cell_boxes<8><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode);
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode,
+                       float4* lbox) {
+#define TB_CB(MB) k_cell_boxes<MB><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode, lbox)
+  if (minb <= 4) TB_CB(4);
+  else if (minb <= 6) TB_CB(6);
+  else TB_CB(8);
+#undef TB_CB
 }
 
 void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
-                       const float4* cbox, const float4* tnode, unsigned long long* acc) {
+                       const float4* cbox, const float4* lbox, int* ext, unsigned long long* acc) {
+  set_smem(k_leaf_seeds, smem);
+  k_leaf_seeds<<<grid, 256, smem, st>>>(bi, chunks, chunk_cta, nchunks, pfirst, pairs, lbox, ext);
 #define TB_CPP(MB)                                                                                           \
   do {                                                                                                       \
     set_smem(k_cell_pairs<MB>, smem);                                                                        \
     k_cell_pairs<MB><<<grid, 256, smem, st>>>(x, conn8, cell_nv, bi, leaves, chunks, chunk_cta, nchunks, pfirst, \
-                                              pairs, cbox, tnode, acc);                                      \
+                                              pairs, cbox, lbox, ext, acc);                                  \
   } while (0)
   if (minb <= 2) TB_CPP(2);
   else if (minb == 3) TB_CPP(3);
@@ -1157,10 +1274,12 @@ void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const 
 }
 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
-// rounded outward), so the query gathering can skip tiles far from a region.
+// rounded outward), so the query gathering can skip tiles far from a region;
+// with xf, every node's coordinates rounded to nearest FP32 (k_cell_boxes).
 __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
                                                     int nb, const long long* __restrict__ tile_base,
-                                                    float4* __restrict__ tbox, const int* __restrict__ node_order) {
+                                                    float4* __restrict__ tbox, const int* __restrict__ node_order,
+                                                    float4* __restrict__ xf) {
   __shared__ float sh[6][8];
   const long long T = blockIdx.x;
   const int b = block_of_tile(tile_base, nb, T);
@@ -1168,8 +1287,10 @@ __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int i = t0 + threadIdx.x; i < min(t0 + kNodeTile, B.nnodes); i += blockDim.x) {
-    const double* p = x + 3 * (long long)node_order[B.node_off + i];
+    const int nd = node_order[B.node_off + i];
+    const double* p = x + 3 * (long long)nd;
     const float4 v = make_float4(__double2float_rn(p[0]), __double2float_rn(p[1]), __double2float_rn(p[2]), 0.f);
+    if (xf) xf[nd] = v;
     lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
     hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
   }
