@@ -43,6 +43,8 @@ from tioga_b200.capi import TiogaLibrary  # noqa: E402
 
 METRIC = "connectivity receptors/s & p99 latency vs plain GPU form, 0 iblank/donor mismatch"
 UNIT = "receptors/s"
+WORKLOAD0 = ("cfg0: 65^3 all-hex background on [-5,5]^3 + one all-hex spherical shell 33x33x65 (radii 0.5-2.0, "
+             "radial stretching 1.1), interior nodes perturbed by 5% of the spacing")
 WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherical shells "
             "65x65x129 (first 4 radial layers split into tets/prisms/pyramids), seed 1")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
@@ -87,8 +89,9 @@ def parse():
     p.add_argument("--cpu-reps", type=int, default=3)
     p.add_argument("--size", default="full", choices=["full", "medium", "small"],
                    help="cfg1 at full size, at 161^3 + 49x49x97 shells (profiling), or at test size")
-    p.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg3", "cfg4"],
-                   help="cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems; "
+    p.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"],
+                   help="cfg0: the small all-hex system, CPU-runnable at full size (its reference arm times it "
+                        "whole); cfg1: one mixed-element system (default); cfg2: the batched form, 64 systems; "
                         "cfg3: the serving form, Poisson requests over resident moving systems; "
                         "cfg4: the high-order path, degree-3 Lagrange shell over a degree-1 background")
     p.add_argument("--rates", default="",
@@ -307,7 +310,9 @@ def run_gpu(args, ws, rank, local, dist):
     import tioga_b200 as tb
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    if args.size == "small":
+    if args.workload == "cfg0":
+        system = cases.small_config0(args.seed) if args.size == "small" else cases.config0(args.seed)
+    elif args.size == "small":
         system = cases.small_config1(args.seed)
     elif args.size == "medium":
         system = cases.config1(args.seed, nbg=161, nshell=3, nr=49, nt=49, nphi=97, split_layers=4)
@@ -401,7 +406,8 @@ def run_gpu(args, ws, rank, local, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded mesh generator tioga_b200.cases)",
-        "config": {"workload": WORKLOAD if args.size == "full" else f"cfg1 geometry, {args.size} size",
+        "config": {"workload": (WORKLOAD0 if args.workload == "cfg0" else WORKLOAD) if args.size == "full"
+                   else f"{args.workload} geometry, {args.size} size",
                    "nodes": system.nnodes, "cells": system.ncells, "blocks": len(system.blocks),
                    "query_points": Q, "receptors": st["nreceptor"], "holes": st["nhole"],
                    "precision": "fp32 Newton screen + fp64 refinement",
@@ -428,7 +434,7 @@ def run_gpu(args, ws, rank, local, dist):
         "clocks": clk,
     }
     # parity of the timed configuration against the compiled reference
-    if args.size == "full" and args.seed == 1 and not args.no_parity:
+    if args.workload == "cfg1" and args.size == "full" and args.seed == 1 and not args.no_parity:
         out["parity"] = parity_vs_reference(lib, tb, psys, "cfg1_full", 21)
     # the whole call against its compulsory bytes (B_conn): every array of the
     # path read or written once -- coordinates, connectivity, cell and node
@@ -1009,12 +1015,12 @@ def sample_query_count(sample):
     return tot
 
 
-def cpu_reference(reps: int, warmup: int = 1):
+def cpu_reference(reps: int, warmup: int = 1, whole_cfg0: bool = False):
     lib = REF_LIB if os.path.exists(REF_LIB) else PORT_LIB
     kind = "reference" if lib == REF_LIB else "port"
     if not os.path.exists(lib):
         return None, "no CPU build of the reference or the port (run `make -C oracle`)"
-    sample = cases.config1(1, **CPU_SAMPLE)
+    sample = cases.config0(1) if whole_cfg0 else cases.config1(1, **CPU_SAMPLE)
     Q = sample_query_count(sample)
     t = TiogaLibrary(lib)
     t.init()
@@ -1030,7 +1036,8 @@ def cpu_reference(reps: int, warmup: int = 1):
     t.delete()
     mean = float(np.mean(times))
     return {"value": Q / mean, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": CPU_SAMPLE_TEXT + f" (Q={Q} query points, {reps} timed calls, mean {mean:.2f} s)",
+            "sample": ("the whole cfg0 system, seed 1" if whole_cfg0 else CPU_SAMPLE_TEXT)
+            + f" (Q={Q} query points, {reps} timed calls, mean {mean:.2f} s)",
             "per_step_s": times}, None
 
 
@@ -1176,7 +1183,7 @@ def main():
                               "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                       "d2h_bytes_per_step": 0}}))
             return 0
-        res, why = cpu_reference(args.steps, args.warmup)
+        res, why = cpu_reference(args.steps, args.warmup, whole_cfg0=(args.workload == "cfg0"))
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return 0
@@ -1185,7 +1192,7 @@ def main():
                 "ms_per_step": 1e3 * float(np.mean(res["per_step_s"])), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded mesh generator tioga_b200.cases)",
-                "config": {"workload": WORKLOAD, "sample": res["sample"]},
+                "config": {"workload": WORKLOAD0 if args.workload == "cfg0" else WORKLOAD, "sample": res["sample"]},
                 "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -1237,7 +1244,7 @@ def main():
                     "split form's weight error against FP64 is 0"}
     if rank == 0:
         if ws == 1 and not args.no_cpu_baseline:
-            res, why = cpu_reference(args.cpu_reps)
+            res, why = cpu_reference(args.cpu_reps, whole_cfg0=(args.workload == "cfg0"))
             out["cpu_baseline"] = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                    if res else {"unavailable": why})
             if res and system is not None and args.workload == "cfg1" and args.size == "full" \

@@ -1226,7 +1226,11 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pass64(
 // over 48 KB, so the kernels opt in to the size they are launched with.
 template <class K>
 static void set_smem(K kern, size_t smem) {
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // Above the default 48 KB the limit is raised to the largest a CTA may
+  // have, never set to this launch's size: engines on other host threads
+  // (the server's slots) launch the same kernels, and a smaller limit set
+  // between another thread's call and its launch would fail that launch.
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
@@ -1769,7 +1773,7 @@ __device__ __forceinline__ void record_accept(int q, int c, int cls, unsigned lo
 // 3; FORM 0 decides everything with the reference's FP64 arithmetic.
 // ---------------------------------------------------------------------------
 template <int FORM>
-__global__ void __launch_bounds__(256, 2) k_candidates(
+__global__ void __launch_bounds__(256, FORM == 1 ? 3 : 2) k_candidates(
     const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
     const double* __restrict__ cell_res, const int* __restrict__ sorted_cell, const int* __restrict__ qnode,
     const int2* __restrict__ cand, int ncand, unsigned long long* __restrict__ qkey,
