@@ -50,9 +50,8 @@ WORKLOAD = ("cfg1: 257^3 background (z<0 hexes split into 2 prisms) + 3 spherica
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 # DRAM bytes (read + write) of one k_cell_boxes launch per cell, from an ncu
-# capture on the full workload (profiles/k_cell_boxes_cfg1.md); None until
-# one is made for the current kernel.
-CELL_BOX_DRAM_BYTES_PER_CELL = None
+# capture on the full workload (profiles/k_cell_boxes_cfg1.md).
+CELL_BOX_DRAM_BYTES_PER_CELL = 2443511296 / 26961129  # 90.63 B
 
 
 def cell_box_bytes(system, st):
@@ -106,7 +105,7 @@ def parse():
     p.add_argument("--tuning", default="",
                    help="launch shapes by hand instead of the autotuner, tioga_b200_tuning_'s order: cell-pass "
                         "CTAs/SM, pairs per cell-pass CTA, query CTAs/SM, traversal CTAs/SM, candidate CTAs/SM, "
-                        "cell-box CTAs/SM; e.g. 3,128,16,64,16,6")
+                        "cell-box CTAs/SM, traversal variant + 1 (1: leaves as met, 2: leaves postponed); e.g. 3,128,16,64,16,6,2")
     p.add_argument("--no-forms", action="store_true",
                    help="cfg1: skip the batched (cfg2) and served (cfg3) summaries added to the line")
     p.add_argument("--forms", default="split,plain,e2e,e2e_pageable",
@@ -236,8 +235,8 @@ def pinned_copy(system):
 
 def set_tuning(lib, text: str):
     v = [int(t) for t in text.split(",")]
-    v += [0] * (6 - len(v))
-    lib.lib.tioga_b200_set_tuning_((C.c_int * 6)(*v[:6]))
+    v += [0] * (7 - len(v))
+    lib.lib.tioga_b200_set_tuning_((C.c_int * 7)(*v[:7]))
 
 
 def autotune(lib, tb, reps: int = 2) -> dict:
@@ -254,7 +253,7 @@ def read_tuning(lib) -> dict:
     out = (C.c_int * 8)()
     lib.lib.tioga_b200_tuning_(out)
     keys = ["cell_pass_ctas_per_sm", "pairs_per_cell_pass_cta", "query_ctas_per_sm", "traverse_ctas_per_sm",
-            "candidate_ctas_per_sm", "cell_box_ctas_per_sm"]
+            "candidate_ctas_per_sm", "cell_box_ctas_per_sm", "traverse_variant"]
     return {k: int(out[i]) for i, k in enumerate(keys)}
 
 

@@ -256,11 +256,14 @@ void tioga_b200_server_stats(void *srv, long long out[16]);
 void tioga_b200_autotune_(int *reps);
 /* The shapes in use: [0] cell-pass CTAs per SM, [1] pairs per cell-pass CTA,
  * [2] query CTAs per SM, [3] traversal CTAs per SM, [4] candidate CTAs per SM,
- * [5] CTAs per SM of the split form's cell-box kernel. */
+ * [5] CTAs per SM of the split form's cell-box kernel, [6] the split form's
+ * traversal: 0 walks and tests leaves as it meets them, 1 postpones leaves
+ * until every lane of a warp holds one. */
 void tioga_b200_tuning_(int out[8]);
-/* Set the shapes by hand, in tioga_b200_tuning_'s order [0..5]; values <= 0
- * keep a shape. */
-void tioga_b200_set_tuning_(const int in[6]);
+/* Set the shapes by hand, in tioga_b200_tuning_'s order [0..6]; values <= 0
+ * keep a shape, except [6], which takes the traversal variant plus one (1 or
+ * 2; 0 keeps it). */
+void tioga_b200_set_tuning_(const int in[7]);
 
 /* 0 when the last call succeeded, else a negative code. */
 int tioga_b200_last_error(void);

@@ -250,6 +250,7 @@ def test_autotune_keeps_results():
     t.lib.tioga_b200_tuning_(out)
     assert out[0] in (2, 3, 4) and out[1] in (32, 64, 128) and out[2] in (4, 8, 16, 32, 64)
     assert out[3] in (16, 32, 64, 128) and out[4] in (8, 16, 32, 64)
+    assert out[5] in (4, 6, 8) and out[6] in (0, 1)
     for b in system.blocks:
         ib, (r, i, f) = before[b.tag]
         r2, i2, f2 = t.getdonorinfo(b.tag)
@@ -257,6 +258,31 @@ def test_autotune_keeps_results():
         assert np.array_equal(r, r2) and np.array_equal(i, i2)
         assert np.array_equal(f.view(np.int64), f2.view(np.int64))
     t.delete()
+
+
+@pytest.mark.parametrize("name", ["cfg0", "cfg1-small-seed3"])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_traversal_variants_match_oracle(name, variant, oracle_lib):
+    """Both traversals of the split form (leaves tested as met, and leaves
+    postponed until every lane of a warp holds one) give the oracle's results."""
+    import ctypes as C
+    system = CASES[name]()
+    q = cases.fields(system, nvar=3, seed=17)
+
+    def setup(t):
+        _gpu_setup(1)(t)
+        t.lib.tioga_b200_set_tuning_((C.c_int * 7)(0, 0, 0, 0, 0, 0, variant))
+
+    def variant_in_use(t):
+        out = (C.c_int * 8)()
+        tb.extras(t.lib).tioga_b200_tuning_(out)
+        return out[6]
+
+    ref = run_system(oracle_lib, system, q_blocks=q, nvar=3)
+    gpu = run_system(tb.library_path(), system, q_blocks=q, nvar=3, setup=setup, after=variant_in_use)
+    assert gpu["after"] == variant - 1
+    problems = diff_runs(system, ref, gpu)
+    assert not problems, "\n".join(problems)
 
 
 def _reduce(t):

@@ -350,9 +350,10 @@ void tioga_b200_tuning_(int out[8]) {
   out[3] = t.traverse_per_sm;
   out[4] = t.candidates_per_sm;
   out[5] = t.cell_box_per_sm;
+  out[6] = t.traverse_variant;
 }
 
-void tioga_b200_set_tuning_(const int in[6]) {
+void tioga_b200_set_tuning_(const int in[7]) {
   if (!ready("tioga_b200_set_tuning_")) return;
   set_rc(g_tg->set_tuning(in));
 }

@@ -1233,7 +1233,8 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
-    launch_traverse(form, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq, d_bi_.p, cbox_.p,
+    launch_traverse(form, tune_.traverse_variant, grid_for(nq, 256, 148 * tune_.traverse_per_sm), stream_, xq,
+                    d_bi_.p, cbox_.p,
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p, skip_uhex);
     TB_LAUNCHED("k_traverse");
@@ -1917,6 +1918,7 @@ int Engine::autotune(int reps) {
       {&tune_.chunk_pairs, {32, 64, 128}, &Timing::cell_pass},
       {&tune_.query_per_sm, {4, 8, 16, 32, 64}, &Timing::query},
       {&tune_.cell_box_per_sm, {4, 6, 8}, &Timing::cell_boxes},
+      {&tune_.traverse_variant, {0, 1}, &Timing::traverse},
       {&tune_.traverse_per_sm, {16, 32, 64, 128}, &Timing::traverse},
       {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
   };

@@ -236,6 +236,7 @@ struct Stats {
 struct Tuning {
   int cell_pass_per_sm = 3, query_per_sm = 16, traverse_per_sm = 64, candidates_per_sm = 16, chunk_pairs = 128;
   int cell_box_per_sm = 6;  // split form: CTAs per SM of the box kernel (4, 6 or 8)
+  int traverse_variant = 0; // split form: k_traverse (0) or k_traverse_ww, leaves postponed (1)
 };
 
 struct Timing {
@@ -254,13 +255,14 @@ class Engine {
   // Lowered device bounds for tests of the error paths (0 = the normal
   // bound): which 0 = hole-map fill rounds, 1 = donor-record capacity.
   // launch shapes set by hand (the tuning array's order; values <= 0 keep
-  // the current shape)
-  int set_tuning(const int in[6]) {
+  // the current shape; [6] takes the traversal variant plus one)
+  int set_tuning(const int in[7]) {
     int* v[5] = {&tune_.cell_pass_per_sm, &tune_.chunk_pairs, &tune_.query_per_sm, &tune_.traverse_per_sm,
                  &tune_.candidates_per_sm};
     for (int i = 0; i < 5; i++)
       if (in[i] > 0) *v[i] = in[i];
     if (in[5] > 0) tune_.cell_box_per_sm = in[5];
+    if (in[6] == 1 || in[6] == 2) tune_.traverse_variant = in[6] - 1;
     return 0;
   }
   int set_test_bound(int which, int value) {

@@ -146,7 +146,7 @@ __global__ void k_query_write(const double* x, const BlockInfo* bi, const PairIn
                               const long long* tile_base, const int* node_order);
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
-void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
+void launch_traverse(int form, int variant, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex);

@@ -1736,6 +1736,152 @@ __global__ void __launch_bounds__(256) k_traverse(
   }
 }
 
+// The split form's traversal with postponed leaves: each lane walks its
+// query's tree until it holds a hit leaf or has nothing left, and only when no
+// lane of the warp still walks (every lane holds a leaf or is done) does the
+// warp test the held leaves' cells together; then the walk resumes.  Node
+// visits and leaf tests each run with the lanes that need them side by side,
+// where the walk of k_traverse mixes them within a warp.  The trail keeps,
+// per depth, the hit children (leaves and internal nodes) still to visit;
+// the deepest goes first, so the order is a depth-first one as in
+// k_traverse, and every hit leaf's cells are tested, so each query gets the
+// same candidates (in another order, which the selection does not see).
+__global__ void __launch_bounds__(256) k_traverse_ww(
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
+    const float4* __restrict__ tnode, const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq,
+    int* __restrict__ slots, int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap,
+    unsigned* __restrict__ novf, unsigned* __restrict__ err, int skip_uhex) {
+  __shared__ int s_base[kMaxTreeDepth][256];
+  const int t = threadIdx.x, lane = t & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q0 = blockIdx.x * (long long)blockDim.x + (t & ~31); q0 < nq; q0 += stride) {
+    const long long q = q0 + lane;
+    bool active = q < nq;
+    int root = -1;
+    if (active) {
+      const BlockInfo& B = bi[qdon[q]];
+      root = B.root;
+      if (skip_uhex && B.uhex) {  // searched by k_uhex_search instead
+        ncand_q[q] = 0;
+        active = false;
+      }
+    }
+    int n = 0;
+    float plo[3] = {0.f, 0.f, 0.f}, phi[3] = {0.f, 0.f, 0.f};  // the point widened as in k_traverse
+    if (active) {
+      const int g = qnode[q];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const float p32 = (float)x[3 * (long long)g + k];
+        const float e = fabsf(p32) * 9.6e-7f + 2e-9f;
+        plo[k] = p32 - e;
+        phi[k] = p32 + e;
+      }
+    }
+    int base = -1, depth = 0;             // the next group to visit and its depth
+    unsigned long long tr0 = 0, tr1 = 0;  // hit children still to visit, 4 bits per depth (0-15, 16-31)
+    int lf0 = 0, lfn = 0;                 // the held leaf: first cell, cells
+    if (active && root >= 0) {
+      const float4 RA = tnode[2 * root], RB = tnode[2 * root + 1];
+      const int rlink = __float_as_int(RB.z), rcnt = __float_as_int(RB.w);
+      if (hit_ab(RA, RB, plo, phi)) {
+        if (rcnt > 0) {
+          lf0 = rlink;
+          lfn = rcnt;
+        } else if (rcnt < 0) {
+          base = rlink;
+        }
+      }
+    }
+    for (;;) {
+      for (;;) {  // walk until every lane holds a leaf or is done
+        const bool walk = lfn == 0 && (base >= 0 || (tr0 | tr1) != 0ull);
+        if (!__any_sync(0xffffffffu, walk)) break;
+        if (!walk) continue;
+        if (base < 0) {  // the deepest child still to visit
+          int d2;
+          unsigned mm;
+          if (tr1) {
+            d2 = 16 + ((63 - __clzll((long long)tr1)) >> 2);
+            mm = (unsigned)(tr1 >> (4 * (d2 - 16))) & 0xFu;
+            tr1 &= ~(1ull << (4 * (d2 - 16) + __ffs(mm) - 1));
+          } else {
+            d2 = (63 - __clzll((long long)tr0)) >> 2;
+            mm = (unsigned)(tr0 >> (4 * d2)) & 0xFu;
+            tr0 &= ~(1ull << (4 * d2 + __ffs(mm) - 1));
+          }
+          const long long sl = s_base[d2][t] + __ffs(mm) - 1;
+          const float4 B = tnode[2 * sl + 1];
+          const int lk = __float_as_int(B.z), cnt = __float_as_int(B.w);
+          if (cnt > 0) {
+            lf0 = lk;
+            lfn = cnt;
+          } else if (d2 + 1 < kMaxTreeDepth) {
+            base = lk;
+            depth = d2 + 1;
+          } else {  // deeper than the trail (the build refuses such trees)
+            atomicOr(err, kErrTraversalOverflow);
+            tr0 = tr1 = 0ull;
+          }
+          continue;
+        }
+        int lk[4], lc[4];
+        unsigned h = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const long long sl = base + k;
+          const float4 A = tnode[2 * sl], B = tnode[2 * sl + 1];
+          lk[k] = __float_as_int(B.z);
+          lc[k] = __float_as_int(B.w);
+          if (hit_ab(A, B, plo, phi)) h |= 1u << k;
+        }
+        const int gbase = base;
+        base = -1;
+        if (h) {
+          const int k = __ffs(h) - 1;
+          h &= h - 1;
+          if (h) {
+            if (depth < 16) tr0 |= (unsigned long long)h << (4 * depth);
+            else tr1 |= (unsigned long long)h << (4 * (depth - 16));
+            s_base[depth][t] = gbase;
+          }
+          const int ck = pick4(k, lk[0], lk[1], lk[2], lk[3]), cc = pick4(k, lc[0], lc[1], lc[2], lc[3]);
+          if (cc > 0) {
+            lf0 = ck;
+            lfn = cc;
+          } else if (depth + 1 < kMaxTreeDepth) {
+            base = ck;
+            depth++;
+          } else {  // deeper than the trail (the build refuses such trees)
+            atomicOr(err, kErrTraversalOverflow);
+            tr0 = tr1 = 0ull;
+          }
+        }
+      }
+      if (lfn > 0) {  // the held leaves, side by side: all box loads first, then the tests
+        float4 A[kMaxLeafCells], B[kMaxLeafCells];
+#pragma unroll
+        for (int j = 0; j < kMaxLeafCells; j++) {
+          const long long c = lf0 + min(j, lfn - 1);
+          A[j] = cbox[2 * c];
+          B[j] = cbox[2 * c + 1];
+        }
+        unsigned hit = 0;
+#pragma unroll
+        for (int j = 0; j < kMaxLeafCells; j++) hit |= (unsigned)(hit_ab(A[j], B[j], plo, phi) && j < lfn) << j;
+        while (hit) {
+          const int j = __ffs(hit) - 1;
+          hit &= hit - 1;
+          add_candidate((int)q, lf0 + j, n, slots, ovf, ovf_cap, novf);
+        }
+        lfn = 0;
+      }
+      if (!__any_sync(0xffffffffu, base >= 0 || (tr0 | tr1) != 0ull)) break;
+    }
+    if (active) ncand_q[q] = n;
+  }
+}
+
 // Dense, query-ordered candidate list from the slots and the overflow list
 // (off = exclusive scan of the per-query counts).
 __global__ void k_gather_candidates(const int* __restrict__ slots, const int* __restrict__ ncand_q,
@@ -1894,11 +2040,14 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
   }
 }
 
-void launch_traverse(int form, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
+void launch_traverse(int form, int variant, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
                      const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex) {
-  if (form == 0)
+  if (form == 1 && variant == 1)
+    k_traverse_ww<<<blocks, 256, 0, st>>>(x, bi, cbox, tnode, qnode, qdon, nq, slots, ncand_q, ovf, ovf_cap, novf,
+                                          err, skip_uhex);
+  else if (form == 0)
     k_traverse<0><<<blocks, 256, 0, st>>>(x, bi, cbox, cbox64, tnode, tnode64, qnode, qdon, nq, slots, ncand_q,
                                           ovf, ovf_cap, novf, err, skip_uhex);
   else
