@@ -32,6 +32,8 @@ Engine::Engine() {
   for (auto& e : sev_) cudaEventCreate(&e);
   for (auto& e : cev_) cudaEventCreate(&e);
   cudaEventCreateWithFlags(&pev_, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
+  for (auto& e : hev_) cudaEventCreate(&e);
 }
 
 Engine::~Engine() {
@@ -42,6 +44,12 @@ Engine::~Engine() {
   for (auto& e : sev_) cudaEventDestroy(e);
   for (auto& e : cev_) cudaEventDestroy(e);
   cudaEventDestroy(pev_);
+  if (side_) cudaStreamSynchronize(side_);
+  for (auto& e : hev_) cudaEventDestroy(e);
+  if (side_) cudaStreamDestroy(side_);
+  if (h_hm_init_) cudaFreeHost(h_hm_init_);
+  if (h_hm_info_) cudaFreeHost(h_hm_info_);
+  if (h_hm_dev_) cudaFreeHost(h_hm_dev_);
   x_.release(); node_res_.release(); cell_res_.release(); iblank_.release(); iblank_cell_.release();
   conn8_.release(); node_blk_.release(); cell_blk_.release(); cell_nv_.release(); wallf_.release();
   obcf_.release(); ex0_.release(); ex1_.release(); m0_.release(); m1_.release(); cmark_.release();
@@ -53,7 +61,7 @@ Engine::~Engine() {
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
-  qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); slot_.release();
+  qtie_.release(); qcount_.release(); tile_cnt_.release(); tile_off_.release(); tile_mask_.release(); slot_.release();
   rkey_.release(); rkey_alt_.release(); rval_.release(); rval_alt_.release(); rcount_.release();
   reset_t_.release(); interp2rec_.release(); it_node_.release(); it_w_.release(); it_rec_.release();
   it_don_.release(); it_nv_.release(); it_cancel_.release(); rres_.release(); q_.release();
@@ -896,45 +904,77 @@ int Engine::preprocess_resolutions() {
 // ---------------------------------------------------------------------------
 // connectivity (src/tioga.C:112-160)
 // ---------------------------------------------------------------------------
-int Engine::run_holemaps() {
-  // every wall-bearing block's map at once: wall bounds -> extents and sizes
-  // -> mark -> fill -> final
+// Every wall-bearing block's map at once: wall bounds -> extents and sizes
+// -> mark -> fill -> final, on the side stream after hev_[0].  The first
+// half ends with the maps' extents copied to pinned host memory (hev_[1]);
+// holemaps_end reads them once the main stream's work is queued.
+int Engine::holemaps_begin() {
+  TB_CUDA(cudaStreamSynchronize(side_));  // idle unless the last call stopped early: the staging is reused
   const int nh = nhm_all_;
   nhm_ = 0;
+  hm_pending_ = false;
   if (nh == 0) return 0;
-  std::vector<unsigned long long> init(6 * (size_t)nh);
+  if (h_hm_cap_ < nh) {
+    if (h_hm_init_) cudaFreeHost(h_hm_init_);
+    if (h_hm_info_) cudaFreeHost(h_hm_info_);
+    if (h_hm_dev_) cudaFreeHost(h_hm_dev_);
+    h_hm_init_ = nullptr;
+    h_hm_info_ = nullptr;
+    h_hm_dev_ = nullptr;
+    h_hm_cap_ = 0;
+    TB_CUDA(cudaMallocHost(&h_hm_init_, 6 * (size_t)nh * sizeof(unsigned long long)));
+    TB_CUDA(cudaMallocHost(&h_hm_info_, (size_t)nh * sizeof(HoleMapInfo)));
+    TB_CUDA(cudaMallocHost(&h_hm_dev_, (size_t)nh * sizeof(HoleMapDev)));
+    h_hm_cap_ = nh;
+  }
+  cudaStream_t hs = side_;
+  TB_CUDA(cudaStreamWaitEvent(hs, hev_[0], 0));
   for (int t = 0; t < nh; t++)
     for (int j = 0; j < 3; j++) {  // identity elements of min (all ones) and max (zero) over ordered keys
-      init[6 * t + j] = ~0ull;
-      init[6 * t + j + 3] = 0ull;
+      h_hm_init_[6 * t + j] = ~0ull;
+      h_hm_init_[6 * t + j + 3] = 0ull;
     }
-  TB_CUDA(cudaMemcpyAsync(wall_bb_.p, init.data(), init.size() * sizeof(unsigned long long),
-                          cudaMemcpyHostToDevice, stream_));
+  TB_CUDA(cudaMemcpyAsync(wall_bb_.p, h_hm_init_, 6 * (size_t)nh * sizeof(unsigned long long),
+                          cudaMemcpyHostToDevice, hs));
   const unsigned nw = (unsigned)h_wall_.size();
   int maxw = 1;
   for (const WallBlock& W : h_wall_) maxw = std::max(maxw, W.nwall);
-  k_wall_bounds<<<dim3(grid_for(maxw, kT, 148), nw), kT, 0, stream_>>>(x_.p, wall_list_.p, d_wall_.p, wall_bb_.p);
-  TB_LAUNCHED("k_wall_bounds");
-  k_holemap_setup<<<(nh + 127) / 128, 128, 0, stream_>>>(wall_bb_.p, d_hm_.p, nh);
-  TB_LAUNCHED("k_holemap_setup");
+  k_wall_bounds<<<dim3(grid_for(maxw, kT, 148), nw), kT, 0, hs>>>(x_.p, wall_list_.p, d_wall_.p, wall_bb_.p);
+  TB_LAUNCHED_ON("k_wall_bounds", hs);
+  k_holemap_setup<<<(nh + 127) / 128, 128, 0, hs>>>(wall_bb_.p, d_hm_.p, nh);
+  TB_LAUNCHED_ON("k_holemap_setup", hs);
   const bool planar = (isym_ == 1 || isym_ == 2 || isym_ == 3);
   // the plane fill rewrites every cell of its map, so only this call's marks
   // (2) count there; the 6-neighbour fill reads the map as it is
-  if (!planar) TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nh * kHoleMapCap, stream_));
+  if (!planar) TB_CUDA(cudaMemsetAsync(hm_state_.p, 0, (size_t)nh * kHoleMapCap, hs));
   if (nwall_cells_ > 0 && planar) {  // the boxes the plane fill marks in shared memory
-    k_holemap_boxes<<<grid_for(nwall_cells_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
-                                                                    nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
-                                                                    wall_box_.p);
-    TB_LAUNCHED("k_holemap_boxes");
+    k_holemap_boxes<<<grid_for(nwall_cells_, kT), kT, 0, hs>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
+                                                               nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
+                                                               wall_box_.p);
+    TB_LAUNCHED_ON("k_holemap_boxes", hs);
   } else if (nwall_cells_ > 0) {
-    k_holemap_mark<<<grid_for(nwall_cells_, kT), kT, 0, stream_>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
-                                                                   nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
-                                                                   hm_state_.p, kHoleMapCap);
-    TB_LAUNCHED("k_holemap_mark");
+    k_holemap_mark<<<grid_for(nwall_cells_, kT), kT, 0, hs>>>(x_.p, conn8_.p, cell_nv_.p, wall_cells_.p,
+                                                              nwall_cells_, cell_blk_.p, d_bi_.p, d_hm_.p,
+                                                              hm_state_.p, kHoleMapCap);
+    TB_LAUNCHED_ON("k_holemap_mark", hs);
   }
-  std::vector<HoleMapInfo> hinfo(nh);
-  TB_CUDA(cudaMemcpyAsync(hinfo.data(), d_hm_.p, nh * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
+  TB_CUDA(cudaMemcpyAsync(h_hm_info_, d_hm_.p, nh * sizeof(HoleMapInfo), cudaMemcpyDeviceToHost, hs));
+  TB_CUDA(cudaEventRecord(hev_[1], hs));
+  hm_pending_ = true;
+  return 0;
+}
+
+int Engine::holemaps_end() {
+  const int nh = nhm_all_;
+  if (!hm_pending_) {  // no maps: the donor phase's wait on hev_[2] passes at once
+    TB_CUDA(cudaEventRecord(hev_[2], side_));
+    return 0;
+  }
+  hm_pending_ = false;
+  cudaStream_t hs = side_;
+  TB_CUDA(cudaEventSynchronize(hev_[1]));
+  const HoleMapInfo* hinfo = h_hm_info_;
+  const bool planar = (isym_ == 1 || isym_ == 2 || isym_ == 3);
   const int isym = isym_;
   const int pa = (isym == 1) ? 0 : (isym == 2) ? 1 : 2;
   const int a0 = (pa == 0) ? 1 : 0, a1 = (pa == 2) ? 1 : 2;
@@ -945,6 +985,7 @@ int Engine::run_holemaps() {
     const HoleMapInfo& h = hinfo[t];
     if (h.nx[0] > 197 || h.nx[1] > 197 || h.nx[2] > 197 || h.nx[0] < 1 || h.nx[1] < 1 || h.nx[2] < 1) {
       fprintf(stderr, "#tioga_b200: hole map %d has an unexpected size\n", t);
+      TB_CUDA(cudaEventRecord(hev_[2], hs));
       return -1;
     }
     maxpl = std::max(maxpl, h.nx[pa]);
@@ -953,44 +994,45 @@ int Engine::run_holemaps() {
     stats_.holemap_cells += (long long)h.nx[0] * h.nx[1] * h.nx[2];
   }
   if (planar) {  // fill and final map in one pass
-    k_holemap_fill_bits<<<dim3(std::min(maxpl, 148 * 4), nh), 256, 0, stream_>>>(
+    k_holemap_fill_bits<<<dim3(std::min(maxpl, 148 * 4), nh), 256, 0, hs>>>(
         hm_state_.p, d_hm_.p, kHoleMapCap, wall_box_.p, wall_box_first_.p, isym, test_fill_rounds_, err_.p);
-    TB_LAUNCHED("k_holemap_fill_bits");
+    TB_LAUNCHED_ON("k_holemap_fill_bits", hs);
   } else {
-    k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, stream_>>>(hm_state_.p, d_hm_.p,
-                                                                                     kHoleMapCap, 3, 1, err_.p);
-    TB_LAUNCHED("k_holemap_fill_planes");  // 6-neighbour fill: line sweeps over the three axes until no map changes
+    k_holemap_fill_planes<<<dim3(std::min(maxpl, 148 * 4), nh), 256, smem, hs>>>(hm_state_.p, d_hm_.p,
+                                                                                kHoleMapCap, 3, 1, err_.p);
+    TB_LAUNCHED_ON("k_holemap_fill_planes", hs);  // 6-neighbour fill: line sweeps over the three axes until no map changes
     unsigned* d_changed = err_.p + 1;
     int maxsum = 0;
-    for (const HoleMapInfo& h : hinfo) maxsum = std::max(maxsum, h.nx[0] + h.nx[1] + h.nx[2]);
+    for (int t = 0; t < nh; t++) maxsum = std::max(maxsum, hinfo[t].nx[0] + hinfo[t].nx[1] + hinfo[t].nx[2]);
     for (int round = 0; round < 4 * maxsum; round++) {
-      TB_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(unsigned), stream_));
+      TB_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(unsigned), hs));
       for (int axis = 0; axis < 3; axis++) {
-        k_holemap_lines<<<dim3(grid_for(maxcells / 64 + 1, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p,
-                                                                                      kHoleMapCap, axis, d_changed);
-        TB_LAUNCHED("k_holemap_lines");
+        k_holemap_lines<<<dim3(grid_for(maxcells / 64 + 1, kT), nh), kT, 0, hs>>>(hm_state_.p, d_hm_.p,
+                                                                                 kHoleMapCap, axis, d_changed);
+        TB_LAUNCHED_ON("k_holemap_lines", hs);
       }
       unsigned ch = 0;
-      TB_CUDA(cudaMemcpyAsync(&ch, d_changed, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-      TB_CUDA(cudaStreamSynchronize(stream_));
+      TB_CUDA(cudaMemcpyAsync(&ch, d_changed, sizeof(unsigned), cudaMemcpyDeviceToHost, hs));
+      TB_CUDA(cudaStreamSynchronize(hs));
       if (!ch) break;
     }
-    k_holemap_final<<<dim3(grid_for(maxcells, kT), nh), kT, 0, stream_>>>(hm_state_.p, d_hm_.p, kHoleMapCap);
-    TB_LAUNCHED("k_holemap_final");
+    k_holemap_final<<<dim3(grid_for(maxcells, kT), nh), kT, 0, hs>>>(hm_state_.p, d_hm_.p, kHoleMapCap);
+    TB_LAUNCHED_ON("k_holemap_final", hs);
   }
-  std::vector<HoleMapDev> hdev(nh);
   for (int b = 0; b < (int)bi_.size(); b++) {
     const int t = bi_[b].hm;
     if (t < 0) continue;
-    HoleMapDev& d = hdev[t];
+    HoleMapDev& d = h_hm_dev_[t];
     d.tagidx = bi_[b].tag - 1;
     for (int j = 0; j < 3; j++) d.nx[j] = hinfo[t].nx[j];
     for (int j = 0; j < 6; j++) d.ext[j] = hinfo[t].ext[j];
     d.hole = hm_state_.p + (size_t)t * kHoleMapCap;
   }
   nhm_ = nh;
-  TB_CUDA(cudaMemcpyAsync(d_hmdev_.p, hdev.data(), nh * sizeof(HoleMapDev), cudaMemcpyHostToDevice, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));  // host tables go out of scope
+  // pinned source: the copy does not hold the host; the buffer is next
+  // written by the next call, after this call's final synchronisation
+  TB_CUDA(cudaMemcpyAsync(d_hmdev_.p, h_hm_dev_, nh * sizeof(HoleMapDev), cudaMemcpyHostToDevice, hs));
+  TB_CUDA(cudaEventRecord(hev_[2], hs));
   return 0;
 }
 
@@ -1138,8 +1180,9 @@ int Engine::run_queries() {
   TB_CUDA(tile_off_.ensure(ntiles + 1));
   TB_CUDA(cudaMemsetAsync(tile_cnt_.p, 0, (ntiles + 1) * sizeof(int), stream_));
   const unsigned grid = (unsigned)std::max(1ll, std::min(ntiles, 148ll * tune_.query_per_sm));
+  TB_CUDA(tile_mask_.ensure(ntiles * 256));  // per tile and thread: which of its 8 nodes are inside
   k_query_count<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_cnt_.p,
-                                           tbox_.p, tile_base_.p, node_order_.p);
+                                           tbox_.p, tile_base_.p, node_order_.p, tile_mask_.p);
   TB_LAUNCHED("k_query_count");
   size_t tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp, tile_cnt_.p, tile_off_.p, (int)(ntiles + 1), stream_);
@@ -1156,9 +1199,8 @@ int Engine::run_queries() {
   TB_CUDA(qtie_.ensure(nq));
   TB_CUDA(interp2rec_.ensure(nq));
   if (nq > 0) {
-    k_query_write<<<grid, 256, 0, stream_>>>(x_.p, d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_off_.p,
-                                             node_res_.p, qnode_.p, qdon_.p, qres_.p, tbox_.p, tile_base_.p,
-                                             node_order_.p);
+    k_query_write<<<grid, 256, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, d_pair_t0_.p, tile, tile_off_.p,
+                                             node_res_.p, qnode_.p, qdon_.p, qres_.p, node_order_.p, tile_mask_.p);
     TB_LAUNCHED("k_query_write");
   }
   dedup_ran_ = false;
@@ -1958,10 +2000,15 @@ int Engine::connectivity() {
   TB_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), stream_));  // this call's device errors only
   if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
-  int rc = run_holemaps();
+  // the hole maps start on the side stream; their second half is queued once
+  // the cell pass is, and the donor phase waits for them
+  TB_CUDA(cudaEventRecord(hev_[0], stream_));
+  int rc = holemaps_begin();
   if (rc) return rc;
   TB_CUDA(cudaEventRecord(ev_[2], stream_));
   rc = run_pairs_and_refit();
+  if (rc) return rc;
+  rc = holemaps_end();
   if (rc) return rc;
   TB_CUDA(cudaEventRecord(ev_[3], stream_));
   nq_ = 0;
@@ -1976,6 +2023,7 @@ int Engine::connectivity() {
     TB_CUDA(cudaEventRecord(ev_[4], stream_));
   }
   TB_CUDA(cudaEventRecord(ev_[5], stream_));
+  TB_CUDA(cudaStreamWaitEvent(stream_, hev_[2], 0));
   rc = run_donors();
   if (rc) return rc;
   TB_CUDA(cudaEventRecord(ev_[6], stream_));
@@ -2008,7 +2056,8 @@ int Engine::connectivity() {
   float ms[9];
   for (int i = 1; i < 9; i++) cudaEventElapsedTime(&ms[i], ev_[i - 1], ev_[i]);
   timing_.upload = ms[1];
-  timing_.holemap = ms[2];
+  timing_.holemap = 0;  // on the side stream, beside the cell pass and the search
+  cudaEventElapsedTime(&timing_.holemap, hev_[0], hev_[2]);
   timing_.boxes = ms[3];
   timing_.query = ms[4];
   timing_.search = ms[5];

@@ -355,7 +355,8 @@ class Engine {
   int build_tree_topology();
   int upload_coords();
   int check_coords();
-  int run_holemaps();
+  int holemaps_begin();    // side stream: wall bounds, map extents, wall-cell boxes, extents to the host
+  int holemaps_end();      // host: map sizes; side stream: fill and final maps (joined before the donors)
   int preprocess_resolutions();
   int run_pairs_and_refit();
   int setup_uniform_hex();
@@ -423,6 +424,19 @@ class Engine {
   cudaStream_t own_stream_ = nullptr;
   long long nlaunch_ = 0;
   cudaEvent_t ev_[12];
+  // The hole maps run on a stream of their own beside the cell pass, the
+  // query gathering and the search, and join before the donor phase:
+  // hev_[0] = the coordinates are on the device (main stream), [1] = the
+  // maps' extents are on the host, [2] = the maps are done (side stream).
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t hev_[3];
+  bool hm_pending_ = false;  // holemaps_begin ran and holemaps_end has not
+  // pinned host staging of the hole maps (so the side stream's copies never
+  // block the host): ordered-key initial bounds, extents read back, map views
+  unsigned long long* h_hm_init_ = nullptr;
+  HoleMapInfo* h_hm_info_ = nullptr;
+  HoleMapDev* h_hm_dev_ = nullptr;
+  int h_hm_cap_ = 0;
   cudaEvent_t sev_[4];
   cudaEvent_t cev_[3];  // around the cell pass (split form: and between its two kernels)
   cudaEvent_t pev_;     // the pairs' copy to the host has landed
@@ -512,6 +526,7 @@ class Engine {
   DBuf<unsigned char> qtie_;
   DBuf<int> qcount_;
   DBuf<int> tile_cnt_, tile_off_;
+  DBuf<unsigned char> tile_mask_;  // query gathering: per node tile and thread, its 8 nodes' region test
   long long qcap_ = 0;
   // donors
   DBuf<int> slot_;          // K per node

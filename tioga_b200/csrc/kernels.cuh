@@ -139,11 +139,10 @@ __global__ void k_remap(int* idx, long long n, const int* map);
 __global__ void k_scatter_f64(const double* src, long long n, const int* inv, long long base, double* dst);
 __global__ void k_query_count(const double* x, const BlockInfo* bi, const PairInfo* pairs, int npairs,
                               const long long* pair_t0, int tile, int* tile_cnt, const float4* tbox,
-                              const long long* tile_base, const int* node_order);
-__global__ void k_query_write(const double* x, const BlockInfo* bi, const PairInfo* pairs, int npairs,
-                              const long long* pair_t0, int tile, const int* tile_off, const double* node_res,
-                              int* qnode, int* qdon, double* qres, const float4* tbox,
-                              const long long* tile_base, const int* node_order);
+                              const long long* tile_base, const int* node_order, unsigned char* tile_mask);
+__global__ void k_query_write(const BlockInfo* bi, const PairInfo* pairs, int npairs, const long long* pair_t0,
+                              int tile, const int* tile_off, const double* node_res, int* qnode, int* qdon,
+                              double* qres, const int* node_order, const unsigned char* tile_mask);
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
 void launch_traverse(int form, int variant, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,

@@ -1367,7 +1367,8 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
                                                            int* __restrict__ tile_cnt,
                                                            const float4* __restrict__ tbox,
                                                            const long long* __restrict__ tile_base,
-                                                           const int* __restrict__ node_order) {
+                                                           const int* __restrict__ node_order,
+                                                           unsigned char* __restrict__ tile_mask) {
   __shared__ int sh[kQThreads / 32];
   const long long ntiles = pair_t0[npairs];
   for (long long T = blockIdx.x; T < ntiles; T += gridDim.x) {
@@ -1381,12 +1382,13 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
       continue;
     }
     const Obb reg = P.region;
-    int cnt = 0;
+    unsigned mask = 0;
     for (int k = 0; k < kQItems; k++) {
       int i = n0 + threadIdx.x * kQItems + k;
-      if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) cnt++;
+      if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) mask |= 1u << k;
     }
-    int w = cnt;
+    tile_mask[T * kQThreads + threadIdx.x] = (unsigned char)mask;  // for k_query_write
+    int w = __popc(mask);
     for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = w;
     __syncthreads();
@@ -1399,38 +1401,28 @@ __global__ void __launch_bounds__(kQThreads) k_query_count(const double* __restr
   }
 }
 
-__global__ void __launch_bounds__(kQThreads) k_query_write(const double* __restrict__ x,
-                                                           const BlockInfo* __restrict__ bi,
+__global__ void __launch_bounds__(kQThreads) k_query_write(const BlockInfo* __restrict__ bi,
                                                            const PairInfo* __restrict__ pairs, int npairs,
                                                            const long long* __restrict__ pair_t0, int tile,
                                                            const int* __restrict__ tile_off,
                                                            const double* __restrict__ node_res,
                                                            int* __restrict__ qnode, int* __restrict__ qdon,
-                                                           double* __restrict__ qres, const float4* __restrict__ tbox,
-                                                           const long long* __restrict__ tile_base,
-                                                           const int* __restrict__ node_order) {
+                                                           double* __restrict__ qres,
+                                                           const int* __restrict__ node_order,
+                                                           const unsigned char* __restrict__ tile_mask) {
   typedef cub::BlockScan<int, kQThreads> Scan;
   __shared__ typename Scan::TempStorage tmp;
   const long long ntiles = pair_t0[npairs];
   for (long long T = blockIdx.x; T < ntiles; T += gridDim.x) {
+    if (tile_off[T + 1] == tile_off[T]) continue;  // culled, or no node inside
     const int p = pair_of_tile(pair_t0, npairs, T);
     const int t = (int)(T - pair_t0[p]);
     const PairInfo& P = pairs[p];
     const BlockInfo& R = bi[P.rec];
     const int n0 = t * tile;
-    if (!tile_may_hit(tbox, tile_base[P.rec] + t, P)) continue;
-    const Obb reg = P.region;
-    unsigned mask = 0;
-    int cnt = 0;
-    for (int k = 0; k < kQItems; k++) {
-      int i = n0 + threadIdx.x * kQItems + k;
-      if (i < R.nnodes && in_region(x + 3 * (long long)node_order[R.node_off + i], reg)) {
-        mask |= 1u << k;
-        cnt++;
-      }
-    }
+    const unsigned mask = tile_mask[T * kQThreads + threadIdx.x];  // k_query_count's test
     int pos;
-    Scan(tmp).ExclusiveSum(cnt, pos);
+    Scan(tmp).ExclusiveSum(__popc(mask), pos);
     long long o = (long long)tile_off[T] + pos;
     for (int k = 0; k < kQItems; k++) {
       if (mask & (1u << k)) {

@@ -465,14 +465,14 @@ __global__ void k_cell_iblank_sparse(const int* __restrict__ mlist, const int* _
                                      const unsigned char* __restrict__ cell_nv, const int* __restrict__ iblank,
                                      int* __restrict__ iblank_cell) {
   const int nh = dcnt[kHoles], R = *rcount;
-  const int lane = threadIdx.x & 31;  // a warp per node, its lanes over the node's cells
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nh + R; i += nw) {
+  const int sub = threadIdx.x & 7;  // eight lanes per node (a hexahedral node has eight cells) over its cells
+  const int ng = (gridDim.x * blockDim.x) >> 3;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < nh + R; i += ng) {
     int v;
     if (i < nh) v = mlist[i];
     else if (!it_cancel[i - nh]) v = it_rec[i - nh];
     else continue;
-    for (int k = csr_off[v] + lane; k < csr_off[v + 1]; k += 32) {
+    for (int k = csr_off[v] + sub; k < csr_off[v + 1]; k += 8) {
       const int c = csr_cell[k];
       iblank_cell[c] = cell_iblank_of(conn8, cell_nv, iblank, c);
     }
