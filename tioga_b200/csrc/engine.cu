@@ -34,6 +34,7 @@ Engine::Engine() {
   cudaEventCreateWithFlags(&pev_, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
   for (auto& e : hev_) cudaEventCreate(&e);
+  for (auto& e : cib_ev_) cudaEventCreate(&e);
 }
 
 Engine::~Engine() {
@@ -46,6 +47,7 @@ Engine::~Engine() {
   cudaEventDestroy(pev_);
   if (side_) cudaStreamSynchronize(side_);
   for (auto& e : hev_) cudaEventDestroy(e);
+  for (auto& e : cib_ev_) cudaEventDestroy(e);
   if (side_) cudaStreamDestroy(side_);
   if (h_hm_init_) cudaFreeHost(h_hm_init_);
   if (h_hm_info_) cudaFreeHost(h_hm_info_);
@@ -1138,12 +1140,14 @@ int Engine::run_pairs_and_refit() {
                        leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p,
                        cbox64_.p, tnode_.p, tnode64_.p, pair_acc_.p);
     TB_CUDA(cudaEventRecord(cev_[2], stream_));
+    TB_CUDA(cudaEventRecord(hev_[0], stream_));  // the hole maps may start
   } else {
     const int mb = tune_.cell_box_per_sm;
     TB_CUDA(lbox_.ensure(2 * nleaf_total_));
     launch_cell_boxes(mb, (int)grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p,
                       cell_nv_.p, leaves_.p, nleaf_total_, cbox_.p, tnode_.p, lbox_.p);
     TB_LAUNCHED("k_cell_boxes");
+    TB_CUDA(cudaEventRecord(hev_[0], stream_));  // the hole maps may start
     TB_CUDA(cudaEventRecord(cev_[2], stream_));
     launch_cell_pairs(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
                       leaves_.p, d_chunks_.p, d_chunk_cta_.p, (int)chunks.size(), d_pfirst_.p, d_pairs_.p, cbox_.p,
@@ -1915,11 +1919,16 @@ int Engine::reduce_fringes() {
 }
 
 int Engine::run_celliblank() {
-  // cells around the holes and the final receptors (all others are 1)
-  k_cell_iblank_sparse<<<148 * 16, kT, 0, stream_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p, rcount_.p,
-                                                    csr_off_.p, csr_cell_.p, conn8_.p, cell_nv_.p, iblank_.p,
-                                                    iblank_cell_.p);
-  TB_LAUNCHED("k_cell_iblank_sparse");
+  // cells around the holes and the final receptors (all others are 1), on
+  // the side stream while the main stream copies the node iblanks out;
+  // download_iblank waits for them before it copies the cell iblanks
+  TB_CUDA(cudaEventRecord(cib_ev_[0], stream_));
+  TB_CUDA(cudaStreamWaitEvent(side_, cib_ev_[0], 0));
+  k_cell_iblank_sparse<<<148 * 16, kT, 0, side_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p, rcount_.p,
+                                                  csr_off_.p, csr_cell_.p, conn8_.p, cell_nv_.p, iblank_.p,
+                                                  iblank_cell_.p);
+  TB_LAUNCHED_ON("k_cell_iblank_sparse", side_);
+  TB_CUDA(cudaEventRecord(cib_ev_[1], side_));
   return 0;
 }
 
@@ -1931,6 +1940,9 @@ int Engine::download_iblank() {
     else
       TB_CUDA(cudaMemcpyAsync(hb_[b].hibl, iblank_.p + bi_[b].node_off, hb_[b].nnodes * sizeof(int),
                               cudaMemcpyDeviceToHost, stream_));
+  }
+  TB_CUDA(cudaStreamWaitEvent(stream_, cib_ev_[1], 0));  // the cell iblanks (run_celliblank, side stream)
+  for (size_t b = 0; b < hb_.size(); b++) {
     if (hb_[b].h_iblank_cell) {
       TB_CUDA(cell_stage_.ensure(hb_[b].ncells));
       k_gather_cells_i32<<<grid_for(hb_[b].ncells, kT), kT, 0, stream_>>>(iblank_cell_.p, inv_sorted_.p,
@@ -2000,13 +2012,14 @@ int Engine::connectivity() {
   TB_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), stream_));  // this call's device errors only
   if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
-  // the hole maps start on the side stream; their second half is queued once
-  // the cell pass is, and the donor phase waits for them
+  // The hole maps run on the side stream after the cell boxes (hev_[0],
+  // recorded again after the box kernel), beside the latency-bound pair,
+  // query and search kernels; the donor phase waits for them.
   TB_CUDA(cudaEventRecord(hev_[0], stream_));
-  int rc = holemaps_begin();
-  if (rc) return rc;
   TB_CUDA(cudaEventRecord(ev_[2], stream_));
-  rc = run_pairs_and_refit();
+  int rc = run_pairs_and_refit();
+  if (rc) return rc;
+  rc = holemaps_begin();
   if (rc) return rc;
   rc = holemaps_end();
   if (rc) return rc;
@@ -2062,7 +2075,8 @@ int Engine::connectivity() {
   timing_.query = ms[4];
   timing_.search = ms[5];
   timing_.donors = ms[6];
-  timing_.celliblank = ms[7];
+  timing_.celliblank = 0;  // on the side stream, beside the node iblanks' copies
+  cudaEventElapsedTime(&timing_.celliblank, cib_ev_[0], cib_ev_[1]);
   timing_.download = ms[8];
   cudaEventElapsedTime(&timing_.total, ev_[0], ev_[8]);
   timing_.traverse = timing_.candidates = timing_.refine = 0;

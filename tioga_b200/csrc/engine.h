@@ -430,6 +430,7 @@ class Engine {
   // maps' extents are on the host, [2] = the maps are done (side stream).
   cudaStream_t side_ = nullptr;
   cudaEvent_t hev_[3];
+  cudaEvent_t cib_ev_[2];  // the cell iblanks on the side stream: start (main), done (side)
   bool hm_pending_ = false;  // holemaps_begin ran and holemaps_end has not
   // pinned host staging of the hole maps (so the side stream's copies never
   // block the host): ordered-key initial bounds, extents read back, map views
