@@ -35,6 +35,8 @@ Engine::Engine() {
   cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
   for (auto& e : hev_) cudaEventCreate(&e);
   for (auto& e : cib_ev_) cudaEventCreate(&e);
+  cudaEventCreateWithFlags(&dr_ev_, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&rf_ev_, cudaEventDisableTiming);
 }
 
 Engine::~Engine() {
@@ -48,6 +50,8 @@ Engine::~Engine() {
   if (side_) cudaStreamSynchronize(side_);
   for (auto& e : hev_) cudaEventDestroy(e);
   for (auto& e : cib_ev_) cudaEventDestroy(e);
+  cudaEventDestroy(dr_ev_);
+  cudaEventDestroy(rf_ev_);
   if (side_) cudaStreamDestroy(side_);
   if (h_hm_init_) cudaFreeHost(h_hm_init_);
   if (h_hm_info_) cudaFreeHost(h_hm_info_);
@@ -911,7 +915,6 @@ int Engine::preprocess_resolutions() {
 // half ends with the maps' extents copied to pinned host memory (hev_[1]);
 // holemaps_end reads them once the main stream's work is queued.
 int Engine::holemaps_begin() {
-  TB_CUDA(cudaStreamSynchronize(side_));  // idle unless the last call stopped early: the staging is reused
   const int nh = nhm_all_;
   nhm_ = 0;
   hm_pending_ = false;
@@ -1157,13 +1160,17 @@ int Engine::run_pairs_and_refit() {
   TB_LAUNCHED("k_cell_pass");
   TB_CUDA(cudaEventRecord(cev_[1], stream_));
   cell_timed_ = true;
-  if (nrefit_start_ > 0) {  // internal nodes from the leaves the cell pass wrote, in one launch
-    TB_CUDA(cudaMemsetAsync(refit_cnt_.p, 0, (tree_nodes_ / 4) * sizeof(int), stream_));
-    k_refit_fused<<<grid_for(nrefit_start_, kT), kT, 0, stream_>>>(refit_start_.p, nrefit_start_, gparent_.p,
-                                                                   gnint_.p, (int)hb_.size(), refit_cnt_.p, tnode_.p,
-                                                                   fp64 ? tnode64_.p : nullptr);
-    TB_LAUNCHED("k_refit_fused");
+  // internal nodes from the leaves the cell pass wrote, in one launch on the
+  // side stream: only the traversal reads them (it waits for rf_ev_)
+  TB_CUDA(cudaStreamWaitEvent(side_, hev_[0], 0));
+  if (nrefit_start_ > 0) {
+    TB_CUDA(cudaMemsetAsync(refit_cnt_.p, 0, (tree_nodes_ / 4) * sizeof(int), side_));
+    k_refit_fused<<<grid_for(nrefit_start_, kT), kT, 0, side_>>>(refit_start_.p, nrefit_start_, gparent_.p,
+                                                                 gnint_.p, (int)hb_.size(), refit_cnt_.p, tnode_.p,
+                                                                 fp64 ? tnode64_.p : nullptr);
+    TB_LAUNCHED_ON("k_refit_fused", side_);
   }
+  TB_CUDA(cudaEventRecord(rf_ev_, side_));
   k_pair_finish<<<(npairs_ + 63) / 64, 64, 0, stream_>>>(d_bi_.p, d_pairs_.p, npairs_, pair_acc_.p);
   TB_LAUNCHED("k_pair_finish");
   return 0;
@@ -1669,17 +1676,24 @@ int Engine::donor_rest_init() {
   return 0;
 }
 
-int Engine::run_donors() {
+// Undo the previous call's holes, receptors and layers on the side stream
+// (after the call's start on the main stream); nothing before the donor
+// phase reads that state, and the donor phase waits for the side stream.
+int Engine::donor_reset_begin() {
   if (!donor_rest_) TB_TRY(donor_rest_init());
-  // undo the previous call's holes, receptors and layers
   TB_CUDA(it_rec_.ensure(1));
   TB_CUDA(it_cancel_.ensure(1));
-  k_donor_reset<<<148 * 16, kT, 0, stream_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p,
-                                                                   prev_nrec_, csr_off_.p, csr_cell_.p, iblank_.p,
-                                                                   m0_.p, m1_.p, iblank_cell_.p);
-  TB_LAUNCHED("k_donor_reset");
+  TB_CUDA(cudaEventRecord(dr_ev_, stream_));
+  TB_CUDA(cudaStreamWaitEvent(side_, dr_ev_, 0));
+  k_donor_reset<<<148 * 16, kT, 0, side_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p, prev_nrec_, csr_off_.p,
+                                            csr_cell_.p, iblank_.p, m0_.p, m1_.p, iblank_cell_.p);
+  TB_LAUNCHED_ON("k_donor_reset", side_);
   prev_nrec_ = 0;
-  TB_CUDA(cudaMemsetAsync(dcnt_.p, 0, 8 * sizeof(int), stream_));
+  TB_CUDA(cudaMemsetAsync(dcnt_.p, 0, 8 * sizeof(int), side_));
+  return 0;
+}
+
+int Engine::run_donors() {
   // candidate slots: one per (receptor node, donor block)
   if (nq_ > 0) {
     k_fill_slots<<<grid_for(nq_, kT), kT, 0, stream_>>>(qnode_.p, qdon_.p, qcell_.p, nq_, K_, ntot_, ctot_,
@@ -1786,10 +1800,6 @@ int Engine::run_donors() {
     TB_LAUNCHED("k_iblank_final");
   }
   prev_nrec_ = R;
-  // back to rest for the next call: slots, cancel marks
-  k_donor_clear<<<grid_for(std::max<long long>(nq_, 1), kT), kT, 0, stream_>>>(
-      qnode_.p, qdon_.p, qcell_.p, nq_, K_, d_bi_.p, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
-  TB_LAUNCHED("k_donor_clear");
   return 0;
 }
 
@@ -1919,15 +1929,20 @@ int Engine::reduce_fringes() {
 }
 
 int Engine::run_celliblank() {
-  // cells around the holes and the final receptors (all others are 1), on
-  // the side stream while the main stream copies the node iblanks out;
-  // download_iblank waits for them before it copies the cell iblanks
+  // cells around the holes and the final receptors (all others are 1), then
+  // the donor slots and cancel marks back to rest, on the side stream while
+  // the main stream copies the node iblanks out; download_iblank waits for
+  // them before it copies the cell iblanks
   TB_CUDA(cudaEventRecord(cib_ev_[0], stream_));
   TB_CUDA(cudaStreamWaitEvent(side_, cib_ev_[0], 0));
   k_cell_iblank_sparse<<<148 * 16, kT, 0, side_>>>(mlist_.p, dcnt_.p, it_rec_.p, it_cancel_.p, rcount_.p,
                                                   csr_off_.p, csr_cell_.p, conn8_.p, cell_nv_.p, iblank_.p,
                                                   iblank_cell_.p);
   TB_LAUNCHED_ON("k_cell_iblank_sparse", side_);
+  // back to rest for the next call: slots, cancel marks
+  k_donor_clear<<<grid_for(std::max<long long>(nq_, 1), kT), kT, 0, side_>>>(
+      qnode_.p, qdon_.p, qcell_.p, nq_, K_, d_bi_.p, slot_.p, cmlist_.p, dcnt_.p, cmark_.p, reset_t_.p);
+  TB_LAUNCHED_ON("k_donor_clear", side_);
   TB_CUDA(cudaEventRecord(cib_ev_[1], side_));
   return 0;
 }
@@ -2010,6 +2025,11 @@ int Engine::connectivity() {
   TB_CUDA(cudaEventRecord(ev_[0], stream_));
   TB_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned long long), stream_));
   TB_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), stream_));  // this call's device errors only
+  // the side stream is idle unless the last call stopped early (its pinned
+  // staging is reused below); then the previous call's donor marks go back
+  // to rest on it, beside everything up to the donor phase
+  TB_CUDA(cudaStreamSynchronize(side_));
+  TB_TRY(donor_reset_begin());
   if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
   // The hole maps run on the side stream after the cell boxes (hev_[0],
@@ -2030,6 +2050,7 @@ int Engine::connectivity() {
     rc = run_queries();
     if (rc) return rc;
     TB_CUDA(cudaEventRecord(ev_[4], stream_));
+    TB_CUDA(cudaStreamWaitEvent(stream_, rf_ev_, 0));  // the refitted tree
     rc = run_search();
     if (rc) return rc;
   } else {

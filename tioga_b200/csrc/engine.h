@@ -355,6 +355,7 @@ class Engine {
   int build_tree_topology();
   int upload_coords();
   int check_coords();
+  int donor_reset_begin(); // side stream: the previous call's donor marks back to rest
   int holemaps_begin();    // side stream: wall bounds, map extents, wall-cell boxes, extents to the host
   int holemaps_end();      // host: map sizes; side stream: fill and final maps (joined before the donors)
   int preprocess_resolutions();
@@ -431,6 +432,8 @@ class Engine {
   cudaStream_t side_ = nullptr;
   cudaEvent_t hev_[3];
   cudaEvent_t cib_ev_[2];  // the cell iblanks on the side stream: start (main), done (side)
+  cudaEvent_t dr_ev_;      // call start (main): the previous call's donor marks go back to rest on the side stream
+  cudaEvent_t rf_ev_;      // the tree refit (side stream) is done: the traversal may start
   bool hm_pending_ = false;  // holemaps_begin ran and holemaps_end has not
   // pinned host staging of the hole maps (so the side stream's copies never
   // block the host): ordered-key initial bounds, extents read back, map views
