@@ -51,7 +51,7 @@ REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtioga_ref.so")
 PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 # DRAM bytes (read + write) of one k_cell_boxes launch per cell, from an ncu
 # capture on the full workload (profiles/k_cell_boxes_cfg1.md).
-CELL_BOX_DRAM_BYTES_PER_CELL = 2443511296 / 26961129  # 90.63 B
+CELL_BOX_DRAM_BYTES_PER_CELL = 2235169536 / 26961129  # 82.90 B
 
 
 def cell_box_bytes(system, st):
@@ -1218,7 +1218,8 @@ def main():
                                             "tuning", "gpu_launches", "clocks")}
         out["batched"]["config"] = b["config"]
         a3 = copy.copy(args)
-        a3.size, a3.seconds, a3.slots, a3.rates = "medium", 3.0, 16, ""
+        # the cfg3 stream itself (200 resident systems), 2 s per arrival rate
+        a3.size, a3.seconds, a3.slots, a3.rates, a3.nsys = "full", 2.0, 16, "", 200
         sv = run_gpu_serving(a3, ws, rank, local, Dist(1, None))
         out["served"] = {k: sv[k] for k in ("value", "unit", "latency_ms", "serving", "e2e", "clocks")}
         out["served"]["config"] = sv["config"]

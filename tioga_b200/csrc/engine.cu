@@ -776,7 +776,7 @@ int Engine::build_tree_topology() {
   TB_CUDA(cudaMemcpyAsync(tile_base_.p, h_tile_base_.data(), h_tile_base_.size() * sizeof(long long),
                           cudaMemcpyHostToDevice, stream_));
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
-  TB_CUDA(cbox_.ensure(2 * ctot_));
+  TB_CUDA(cbox_.ensure(3 * ctot_));
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   topo_gen_++;  // the cell arrays were replaced by their storage-order copies
   return 0;

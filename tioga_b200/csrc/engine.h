@@ -509,7 +509,7 @@ class Engine {
   DBuf<unsigned long long> wall_bb_;
   // tree
   DBuf<int> sorted_cell_;
-  DBuf<float4> cbox_;      // split form: 2 per sorted cell (FP32 box rounded outward)
+  DBuf<float2> cbox_;      // split form: 3 per sorted cell (FP32 box rounded outward, 24 bytes)
   DBuf<float4> lbox_;      // split form: 2 per leaf, in leaf order (its box, and its block in the 7th word)
   DBuf<int> pair_ext_;     // split form: 6 per pair, the seeds of the extents' bounds (fkey order)
   DBuf<float4> xf_;        // coordinates rounded to FP32, one per node (split-form cell boxes)

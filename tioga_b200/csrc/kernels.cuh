@@ -102,12 +102,12 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode,
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float2* cbox, float4* tnode,
                        float4* lbox);
 void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
-                       const float4* cbox, const float4* lbox, int* ext, unsigned long long* acc);
+                       const float2* cbox, const float4* lbox, int* ext, unsigned long long* acc);
 void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                         const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                         const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs, double* cbox64,
@@ -146,7 +146,7 @@ __global__ void k_query_write(const BlockInfo* bi, const PairInfo* pairs, int np
 // host launchers of the templated search stages (same translation unit as
 // their instantiations)
 void launch_traverse(int form, int variant, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const float2* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex);
 __global__ void k_gather_candidates(const int* slots, const int* ncand_q, const int* off, long long nq,

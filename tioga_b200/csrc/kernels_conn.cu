@@ -952,6 +952,15 @@ __device__ __forceinline__ void leaf_lane_load(const float4* __restrict__ lbox, 
   }
 }
 
+// A cell's FP32 box is three float2 (24 bytes): (lo.x, lo.y), (lo.z, hi.x),
+// (hi.y, hi.z); as the (lo.xyz, hi.x) / (hi.yz) pair of float4 the box tests
+// take.
+__device__ __forceinline__ void cell_box_load(const float2* __restrict__ cbox, long long c, float4& A, float4& B) {
+  const float2 a = cbox[3 * c], b = cbox[3 * c + 1], d = cbox[3 * c + 2];
+  A = make_float4(a.x, a.y, b.x, b.y);
+  B = make_float4(d.x, d.y, 0.f, 0.f);
+}
+
 // Cell pass of the split form, in three kernels.
 //
 // k_cell_boxes: leaf by leaf (32 / kMaxLeafCells leaves per warp, one lane per
@@ -967,7 +976,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restri
                                                           const int* __restrict__ conn8,
                                                           const unsigned char* __restrict__ cell_nv,
                                                           const int4* __restrict__ leaves, long long nleaf,
-                                                          float4* __restrict__ cbox, float4* __restrict__ tnode,
+                                                          float2* __restrict__ cbox, float4* __restrict__ tnode,
                                                           float4* __restrict__ lbox) {
   constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
   const int lane = threadIdx.x & 31;
@@ -998,8 +1007,9 @@ __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restri
       f[k + 3] = valid ? f_up(hi[k]) : -INFINITY;
     }
     if (valid) {
-      cbox[2 * c] = make_float4(f[0], f[1], f[2], f[3]);
-      cbox[2 * c + 1] = make_float4(f[4], f[5], 0.f, 0.f);
+      cbox[3 * c] = make_float2(f[0], f[1]);
+      cbox[3 * c + 1] = make_float2(f[2], f[3]);
+      cbox[3 * c + 2] = make_float2(f[4], f[5]);
     }
     for (int o = 1; o < LC; o <<= 1)
       for (int k = 0; k < 3; k++) {
@@ -1069,7 +1079,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pairs(
     const double* __restrict__ x, const int* __restrict__ conn8, const unsigned char* __restrict__ cell_nv,
     const BlockInfo* __restrict__ bi, const int4* __restrict__ leaves, const int4* __restrict__ chunks,
     const int* __restrict__ chunk_cta, int nchunks, const int* __restrict__ pfirst,
-    const PairInfo* __restrict__ pairs, const float4* __restrict__ cbox, const float4* __restrict__ lbox,
+    const PairInfo* __restrict__ pairs, const float2* __restrict__ cbox, const float4* __restrict__ lbox,
     const int* __restrict__ ext, unsigned long long* __restrict__ acc) {
   extern __shared__ unsigned long long s_dyn[];
   int cta, ncta;
@@ -1113,7 +1123,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pairs(
       float hh[3] = {0.f, 0.f, 0.f};
       if (valid) {
         nv = cell_nv[c];
-        const float4 A = cbox[2 * c], B = cbox[2 * c + 1];
+        float4 A, B;
+        cell_box_load(cbox, c, A, B);
         const float fb[6] = {A.x, A.y, A.z, A.w, B.x, B.y};
         for (int k = 0; k < 3; k++) {
           cc[k] = 0.5 * ((double)fb[k] + (double)fb[k + 3]);
@@ -1234,7 +1245,7 @@ static void set_smem(K kern, size_t smem) {
 }
 
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float4* cbox, float4* tnode,
+                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float2* cbox, float4* tnode,
                        float4* lbox) {
 #define TB_CB(MB) k_cell_boxes<MB><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode, lbox)
   if (minb <= 4) TB_CB(4);
@@ -1246,7 +1257,7 @@ void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, co
 void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,
-                       const float4* cbox, const float4* lbox, int* ext, unsigned long long* acc) {
+                       const float2* cbox, const float4* lbox, int* ext, unsigned long long* acc) {
   set_smem(k_leaf_seeds, smem);
   k_leaf_seeds<<<grid, 256, smem, st>>>(bi, chunks, chunk_cta, nchunks, pfirst, pairs, lbox, ext);
 #define TB_CPP(MB)                                                                                           \
@@ -1604,7 +1615,7 @@ __device__ __forceinline__ int pick4(int k, int a0, int a1, int a2, int a3) {
 // deepest non-empty mask.
 template <int FORM>
 __global__ void __launch_bounds__(256) k_traverse(
-    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float2* __restrict__ cbox,
     const double* __restrict__ cbox64, const float4* __restrict__ tnode, const double* __restrict__ tnode64,
     const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq, int* __restrict__ slots,
     int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap, unsigned* __restrict__ novf,
@@ -1649,9 +1660,7 @@ __global__ void __launch_bounds__(256) k_traverse(
         float4 A[kMaxLeafCells], B[kMaxLeafCells];
 #pragma unroll
         for (int j = 0; j < kMaxLeafCells; j++) {
-          const long long c = c0 + min(j, ncell - 1);
-          A[j] = cbox[2 * c];
-          B[j] = cbox[2 * c + 1];
+          cell_box_load(cbox, c0 + min(j, ncell - 1), A[j], B[j]);
         }
 #pragma unroll
         for (int j = 0; j < kMaxLeafCells; j++) hit |= (unsigned)(hit_ab(A[j], B[j], plo, phi) && j < ncell) << j;
@@ -1739,7 +1748,7 @@ __global__ void __launch_bounds__(256) k_traverse(
 // k_traverse, and every hit leaf's cells are tested, so each query gets the
 // same candidates (in another order, which the selection does not see).
 __global__ void __launch_bounds__(256) k_traverse_ww(
-    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float4* __restrict__ cbox,
+    const double* __restrict__ x, const BlockInfo* __restrict__ bi, const float2* __restrict__ cbox,
     const float4* __restrict__ tnode, const int* __restrict__ qnode, const int* __restrict__ qdon, long long nq,
     int* __restrict__ slots, int* __restrict__ ncand_q, int3* __restrict__ ovf, int ovf_cap,
     unsigned* __restrict__ novf, unsigned* __restrict__ err, int skip_uhex) {
@@ -1854,9 +1863,7 @@ __global__ void __launch_bounds__(256) k_traverse_ww(
         float4 A[kMaxLeafCells], B[kMaxLeafCells];
 #pragma unroll
         for (int j = 0; j < kMaxLeafCells; j++) {
-          const long long c = lf0 + min(j, lfn - 1);
-          A[j] = cbox[2 * c];
-          B[j] = cbox[2 * c + 1];
+          cell_box_load(cbox, lf0 + min(j, lfn - 1), A[j], B[j]);
         }
         unsigned hit = 0;
 #pragma unroll
@@ -2033,7 +2040,7 @@ __global__ void k_search_finish(const unsigned long long* __restrict__ qkey, con
 }
 
 void launch_traverse(int form, int variant, int blocks, cudaStream_t st, const double* x, const BlockInfo* bi,
-                     const float4* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
+                     const float2* cbox, const double* cbox64, const float4* tnode, const double* tnode64,
                      const int* qnode, const int* qdon, long long nq, int* slots, int* ncand_q, int3* ovf,
                      int ovf_cap, unsigned* novf, unsigned* err, int skip_uhex) {
   if (form == 1 && variant == 1)
