@@ -37,6 +37,8 @@ Engine::Engine() {
   for (auto& e : cib_ev_) cudaEventCreate(&e);
   cudaEventCreateWithFlags(&dr_ev_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&rf_ev_, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&up_, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&up_start_, cudaEventDisableTiming);
 }
 
 Engine::~Engine() {
@@ -52,6 +54,10 @@ Engine::~Engine() {
   for (auto& e : cib_ev_) cudaEventDestroy(e);
   cudaEventDestroy(dr_ev_);
   cudaEventDestroy(rf_ev_);
+  if (up_) cudaStreamSynchronize(up_);
+  for (auto& e : up_ev_) cudaEventDestroy(e);
+  cudaEventDestroy(up_start_);
+  if (up_) cudaStreamDestroy(up_);
   if (side_) cudaStreamDestroy(side_);
   if (h_hm_init_) cudaFreeHost(h_hm_init_);
   if (h_hm_info_) cudaFreeHost(h_hm_info_);
@@ -63,7 +69,7 @@ Engine::~Engine() {
   d_bi_.release(); d_pairs_.release(); d_npairs_.release(); d_hm_.release(); d_hmdev_.release();
   hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); xf_.release(); tnode_.release(); tnode64_.release();
-  leaves_.release(); lbox_.release(); pair_ext_.release(); gparent_.release(); gnk_.release();
+  leaves_.release(); lbox_.release(); pair_ext_.release(); gparent_.release(); gnk_.release(); up_leaf_ids_.release();
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
@@ -455,6 +461,94 @@ int Engine::upload_coords() {
   return check_coords();
 }
 
+// The leaves of each upload chunk: a leaf belongs to the chunk that holds its
+// largest vertex id, so its cell boxes can be made once that chunk has landed
+// (chunks land in order).  Leaf ids sorted by chunk, offsets on the host.
+int Engine::build_upload_chunks() {
+  const long long nl = nleaf_total_;
+  const int nch = (int)((ntot_ + kUpChunk - 1) / kUpChunk);
+  h_up_leaf_off_.assign(nch + 1, 0);
+  if (nl == 0 || nch == 0) return 0;
+  DBuf<int> key, id, key2;
+  TB_CUDA(key.ensure(nl));
+  TB_CUDA(id.ensure(nl));
+  TB_CUDA(key2.ensure(nl));
+  TB_CUDA(up_leaf_ids_.ensure(nl));
+  k_leaf_chunk<<<grid_for(nl, kT), kT, 0, stream_>>>(leaves_.p, nl, conn8_.p, cell_nv_.p, kUpChunk, key.p, id.p);
+  TB_LAUNCHED("k_leaf_chunk");
+  int hi_bit = 1;
+  while ((1 << hi_bit) < nch) hi_bit++;
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, id.p, up_leaf_ids_.p, (int)nl, 0, hi_bit, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, key.p, key2.p, id.p, up_leaf_ids_.p, (int)nl, 0, hi_bit,
+                                  stream_);
+  std::vector<int> hk(nl);
+  TB_CUDA(cudaMemcpyAsync(hk.data(), key2.p, nl * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  for (long long l = 0; l < nl; l++) h_up_leaf_off_[hk[l] + 1]++;
+  for (int k = 0; k < nch; k++) h_up_leaf_off_[k + 1] += h_up_leaf_off_[k];
+  return 0;
+}
+
+// Coordinates up in chunks on up_; as chunk k lands the main stream checks
+// it is finite, makes its FP32 copy and the cell boxes of chunk k's leaves
+// (k_cell_boxes over an id list), while the next chunks are in flight.  The
+// host reads the finite check once the last chunk is done, before any
+// kernel derives an index from a coordinate.
+int Engine::upload_chunked() {
+  const int nch = (int)h_up_leaf_off_.size() - 1;
+  while ((int)up_ev_.size() < nch) {
+    cudaEvent_t e;
+    TB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    up_ev_.push_back(e);
+  }
+  TB_CUDA(xf_.ensure(ntot_));
+  TB_CUDA(lbox_.ensure(2 * nleaf_total_));
+  TB_CUDA(coord_err_.ensure(1));
+  TB_CUDA(cudaMemsetAsync(coord_err_.p, 0, sizeof(unsigned), stream_));
+  TB_CUDA(cudaEventRecord(up_start_, stream_));
+  TB_CUDA(cudaStreamWaitEvent(up_, up_start_, 0));
+  for (int k = 0; k < nch; k++) {
+    const long long g0 = (long long)k * kUpChunk, g1 = std::min<long long>(ntot_, g0 + kUpChunk);
+    for (size_t b = 0; b < hb_.size(); b++) {
+      const long long o = bi_[b].node_off, e = o + hb_[b].nnodes;
+      const long long a = std::max(g0, o), z = std::min(g1, e);
+      if (a < z)
+        TB_CUDA(cudaMemcpyAsync(x_.p + 3 * a, hb_[b].hx + 3 * (a - o), 3 * (size_t)(z - a) * sizeof(double),
+                                cudaMemcpyHostToDevice, up_));
+    }
+    TB_CUDA(cudaEventRecord(up_ev_[k], up_));
+  }
+  const int mb = tune_.cell_box_per_sm;
+  for (int k = 0; k < nch; k++) {
+    const long long g0 = (long long)k * kUpChunk, g1 = std::min<long long>(ntot_, g0 + kUpChunk);
+    TB_CUDA(cudaStreamWaitEvent(stream_, up_ev_[k], 0));
+    k_check_finite<<<grid_for(3 * (g1 - g0), kT), kT, 0, stream_>>>(x_.p + 3 * g0, 3 * (g1 - g0), coord_err_.p);
+    TB_LAUNCHED("k_check_finite");
+    k_round_nodes<<<grid_for(g1 - g0, kT), kT, 0, stream_>>>(x_.p, g0, g1, xf_.p);
+    TB_LAUNCHED("k_round_nodes");
+    const long long l0 = h_up_leaf_off_[k], nl = h_up_leaf_off_[k + 1] - l0;
+    if (nl > 0) {
+      launch_cell_boxes(mb, (int)grid_for(nl * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p, cell_nv_.p,
+                        leaves_.p, up_leaf_ids_.p + l0, nl, cbox_.p, tnode_.p, lbox_.p);
+      TB_LAUNCHED("k_cell_boxes");
+    }
+  }
+  unsigned e = 0;
+  TB_CUDA(cudaMemcpyAsync(&e, coord_err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  if (e) {
+    fprintf(stderr, "#tioga_b200: a node coordinate is not finite (NaN or infinite)\n");
+    coords_on_device_ = false;
+    return -1;
+  }
+  coords_on_device_ = true;
+  gate_valid_ = false;  // the caller may have moved the nodes any way
+  boxes_ready_ = true;
+  return 0;
+}
+
 // Refuse non-finite coordinates before any kernel derives an index (hole-map
 // cells, Morton keys) from them.
 int Engine::check_coords() {
@@ -727,6 +821,7 @@ int Engine::build_tree_topology() {
     TB_CUDA(cudaStreamSynchronize(stream_));
     for (int b = nb - 1; b >= 0; b--)
       if (h_blk_leaf_[b] < 0) h_blk_leaf_[b] = h_blk_leaf_[b + 1];
+    TB_TRY(build_upload_chunks());
   }
   // cells (storage order) that mark their wall-bearing block's hole map
   {
@@ -1062,7 +1157,8 @@ int Engine::run_pairs_and_refit() {
   if (h_tile_base_.back() > 0) {
     k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
                                                                       node_order_.p,
-                                                                      precision_ != 0 ? xf_.p : nullptr);
+                                                                      precision_ != 0 && !boxes_ready_ ? xf_.p
+                                                                                                       : nullptr);
     TB_LAUNCHED("k_node_tiles");
   }
   TB_CUDA(cudaEventSynchronize(pev_));
@@ -1147,9 +1243,11 @@ int Engine::run_pairs_and_refit() {
   } else {
     const int mb = tune_.cell_box_per_sm;
     TB_CUDA(lbox_.ensure(2 * nleaf_total_));
-    launch_cell_boxes(mb, (int)grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p,
-                      cell_nv_.p, leaves_.p, nleaf_total_, cbox_.p, tnode_.p, lbox_.p);
-    TB_LAUNCHED("k_cell_boxes");
+    if (!boxes_ready_) {  // else made during the chunked upload
+      launch_cell_boxes(mb, (int)grid_for(nleaf_total_ * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p,
+                        cell_nv_.p, leaves_.p, nullptr, nleaf_total_, cbox_.p, tnode_.p, lbox_.p);
+      TB_LAUNCHED("k_cell_boxes");
+    }
     TB_CUDA(cudaEventRecord(hev_[0], stream_));  // the hole maps may start
     TB_CUDA(cudaEventRecord(cev_[2], stream_));
     launch_cell_pairs(tune_.cell_pass_per_sm, ccta.back(), smem, stream_, x_.p, conn8_.p, cell_nv_.p, d_bi_.p,
@@ -2030,7 +2128,11 @@ int Engine::connectivity() {
   // to rest on it, beside everything up to the donor phase
   TB_CUDA(cudaStreamSynchronize(side_));
   TB_TRY(donor_reset_begin());
-  if (!coords_resident_ || !coords_on_device_) TB_TRY(upload_coords());
+  boxes_ready_ = false;
+  if (!coords_resident_ || !coords_on_device_) {
+    if (precision_ != 0 && nleaf_total_ > 0 && h_up_leaf_off_.size() > 1) TB_TRY(upload_chunked());
+    else TB_TRY(upload_coords());
+  }
   TB_CUDA(cudaEventRecord(ev_[1], stream_));
   // The hole maps run on the side stream after the cell boxes (hev_[0],
   // recorded again after the box kernel), beside the latency-bound pair,

@@ -355,6 +355,8 @@ class Engine {
   int build_tree_topology();
   int upload_coords();
   int check_coords();
+  int build_upload_chunks();  // preprocess: the leaves of each upload chunk
+  int upload_chunked();       // coordinates up in chunks, the cell boxes made as they land
   int donor_reset_begin(); // side stream: the previous call's donor marks back to rest
   int holemaps_begin();    // side stream: wall bounds, map extents, wall-cell boxes, extents to the host
   int holemaps_end();      // host: map sizes; side stream: fill and final maps (joined before the donors)
@@ -434,6 +436,17 @@ class Engine {
   cudaEvent_t cib_ev_[2];  // the cell iblanks on the side stream: start (main), done (side)
   cudaEvent_t dr_ev_;      // call start (main): the previous call's donor marks go back to rest on the side stream
   cudaEvent_t rf_ev_;      // the tree refit (side stream) is done: the traversal may start
+  // Chunked upload (split form, coordinates not resident): the coordinates go
+  // up in chunks of kUpChunk global node ids on up_, and as each lands the
+  // main stream checks it, makes its FP32 copy and the cell boxes of the
+  // leaves whose last vertex it holds, beside the rest of the upload.
+  static constexpr int kUpChunk = 1 << 21;
+  cudaStream_t up_ = nullptr;
+  cudaEvent_t up_start_ = nullptr;
+  std::vector<cudaEvent_t> up_ev_;
+  DBuf<int> up_leaf_ids_;                 // leaf ids sorted by upload chunk
+  std::vector<long long> h_up_leaf_off_;  // chunk k's leaves: up_leaf_ids_[off[k] .. off[k + 1])
+  bool boxes_ready_ = false;              // this call's cell boxes were made during the upload
   bool hm_pending_ = false;  // holemaps_begin ran and holemaps_end has not
   // pinned host staging of the hole maps (so the side stream's copies never
   // block the host): ordered-key initial bounds, extents read back, map views

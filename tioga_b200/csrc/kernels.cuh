@@ -102,8 +102,11 @@ __global__ void k_pairs(const BlockInfo* bi, int nb, const int2* cand, int ncand
 __global__ void k_pair_finish(const BlockInfo* bi, PairInfo* pairs, int npairs,
                               const unsigned long long* acc);
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float2* cbox, float4* tnode,
-                       float4* lbox);
+                       const unsigned char* cell_nv, const int4* leaves, const int* ids, long long nleaf, float2* cbox,
+                       float4* tnode, float4* lbox);
+__global__ void k_leaf_chunk(const int4* leaves, long long nleaf, const int* conn8, const unsigned char* cell_nv,
+                             int chunk, int* key, int* id);
+__global__ void k_round_nodes(const double* x, long long lo, long long hi, float4* xf);
 void launch_cell_pairs(int minb, int grid, size_t smem, cudaStream_t st, const double* x, const int* conn8,
                        const unsigned char* cell_nv, const BlockInfo* bi, const int4* leaves, const int4* chunks,
                        const int* chunk_cta, int nchunks, const int* pfirst, const PairInfo* pairs,

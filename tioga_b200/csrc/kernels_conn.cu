@@ -970,12 +970,14 @@ __device__ __forceinline__ void cell_box_load(const float2* __restrict__ cbox, l
 // box outward (f_down/f_up cover every double that rounds onto a vertex) into
 // cbox, and the leaf's lanes write the union to the leaf's tree slot and,
 // with the leaf's block, to lbox (leaf order).  It holds nothing else, so it
-// runs at a high occupancy that hides the gathers.
+// runs at a high occupancy that hides the gathers.  With ids it takes only the
+// nleaf leaves listed there (those whose coordinates have been uploaded).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restrict__ xf,
                                                           const int* __restrict__ conn8,
                                                           const unsigned char* __restrict__ cell_nv,
-                                                          const int4* __restrict__ leaves, long long nleaf,
+                                                          const int4* __restrict__ leaves,
+                                                          const int* __restrict__ ids, long long nleaf,
                                                           float2* __restrict__ cbox, float4* __restrict__ tnode,
                                                           float4* __restrict__ lbox) {
   constexpr int LC = kMaxLeafCells, LPW = 32 / kMaxLeafCells;
@@ -983,8 +985,9 @@ __global__ void __launch_bounds__(256, MINB) k_cell_boxes(const float4* __restri
   const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long base = LPW * warp0; base < nleaf; base += LPW * nwarps) {
-    const long long leaf = base + lane / LC;
-    const bool leaf_ok = leaf < nleaf;
+    const long long li = base + lane / LC;
+    const bool leaf_ok = li < nleaf;
+    const long long leaf = (ids && leaf_ok) ? ids[li] : li;  // the leaves listed in ids, else all
     const int4 L = leaf_ok ? leaves[leaf] : make_int4(0, 0, 0, 0);  // first cell, cells, slot, block
     const bool valid = leaf_ok && lane % LC < L.y;
     const long long c = (long long)L.x + lane % LC;
@@ -1138,6 +1141,34 @@ __global__ void __launch_bounds__(256, MINB) k_cell_pairs(
   cell_pass_flush(s_acc, p0, CH.w, acc);
 }
 
+// Upload chunk of every leaf: the chunk (of `chunk` consecutive global node
+// ids) holding the largest vertex id of its cells, so the leaf's cell boxes
+// can be computed once that chunk has landed.
+__global__ void k_leaf_chunk(const int4* __restrict__ leaves, long long nleaf, const int* __restrict__ conn8,
+                             const unsigned char* __restrict__ cell_nv, int chunk, int* __restrict__ key,
+                             int* __restrict__ id) {
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nleaf;
+       l += (long long)gridDim.x * blockDim.x) {
+    const int4 L = leaves[l];
+    int vmax = 0;
+    for (int j = 0; j < L.y; j++) {
+      const long long c = (long long)L.x + j;
+      const int nv = cell_nv[c];
+      for (int m = 0; m < nv; m++) vmax = max(vmax, conn8[8 * c + m]);
+    }
+    key[l] = vmax / chunk;
+    id[l] = (int)l;
+  }
+}
+
+// FP32 copy (rounded to nearest) of the coordinates of nodes [lo, hi)
+__global__ void k_round_nodes(const double* __restrict__ x, long long lo, long long hi, float4* __restrict__ xf) {
+  for (long long i = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < hi;
+       i += (long long)gridDim.x * blockDim.x)
+    xf[i] = make_float4(__double2float_rn(x[3 * i]), __double2float_rn(x[3 * i + 1]), __double2float_rn(x[3 * i + 2]),
+                        0.f);
+}
+
 // Cell pass of the FP64 form, leaf by leaf (32 / kMaxLeafCells leaves per
 // warp, one lane per cell; chunk work items are leaves): the FP64 element
 // box of every cell (cbox64, exact) and of every leaf (tnode64), their FP32
@@ -1245,9 +1276,9 @@ static void set_smem(K kern, size_t smem) {
 }
 
 void launch_cell_boxes(int minb, int grid, cudaStream_t st, const float4* xf, const int* conn8,
-                       const unsigned char* cell_nv, const int4* leaves, long long nleaf, float2* cbox, float4* tnode,
-                       float4* lbox) {
-#define TB_CB(MB) k_cell_boxes<MB><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, nleaf, cbox, tnode, lbox)
+                       const unsigned char* cell_nv, const int4* leaves, const int* ids, long long nleaf, float2* cbox,
+                       float4* tnode, float4* lbox) {
+#define TB_CB(MB) k_cell_boxes<MB><<<grid, 256, 0, st>>>(xf, conn8, cell_nv, leaves, ids, nleaf, cbox, tnode, lbox)
   if (minb <= 4) TB_CB(4);
   else if (minb <= 6) TB_CB(6);
   else TB_CB(8);
