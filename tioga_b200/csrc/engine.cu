@@ -1381,6 +1381,8 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
   long long ovf_cap = std::max<long long>(cand_cap_, std::max<long long>(nq / 8, 1 << 16));
   unsigned novf = 0;
   count = 0;
+  // traversal and the scan of the per-query counts, then one read-back of
+  // the overflow count and the total; an overflow grows the list and repeats
   for (int attempt = 0; attempt < 2; attempt++) {
     TB_CUDA(ovf_.ensure(ovf_cap));
     TB_CUDA(cudaMemsetAsync(scount_.p, 0, sizeof(unsigned), stream_));
@@ -1389,18 +1391,17 @@ int Engine::traverse_and_gather(const double* xq, const int* qn, const int* qd, 
                     form == 0 ? cbox64_.p : nullptr, tnode_.p, form == 0 ? tnode64_.p : nullptr, qn, qd, nq,
                     slots_.p, ncand_q_.p, ovf_.p, (int)ovf_cap, scount_.p, err_.p, skip_uhex);
     TB_LAUNCHED("k_traverse");
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
+    TB_CUDA(cub_tmp_.ensure(tmp));
+    cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
     TB_CUDA(cudaMemcpyAsync(&novf, scount_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(&count, cand_off_.p + nq, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     TB_CUDA(cudaStreamSynchronize(stream_));
     cand_cap_ = ovf_cap;
     if ((long long)novf <= ovf_cap) break;
     ovf_cap = (long long)novf + novf / 4 + 1024;  // grow the overflow list and traverse again
   }
-  size_t tmp = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
-  TB_CUDA(cub_tmp_.ensure(tmp));
-  cub::DeviceScan::ExclusiveSum(cub_tmp_.p, tmp, ncand_q_.p, cand_off_.p, (int)(nq + 1), stream_);
-  TB_CUDA(cudaMemcpyAsync(&count, cand_off_.p + nq, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-  TB_CUDA(cudaStreamSynchronize(stream_));
   TB_CUDA(cand_.ensure(std::max(1u, count)));
   if (count > 0) {
     k_gather_candidates<<<grid_for(nq, kT), kT, 0, stream_>>>(slots_.p, ncand_q_.p, cand_off_.p, nq, ovf_.p,
@@ -2090,6 +2091,16 @@ int Engine::autotune(int reps) {
       {&tune_.candidates_per_sm, {8, 16, 32, 64}, &Timing::candidates},
   };
   reps = std::max(1, reps);
+  // Shapes are timed on device-resident coordinates (a first call uploads
+  // them): with an upload every call, the split form makes its cell boxes
+  // inside the chunked upload, where the box kernel's shape is not timed.
+  struct Restore {
+    int& flag;
+    int value;
+    ~Restore() { flag = value; }
+  } restore{coords_resident_, coords_resident_};
+  coords_resident_ = 1;
+  TB_TRY(connectivity());
   for (const Knob& k : knobs) {
     int best = *k.v;
     float tbest = 1e30f;
