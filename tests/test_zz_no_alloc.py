@@ -5,7 +5,7 @@ fields -- a solver stepping inside a captured CUDA graph, or one whose memory
 pool must not see cudaMalloc's device-wide synchronisation.  Checked through
 the C ABI against the regular data update (tioga_dataupdate_mb_) on the same
 connectivity, bit for bit, on two updates in a row in the row and the column
-layouts; the staging array is
+layouts, and on a third captured in a CUDA graph and replayed; the staging array is
 shared by all calls, so the second call also shows that nothing is left over
 from the first.  The file name sorts last so a stop-at-first-failure run has
 run every other test before this one.
@@ -91,6 +91,22 @@ def test_noalloc_matches_dataupdate_twice():
         torch.cuda.synchronize()
         got = d_q.cpu().numpy()
         assert np.array_equal(got.view(np.int64), expect.view(np.int64))
+    # inside a captured CUDA graph, the case the entry point exists for: a
+    # third update, captured once (after the eager calls above made the
+    # first-call set-up) and replayed, against the regular entry point's
+    t.dataupdate_mb(nvar, "row")
+    third = np.concatenate([q.copy() for q in qs])
+    graph = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(graph):
+        rcs.append(fn(d_inode.data_ptr(), d_w.data_ptr(), d_nw.data_ptr(), d_recv.data_ptr(), nrec,
+                      d_q.data_ptr(), off, nvar, 0, torch.cuda.current_stream().cuda_stream))
+    assert rcs == [0]
+    torch.cuda.synchronize()
+    assert np.array_equal(d_q.cpu().numpy().view(np.int64), second.view(np.int64))  # captured, not run
+    graph.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(d_q.cpu().numpy().view(np.int64), third.view(np.int64))
     # the column layout (q[k*nnodes+node]) against tioga_dataupdate_mb_'s, twice
     qc = [np.array(q, copy=True) for q in q0]  # read as column-layout arrays of each block
     for b, q in zip(system.blocks, qc):
