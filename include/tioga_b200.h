@@ -344,11 +344,13 @@ void tioga_b200_set_nodegid_merge_(int *on);
  * (MeshBlock::search_uniform_hex, src/search.C:271-341).  The high-order
  * point search keeps the tree for such blocks. */
 void tioga_b200_set_uniform_hex_flag_(int *btag, int *flag);
-/* For tests of the error paths: lower one device bound to *value (0 restores
- * it).  *which 0 = line passes of a hole-map fill (at the bound the fill stops and
- * error bit 8 is reported), 1 = donor-record capacity (error bit 2).  The
- * connectivity call then returns its error bits through
- * tioga_b200_last_error(); no counterpart in TIOGA. */
+/* For tests: lower one bound to *value (0 restores it).  *which 0 = line
+ * passes of a hole-map fill (at the bound the fill stops and error bit 8 is
+ * reported), 1 = donor-record capacity (error bit 2); the connectivity call
+ * then returns its error bits through tioga_b200_last_error().  2 = nodes
+ * per chunk of the split form's chunked coordinate upload (from the next
+ * preprocess), to run it over many chunks on small meshes.  No counterpart
+ * in TIOGA. */
 void tioga_b200_set_test_bound_(int *which, int *value);
 /* Device time (ms) of the last connectivity call per phase: [0] coordinate
  * upload, [1] hole maps, [2] box pairs + tree refit, [3] query gather,

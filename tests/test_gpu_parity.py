@@ -285,6 +285,26 @@ def test_traversal_variants_match_oracle(name, variant, oracle_lib):
     assert not problems, "\n".join(problems)
 
 
+@pytest.mark.parametrize("chunk", [4096, 65537])
+def test_chunked_upload_matches_oracle(chunk, oracle_lib):
+    """The split form uploads the coordinates in chunks and makes each chunk's
+    cell boxes as it lands.  With chunks far smaller than the default, cfg0's
+    background spans many chunks and a chunk spans the background's end and
+    the shell's start; the results equal the oracle's."""
+    import ctypes as C
+    system = CASES["cfg0"]()
+    q = cases.fields(system, nvar=3, seed=23)
+
+    def setup(t):
+        _gpu_setup(1)(t)
+        t.lib.tioga_b200_set_test_bound_(C.byref(C.c_int(2)), C.byref(C.c_int(chunk)))
+
+    ref = run_system(oracle_lib, system, q_blocks=q, nvar=3)
+    gpu = run_system(tb.library_path(), system, q_blocks=q, nvar=3, setup=setup)
+    problems = diff_runs(system, ref, gpu)
+    assert not problems, "\n".join(problems)
+
+
 def _reduce(t):
     t.lib.tioga_reduce_fringes_()
 

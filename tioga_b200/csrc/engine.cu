@@ -466,7 +466,7 @@ int Engine::upload_coords() {
 // (chunks land in order).  Leaf ids sorted by chunk, offsets on the host.
 int Engine::build_upload_chunks() {
   const long long nl = nleaf_total_;
-  const int nch = (int)((ntot_ + kUpChunk - 1) / kUpChunk);
+  const int nch = (int)((ntot_ + up_chunk_ - 1) / up_chunk_);
   h_up_leaf_off_.assign(nch + 1, 0);
   if (nl == 0 || nch == 0) return 0;
   DBuf<int> key, id, key2;
@@ -474,7 +474,7 @@ int Engine::build_upload_chunks() {
   TB_CUDA(id.ensure(nl));
   TB_CUDA(key2.ensure(nl));
   TB_CUDA(up_leaf_ids_.ensure(nl));
-  k_leaf_chunk<<<grid_for(nl, kT), kT, 0, stream_>>>(leaves_.p, nl, conn8_.p, cell_nv_.p, kUpChunk, key.p, id.p);
+  k_leaf_chunk<<<grid_for(nl, kT), kT, 0, stream_>>>(leaves_.p, nl, conn8_.p, cell_nv_.p, up_chunk_, key.p, id.p);
   TB_LAUNCHED("k_leaf_chunk");
   int hi_bit = 1;
   while ((1 << hi_bit) < nch) hi_bit++;
@@ -510,7 +510,7 @@ int Engine::upload_chunked() {
   TB_CUDA(cudaEventRecord(up_start_, stream_));
   TB_CUDA(cudaStreamWaitEvent(up_, up_start_, 0));
   for (int k = 0; k < nch; k++) {
-    const long long g0 = (long long)k * kUpChunk, g1 = std::min<long long>(ntot_, g0 + kUpChunk);
+    const long long g0 = (long long)k * up_chunk_, g1 = std::min<long long>(ntot_, g0 + up_chunk_);
     for (size_t b = 0; b < hb_.size(); b++) {
       const long long o = bi_[b].node_off, e = o + hb_[b].nnodes;
       const long long a = std::max(g0, o), z = std::min(g1, e);
@@ -522,7 +522,7 @@ int Engine::upload_chunked() {
   }
   const int mb = tune_.cell_box_per_sm;
   for (int k = 0; k < nch; k++) {
-    const long long g0 = (long long)k * kUpChunk, g1 = std::min<long long>(ntot_, g0 + kUpChunk);
+    const long long g0 = (long long)k * up_chunk_, g1 = std::min<long long>(ntot_, g0 + up_chunk_);
     TB_CUDA(cudaStreamWaitEvent(stream_, up_ev_[k], 0));
     k_check_finite<<<grid_for(3 * (g1 - g0), kT), kT, 0, stream_>>>(x_.p + 3 * g0, 3 * (g1 - g0), coord_err_.p);
     TB_LAUNCHED("k_check_finite");

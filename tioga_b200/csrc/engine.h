@@ -268,6 +268,7 @@ class Engine {
   int set_test_bound(int which, int value) {
     if (which == 0) test_fill_rounds_ = value;
     else if (which == 1) test_rcap_ = value;
+    else if (which == 2) up_chunk_ = value > 0 ? value : kUpChunk;  // takes effect at the next preprocess
     else return -1;
     return 0;
   }
@@ -441,6 +442,7 @@ class Engine {
   // main stream checks it, makes its FP32 copy and the cell boxes of the
   // leaves whose last vertex it holds, beside the rest of the upload.
   static constexpr int kUpChunk = 1 << 21;
+  int up_chunk_ = kUpChunk;  // the chunk size in use (smaller only in tests)
   cudaStream_t up_ = nullptr;
   cudaEvent_t up_start_ = nullptr;
   std::vector<cudaEvent_t> up_ev_;
