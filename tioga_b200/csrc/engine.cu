@@ -70,6 +70,7 @@ Engine::~Engine() {
   hm_state_.release();
   wall_bb_.release(); sorted_cell_.release(); cbox_.release(); xf_.release(); tnode_.release(); tnode64_.release();
   leaves_.release(); lbox_.release(); pair_ext_.release(); gparent_.release(); gnk_.release(); up_leaf_ids_.release();
+  up_tile_ids_.release();
   gnint_.release(); refit_start_.release(); refit_cnt_.release();
   mlist_.release(); cmlist_.release(); dcnt_.release(); node_bin_.release();
   cbox64_.release(); qnode_.release(); qdon_.release(); qcell_.release(); qres_.release();
@@ -491,6 +492,36 @@ int Engine::build_upload_chunks() {
   return 0;
 }
 
+// The node tiles of each upload chunk, as for the leaves: a tile's box can be
+// made once the chunk holding its largest node id has landed.
+int Engine::build_tile_chunks() {
+  const long long nt = h_tile_base_.empty() ? 0 : h_tile_base_.back();
+  const int nch = (int)((ntot_ + up_chunk_ - 1) / up_chunk_);
+  h_up_tile_off_.assign(nch + 1, 0);
+  if (nt == 0 || nch == 0) return 0;
+  DBuf<int> key, id, key2;
+  TB_CUDA(key.ensure(nt));
+  TB_CUDA(id.ensure(nt));
+  TB_CUDA(key2.ensure(nt));
+  TB_CUDA(up_tile_ids_.ensure(nt));
+  k_tile_chunk<<<grid_for(nt, kT), kT, 0, stream_>>>(d_bi_.p, (int)bi_.size(), tile_base_.p, node_order_.p,
+                                                     up_chunk_, key.p, id.p);
+  TB_LAUNCHED("k_tile_chunk");
+  int hi_bit = 1;
+  while ((1 << hi_bit) < nch) hi_bit++;
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, id.p, up_tile_ids_.p, (int)nt, 0, hi_bit, stream_);
+  TB_CUDA(cub_tmp_.ensure(tmp));
+  cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, key.p, key2.p, id.p, up_tile_ids_.p, (int)nt, 0, hi_bit,
+                                  stream_);
+  std::vector<int> hk(nt);
+  TB_CUDA(cudaMemcpyAsync(hk.data(), key2.p, nt * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  TB_CUDA(cudaStreamSynchronize(stream_));
+  for (long long i = 0; i < nt; i++) h_up_tile_off_[hk[i] + 1]++;
+  for (int k = 0; k < nch; k++) h_up_tile_off_[k + 1] += h_up_tile_off_[k];
+  return 0;
+}
+
 // Coordinates up in chunks on up_; as chunk k lands the main stream checks
 // it is finite, makes its FP32 copy and the cell boxes of chunk k's leaves
 // (k_cell_boxes over an id list), while the next chunks are in flight.  The
@@ -528,6 +559,14 @@ int Engine::upload_chunked() {
     TB_LAUNCHED("k_check_finite");
     k_round_nodes<<<grid_for(g1 - g0, kT), kT, 0, stream_>>>(x_.p, g0, g1, xf_.p);
     TB_LAUNCHED("k_round_nodes");
+    if (h_up_tile_off_.size() == h_up_leaf_off_.size()) {  // the tiles whose last node is in this chunk
+      const long long t0 = h_up_tile_off_[k], ntl = h_up_tile_off_[k + 1] - t0;
+      if (ntl > 0) {
+        k_node_tiles<<<(unsigned)ntl, 256, 0, stream_>>>(x_.p, d_bi_.p, (int)bi_.size(), tile_base_.p, tbox_.p,
+                                                         node_order_.p, nullptr, up_tile_ids_.p + t0);
+        TB_LAUNCHED("k_node_tiles");
+      }
+    }
     const long long l0 = h_up_leaf_off_[k], nl = h_up_leaf_off_[k + 1] - l0;
     if (nl > 0) {
       launch_cell_boxes(mb, (int)grid_for(nl * kMaxLeafCells, 256, 148 * mb), stream_, xf_.p, conn8_.p, cell_nv_.p,
@@ -546,6 +585,7 @@ int Engine::upload_chunked() {
   coords_on_device_ = true;
   gate_valid_ = false;  // the caller may have moved the nodes any way
   boxes_ready_ = true;
+  tiles_ready_ = h_up_tile_off_.size() == h_up_leaf_off_.size();
   return 0;
 }
 
@@ -872,6 +912,7 @@ int Engine::build_tree_topology() {
                           cudaMemcpyHostToDevice, stream_));
   TB_CUDA(tbox_.ensure(2 * std::max(1ll, h_tile_base_.back())));
   TB_CUDA(cbox_.ensure(3 * ctot_));
+  TB_TRY(build_tile_chunks());
   TB_CUDA(cudaStreamSynchronize(stream_));  // host tables above stay valid
   topo_gen_++;  // the cell arrays were replaced by their storage-order copies
   return 0;
@@ -1154,11 +1195,12 @@ int Engine::run_pairs_and_refit() {
   // form's cell boxes, the FP32 copy of the coordinates, while the host
   // waits for the pairs
   if (precision_ != 0) TB_CUDA(xf_.ensure(ntot_));
-  if (h_tile_base_.back() > 0) {
+  if (h_tile_base_.back() > 0 && !tiles_ready_) {  // (else made during the chunked upload)
     k_node_tiles<<<(unsigned)h_tile_base_.back(), 256, 0, stream_>>>(x_.p, d_bi_.p, nb, tile_base_.p, tbox_.p,
                                                                       node_order_.p,
                                                                       precision_ != 0 && !boxes_ready_ ? xf_.p
-                                                                                                       : nullptr);
+                                                                                                       : nullptr,
+                                                                      nullptr);
     TB_LAUNCHED("k_node_tiles");
   }
   TB_CUDA(cudaEventSynchronize(pev_));
@@ -2140,6 +2182,7 @@ int Engine::connectivity() {
   TB_CUDA(cudaStreamSynchronize(side_));
   TB_TRY(donor_reset_begin());
   boxes_ready_ = false;
+  tiles_ready_ = false;
   if (!coords_resident_ || !coords_on_device_) {
     if (precision_ != 0 && nleaf_total_ > 0 && h_up_leaf_off_.size() > 1) TB_TRY(upload_chunked());
     else TB_TRY(upload_coords());

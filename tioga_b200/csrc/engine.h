@@ -357,6 +357,7 @@ class Engine {
   int upload_coords();
   int check_coords();
   int build_upload_chunks();  // preprocess: the leaves of each upload chunk
+  int build_tile_chunks();    // preprocess: the node tiles of each upload chunk
   int upload_chunked();       // coordinates up in chunks, the cell boxes made as they land
   int donor_reset_begin(); // side stream: the previous call's donor marks back to rest
   int holemaps_begin();    // side stream: wall bounds, map extents, wall-cell boxes, extents to the host
@@ -448,7 +449,10 @@ class Engine {
   std::vector<cudaEvent_t> up_ev_;
   DBuf<int> up_leaf_ids_;                 // leaf ids sorted by upload chunk
   std::vector<long long> h_up_leaf_off_;  // chunk k's leaves: up_leaf_ids_[off[k] .. off[k + 1])
+  DBuf<int> up_tile_ids_;                 // node-tile ids sorted by upload chunk
+  std::vector<long long> h_up_tile_off_;  // chunk k's tiles: up_tile_ids_[off[k] .. off[k + 1])
   bool boxes_ready_ = false;              // this call's cell boxes were made during the upload
+  bool tiles_ready_ = false;              // and its node tiles' boxes
   bool hm_pending_ = false;  // holemaps_begin ran and holemaps_end has not
   // pinned host staging of the hole maps (so the side stream's copies never
   // block the host): ordered-key initial bounds, extents read back, map views

@@ -131,7 +131,9 @@ __global__ void k_group_nint(const float4* tnode, int g_root, int ngroups, int* 
 __global__ void k_refit_fused(const int* start, int nstart, const int* gparent, const int* nint, int g_root,
                               int* cnt, float4* tnode, double* tnode64);
 __global__ void k_node_tiles(const double* x, const BlockInfo* bi, int nb, const long long* tile_base,
-                             float4* tbox, const int* node_order, float4* xf);
+                             float4* tbox, const int* node_order, float4* xf, const int* ids);
+__global__ void k_tile_chunk(const BlockInfo* bi, int nb, const long long* tile_base, const int* node_order, int chunk,
+                             int* key, int* id);
 __global__ void k_morton_nodes(const double* x, const blk_t* node_blk, const BlockInfo* bi,
                                long long ntot, unsigned long long* key, int* val);
 __global__ void k_invert(const int* perm, long long n, int* inv);

@@ -1161,6 +1161,24 @@ __global__ void k_leaf_chunk(const int4* __restrict__ leaves, long long nleaf, c
   }
 }
 
+// Upload chunk of every node tile: the chunk holding the largest node id of
+// the tile (its kNodeTile Morton-ordered nodes), as for the leaves.
+__global__ void k_tile_chunk(const BlockInfo* __restrict__ bi, int nb, const long long* __restrict__ tile_base,
+                             const int* __restrict__ node_order, int chunk, int* __restrict__ key,
+                             int* __restrict__ id) {
+  const long long ntile = tile_base[nb];
+  for (long long T = blockIdx.x * (long long)blockDim.x + threadIdx.x; T < ntile;
+       T += (long long)gridDim.x * blockDim.x) {
+    const int b = block_of_tile(tile_base, nb, T);
+    const BlockInfo& B = bi[b];
+    const int t0 = (int)(T - tile_base[b]) * kNodeTile;
+    int vmax = 0;
+    for (int i = t0; i < min(t0 + kNodeTile, B.nnodes); i++) vmax = max(vmax, node_order[B.node_off + i]);
+    key[T] = vmax / chunk;
+    id[T] = (int)T;
+  }
+}
+
 // FP32 copy (rounded to nearest) of the coordinates of nodes [lo, hi)
 __global__ void k_round_nodes(const double* __restrict__ x, long long lo, long long hi, float4* __restrict__ xf) {
   for (long long i = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < hi;
@@ -1322,12 +1340,13 @@ void launch_cell_pass64(int minb, int grid, size_t smem, cudaStream_t st, const 
 // Bounding box of every tile of kNodeTile consecutive nodes of a block (FP32,
 // rounded outward), so the query gathering can skip tiles far from a region;
 // with xf, every node's coordinates rounded to nearest FP32 (k_cell_boxes).
+// With ids, one CTA per tile listed there (those whose nodes have landed).
 __global__ void __launch_bounds__(256) k_node_tiles(const double* __restrict__ x, const BlockInfo* __restrict__ bi,
                                                     int nb, const long long* __restrict__ tile_base,
                                                     float4* __restrict__ tbox, const int* __restrict__ node_order,
-                                                    float4* __restrict__ xf) {
+                                                    float4* __restrict__ xf, const int* __restrict__ ids) {
   __shared__ float sh[6][8];
-  const long long T = blockIdx.x;
+  const long long T = ids ? ids[blockIdx.x] : blockIdx.x;  // the tiles listed in ids, else all
   const int b = block_of_tile(tile_base, nb, T);
   const BlockInfo& B = bi[b];
   const int t0 = (int)(T - tile_base[b]) * kNodeTile;
